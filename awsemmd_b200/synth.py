@@ -1,0 +1,526 @@
+"""Seeded synthetic AWSEM systems (the workloads the engine is measured on).
+
+A chain is built the way the benchmark configurations describe it:
+
+* sequence i.i.d. uniform over the 20 amino acids;
+* C-alpha trace: self-avoiding random walk with 3.8 A virtual bonds,
+  CA-CA-CA angles ~ N(110 deg, 10 deg), dihedrals uniform in [-180, 180) deg,
+  rejection of any non-bonded CA pair (|i-j| >= 2) closer than 4 A;
+* CB (H-beta for glycine, 1.09 A) and O from local ideal geometry
+  (CA-CB 1.53 A, CA-O 2.40 A, O-CA(i+1) 2.76 A), CB on the side that gives
+  the L-chirality sign of the reference chi term (chi0 < 0);
+* secondary structure: random H/E/C segments of length 4-12, written as the
+  two ssweight columns (H -> 1 0, E -> 0 1, C -> 0 0);
+* fragment memories: for every 9-residue window, 20 memories that are copies
+  of the chain's own window with N(0, 1 A) noise on every CA/CB coordinate,
+  weight 1, gamma from ``uniform.gamma``.
+
+Systems are written in the reference's input formats: a LAMMPS data file for
+``atom_style awsemmd`` (``id molecule residue type q x y z``, types 1 CA,
+3 O, 4 CB, 5 H-beta; masses 27/14/28/60/2; harmonic bonds CA-CA 3.816,
+CA-O 2.40, O-CA 2.76, CA-CB 1.53, CA-HB 1.09 with K = 60), the sequence file,
+``ssweight``, a ``.mem`` list with ``.gro`` memory structures (nm), the
+parameter tables, and a ``fix_backbone_coeff.data`` that is the default
+parameter file with a ``[Fragment_Memory]`` section enabled.
+
+Seeds: configuration index * 1000 + replica id.
+"""
+from __future__ import annotations
+
+import math
+import os
+import shutil
+from dataclasses import dataclass, field
+
+import numpy as np
+
+AA = "ARNDCQEGHILKMFPSTWYV"
+THREE = {
+    "A": "ALA", "R": "ARG", "N": "ASN", "D": "ASP", "C": "CYS", "Q": "GLN", "E": "GLU",
+    "G": "GLY", "H": "HIS", "I": "ILE", "L": "LEU", "K": "LYS", "M": "MET", "F": "PHE",
+    "P": "PRO", "S": "SER", "T": "THR", "W": "TRP", "Y": "TYR", "V": "VAL",
+}
+MASSES = {1: 27.0, 2: 14.0, 3: 28.0, 4: 60.0, 5: 2.0}
+BOND_COEFFS = {1: (60.0, 3.816), 2: (60.0, 2.40), 3: (60.0, 2.76), 4: (60.0, 1.53), 5: (60.0, 1.09)}
+# pair_style vexcluded 2 3.5 3.5 and the pair_coeff lines of the shipped examples
+PAIR_STYLE = "2 3.5 3.5"
+PAIR_COEFFS = ["* * 0.0", "1 1 20.0 3.5 4.5", "1 4 20.0 3.5 4.5", "4 4 20.0 3.5 4.5", "3 3 20.0 3.5 3.5"]
+
+BOLTZ_REAL = 0.0019872067
+MVV2E_REAL = 48.88821291 * 48.88821291
+
+PARAM_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "params")
+PARAM_TABLES = ["anti_HB", "anti_NHB", "anti_one", "para_HB", "para_one", "gamma.dat",
+                "burial_gamma.dat", "uniform.gamma"]
+
+WINDOW = 9
+MEMS_PER_WINDOW = 20
+
+
+@dataclass
+class Chain:
+    seq: str
+    ca: np.ndarray          # (L,3)
+    cb: np.ndarray          # (L,3) H-beta position for glycine
+    o: np.ndarray           # (L,3)
+    ss: str                 # 'H','E','C' per residue
+    # memories: (W, MEMS_PER_WINDOW, WINDOW, 3) in A, already rounded to the
+    # .gro text precision; NaN for the CB of glycine
+    mem_ca: np.ndarray | None = None
+    mem_cb: np.ndarray | None = None
+    mem_text: list | None = None  # per window: list of per-memory per-residue (ca_txt, cb_txt)
+
+    @property
+    def length(self) -> int:
+        return len(self.seq)
+
+
+@dataclass
+class System:
+    chains: list
+    box: float
+    periodic: bool = False
+    velocities: np.ndarray | None = None   # (natoms,3) in A/fs, data-file atom order
+    temperature: float = 300.0
+    seed: int = 0
+    extra: dict = field(default_factory=dict)
+
+    @property
+    def n_res(self) -> int:
+        return sum(c.length for c in self.chains)
+
+    @property
+    def n_atoms(self) -> int:
+        return 3 * self.n_res
+
+
+# --------------------------------------------------------------------------
+# geometry
+
+def _nerf(a, b, c, bond, angle, torsion):
+    bc = c - b
+    bc /= np.linalg.norm(bc)
+    n = np.cross(b - a, bc)
+    nn = np.linalg.norm(n)
+    if nn < 1e-8:
+        n = np.cross(bc, np.array([1.0, 0.0, 0.0]) if abs(bc[0]) < 0.9 else np.array([0.0, 1.0, 0.0]))
+        nn = np.linalg.norm(n)
+    n /= nn
+    m = np.cross(n, bc)
+    d2 = np.array([-bond * math.cos(angle), bond * math.sin(angle) * math.cos(torsion),
+                   bond * math.sin(angle) * math.sin(torsion)])
+    return c + d2[0] * bc + d2[1] * m + d2[2] * n
+
+
+def ca_trace(L: int, rng: np.random.Generator, bond=3.8, min_dist=4.0) -> np.ndarray:
+    """Self-avoiding CA walk (non-bonded CA pairs >= min_dist)."""
+    ca = np.zeros((max(L, 3), 3))
+    ca[1] = [bond, 0.0, 0.0]
+    th = math.radians(rng.normal(110.0, 10.0))
+    ca[2] = ca[1] + bond * np.array([-math.cos(th), math.sin(th), 0.0])
+    k = 3
+    fails = 0
+    while k < L:
+        ok = False
+        for _ in range(60):
+            th = math.radians(rng.normal(110.0, 10.0))
+            tor = rng.uniform(-math.pi, math.pi)
+            p = _nerf(ca[k - 3], ca[k - 2], ca[k - 1], bond, th, tor)
+            d = np.linalg.norm(ca[: k - 1] - p, axis=1)
+            if d.min() >= min_dist:
+                ok = True
+                break
+        if ok:
+            ca[k] = p
+            k += 1
+            fails = 0
+        else:
+            fails += 1
+            k = max(3, k - 3 * fails)
+    return ca[:L].copy()
+
+
+def _local_frame(ca, i):
+    L = len(ca)
+    prev = ca[i - 1] if i > 0 else 2 * ca[0] - ca[1]
+    nxt = ca[i + 1] if i < L - 1 else 2 * ca[L - 1] - ca[L - 2]
+    b1 = ca[i] - prev
+    b2 = nxt - ca[i]
+    e1 = b1 / np.linalg.norm(b1)
+    e2 = b2 / np.linalg.norm(b2)
+    u = e1 - e2
+    nu = np.linalg.norm(u)
+    u = u / nu if nu > 1e-8 else np.cross(e1, [0.0, 0.0, 1.0])
+    n = np.cross(b1, b2)
+    nn = np.linalg.norm(n)
+    if nn < 1e-8:
+        n = np.cross(e1, [1.0, 0.0, 0.0] if abs(e1[0]) < 0.9 else [0.0, 1.0, 0.0])
+        nn = np.linalg.norm(n)
+    n = n / nn
+    return u, n, e2, nxt
+
+
+def place_beads(ca: np.ndarray, seq: str):
+    """CB/HB and O from local ideal geometry around the CA trace."""
+    L = len(ca)
+    cb = np.zeros_like(ca)
+    o = np.zeros_like(ca)
+    # O_i in the triangle CA_i, CA_{i+1}: |CA_i O| = 2.40, |O CA_{i+1}| = 2.76
+    d = 3.8
+    along = (2.40 ** 2 - 2.76 ** 2 + d ** 2) / (2 * d)
+    perp = math.sqrt(max(2.40 ** 2 - along ** 2, 0.0))
+    alpha = math.radians(52.0)
+    for i in range(L):
+        u, n, e2, nxt = _local_frame(ca, i)
+        sgn = 1.0 if i % 2 == 0 else -1.0
+        o[i] = ca[i] + along * e2 + perp * sgn * n
+        r = 1.09 if seq[i] == "G" else 1.53
+        cb[i] = ca[i] + r * (math.cos(alpha) * u - math.sin(alpha) * n)
+    return cb, o
+
+
+def _chi_sign_fix(ca, cb, o, seq):
+    """Flip CB across the CA plane where that brings chi (the reference chi
+    term's triple product) to the L side (negative)."""
+    an, bn, cn = 0.483, 0.703, -0.186
+    ap, bp, cp = 0.444, 0.235, 0.321
+    L = len(ca)
+    for i in range(1, L - 1):
+        n_i = an * ca[i - 1] + bn * ca[i] + cn * o[i - 1]
+        cp_i = ap * ca[i] + bp * ca[i + 1] + cp * o[i]
+        a = cp_i - ca[i]
+        b = ca[i] - n_i
+        c = ca[i] - cb[i]
+        chi = np.dot(np.cross(a, b), c) / (np.linalg.norm(a) * np.linalg.norm(b) * np.linalg.norm(c))
+        if chi > 0:
+            _, n, _, _ = _local_frame(ca, i)
+            v = cb[i] - ca[i]
+            cb[i] = ca[i] + v - 2.0 * np.dot(v, n) * n
+    return cb
+
+
+def ss_segments(L: int, rng: np.random.Generator) -> str:
+    out = []
+    while len(out) < L:
+        kind = "HEC"[rng.integers(0, 3)]
+        out.extend(kind * int(rng.integers(4, 13)))
+    return "".join(out[:L])
+
+
+def _fmt_nm(x_a: float) -> str:
+    return f"{x_a / 10.0:.5f}"
+
+
+def build_memories(ch: Chain, rng: np.random.Generator, n_per=MEMS_PER_WINDOW, win=WINDOW, sigma=1.0):
+    """Noisy copies of every window.  Coordinates are rounded to the .gro text
+    that gets written (nm, 5 decimals) and read back as float(text) * 10, the
+    same arithmetic the reference's .gro reader applies."""
+    L = ch.length
+    W = max(L - win + 1, 0)
+    mem_ca = np.zeros((W, n_per, win, 3))
+    mem_cb = np.full((W, n_per, win, 3), np.nan)
+    text = []
+    for w in range(W):
+        wt = []
+        for m in range(n_per):
+            noise_ca = rng.normal(0.0, sigma, size=(win, 3))
+            noise_cb = rng.normal(0.0, sigma, size=(win, 3))
+            rows = []
+            for r in range(win):
+                i = w + r
+                ca_txt = [_fmt_nm(v) for v in ch.ca[i] + noise_ca[r]]
+                mem_ca[w, m, r] = [float(t) * 10 for t in ca_txt]
+                cb_txt = None
+                if ch.seq[i] != "G":
+                    cb_txt = [_fmt_nm(v) for v in ch.cb[i] + noise_cb[r]]
+                    mem_cb[w, m, r] = [float(t) * 10 for t in cb_txt]
+                rows.append((ca_txt, cb_txt))
+            wt.append(rows)
+        text.append(wt)
+    ch.mem_ca, ch.mem_cb, ch.mem_text = mem_ca, mem_cb, text
+
+
+def make_chain(L: int, rng: np.random.Generator, memories=True) -> Chain:
+    seq = "".join(AA[k] for k in rng.integers(0, 20, size=L))
+    ca = ca_trace(L, rng)
+    cb, o = place_beads(ca, seq)
+    cb = _chi_sign_fix(ca, cb, o, seq)
+    ss = ss_segments(L, rng)
+    ch = Chain(seq=seq, ca=ca, cb=cb, o=o, ss=ss)
+    if memories:
+        build_memories(ch, rng)
+    return ch
+
+
+def _random_rotation(rng):
+    q = rng.normal(size=4)
+    q /= np.linalg.norm(q)
+    a, b, c, d = q
+    return np.array([
+        [a * a + b * b - c * c - d * d, 2 * (b * c - a * d), 2 * (b * d + a * c)],
+        [2 * (b * c + a * d), a * a - b * b + c * c - d * d, 2 * (c * d - a * b)],
+        [2 * (b * d - a * c), 2 * (c * d + a * b), a * a - b * b - c * c + d * d],
+    ])
+
+
+def pack_chains(chains, box: float, rng: np.random.Generator, min_dist=4.0, tries=200):
+    """Random rotation + translation of each chain, rejecting placements with
+    an inter-chain CA pair closer than min_dist."""
+    from scipy.spatial import cKDTree
+
+    placed = []
+    tree_pts = np.zeros((0, 3))
+    for ch in chains:
+        com = ch.ca.mean(axis=0)
+        for attempt in range(tries):
+            R = _random_rotation(rng)
+            shift = rng.uniform(-box / 2, box / 2, size=3)
+            new_ca = (ch.ca - com) @ R.T + shift
+            if len(tree_pts) == 0:
+                ok = True
+            else:
+                d, _ = cKDTree(tree_pts).query(new_ca, k=1)
+                ok = d.min() >= min_dist
+            if ok:
+                break
+        else:
+            raise RuntimeError("could not place chain without overlap")
+        for name in ("ca", "cb", "o"):
+            setattr(ch, name, (getattr(ch, name) - com) @ R.T + shift)
+        if ch.mem_ca is not None:
+            pass  # memories are internal distances only; orientation does not matter
+        tree_pts = np.vstack([tree_pts, ch.ca])
+        placed.append(ch)
+    return placed
+
+
+def atom_arrays(sys_: System):
+    """Data-file order: per residue CA, O, CB/HB.  Returns (x, type, mol, res)."""
+    xs, types, mols, ress = [], [], [], []
+    r = 0
+    for ci, ch in enumerate(sys_.chains):
+        for i in range(ch.length):
+            r += 1
+            xs += [ch.ca[i], ch.o[i], ch.cb[i]]
+            types += [1, 3, 5 if ch.seq[i] == "G" else 4]
+            mols += [ci + 1] * 3
+            ress += [r] * 3
+    return np.array(xs, dtype=np.float64), np.array(types, np.int32), np.array(mols, np.int32), np.array(ress, np.int32)
+
+
+def bond_list(sys_: System):
+    """(type, atom_i, atom_j) with 0-based atom indices in data-file order."""
+    bonds = []
+    base = 0
+    for ch in sys_.chains:
+        L = ch.length
+        for i in range(L):
+            a_ca, a_o, a_cb = base + 3 * i, base + 3 * i + 1, base + 3 * i + 2
+            bonds.append((2, a_ca, a_o))
+            bonds.append((5 if ch.seq[i] == "G" else 4, a_ca, a_cb))
+            if i < L - 1:
+                bonds.append((1, a_ca, base + 3 * (i + 1)))
+                bonds.append((3, a_o, base + 3 * (i + 1)))
+        base += 3 * L
+    return bonds
+
+
+def maxwell_velocities(types: np.ndarray, T: float, rng: np.random.Generator) -> np.ndarray:
+    """Gaussian velocities (A/fs), zero total momentum, scaled to T exactly
+    with 3N-3 degrees of freedom (LAMMPS compute temp)."""
+    m = np.array([MASSES[int(t)] for t in types])
+    v = rng.normal(size=(len(types), 3)) / np.sqrt(m)[:, None]
+    p = (m[:, None] * v).sum(axis=0) / m.sum()
+    v -= p
+    ke2 = (m[:, None] * v * v).sum() * MVV2E_REAL
+    dof = 3 * len(types) - 3
+    t_now = ke2 / (dof * BOLTZ_REAL)
+    return v * math.sqrt(T / t_now)
+
+
+def make_system(chain_lengths, box: float, seed: int, T=300.0, memories=True) -> System:
+    rng = np.random.default_rng(seed)
+    chains = [make_chain(L, rng, memories=memories) for L in chain_lengths]
+    if len(chains) > 1:
+        chains = pack_chains(chains, box, rng)
+    else:
+        com = chains[0].ca.mean(axis=0)
+        for name in ("ca", "cb", "o"):
+            setattr(chains[0], name, getattr(chains[0], name) - com)
+    s = System(chains=chains, box=box, temperature=T, seed=seed)
+    _, types, _, _ = atom_arrays(s)
+    s.velocities = maxwell_velocities(types, T, rng)
+    return s
+
+
+# --------------------------------------------------------------------------
+# benchmark configurations
+
+CONFIGS = {
+    0: dict(name="c0_1x100", chains=[100], box=300.0, steps=1000, T=300.0, dt=2.0, damp=500.0),
+    1: dict(name="c1_8x250", chains=[250] * 8, box=150.0, steps=1000, T=300.0, dt=2.0, damp=500.0),
+    2: dict(name="c2_160x250", chains=[250] * 160, box=320.0, steps=500, T=300.0, dt=2.0, damp=500.0,
+            skin=2.0, every=10),
+}
+
+
+def config_system(k: int, replica: int = 0, memories=True) -> System:
+    c = CONFIGS[k]
+    return make_system(c["chains"], c["box"], seed=k * 1000 + replica, T=c["T"], memories=memories)
+
+
+def replica_lengths(n=1024, lo=40, hi=500, seed=3000):
+    """Chain lengths of the batched-replica workload: uniform in [lo, hi]."""
+    rng = np.random.default_rng(seed)
+    return [int(x) for x in rng.integers(lo, hi + 1, size=n)]
+
+
+# --------------------------------------------------------------------------
+# writers (the reference's input formats)
+
+def coeff_text(k_fm=1.0, mem_file="frags.mem", gamma_file="uniform.gamma") -> str:
+    with open(os.path.join(PARAM_DIR, "fix_backbone_coeff.data")) as f:
+        base = f.read()
+    return base.rstrip("\n") + f"\n\n[Fragment_Memory]\n{k_fm}\n{mem_file}\n{gamma_file}\n"
+
+
+def write_system(sys_: System, outdir: str, with_fm=True) -> dict:
+    os.makedirs(outdir, exist_ok=True)
+    x, types, mols, ress = atom_arrays(sys_)
+    bonds = bond_list(sys_)
+    h = sys_.box / 2
+    lines = ["LAMMPS data file (synthetic AWSEM system)", "",
+             f"{len(x)} atoms", f"{len(bonds)} bonds", "0 angles", "0 dihedrals", "0 impropers", "",
+             "5 atom types", "5 bond types", "0 angle types", "0 dihedral types", "0 improper types", "",
+             f"{-h:.1f} {h:.1f} xlo xhi", f"{-h:.1f} {h:.1f} ylo yhi", f"{-h:.1f} {h:.1f} zlo zhi", "",
+             "Masses", ""]
+    lines += [f"{t} {MASSES[t]}" for t in range(1, 6)]
+    lines += ["", "Atoms", ""]
+    for i in range(len(x)):
+        lines.append(f"{i + 1} {mols[i]} {ress[i]} {types[i]} 0.0 {float(x[i, 0])!r} {float(x[i, 1])!r} {float(x[i, 2])!r}")
+    if sys_.velocities is not None:
+        lines += ["", "Velocities", ""]
+        v = sys_.velocities
+        for i in range(len(x)):
+            lines.append(f"{i + 1} {float(v[i, 0])!r} {float(v[i, 1])!r} {float(v[i, 2])!r}")
+    lines += ["", "Bond Coeffs", ""]
+    lines += [f"{t} {BOND_COEFFS[t][0]} {BOND_COEFFS[t][1]}" for t in range(1, 6)]
+    lines += ["", "Bonds", ""]
+    for b, (t, i, j) in enumerate(bonds):
+        lines.append(f"{b + 1} {t} {i + 1} {j + 1}")
+    with open(os.path.join(outdir, "data.awsem"), "w") as f:
+        f.write("\n".join(lines) + "\n")
+    with open(os.path.join(outdir, "protein.seq"), "w") as f:
+        f.write("\n".join(c.seq for c in sys_.chains) + "\n")
+    with open(os.path.join(outdir, "ssweight"), "w") as f:
+        for c in sys_.chains:
+            for s in c.ss:
+                f.write({"H": "1.0 0.0\n", "E": "0.0 1.0\n", "C": "0.0 0.0\n"}[s])
+    for t in PARAM_TABLES:
+        shutil.copy(os.path.join(PARAM_DIR, t), os.path.join(outdir, t))
+    with open(os.path.join(outdir, "fix_backbone_coeff.data"), "w") as f:
+        if with_fm:
+            f.write(coeff_text())
+        else:
+            with open(os.path.join(PARAM_DIR, "fix_backbone_coeff.data")) as g:
+                f.write(g.read())
+    if with_fm:
+        _write_memories(sys_, outdir)
+    return {"workdir": outdir, "data": "data.awsem", "coeff": "fix_backbone_coeff.data",
+            "seq": "protein.seq", "pair_style": PAIR_STYLE, "pair_coeffs": ";".join(PAIR_COEFFS)}
+
+
+def _write_memories(sys_: System, outdir: str):
+    memdir = os.path.join(outdir, "mems")
+    os.makedirs(memdir, exist_ok=True)
+    mem_lines = ["[Target]", "query", "", "[Memories]"]
+    res0 = 0
+    for ci, ch in enumerate(sys_.chains):
+        for w, wt in enumerate(ch.mem_text):
+            fname = f"mems/c{ci + 1:03d}_w{w + 1:04d}.gro"
+            rows = []
+            atom = 0
+            for m, mem in enumerate(wt):
+                for r, (ca_txt, cb_txt) in enumerate(mem):
+                    resnum = m * WINDOW + r + 1
+                    rn = THREE[ch.seq[w + r]]
+                    atom += 1
+                    rows.append(f"{resnum} {rn} CA {atom} {ca_txt[0]} {ca_txt[1]} {ca_txt[2]}")
+                    if cb_txt is not None:
+                        atom += 1
+                        rows.append(f"{resnum} {rn} CB {atom} {cb_txt[0]} {cb_txt[1]} {cb_txt[2]}")
+            with open(os.path.join(outdir, fname), "w") as f:
+                f.write(f"memory window {w + 1} of chain {ci + 1}\n{len(rows)}\n" + "\n".join(rows) + "\n0.0 0.0 0.0\n")
+            for m in range(len(wt)):
+                mem_lines.append(f"{fname} {res0 + w + 1} {m * WINDOW + 1} {WINDOW} 1")
+        res0 += ch.length
+    with open(os.path.join(outdir, "frags.mem"), "w") as f:
+        f.write("\n".join(mem_lines) + "\n")
+
+
+# --------------------------------------------------------------------------
+# beta-sheet test system: exercises the hydrogen-bond (all separation
+# classes below 45), P_AP (medium, long, parallel, inter-chain) and burial
+# branches that random-coil chains barely reach
+
+def _arc(p, q, n_inner: int, step: float, bulge: np.ndarray) -> np.ndarray:
+    """n_inner points on a circular arc from p to q (exclusive) with spacing
+    close to `step`, bulging towards `bulge`."""
+    c = np.linalg.norm(q - p)
+    s = (n_inner + 1) * step
+    # solve 2 R sin(t/2) = c, R t = s for t in (0, 2 pi)
+    lo, hi = 1e-6, 2 * math.pi - 1e-6
+    for _ in range(200):
+        t = 0.5 * (lo + hi)
+        if 2 * (s / t) * math.sin(t / 2) > c:
+            lo = t
+        else:
+            hi = t
+    R = s / t
+    e = (q - p) / c
+    b = bulge - np.dot(bulge, e) * e
+    b /= np.linalg.norm(b)
+    mid = 0.5 * (p + q)
+    h = R * math.cos(t / 2)
+    center = mid - h * b
+    u0 = (p - center) / R
+    w = np.cross(u0, (q - center) / R)
+    w /= np.linalg.norm(w)
+    v0 = np.cross(w, u0)
+    return np.array([center + R * (math.cos(a) * u0 + math.sin(a) * v0)
+                     for a in np.linspace(0, t, n_inner + 2)[1:-1]])
+
+
+def sheet_system(seed=7, T=300.0) -> System:
+    rng = np.random.default_rng(seed)
+    rise, gap, pleat = 3.3, 4.8, 0.9
+
+    def strand(n, x0, y, direction, z0=0.0):
+        return np.array([[x0 + direction * rise * k, y, z0 + pleat * (1 if k % 2 == 0 else -1)] for k in range(n)])
+
+    chains = []
+    # chain 1: strand(12) - turn(4) - strand(12) - loop(6) - strand(10), a three-stranded sheet
+    s1 = strand(12, 0.0, 0.0, +1)
+    s2 = strand(12, s1[-1, 0], gap, -1)
+    turn = _arc(s1[-1], s2[0], 4, 3.8, np.array([1.0, 0.0, 0.0]))
+    s3 = strand(10, s2[-1, 0] + 0.0, 2 * gap, +1)
+    loop = _arc(s2[-1], s3[0], 6, 3.8, np.array([-1.0, 0.0, 0.6]))
+    ca1 = np.vstack([s1, turn, s2, loop, s3])
+    # chain 2: strand parallel to s1 on the other side, plus a short tail
+    s4 = strand(12, 0.0, -gap, +1)
+    # chain 3: a strand antiparallel to s3 beyond it
+    s5 = strand(10, s3[-1, 0], 3 * gap, -1)
+    for ca in (ca1, s4, s5):
+        L = len(ca)
+        seq = "".join(AA[k] for k in rng.integers(0, 20, size=L))
+        seq = seq.replace("P", "V")  # keep prolines out of the sheet
+        cb, o = place_beads(ca, seq)
+        cb = _chi_sign_fix(ca, cb, o, seq)
+        ss = "".join("E" for _ in range(L))
+        ch = Chain(seq=seq, ca=ca, cb=cb, o=o, ss=ss)
+        build_memories(ch, rng)
+        chains.append(ch)
+    s = System(chains=chains, box=200.0, temperature=T, seed=seed)
+    _, types, _, _ = atom_arrays(s)
+    s.velocities = maxwell_velocities(types, T, rng)
+    return s

@@ -1,0 +1,1704 @@
+/* FP64 CPU restatement of AWSEM-MD's per-step force and energy evaluation.
+
+   ORACLE -- test infrastructure.  Only tests/, the package smoke check and
+   bench.py's CPU-baseline leg load this library, and only as the checker.
+
+   It restates, in plain loops over residue pairs (no neighbour list, no
+   caches), the reference algorithm of:
+     fix backbone      src/fix_backbone.cpp (adavtyan/awsemmd)
+     fragment memory   src/fragment_memory.cpp
+     pair vexcluded    src/pair_excluded_volume.cpp
+   for the terms enabled by the default parameter file plus fragment memory:
+   Chain, Chi, Rama (+Rama_P, SSWeight), ABC, Dssp_Hdrgn, P_AP, Water,
+   Burial, Helix, Fragment_Memory, Epsilon.  Each function cites the
+   reference lines it follows.  The LAMMPS pieces around the fix (harmonic
+   bonds, velocity Verlet, Langevin, units real) are restated from the LAMMPS
+   documentation; the Langevin noise uses the same counter-based uniform
+   stream as the GPU engine (SplitMix64 finaliser keyed by seed, step, atom
+   id and component).
+
+   The restatement is checked against the reference compiled against the
+   LAMMPS-API shim (oracle/_ref) on the same inputs. */
+#include "awsem_oracle.h"
+
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <map>
+#include <sstream>
+#include <stdexcept>
+#include <string>
+#include <vector>
+#include <algorithm>
+
+namespace {
+
+const double BOLTZ = 0.0019872067;
+const double MVV2E = 48.88821291 * 48.88821291;
+const double FTM2V = 1.0 / 48.88821291 / 48.88821291;
+
+const char AA[] = "ARNDCQEGHILKMFPSTWYV";
+
+int aa_index(char c)
+{
+  for (int k = 0; k < 20; k++)
+    if (AA[k] == c) return k;
+  return 0;  // the reference maps unknown letters to 0 (se_map, fix_backbone.cpp:55)
+}
+
+/* four residue classes of Gamma_Array (fragment_memory.cpp:28): 1 SHL,
+   2 AHL, 3 BAS, 4 HPB, indexed by the AA order above */
+int four_class(int t)
+{
+  static const int m[20] = {1, 3, 2, 2, 4, 2, 2, 1, 3, 4, 4, 3, 4, 4, 1, 1, 1, 4, 4, 4};
+  return m[t];
+}
+
+inline uint64_t mix64(uint64_t z)
+{
+  z += 0x9E3779B97F4A7C15ULL;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+  return z ^ (z >> 31);
+}
+inline double uniform01(uint64_t seed, int64_t step, int64_t tag, int comp)
+{
+  uint64_t key = mix64(seed ^ mix64((uint64_t) step));
+  uint64_t r = mix64(key ^ ((uint64_t) tag * 4ULL + (uint64_t) comp));
+  return (double) (r >> 11) * (1.0 / 9007199254740992.0);
+}
+
+std::vector<std::string> words(const std::string &s)
+{
+  std::istringstream is(s);
+  std::vector<std::string> v;
+  std::string t;
+  while (is >> t) v.push_back(t);
+  return v;
+}
+
+std::string join(const std::string &dir, const std::string &f)
+{
+  if (f.empty() || f[0] == '/' || dir.empty()) return f;
+  return dir + "/" + f;
+}
+
+enum { ET_TOTAL = 0, ET_CHAIN, ET_SHAKE, ET_CHI, ET_RAMA, ET_VEXCLUDED, ET_DSSP, ET_PAP, ET_WATER,
+       ET_BURIAL, ET_HELIX, ET_AMHGO, ET_FRAGMEM, ET_VFRAGMEM, ET_CONT_REST, ET_MEMB, ET_SSB, ET_DH, NET };
+
+struct Params {
+  double epsilon = 1.0;
+  bool abc = 0, chain = 0, chi = 0, rama = 0, rama_p = 0, ssw = 0, dssp = 0, pap = 0, water = 0,
+       burial = 0, helix = 0, fm = 0;
+  // defaults of fix_backbone.cpp:136-143
+  double an = 0.4831806, bn = 0.7032820, cn = -0.1864262;
+  double ap = 0.4436538, bp = 0.2352006, cp = 0.3211455;
+  double ah = 0.8409657, bh = 0.8929599, ch = -0.7338894;
+  double k_chain[3] = {0, 0, 0}, r_ncb0 = 0, r_cpcb0 = 0, r_ncp0 = 0;
+  double k_chi = 0, chi0 = 0;
+  double k_rama = 0;
+  int n_rama = 0, n_rama_p = 0;
+  static const int i_rp = 6;
+  double w[12] = {0}, sigma[12] = {0}, phiw[12] = {0}, phi0[12] = {0}, psiw[12] = {0}, psi0[12] = {0};
+  bool ssweight[12] = {0};
+  double hbscl[4][9] = {{0}};
+  double sigma_NO = 0, sigma_HO = 0, NO_zero = 0, HO_zero = 0, k_dssp = 0, dssp_cut = 0, dssp_cut_sq = 0;
+  double pref[2] = {0, 0}, d_nu0 = 0, nu_cut1_sq = 0, nu_cut2_sq = 0, sigma_NO_sqinv = 0, sigma_HO_sqinv = 0;
+  double k_global_pap = 0, k_betapred_pap = 0, k_pap[3] = {0, 0, 0}, pap_cut = 0, pap_pref = 0,
+         pap_cutoff_sq = 0;
+  int i_med_min = 0, i_med_max = 0, i_diff_pap = 0;
+  double k_water = 0, water_kappa = 0, water_kappa_sigma = 0, treshold = 0;
+  int contact_cutoff = 0, n_wells = 0, well_flag[5] = {0};
+  double well_rmin[5] = {0}, well_rmax[5] = {0};
+  double k_burial = 0, burial_kappa = 0, burial_ro_min[3] = {0}, burial_ro_max[3] = {0};
+  double k_helix = 0, helix_gamma_p = 0, helix_gamma_w = 0, helix_kappa = 0, helix_kappa_sigma = 0,
+         helix_treshold = 0, helix_cutoff = 0, helix_cutoff_sq = 0;
+  int helix_i_diff = 0, pro_acc_flag = 0;
+  double helix_rmin = 0, helix_rmax = 0, h4prob[20] = {0}, h4prob_pro = 0;
+  double helix_sigma_HO = 0, helix_sigma_NO = 0, helix_HO_zero = 0, helix_NO_zero = 0,
+         helix_sigma_HO_sqinv = 0, helix_sigma_NO_sqinv = 0;
+  double k_fm = 0, fm_sigma_exp = 0.15;
+  std::string fm_file, fm_gamma_file;
+  double m_anti_HB[20][20][2], m_anti_NHB[20][20][2], m_para_HB[20][20][2], m_para_one[20], m_anti_one[20];
+  double water_gamma[5][20][20][2];
+  double burial_gamma[20][3];
+  // derived well supports (smart_matrix_lib.h:363-368)
+  double w_rmin_th[5], w_rmax_th[5], w_rmin_sq[5], w_rmax_sq[5];
+  double h_rmin_th, h_rmax_th, h_rmin_sq, h_rmax_sq;
+  double pap_drmin_sq, pap_drmax_sq;
+};
+
+/* Gamma_Array (fragment_memory.cpp:275-454) */
+struct GammaArray {
+  int nseq_cl = 0, nres_cl = 0;
+  bool frag_resty = false;
+  int i_sep[10];
+  std::vector<double> g;
+
+  int min_sep() const { return i_sep[0]; }
+  int max_sep() const { return i_sep[nseq_cl]; }
+
+  void idx_list(const std::string &t, std::vector<int> &out)
+  {
+    out.clear();
+    if (t == "ALL") {
+      for (int i = 0; i < nres_cl; i++) out.push_back(i);
+    } else if (t.size() == 1) {
+      if (nres_cl < 20) throw std::runtime_error("gamma file: residue code needs 20 classes");
+      out.push_back(aa_index(t[0]));
+    } else if (t.size() == 3) {
+      int c = t == "SHL" ? 1 : t == "AHL" ? 2 : t == "BAS" ? 3 : t == "HPB" ? 4 : 0;
+      if (!c) throw std::runtime_error("gamma file: unknown residue class " + t);
+      if (nres_cl == 4) out.push_back(c - 1);
+      else
+        for (int i = 0; i < 20; i++)
+          if (four_class(i) == c) out.push_back(i);
+    } else
+      throw std::runtime_error("gamma file: bad residue code " + t);
+  }
+
+  void load(const std::string &path)
+  {
+    std::ifstream in(path);
+    if (!in) throw std::runtime_error("Fragment_Memory: Cannot read gamma file " + path);
+    std::vector<std::vector<std::string>> rows;
+    std::string line;
+    bool first = true;
+    while (std::getline(in, line)) {
+      if (!line.empty() && line[0] == '#') continue;
+      auto v = words(line);
+      if (v.empty()) continue;
+      if (first) {
+        int ns = 0;
+        for (auto &t : v) {
+          ns++;
+          if (t == "inf") {
+            i_sep[ns - 1] = -1;
+            break;
+          }
+          i_sep[ns - 1] = atoi(t.c_str());
+        }
+        nseq_cl = ns - 1;
+        if (nseq_cl == 0) throw std::runtime_error("gamma file: no separation classes");
+        first = false;
+        continue;
+      }
+      if (v.size() != 4 && v.size() != 6) throw std::runtime_error("gamma file: bad entry");
+      rows.push_back(v);
+    }
+    if (rows.empty()) throw std::runtime_error("gamma file: no entries");
+    frag_resty = rows[0].size() == 6;
+    for (auto &r : rows) {
+      if ((r.size() == 6) != frag_resty) throw std::runtime_error("gamma file: mixed entry forms");
+      for (size_t k = 0; k + 2 < r.size(); k++) {
+        const std::string &t = r[k];
+        if (t == "ALL") nres_cl = std::max(nres_cl, 1);
+        else if (t.size() == 3) nres_cl = std::max(nres_cl, 4);
+        else if (t.size() == 1) nres_cl = std::max(nres_cl, 20);
+      }
+    }
+    int n2 = nres_cl * nres_cl;
+    g.assign((size_t) nseq_cl * (frag_resty ? n2 * n2 : n2), 0.0);
+    std::vector<int> is, js, ks, ls;
+    for (auto &r : rows) {
+      if (!frag_resty) {
+        int cl = atoi(r[2].c_str());
+        double gm = atof(r[3].c_str());
+        idx_list(r[0], is);
+        idx_list(r[1], js);
+        for (int a : is)
+          for (int b : js) {
+            g[(size_t) (cl - 1) * n2 + a * nres_cl + b] = gm;
+            g[(size_t) (cl - 1) * n2 + b * nres_cl + a] = gm;
+          }
+      } else {
+        // the reference passes the i-fragment class twice (fragment_memory.cpp:369)
+        int cl = atoi(r[4].c_str());
+        double gm = atof(r[5].c_str());
+        idx_list(r[0], is);
+        idx_list(r[1], js);
+        idx_list(r[2], ks);
+        idx_list(r[2], ls);
+        size_t base = (size_t) (cl - 1) * n2 * n2;
+        for (int a : is)
+          for (int b : js)
+            for (int c : ks)
+              for (int d : ls) {
+                g[base + ((size_t) a * nres_cl + b) * n2 + c * nres_cl + d] = gm;
+                g[base + ((size_t) b * nres_cl + a) * n2 + c * nres_cl + d] = gm;
+                g[base + ((size_t) a * nres_cl + b) * n2 + d * nres_cl + c] = gm;
+                g[base + ((size_t) b * nres_cl + a) * n2 + d * nres_cl + c] = gm;
+              }
+      }
+    }
+  }
+
+  /* getGamma, fragment_memory.cpp:400-454 */
+  double get(int ti, int tj, int tfi, int tfj, int ires, int jres) const
+  {
+    int dij = abs(ires - jres);
+    if (dij < i_sep[0] || (i_sep[nseq_cl] != -1 && dij > i_sep[nseq_cl])) return 0.0;
+    int cl;
+    for (cl = 1; cl < nseq_cl && dij >= i_sep[cl]; cl++) {}
+    if (nres_cl == 1) return g[cl - 1];
+    auto c = [&](int t) { return nres_cl == 4 ? four_class(t) - 1 : t; };
+    int n2 = nres_cl * nres_cl;
+    if (!frag_resty) return g[(size_t) (cl - 1) * n2 + c(ti) * nres_cl + c(tj)];
+    return g[(size_t) (cl - 1) * n2 * n2 + ((size_t) c(ti) * nres_cl + c(tj)) * n2 + c(tfi) * nres_cl + c(tfj)];
+  }
+};
+
+/* one fragment memory (fragment_memory.cpp:34-176): residues pos..pos+len-1
+   of the target, CA/CB coordinates read from a .gro file (nm -> A) */
+struct Memory {
+  int pos, len;
+  double weight;
+  std::string se;
+  std::vector<double> rf0, rf1;  // [len*len]: CA-CA (i<j) / CB-CB (i>j); CA_i-CB_j
+
+  double R(const double *a, const double *b) const
+  {
+    return sqrt((a[0] - b[0]) * (a[0] - b[0]) + (a[1] - b[1]) * (a[1] - b[1]) + (a[2] - b[2]) * (a[2] - b[2]));
+  }
+
+  /* Rf(ires, iatom, jres, jatom), fragment_memory.cpp:190-202; atom 1 CA, 2 CB */
+  double rf(int ires, int iat, int jres, int jat) const
+  {
+    ires -= pos;
+    jres -= pos;
+    if (iat == 1 && jat == 1) return rf0[std::min(ires, jres) * len + std::max(ires, jres)];
+    if (iat == 2 && jat == 2) return rf0[std::max(ires, jres) * len + std::min(ires, jres)];
+    return iat == 1 ? rf1[ires * len + jres] : rf1[jres * len + ires];
+  }
+};
+
+char three_to_one(const std::string &t)
+{
+  static const char *names[20] = {"ALA", "ARG", "ASN", "ASP", "CYS", "GLN", "GLU", "GLY", "HIS", "ILE",
+                                  "LEU", "LYS", "MET", "PHE", "PRO", "SER", "THR", "TRP", "TYR", "VAL"};
+  for (int k = 0; k < 20; k++)
+    if (t == names[k]) return AA[k];
+  return '?';
+}
+
+struct System {
+  std::string workdir;
+  Params P;
+  GammaArray G;
+  std::vector<Memory> mems;
+  std::vector<std::vector<int>> fm_map;  // per residue: memories listing it
+
+  // topology
+  int natoms = 0, n = 0, nch = 0;
+  std::vector<int> ch_pos1, ch_len;  // 1-based first residue, length
+  std::string se;
+  std::vector<int> ca, cb, o;  // atom index per residue (cb = CB or H-beta)
+  std::vector<int> chain_of;   // 0-based chain of residue
+  std::vector<double> aps[12];
+  std::vector<int> atype, amol, ares, tag;
+  std::vector<double> mass;  // by type
+  // bonds
+  std::vector<int> b_t, b_i, b_j;
+  std::vector<double> bk, br0;
+  std::vector<std::vector<int>> special;
+  // pair vexcluded
+  int ev_p = 2;
+  double ev_cs_glob = 0, ev_cl_glob = 0;
+  std::vector<double> ev_lambda, ev_cs, ev_cl;  // [(ntypes+1)^2]
+  std::vector<int> ev_set;
+  int ntypes = 0;
+
+  // per-step working arrays
+  std::vector<double> xca, xcb, xo, xn, xh, xcp;  // [n*3]
+  std::vector<double> rho_w, rho_h, sig_w, sigp_w, sig_h, sigp_h, xi_w, xi1, xi2, bur;
+  double E[NET];
+  double e_pair = 0, e_bond = 0;
+  unsigned long long sel_count[2];
+  unsigned long long sel_hash;
+
+  bool first(int i) const { return ch_pos1[chain_of[i]] == i + 1; }
+  bool last(int i) const { return ch_pos1[chain_of[i]] + ch_len[chain_of[i]] - 1 == i + 1; }
+  int type_of(int i) const { return aa_index(se[i]); }
+  int contact_atom(int i) const { return se[i] == 'G' ? ca[i] : cb[i]; }
+
+  void read_coeff(const std::string &path);
+  void read_tables();
+  void read_data(const std::string &path);
+  void read_seq(const std::string &path);
+  void read_mems();
+  void pair_setup(const std::string &style, const std::string &coeffs);
+  void compute(const double *x, double *f);
+  void backbone_atoms(const double *x);
+  void chain_term(int i, double *f);
+  void chi_term(int i, double *f);
+  void rama_term(int i, double *f);
+  void dihedral_slopes(int i, int iang, double &angle, double ys[5][3], double xs[5][3]);
+  void dssp_term(int i, int j, double *f);
+  void pap_nu(int i, int j, double &nu, double &prd);
+  void pap_term(int i, int j, double *f);
+  void helix_pair(int i, int j, double *f);
+  void fm_term(int i, double *f);
+  void pair_terms(const double *x, double *f);
+  void excluded_volume(const double *x, double *f);
+  void bonds(const double *x, double *f);
+};
+
+/* coefficient file: section loop and epsilon scaling, fix_backbone.cpp:164-516 */
+void System::read_coeff(const std::string &path)
+{
+  std::ifstream in(path);
+  if (!in) throw std::runtime_error("Coefficient file was not found!");
+  Params &p = P;
+  std::string s;
+  static const char *unsupported[] = {"[Shake]", "[Excluded]", "[Excluded_P]", "[Excluded_R6]", "[AMH-Go]",
+                                      "[Fragment_Memory_Table]", "[Contact_Restraints]",
+                                      "[Vector_Fragment_Memory]", "[Solvent_Barrier]", "[Membrane]",
+                                      "[Fragment_Frustratometer]", "[Tertiary_Frustratometer]",
+                                      "[Nmer_Frustratometer]", "[Phosphorylation]", "[Amylometer]",
+                                      "[Selection_Temperature]", "[Monte_Carlo_Seq_Opt]", "[Optimization]",
+                                      "[Burial_Optimization]", "[DebyeHuckel]", "[DebyeHuckel_Optimization]",
+                                      "[Shuffler]", "[Mutate_Sequence]"};
+  while (in >> s) {
+    if (s == "[ABC]") {
+      p.abc = 1;
+      in >> p.an >> p.bn >> p.cn >> p.ap >> p.bp >> p.cp >> p.ah >> p.bh >> p.ch;
+    } else if (s == "[Chain]") {
+      p.chain = 1;
+      in >> p.k_chain[0] >> p.k_chain[1] >> p.k_chain[2] >> p.r_ncb0 >> p.r_cpcb0 >> p.r_ncp0;
+    } else if (s == "[Chi]") {
+      p.chi = 1;
+      in >> p.k_chi >> p.chi0;
+    } else if (s == "[Rama]") {
+      p.rama = 1;
+      in >> p.k_rama >> p.n_rama;
+      for (int j = 0; j < p.n_rama; j++) {
+        in >> p.w[j] >> p.sigma[j] >> p.phiw[j] >> p.phi0[j] >> p.psiw[j] >> p.psi0[j];
+        p.phiw[j] *= p.sigma[j];
+        p.psiw[j] *= p.sigma[j];
+      }
+    } else if (s == "[Rama_P]") {
+      p.rama_p = 1;
+      in >> p.n_rama_p;
+      for (int j = 0; j < p.n_rama_p; j++) {
+        int q = j + Params::i_rp;
+        in >> p.w[q] >> p.sigma[q] >> p.phiw[q] >> p.phi0[q] >> p.psiw[q] >> p.psi0[q];
+        p.phiw[q] *= p.sigma[q];
+        p.psiw[q] *= p.sigma[q];
+      }
+    } else if (s == "[SSWeight]") {
+      p.ssw = 1;
+      for (int j = 0; j < 12; j++) {
+        int v;
+        in >> v;
+        p.ssweight[j] = v != 0;
+      }
+    } else if (s == "[Dssp_Hdrgn]") {
+      p.dssp = 1;
+      in >> p.k_dssp >> p.hbscl[0][0] >> p.hbscl[0][1];
+      for (int j = 0; j < 7; j++) in >> p.hbscl[1][j];
+      for (int j = 0; j < 9; j++) in >> p.hbscl[2][j];
+      for (int j = 0; j < 9; j++) in >> p.hbscl[3][j];
+      in >> p.sigma_HO >> p.sigma_NO >> p.HO_zero >> p.NO_zero >> p.dssp_cut >> p.pref[0] >> p.pref[1] >> p.d_nu0;
+      p.dssp_cut_sq = p.dssp_cut * p.dssp_cut;
+      p.nu_cut1_sq = pow(p.d_nu0 + atanh(2.0 * 1e-4 - 1.0) / p.pref[0], 2);
+      p.nu_cut2_sq = pow(p.d_nu0 + atanh(2.0 * 1e-4 - 1.0) / p.pref[1], 2);
+      p.sigma_HO_sqinv = 1.0 / (p.sigma_HO * p.sigma_HO);
+      p.sigma_NO_sqinv = 1.0 / (p.sigma_NO * p.sigma_NO);
+    } else if (s == "[P_AP]") {
+      p.pap = 1;
+      in >> p.k_global_pap >> p.k_betapred_pap >> p.k_pap[0] >> p.k_pap[1] >> p.k_pap[2] >> p.pap_cut >>
+          p.pap_pref >> p.i_med_min >> p.i_med_max >> p.i_diff_pap;
+      p.pap_cutoff_sq = pow(p.pap_cut + atanh(1.0 - 2.0 * 1e-12) / p.pap_pref, 2);
+    } else if (s == "[Water]") {
+      p.water = 1;
+      in >> p.k_water >> p.water_kappa >> p.water_kappa_sigma >> p.treshold >> p.contact_cutoff >> p.n_wells;
+      for (int j = 0; j < p.n_wells; j++) in >> p.well_rmin[j] >> p.well_rmax[j] >> p.well_flag[j];
+    } else if (s == "[Burial]") {
+      p.burial = 1;
+      in >> p.k_burial >> p.burial_kappa;
+      for (int j = 0; j < 3; j++) in >> p.burial_ro_min[j] >> p.burial_ro_max[j];
+    } else if (s == "[Helix]") {
+      p.helix = 1;
+      in >> p.k_helix >> p.helix_gamma_p >> p.helix_gamma_w >> p.helix_kappa >> p.helix_kappa_sigma >>
+          p.helix_treshold >> p.helix_i_diff >> p.helix_cutoff;
+      p.helix_cutoff_sq = p.helix_cutoff * p.helix_cutoff;
+      in >> p.helix_rmin >> p.helix_rmax;
+      for (int j = 0; j < 20; j++) in >> p.h4prob[j];
+      in >> p.pro_acc_flag >> p.h4prob_pro >> p.helix_sigma_HO >> p.helix_sigma_NO >> p.helix_HO_zero >>
+          p.helix_NO_zero;
+      p.helix_sigma_HO_sqinv = 1.0 / (p.helix_sigma_HO * p.helix_sigma_HO);
+      p.helix_sigma_NO_sqinv = 1.0 / (p.helix_sigma_NO * p.helix_sigma_NO);
+    } else if (s == "[Fragment_Memory]") {
+      p.fm = 1;
+      in >> p.k_fm >> p.fm_file >> p.fm_gamma_file;
+    } else if (s == "[Epsilon]") {
+      in >> p.epsilon;
+    } else {
+      for (const char *u : unsupported)
+        if (s == u) throw std::runtime_error("oracle: section " + s + " is not part of the restated path");
+    }
+  }
+  // epsilon scaling (fix_backbone.cpp:501-516)
+  for (double &k : p.k_chain) k *= p.epsilon;
+  p.k_chi *= p.epsilon;
+  p.k_rama *= p.epsilon;
+  p.k_water *= p.epsilon;
+  p.k_burial *= p.epsilon;
+  p.k_helix *= p.epsilon;
+  p.k_dssp *= p.epsilon;
+  p.k_global_pap *= p.epsilon;
+  for (int j = 0; j < p.n_rama; j++) p.w[j] *= p.k_rama;
+  for (int j = 0; j < p.n_rama_p; j++) p.w[j + Params::i_rp] *= p.k_rama;
+  // well supports: rmin - 8 ln10/kappa, rmax + 8 ln10/kappa (smart_matrix_lib.h:363-368)
+  for (int k = 0; k < p.n_wells; k++) {
+    p.w_rmin_th[k] = p.well_rmin[k] - 8.0 * 2.302585 / p.water_kappa;
+    p.w_rmax_th[k] = p.well_rmax[k] + 8.0 * 2.302585 / p.water_kappa;
+    p.w_rmin_sq[k] = p.w_rmin_th[k] * p.w_rmin_th[k];
+    p.w_rmax_sq[k] = p.w_rmax_th[k] * p.w_rmax_th[k];
+  }
+  if (p.helix) {
+    p.h_rmin_th = p.helix_rmin - 8.0 * 2.302585 / p.helix_kappa;
+    p.h_rmax_th = p.helix_rmax + 8.0 * 2.302585 / p.helix_kappa;
+    p.h_rmin_sq = p.h_rmin_th * p.h_rmin_th;
+    p.h_rmax_sq = p.h_rmax_th * p.h_rmax_th;
+  }
+  if (p.pap) {
+    // smart_matrix_lib.h:110-115
+    double drmax = p.pap_cut + double(int(8.0 * 2.302585 / p.pap_pref) + 1);
+    double drmin = p.pap_cut - double(int(8.0 * 2.302585 / p.pap_pref) + 1);
+    p.pap_drmax_sq = drmax * drmax;
+    p.pap_drmin_sq = drmin * drmin;
+  }
+}
+
+/* parameter tables read from the working directory (fix_backbone.cpp:555-693) */
+void System::read_tables()
+{
+  Params &p = P;
+  if (p.dssp) {
+    std::ifstream a(join(workdir, "anti_HB")), b(join(workdir, "anti_NHB")), c(join(workdir, "para_HB")),
+        d(join(workdir, "para_one")), e(join(workdir, "anti_one"));
+    if (!a || !b || !c || !d || !e) throw std::runtime_error("DSSP table file missing");
+    for (int i = 0; i < 20; i++) {
+      d >> p.m_para_one[i];
+      e >> p.m_anti_one[i];
+      for (int j = 0; j < 20; j++) {
+        a >> p.m_anti_HB[i][j][0];
+        b >> p.m_anti_NHB[i][j][0];
+        c >> p.m_para_HB[i][j][0];
+      }
+    }
+    for (int i = 0; i < 20; i++)
+      for (int j = 0; j < 20; j++) {
+        a >> p.m_anti_HB[i][j][1];
+        b >> p.m_anti_NHB[i][j][1];
+        c >> p.m_para_HB[i][j][1];
+      }
+    if (!a || !b || !c || !d || !e) throw std::runtime_error("DSSP file format error");
+  }
+  for (int k = 0; k < 12; k++) aps[k].assign(n, 0.0);
+  if (p.ssw) {
+    std::ifstream in(join(workdir, "ssweight"));
+    if (!in) throw std::runtime_error("File ssweight doesn't exist");
+    for (int j = 0; j < n; j++)
+      for (int k = 0; k < 12; k++)
+        if (p.ssweight[k]) in >> aps[k][j];
+  }
+  if (p.water) {
+    std::ifstream in(join(workdir, "gamma.dat"));
+    if (!in) throw std::runtime_error("File gamma.dat doesn't exist");
+    for (int w = 0; w < p.n_wells; w++)
+      for (int i = 0; i < 20; i++)
+        for (int j = i; j < 20; j++) {
+          in >> p.water_gamma[w][i][j][0] >> p.water_gamma[w][i][j][1];
+          if (!in) throw std::runtime_error("gamma.dat format error");
+          p.water_gamma[w][i][j][0] *= p.k_water;
+          p.water_gamma[w][i][j][1] *= p.k_water;
+          p.water_gamma[w][j][i][0] = p.water_gamma[w][i][j][0];
+          p.water_gamma[w][j][i][1] = p.water_gamma[w][i][j][1];
+        }
+  }
+  if (p.burial) {
+    std::ifstream in(join(workdir, "burial_gamma.dat"));
+    if (!in) throw std::runtime_error("File burial_gamma.dat doesn't exist");
+    for (int i = 0; i < 20; i++) in >> p.burial_gamma[i][0] >> p.burial_gamma[i][1] >> p.burial_gamma[i][2];
+    if (!in) throw std::runtime_error("burial_gamma.dat format error");
+  }
+}
+
+void System::read_seq(const std::string &path)
+{
+  std::ifstream in(path);
+  if (!in) throw std::runtime_error("Sequence file was not found");
+  std::string t;
+  while (in >> t) {
+    if (t[0] == '#') continue;
+    ch_pos1.push_back((int) se.size() + 1);
+    ch_len.push_back((int) t.size());
+    se += t;
+  }
+  nch = (int) ch_len.size();
+}
+
+/* LAMMPS data file, atom_style awsemmd */
+void System::read_data(const std::string &path)
+{
+  std::ifstream in(path);
+  if (!in) throw std::runtime_error("cannot open data file " + path);
+  std::string line;
+  std::getline(in, line);
+  int nbonds = 0, nbt = 0;
+  std::vector<std::string> section;
+  std::map<std::string, std::vector<std::string>> sections;
+  std::string cur;
+  while (std::getline(in, line)) {
+    auto h = line.find('#');
+    if (h != std::string::npos) line = line.substr(0, h);
+    auto v = words(line);
+    if (v.empty()) continue;
+    if (cur.empty()) {
+      if (v.size() >= 2 && v[1] == "atoms") { natoms = atoi(v[0].c_str()); continue; }
+      if (v.size() >= 2 && v[1] == "bonds") { nbonds = atoi(v[0].c_str()); continue; }
+      if (v.size() >= 3 && v[1] == "atom" && v[2] == "types") { ntypes = atoi(v[0].c_str()); continue; }
+      if (v.size() >= 3 && v[1] == "bond" && v[2] == "types") { nbt = atoi(v[0].c_str()); continue; }
+      if (v.size() >= 3 && (v[2] == "types" || v[2] == "xlo" || v[2] == "ylo" || v[2] == "zlo")) continue;
+      if (v.size() >= 2 && (v[1] == "angles" || v[1] == "dihedrals" || v[1] == "impropers")) continue;
+    }
+    if (v[0] == "Masses" || v[0] == "Atoms" || v[0] == "Velocities" || v[0] == "Bonds" ||
+        (v[0] == "Bond" && v.size() > 1 && v[1] == "Coeffs")) {
+      cur = v[0] == "Bond" ? "Bond Coeffs" : v[0];
+      continue;
+    }
+    if (cur.empty()) throw std::runtime_error("data file: unexpected line " + line);
+    sections[cur].push_back(line);
+  }
+  mass.assign(ntypes + 1, 0.0);
+  for (auto &l : sections["Masses"]) {
+    auto v = words(l);
+    mass[atoi(v[0].c_str())] = atof(v[1].c_str());
+  }
+  std::vector<std::pair<int, std::vector<std::string>>> rows;
+  for (auto &l : sections["Atoms"]) {
+    auto v = words(l);
+    rows.push_back({atoi(v[0].c_str()), v});
+  }
+  std::sort(rows.begin(), rows.end(), [](auto &a, auto &b) { return a.first < b.first; });
+  if ((int) rows.size() != natoms) throw std::runtime_error("data file: atom count mismatch");
+  atype.resize(natoms);
+  amol.resize(natoms);
+  ares.resize(natoms);
+  tag.resize(natoms);
+  std::map<int, int> t2i;
+  for (int i = 0; i < natoms; i++) {
+    auto &v = rows[i].second;
+    tag[i] = atoi(v[0].c_str());
+    amol[i] = atoi(v[1].c_str());
+    ares[i] = atoi(v[2].c_str());
+    atype[i] = atoi(v[3].c_str());
+    t2i[tag[i]] = i;
+  }
+  bk.assign(nbt + 1, 0.0);
+  br0.assign(nbt + 1, 0.0);
+  for (auto &l : sections["Bond Coeffs"]) {
+    auto v = words(l);
+    bk[atoi(v[0].c_str())] = atof(v[1].c_str());
+    br0[atoi(v[0].c_str())] = atof(v[2].c_str());
+  }
+  special.assign(natoms, {});
+  for (auto &l : sections["Bonds"]) {
+    auto v = words(l);
+    int i = t2i.at(atoi(v[2].c_str())), j = t2i.at(atoi(v[3].c_str()));
+    b_t.push_back(atoi(v[1].c_str()));
+    b_i.push_back(i);
+    b_j.push_back(j);
+    special[i].push_back(j);
+    special[j].push_back(i);
+  }
+  (void) nbonds;
+}
+
+/* .mem list and .gro memories (fix_backbone.cpp:1966-2042,
+   fragment_memory.cpp:34-176) and the residue -> memory map (:749-791) */
+void System::read_mems()
+{
+  std::ifstream in(join(workdir, P.fm_file));
+  if (!in) throw std::runtime_error("Fragment_Memory: Error opening mem file");
+  std::string line;
+  int state = 0;  // 0 none, 1 target, 2 memories
+  while (std::getline(in, line)) {
+    auto v = words(line);
+    std::string t = v.empty() ? "" : v[0];
+    if (!t.empty() && t[0] == '#') continue;
+    if (!t.empty() && t[0] == '[') state = 0;
+    if (v.empty()) {
+      state = 0;
+      continue;
+    }
+    if (state == 2) {
+      if (v.size() != 5) throw std::runtime_error("Fragment_Memory: Error reading mem file");
+      Memory m;
+      m.pos = atoi(v[1].c_str()) - 1;
+      int fpos = atoi(v[2].c_str()) - 1;
+      m.len = atoi(v[3].c_str());
+      m.weight = atof(v[4].c_str());
+      m.se.assign(m.len, '?');
+      std::vector<double> xa((size_t) m.len * 3, 0.0), xb((size_t) m.len * 3, 0.0);
+      FILE *fg = fopen(join(workdir, v[0]).c_str(), "r");
+      if (!fg) throw std::runtime_error("Fragment_Memory: Cannot read the file " + v[0]);
+      char buf[256];
+      if (!fgets(buf, sizeof buf, fg)) throw std::runtime_error("bad gro");
+      int nat = 0;
+      if (fscanf(fg, "%d", &nat) != 1) throw std::runtime_error("bad gro");
+      int nca = 0;
+      for (int a = 0; a < nat; a++) {
+        int ires, iatom;
+        char resty[16], atomty[16];
+        double x, y, z;
+        if (fscanf(fg, "%d %15s %15s %d %lf %lf %lf", &ires, resty, atomty, &iatom, &x, &y, &z) != 7) break;
+        if (ires > fpos + m.len) break;
+        if (ires > fpos && ires <= fpos + m.len) {
+          int r = ires - fpos - 1;
+          x *= 10;
+          y *= 10;
+          z *= 10;
+          if (!strcmp(atomty, "CA")) {
+            m.se[r] = three_to_one(resty);
+            xa[3 * r] = x;
+            xa[3 * r + 1] = y;
+            xa[3 * r + 2] = z;
+            nca++;
+          } else if (!strcmp(atomty, "CB")) {
+            xb[3 * r] = x;
+            xb[3 * r + 1] = y;
+            xb[3 * r + 2] = z;
+          }
+        }
+      }
+      fclose(fg);
+      if (nca != m.len) throw std::runtime_error("Fragment_Memory: Wrong atom count in memory structure file");
+      m.rf0.assign((size_t) m.len * m.len, 0.0);
+      m.rf1.assign((size_t) m.len * m.len, 0.0);
+      for (int i = 0; i < m.len; i++)
+        for (int j = 0; j < m.len; j++) {
+          m.rf0[i * m.len + j] = i < j ? m.R(&xa[3 * i], &xa[3 * j]) : (i > j ? m.R(&xb[3 * i], &xb[3 * j]) : 0.0);
+          m.rf1[i * m.len + j] = m.R(&xa[3 * i], &xb[3 * j]);
+        }
+      if (m.pos + m.len > n) throw std::runtime_error("Fragment_Memory: Incorrectly defined memory fragment");
+      mems.push_back(m);
+    } else if (state == 0) {
+      if (t == "[Target]") state = 1;
+      else if (t == "[Memories]") state = 2;
+    }
+  }
+  G.load(join(workdir, P.fm_gamma_file));
+  fm_map.assign(n, {});
+  int min_sep = G.min_sep();
+  for (int k = 0; k < (int) mems.size(); k++)
+    for (int i = mems[k].pos; i < mems[k].pos + mems[k].len - min_sep; i++) fm_map[i].push_back(k);
+}
+
+/* pair_style vexcluded settings/coeff/init_one (pair_excluded_volume.cpp:175-265) */
+void System::pair_setup(const std::string &style, const std::string &coeffs)
+{
+  auto v = words(style);
+  ev_p = atoi(v[0].c_str());
+  ev_cs_glob = atof(v[1].c_str());
+  ev_cl_glob = atof(v[2].c_str());
+  int N = ntypes + 1;
+  ev_lambda.assign(N * N, 0.0);
+  ev_cs.assign(N * N, 0.0);
+  ev_cl.assign(N * N, 0.0);
+  ev_set.assign(N * N, 0);
+  std::stringstream ss(coeffs);
+  std::string rec;
+  auto range = [&](const std::string &t, int &lo, int &hi) {
+    size_t s = t.find('*');
+    if (s == std::string::npos) lo = hi = atoi(t.c_str());
+    else {
+      lo = s == 0 ? 1 : atoi(t.substr(0, s).c_str());
+      hi = s == t.size() - 1 ? ntypes : atoi(t.substr(s + 1).c_str());
+    }
+  };
+  while (std::getline(ss, rec, ';')) {
+    auto c = words(rec);
+    if (c.empty()) continue;
+    int ilo, ihi, jlo, jhi;
+    range(c[0], ilo, ihi);
+    range(c[1], jlo, jhi);
+    double lam = atof(c[2].c_str());
+    double cs = c.size() == 5 ? atof(c[3].c_str()) : ev_cs_glob;
+    double cl = c.size() == 5 ? atof(c[4].c_str()) : ev_cl_glob;
+    for (int i = ilo; i <= ihi; i++)
+      for (int j = std::max(jlo, i); j <= jhi; j++) {
+        ev_lambda[i * N + j] = lam;
+        ev_cs[i * N + j] = cs;
+        ev_cl[i * N + j] = cl;
+        ev_set[i * N + j] = 1;
+      }
+  }
+  for (int i = 1; i <= ntypes; i++)
+    for (int j = i; j <= ntypes; j++) {
+      if (!ev_set[i * N + j]) {
+        ev_lambda[i * N + j] = sqrt(ev_lambda[i * N + i] * ev_lambda[j * N + j]);
+        ev_cs[i * N + j] = sqrt(ev_cs[i * N + i] * ev_cs[j * N + j]);
+        ev_cl[i * N + j] = sqrt(ev_cl[i * N + i] * ev_cl[j * N + j]);
+      }
+      ev_lambda[j * N + i] = ev_lambda[i * N + j];
+      ev_cs[j * N + i] = ev_cs[i * N + j];
+      ev_cl[j * N + i] = ev_cl[i * N + j];
+    }
+}
+
+/* residue bookkeeping from atom groups: CA type 1, CB/H-beta types 4/5,
+   O type 3, residue order by residue id (Construct_Computational_Arrays,
+   fix_backbone.cpp:1590-1698, for a serial system with every residue local) */
+static void build_residues(System &S)
+{
+  S.n = (int) S.se.size();
+  S.ca.assign(S.n, -1);
+  S.cb.assign(S.n, -1);
+  S.o.assign(S.n, -1);
+  S.chain_of.assign(S.n, -1);
+  for (int a = 0; a < S.natoms; a++) {
+    int r = S.ares[a] - 1;
+    if (r < 0 || r >= S.n) throw std::runtime_error("Residue tag is out of range");
+    int t = S.atype[a];
+    if (t == 1) S.ca[r] = a;
+    else if (t == 4 || t == 5) S.cb[r] = a;
+    else if (t == 3) S.o[r] = a;
+    S.chain_of[r] = S.amol[a] - 1;
+  }
+  for (int r = 0; r < S.n; r++) {
+    if (S.ca[r] < 0 || S.cb[r] < 0 || S.o[r] < 0) throw std::runtime_error("Missing neighbor atoms in fix backbone");
+    int c = S.chain_of[r];
+    if (c < 0 || c >= S.nch) throw std::runtime_error("Chain tag is out of range");
+    if (r + 1 < S.ch_pos1[c] || r + 1 > S.ch_pos1[c] + S.ch_len[c] - 1)
+      throw std::runtime_error("Residue tag is out of range");
+  }
+}
+
+/* coordinates and virtual N, H, C' (fix_backbone.cpp:7067-7138) */
+void System::backbone_atoms(const double *x)
+{
+  const Params &p = P;
+  xca.assign(3 * n, 0.0);
+  xcb.assign(3 * n, 0.0);
+  xo.assign(3 * n, 0.0);
+  xn.assign(3 * n, 0.0);
+  xh.assign(3 * n, 0.0);
+  xcp.assign(3 * n, 0.0);
+  for (int i = 0; i < n; i++)
+    for (int k = 0; k < 3; k++) {
+      xca[3 * i + k] = x[3 * ca[i] + k];
+      xcb[3 * i + k] = x[3 * cb[i] + k];
+      xo[3 * i + k] = x[3 * o[i] + k];
+    }
+  for (int i = 0; i < n; i++) {
+    int im1 = i > 0 ? i - 1 : -1;
+    if (im1 != -1 && !first(i)) {
+      for (int k = 0; k < 3; k++) {
+        xn[3 * i + k] = p.an * xca[3 * im1 + k] + p.bn * xca[3 * i + k] + p.cn * xo[3 * im1 + k];
+        xh[3 * i + k] = p.ah * xca[3 * im1 + k] + p.bh * xca[3 * i + k] + p.ch * xo[3 * im1 + k];
+        xcp[3 * im1 + k] = p.ap * xca[3 * im1 + k] + p.bp * xca[3 * i + k] + p.cp * xo[3 * im1 + k];
+      }
+    } else if (im1 != -1) {
+      for (int k = 0; k < 3; k++) xcp[3 * im1 + k] = 0.0;
+    }
+  }
+}
+
+inline void addf(double *f, int atom, double a, double b, double c)
+{
+  f[3 * atom] += a;
+  f[3 * atom + 1] += b;
+  f[3 * atom + 2] += c;
+}
+
+/* compute_chain_potential, fix_backbone.cpp:2062-2170 */
+void System::chain_term(int i, double *f)
+{
+  const Params &p = P;
+  double dx[3], r, dr, force;
+  if (!first(i) && se[i] != 'G') {
+    int im1 = i - 1;
+    for (int k = 0; k < 3; k++) dx[k] = xn[3 * i + k] - xcb[3 * i + k];
+    r = sqrt(dx[0] * dx[0] + dx[1] * dx[1] + dx[2] * dx[2]);
+    dr = r - p.r_ncb0;
+    force = 2 * p.k_chain[0] * dr / r;
+    E[ET_CHAIN] += p.k_chain[0] * dr * dr;
+    for (int k = 0; k < 3; k++) {
+      f[3 * ca[im1] + k] -= p.an * dx[k] * force;
+      f[3 * o[im1] + k] -= p.cn * dx[k] * force;
+      f[3 * ca[i] + k] -= p.bn * dx[k] * force;
+      f[3 * cb[i] + k] -= -dx[k] * force;
+    }
+  }
+  if (!last(i) && se[i] != 'G') {
+    int ip1 = i + 1;
+    for (int k = 0; k < 3; k++) dx[k] = xcp[3 * i + k] - xcb[3 * i + k];
+    r = sqrt(dx[0] * dx[0] + dx[1] * dx[1] + dx[2] * dx[2]);
+    dr = r - p.r_cpcb0;
+    force = 2 * p.k_chain[1] * dr / r;
+    E[ET_CHAIN] += p.k_chain[1] * dr * dr;
+    for (int k = 0; k < 3; k++) {
+      f[3 * ca[ip1] + k] -= p.bp * dx[k] * force;
+      f[3 * ca[i] + k] -= p.ap * dx[k] * force;
+      f[3 * o[i] + k] -= p.cp * dx[k] * force;
+      f[3 * cb[i] + k] -= -dx[k] * force;
+    }
+  }
+  if (!first(i) && !last(i)) {
+    int im1 = i - 1, ip1 = i + 1;
+    for (int k = 0; k < 3; k++) dx[k] = xn[3 * i + k] - xcp[3 * i + k];
+    r = sqrt(dx[0] * dx[0] + dx[1] * dx[1] + dx[2] * dx[2]);
+    dr = r - p.r_ncp0;
+    force = 2 * p.k_chain[2] * dr / r;
+    E[ET_CHAIN] += p.k_chain[2] * dr * dr;
+    for (int k = 0; k < 3; k++) {
+      f[3 * ca[im1] + k] -= p.an * dx[k] * force;
+      f[3 * o[im1] + k] -= p.cn * dx[k] * force;
+      f[3 * ca[ip1] + k] -= -p.bp * dx[k] * force;
+      f[3 * ca[i] + k] -= (p.bn - p.ap) * dx[k] * force;
+      f[3 * o[i] + k] -= -p.cp * dx[k] * force;
+    }
+  }
+}
+
+inline double dot3(const double *a, const double *b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+inline void cross3(const double *a, const double *b, double *c)
+{
+  c[0] = a[1] * b[2] - a[2] * b[1];
+  c[1] = a[2] * b[0] - a[0] * b[2];
+  c[2] = a[0] * b[1] - a[1] * b[0];
+}
+
+/* compute_chi_potential, fix_backbone.cpp:2239-2339 */
+void System::chi_term(int i, double *f)
+{
+  const Params &p = P;
+  double a[3], b[3], c[3], axb[3], cxa[3], bxc[3], aprl[3], bprl[3], cprl[3];
+  for (int k = 0; k < 3; k++) {
+    a[k] = xcp[3 * i + k] - xca[3 * i + k];
+    b[k] = xca[3 * i + k] - xn[3 * i + k];
+    c[k] = xca[3 * i + k] - xcb[3 * i + k];
+  }
+  double arvsq = 1.0 / dot3(a, a), brvsq = 1.0 / dot3(b, b), crvsq = 1.0 / dot3(c, c);
+  double norm = sqrt(arvsq * brvsq * crvsq);
+  cross3(a, b, axb);
+  cross3(c, a, cxa);
+  cross3(b, c, bxc);
+  double chi = dot3(axb, c) * norm;
+  for (int k = 0; k < 3; k++) {
+    aprl[k] = norm * bxc[k] - arvsq * chi * a[k];
+    bprl[k] = norm * cxa[k] - brvsq * chi * b[k];
+    cprl[k] = norm * axb[k] - crvsq * chi * c[k];
+  }
+  double dchi = chi - p.chi0;
+  double force = 2 * p.k_chi * dchi;
+  E[ET_CHI] += p.k_chi * dchi * dchi;
+  int im1 = i - 1, ip1 = i + 1;
+  for (int k = 0; k < 3; k++) {
+    f[3 * ca[im1] + k] -= -p.an * bprl[k] * force;
+    f[3 * o[im1] + k] -= -p.cn * bprl[k] * force;
+    f[3 * ca[ip1] + k] -= p.bp * aprl[k] * force;
+    f[3 * ca[i] + k] -= (cprl[k] + (1 - p.bn) * bprl[k] + (p.ap - 1) * aprl[k]) * force;
+    f[3 * o[i] + k] -= p.cp * aprl[k] * force;
+    f[3 * cb[i] + k] -= -cprl[k] * force;
+  }
+}
+
+/* calcDihedralAndSlopes, fix_backbone.cpp:2341-2453; atoms CA0, CA1, CA2, O0, O1 */
+void System::dihedral_slopes(int i, int iang, double &angle, double ys[5][3], double xs[5][3])
+{
+  const Params &p = P;
+  double a[3], b[3], c[3], bxa[3], cxa[3], cxb[3];
+  for (int k = 0; k < 3; k++) {
+    if (iang == 0) {
+      a[k] = xcp[3 * i + k] - xca[3 * i + k];
+      b[k] = xca[3 * i + k] - xn[3 * i + k];
+      c[k] = xn[3 * i + k] - xcp[3 * (i - 1) + k];
+    } else {
+      a[k] = xn[3 * (i + 1) + k] - xcp[3 * i + k];
+      b[k] = xcp[3 * i + k] - xca[3 * i + k];
+      c[k] = xca[3 * i + k] - xn[3 * i + k];
+    }
+  }
+  double adb = dot3(a, b), bdc = dot3(b, c), adc = dot3(a, c), b2 = dot3(b, b), bm = sqrt(b2);
+  cross3(b, a, bxa);
+  cross3(c, a, cxa);
+  cross3(c, b, cxb);
+  double cdbxa = dot3(c, bxa);
+  double Y = bm * cdbxa, X = adb * bdc - b2 * adc;
+  angle = atan2(Y, X);
+  double X2Y2 = 1.0 / (X * X + Y * Y);
+  double dy = X * X2Y2, dxx = -Y * X2Y2;
+  b2 *= dxx;
+  adb *= dxx;
+  adc *= dxx;
+  bdc *= dxx;
+  cdbxa *= dy / bm;
+  bm *= dy;
+  const double an = p.an, bn = p.bn, cn = p.cn, ap = p.ap, bp = p.bp, cp = p.cp;
+  for (int l = 0; l < 3; l++) {
+    double h1, h2, h3, h4;
+    if (iang == 0) {
+      h1 = cxb[l] * bm;
+      h2 = cxa[l] * bm;
+      h3 = bxa[l] * bm;
+      h4 = b[l] * cdbxa;
+      ys[0][l] = -an * h4 + (an - ap) * h3 + an * h2;
+      ys[1][l] = (1.0 - bn) * h4 + (bn - bp) * h3 + (ap - 1.0) * h1 - (1.0 - bn) * h2;
+      ys[2][l] = bp * h1;
+      ys[3][l] = -cn * h4 + (cn - cp) * h3 + cn * h2;
+      ys[4][l] = cp * h1;
+      h1 = b[l] * bdc - c[l] * b2;
+      h2 = a[l] * bdc - 2.0 * b[l] * adc + c[l] * adb;
+      h3 = b[l] * adb - a[l] * b2;
+      xs[0][l] = -an * h2 + (an - ap) * h3;
+      xs[1][l] = (ap - 1.0) * h1 + (1.0 - bn) * h2 + (bn - bp) * h3;
+      xs[2][l] = bp * h1;
+      xs[3][l] = -cn * h2 + (cn - cp) * h3;
+      xs[4][l] = cp * h1;
+    } else {
+      h1 = bxa[l] * bm;
+      h2 = cxb[l] * bm;
+      h3 = cxa[l] * bm;
+      h4 = b[l] * cdbxa;
+      ys[0][l] = -an * h1;
+      ys[1][l] = (ap - 1.0) * h4 + (1.0 - bn) * h1 + (an - ap) * h2 - (ap - 1) * h3;
+      ys[2][l] = bp * h4 + (bn - bp) * h2 - bp * h3;
+      ys[3][l] = -cn * h1;
+      ys[4][l] = cp * h4 + (cn - cp) * h2 - cp * h3;
+      h1 = b[l] * bdc - c[l] * b2;
+      h2 = a[l] * bdc - 2.0 * b[l] * adc + c[l] * adb;
+      h3 = b[l] * adb - a[l] * b2;
+      xs[0][l] = -an * h3;
+      xs[1][l] = (an - ap) * h1 + (ap - 1.0) * h2 + (1.0 - bn) * h3;
+      xs[2][l] = (bn - bp) * h1 + bp * h2;
+      xs[3][l] = -cn * h3;
+      xs[4][l] = (cn - cp) * h1 + cp * h2;
+    }
+  }
+}
+
+/* compute_rama_potential + compute_rama_force, fix_backbone.cpp:2455-2546 */
+void System::rama_term(int i, double *f)
+{
+  const Params &p = P;
+  double phi, psi, ys[2][5][3], xs[2][5][3];
+  dihedral_slopes(i, 0, phi, ys[0], xs[0]);
+  dihedral_slopes(i, 1, psi, ys[1], xs[1]);
+  int j0 = 0, j1 = p.n_rama;
+  if (se[i] == 'P' && p.rama_p) {
+    j0 = Params::i_rp;
+    j1 = Params::i_rp + p.n_rama_p;
+  }
+  int atoms[5] = {ca[i - 1], ca[i], ca[i + 1], o[i - 1], o[i]};
+  for (int j = j0; j < j1; j++) {
+    if (p.ssweight[j] && aps[j][i] == 0.0) continue;
+    double cos_phi = cos(phi + p.phi0[j]) - 1.0;
+    double cos_psi = cos(psi + p.psi0[j]) - 1.0;
+    double pc = p.phiw[j] * cos_phi, sc = p.psiw[j] * cos_psi;
+    double V = p.w[j] * exp(-cos_phi * pc - cos_psi * sc);
+    if (p.ssweight[j]) V *= aps[j][i];
+    double force = 2.0 * V;
+    double f1[2] = {force * pc * sin(phi + p.phi0[j]), force * sc * sin(psi + p.psi0[j])};
+    E[ET_RAMA] += -V;
+    for (int ia = 0; ia < 2; ia++)
+      for (int at = 0; at < 5; at++)
+        for (int l = 0; l < 3; l++) f[3 * atoms[at] + l] += f1[ia] * (ys[ia][at][l] + xs[ia][at][l]);
+  }
+}
+
+/* compute_dssp_hdrgn(i, j), fix_backbone.cpp:2902-3277 (O of i, N-H of j) */
+void System::dssp_term(int i, int j, double *f)
+{
+  const Params &p = P;
+  auto rNO = [&](int a, int b) {
+    return sqrt(pow(xo[3 * a] - xn[3 * b], 2) + pow(xo[3 * a + 1] - xn[3 * b + 1], 2) +
+                pow(xo[3 * a + 2] - xn[3 * b + 2], 2));
+  };
+  auto rHO = [&](int a, int b) {
+    return sqrt(pow(xo[3 * a] - xh[3 * b], 2) + pow(xo[3 * a + 1] - xh[3 * b + 1], 2) +
+                pow(xo[3 * a + 2] - xh[3 * b + 2], 2));
+  };
+  if (rNO(i, j) > p.dssp_cut) return;
+  int ic = chain_of[i], jc = chain_of[j];
+  int i_ch_start = ch_pos1[ic], j_ch_start = ch_pos1[jc];
+  int i_ch_end = ch_pos1[ic] + ch_len[ic] - 1, j_ch_end = ch_pos1[jc] + ch_len[jc] - 1;
+  bool i_rep = true, i_AP = true, i_P = true;
+  if (last(j) || se[j + 1] == 'P') i_rep = false;
+  if (first(i) || last(j) || se[i] == 'P') i_AP = false;
+  if (i >= i_ch_end - 2 || last(j) || se[i + 2] == 'P') i_P = false;
+  auto aHB = [&](char a, char b, int k) { return p.m_anti_HB[aa_index(a)][aa_index(b)][k]; };
+  auto aNHB = [&](char a, char b, int k) { return p.m_anti_NHB[aa_index(a)][aa_index(b)][k]; };
+  auto pHB = [&](char a, char b, int k) { return p.m_para_HB[aa_index(a)][aa_index(b)][k]; };
+  auto p1 = [&](char a) { return p.m_para_one[aa_index(a)]; };
+  auto a1 = [&](char a) { return p.m_anti_one[aa_index(a)]; };
+  double ts_aHB[2], ts_aNHB[2], ts_pHB[2];
+  for (int k = 0; k < 2; k++) {
+    if (i_AP) {
+      ts_aHB[k] = 0.5 * aHB(se[i], se[j], k);
+      ts_aNHB[k] = 0.25 * (aNHB(se[i + 1], se[j - 1], k) + aNHB(se[i - 1], se[j + 1], k));
+    } else
+      ts_aHB[k] = ts_aNHB[k] = 0.0;
+    ts_pHB[k] = i_P ? pHB(se[i + 1], se[j], k) : 0.0;
+  }
+  double lambda[4];
+  int hb_class;
+  if (ic == jc && abs(j - i) < 45) {
+    if (abs(j - i) < 4) {
+      lambda[0] = -p.hbscl[0][0];
+      lambda[1] = -p.hbscl[0][1];
+      lambda[2] = 0.0;
+      lambda[3] = 0.0;
+      hb_class = 1;
+    } else if (abs(j - i) < 18) {
+      if (p.n_rama > 0 && aps[p.n_rama - 1][i] == 1.0 && aps[p.n_rama - 1][j] == 1.0) {
+        lambda[0] = -p.hbscl[1][0];
+        lambda[1] = -p.hbscl[1][1];
+        lambda[2] = -p.hbscl[1][2] - p.hbscl[1][3] * ts_aHB[0] - p.hbscl[1][4] * ts_aNHB[0] -
+                    p.hbscl[1][5] * (a1(se[i]) + a1(se[j]));
+        lambda[3] = -p.hbscl[1][6];
+      } else {
+        lambda[0] = 0.0;
+        lambda[1] = -p.hbscl[1][1];
+        lambda[2] = 0.0;
+        lambda[3] = 0.0;
+      }
+      hb_class = 2;
+    } else {
+      lambda[0] = -p.hbscl[2][0];
+      lambda[1] = -p.hbscl[2][1];
+      lambda[2] = -p.hbscl[2][2] - p.hbscl[2][3] * ts_aHB[1] - p.hbscl[2][4] * ts_aNHB[1] -
+                  p.hbscl[2][5] * (a1(se[i]) + a1(se[j]));
+      lambda[3] = -p.hbscl[2][6] - p.hbscl[2][7] * ts_pHB[1] - p.hbscl[2][8] * (p1(se[i + 1]) + p1(se[j]));
+      hb_class = 3;
+    }
+  } else {
+    lambda[0] = -p.hbscl[3][0];
+    lambda[1] = -p.hbscl[3][1];
+    lambda[2] = -p.hbscl[3][2] - p.hbscl[3][3] * ts_aHB[1] - p.hbscl[3][4] * ts_aNHB[1] -
+                p.hbscl[3][5] * (a1(se[i]) + a1(se[j]));
+    lambda[3] = -p.hbscl[3][6] - p.hbscl[3][7] * ts_pHB[1] - p.hbscl[3][8] * (p1(se[i + 1]) + p1(se[j]));
+    hb_class = 4;
+  }
+  double nu[2], prdnu[2], dxnu[2][3], r_nu;
+  bool use_nu[2];
+  use_nu[0] = i - 2 >= i_ch_start - 1 && i + 2 < i_ch_end && hb_class != 2;
+  use_nu[1] = j - 2 >= j_ch_start - 1 && j + 2 < j_ch_end && hb_class != 2;
+  int cen[2] = {i, j};
+  for (int s = 0; s < 2; s++) {
+    nu[s] = prdnu[s] = 0.0;
+    if (use_nu[s]) {
+      int c = cen[s];
+      for (int k = 0; k < 3; k++) dxnu[s][k] = xca[3 * (c + 2) + k] - xca[3 * (c - 2) + k];
+      r_nu = dxnu[s][0] * dxnu[s][0] + dxnu[s][1] * dxnu[s][1] + dxnu[s][2] * dxnu[s][2];
+      if (r_nu > (s == 0 ? p.nu_cut1_sq : p.nu_cut2_sq)) {
+        r_nu = sqrt(r_nu);
+        double th = tanh(p.pref[s] * (r_nu - p.d_nu0));
+        nu[s] = 0.5 * (1.0 + th);
+        prdnu[s] = p.pref[s] * nu[s] * (1.0 - th) / r_nu;
+      }
+    } else
+      nu[s] = 1.0;
+  }
+  if (nu[0] < 1e-4 || nu[1] < 1e-4) return;
+  bool i_theta[4] = {true, i_rep, i_AP, i_P};
+  // (acceptor O residue, donor N-H residue) of the four Gaussians
+  int acc[4] = {i, i, j, j}, don[4] = {j, j + 1, i, i + 2};
+  double R_NO[4], R_HO[4], xNO[4][3], xHO[4][3], theta[4], prd[4][2];
+  for (int k = 0; k < 4; k++) {
+    if (!i_theta[k]) {
+      theta[k] = 0.0;
+      prd[k][0] = prd[k][1] = 0.0;
+      continue;
+    }
+    int a = acc[k], d = don[k];
+    R_NO[k] = rNO(a, d);
+    R_HO[k] = rHO(a, d);
+    for (int l = 0; l < 3; l++) {
+      xNO[k][l] = xo[3 * a + l] - xn[3 * d + l];
+      xHO[k][l] = xo[3 * a + l] - xh[3 * d + l];
+    }
+    double dNO = (R_NO[k] - p.NO_zero) * p.sigma_NO_sqinv;
+    double dHO = (R_HO[k] - p.HO_zero) * p.sigma_HO_sqinv;
+    theta[k] = exp(-0.5 * ((R_NO[k] - p.NO_zero) * dNO + (R_HO[k] - p.HO_zero) * dHO));
+    prd[k][0] = -dNO / R_NO[k];
+    prd[k][1] = -dHO / R_HO[k];
+  }
+  double ff1 = p.k_dssp * theta[0];
+  double V[4] = {lambda[0], lambda[1] * theta[1], lambda[2] * theta[2], lambda[3] * theta[3]};
+  double theta_sum = ff1 * (V[0] + V[1] + V[2] + V[3]);
+  ff1 *= nu[0] * nu[1];
+  for (double &v : V) v *= ff1;
+  double VT = V[0] + V[1] + V[2] + V[3];
+  E[ET_DSSP] += VT;
+  if (use_nu[0]) {
+    double g = theta_sum * prdnu[0] * nu[1];
+    for (int k = 0; k < 3; k++) {
+      f[3 * ca[i - 2] + k] -= -g * dxnu[0][k];
+      f[3 * ca[i + 2] + k] -= g * dxnu[0][k];
+    }
+  }
+  if (use_nu[1]) {
+    double g = theta_sum * nu[0] * prdnu[1];
+    for (int k = 0; k < 3; k++) {
+      f[3 * ca[j - 2] + k] -= -g * dxnu[1][k];
+      f[3 * ca[j + 2] + k] -= g * dxnu[1][k];
+    }
+  }
+  double scale[4] = {VT, V[1], V[2], V[3]};
+  for (int k = 0; k < 4; k++) {
+    if (!i_theta[k]) continue;
+    double q0 = prd[k][0] * scale[k], q1 = prd[k][1] * scale[k];
+    int a = acc[k], d = don[k];
+    for (int l = 0; l < 3; l++) {
+      f[3 * o[a] + l] -= q0 * xNO[k][l] + q1 * xHO[k][l];
+      f[3 * ca[d - 1] + l] += p.an * q0 * xNO[k][l] + p.ah * q1 * xHO[k][l];
+      f[3 * ca[d] + l] += p.bn * q0 * xNO[k][l] + p.bh * q1 * xHO[k][l];
+      f[3 * o[d - 1] + l] += p.cn * q0 * xNO[k][l] + p.ch * q1 * xHO[k][l];
+    }
+  }
+}
+
+/* cP_AP::compute, smart_matrix_lib.h:178-203 */
+void System::pap_nu(int i, int j, double &nu, double &prd)
+{
+  const Params &p = P;
+  double dx0 = xca[3 * i] - xca[3 * j], dx1 = xca[3 * i + 1] - xca[3 * j + 1], dx2 = xca[3 * i + 2] - xca[3 * j + 2];
+  double drsq = pow(dx0, 2) + pow(dx1, 2) + pow(dx2, 2);
+  if (drsq > p.pap_drmax_sq) {
+    nu = 0.0;
+    prd = 0.0;
+  } else if (drsq < p.pap_drmin_sq) {
+    nu = 1.0;
+    prd = 0.0;
+  } else {
+    double dr = sqrt(drsq);
+    double th = tanh(p.pap_pref * (p.pap_cut - dr));
+    nu = 0.5 * (1 + th);
+    prd = 0.5 * p.pap_pref * (1 - pow(th, 2)) / dr;
+  }
+}
+
+/* compute_P_AP_potential(i, j), i < j, fix_backbone.cpp:3279-3383 */
+void System::pap_term(int i, int j, double *f)
+{
+  const Params &p = P;
+  double nu_ij, prd_ij;
+  pap_nu(i, j, nu_ij, prd_ij);
+  if (nu_ij < 1e-12) return;
+  int ic = chain_of[i], jc = chain_of[j], d = p.i_diff_pap;
+  int i_ch_end = ch_pos1[ic] + ch_len[ic] - 1, j_ch_end = ch_pos1[jc] + ch_len[jc] - 1;
+  bool ap_med = ic == jc && i < i_ch_end - (p.i_med_min + 2 * d) && j >= i + (p.i_med_min + 2 * d) &&
+                j <= std::min(i + p.i_med_max + 2 * d, i_ch_end - 1);
+  bool ap_long = (ic == jc && i < i_ch_end - (p.i_med_max + 2 * d + 1) && j >= i + (p.i_med_max + 2 * d + 1) &&
+                  j < j_ch_end) ||
+                 (ic != jc && i + d < n && j - d >= 0 && chain_of[i + d] == ic && chain_of[j - d] == jc);
+  bool par = (ic == jc && i < i_ch_end - (p.i_med_max + 1 + d) && j >= i + (p.i_med_max + 1) && j < i_ch_end - d) ||
+             (ic != jc && i + d < n && j + d < n && chain_of[i + d] == ic && chain_of[j + d] == jc);
+  bool beta = p.n_rama > 0 && aps[p.n_rama - 1][i] == 1.0 && aps[p.n_rama - 1][j] == 1.0;
+  auto apply = [&](double K, int i2, int j2) {
+    double nu2, prd2;
+    pap_nu(i2, j2, nu2, prd2);
+    E[ET_PAP] += -p.k_global_pap * K * nu_ij * nu2;
+    double f0 = p.k_global_pap * K * prd_ij * nu2;
+    double f1 = p.k_global_pap * K * nu_ij * prd2;
+    for (int k = 0; k < 3; k++) {
+      double d0 = xca[3 * i + k] - xca[3 * j + k];
+      double d1 = xca[3 * i2 + k] - xca[3 * j2 + k];
+      f[3 * ca[i] + k] -= f0 * d0;
+      f[3 * ca[j] + k] -= -f0 * d0;
+      f[3 * ca[i2] + k] -= f1 * d1;
+      f[3 * ca[j2] + k] -= -f1 * d1;
+    }
+  };
+  if (ap_med || ap_long) {
+    double K = beta ? (ap_med ? p.k_pap[0] : 0.0) + (ap_long ? p.k_pap[1] * p.k_betapred_pap : 0.0)
+                    : (ap_med ? p.k_pap[0] : 0.0) + (ap_long ? p.k_pap[1] : 0.0);
+    apply(K, i + d, j - d);
+  }
+  if (par) {
+    double K = beta ? p.k_pap[2] * p.k_betapred_pap : p.k_pap[2];
+    apply(K, i + d, j + d);
+  }
+}
+
+/* compute_helix_dtheta_pair(i, j = i + 4), fix_backbone.cpp:3706-3785 */
+void System::helix_pair(int i, int j, double *f)
+{
+  const Params &p = P;
+  double xNO[3], xHO[3];
+  for (int k = 0; k < 3; k++) {
+    xNO[k] = xo[3 * i + k] - xn[3 * j + k];
+    xHO[k] = xo[3 * i + k] - xh[3 * j + k];
+  }
+  double R_NO = sqrt(pow(xNO[0], 2) + pow(xNO[1], 2) + pow(xNO[2], 2));
+  if (R_NO > p.helix_cutoff) return;
+  if (chain_of[i] != chain_of[j]) return;
+  double R_HO = sqrt(pow(xHO[0], 2) + pow(xHO[1], 2) + pow(xHO[2], 2));
+  double h4i = p.h4prob[type_of(i)];
+  if (se[i] == 'P' && p.pro_acc_flag) h4i = p.h4prob_pro;
+  double prob_sum = h4i + p.h4prob[type_of(j)];
+  double dNO = R_NO - p.helix_NO_zero, dHO = R_HO - p.helix_HO_zero;
+  double dNOs = dNO * p.helix_sigma_NO_sqinv, dHOs = dHO * p.helix_sigma_HO_sqinv;
+  double pair_theta = -p.k_helix * prob_sum * exp(-0.5 * (dNO * dNOs + dHO * dHOs));
+  double prd0 = -dNOs / R_NO, prd1 = -dHOs / R_HO;
+  double sigma_gamma = p.helix_gamma_p + (p.helix_gamma_w - p.helix_gamma_p) * sig_h[i] * sig_h[j];
+  xi1[i] = (p.helix_gamma_w - p.helix_gamma_p) * pair_theta * sigp_h[i] * sig_h[j];
+  xi2[i] = (p.helix_gamma_w - p.helix_gamma_p) * pair_theta * sig_h[i] * sigp_h[j];
+  double V = sigma_gamma * pair_theta;
+  E[ET_HELIX] += V;
+  for (int k = 0; k < 3; k++) {
+    f[3 * ca[j - 1] + k] -= -V * (p.an * prd0 * xNO[k] + p.ah * prd1 * xHO[k]);
+    f[3 * ca[j] + k] -= -V * (p.bn * prd0 * xNO[k] + p.bh * prd1 * xHO[k]);
+    f[3 * o[j - 1] + k] -= -V * (p.cn * prd0 * xNO[k] + p.ch * prd1 * xHO[k]);
+    f[3 * o[i] + k] -= V * (prd0 * xNO[k] + prd1 * xHO[k]);
+  }
+}
+
+/* compute_fragment_memory_potential(i), fix_backbone.cpp:4079-4177 */
+void System::fm_term(int i, double *f)
+{
+  const Params &p = P;
+  static const int it[4] = {1, 1, 2, 2}, jt[4] = {1, 2, 1, 2};
+  for (int km : fm_map[i]) {
+    const Memory &m = mems[km];
+    double ekw = p.epsilon * p.k_fm * m.weight;
+    int js = i + G.min_sep();
+    int je = m.pos + m.len - 1;
+    if (G.max_sep() != -1) je = std::min(je, i + G.max_sep());
+    if (je >= n) throw std::runtime_error("Missing residues in memory potential");
+    for (int j = js; j <= je; j++) {
+      if (chain_of[i] != chain_of[j])
+        throw std::runtime_error("Fragment Memory: Interaction between residues of different chains");
+      double sig_sq = pow(abs(i - j), 2 * p.fm_sigma_exp);
+      double gam = G.get(type_of(i), type_of(j), aa_index(m.se[i - m.pos]), aa_index(m.se[j - m.pos]), i, j);
+      double ekwg = ekw * gam;
+      int ia[4] = {ca[i], ca[i], cb[i], cb[i]}, ja[4] = {ca[j], cb[j], ca[j], cb[j]};
+      const double *xi[4] = {&xca[3 * i], &xca[3 * i], &xcb[3 * i], &xcb[3 * i]};
+      const double *xj[4] = {&xca[3 * j], &xcb[3 * j], &xca[3 * j], &xcb[3 * j]};
+      for (int k = 0; k < 4; k++) {
+        if (it[k] == 2 && (se[i] == 'G' || m.se[i - m.pos] == 'G')) continue;
+        if (jt[k] == 2 && (se[j] == 'G' || m.se[j - m.pos] == 'G')) continue;
+        double dx[3] = {xi[k][0] - xj[k][0], xi[k][1] - xj[k][1], xi[k][2] - xj[k][2]};
+        double r = sqrt(dx[0] * dx[0] + dx[1] * dx[1] + dx[2] * dx[2]);
+        double dr = r - m.rf(i, it[k], j, jt[k]);
+        double V = -ekwg * exp(-dr * dr / (2.0 * sig_sq));
+        E[ET_FRAGMEM] += V;
+        double force = V * dr / (sig_sq * r);
+        addf(f, ia[k], force * dx[0], force * dx[1], force * dx[2]);
+        addf(f, ja[k], -force * dx[0], -force * dx[1], -force * dx[2]);
+      }
+    }
+  }
+}
+
+/* theta of a density well and its radial derivative over r
+   (cWell::compute_theta_pair, smart_matrix_lib.h:612-628) */
+inline void well_theta(double r, double rmin_th, double rmax_th, double kappa, double rmin, double rmax,
+                       double &theta, double &prd)
+{
+  if (r < rmin_th || r > rmax_th) {
+    theta = prd = 0.0;
+    return;
+  }
+  double t_min = tanh(kappa * (r - rmin));
+  double t_max = tanh(kappa * (rmax - r));
+  theta = 0.25 * (1.0 + t_min) * (1.0 + t_max);
+  prd = kappa * theta * (t_max - t_min) / r;
+}
+
+/* compute_pair, fix_backbone.cpp:7677-8135: densities (DL1), switching
+   functions, burial and helix pairs (SL), water xi (DL2), main loop (DL3) */
+void System::pair_terms(const double *x, double *f)
+{
+  const Params &p = P;
+  rho_w.assign(n, 0.0);
+  rho_h.assign(n, 0.0);
+  sig_w.assign(n, 0.0);
+  sigp_w.assign(n, 0.0);
+  sig_h.assign(n, 0.0);
+  sigp_h.assign(n, 0.0);
+  xi_w.assign(n, 0.0);
+  xi1.assign(n, 0.0);
+  xi2.assign(n, 0.0);
+  bur.assign(n, 0.0);
+  sel_count[0] = sel_count[1] = 0;
+  sel_hash = 0;
+  auto cpos = [&](int i) { return &x[3 * contact_atom(i)]; };
+  // DL1
+  for (int i = 0; i < n; i++)
+    for (int j = i + 1; j < n; j++) {
+      if (!(chain_of[i] != chain_of[j] || abs(i - j) > 1)) continue;
+      const double *a = cpos(i), *b = cpos(j);
+      double dx0 = a[0] - b[0], dx1 = a[1] - b[1], dx2 = a[2] - b[2];
+      double rsq = dx0 * dx0 + dx1 * dx1 + dx2 * dx2;
+      if (p.water && rsq > p.w_rmin_sq[0] && rsq < p.w_rmax_sq[0]) {
+        double th, pr;
+        well_theta(sqrt(rsq), p.w_rmin_th[0], p.w_rmax_th[0], p.water_kappa, p.well_rmin[0], p.well_rmax[0], th, pr);
+        rho_w[i] += th;
+        rho_w[j] += th;
+        sel_count[0]++;
+        sel_hash += mix64(((uint64_t) i << 32) ^ (uint64_t) j ^ (1ULL << 62));
+      }
+      if (p.helix && rsq > p.h_rmin_sq && rsq < p.h_rmax_sq) {
+        double th, pr;
+        well_theta(sqrt(rsq), p.h_rmin_th, p.h_rmax_th, p.helix_kappa, p.helix_rmin, p.helix_rmax, th, pr);
+        rho_h[i] += th;
+        rho_h[j] += th;
+        sel_count[1]++;
+        sel_hash += mix64(((uint64_t) i << 32) ^ (uint64_t) j ^ (2ULL << 62));
+      }
+    }
+  // SL: switching functions and burial (:7795-7841)
+  for (int i = 0; i < n; i++) {
+    if (p.water) {
+      double th = tanh(p.water_kappa_sigma * (rho_w[i] - p.treshold));
+      sig_w[i] = 0.5 * (1.0 - th);
+      sigp_w[i] = -p.water_kappa_sigma * sig_w[i] * (1.0 + th);
+    }
+    if (p.helix) {
+      double th = tanh(p.helix_kappa_sigma * (rho_h[i] - p.helix_treshold));
+      sig_h[i] = 0.5 * (1.0 - th);
+      sigp_h[i] = -p.helix_kappa_sigma * sig_h[i] * (1.0 + th);
+    }
+    if (p.burial) {
+      double t[3][2];
+      for (int k = 0; k < 3; k++) {
+        t[k][0] = tanh(p.burial_kappa * (rho_w[i] - p.burial_ro_min[k]));
+        t[k][1] = tanh(p.burial_kappa * (p.burial_ro_max[k] - rho_w[i]));
+      }
+      int ty = type_of(i);
+      for (int k = 0; k < 3; k++) E[ET_BURIAL] += -0.5 * p.k_burial * p.burial_gamma[ty][k] * (t[k][0] + t[k][1]);
+      bur[i] = p.burial_gamma[ty][0] * (t[0][1] * t[0][1] - t[0][0] * t[0][0]);
+      bur[i] += p.burial_gamma[ty][1] * (t[1][1] * t[1][1] - t[1][0] * t[1][0]);
+      bur[i] += p.burial_gamma[ty][2] * (t[2][1] * t[2][1] - t[2][0] * t[2][0]);
+      bur[i] *= 0.5 * p.k_burial * p.burial_kappa;
+    }
+  }
+  // SL: helical (i, i+4) pairs (:7843-7868)
+  if (p.helix) {
+    int d = p.helix_i_diff;
+    for (int i = 0; i < n; i++) {
+      int j = i + d;
+      if (j >= n || chain_of[j] != chain_of[i]) continue;
+      double dx0 = xo[3 * i] - xn[3 * j], dx1 = xo[3 * i + 1] - xn[3 * j + 1], dx2 = xo[3 * i + 2] - xn[3 * j + 2];
+      if (dx0 * dx0 + dx1 * dx1 + dx2 * dx2 < p.helix_cutoff_sq) helix_pair(i, j, f);
+    }
+  }
+  // DL2: water xi (:7877-7954)
+  if (p.water) {
+    for (int i = 0; i < n; i++)
+      for (int j = i + 1; j < n; j++) {
+        if (!(chain_of[i] != chain_of[j] || abs(i - j) >= p.contact_cutoff)) continue;
+        const double *a = cpos(i), *b = cpos(j);
+        double dx0 = a[0] - b[0], dx1 = a[1] - b[1], dx2 = a[2] - b[2];
+        double rsq = dx0 * dx0 + dx1 * dx1 + dx2 * dx2;
+        int ti = type_of(i), tj = type_of(j);
+        for (int w = 0; w < p.n_wells; w++) {
+          if (!p.well_flag[w]) continue;
+          double g0 = p.water_gamma[w][ti][tj][0], g1 = p.water_gamma[w][ti][tj][1];
+          // `!fabs(g0 - g1) < delta` in the reference is true exactly when g0 != g1
+          if (g0 != g1 && rsq > p.w_rmin_sq[w] && rsq < p.w_rmax_sq[w]) {
+            double th, pr;
+            well_theta(sqrt(rsq), p.w_rmin_th[w], p.w_rmax_th[w], p.water_kappa, p.well_rmin[w], p.well_rmax[w], th, pr);
+            double tg = (g1 - g0) * th;
+            xi_w[i] += tg * sig_w[j];
+            xi_w[j] += tg * sig_w[i];
+          }
+        }
+      }
+    for (int i = 0; i < n; i++) xi_w[i] *= sigp_w[i];
+  }
+  // DL3: water, burial, helix-density radial forces (:7958-8057, 8116-8128)
+  for (int i = 0; i < n; i++)
+    for (int j = i + 1; j < n; j++) {
+      if (!(chain_of[i] != chain_of[j] || abs(i - j) > 1)) continue;
+      int ai = contact_atom(i), aj = contact_atom(j);
+      const double *a = &x[3 * ai], *b = &x[3 * aj];
+      double dx[3] = {a[0] - b[0], a[1] - b[1], a[2] - b[2]};
+      double rsq = dx[0] * dx[0] + dx[1] * dx[1] + dx[2] * dx[2];
+      double force = 0.0;
+      bool other = chain_of[i] != chain_of[j];
+      double r = sqrt(rsq);
+      if (p.water) {
+        int ti = type_of(i), tj = type_of(j);
+        for (int w = 0; w < p.n_wells; w++) {
+          if (!p.well_flag[w]) continue;
+          if ((other || abs(j - i) >= p.contact_cutoff) && rsq > p.w_rmin_sq[w] && rsq < p.w_rmax_sq[w]) {
+            double g0 = p.water_gamma[w][ti][tj][0], g1 = p.water_gamma[w][ti][tj][1];
+            double sg = fabs(g0 - g1) < 1e-5 ? 0.5 * (g0 + g1) : g0 + (g1 - g0) * sig_w[i] * sig_w[j];
+            double th, pr;
+            well_theta(r, p.w_rmin_th[w], p.w_rmax_th[w], p.water_kappa, p.well_rmin[w], p.well_rmax[w], th, pr);
+            E[ET_WATER] += -sg * th;
+            force += sg * pr;
+          }
+        }
+        if (rsq > p.w_rmin_sq[0] && rsq < p.w_rmax_sq[0]) {
+          double th, pr;
+          well_theta(r, p.w_rmin_th[0], p.w_rmax_th[0], p.water_kappa, p.well_rmin[0], p.well_rmax[0], th, pr);
+          if (fabs(xi_w[i]) > 1e-8) force += pr * xi_w[i];
+          if (fabs(xi_w[j]) > 1e-8) force += pr * xi_w[j];
+        }
+      }
+      if (p.burial && rsq > p.w_rmin_sq[0] && rsq < p.w_rmax_sq[0]) {
+        double th, pr;
+        well_theta(r, p.w_rmin_th[0], p.w_rmax_th[0], p.water_kappa, p.well_rmin[0], p.well_rmax[0], th, pr);
+        force += (bur[i] + bur[j]) * pr;
+      }
+      if (p.helix && rsq > p.h_rmin_sq && rsq < p.h_rmax_sq) {
+        int d = p.helix_i_diff;
+        double fac = xi1[i] + xi1[j];
+        if (i - d >= 0) fac += xi2[i - d];
+        if (j - d >= 0) fac += xi2[j - d];
+        if (fabs(fac) > 1e-6) {
+          double th, pr;
+          well_theta(r, p.h_rmin_th, p.h_rmax_th, p.helix_kappa, p.helix_rmin, p.helix_rmax, th, pr);
+          force += -fac * pr;
+        }
+      }
+      if (force != 0.0) {
+        addf(f, ai, force * dx[0], force * dx[1], force * dx[2]);
+        addf(f, aj, -force * dx[0], -force * dx[1], -force * dx[2]);
+      }
+    }
+  // DL3: DSSP, (O_i, N_j) for ordered residue pairs (:8064-8094)
+  if (p.dssp)
+    for (int i = 0; i < n; i++)
+      for (int j = 0; j < n; j++) {
+        if (i == j) continue;
+        if (!(chain_of[i] != chain_of[j] || abs(j - i) > 2)) continue;
+        if (se[j] == 'P' || last(i) || first(j)) continue;
+        if (j == 0) continue;
+        double dx0 = xo[3 * i] - xn[3 * j], dx1 = xo[3 * i + 1] - xn[3 * j + 1], dx2 = xo[3 * i + 2] - xn[3 * j + 2];
+        if (dx0 * dx0 + dx1 * dx1 + dx2 * dx2 < p.dssp_cut_sq) dssp_term(i, j, f);
+      }
+  // DL3: P_AP on CA pairs (:8096-8103)
+  if (p.pap)
+    for (int i = 0; i < n; i++)
+      for (int j = i + 1; j < n; j++) {
+        const double *a = &x[3 * ca[i]], *b = &x[3 * ca[j]];
+        double dx0 = a[0] - b[0], dx1 = a[1] - b[1], dx2 = a[2] - b[2];
+        if (dx0 * dx0 + dx1 * dx1 + dx2 * dx2 < p.pap_cutoff_sq) pap_term(i, j, f);
+      }
+}
+
+/* PairExcludedVolume::compute, pair_excluded_volume.cpp:50-138, over all
+   atom pairs except 1-2 bonded ones (special_bonds fene) */
+void System::excluded_volume(const double *x, double *f)
+{
+  int N = ntypes + 1;
+  int sign = ev_p % 2 == 0 ? 1 : -1;
+  e_pair = 0.0;
+  for (int i = 0; i < natoms; i++)
+    for (int j = i + 1; j < natoms; j++) {
+      int ti = atype[i], tj = atype[j];
+      double rc = (abs(ares[i] - ares[j]) < 5 && amol[i] == amol[j]) ? ev_cs[ti * N + tj] : ev_cl[ti * N + tj];
+      double dx = x[3 * i] - x[3 * j], dy = x[3 * i + 1] - x[3 * j + 1], dz = x[3 * i + 2] - x[3 * j + 2];
+      double rsq = dx * dx + dy * dy + dz * dz;
+      double r = sqrt(rsq);
+      if (!(r < rc)) continue;
+      bool excl = false;
+      for (int s : special[i])
+        if (s == j) excl = true;
+      if (excl) continue;
+      double dr = r - rc;
+      double pref = ev_lambda[ti * N + tj] * sign * pow(dr, ev_p - 1);
+      double fpair = r > 0.0 ? -pref * ev_p / r : 0.0;
+      addf(f, i, dx * fpair, dy * fpair, dz * fpair);
+      addf(f, j, -dx * fpair, -dy * fpair, -dz * fpair);
+      e_pair += pref * dr;
+    }
+}
+
+/* bond_style harmonic (LAMMPS documentation: E = K (r - r0)^2) */
+void System::bonds(const double *x, double *f)
+{
+  e_bond = 0.0;
+  for (size_t b = 0; b < b_t.size(); b++) {
+    int i = b_i[b], j = b_j[b];
+    double dx = x[3 * i] - x[3 * j], dy = x[3 * i + 1] - x[3 * j + 1], dz = x[3 * i + 2] - x[3 * j + 2];
+    double r = sqrt(dx * dx + dy * dy + dz * dz);
+    double dr = r - br0[b_t[b]];
+    double rk = bk[b_t[b]] * dr;
+    double fb = r > 0.0 ? -2.0 * rk / r : 0.0;
+    e_bond += rk * dr;
+    addf(f, i, dx * fb, dy * fb, dz * fb);
+    addf(f, j, -dx * fb, -dy * fb, -dz * fb);
+  }
+}
+
+/* compute_backbone, fix_backbone.cpp:7047-7673, then vexcluded and bonds */
+void System::compute(const double *x, double *f)
+{
+  const Params &p = P;
+  for (double &e : E) e = 0.0;
+  for (int k = 0; k < 3 * natoms; k++) f[k] = 0.0;
+  backbone_atoms(x);
+  for (int i = 0; i < n; i++) {
+    if (p.chain) chain_term(i, f);
+    if (!first(i) && !last(i) && p.chi && se[i] != 'G') chi_term(i, f);
+    if (!first(i) && !last(i) && p.rama && se[i] != 'G') rama_term(i, f);
+    if (p.fm) fm_term(i, f);
+  }
+  pair_terms(x, f);
+  for (int k = 1; k < NET; k++) E[ET_TOTAL] += E[k];
+  excluded_volume(x, f);
+  bonds(x, f);
+}
+
+thread_local std::string g_err;
+
+}  // namespace
+
+extern "C" {
+
+const char *oracle_last_error(void) { return g_err.c_str(); }
+
+void *oracle_create(const char *workdir, const char *data_file, const char *coeff_file, const char *seq_file,
+                    const char *pair_style, const char *pair_coeffs)
+{
+  System *S = new System();
+  try {
+    S->workdir = workdir ? workdir : "";
+    S->read_coeff(join(S->workdir, coeff_file));
+    S->read_seq(join(S->workdir, seq_file));
+    S->read_data(join(S->workdir, data_file));
+    build_residues(*S);
+    S->read_tables();
+    if (S->P.fm) S->read_mems();
+    S->pair_setup(pair_style, pair_coeffs ? pair_coeffs : "");
+  } catch (std::exception &e) {
+    g_err = e.what();
+    delete S;
+    return nullptr;
+  }
+  return S;
+}
+
+void oracle_destroy(void *h) { delete (System *) h; }
+int oracle_natoms(void *h) { return ((System *) h)->natoms; }
+int oracle_nres(void *h) { return ((System *) h)->n; }
+
+int oracle_compute(void *h, const double *x, double *f, double *energies)
+{
+  System *S = (System *) h;
+  try {
+    std::vector<double> tmp;
+    if (!f) {
+      tmp.resize(3 * S->natoms);
+      f = tmp.data();
+    }
+    S->compute(x, f);
+    if (energies) {
+      for (int k = 0; k < NET; k++) energies[k] = S->E[k];
+      energies[18] = S->e_pair;
+      energies[19] = S->e_bond;
+      energies[20] = 0.0;
+    }
+  } catch (std::exception &e) {
+    g_err = e.what();
+    return -1;
+  }
+  return 0;
+}
+
+int oracle_residue_arrays(void *h, double *out)
+{
+  System *S = (System *) h;
+  for (int i = 0; i < S->n; i++) {
+    out[8 * i + 0] = S->rho_w[i];
+    out[8 * i + 1] = S->rho_h[i];
+    out[8 * i + 2] = S->xi_w[i];
+    out[8 * i + 3] = S->xi1[i];
+    out[8 * i + 4] = S->xi2[i];
+    out[8 * i + 5] = S->bur[i];
+    out[8 * i + 6] = S->sig_w[i];
+    out[8 * i + 7] = S->sig_h[i];
+  }
+  return S->n;
+}
+
+int oracle_selection_digest(void *h, unsigned long long *counts, unsigned long long *hash)
+{
+  System *S = (System *) h;
+  counts[0] = S->sel_count[0];
+  counts[1] = S->sel_count[1];
+  *hash = S->sel_hash;
+  return 0;
+}
+
+int oracle_run(void *h, double *x, double *v, long long step0, long long nsteps, double dt, int langevin,
+               double t_start, double t_stop, double damp, unsigned long long seed, double *thermo)
+{
+  System *S = (System *) h;
+  try {
+    int N = S->natoms;
+    std::vector<double> f(3 * N);
+    long long begin = step0, end = step0 + nsteps;
+    auto ke = [&]() {
+      double s = 0.0;
+      for (int i = 0; i < N; i++) {
+        double m = S->mass[S->atype[i]];
+        s += m * (v[3 * i] * v[3 * i] + v[3 * i + 1] * v[3 * i + 1] + v[3 * i + 2] * v[3 * i + 2]);
+      }
+      return 0.5 * MVV2E * s;
+    };
+    /* fix langevin post_force: uniform noise, units real */
+    auto langevin_force = [&](long long step) {
+      if (!langevin) return;
+      double delta = end != begin ? (double) (step - begin) / (double) (end - begin) : 0.0;
+      double tsqrt = sqrt(t_start + delta * (t_stop - t_start));
+      for (int i = 0; i < N; i++) {
+        double m = S->mass[S->atype[i]];
+        double g1 = -m / damp / FTM2V;
+        double g2 = sqrt(m) * sqrt(24.0 * BOLTZ / damp / dt / MVV2E) / FTM2V * tsqrt;
+        for (int k = 0; k < 3; k++)
+          f[3 * i + k] += g1 * v[3 * i + k] + g2 * (uniform01(seed, step, S->tag[i], k) - 0.5);
+      }
+    };
+    auto row = [&](long long r) {
+      if (!thermo) return;
+      thermo[4 * r + 0] = S->E[ET_TOTAL];
+      thermo[4 * r + 1] = S->e_pair;
+      thermo[4 * r + 2] = S->e_bond;
+      thermo[4 * r + 3] = ke();
+    };
+    S->compute(x, f.data());
+    langevin_force(begin);
+    row(0);
+    double dtf = 0.5 * dt * FTM2V;
+    for (long long s = 1; s <= nsteps; s++) {
+      for (int i = 0; i < N; i++) {
+        double dtfm = dtf / S->mass[S->atype[i]];
+        for (int k = 0; k < 3; k++) {
+          v[3 * i + k] += dtfm * f[3 * i + k];
+          x[3 * i + k] += dt * v[3 * i + k];
+        }
+      }
+      S->compute(x, f.data());
+      langevin_force(begin + s);
+      for (int i = 0; i < N; i++) {
+        double dtfm = dtf / S->mass[S->atype[i]];
+        for (int k = 0; k < 3; k++) v[3 * i + k] += dtfm * f[3 * i + k];
+      }
+      row(s);
+    }
+  } catch (std::exception &e) {
+    g_err = e.what();
+    return -1;
+  }
+  return 0;
+}
+
+double oracle_uniform(unsigned long long seed, long long step, long long tag, int comp)
+{
+  return uniform01(seed, step, tag, comp);
+}
+
+}  // extern "C"

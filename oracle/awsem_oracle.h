@@ -1,0 +1,43 @@
+/* FP64 CPU restatement of the AWSEM-MD per-step force and energy path
+   (oracle; test infrastructure only -- never part of the product path).
+
+   C ABI, loaded with ctypes by tests/ and bench.py's CPU baseline.  Arrays
+   of positions, velocities and forces are [natoms][3] doubles in data-file
+   atom order (sorted by atom id).  Energies: out[0..17] follow the reference
+   energy[] enum (fix_backbone.h:330-332: total, chain, shake, chi, rama,
+   excluded, dssp, p_ap, water, burial, helix, amh-go, frag_mem, vec_fm,
+   contact_restraints, membrane, ssb, dh), out[18] = pair vexcluded,
+   out[19] = harmonic bonds, out[20] = kinetic energy. */
+#ifndef AWSEM_ORACLE_H
+#define AWSEM_ORACLE_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+void *oracle_create(const char *workdir, const char *data_file, const char *coeff_file,
+                    const char *seq_file, const char *pair_style, const char *pair_coeffs);
+void oracle_destroy(void *h);
+const char *oracle_last_error(void);
+int oracle_natoms(void *h);
+int oracle_nres(void *h);
+/* positions / velocities in, forces and energies out (no Langevin force) */
+int oracle_compute(void *h, const double *x, double *f, double *energies);
+/* per-residue intermediates of the last compute: rho_w, rho_h, xi_w, xi1_h,
+   xi2_h, burial_coefficient, sigma_w, sigma_h ([n][8]) */
+int oracle_residue_arrays(void *h, double *out);
+/* number of (i<j) contact-bead pairs selected into each density well by the
+   last compute: counts[0] water well 0 (DL1), counts[1] helix well (DL1),
+   and a 64-bit order-independent hash of the selected (i, j, well) triples */
+int oracle_selection_digest(void *h, unsigned long long *counts, unsigned long long *hash);
+/* nsteps of velocity Verlet (+ Langevin); x and v updated in place.
+   thermo (optional): (nsteps+1) x 4 rows of [fix total, vexcluded, bonds, ke]. */
+int oracle_run(void *h, double *x, double *v, long long step0, long long nsteps, double dt,
+               int langevin, double t_start, double t_stop, double damp,
+               unsigned long long seed, double *thermo);
+double oracle_uniform(unsigned long long seed, long long step, long long tag, int comp);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

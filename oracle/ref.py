@@ -1,0 +1,182 @@
+"""ctypes bindings for the oracle libraries (test infrastructure only).
+
+* ``RefSystem``: the reference FixBackbone + PairExcludedVolume, compiled
+  unmodified from the reference sources against the LAMMPS-API shim
+  (``oracle/_ref/libawsem_ref.so``, built by ``make -C oracle ref``).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_LIB = os.path.join(HERE, "_ref", "libawsem_ref.so")
+
+_ref = None
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_LIB)
+
+
+def _load_ref():
+    global _ref
+    if _ref is None:
+        lib = C.CDLL(REF_LIB)
+        lib.ref_create.restype = C.c_void_p
+        lib.ref_create.argtypes = [C.c_char_p] * 6 + [C.c_double, C.c_int, C.c_int, C.c_int]
+        lib.ref_destroy.argtypes = [C.c_void_p]
+        lib.ref_natoms.argtypes = [C.c_void_p]
+        lib.ref_fix_cutoff.argtypes = [C.c_void_p]
+        lib.ref_fix_cutoff.restype = C.c_double
+        lib.ref_get.argtypes = [C.c_void_p, C.c_char_p, C.c_void_p]
+        lib.ref_set.argtypes = [C.c_void_p, C.c_char_p, C.c_void_p]
+        lib.ref_energies.argtypes = [C.c_void_p, C.c_void_p]
+        lib.ref_compute.argtypes = [C.c_void_p, C.c_longlong, C.c_void_p]
+        lib.ref_residue_arrays.argtypes = [C.c_void_p, C.c_void_p]
+        lib.ref_run.argtypes = [C.c_void_p, C.c_longlong, C.c_double, C.c_int, C.c_double, C.c_double,
+                                C.c_double, C.c_ulonglong, C.c_void_p]
+        lib.ref_nbuilds.argtypes = [C.c_void_p]
+        lib.ref_nbuilds.restype = C.c_long
+        lib.ref_last_error.restype = C.c_char_p
+        lib.ref_uniform.restype = C.c_double
+        lib.ref_uniform.argtypes = [C.c_ulonglong, C.c_longlong, C.c_longlong, C.c_int]
+        _ref = lib
+    return _ref
+
+
+class RefSystem:
+    """One reference FixBackbone system hosted by the shim MD loop."""
+
+    def __init__(self, files: dict, skin=2.0, every=1, delay=0, check=1):
+        lib = _load_ref()
+        self.lib = lib
+        self.h = lib.ref_create(files["workdir"].encode(), files["data"].encode(), files["coeff"].encode(),
+                                files["seq"].encode(), files["pair_style"].encode(),
+                                files["pair_coeffs"].encode(), skin, every, delay, check)
+        if not self.h:
+            raise RuntimeError(lib.ref_last_error().decode())
+        self.natoms = lib.ref_natoms(self.h)
+
+    def close(self):
+        if self.h:
+            self.lib.ref_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def get(self, what: str) -> np.ndarray:
+        out = np.zeros((self.natoms, 3))
+        self.lib.ref_get(self.h, what.encode(), out.ctypes.data)
+        return out
+
+    def set(self, what: str, arr: np.ndarray):
+        a = np.ascontiguousarray(arr, dtype=np.float64)
+        self.lib.ref_set(self.h, what.encode(), a.ctypes.data)
+
+    def energies(self) -> np.ndarray:
+        out = np.zeros(21)
+        self.lib.ref_energies(self.h, out.ctypes.data)
+        return out
+
+    def compute(self, step=0) -> np.ndarray:
+        f = np.zeros((self.natoms, 3))
+        if self.lib.ref_compute(self.h, step, f.ctypes.data) != 0:
+            raise RuntimeError(self.lib.ref_last_error().decode())
+        return f
+
+    def residue_arrays(self, n_res: int) -> np.ndarray:
+        out = np.zeros((n_res, 6))
+        self.lib.ref_residue_arrays(self.h, out.ctypes.data)
+        return out
+
+    def run(self, nsteps, dt=2.0, langevin=True, t_start=300.0, t_stop=300.0, damp=500.0, seed=1):
+        thermo = np.zeros((nsteps + 1, 4))
+        if self.lib.ref_run(self.h, nsteps, dt, int(langevin), t_start, t_stop, damp, seed, thermo.ctypes.data) != 0:
+            raise RuntimeError(self.lib.ref_last_error().decode())
+        return thermo
+
+
+# --------------------------------------------------------------------------
+# FP64 restatement (oracle/_build/liboracle.so, built by ``make -C oracle``)
+
+ORACLE_LIB = os.path.join(HERE, "_build", "liboracle.so")
+_orc = None
+
+
+def oracle_available() -> bool:
+    return os.path.exists(ORACLE_LIB)
+
+
+def _load_oracle():
+    global _orc
+    if _orc is None:
+        lib = C.CDLL(ORACLE_LIB)
+        lib.oracle_create.restype = C.c_void_p
+        lib.oracle_create.argtypes = [C.c_char_p] * 6
+        lib.oracle_destroy.argtypes = [C.c_void_p]
+        lib.oracle_last_error.restype = C.c_char_p
+        lib.oracle_natoms.argtypes = [C.c_void_p]
+        lib.oracle_nres.argtypes = [C.c_void_p]
+        lib.oracle_compute.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        lib.oracle_residue_arrays.argtypes = [C.c_void_p, C.c_void_p]
+        lib.oracle_selection_digest.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        lib.oracle_run.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_longlong, C.c_longlong, C.c_double,
+                                   C.c_int, C.c_double, C.c_double, C.c_double, C.c_ulonglong, C.c_void_p]
+        lib.oracle_uniform.restype = C.c_double
+        lib.oracle_uniform.argtypes = [C.c_ulonglong, C.c_longlong, C.c_longlong, C.c_int]
+        _orc = lib
+    return _orc
+
+
+class OracleSystem:
+    """FP64 restatement of the AWSEM force field (the oracle proper)."""
+
+    def __init__(self, files: dict):
+        lib = _load_oracle()
+        self.lib = lib
+        self.h = lib.oracle_create(files["workdir"].encode(), files["data"].encode(), files["coeff"].encode(),
+                                   files["seq"].encode(), files["pair_style"].encode(), files["pair_coeffs"].encode())
+        if not self.h:
+            raise RuntimeError(lib.oracle_last_error().decode())
+        self.natoms = lib.oracle_natoms(self.h)
+        self.nres = lib.oracle_nres(self.h)
+
+    def close(self):
+        if self.h:
+            self.lib.oracle_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def compute(self, x: np.ndarray):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        f = np.zeros((self.natoms, 3))
+        e = np.zeros(21)
+        if self.lib.oracle_compute(self.h, x.ctypes.data, f.ctypes.data, e.ctypes.data) != 0:
+            raise RuntimeError(self.lib.oracle_last_error().decode())
+        return f, e
+
+    def residue_arrays(self) -> np.ndarray:
+        out = np.zeros((self.nres, 8))
+        self.lib.oracle_residue_arrays(self.h, out.ctypes.data)
+        return out
+
+    def selection_digest(self):
+        counts = np.zeros(2, dtype=np.uint64)
+        h = np.zeros(1, dtype=np.uint64)
+        self.lib.oracle_selection_digest(self.h, counts.ctypes.data, h.ctypes.data)
+        return int(counts[0]), int(counts[1]), int(h[0])
+
+    def run(self, x, v, nsteps, step0=0, dt=2.0, langevin=True, t_start=300.0, t_stop=300.0, damp=500.0, seed=1):
+        x = np.ascontiguousarray(x, dtype=np.float64).copy()
+        v = np.ascontiguousarray(v, dtype=np.float64).copy()
+        thermo = np.zeros((nsteps + 1, 4))
+        if self.lib.oracle_run(self.h, x.ctypes.data, v.ctypes.data, step0, nsteps, dt, int(langevin), t_start,
+                               t_stop, damp, seed, thermo.ctypes.data) != 0:
+            raise RuntimeError(self.lib.oracle_last_error().decode())
+        return x, v, thermo
