@@ -1,0 +1,843 @@
+// Single-system AWSEM engine: device buffers, the per-step launch sequence,
+// CUDA-graph capture of MD steps, and the C ABI of include/awsem_gpu.h.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "awsem_gpu.h"
+#include "awsem_kernels.cuh"
+#include "awsem_model.h"
+
+namespace awsem {
+
+static thread_local std::string g_last_error;
+
+struct CudaError : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+
+#define CK(call)                                                                                 \
+  do {                                                                                           \
+    cudaError_t e_ = (call);                                                                     \
+    if (e_ != cudaSuccess)                                                                       \
+      throw CudaError(std::string(#call) + ": " + cudaGetErrorString(e_) + " (" __FILE__ ":" + \
+                      std::to_string(__LINE__) + ")");                                           \
+  } while (0)
+
+template <typename T> struct DBuf {
+  T *p = nullptr;
+  size_t n = 0;
+  DBuf() = default;
+  DBuf(const DBuf &) = delete;
+  DBuf &operator=(const DBuf &) = delete;
+  ~DBuf() { release(); }
+  void release()
+  {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  void alloc(size_t count)
+  {
+    release();
+    n = count;
+    if (count) CK(cudaMalloc(&p, count * sizeof(T)));
+  }
+  void upload(const std::vector<T> &h, cudaStream_t s)
+  {
+    alloc(std::max<size_t>(h.size(), 1));
+    if (!h.empty()) CK(cudaMemcpyAsync(p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, s));
+  }
+  void zero(cudaStream_t s)
+  {
+    if (n) CK(cudaMemsetAsync(p, 0, n * sizeof(T), s));
+  }
+};
+
+constexpr double FTM2V = 1.0 / 48.88821291 / 48.88821291;
+constexpr double MVV2E = 48.88821291 * 48.88821291;
+constexpr double BOLTZ = 0.0019872067;
+
+class EngineBase {
+ public:
+  virtual ~EngineBase() {}
+  SystemInput in;
+  int device = 0;
+  long long step = 0;
+  virtual void setup() = 0;
+  virtual void compute(long long step, const double *x_ext, double *f_ext, double *energies, int groups) = 0;
+  virtual void set_state(const double *x_ext, const double *v_ext) = 0;
+  virtual void get_state(double *x_ext, double *v_ext) = 0;
+  virtual void run(long long nsteps, const awsem_run_params &rp, double *thermo) = 0;
+  virtual void energies(double *out) = 0;
+  virtual void forces(double *f_ext) = 0;
+  virtual void residue_arrays(double *out) = 0;
+  virtual void nl_stats(int *nbuilds, double *radius, int *maxc, int *overflow) = 0;
+  virtual void profile(int reps, double *ms) = 0;
+  virtual void model_info(long long *info) = 0;
+  virtual double run_ms() const = 0;
+};
+
+static const char *kKernelNames[AWSEM_NKERNELS] = {"prepare", "nl_decide", "nl_build", "density", "residue",
+                                                   "water_xi", "pair", "fragmem", "bonds", "finish"};
+
+template <typename R> class Engine : public EngineBase {
+
+ public:
+  cudaStream_t s0 = nullptr, s1 = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  DBuf<int> res_type, res_flags, res_chain, chain_start, chain_end, atom_tag, atom_type;
+  DBuf<double> aps, tables, x, v, mass, g1, g2, ftot, work, e_res, energy;
+  DBuf<double4> pos, cb_build;
+  DBuf<unsigned long long> facc;
+  DBuf<int> nbr, ncount;
+  DBuf<dev::NLState> nl;
+  DBuf<long long> dstep;
+  DBuf<double> ev_pref, ev_cs, ev_cl;
+  DBuf<unsigned> excl_self, excl_next;
+  DBuf<int> bond_start, bond_i, bond_j;
+  DBuf<double> bond_k, bond_r0;
+  DBuf<int> fm_row;
+  DBuf<R> fm_rf, fm_coef;
+  DBuf<double> thermo_rows;
+  int cap = 0;
+  int groups_all = dev::G_FIX | dev::G_PAIR | dev::G_BOND;
+  double skin = 2.0;
+  int neigh_every = 0;
+  std::vector<double> hx, hv;  // host staging (internal order)
+
+  ~Engine() override
+  {
+    release_graphs();
+    if (ev_run0) cudaEventDestroy(ev_run0);
+    if (ev_run1) cudaEventDestroy(ev_run1);
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    if (ev_join) cudaEventDestroy(ev_join);
+    if (s0) cudaStreamDestroy(s0);
+    if (s1) cudaStreamDestroy(s1);
+  }
+
+  int n() const { return in.top.n_res; }
+  int natoms() const { return in.top.n_atoms; }
+
+  dev::StepArgs<R> args(int groups)
+  {
+    dev::StepArgs<R> a{};
+    a.s.n_res = n();
+    a.s.res_type = res_type.p;
+    a.s.res_flags = res_flags.p;
+    a.s.res_chain = res_chain.p;
+    a.s.chain_start = chain_start.p;
+    a.s.chain_end = chain_end.p;
+    a.s.aps = aps.p;
+    a.s.tables = tables.p;
+    a.s.pos = pos.p;
+    a.s.facc = facc.p;
+    a.n_atoms = natoms();
+    a.x = x.p;
+    a.v = v.p;
+    a.mass = mass.p;
+    a.atom_tag = atom_tag.p;
+    double *w = work.p;
+    size_t nn = (size_t) n();
+    a.rho_w = w;
+    a.rho_h = w + nn;
+    a.sig_w = w + 2 * nn;
+    a.sigp_w = w + 3 * nn;
+    a.sig_h = w + 4 * nn;
+    a.sigp_h = w + 5 * nn;
+    a.xi_w = w + 6 * nn;
+    a.xi1 = w + 7 * nn;
+    a.xi2 = w + 8 * nn;
+    a.bur = w + 9 * nn;
+    a.e_res = e_res.p;
+    a.nbr = nbr.p;
+    a.ncount = ncount.p;
+    a.cap = cap;
+    a.cb_build = cb_build.p;
+    a.nl = nl.p;
+    a.ntypes = in.top.ntypes;
+    a.ev_p = in.top.ev_p;
+    a.ev_pref = ev_pref.p;
+    a.ev_cs = ev_cs.p;
+    a.ev_cl = ev_cl.p;
+    a.atom_type = atom_type.p;
+    a.excl_self = excl_self.p;
+    a.excl_next = excl_next.p;
+    a.bond_start = bond_start.p;
+    a.bond_i = bond_i.p;
+    a.bond_j = bond_j.p;
+    a.bond_k = bond_k.p;
+    a.bond_r0 = bond_r0.p;
+    a.fm_row = fm_row.p;
+    a.fm_rf = fm_rf.p;
+    a.fm_coef = in.fm.uniform ? nullptr : fm_coef.p;
+    a.fm_uniform = in.fm.uniform_coef;
+    a.groups = groups;
+    a.step = dstep.p;
+    return a;
+  }
+
+  void setup() override
+  {
+    CK(cudaSetDevice(device));
+    CK(cudaStreamCreateWithFlags(&s0, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&s1, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
+    const Topology &t = in.top;
+    int nn = n(), na = natoms();
+    res_type.upload(t.res_type, s0);
+    res_flags.upload(t.res_flags, s0);
+    res_chain.upload(t.res_chain, s0);
+    chain_start.upload(t.chain_start, s0);
+    chain_end.upload(t.chain_end, s0);
+    atom_tag.upload(t.atom_tag, s0);
+    atom_type.upload(t.atom_type, s0);
+    aps.upload(t.aps, s0);
+    tables.upload(in.ff.tables, s0);
+    x.upload(in.x, s0);
+    v.upload(in.v, s0);
+    mass.upload(t.mass, s0);
+    g1.alloc(na);
+    g2.alloc(na);
+    ftot.alloc((size_t) 3 * na);
+    ftot.zero(s0);
+    work.alloc((size_t) 10 * nn);
+    work.zero(s0);
+    e_res.alloc((size_t) E_SLOTS * nn);
+    e_res.zero(s0);
+    energy.alloc(E_SLOTS);
+    pos.alloc((size_t) dev::N_BEADS * nn);
+    cb_build.alloc(nn);
+    cb_build.zero(s0);
+    facc.alloc((size_t) 3 * na);
+    facc.zero(s0);
+    ncount.alloc(nn);
+    ncount.zero(s0);
+    nl.alloc(1);
+    dstep.alloc(1);
+    ev_pref.upload(t.ev_pref, s0);
+    ev_cs.upload(t.ev_cs, s0);
+    ev_cl.upload(t.ev_cl, s0);
+    excl_self.upload(t.excl_self, s0);
+    excl_next.upload(t.excl_next, s0);
+    // bonds grouped by the residue of their first atom (stable)
+    std::vector<int> order(t.bond_i.size());
+    for (size_t b = 0; b < order.size(); b++) order[b] = (int) b;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return t.bond_i[a] / 3 < t.bond_i[b] / 3; });
+    std::vector<int> bs(nn + 1, 0), bi, bj;
+    std::vector<double> bk, br;
+    for (int b : order) {
+      bs[t.bond_i[b] / 3 + 1]++;
+      bi.push_back(t.bond_i[b]);
+      bj.push_back(t.bond_j[b]);
+      bk.push_back(t.bond_k[b]);
+      br.push_back(t.bond_r0[b]);
+    }
+    for (int r = 0; r < nn; r++) bs[r + 1] += bs[r];
+    bond_start.upload(bs, s0);
+    bond_i.upload(bi, s0);
+    bond_j.upload(bj, s0);
+    bond_k.upload(bk, s0);
+    bond_r0.upload(br, s0);
+    // fragment memory in the engine's arithmetic type
+    const FMTable &fm = in.fm;
+    std::vector<int> rows = fm.row_start;
+    if (rows.empty()) rows.assign((size_t) nn * std::max(fm.nd, 1) + 1, 0);
+    fm_row.upload(rows, s0);
+    std::vector<R> rf(fm.rf.begin(), fm.rf.end()), cf(fm.coef.begin(), fm.coef.end());
+    fm_rf.upload(rf, s0);
+    fm_coef.upload(cf, s0);
+    if (!(in.ff.p.terms & T_FM)) in.ff.p.fm_nd = 0;
+    // pair-list radii of the terms
+    dev::NLState st{};
+    const FFParams &p = in.ff.p;
+    float rc = 0.f;
+    for (int w = 0; w < p.n_wells; w++) rc = std::max(rc, (float) p.w_rmax_th[w]);
+    if (p.terms & T_HELIX) rc = std::max(rc, (float) p.h_rmax_th);
+    st.r_contact = rc;
+    st.r_dssp = (p.terms & T_DSSP) ? (float) p.dssp_cut : 0.f;
+    st.r_pap = (p.terms & T_PAP) ? (float) sqrt(p.pap_cutoff_sq) : 0.f;
+    double evmax = 0.0;
+    int N = t.ntypes + 1;
+    for (int a = 1; a <= t.ntypes; a++)
+      for (int b = 1; b <= t.ntypes; b++)
+        if (t.ev_pref[a * N + b] != 0.0) evmax = std::max(evmax, std::max(t.ev_cl[a * N + b], t.ev_cs[a * N + b]));
+    st.r_ev = (float) evmax;
+    st.skin = (float) skin;
+    CK(cudaMemcpyAsync(nl.p, &st, sizeof st, cudaMemcpyHostToDevice, s0));
+    long long s = step;
+    CK(cudaMemcpyAsync(dstep.p, &s, sizeof s, cudaMemcpyHostToDevice, s0));
+    // size the pair list from a first build
+    cap = 32;
+    nbr.alloc((size_t) cap * nn);
+    for (int attempt = 0; attempt < 8; attempt++) {
+      launch_prepare_and_list(args(groups_all), s0, true, false);
+      dev::NLState got;
+      CK(cudaMemcpyAsync(&got, nl.p, sizeof got, cudaMemcpyDeviceToHost, s0));
+      CK(cudaStreamSynchronize(s0));
+      if (!got.overflow) {
+        int maxc = max_count();
+        int want = std::max(64, ((2 * maxc + 31) / 32) * 32);
+        if (want > cap) {
+          resize_list(want);
+          continue;
+        }
+        break;
+      }
+      resize_list(std::max(2 * cap, ((2 * got.overflow + 31) / 32) * 32));
+    }
+  }
+
+  int max_count()
+  {
+    std::vector<int> c(n());
+    CK(cudaMemcpyAsync(c.data(), ncount.p, sizeof(int) * n(), cudaMemcpyDeviceToHost, s0));
+    CK(cudaStreamSynchronize(s0));
+    return c.empty() ? 0 : *std::max_element(c.begin(), c.end());
+  }
+
+  void resize_list(int newcap)
+  {
+    cap = newcap;
+    nbr.alloc((size_t) cap * n());
+    dev::NLState st;
+    CK(cudaMemcpyAsync(&st, nl.p, sizeof st, cudaMemcpyDeviceToHost, s0));
+    CK(cudaStreamSynchronize(s0));
+    st.overflow = 0;
+    st.r_list = 0.f;  // forces a rebuild
+    CK(cudaMemcpyAsync(nl.p, &st, sizeof st, cudaMemcpyHostToDevice, s0));
+  }
+
+  void launch_prepare_and_list(const dev::StepArgs<R> &a, cudaStream_t s, bool force, bool advance)
+  {
+    const FFParams &p = in.ff.p;
+    int nn = n();
+    int tb = 128, nb = (nn + tb - 1) / tb, wb = (nn * 32 + tb - 1) / tb;
+    dev::k_prepare<R><<<nb, tb, 0, s>>>(a, p);
+    dev::k_nl_decide<<<1, 1, 0, s>>>(nl.p, force ? 1 : 0, advance ? dstep.p : nullptr);
+    dev::k_nl_build<R><<<wb, tb, 0, s>>>(a, 0, nn);
+  }
+
+  // one force evaluation (everything up to the fixed-point force sums)
+  void launch_eval(const dev::StepArgs<R> &a, bool advance)
+  {
+    const FFParams &p = in.ff.p;
+    int nn = n();
+    int tb = 128, nb = (nn + tb - 1) / tb, wb = (nn * 32 + tb - 1) / tb;
+    launch_prepare_and_list(a, s0, false, advance);
+    bool fm = (a.groups & dev::G_FIX) && p.fm_nd > 0;
+    if (fm) {
+      // fragment memory is independent of the pair passes: second stream
+      CK(cudaEventRecord(ev_fork, s0));
+      CK(cudaStreamWaitEvent(s1, ev_fork, 0));
+      dev::k_fragmem<R><<<wb, tb, 0, s1>>>(a, p);
+      CK(cudaEventRecord(ev_join, s1));
+    }
+    dev::k_density<R><<<wb, tb, 0, s0>>>(a, p);
+    dev::k_residue<R><<<nb, tb, 0, s0>>>(a, p);
+    dev::k_water_xi<R><<<wb, tb, 0, s0>>>(a, p);
+    dev::k_pair<R><<<wb, tb, 0, s0>>>(a, p);
+    if (a.groups & dev::G_BOND) dev::k_bonds<R><<<nb, tb, 0, s0>>>(a);
+    if (fm) CK(cudaStreamWaitEvent(s0, ev_join, 0));
+  }
+
+  void zero_unwritten_energies(int groups)
+  {
+    // slots the selected groups do not write must read as zero
+    int nn = n();
+    if (!(groups & dev::G_FIX) || !(in.ff.p.terms & T_FM) || in.ff.p.fm_nd == 0)
+      CK(cudaMemsetAsync(e_res.p + (size_t) E_FRAGMEM * nn, 0, sizeof(double) * nn, s0));
+    if (!(groups & dev::G_BOND)) CK(cudaMemsetAsync(e_res.p + (size_t) E_BOND * nn, 0, sizeof(double) * nn, s0));
+  }
+
+  void reduce_energies()
+  {
+    dev::k_energy_reduce<<<E_SLOTS, 256, 0, s0>>>(e_res.p, n(), 0, n(), energy.p);
+  }
+
+  void compute(long long st, const double *x_ext, double *f_ext, double *energies_out, int groups) override
+  {
+    const Topology &t = in.top;
+    int na = natoms();
+    hx.resize((size_t) 3 * na);
+    for (int a = 0; a < na; a++)
+      for (int k = 0; k < 3; k++) hx[3 * a + k] = x_ext[3 * t.ext_of[a] + k];
+    CK(cudaMemcpyAsync(x.p, hx.data(), sizeof(double) * 3 * na, cudaMemcpyHostToDevice, s0));
+    CK(cudaMemcpyAsync(dstep.p, &st, sizeof st, cudaMemcpyHostToDevice, s0));
+    step = st;
+    zero_unwritten_energies(groups);
+    auto a = args(groups);
+    launch_eval(a, false);
+    int tb = 256;
+    dev::k_total_force<R><<<(3 * na + tb - 1) / tb, tb, 0, s0>>>(a, ftot.p);
+    reduce_energies();
+    CK(cudaGetLastError());
+    std::vector<double> f((size_t) 3 * na);
+    CK(cudaMemcpyAsync(f.data(), ftot.p, sizeof(double) * 3 * na, cudaMemcpyDeviceToHost, s0));
+    double e[E_SLOTS];
+    CK(cudaMemcpyAsync(e, energy.p, sizeof e, cudaMemcpyDeviceToHost, s0));
+    CK(cudaStreamSynchronize(s0));
+    check_list();
+    for (int at = 0; at < na; at++)
+      for (int k = 0; k < 3; k++) f_ext[3 * t.ext_of[at] + k] += f[3 * at + k];
+    if (energies_out) finish_energies(e, energies_out, false);
+  }
+
+  void finish_energies(const double *e, double *out, bool with_ke)
+  {
+    for (int k = 0; k < E_SLOTS; k++) out[k] = e[k];
+    out[E_TOTAL] = 0.0;
+    for (int k = 1; k < E_FIX_TERMS; k++) out[E_TOTAL] += e[k];
+    if (!with_ke) out[E_KIN] = 0.0;
+  }
+
+  void check_list()
+  {
+    dev::NLState st;
+    CK(cudaMemcpy(&st, nl.p, sizeof st, cudaMemcpyDeviceToHost));
+    if (st.overflow)
+      throw std::runtime_error("residue pair list overflow (capacity " + std::to_string(cap) + ", needed " +
+                               std::to_string(st.overflow) + "); results of this call are invalid");
+  }
+
+  void set_state(const double *x_ext, const double *v_ext) override
+  {
+    const Topology &t = in.top;
+    int na = natoms();
+    for (int a = 0; a < na; a++)
+      for (int k = 0; k < 3; k++) {
+        if (x_ext) in.x[3 * a + k] = x_ext[3 * t.ext_of[a] + k];
+        if (v_ext) in.v[3 * a + k] = v_ext[3 * t.ext_of[a] + k];
+      }
+    if (x_ext) CK(cudaMemcpyAsync(x.p, in.x.data(), sizeof(double) * 3 * na, cudaMemcpyHostToDevice, s0));
+    if (v_ext) CK(cudaMemcpyAsync(v.p, in.v.data(), sizeof(double) * 3 * na, cudaMemcpyHostToDevice, s0));
+    CK(cudaStreamSynchronize(s0));
+  }
+
+  void get_state(double *x_ext, double *v_ext) override
+  {
+    const Topology &t = in.top;
+    int na = natoms();
+    std::vector<double> hx2((size_t) 3 * na), hv2((size_t) 3 * na);
+    CK(cudaMemcpyAsync(hx2.data(), x.p, sizeof(double) * 3 * na, cudaMemcpyDeviceToHost, s0));
+    CK(cudaMemcpyAsync(hv2.data(), v.p, sizeof(double) * 3 * na, cudaMemcpyDeviceToHost, s0));
+    CK(cudaStreamSynchronize(s0));
+    for (int a = 0; a < na; a++)
+      for (int k = 0; k < 3; k++) {
+        if (x_ext) x_ext[3 * t.ext_of[a] + k] = hx2[3 * a + k];
+        if (v_ext) v_ext[3 * t.ext_of[a] + k] = hv2[3 * a + k];
+      }
+  }
+
+  // Graphs of `count` consecutive MD steps.  Every per-run value (integrator
+  // parameters, step counter, thermo buffer) lives in device memory, so a
+  // graph stays valid across runs and is instantiated once.
+  cudaGraphExec_t graphs[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [thermo][chunk]
+  static constexpr int kChunk = 25;
+  DBuf<dev::Integrator> d_integ;
+  DBuf<double *> d_thermo_ptr;
+  cudaEvent_t ev_run0 = nullptr, ev_run1 = nullptr;
+  double last_run_ms = 0.0;
+
+  void capture_steps(cudaGraphExec_t &exec, int count, bool thermo)
+  {
+    auto a = args(groups_all);
+    int nn = n(), tb = 128, nb = (nn + tb - 1) / tb;
+    cudaGraph_t graph;
+    CK(cudaStreamBeginCapture(s0, cudaStreamCaptureModeThreadLocal));
+    for (int c = 0; c < count; c++) {
+      launch_eval(a, true);
+      dev::k_finish<R><<<nb, tb, 0, s0>>>(a, d_integ.p, g1.p, g2.p, ftot.p, x.p);
+      if (thermo) dev::k_thermo<<<1, 256, 0, s0>>>(e_res.p, nn, dstep.p, d_integ.p, thermo_rows.p);
+    }
+    CK(cudaStreamEndCapture(s0, &graph));
+    CK(cudaGraphInstantiate(&exec, graph, 0));
+    CK(cudaGraphDestroy(graph));
+  }
+
+  void release_graphs()
+  {
+    for (auto &row : graphs)
+      for (auto &g : row)
+        if (g) {
+          cudaGraphExecDestroy(g);
+          g = nullptr;
+        }
+  }
+
+  awsem_run_params last_rp{2.0, 1, 300.0, 300.0, 500.0, 1ull, 2.0, 0};
+
+  void upload_integrator(const dev::Integrator &integ)
+  {
+    if (!d_integ.p) d_integ.alloc(1);
+    CK(cudaMemcpyAsync(d_integ.p, &integ, sizeof integ, cudaMemcpyHostToDevice, s0));
+  }
+
+  void profile(int reps, double *ms) override
+  {
+    if (reps <= 0) throw std::invalid_argument("reps must be positive");
+    set_thermostat(last_rp);
+    upload_integrator(make_integrator(last_rp, step, step + reps + 1));
+    long long pre = step;  // profiled steps continue the trajectory
+    CK(cudaMemcpyAsync(dstep.p, &pre, sizeof pre, cudaMemcpyHostToDevice, s0));
+    const FFParams &p = in.ff.p;
+    auto a = args(groups_all);
+    int nn = n(), tb = 128, nb = (nn + tb - 1) / tb, wb = (nn * 32 + tb - 1) / tb;
+    std::vector<cudaEvent_t> ev(2 * AWSEM_NKERNELS);
+    for (auto &e : ev) CK(cudaEventCreate(&e));
+    std::vector<double> acc(AWSEM_NKERNELS, 0.0);
+    bool fm = p.fm_nd > 0;
+    for (int r = 0; r < reps; r++) {
+      for (int k = 0; k < AWSEM_NKERNELS; k++) {
+        CK(cudaEventRecord(ev[2 * k], s0));
+        switch (k) {
+          case 0: dev::k_prepare<R><<<nb, tb, 0, s0>>>(a, p); break;
+          case 1: dev::k_nl_decide<<<1, 1, 0, s0>>>(nl.p, 0, dstep.p); break;
+          case 2: dev::k_nl_build<R><<<wb, tb, 0, s0>>>(a, 0, nn); break;
+          case 3: dev::k_density<R><<<wb, tb, 0, s0>>>(a, p); break;
+          case 4: dev::k_residue<R><<<nb, tb, 0, s0>>>(a, p); break;
+          case 5: dev::k_water_xi<R><<<wb, tb, 0, s0>>>(a, p); break;
+          case 6: dev::k_pair<R><<<wb, tb, 0, s0>>>(a, p); break;
+          case 7: if (fm) dev::k_fragmem<R><<<wb, tb, 0, s0>>>(a, p); break;
+          case 8: dev::k_bonds<R><<<nb, tb, 0, s0>>>(a); break;
+          case 9: dev::k_finish<R><<<nb, tb, 0, s0>>>(a, d_integ.p, g1.p, g2.p, ftot.p, x.p); break;
+        }
+        CK(cudaEventRecord(ev[2 * k + 1], s0));
+      }
+      CK(cudaStreamSynchronize(s0));
+      for (int k = 0; k < AWSEM_NKERNELS; k++) {
+        float t = 0.f;
+        CK(cudaEventElapsedTime(&t, ev[2 * k], ev[2 * k + 1]));
+        acc[k] += t;
+      }
+    }
+    for (auto &e : ev) cudaEventDestroy(e);
+    for (int k = 0; k < AWSEM_NKERNELS; k++) ms[k] = acc[k] / reps;
+    step += reps;
+    check_list();
+  }
+
+  double run_ms() const override { return last_run_ms; }
+
+  void model_info(long long *info) override
+  {
+    info[0] = n();
+    info[1] = natoms();
+    info[2] = in.fm.records();
+    info[3] = sizeof(R);
+    info[4] = in.ff.p.fm_nd;
+    info[5] = cap;
+    std::vector<int> c(n());
+    CK(cudaMemcpyAsync(c.data(), ncount.p, sizeof(int) * n(), cudaMemcpyDeviceToHost, s0));
+    CK(cudaStreamSynchronize(s0));
+    long long tot = 0;
+    for (int v2 : c) tot += v2;
+    info[6] = tot;
+    info[7] = in.fm.uniform ? 0 : 1;
+  }
+
+  awsem_run_params thermostat_rp{0, 0, 0, 0, 0, 0, 0, 0};
+
+  void set_thermostat(const awsem_run_params &rp)
+  {
+    if (rp.dt == thermostat_rp.dt && rp.damp == thermostat_rp.damp) return;
+    const Topology &t = in.top;
+    int na = natoms();
+    std::vector<double> h1(na), h2(na);
+    for (int a = 0; a < na; a++) {
+      double m = t.mass[a];
+      h1[a] = -m / rp.damp / FTM2V;
+      h2[a] = sqrt(m) * sqrt(24.0 * BOLTZ / rp.damp / rp.dt / MVV2E) / FTM2V;
+    }
+    CK(cudaMemcpyAsync(g1.p, h1.data(), sizeof(double) * na, cudaMemcpyHostToDevice, s0));
+    CK(cudaMemcpyAsync(g2.p, h2.data(), sizeof(double) * na, cudaMemcpyHostToDevice, s0));
+    CK(cudaStreamSynchronize(s0));
+    thermostat_rp = rp;
+  }
+
+  dev::Integrator make_integrator(const awsem_run_params &rp, long long begin, long long end)
+  {
+    dev::Integrator integ{};
+    integ.dt = rp.dt;
+    integ.dtf = 0.5 * rp.dt * FTM2V;
+    integ.langevin = rp.langevin;
+    integ.t_start = rp.t_start;
+    integ.t_stop = rp.t_stop;
+    integ.begin = begin;
+    integ.end = end;
+    integ.damp = rp.damp;
+    integ.seed = rp.seed;
+    return integ;
+  }
+
+  void run(long long nsteps, const awsem_run_params &rp, double *thermo) override
+  {
+    if (nsteps < 0) throw std::invalid_argument("nsteps must be >= 0");
+    last_rp = rp;
+    // thermostat factors per atom (fix langevin, units real)
+    set_thermostat(rp);
+    if (rp.skin > 0 && rp.skin != skin) {
+      skin = rp.skin;
+      set_nl_field(&dev::NLState::skin, (float) skin);
+    }
+    if (rp.neigh_every != neigh_every) {
+      neigh_every = rp.neigh_every;
+      set_nl_field(&dev::NLState::every, neigh_every);
+    }
+    upload_integrator(make_integrator(rp, step, step + nsteps));
+    long long pre = step - 1;  // the setup evaluation advances the counter to `step`
+    CK(cudaMemcpyAsync(dstep.p, &pre, sizeof pre, cudaMemcpyHostToDevice, s0));
+    bool want_thermo = thermo != nullptr;
+    int tv = want_thermo ? 1 : 0;
+    if (want_thermo) {
+      // thermo graphs bake the row buffer's address: rebuilt per run
+      thermo_rows.alloc((size_t) 4 * (nsteps + 1));
+      for (auto &g : graphs[1])
+        if (g) {
+          cudaGraphExecDestroy(g);
+          g = nullptr;
+        }
+    }
+    long long total = nsteps + 1;
+    if (!graphs[tv][0]) capture_steps(graphs[tv][0], 1, want_thermo);
+    if (total >= kChunk && !graphs[tv][1]) capture_steps(graphs[tv][1], kChunk, want_thermo);
+    if (!ev_run0) {
+      CK(cudaEventCreate(&ev_run0));
+      CK(cudaEventCreate(&ev_run1));
+    }
+    long long done = 0;
+    CK(cudaEventRecord(ev_run0, s0));
+    while (total - done >= kChunk) {
+      CK(cudaGraphLaunch(graphs[tv][1], s0));
+      done += kChunk;
+    }
+    while (done < total) {
+      CK(cudaGraphLaunch(graphs[tv][0], s0));
+      done++;
+    }
+    CK(cudaEventRecord(ev_run1, s0));
+    CK(cudaStreamSynchronize(s0));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, ev_run0, ev_run1));
+    last_run_ms = ms;
+    step += nsteps;
+    check_list();
+    if (want_thermo)
+      CK(cudaMemcpy(thermo, thermo_rows.p, sizeof(double) * 4 * (nsteps + 1), cudaMemcpyDeviceToHost));
+  }
+
+  template <typename F> void set_nl_field(F dev::NLState::*field, F value)
+  {
+    dev::NLState st;
+    CK(cudaMemcpyAsync(&st, nl.p, sizeof st, cudaMemcpyDeviceToHost, s0));
+    CK(cudaStreamSynchronize(s0));
+    st.*field = value;
+    CK(cudaMemcpyAsync(nl.p, &st, sizeof st, cudaMemcpyHostToDevice, s0));
+  }
+
+  void energies(double *out) override
+  {
+    reduce_energies();
+    double e[E_SLOTS];
+    CK(cudaMemcpyAsync(e, energy.p, sizeof e, cudaMemcpyDeviceToHost, s0));
+    CK(cudaStreamSynchronize(s0));
+    finish_energies(e, out, true);
+  }
+
+  void forces(double *f_ext) override
+  {
+    const Topology &t = in.top;
+    int na = natoms();
+    std::vector<double> f((size_t) 3 * na);
+    CK(cudaMemcpyAsync(f.data(), ftot.p, sizeof(double) * 3 * na, cudaMemcpyDeviceToHost, s0));
+    CK(cudaStreamSynchronize(s0));
+    for (int at = 0; at < na; at++)
+      for (int k = 0; k < 3; k++) f_ext[3 * t.ext_of[at] + k] = f[3 * at + k];
+  }
+
+  void residue_arrays(double *out) override
+  {
+    int nn = n();
+    std::vector<double> w((size_t) 10 * nn);
+    CK(cudaMemcpyAsync(w.data(), work.p, sizeof(double) * 10 * nn, cudaMemcpyDeviceToHost, s0));
+    CK(cudaStreamSynchronize(s0));
+    // device order: rho_w rho_h sig_w sigp_w sig_h sigp_h xi_w xi1 xi2 bur
+    const int src[8] = {0, 1, 6, 7, 8, 9, 2, 4};
+    for (int r = 0; r < nn; r++)
+      for (int c = 0; c < 8; c++) out[8 * r + c] = w[(size_t) src[c] * nn + r];
+  }
+
+  void nl_stats(int *nbuilds, double *radius, int *maxc, int *overflow) override
+  {
+    dev::NLState st;
+    CK(cudaMemcpyAsync(&st, nl.p, sizeof st, cudaMemcpyDeviceToHost, s0));
+    CK(cudaStreamSynchronize(s0));
+    if (nbuilds) *nbuilds = st.nbuilds;
+    if (radius) *radius = st.r_list;
+    if (overflow) *overflow = st.overflow;
+    if (maxc) *maxc = max_count();
+  }
+};
+
+}  // namespace awsem
+
+using namespace awsem;
+
+struct awsem_system {
+  std::unique_ptr<EngineBase> eng;
+};
+
+template <typename Fn> static int guarded(Fn fn)
+{
+  try {
+    fn();
+    return AWSEM_OK;
+  } catch (CudaError &e) {
+    g_last_error = e.what();
+    return AWSEM_ECUDA;
+  } catch (std::invalid_argument &e) {
+    g_last_error = e.what();
+    return AWSEM_EINVAL;
+  } catch (std::bad_alloc &) {
+    g_last_error = "host allocation failed";
+    return AWSEM_ENOMEM;
+  } catch (std::runtime_error &e) {
+    g_last_error = e.what();
+    std::string m = e.what();
+    return m.find("overflow") != std::string::npos ? AWSEM_ESTATE : AWSEM_EPARSE;
+  } catch (std::exception &e) {
+    g_last_error = e.what();
+    return AWSEM_EINVAL;
+  }
+}
+
+extern "C" {
+
+const char *awsem_last_error(void) { return g_last_error.c_str(); }
+
+int awsem_version(void) { return 1; }
+
+int awsem_create_from_files(const char *workdir, const char *data_file, const char *coeff_file, const char *seq_file,
+                            const char *pair_style, const char *pair_coeffs, int precision, int device,
+                            awsem_system **out)
+{
+  if (!out || !data_file || !coeff_file || !seq_file || !pair_style) {
+    g_last_error = "awsem_create_from_files: null argument";
+    return AWSEM_EINVAL;
+  }
+  if (precision != AWSEM_FP64 && precision != AWSEM_MIXED) {
+    g_last_error = "awsem_create_from_files: precision must be AWSEM_FP64 or AWSEM_MIXED";
+    return AWSEM_EINVAL;
+  }
+  *out = nullptr;
+  auto *sys = new awsem_system();
+  int rc = guarded([&] {
+    if (precision == AWSEM_FP64) sys->eng.reset(new Engine<double>());
+    else sys->eng.reset(new Engine<float>());
+    sys->eng->device = device;
+    load_system_dir(workdir ? workdir : "", data_file, coeff_file, seq_file, pair_style, pair_coeffs ? pair_coeffs : "",
+                    sys->eng->in);
+    sys->eng->setup();
+  });
+  if (rc != AWSEM_OK) {
+    delete sys;
+    return rc;
+  }
+  *out = sys;
+  return AWSEM_OK;
+}
+
+void awsem_destroy(awsem_system *sys) { delete sys; }
+
+int awsem_natoms(const awsem_system *sys) { return sys ? sys->eng->in.top.n_atoms : 0; }
+int awsem_nres(const awsem_system *sys) { return sys ? sys->eng->in.top.n_res : 0; }
+long long awsem_step(const awsem_system *sys) { return sys ? sys->eng->step : 0; }
+
+int awsem_compute(awsem_system *sys, long long step, const double *x, double *f, double *energies, int terms)
+{
+  if (!sys || !x || !f) {
+    g_last_error = "awsem_compute: null argument";
+    return AWSEM_EINVAL;
+  }
+  if (terms <= 0 || terms > AWSEM_TERMS_ALL) {
+    g_last_error = "awsem_compute: terms must be a non-empty set of AWSEM_TERMS_* bits";
+    return AWSEM_EINVAL;
+  }
+  return guarded([&] { sys->eng->compute(step, x, f, energies, terms); });
+}
+
+int awsem_set_state(awsem_system *sys, const double *x, const double *v)
+{
+  if (!sys) return AWSEM_EINVAL;
+  return guarded([&] { sys->eng->set_state(x, v); });
+}
+
+int awsem_get_state(awsem_system *sys, double *x, double *v)
+{
+  if (!sys) return AWSEM_EINVAL;
+  return guarded([&] { sys->eng->get_state(x, v); });
+}
+
+int awsem_run(awsem_system *sys, long long nsteps, const awsem_run_params *rp, double *thermo)
+{
+  if (!sys || !rp) {
+    g_last_error = "awsem_run: null argument";
+    return AWSEM_EINVAL;
+  }
+  if (rp->dt <= 0 || rp->damp <= 0 || (rp->langevin && (rp->t_start < 0 || rp->t_stop < 0))) {
+    g_last_error = "awsem_run: dt and damp must be positive, temperatures non-negative";
+    return AWSEM_EINVAL;
+  }
+  return guarded([&] { sys->eng->run(nsteps, *rp, thermo); });
+}
+
+int awsem_energies(awsem_system *sys, double *energies)
+{
+  if (!sys || !energies) return AWSEM_EINVAL;
+  return guarded([&] { sys->eng->energies(energies); });
+}
+
+int awsem_forces(awsem_system *sys, double *f)
+{
+  if (!sys || !f) return AWSEM_EINVAL;
+  return guarded([&] { sys->eng->forces(f); });
+}
+
+int awsem_residue_arrays(awsem_system *sys, double *out)
+{
+  if (!sys || !out) return AWSEM_EINVAL;
+  return guarded([&] { sys->eng->residue_arrays(out); });
+}
+
+int awsem_neighbor_stats(awsem_system *sys, int *nbuilds, double *radius, int *max_count, int *overflow)
+{
+  if (!sys) return AWSEM_EINVAL;
+  return guarded([&] { sys->eng->nl_stats(nbuilds, radius, max_count, overflow); });
+}
+
+double awsem_last_run_ms(const awsem_system *sys) { return sys ? sys->eng->run_ms() : 0.0; }
+
+const char *awsem_kernel_name(int k) { return (k >= 0 && k < AWSEM_NKERNELS) ? kKernelNames[k] : ""; }
+
+int awsem_profile_step(awsem_system *sys, int reps, double *ms)
+{
+  if (!sys || !ms) return AWSEM_EINVAL;
+  return guarded([&] { sys->eng->profile(reps, ms); });
+}
+
+int awsem_model_info(awsem_system *sys, long long *info)
+{
+  if (!sys || !info) return AWSEM_EINVAL;
+  return guarded([&] { sys->eng->model_info(info); });
+}
+
+}  // extern "C"

@@ -1,0 +1,740 @@
+// Per-step kernels of the AWSEM engine (sm_100a).
+//
+// One MD step is this chain of launches (captured into a CUDA graph):
+//   prepare      thread/residue: CA, CB, O -> working copy + virtual N, H, C'
+//                (fix_backbone.cpp:7067-7138); zero forces; list-check data
+//   nl_decide    1 thread: rebuild decision for the residue pair list
+//   nl_build     warp/residue: contact-bead pairs within the list radius
+//   density      warp/residue: rho_water, rho_helix (DL1, :7728-7791)
+//   residue      thread/residue: switching functions, burial (SL, :7795-7841),
+//                helical (i,i+4) pairs (:7843-7868), chain/chi/rama
+//   water_xi     warp/residue: xi_water (DL2, :7877-7954)
+//   pair         warp/residue: water/burial/helix radial forces, excluded
+//                volume, DSSP hydrogen bonds, P_AP (DL3, :7956-8134)
+//   fragmem      warp/residue: fragment-memory Gaussians (:4079-4177)
+//   bonds        thread/residue: harmonic bonds
+//   finish       thread/residue: fixed-point -> FP64 forces, Langevin,
+//                velocity-Verlet half kicks and drift
+// Residue-owned quantities are written by their owner without atomics;
+// forces scattered to other residues' beads use 64-bit integer atomics.
+#pragma once
+
+#include "awsem_device.cuh"
+
+namespace awsem {
+namespace dev {
+
+struct NLState {
+  float d2max;        // max contact-bead displacement^2 since the last build
+  float bO, bN, bCA, bAll;  // max bead offsets from the contact bead
+  float r_list;       // list radius of the current list
+  int rebuild;        // decision for this step
+  int steps_since;    // steps since the last build
+  int every;          // forced rebuild period (0: displacement check only)
+  int nbuilds;
+  int overflow;       // max neighbour count seen when it exceeded capacity
+  float skin;
+  float r_contact, r_dssp, r_pap, r_ev;  // term cutoffs on the bead pairs they test
+};
+
+template <typename R> struct StepArgs {
+  DevSys<R> s;
+  int n_atoms;
+  const double *x;  // [n_atoms][3]
+  double *v;
+  const double *mass;
+  const int *atom_tag;
+  // per-residue pair-pass intermediates
+  double *rho_w, *rho_h, *sig_w, *sigp_w, *sig_h, *sigp_h, *xi_w, *xi1, *xi2, *bur;
+  double *e_res;  // [E_SLOTS][n_res]
+  // residue pair list
+  int *nbr, *ncount, cap;
+  double4 *cb_build;
+  NLState *nl;
+  // excluded volume
+  int ntypes, ev_p;
+  const double *ev_pref, *ev_cs, *ev_cl;
+  const int *atom_type;
+  const unsigned *excl_self, *excl_next;
+  // bonds grouped by the residue of their first atom
+  const int *bond_start, *bond_i, *bond_j;
+  const double *bond_k, *bond_r0;
+  // fragment memory
+  const int *fm_row;
+  const R *fm_rf;
+  const R *fm_coef;  // nullptr when uniform
+  double fm_uniform;
+  int groups;        // AWSEM_TERMS_* bits: 1 fix backbone, 2 pair vexcluded, 4 bonds
+  long long *step;   // device step counter (advanced by k_nl_decide)
+};
+
+enum Group { G_FIX = 1, G_PAIR = 2, G_BOND = 4 };
+
+__device__ __forceinline__ void atomic_max_f(float *addr, float v)
+{
+  // non-negative floats order like their bit patterns
+  atomicMax((int *) addr, __float_as_int(v));
+}
+
+template <typename R> __global__ void k_prepare(StepArgs<R> a, FFParams p)
+{
+  int r = blockIdx.x * blockDim.x + threadIdx.x;
+  float d2 = 0.f, oO = 0.f, oN = 0.f, oCA = 0.f, oAll = 0.f;
+  if (r < a.s.n_res) {
+    const double *x = a.x;
+    int fl = a.s.res_flags[r];
+    double ca[3], cb[3], o[3], n[3] = {0, 0, 0}, h[3] = {0, 0, 0}, cp[3] = {0, 0, 0};
+    for (int k = 0; k < 3; k++) {
+      ca[k] = x[(3 * r + 0) * 3 + k];
+      cb[k] = x[(3 * r + 1) * 3 + k];
+      o[k] = x[(3 * r + 2) * 3 + k];
+    }
+    if (!(fl & R_FIRST)) {
+      for (int k = 0; k < 3; k++) {
+        double ca0 = x[(3 * (r - 1) + 0) * 3 + k], o0 = x[(3 * (r - 1) + 2) * 3 + k];
+        n[k] = __dadd_rn(__dadd_rn(__dmul_rn(p.an, ca0), __dmul_rn(p.bn, ca[k])), __dmul_rn(p.cn, o0));
+        h[k] = __dadd_rn(__dadd_rn(__dmul_rn(p.ah, ca0), __dmul_rn(p.bh, ca[k])), __dmul_rn(p.ch, o0));
+      }
+    }
+    if (!(fl & R_LAST)) {
+      for (int k = 0; k < 3; k++) {
+        double ca1 = x[(3 * (r + 1) + 0) * 3 + k];
+        cp[k] = __dadd_rn(__dadd_rn(__dmul_rn(p.ap, ca[k]), __dmul_rn(p.bp, ca1)), __dmul_rn(p.cp, o[k]));
+      }
+    }
+    double4 *w = const_cast<double4 *>(a.s.pos) + (size_t) r * N_BEADS;
+    w[B_CA] = make_double4(ca[0], ca[1], ca[2], 0.0);
+    w[B_CB] = make_double4(cb[0], cb[1], cb[2], 0.0);
+    w[B_O] = make_double4(o[0], o[1], o[2], 0.0);
+    w[B_N] = make_double4(n[0], n[1], n[2], 0.0);
+    w[B_H] = make_double4(h[0], h[1], h[2], 0.0);
+    w[B_CP] = make_double4(cp[0], cp[1], cp[2], 0.0);
+    unsigned long long *f = a.s.facc + (size_t) 9 * r;
+    for (int k = 0; k < 9; k++) f[k] = 0ull;
+    // list-validity data: contact-bead displacement and bead offsets
+    const double *c = (fl & R_GLY) ? ca : cb;
+    double4 b0 = a.cb_build[r];
+    double dx = c[0] - b0.x, dy = c[1] - b0.y, dz = c[2] - b0.z;
+    d2 = (float) (dx * dx + dy * dy + dz * dz);
+    auto off = [&](const double *q) {
+      double ex = q[0] - c[0], ey = q[1] - c[1], ez = q[2] - c[2];
+      return (float) sqrt(ex * ex + ey * ey + ez * ez);
+    };
+    oO = off(o);
+    oCA = off(ca);
+    oAll = fmaxf(fmaxf(off(ca), off(cb)), off(o));
+    if (!(fl & R_FIRST)) oN = off(n);
+  }
+  // block max, then one atomic per block
+  for (int s = 16; s > 0; s >>= 1) {
+    d2 = fmaxf(d2, __shfl_xor_sync(0xffffffffu, d2, s));
+    oO = fmaxf(oO, __shfl_xor_sync(0xffffffffu, oO, s));
+    oN = fmaxf(oN, __shfl_xor_sync(0xffffffffu, oN, s));
+    oCA = fmaxf(oCA, __shfl_xor_sync(0xffffffffu, oCA, s));
+    oAll = fmaxf(oAll, __shfl_xor_sync(0xffffffffu, oAll, s));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomic_max_f(&a.nl->d2max, d2);
+    atomic_max_f(&a.nl->bO, oO);
+    atomic_max_f(&a.nl->bN, oN);
+    atomic_max_f(&a.nl->bCA, oCA);
+    atomic_max_f(&a.nl->bAll, oAll);
+  }
+}
+
+// Pair-list rebuild decision.  A residue pair is needed when one of its
+// tested bead pairs is inside that term's cutoff; in contact-bead distance
+// that is at most R_need = max(r_contact, r_dssp + bO + bN, r_pap + 2 bCA,
+// r_ev + 2 bAll).  The list built at t0 with radius R_need(t0) + skin stays
+// complete while R_need(t) + 2 * max displacement <= radius.
+__global__ void k_nl_decide(NLState *nl, int force, long long *step)
+{
+  if (step) (*step)++;
+  NLState &s = *nl;
+  float need = fmaxf(fmaxf(s.r_contact, s.r_dssp + s.bO + s.bN), fmaxf(s.r_pap + 2.f * s.bCA, s.r_ev + 2.f * s.bAll));
+  float disp = sqrtf(s.d2max);
+  bool rb = force || s.r_list <= 0.f || need + 2.f * disp > s.r_list || (s.every > 0 && s.steps_since + 1 >= s.every);
+  if (rb) {
+    s.r_list = need + s.skin;
+    s.steps_since = 0;
+    s.nbuilds++;
+  } else {
+    s.steps_since++;
+  }
+  s.rebuild = rb;
+  s.d2max = s.bO = s.bN = s.bCA = s.bAll = 0.f;
+}
+
+template <typename R> __device__ __forceinline__ V3<double> contact(const DevSys<R> &s, int r)
+{
+  return bead(s, r, (s.res_flags[r] & R_GLY) ? B_CA : B_CB);
+}
+
+// Full residue pair list (both directions) over contact beads within r_list,
+// written in ascending j.  Brute force over the system, one warp per residue.
+template <typename R> __global__ void k_nl_build(StepArgs<R> a, int sys_begin, int sys_end)
+{
+  if (!a.nl->rebuild) return;
+  int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  int i = sys_begin + warp;
+  if (i >= sys_end) return;
+  const DevSys<R> &s = a.s;
+  V3<double> ci = contact(s, i);
+  R rl = (R) a.nl->r_list, rl2 = rl * rl;
+  int count = 0;
+  int *out = a.nbr + (size_t) i * a.cap;
+  for (int j0 = sys_begin; j0 < sys_end; j0 += 32) {
+    int j = j0 + lane;
+    bool take = false;
+    if (j < sys_end && j != i) {
+      V3<R> d = diff<R>(ci, contact(s, j));
+      take = norm2(d) < rl2;
+    }
+    unsigned m = __ballot_sync(0xffffffffu, take);
+    int at = count + __popc(m & ((1u << lane) - 1u));
+    if (take && at < a.cap) out[at] = j;
+    count += __popc(m);
+  }
+  if (lane == 0) {
+    a.ncount[i] = min(count, a.cap);
+    if (count > a.cap) atomicMax(&a.nl->overflow, count);
+    a.cb_build[i] = make_double4(ci.x, ci.y, ci.z, 0.0);
+  }
+}
+
+// DL1: local densities of contact beads (fix_backbone.cpp:7728-7791)
+template <typename R> __global__ void k_density(StepArgs<R> a, FFParams p)
+{
+  int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  const DevSys<R> &s = a.s;
+  if (i >= s.n_res) return;
+  V3<double> ci = contact(s, i);
+  int chi = s.res_chain[i];
+  long long aw = 0, ah = 0;
+  const bool fix = a.groups & G_FIX;
+  int cnt = fix ? a.ncount[i] : 0;
+  const int *nb = a.nbr + (size_t) i * a.cap;
+  bool water = p.terms & T_WATER, helix = p.terms & T_HELIX;
+  for (int k = lane; k < cnt; k += 32) {
+    int j = nb[k];
+    if (s.res_chain[j] == chi && abs(i - j) <= 1) continue;
+    V3<R> d = diff<R>(ci, contact(s, j));
+    R rsq = norm2(d);
+    if (water && rsq > R(p.w_rmin_sq[0]) && rsq < R(p.w_rmax_sq[0])) {
+      R th, pr;
+      well_theta(m_sqrt(rsq), R(p.w_rmin_th[0]), R(p.w_rmax_th[0]), R(p.water_kappa), R(p.well_rmin[0]),
+                 R(p.well_rmax[0]), th, pr);
+      aw += fix_dens((double) th);
+    }
+    if (helix && rsq > R(p.h_rmin_sq) && rsq < R(p.h_rmax_sq)) {
+      R th, pr;
+      well_theta(m_sqrt(rsq), R(p.h_rmin_th), R(p.h_rmax_th), R(p.helix_kappa), R(p.helix_rmin), R(p.helix_rmax), th, pr);
+      ah += fix_dens((double) th);
+    }
+  }
+  aw = warp_sum(aw);
+  ah = warp_sum(ah);
+  if (lane == 0) {
+    a.rho_w[i] = (double) aw * D_UNSCALE;
+    a.rho_h[i] = (double) ah * D_UNSCALE;
+  }
+}
+
+__device__ __forceinline__ void switching(double rho, double kappa_sigma, double thr, double &sig, double &sigp)
+{
+  double th = tanh(kappa_sigma * (rho - thr));
+  sig = 0.5 * (1.0 - th);
+  sigp = -kappa_sigma * sig * (1.0 + th);
+}
+
+// Excluded volume between beads (PairExcludedVolume::compute,
+// pair_excluded_volume.cpp:50-138).  Returns the pair energy and the force
+// on bead a (the force on b is its negative).
+template <typename R>
+__device__ __forceinline__ R ev_pair(const StepArgs<R> &a, int ta, int tb, bool short_range, V3<R> d, V3<R> &f)
+{
+  int N = a.ntypes + 1;
+  double pref = a.ev_pref[ta * N + tb];
+  f = {R(0), R(0), R(0)};
+  if (pref == 0.0) return R(0);
+  R rc = (R) (short_range ? a.ev_cs[ta * N + tb] : a.ev_cl[ta * N + tb]);
+  R r = m_sqrt(norm2(d));
+  if (!(r < rc)) return R(0);
+  R dr = r - rc;
+  R pw = R(1);
+  for (int k = 1; k < a.ev_p; k++) pw *= dr;  // dr^(p-1)
+  R pr = R(pref) * pw;
+  R fp = r > R(0) ? -pr * R(a.ev_p) / r : R(0);
+  f = {d.x * fp, d.y * fp, d.z * fp};
+  return pr * dr;
+}
+
+// SL and the per-residue backbone terms
+template <typename R> __global__ void k_residue(StepArgs<R> a, FFParams p)
+{
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const DevSys<R> &s = a.s;
+  if (i >= s.n_res) return;
+  int n = s.n_res, fl = s.res_flags[i];
+  double *E = a.e_res;
+  const bool fix = a.groups & G_FIX;
+  bool water = fix && (p.terms & T_WATER), helix = fix && (p.terms & T_HELIX);
+  double sw = 0, swp = 0, sh = 0, shp = 0;
+  if (water) switching(a.rho_w[i], p.water_kappa_sigma, p.treshold, sw, swp);
+  if (helix) switching(a.rho_h[i], p.helix_kappa_sigma, p.helix_treshold, sh, shp);
+  a.sig_w[i] = sw;
+  a.sigp_w[i] = swp;
+  a.sig_h[i] = sh;
+  a.sigp_h[i] = shp;
+  double eb = 0.0, bc = 0.0;
+  if (fix && (p.terms & T_BURIAL)) {
+    double rho = a.rho_w[i];
+    const double *g = s.tables + TB_BURIAL + 3 * s.res_type[i];
+    double t[3][2];
+    for (int k = 0; k < 3; k++) {
+      t[k][0] = tanh(p.burial_kappa * (rho - p.burial_ro_min[k]));
+      t[k][1] = tanh(p.burial_kappa * (p.burial_ro_max[k] - rho));
+      eb += -0.5 * p.k_burial * g[k] * (t[k][0] + t[k][1]);
+    }
+    bc = g[0] * (t[0][1] * t[0][1] - t[0][0] * t[0][0]);
+    bc += g[1] * (t[1][1] * t[1][1] - t[1][0] * t[1][0]);
+    bc += g[2] * (t[2][1] * t[2][1] - t[2][0] * t[2][0]);
+    bc *= 0.5 * p.k_burial * p.burial_kappa;
+  }
+  a.bur[i] = bc;
+  E[(size_t) E_BURIAL * n + i] = eb;
+  // helical (i, i+d) pair; sigma of the partner is recomputed from its density
+  double x1 = 0.0, x2 = 0.0, eh = 0.0;
+  int j = i + p.helix_i_diff;
+  if (helix && j < n && s.res_chain[j] == s.res_chain[i]) {
+    V3<R> d = diff<R>(bead(s, i, B_O), bead(s, j, B_N));
+    if (norm2(d) < R(p.helix_cutoff_sq)) {
+      double shj, shpj;
+      switching(a.rho_h[j], p.helix_kappa_sigma, p.helix_treshold, shj, shpj);
+      eh = (double) helix_pair(s, p, i, j, sh, shp, shj, shpj, x1, x2);
+    }
+  }
+  a.xi1[i] = x1;
+  a.xi2[i] = x2;
+  E[(size_t) E_HELIX * n + i] = eh;
+  double ec = 0.0, ex = 0.0, er = 0.0;
+  if (fix && (p.terms & T_CHAIN)) ec = (double) chain_term(s, p, i);
+  bool inner = fix && !(fl & (R_FIRST | R_LAST | R_GLY));
+  if (inner && (p.terms & T_CHI)) ex = (double) chi_term(s, p, i);
+  if (inner && (p.terms & T_RAMA)) er = (double) rama_term(s, p, i);
+  E[(size_t) E_CHAIN * n + i] = ec;
+  E[(size_t) E_CHI * n + i] = ex;
+  E[(size_t) E_RAMA * n + i] = er;
+  // excluded volume inside the residue (1-3 pairs; 1-2 pairs are excluded)
+  double ev = 0.0;
+  unsigned ex_self = (a.groups & G_PAIR) ? a.excl_self[i] : 0x1ffu;
+  for (int b0 = 0; b0 < 3; b0++)
+    for (int b1 = b0 + 1; b1 < 3; b1++) {
+      if (ex_self & (1u << (b0 * 3 + b1))) continue;
+      V3<R> f;
+      R e = ev_pair(a, a.atom_type[3 * i + b0], a.atom_type[3 * i + b1], true,
+                    diff<R>(bead(s, i, b0), bead(s, i, b1)), f);
+      if (e != R(0) || f.x != R(0) || f.y != R(0) || f.z != R(0)) {
+        ev += (double) e;
+        scatter(s, i, b0, f);
+        scatter(s, i, b1, -f.x, -f.y, -f.z);
+      }
+    }
+  E[(size_t) E_PAIR * n + i] = ev;
+}
+
+// DL2: water-mediated density derivative coefficients (fix_backbone.cpp:7877-7954)
+template <typename R> __global__ void k_water_xi(StepArgs<R> a, FFParams p)
+{
+  int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  const DevSys<R> &s = a.s;
+  if (i >= s.n_res) return;
+  if (!(p.terms & T_WATER) || !(a.groups & G_FIX)) {
+    if (lane == 0) a.xi_w[i] = 0.0;
+    return;
+  }
+  V3<double> ci = contact(s, i);
+  int chi = s.res_chain[i], ti = s.res_type[i];
+  long long acc = 0;
+  int cnt = a.ncount[i];
+  const int *nb = a.nbr + (size_t) i * a.cap;
+  const double *WG = s.tables + TB_WATER;
+  for (int k = lane; k < cnt; k += 32) {
+    int j = nb[k];
+    if (s.res_chain[j] == chi && abs(i - j) < p.contact_cutoff) continue;
+    V3<R> d = diff<R>(ci, contact(s, j));
+    R rsq = norm2(d);
+    int tj = s.res_type[j];
+    for (int w = 0; w < p.n_wells; w++) {
+      if (!p.well_flag[w]) continue;
+      double g0 = WG[w * 800 + (ti * 20 + tj) * 2], g1 = WG[w * 800 + (ti * 20 + tj) * 2 + 1];
+      // the reference's `!fabs(g0 - g1) < delta` holds exactly when g0 != g1
+      if (g0 != g1 && rsq > R(p.w_rmin_sq[w]) && rsq < R(p.w_rmax_sq[w])) {
+        R th, pr;
+        well_theta(m_sqrt(rsq), R(p.w_rmin_th[w]), R(p.w_rmax_th[w]), R(p.water_kappa), R(p.well_rmin[w]),
+                   R(p.well_rmax[w]), th, pr);
+        acc += fix_dens((g1 - g0) * (double) th * a.sig_w[j]);
+      }
+    }
+  }
+  acc = warp_sum(acc);
+  if (lane == 0) a.xi_w[i] = (double) acc * D_UNSCALE * a.sigp_w[i];
+}
+
+// DL3: main pair loop (fix_backbone.cpp:7956-8134) plus excluded volume
+// between residues.  Radial contact forces and excluded volume act on the
+// owner's beads only (each pair is visited from both sides); DSSP and P_AP
+// are visited once and scatter.
+template <typename R> __global__ void k_pair(StepArgs<R> a, FFParams p)
+{
+  int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  const DevSys<R> &s = a.s;
+  if (i >= s.n_res) return;
+  int n = s.n_res, fli = s.res_flags[i], chi = s.res_chain[i], ti = s.res_type[i];
+  int cbi = (fli & R_GLY) ? B_CA : B_CB;
+  V3<double> bi[3] = {bead(s, i, B_CA), bead(s, i, B_CB), bead(s, i, B_O)};
+  V3<double> ci = bi[cbi];
+  V3<double> oi = bi[2];
+  int tat[3] = {a.atom_type[3 * i], a.atom_type[3 * i + 1], a.atom_type[3 * i + 2]};
+  double xi_i = a.xi_w[i], bur_i = a.bur[i], x1_i = a.xi1[i];
+  int dh = p.helix_i_diff;
+  double x2_i = i - dh >= 0 ? a.xi2[i - dh] : 0.0;
+  double sw_i = a.sig_w[i];
+  long long F[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+  double e_water = 0.0, e_ev = 0.0, e_dssp = 0.0, e_pap = 0.0;
+  const double *WG = s.tables + TB_WATER;
+  const bool fix = a.groups & G_FIX, evon = a.groups & G_PAIR;
+  uint32_t T = fix ? p.terms : 0u;
+  int cnt = a.ncount[i];
+  const int *nb = a.nbr + (size_t) i * a.cap;
+  for (int k = lane; k < cnt; k += 32) {
+    int j = nb[k];
+    int flj = s.res_flags[j];
+    bool other = s.res_chain[j] != chi;
+    int dij = abs(i - j);
+    bool upper = j > i;
+    // contact-bead radial terms
+    if (fix && (other || dij > 1)) {
+      V3<R> d = diff<R>(ci, contact(s, j));
+      R rsq = norm2(d);
+      R r = m_sqrt(rsq);
+      R force = 0;
+      bool in0 = rsq > R(p.w_rmin_sq[0]) && rsq < R(p.w_rmax_sq[0]);
+      R th0 = 0, pr0 = 0;
+      if ((T & (T_WATER | T_BURIAL)) && in0)
+        well_theta(r, R(p.w_rmin_th[0]), R(p.w_rmax_th[0]), R(p.water_kappa), R(p.well_rmin[0]), R(p.well_rmax[0]),
+                   th0, pr0);
+      if (T & T_WATER) {
+        int tj = s.res_type[j];
+        bool sep = other || dij >= p.contact_cutoff;
+        for (int w = 0; w < p.n_wells; w++) {
+          if (!p.well_flag[w]) continue;
+          if (sep && rsq > R(p.w_rmin_sq[w]) && rsq < R(p.w_rmax_sq[w])) {
+            double g0 = WG[w * 800 + (ti * 20 + tj) * 2], g1 = WG[w * 800 + (ti * 20 + tj) * 2 + 1];
+            double sg = fabs(g0 - g1) < 1e-5 ? 0.5 * (g0 + g1) : g0 + (g1 - g0) * sw_i * a.sig_w[j];
+            R th, pr;
+            if (w == 0) {
+              th = th0;
+              pr = pr0;
+            } else {
+              well_theta(r, R(p.w_rmin_th[w]), R(p.w_rmax_th[w]), R(p.water_kappa), R(p.well_rmin[w]),
+                         R(p.well_rmax[w]), th, pr);
+            }
+            if (upper) e_water += -sg * (double) th;
+            force += R(sg) * pr;
+          }
+        }
+        if (in0) {
+          double xj = a.xi_w[j];
+          if (fabs(xi_i) > 1e-8) force += pr0 * R(xi_i);
+          if (fabs(xj) > 1e-8) force += pr0 * R(xj);
+        }
+      }
+      if ((T & T_BURIAL) && in0) force += R(bur_i + a.bur[j]) * pr0;
+      if ((T & T_HELIX) && rsq > R(p.h_rmin_sq) && rsq < R(p.h_rmax_sq)) {
+        double fac = x1_i + a.xi1[j] + x2_i;
+        if (j - dh >= 0) fac += a.xi2[j - dh];
+        if (fabs(fac) > 1e-6) {
+          R th, pr;
+          well_theta(r, R(p.h_rmin_th), R(p.h_rmax_th), R(p.helix_kappa), R(p.helix_rmin), R(p.helix_rmax), th, pr);
+          force += -R(fac) * pr;
+        }
+      }
+      if (force != R(0)) {
+        F[cbi][0] += fix_force((double) (force * d.x));
+        F[cbi][1] += fix_force((double) (force * d.y));
+        F[cbi][2] += fix_force((double) (force * d.z));
+      }
+    }
+    // excluded volume between beads of i and j (1-2 bonded pairs removed)
+    if (evon) {
+      unsigned excl = 0;
+      if (j == i + 1) excl = a.excl_next[i];
+      bool prev = j == i - 1;
+      unsigned exclp = prev ? a.excl_next[j] : 0u;
+      bool shortr = !other && dij < 5;
+      for (int b1 = 0; b1 < 3; b1++) {
+        V3<double> bj = bead(s, j, b1);
+        int tb = a.atom_type[3 * j + b1];
+        for (int b0 = 0; b0 < 3; b0++) {
+          if (excl & (1u << (b0 * 3 + b1))) continue;
+          if (exclp & (1u << (b1 * 3 + b0))) continue;
+          V3<R> f;
+          R e = ev_pair(a, tat[b0], tb, shortr, diff<R>(bi[b0], bj), f);
+          if (e == R(0) && f.x == R(0) && f.y == R(0) && f.z == R(0)) continue;
+          if (upper) e_ev += (double) e;
+          F[b0][0] += fix_force((double) f.x);
+          F[b0][1] += fix_force((double) f.y);
+          F[b0][2] += fix_force((double) f.z);
+        }
+      }
+    }
+    // DSSP with O(i) as acceptor and N-H(j) as donor (fix_backbone.cpp:8064-8079)
+    if ((T & T_DSSP) && (other || dij > 2) && !(flj & R_PRO) && !(fli & R_LAST) && !(flj & R_FIRST)) {
+      V3<R> d = diff<R>(oi, bead(s, j, B_N));
+      if (norm2(d) < R(p.dssp_cut_sq)) e_dssp += (double) dssp_term(s, p, i, j);
+    }
+    // P_AP on CA pairs, visited from the lower residue (fix_backbone.cpp:8096-8103)
+    if ((T & T_PAP) && upper) {
+      V3<R> d = diff<R>(bi[0], bead(s, j, B_CA));
+      if (norm2(d) < R(p.pap_cutoff_sq)) e_pap += (double) pap_term(s, p, i, j);
+    }
+  }
+  for (int b = 0; b < 3; b++)
+    for (int c = 0; c < 3; c++) F[b][c] = warp_sum(F[b][c]);
+  e_water = warp_sum(e_water);
+  e_ev = warp_sum(e_ev);
+  e_dssp = warp_sum(e_dssp);
+  e_pap = warp_sum(e_pap);
+  if (lane == 0) {
+    unsigned long long *f = s.facc + (size_t) 9 * i;
+    for (int b = 0; b < 3; b++)
+      for (int c = 0; c < 3; c++)
+        if (F[b][c]) atomicAdd(f + 3 * b + c, (unsigned long long) F[b][c]);
+    double *E = a.e_res;
+    E[(size_t) E_WATER * n + i] = e_water;
+    E[(size_t) E_PAIR * n + i] += e_ev;
+    E[(size_t) E_DSSP * n + i] = e_dssp;
+    E[(size_t) E_PAP * n + i] = e_pap;
+  }
+}
+
+// Fragment memory (fix_backbone.cpp:4079-4177) in pair-major form: for target
+// residue i and separation d, lane l handles atom pair k = l & 3 of every
+// eighth memory record of the row; lanes with equal k are then combined.
+template <typename R> __global__ void k_fragmem(StepArgs<R> a, FFParams p)
+{
+  int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  const DevSys<R> &s = a.s;
+  if (i >= s.n_res) return;
+  int n = s.n_res, nd = p.fm_nd;
+  int k = lane & 3;
+  const int ib = (k < 2) ? B_CA : B_CB, jb = (k & 1) ? B_CB : B_CA;
+  V3<double> pi = bead(s, i, ib);
+  long long Fi[3] = {0, 0, 0};
+  double e_tot = 0.0;
+  for (int dd = 0; dd < nd; dd++) {
+    int row = i * nd + dd;
+    int r0 = a.fm_row[row], r1 = a.fm_row[row + 1];
+    if (r1 == r0) continue;
+    int j = i + p.fm_min_sep + dd;
+    V3<R> d = diff<R>(pi, bead(s, j, jb));
+    R r = m_sqrt(norm2(d));
+    R s2 = R(p.fm_sigma_sq[p.fm_min_sep + dd]);
+    R inv2s = R(1) / (R(2) * s2);
+    R esum = 0, fsum = 0;
+    const R *rf = a.fm_rf + (size_t) r0 * 4;
+    int nrec4 = (r1 - r0) * 4;
+    if (a.fm_coef) {
+      for (int e = lane; e < nrec4; e += 32) {
+        R dr = r - rf[e];
+        R g = a.fm_coef[r0 + (e >> 2)] * m_fastexp(-dr * dr * inv2s);
+        esum -= g;
+        fsum -= g * dr;
+      }
+    } else {
+      R c = R(a.fm_uniform);
+      for (int e = lane; e < nrec4; e += 32) {
+        R dr = r - rf[e];
+        R g = c * m_fastexp(-dr * dr * inv2s);
+        esum -= g;
+        fsum -= g * dr;
+      }
+    }
+    // combine lanes with the same atom pair (lane & 3)
+    for (int o = 4; o < 32; o <<= 1) {
+      esum += __shfl_xor_sync(0xffffffffu, esum, o);
+      fsum += __shfl_xor_sync(0xffffffffu, fsum, o);
+    }
+    // row energy: the four atom-pair sums
+    double erow = (double) esum;
+    erow += __shfl_xor_sync(0xffffffffu, erow, 1);
+    erow += __shfl_xor_sync(0xffffffffu, erow, 2);
+    e_tot += erow;
+    if (lane < 4) {
+      R fc = fsum / (s2 * r);
+      if (fsum != R(0)) {
+        long long fx = fix_force((double) (fc * d.x)), fy = fix_force((double) (fc * d.y)),
+                  fz = fix_force((double) (fc * d.z));
+        Fi[0] += fx;
+        Fi[1] += fy;
+        Fi[2] += fz;
+        unsigned long long *fj = s.facc + ((size_t) 3 * j + jb) * 3;
+        atomicAdd(fj + 0, (unsigned long long) (-fx));
+        atomicAdd(fj + 1, (unsigned long long) (-fy));
+        atomicAdd(fj + 2, (unsigned long long) (-fz));
+      }
+    }
+  }
+  // lanes 0,1 act on CA(i), lanes 2,3 on CB(i)
+  for (int c = 0; c < 3; c++) Fi[c] += __shfl_xor_sync(0xffffffffu, Fi[c], 1);
+  if (lane == 0 || lane == 2) {
+    unsigned long long *fi = s.facc + ((size_t) 3 * i + ib) * 3;
+    for (int c = 0; c < 3; c++)
+      if (Fi[c]) atomicAdd(fi + c, (unsigned long long) Fi[c]);
+  }
+  if (lane == 0) a.e_res[(size_t) E_FRAGMEM * n + i] = e_tot;
+}
+
+// bond_style harmonic, bonds grouped by the residue of their first atom
+template <typename R> __global__ void k_bonds(StepArgs<R> a)
+{
+  int r = blockIdx.x * blockDim.x + threadIdx.x;
+  const DevSys<R> &s = a.s;
+  if (r >= s.n_res) return;
+  double e = 0.0;
+  for (int b = a.bond_start[r]; b < a.bond_start[r + 1]; b++) {
+    int ai = a.bond_i[b], aj = a.bond_j[b];
+    V3<R> d = diff<R>(bead(s, ai / 3, ai % 3), bead(s, aj / 3, aj % 3));
+    R rr = m_sqrt(norm2(d));
+    R dr = rr - R(a.bond_r0[b]);
+    R rk = R(a.bond_k[b]) * dr;
+    R fb = rr > R(0) ? R(-2) * rk / rr : R(0);
+    e += (double) (rk * dr);
+    scatter(s, ai / 3, ai % 3, d.x * fb, d.y * fb, d.z * fb);
+    scatter(s, aj / 3, aj % 3, -d.x * fb, -d.y * fb, -d.z * fb);
+  }
+  a.e_res[(size_t) E_BOND * s.n_res + r] = e;
+}
+
+__device__ __forceinline__ uint64_t mix64(uint64_t z)
+{
+  z += 0x9E3779B97F4A7C15ULL;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+  return z ^ (z >> 31);
+}
+
+// Uniform in [0,1) keyed by (seed, step, atom id, component): the Langevin
+// noise stream shared with the CPU oracle.
+__device__ __forceinline__ double uniform01(uint64_t seed, long long step, long long tag, int comp)
+{
+  uint64_t key = mix64(seed ^ mix64((uint64_t) step));
+  uint64_t r = mix64(key ^ ((uint64_t) tag * 4ULL + (uint64_t) comp));
+  return (double) (r >> 11) * (1.0 / 9007199254740992.0);
+}
+
+struct Integrator {
+  double dt, dtf;           // dtf = 0.5 * dt * ftm2v
+  int langevin;
+  double t_start, t_stop;   // thermostat ramp over [begin, end]
+  long long begin, end;
+  double damp;
+  unsigned long long seed;
+};
+
+// Total force (fixed point -> FP64, plus Langevin at `step`), then
+// final_integrate of `step` (half kick) and, if `next`, initial_integrate of
+// step+1 (half kick + drift) -- LAMMPS fix nve / fix langevin order.
+template <typename R>
+__global__ void k_finish(StepArgs<R> a, const Integrator *inp, const double *g1, const double *g2, double *ftot,
+                         double *x_out)
+{
+  int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= a.s.n_res) return;
+  const Integrator in = *inp;
+  const long long step = *a.step;
+  const bool final_kick = step > in.begin, next = step < in.end;
+  double tsqrt = 0.0;
+  if (in.langevin) {
+    double delta = in.end != in.begin ? (double) (step - in.begin) / (double) (in.end - in.begin) : 0.0;
+    tsqrt = sqrt(in.t_start + delta * (in.t_stop - in.t_start));
+  }
+  double ke = 0.0;
+  for (int b = 0; b < 3; b++) {
+    int at = 3 * r + b;
+    double m = a.mass[at];
+    double dtfm = in.dtf / m;
+    const unsigned long long *fa = a.s.facc + (size_t) 3 * at;
+    for (int c = 0; c < 3; c++) {
+      double f = (double) (long long) fa[c] * F_UNSCALE;
+      double v = a.v[3 * at + c];
+      if (in.langevin) f += g1[at] * v + g2[at] * tsqrt * (uniform01(in.seed, step, a.atom_tag[at], c) - 0.5);
+      if (ftot) ftot[3 * at + c] = f;
+      if (final_kick) v += dtfm * f;
+      ke += m * v * v;
+      if (next) {
+        v += dtfm * f;
+        x_out[3 * at + c] += in.dt * v;
+      }
+      a.v[3 * at + c] = v;
+    }
+  }
+  // kinetic energy after the final half kick (thermo output of the step)
+  a.e_res[(size_t) E_KIN * a.s.n_res + r] = 0.5 * 48.88821291 * 48.88821291 * ke;
+}
+
+// Conservative total force of the last evaluation in FP64 (no Langevin)
+template <typename R> __global__ void k_total_force(StepArgs<R> a, double *ftot)
+{
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= 3 * a.n_atoms) return;
+  ftot[k] = (double) (long long) a.s.facc[k] * F_UNSCALE;
+}
+
+// Thermo row of the current step: [fix total, vexcluded, bonds, kinetic],
+// residue sums in a fixed tree order (one block of 256 threads).
+__global__ void k_thermo(const double *e_res, int n_res, const long long *step, const Integrator *inp, double *rows)
+{
+  const long long begin = inp->begin;
+  __shared__ double sh[4][256];
+  double acc[4] = {0, 0, 0, 0};
+  for (int r = threadIdx.x; r < n_res; r += blockDim.x) {
+    double fx = 0.0;
+    for (int t = 1; t < E_FIX_TERMS; t++) fx += e_res[(size_t) t * n_res + r];
+    acc[0] += fx;
+    acc[1] += e_res[(size_t) E_PAIR * n_res + r];
+    acc[2] += e_res[(size_t) E_BOND * n_res + r];
+    acc[3] += e_res[(size_t) E_KIN * n_res + r];
+  }
+  for (int c = 0; c < 4; c++) sh[c][threadIdx.x] = acc[c];
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w)
+      for (int c = 0; c < 4; c++) sh[c][threadIdx.x] += sh[c][threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    long long row = *step - begin;
+    for (int c = 0; c < 4; c++) rows[4 * row + c] = sh[c][0];
+  }
+}
+
+// Per-term sums over residues [begin, end) in a fixed tree order (one block per term)
+__global__ void k_energy_reduce(const double *e_res, int n_res, int begin, int end, double *out)
+{
+  int t = blockIdx.x;
+  __shared__ double sh[256];
+  double acc = 0.0;
+  for (int r = begin + threadIdx.x; r < end; r += blockDim.x) acc += e_res[(size_t) t * n_res + r];
+  sh[threadIdx.x] = acc;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[t] = sh[0];
+}
+
+}  // namespace dev
+}  // namespace awsem

@@ -1,0 +1,780 @@
+// Host-side model construction: parsers for the reference's input formats and
+// the builders that turn them into the engine's device layouts.
+//
+// Formats and semantics follow the reference:
+//   coefficient file section loop + epsilon scaling   fix_backbone.cpp:164-516
+//   DSSP tables, ssweight, gamma.dat, burial_gamma.dat fix_backbone.cpp:555-693
+//   sequence file                                     fix_backbone.cpp:537-553
+//   .mem list / .gro memories                         fix_backbone.cpp:1966-2042,
+//                                                     fragment_memory.cpp:34-176
+//   gamma file (Gamma_Array)                          fragment_memory.cpp:275-454
+//   residue -> memory map                             fix_backbone.cpp:749-791
+//   pair_style/pair_coeff vexcluded                   pair_excluded_volume.cpp:175-265
+#include "awsem_model.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <map>
+#include <sstream>
+#include <stdexcept>
+
+namespace awsem {
+
+namespace {
+
+const char kAA[] = "ARNDCQEGHILKMFPSTWYV";
+
+int residue_code(char c)
+{
+  const char *p = strchr(kAA, c);
+  return (p && c) ? int(p - kAA) : 0;
+}
+
+int residue_class4(int t)
+{
+  // SHL 1 (A G P S T), AHL 2 (N D Q E), BAS 3 (R H K), HPB 4 (C I L M F W Y V)
+  static const int cls[20] = {1, 3, 2, 2, 4, 2, 2, 1, 3, 4, 4, 3, 4, 4, 1, 1, 1, 4, 4, 4};
+  return cls[t];
+}
+
+std::vector<std::string> tokens(const std::string &line)
+{
+  std::vector<std::string> out;
+  std::istringstream in(line);
+  for (std::string t; in >> t;) out.push_back(t);
+  return out;
+}
+
+std::string path_in(const std::string &dir, const std::string &name)
+{
+  if (name.empty() || name[0] == '/' || dir.empty()) return name;
+  return dir + "/" + name;
+}
+
+[[noreturn]] void fail(const std::string &msg) { throw std::runtime_error(msg); }
+
+char residue_from_three(const char *s)
+{
+  static const char *names[20] = {"ALA", "ARG", "ASN", "ASP", "CYS", "GLN", "GLU", "GLY", "HIS", "ILE",
+                                  "LEU", "LYS", "MET", "PHE", "PRO", "SER", "THR", "TRP", "TYR", "VAL"};
+  for (int k = 0; k < 20; k++)
+    if (!strcmp(s, names[k])) return kAA[k];
+  return '?';
+}
+
+}  // namespace
+
+void read_coeff_file(const std::string &path, ForceField &ff)
+{
+  std::ifstream in(path);
+  if (!in) fail("Coefficient file was not found!");
+  FFParams &p = ff.p;
+  p = FFParams{};
+  p.epsilon = 1.0;
+  p.an = 0.4831806; p.bn = 0.7032820; p.cn = -0.1864262;
+  p.ap = 0.4436538; p.bp = 0.2352006; p.cp = 0.3211455;
+  p.ah = 0.8409657; p.bh = 0.8929599; p.ch = -0.7338894;
+  p.fm_sigma_exp = 0.15;
+  const int i_rp = 6;  // first proline Ramachandran well
+  double k_rama = 0.0, k_water = 0.0;
+  static const char *outside[] = {
+      "[Shake]", "[Excluded]", "[Excluded_P]", "[Excluded_R6]", "[AMH-Go]", "[Fragment_Memory_Table]",
+      "[Contact_Restraints]", "[Vector_Fragment_Memory]", "[Solvent_Barrier]", "[Membrane]",
+      "[Fragment_Frustratometer]", "[Tertiary_Frustratometer]", "[Nmer_Frustratometer]", "[Phosphorylation]",
+      "[Amylometer]", "[Selection_Temperature]", "[Monte_Carlo_Seq_Opt]", "[Optimization]",
+      "[Burial_Optimization]", "[DebyeHuckel]", "[DebyeHuckel_Optimization]", "[Shuffler]", "[Mutate_Sequence]"};
+  std::string s;
+  while (in >> s) {
+    if (s == "[ABC]") {
+      in >> p.an >> p.bn >> p.cn >> p.ap >> p.bp >> p.cp >> p.ah >> p.bh >> p.ch;
+    } else if (s == "[Chain]") {
+      p.terms |= T_CHAIN;
+      in >> p.k_chain[0] >> p.k_chain[1] >> p.k_chain[2] >> p.r_ncb0 >> p.r_cpcb0 >> p.r_ncp0;
+    } else if (s == "[Chi]") {
+      p.terms |= T_CHI;
+      in >> p.k_chi >> p.chi0;
+    } else if (s == "[Rama]") {
+      p.terms |= T_RAMA;
+      in >> k_rama >> p.n_rama;
+      if (p.n_rama > i_rp) fail("Rama: too many wells");
+      for (int j = 0; j < p.n_rama; j++) {
+        double sigma;
+        in >> p.w[j] >> sigma >> p.phiw[j] >> p.phi0[j] >> p.psiw[j] >> p.psi0[j];
+        p.phiw[j] *= sigma;
+        p.psiw[j] *= sigma;
+      }
+    } else if (s == "[Rama_P]") {
+      p.terms |= T_RAMA_P;
+      in >> p.n_rama_p;
+      if (p.n_rama_p > 12 - i_rp) fail("Rama_P: too many wells");
+      for (int j = i_rp; j < i_rp + p.n_rama_p; j++) {
+        double sigma;
+        in >> p.w[j] >> sigma >> p.phiw[j] >> p.phi0[j] >> p.psiw[j] >> p.psi0[j];
+        p.phiw[j] *= sigma;
+        p.psiw[j] *= sigma;
+      }
+    } else if (s == "[SSWeight]") {
+      p.terms |= T_SSW;
+      for (int j = 0; j < 12; j++) in >> p.ssweight[j];
+    } else if (s == "[Dssp_Hdrgn]") {
+      p.terms |= T_DSSP;
+      double sHO, sNO;
+      in >> p.k_dssp >> p.hbscl[0][0] >> p.hbscl[0][1];
+      for (int j = 0; j < 7; j++) in >> p.hbscl[1][j];
+      for (int j = 0; j < 9; j++) in >> p.hbscl[2][j];
+      for (int j = 0; j < 9; j++) in >> p.hbscl[3][j];
+      in >> sHO >> sNO >> p.HO_zero >> p.NO_zero >> p.dssp_cut >> p.pref[0] >> p.pref[1] >> p.d_nu0;
+      p.dssp_cut_sq = p.dssp_cut * p.dssp_cut;
+      for (int k = 0; k < 2; k++) p.nu_cut_sq[k] = pow(p.d_nu0 + atanh(2.0 * 1e-4 - 1.0) / p.pref[k], 2);
+      p.sigma_HO_sqinv = 1.0 / (sHO * sHO);
+      p.sigma_NO_sqinv = 1.0 / (sNO * sNO);
+    } else if (s == "[P_AP]") {
+      p.terms |= T_PAP;
+      in >> p.k_global_pap >> p.k_betapred_pap >> p.k_pap[0] >> p.k_pap[1] >> p.k_pap[2] >> p.pap_cut >>
+          p.pap_pref >> p.i_med_min >> p.i_med_max >> p.i_diff_pap;
+      p.pap_cutoff_sq = pow(p.pap_cut + atanh(1.0 - 2.0 * 1e-12) / p.pap_pref, 2);
+    } else if (s == "[Water]") {
+      p.terms |= T_WATER;
+      in >> k_water >> p.water_kappa >> p.water_kappa_sigma >> p.treshold >> p.contact_cutoff >> p.n_wells;
+      if (p.n_wells > 5) fail("Water: at most 5 wells");
+      for (int j = 0; j < p.n_wells; j++) in >> p.well_rmin[j] >> p.well_rmax[j] >> p.well_flag[j];
+    } else if (s == "[Burial]") {
+      p.terms |= T_BURIAL;
+      in >> p.k_burial >> p.burial_kappa;
+      for (int j = 0; j < 3; j++) in >> p.burial_ro_min[j] >> p.burial_ro_max[j];
+    } else if (s == "[Helix]") {
+      p.terms |= T_HELIX;
+      double sHO, sNO;
+      in >> p.k_helix >> p.helix_gamma_p >> p.helix_gamma_w >> p.helix_kappa >> p.helix_kappa_sigma >>
+          p.helix_treshold >> p.helix_i_diff >> p.helix_cutoff >> p.helix_rmin >> p.helix_rmax;
+      for (int j = 0; j < 20; j++) in >> p.h4prob[j];
+      in >> p.pro_acc_flag >> p.h4prob_pro >> sHO >> sNO >> p.helix_HO_zero >> p.helix_NO_zero;
+      p.helix_cutoff_sq = p.helix_cutoff * p.helix_cutoff;
+      p.helix_sigma_HO_sqinv = 1.0 / (sHO * sHO);
+      p.helix_sigma_NO_sqinv = 1.0 / (sNO * sNO);
+    } else if (s == "[Fragment_Memory]") {
+      p.terms |= T_FM;
+      in >> ff.k_fm_raw >> ff.fm_file >> ff.fm_gamma_file;
+    } else if (s == "[Epsilon]") {
+      in >> p.epsilon;
+    } else {
+      for (const char *o : outside)
+        if (s == o) fail("section " + s + " is not supported by the GPU engine");
+    }
+  }
+  // epsilon scaling (fix_backbone.cpp:501-516)
+  for (double &k : p.k_chain) k *= p.epsilon;
+  p.k_chi *= p.epsilon;
+  k_rama *= p.epsilon;
+  k_water *= p.epsilon;
+  p.k_burial *= p.epsilon;
+  p.k_helix *= p.epsilon;
+  p.k_dssp *= p.epsilon;
+  p.k_global_pap *= p.epsilon;
+  for (int j = 0; j < p.n_rama; j++) p.w[j] *= k_rama;
+  for (int j = 0; j < p.n_rama_p; j++) p.w[j + i_rp] *= k_rama;
+  p.k_fm = ff.k_fm_raw;
+  // density-well supports (smart_matrix_lib.h:363-368) and P_AP saturation (:110-115)
+  for (int k = 0; k < p.n_wells; k++) {
+    p.w_rmin_th[k] = p.well_rmin[k] - 8.0 * 2.302585 / p.water_kappa;
+    p.w_rmax_th[k] = p.well_rmax[k] + 8.0 * 2.302585 / p.water_kappa;
+    p.w_rmin_sq[k] = p.w_rmin_th[k] * p.w_rmin_th[k];
+    p.w_rmax_sq[k] = p.w_rmax_th[k] * p.w_rmax_th[k];
+  }
+  if (p.terms & T_HELIX) {
+    p.h_rmin_th = p.helix_rmin - 8.0 * 2.302585 / p.helix_kappa;
+    p.h_rmax_th = p.helix_rmax + 8.0 * 2.302585 / p.helix_kappa;
+    p.h_rmin_sq = p.h_rmin_th * p.h_rmin_th;
+    p.h_rmax_sq = p.h_rmax_th * p.h_rmax_th;
+  }
+  if (p.terms & T_PAP) {
+    double span = double(int(8.0 * 2.302585 / p.pap_pref) + 1);
+    p.pap_drmax_sq = (p.pap_cut + span) * (p.pap_cut + span);
+    p.pap_drmin_sq = (p.pap_cut - span) * (p.pap_cut - span);
+  }
+  ff.k_water = k_water;
+  ff.tables.assign(TB_SIZE, 0.0);
+}
+
+void read_sequence(const std::string &path, Topology &top)
+{
+  std::ifstream in(path);
+  if (!in) fail("Sequence file was not found");
+  top.seq.clear();
+  top.chain_start.clear();
+  top.chain_end.clear();
+  for (std::string t; in >> t;) {
+    if (t[0] == '#') continue;
+    top.chain_start.push_back((int) top.seq.size());
+    top.seq += t;
+    top.chain_end.push_back((int) top.seq.size() - 1);
+  }
+  top.n_chains = (int) top.chain_start.size();
+  top.n_res = (int) top.seq.size();
+}
+
+void read_tables(const std::string &dir, ForceField &ff, Topology &top)
+{
+  FFParams &p = ff.p;
+  double k_water = ff.k_water;
+  std::vector<double> &T = ff.tables;
+  T.assign(TB_SIZE, 0.0);
+  if (p.terms & T_DSSP) {
+    const char *names[5] = {"anti_HB", "anti_NHB", "para_HB", "para_one", "anti_one"};
+    std::ifstream f[5];
+    for (int k = 0; k < 5; k++) {
+      f[k].open(path_in(dir, names[k]));
+      if (!f[k]) fail(std::string("File ") + names[k] + " doesn't exist");
+    }
+    for (int blk = 0; blk < 2; blk++)
+      for (int i = 0; i < 20; i++) {
+        if (blk == 0) {
+          f[3] >> T[TB_PARA_ONE + i];
+          f[4] >> T[TB_ANTI_ONE + i];
+        }
+        for (int j = 0; j < 20; j++) {
+          int at = (i * 20 + j) * 2 + blk;
+          f[0] >> T[TB_ANTI_HB + at];
+          f[1] >> T[TB_ANTI_NHB + at];
+          f[2] >> T[TB_PARA_HB + at];
+        }
+      }
+    for (auto &s : f)
+      if (!s) fail("DSSP file format error");
+  }
+  top.aps.assign((size_t) 12 * top.n_res, 0.0);
+  if (p.terms & T_SSW) {
+    std::ifstream in(path_in(dir, "ssweight"));
+    if (!in) fail("File ssweight doesn't exist");
+    for (int r = 0; r < top.n_res; r++)
+      for (int k = 0; k < 12; k++)
+        if (p.ssweight[k]) in >> top.aps[(size_t) k * top.n_res + r];
+  }
+  if (p.terms & T_WATER) {
+    std::ifstream in(path_in(dir, "gamma.dat"));
+    if (!in) fail("File gamma.dat doesn't exist");
+    for (int w = 0; w < p.n_wells; w++)
+      for (int i = 0; i < 20; i++)
+        for (int j = i; j < 20; j++) {
+          double g0, g1;
+          in >> g0 >> g1;
+          if (!in) fail("Water potential gamma.dat file format error");
+          g0 *= k_water;
+          g1 *= k_water;
+          for (int s = 0; s < 2; s++) {
+            int a = s ? j : i, b = s ? i : j;
+            T[TB_WATER + w * 800 + (a * 20 + b) * 2 + 0] = g0;
+            T[TB_WATER + w * 800 + (a * 20 + b) * 2 + 1] = g1;
+          }
+        }
+  }
+  if (p.terms & T_BURIAL) {
+    if (!(p.terms & T_WATER)) fail("Cannot use burial without water potential");
+    std::ifstream in(path_in(dir, "burial_gamma.dat"));
+    if (!in) fail("File burial_gamma.dat doesn't exist");
+    for (int i = 0; i < 60; i++) in >> T[TB_BURIAL + i];
+    if (!in) fail("Burial potential burial_gamma.dat file format error");
+  }
+}
+
+double GammaTable::get(int ti, int tj, int tfi, int tfj, int ires, int jres) const
+{
+  int d = std::abs(ires - jres);
+  if (d < i_sep[0] || (i_sep[nseq_cl] != -1 && d > i_sep[nseq_cl])) return 0.0;
+  int cl = 1;
+  while (cl < nseq_cl && d >= i_sep[cl]) cl++;
+  if (nres_cl == 1) return g[cl - 1];
+  auto c = [&](int t) { return nres_cl == 4 ? residue_class4(t) - 1 : t; };
+  size_t n2 = (size_t) nres_cl * nres_cl;
+  if (!frag_resty) return g[(cl - 1) * n2 + c(ti) * nres_cl + c(tj)];
+  return g[(cl - 1) * n2 * n2 + (c(ti) * nres_cl + c(tj)) * n2 + c(tfi) * nres_cl + c(tfj)];
+}
+
+void read_gamma_table(const std::string &path, GammaTable &G)
+{
+  FILE *f = fopen(path.c_str(), "r");
+  if (!f) fail("Fragment_Memory: Cannot read gamma file");
+  char line[512];
+  std::vector<std::vector<std::string>> entries;
+  bool header = true;
+  while (fgets(line, sizeof line, f)) {
+    if (line[0] == '#') continue;
+    auto t = tokens(line);
+    if (t.empty()) continue;
+    if (header) {
+      int ns = 0;
+      for (auto &s : t) {
+        if (ns >= 10) fail("Fragment_Memory: Wrong definition of sequance separation classes");
+        G.i_sep[ns++] = s == "inf" ? -1 : atoi(s.c_str());
+        if (s == "inf") break;
+      }
+      G.nseq_cl = ns - 1;
+      if (G.nseq_cl <= 0) fail("Fragment_Memory: Wrong definition of sequance separation classes");
+      header = false;
+    } else {
+      if (t.size() != 4 && t.size() != 6) fail("Fragment_Memory: Incorrect entery in gamma file");
+      entries.push_back(t);
+    }
+  }
+  fclose(f);
+  if (entries.empty()) fail("Fragment_Memory: Incorrect entery in gamma file");
+  G.frag_resty = entries[0].size() == 6;
+  G.nres_cl = 0;
+  for (auto &e : entries) {
+    if ((e.size() == 6) != G.frag_resty) fail("Fragment_Memory: Incorrect entery in gamma file");
+    for (size_t k = 0; k + 2 < e.size(); k++) {
+      size_t L = e[k].size();
+      if (e[k] == "ALL") G.nres_cl = std::max(G.nres_cl, 1);
+      else if (L == 3) G.nres_cl = std::max(G.nres_cl, 4);
+      else if (L == 1) G.nres_cl = std::max(G.nres_cl, 20);
+      else fail("Fragment_Memory: Incorrect entery in gamma file");
+    }
+  }
+  size_t n2 = (size_t) G.nres_cl * G.nres_cl;
+  G.g.assign(G.nseq_cl * (G.frag_resty ? n2 * n2 : n2), 0.0);
+  auto expand = [&](const std::string &s) {
+    std::vector<int> v;
+    if (s == "ALL") {
+      for (int i = 0; i < G.nres_cl; i++) v.push_back(i);
+    } else if (s.size() == 1) {
+      if (G.nres_cl < 20) fail("Fragment_Memory: Cannot build gamma array");
+      v.push_back(residue_code(s[0]));
+    } else {
+      int c = s == "SHL" ? 1 : s == "AHL" ? 2 : s == "BAS" ? 3 : s == "HPB" ? 4 : 0;
+      if (!c) fail("Fragment_Memory: Incorrect entery in gamma file");
+      if (G.nres_cl == 4) v.push_back(c - 1);
+      else
+        for (int i = 0; i < 20; i++)
+          if (residue_class4(i) == c) v.push_back(i);
+    }
+    return v;
+  };
+  for (auto &e : entries) {
+    if (!G.frag_resty) {
+      int cl = atoi(e[2].c_str());
+      if (cl > G.nseq_cl) fail("Fragment_Memory: Wrong sequance separation class tag");
+      double gm = atof(e[3].c_str());
+      for (int a : expand(e[0]))
+        for (int b : expand(e[1])) {
+          G.g[(cl - 1) * n2 + a * G.nres_cl + b] = gm;
+          G.g[(cl - 1) * n2 + b * G.nres_cl + a] = gm;
+        }
+    } else {
+      int cl = atoi(e[4].c_str());
+      if (cl > G.nseq_cl) fail("Fragment_Memory: Cannot build gamma array");
+      double gm = atof(e[5].c_str());
+      // the reference hands the i-fragment class in for both fragment slots
+      // (fragment_memory.cpp:369); kept as is
+      auto fi = expand(e[2]);
+      for (int a : expand(e[0]))
+        for (int b : expand(e[1]))
+          for (int c : fi)
+            for (int d : fi) {
+              size_t base = (cl - 1) * n2 * n2;
+              G.g[base + (a * G.nres_cl + b) * n2 + c * G.nres_cl + d] = gm;
+              G.g[base + (b * G.nres_cl + a) * n2 + c * G.nres_cl + d] = gm;
+              G.g[base + (a * G.nres_cl + b) * n2 + d * G.nres_cl + c] = gm;
+              G.g[base + (b * G.nres_cl + a) * n2 + d * G.nres_cl + c] = gm;
+            }
+    }
+  }
+}
+
+void read_memories(const std::string &dir, const std::string &mem_file, int n_res, std::vector<Memory> &mems)
+{
+  FILE *f = fopen(path_in(dir, mem_file).c_str(), "r");
+  if (!f) fail("Fragment_Memory: Error opening mem file");
+  char buf[1024];
+  enum { NONE, TARGET, MEMS } state = NONE;
+  std::map<std::string, std::vector<std::string>> gro_cache;
+  while (fgets(buf, sizeof buf, f)) {
+    auto t = tokens(buf);
+    if (!t.empty() && t[0][0] == '#') continue;
+    if (!t.empty() && t[0][0] == '[') state = NONE;
+    if (t.empty()) {
+      state = NONE;
+      continue;
+    }
+    if (state == MEMS) {
+      if (t.size() != 5) fail("Fragment_Memory: Error reading mem file");
+      Memory m;
+      m.pos = atoi(t[1].c_str()) - 1;
+      int fpos = atoi(t[2].c_str()) - 1;
+      m.len = atoi(t[3].c_str());
+      m.weight = atof(t[4].c_str());
+      if (m.len <= 0) fail("Fragment_Memory: Incorrectly defined memory fragment");
+      m.se.assign(m.len, '-');
+      m.xca.assign((size_t) m.len * 3, 0.0);
+      m.xcb.assign((size_t) m.len * 3, 0.0);
+      FILE *g = fopen(path_in(dir, t[0]).c_str(), "r");
+      if (!g) fail("Fragment_Memory: Cannot read the file");
+      char title[256];
+      int nat = 0, nca = 0;
+      if (!fgets(title, sizeof title, g) || fscanf(g, "%d", &nat) != 1) {
+        fclose(g);
+        fail("Fragment_Memory: Wrong atom count in memory structure file");
+      }
+      for (int a = 0; a < nat; a++) {
+        int ires, iat;
+        char rn[32], an[32];
+        double x, y, z;
+        if (fscanf(g, "%d %31s %31s %d %lf %lf %lf", &ires, rn, an, &iat, &x, &y, &z) != 7) break;
+        if (ires > fpos + m.len) break;
+        if (ires <= fpos) continue;
+        int r = ires - fpos - 1;
+        double *dst = nullptr;
+        if (!strcmp(an, "CA")) {
+          m.se[r] = residue_from_three(rn);
+          if (m.se[r] == '?') {
+            fclose(g);
+            fail("Fragment_Memory: Unknown residue");
+          }
+          dst = &m.xca[3 * r];
+          nca++;
+        } else if (!strcmp(an, "CB")) {
+          dst = &m.xcb[3 * r];
+        }
+        if (dst) {
+          dst[0] = x * 10;
+          dst[1] = y * 10;
+          dst[2] = z * 10;
+        }
+      }
+      fclose(g);
+      if (nca != m.len) fail("Fragment_Memory: Wrong atom count in memory structure file");
+      if (m.pos + m.len > n_res) fail("read_mems: Fragment_Memory: Incorrectly defined memory fragment");
+      mems.push_back(std::move(m));
+    } else if (state == NONE) {
+      if (t[0] == "[Target]") state = TARGET;
+      else if (t[0] == "[Memories]") state = MEMS;
+    }
+  }
+  fclose(f);
+}
+
+void build_topology(Topology &top, int n_atoms, const int *role, const int *residue, const int *molecule,
+                    const int *type, const int *tag, const double *mass_by_type, int ntypes)
+{
+  int n = top.n_res;
+  if (n <= 0) fail("sequence must be read before the topology");
+  top.n_atoms = 3 * n;
+  top.ntypes = ntypes;
+  top.ext_of.assign(top.n_atoms, -1);
+  top.atom_type.assign(top.n_atoms, 0);
+  top.atom_tag.assign(top.n_atoms, 0);
+  top.mass.assign(top.n_atoms, 0.0);
+  top.res_chain.assign(n, -1);
+  for (int a = 0; a < n_atoms; a++) {
+    if (role[a] < 0) continue;
+    int r = residue[a] - 1;
+    if (r < 0 || r >= n) fail("Residue tag is out of range");
+    if (residue[a] <= 0) fail("Molecular tag must be positive in fix backbone");
+    int slot = 3 * r + role[a];
+    if (top.ext_of[slot] != -1) fail("two atoms of the same role in one residue");
+    top.ext_of[slot] = a;
+    top.atom_type[slot] = type[a];
+    top.atom_tag[slot] = tag ? tag[a] : a + 1;
+    top.mass[slot] = mass_by_type[type[a]];
+    int c = molecule[a] - 1;
+    if (c < 0 || c >= top.n_chains) fail("Chain tag is out of range");
+    if (top.res_chain[r] == -1) top.res_chain[r] = c;
+    else if (top.res_chain[r] != c) fail("Atoms in a residue have different chain tag");
+  }
+  if (n_atoms != top.n_atoms) fail("every atom must be a CA, CB/H-beta or O of a residue");
+  for (int slot = 0; slot < top.n_atoms; slot++)
+    if (top.ext_of[slot] == -1) fail("Missing neighbor atoms in fix backbone (Code 001)");
+  top.res_type.assign(n, 0);
+  top.res_flags.assign(n, 0);
+  for (int r = 0; r < n; r++) {
+    int c = top.res_chain[r];
+    if (r < top.chain_start[c] || r > top.chain_end[c]) fail("Residue tag is out of range");
+    char s = top.seq[r];
+    top.res_type[r] = residue_code(s);
+    uint32_t fl = 0;
+    if (s == 'G') fl |= R_GLY;
+    if (s == 'P') fl |= R_PRO;
+    if (r == top.chain_start[c]) fl |= R_FIRST;
+    if (r == top.chain_end[c]) fl |= R_LAST;
+    top.res_flags[r] = (int) fl;
+  }
+}
+
+void set_bonds(Topology &top, int nb, const int *bi, const int *bj, const double *k, const double *r0,
+               const int *ext_to_int)
+{
+  top.bond_i.clear();
+  top.bond_j.clear();
+  top.bond_k.clear();
+  top.bond_r0.clear();
+  top.excl_self.assign(top.n_res, 0u);
+  top.excl_next.assign(top.n_res, 0u);
+  for (int b = 0; b < nb; b++) {
+    int a1 = ext_to_int[bi[b]], a2 = ext_to_int[bj[b]];
+    top.bond_i.push_back(a1);
+    top.bond_j.push_back(a2);
+    top.bond_k.push_back(k[b]);
+    top.bond_r0.push_back(r0[b]);
+    int r1 = a1 / 3, r2 = a2 / 3, b1 = a1 % 3, b2 = a2 % 3;
+    if (r1 == r2) {
+      top.excl_self[r1] |= 1u << (b1 * 3 + b2);
+      top.excl_self[r1] |= 1u << (b2 * 3 + b1);
+    } else if (r2 == r1 + 1) {
+      top.excl_next[r1] |= 1u << (b1 * 3 + b2);
+    } else if (r1 == r2 + 1) {
+      top.excl_next[r2] |= 1u << (b2 * 3 + b1);
+    } else {
+      fail("bonds must join beads of the same or adjacent residues");
+    }
+  }
+}
+
+void set_pair_coeffs(Topology &top, const std::string &style, const std::string &coeffs)
+{
+  auto s = tokens(style);
+  if (s.size() != 3) fail("Illegal pair_style command");
+  top.ev_p = atoi(s[0].c_str());
+  double cs_glob = atof(s[1].c_str()), cl_glob = atof(s[2].c_str());
+  int N = top.ntypes + 1;
+  std::vector<double> lam(N * N, 0.0), cs(N * N, 0.0), cl(N * N, 0.0);
+  std::vector<int> set(N * N, 0);
+  std::stringstream ss(coeffs);
+  std::string rec;
+  auto bounds = [&](const std::string &t, int &lo, int &hi) {
+    size_t st = t.find('*');
+    if (st == std::string::npos) lo = hi = atoi(t.c_str());
+    else {
+      lo = st == 0 ? 1 : atoi(t.substr(0, st).c_str());
+      hi = st + 1 == t.size() ? top.ntypes : atoi(t.substr(st + 1).c_str());
+    }
+    if (lo < 1 || hi > top.ntypes || lo > hi) fail("Numeric index is out of bounds");
+  };
+  while (std::getline(ss, rec, ';')) {
+    auto c = tokens(rec);
+    if (c.empty()) continue;
+    if (c.size() != 3 && c.size() != 5) fail("Incorrect args for pair coefficients");
+    int ilo, ihi, jlo, jhi;
+    bounds(c[0], ilo, ihi);
+    bounds(c[1], jlo, jhi);
+    for (int i = ilo; i <= ihi; i++)
+      for (int j = std::max(jlo, i); j <= jhi; j++) {
+        lam[i * N + j] = atof(c[2].c_str());
+        cs[i * N + j] = c.size() == 5 ? atof(c[3].c_str()) : cs_glob;
+        cl[i * N + j] = c.size() == 5 ? atof(c[4].c_str()) : cl_glob;
+        set[i * N + j] = 1;
+      }
+  }
+  // init_one: geometric mixing for unset pairs, then symmetrise
+  int sign = top.ev_p % 2 == 0 ? 1 : -1;
+  top.ev_pref.assign(N * N, 0.0);
+  top.ev_cs.assign(N * N, 0.0);
+  top.ev_cl.assign(N * N, 0.0);
+  for (int i = 1; i <= top.ntypes; i++)
+    for (int j = i; j <= top.ntypes; j++) {
+      if (!set[i * N + j]) {
+        lam[i * N + j] = sqrt(lam[i * N + i] * lam[j * N + j]);
+        cs[i * N + j] = sqrt(cs[i * N + i] * cs[j * N + j]);
+        cl[i * N + j] = sqrt(cl[i * N + i] * cl[j * N + j]);
+      }
+      for (int s2 = 0; s2 < 2; s2++) {
+        int a = s2 ? j : i, b = s2 ? i : j;
+        top.ev_pref[a * N + b] = lam[i * N + j] * sign;
+        top.ev_cs[a * N + b] = cs[i * N + j];
+        top.ev_cl[a * N + b] = cl[i * N + j];
+      }
+    }
+}
+
+void build_fm_table(const ForceField &ff, const Topology &top, const GammaTable &G, const std::vector<Memory> &mems,
+                    FMTable &out)
+{
+  const FFParams &p = ff.p;
+  int n = top.n_res;
+  int min_sep = G.min_sep(), max_sep = G.max_sep();
+  int max_len = 0;
+  for (auto &m : mems) max_len = std::max(max_len, m.len);
+  int dmax = max_sep == -1 ? max_len - 1 : std::min(max_sep, max_len - 1);
+  out.nd = std::max(dmax - min_sep + 1, 0);
+  if (min_sep + out.nd > 64) fail("fragment memory: sequence separations above 63 are not supported");
+  // memories listing residue i (fix_backbone.cpp:772-789), in memory order
+  std::vector<std::vector<int>> listed(n);
+  for (int k = 0; k < (int) mems.size(); k++)
+    for (int i = mems[k].pos; i < mems[k].pos + mems[k].len - min_sep; i++) listed[i].push_back(k);
+  struct Rec {
+    double rf[4];
+    double c;
+  };
+  std::vector<std::vector<Rec>> rows((size_t) n * std::max(out.nd, 1));
+  auto dist = [](const double *a, const double *b) {
+    return sqrt((a[0] - b[0]) * (a[0] - b[0]) + (a[1] - b[1]) * (a[1] - b[1]) + (a[2] - b[2]) * (a[2] - b[2]));
+  };
+  for (int i = 0; i < n; i++) {
+    for (int k : listed[i]) {
+      const Memory &m = mems[k];
+      int je = m.pos + m.len - 1;
+      if (max_sep != -1) je = std::min(je, i + max_sep);
+      if (je >= n) fail("Missing residues in memory potential");
+      double ekw = p.epsilon * p.k_fm * m.weight;
+      for (int j = i + min_sep; j <= je; j++) {
+        if (top.res_chain[i] != top.res_chain[j])
+          fail("Fragment Memory: Interaction between residues of different chains");
+        int d = j - i - min_sep;
+        int li = i - m.pos, lj = j - m.pos;
+        char mi = m.se[li], mj = m.se[lj];
+        double gam = G.get(top.res_type[i], top.res_type[j], residue_code(mi), residue_code(mj), i, j);
+        Rec rec;
+        rec.c = ekw * gam;
+        // atom pairs CA-CA, CA-CB, CB-CA, CB-CB (fix_backbone.cpp:4088-4096, fragment_memory.cpp:190-202)
+        rec.rf[0] = dist(&m.xca[3 * li], &m.xca[3 * lj]);
+        rec.rf[1] = dist(&m.xca[3 * li], &m.xcb[3 * lj]);
+        rec.rf[2] = dist(&m.xca[3 * lj], &m.xcb[3 * li]);
+        rec.rf[3] = dist(&m.xcb[3 * lj], &m.xcb[3 * li]);
+        bool gi = top.seq[i] == 'G' || mi == 'G', gj = top.seq[j] == 'G' || mj == 'G';
+        if (gj) rec.rf[1] = FMTable::FM_SKIP;
+        if (gi) rec.rf[2] = FMTable::FM_SKIP;
+        if (gi || gj) rec.rf[3] = FMTable::FM_SKIP;
+        rows[(size_t) i * out.nd + d].push_back(rec);
+      }
+    }
+  }
+  out.row_start.assign((size_t) n * out.nd + 1, 0);
+  long long tot = 0;
+  for (size_t r = 0; r < rows.size() && out.nd > 0; r++) {
+    out.row_start[r] = (int) tot;
+    tot += (long long) rows[r].size();
+  }
+  if (tot > 0x7fffffffLL) fail("fragment memory table too large");
+  out.row_start[(size_t) n * out.nd] = (int) tot;
+  out.rf.resize((size_t) tot * 4);
+  out.coef.resize((size_t) tot);
+  out.uniform = true;
+  bool have = false;
+  size_t at = 0;
+  for (auto &row : rows)
+    for (auto &rec : row) {
+      for (int k = 0; k < 4; k++) out.rf[4 * at + k] = rec.rf[k];
+      out.coef[at] = rec.c;
+      if (!have) {
+        out.uniform_coef = rec.c;
+        have = true;
+      } else if (rec.c != out.uniform_coef) {
+        out.uniform = false;
+      }
+      at++;
+    }
+  if (out.uniform) out.coef.clear();
+}
+
+void load_system_dir(const std::string &dir, const std::string &data_file, const std::string &coeff_file,
+                     const std::string &seq_file, const std::string &pair_style, const std::string &pair_coeffs,
+                     SystemInput &S)
+{
+  read_coeff_file(path_in(dir, coeff_file), S.ff);
+  read_sequence(path_in(dir, seq_file), S.top);
+  // LAMMPS data file, atom_style awsemmd
+  std::ifstream in(path_in(dir, data_file));
+  if (!in) fail("cannot open data file " + data_file);
+  std::string line;
+  std::getline(in, line);
+  int natoms = 0, ntypes = 0, nbt = 0;
+  std::map<std::string, std::vector<std::string>> sec;
+  std::string cur;
+  while (std::getline(in, line)) {
+    size_t h = line.find('#');
+    if (h != std::string::npos) line.resize(h);
+    auto t = tokens(line);
+    if (t.empty()) continue;
+    if (cur.empty()) {
+      if (t.size() >= 2 && t[1] == "atoms") { natoms = atoi(t[0].c_str()); continue; }
+      if (t.size() >= 3 && t[1] == "atom" && t[2] == "types") { ntypes = atoi(t[0].c_str()); continue; }
+      if (t.size() >= 3 && t[1] == "bond" && t[2] == "types") { nbt = atoi(t[0].c_str()); continue; }
+      if (t.size() >= 2 && (t[1] == "bonds" || t[1] == "angles" || t[1] == "dihedrals" || t[1] == "impropers")) continue;
+      if (t.size() >= 3 && (t[2] == "types" || t[2] == "xlo" || t[2] == "ylo" || t[2] == "zlo")) continue;
+    }
+    if (t[0] == "Masses" || t[0] == "Atoms" || t[0] == "Velocities" || t[0] == "Bonds") {
+      cur = t[0];
+      continue;
+    }
+    if (t[0] == "Bond" && t.size() > 1 && t[1] == "Coeffs") {
+      cur = "Bond Coeffs";
+      continue;
+    }
+    if (cur.empty()) fail("data file: unexpected line: " + line);
+    sec[cur].push_back(line);
+  }
+  std::vector<double> mass(ntypes + 1, 0.0);
+  for (auto &l : sec["Masses"]) {
+    auto t = tokens(l);
+    mass.at(atoi(t[0].c_str())) = atof(t[1].c_str());
+  }
+  if ((int) sec["Atoms"].size() != natoms) fail("data file: Atoms section incomplete");
+  std::vector<std::pair<int, std::vector<std::string>>> rows;
+  for (auto &l : sec["Atoms"]) {
+    auto t = tokens(l);
+    if (t.size() < 8) fail("data file: Atoms line needs id molecule residue type q x y z");
+    rows.push_back({atoi(t[0].c_str()), t});
+  }
+  std::sort(rows.begin(), rows.end(), [](auto &a, auto &b) { return a.first < b.first; });
+  std::vector<int> role(natoms), res(natoms), mol(natoms), typ(natoms), tag(natoms);
+  std::vector<double> xe(3 * natoms), ve(3 * natoms, 0.0);
+  std::map<int, int> tag_to_ext;
+  for (int a = 0; a < natoms; a++) {
+    auto &t = rows[a].second;
+    tag[a] = atoi(t[0].c_str());
+    mol[a] = atoi(t[1].c_str());
+    res[a] = atoi(t[2].c_str());
+    typ[a] = atoi(t[3].c_str());
+    for (int k = 0; k < 3; k++) xe[3 * a + k] = atof(t[5 + k].c_str());
+    // awsemmd type convention: 1 CA, 3 O, 4 CB, 5 H-beta
+    role[a] = typ[a] == 1 ? 0 : (typ[a] == 4 || typ[a] == 5) ? 1 : typ[a] == 3 ? 2 : -1;
+    tag_to_ext[tag[a]] = a;
+  }
+  for (auto &l : sec["Velocities"]) {
+    auto t = tokens(l);
+    int a = tag_to_ext.at(atoi(t[0].c_str()));
+    for (int k = 0; k < 3; k++) ve[3 * a + k] = atof(t[1 + k].c_str());
+  }
+  build_topology(S.top, natoms, role.data(), res.data(), mol.data(), typ.data(), tag.data(), mass.data(), ntypes);
+  std::vector<int> ext_to_int(natoms);
+  for (int s = 0; s < S.top.n_atoms; s++) ext_to_int[S.top.ext_of[s]] = s;
+  std::vector<double> bk(nbt + 1, 0.0), br(nbt + 1, 0.0);
+  for (auto &l : sec["Bond Coeffs"]) {
+    auto t = tokens(l);
+    bk.at(atoi(t[0].c_str())) = atof(t[1].c_str());
+    br.at(atoi(t[0].c_str())) = atof(t[2].c_str());
+  }
+  std::vector<int> bi, bj;
+  std::vector<double> kk, rr;
+  for (auto &l : sec["Bonds"]) {
+    auto t = tokens(l);
+    int bt = atoi(t[1].c_str());
+    bi.push_back(tag_to_ext.at(atoi(t[2].c_str())));
+    bj.push_back(tag_to_ext.at(atoi(t[3].c_str())));
+    kk.push_back(bk.at(bt));
+    rr.push_back(br.at(bt));
+  }
+  set_bonds(S.top, (int) bi.size(), bi.data(), bj.data(), kk.data(), rr.data(), ext_to_int.data());
+  set_pair_coeffs(S.top, pair_style, pair_coeffs);
+  read_tables(dir, S.ff, S.top);
+  if (S.ff.p.terms & T_FM) {
+    read_gamma_table(path_in(dir, S.ff.fm_gamma_file), S.gamma);
+    read_memories(dir, S.ff.fm_file, S.top.n_res, S.mems);
+    S.ff.p.fm_min_sep = S.gamma.min_sep();
+    S.ff.p.fm_max_sep = S.gamma.max_sep();
+    for (int d = 0; d < 64; d++) S.ff.p.fm_sigma_sq[d] = pow((double) d, 2 * S.ff.p.fm_sigma_exp);
+    build_fm_table(S.ff, S.top, S.gamma, S.mems, S.fm);
+    S.ff.p.fm_nd = S.fm.nd;
+  }
+  S.x.assign(3 * S.top.n_atoms, 0.0);
+  S.v.assign(3 * S.top.n_atoms, 0.0);
+  for (int s = 0; s < S.top.n_atoms; s++)
+    for (int k = 0; k < 3; k++) {
+      S.x[3 * s + k] = xe[3 * S.top.ext_of[s] + k];
+      S.v[3 * s + k] = ve[3 * S.top.ext_of[s] + k];
+    }
+}
+
+}  // namespace awsem

@@ -1,0 +1,154 @@
+// Host-side AWSEM model: force-field parameters, system topology and
+// fragment-memory tables, built from the reference's input formats
+// (fix_backbone_coeff.data sections, gamma.dat / burial_gamma.dat / DSSP
+// tables / ssweight, the sequence file, atom_style awsemmd data files and
+// .mem/.gro fragment memories).
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace awsem {
+
+// Energy slots: 0..17 follow the reference fix's energy[] enum
+// (fix_backbone.h:330-332); 18 pair vexcluded, 19 harmonic bonds, 20 kinetic.
+enum Energy {
+  E_TOTAL = 0, E_CHAIN, E_SHAKE, E_CHI, E_RAMA, E_VEXCLUDED, E_DSSP, E_PAP, E_WATER, E_BURIAL,
+  E_HELIX, E_AMHGO, E_FRAGMEM, E_VFRAGMEM, E_CONT_REST, E_MEMB, E_SSB, E_DH,
+  E_FIX_TERMS = 18, E_PAIR = 18, E_BOND = 19, E_KIN = 20, E_SLOTS = 21
+};
+
+enum TermFlag : uint32_t {
+  T_CHAIN = 1u << 0, T_CHI = 1u << 1, T_RAMA = 1u << 2, T_RAMA_P = 1u << 3, T_SSW = 1u << 4,
+  T_DSSP = 1u << 5, T_PAP = 1u << 6, T_WATER = 1u << 7, T_BURIAL = 1u << 8, T_HELIX = 1u << 9,
+  T_FM = 1u << 10
+};
+
+// Residue flags
+enum ResFlag : uint32_t { R_GLY = 1u, R_PRO = 2u, R_FIRST = 4u, R_LAST = 8u };
+
+// Offsets of the lookup tables inside the device table buffer (doubles)
+enum TableOffset {
+  TB_ANTI_HB = 0, TB_ANTI_NHB = 800, TB_PARA_HB = 1600, TB_PARA_ONE = 2400, TB_ANTI_ONE = 2420,
+  TB_BURIAL = 2440, TB_WATER = 2500, TB_SIZE = 2500 + 5 * 800
+};
+
+// Scalar parameters, passed to kernels by value.  Names follow the reference.
+struct FFParams {
+  uint32_t terms;
+  int n_wells, contact_cutoff, helix_i_diff, i_med_min, i_med_max, i_diff_pap;
+  int n_rama, n_rama_p, pro_acc_flag, fm_min_sep, fm_max_sep, fm_nd;
+  int well_flag[5];
+  int ssweight[12];
+  double epsilon;
+  double an, bn, cn, ap, bp, cp, ah, bh, ch;
+  double k_chain[3], r_ncb0, r_cpcb0, r_ncp0, k_chi, chi0;
+  double w[12], phiw[12], phi0[12], psiw[12], psi0[12];
+  double hbscl[4][9];
+  double sigma_NO_sqinv, sigma_HO_sqinv, NO_zero, HO_zero, k_dssp, dssp_cut, dssp_cut_sq;
+  double pref[2], d_nu0, nu_cut_sq[2];
+  double k_global_pap, k_betapred_pap, k_pap[3], pap_cut, pap_pref, pap_cutoff_sq, pap_drmin_sq, pap_drmax_sq;
+  double water_kappa, water_kappa_sigma, treshold;
+  double well_rmin[5], well_rmax[5], w_rmin_th[5], w_rmax_th[5], w_rmin_sq[5], w_rmax_sq[5];
+  double k_burial, burial_kappa, burial_ro_min[3], burial_ro_max[3];
+  double k_helix, helix_gamma_p, helix_gamma_w, helix_kappa, helix_kappa_sigma, helix_treshold;
+  double helix_cutoff, helix_cutoff_sq, helix_rmin, helix_rmax, h_rmin_th, h_rmax_th, h_rmin_sq, h_rmax_sq;
+  double h4prob[20], h4prob_pro, helix_sigma_HO_sqinv, helix_sigma_NO_sqinv, helix_HO_zero, helix_NO_zero;
+  double k_fm, fm_sigma_exp;
+  double fm_sigma_sq[64];  // |i-j|^(2 * fm_sigma_exp) by separation
+};
+
+struct ForceField {
+  FFParams p{};
+  std::vector<double> tables;  // TB_SIZE doubles
+  std::string fm_file, fm_gamma_file;
+  double k_fm_raw = 0.0;
+  double k_water = 0.0;  // epsilon-scaled [Water] strength, applied to gamma.dat
+};
+
+// Gamma_Array (fragment-memory gamma by sequence separation and residue class)
+struct GammaTable {
+  int nseq_cl = 0, nres_cl = 0;
+  bool frag_resty = false;
+  int i_sep[10] = {0};
+  std::vector<double> g;
+  int min_sep() const { return i_sep[0]; }
+  int max_sep() const { return i_sep[nseq_cl]; }
+  double get(int ti, int tj, int tfi, int tfj, int ires, int jres) const;
+};
+
+struct Memory {
+  int pos = 0, len = 0;
+  double weight = 1.0;
+  std::string se;
+  std::vector<double> xca, xcb;  // [len*3], angstrom
+};
+
+// Per-system topology in the engine's internal atom order: atom 3*r + b with
+// b = 0 CA, 1 CB (or H-beta), 2 O, residues in residue-id order.
+struct Topology {
+  int n_res = 0, n_atoms = 0, n_chains = 0;
+  std::string seq;
+  std::vector<int> res_type, res_flags, res_chain, chain_start, chain_end;  // chain_* per chain, inclusive
+  std::vector<double> aps;  // [12][n_res]
+  // external (caller) atom order
+  std::vector<int> ext_of;      // internal atom -> external index
+  std::vector<int> atom_type;   // internal atom -> LAMMPS type
+  std::vector<int> atom_tag;    // internal atom -> atom id (Langevin stream key)
+  std::vector<double> mass;     // internal atom
+  // harmonic bonds (internal atom indices)
+  std::vector<int> bond_i, bond_j;
+  std::vector<double> bond_k, bond_r0;
+  // pair vexcluded
+  int ntypes = 0, ev_p = 2;
+  std::vector<double> ev_pref, ev_cs, ev_cl;  // [(ntypes+1)^2]: lambda*sign, cut_short, cut_long
+  // 1-2 exclusions between beads of residue r and r (self) / r+1 (next): 9-bit masks
+  std::vector<uint32_t> excl_self, excl_next;
+};
+
+// Fragment memory in pair-major form: one row per (target residue i, sep d),
+// each row a run of records (one per covering memory) of 4 distances
+// (CA-CA, CA-CB, CB-CA, CB-CB); skipped glycine pairs hold FM_SKIP.
+struct FMTable {
+  static constexpr double FM_SKIP = 1e30;
+  int nd = 0;                        // rows per residue (d = min_sep .. min_sep+nd-1)
+  std::vector<int> row_start;        // [n_res*nd + 1] record offsets
+  std::vector<double> rf;            // [records*4]
+  std::vector<double> coef;          // [records] eps*k*w*gamma (empty when uniform)
+  double uniform_coef = 0.0;
+  bool uniform = true;
+  long long records() const { return row_start.empty() ? 0 : row_start.back(); }
+};
+
+struct SystemInput {
+  ForceField ff;
+  Topology top;
+  GammaTable gamma;
+  std::vector<Memory> mems;
+  FMTable fm;
+  std::vector<double> x, v;  // internal order [n_atoms*3]
+};
+
+// Parsers (throw std::runtime_error with the reference's message on errors)
+void read_coeff_file(const std::string &path, ForceField &ff);
+void read_tables(const std::string &dir, ForceField &ff, Topology &top);
+void read_sequence(const std::string &path, Topology &top);
+void read_gamma_table(const std::string &path, GammaTable &g);
+void read_memories(const std::string &dir, const std::string &mem_file, int n_res, std::vector<Memory> &mems);
+
+// Topology from per-atom arrays (any order).  role: 0 CA, 1 CB/H-beta, 2 O, -1 other.
+void build_topology(Topology &top, int n_atoms, const int *role, const int *residue, const int *molecule,
+                    const int *type, const int *tag, const double *mass_by_type, int ntypes);
+void set_bonds(Topology &top, int nb, const int *bi, const int *bj, const double *k, const double *r0,
+               const int *ext_to_int);
+void set_pair_coeffs(Topology &top, const std::string &style, const std::string &coeffs);
+void build_fm_table(const ForceField &ff, const Topology &top, const GammaTable &g,
+                    const std::vector<Memory> &mems, FMTable &out);
+
+// Whole system from a directory laid out like a reference run directory.
+void load_system_dir(const std::string &dir, const std::string &data_file, const std::string &coeff_file,
+                     const std::string &seq_file, const std::string &pair_style, const std::string &pair_coeffs,
+                     SystemInput &out);
+
+}  // namespace awsem

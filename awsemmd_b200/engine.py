@@ -1,0 +1,173 @@
+"""Python host API over the C ABI of libawsem_gpu.so (include/awsem_gpu.h).
+
+Mirrors the reference plugin surface for one system:
+
+* construction from a reference-style run directory (``fix backbone``
+  coefficient file and tables, sequence, fragment memories, an
+  ``atom_style awsemmd`` data file, ``pair_style vexcluded`` settings);
+* ``compute`` -- the drop-in force call (FixBackbone::pre_force and
+  PairExcludedVolume::compute: forces added into the caller's array, the
+  18-term energy vector of the fix plus the pair, bond and kinetic terms);
+* ``run`` -- device-resident MD (fix nve + fix langevin) with the step
+  captured in CUDA graphs.
+
+There is no CPU fallback: constructing a system without the CUDA library, or
+without a GPU, raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libawsem_gpu.so")
+
+FP64 = 0
+MIXED = 1
+TERMS_FIX, TERMS_PAIR, TERMS_BOND = 1, 2, 4
+TERMS_ALL = 7
+
+ENERGY_NAMES = ["total", "chain", "shake", "chi", "rama", "excluded", "dssp", "p_ap", "water", "burial",
+                "helix", "amh_go", "frag_mem", "vec_fm", "contact_restraints", "membrane", "ssb", "dh",
+                "vexcluded", "bond", "kinetic"]
+
+
+class RunParams(C.Structure):
+    _fields_ = [("dt", C.c_double), ("langevin", C.c_int), ("t_start", C.c_double), ("t_stop", C.c_double),
+                ("damp", C.c_double), ("seed", C.c_ulonglong), ("skin", C.c_double), ("neigh_every", C.c_int)]
+
+
+class AwsemError(RuntimeError):
+    pass
+
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH):
+    """Load libawsem_gpu.so (raises if it is missing: there is no fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise AwsemError(f"CUDA library not built: {path} (run awsemmd_b200/build.py)")
+    lib = C.CDLL(path)
+    vp, cp, dp, ip = C.c_void_p, C.c_char_p, C.POINTER(C.c_double), C.c_int
+    lib.awsem_last_error.restype = cp
+    lib.awsem_version.restype = ip
+    lib.awsem_create_from_files.argtypes = [cp, cp, cp, cp, cp, cp, ip, ip, C.POINTER(vp)]
+    lib.awsem_destroy.argtypes = [vp]
+    lib.awsem_destroy.restype = None
+    lib.awsem_natoms.argtypes = [vp]
+    lib.awsem_nres.argtypes = [vp]
+    lib.awsem_step.argtypes = [vp]
+    lib.awsem_step.restype = C.c_longlong
+    lib.awsem_compute.argtypes = [vp, C.c_longlong, vp, vp, vp, ip]
+    lib.awsem_set_state.argtypes = [vp, vp, vp]
+    lib.awsem_get_state.argtypes = [vp, vp, vp]
+    lib.awsem_run.argtypes = [vp, C.c_longlong, C.POINTER(RunParams), vp]
+    lib.awsem_energies.argtypes = [vp, vp]
+    lib.awsem_forces.argtypes = [vp, vp]
+    lib.awsem_residue_arrays.argtypes = [vp, vp]
+    lib.awsem_neighbor_stats.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_double), C.POINTER(C.c_int),
+                                         C.POINTER(C.c_int)]
+    _lib = lib
+    return lib
+
+
+def _check(lib, rc: int, what: str):
+    if rc != 0:
+        raise AwsemError(f"{what} failed ({rc}): {lib.awsem_last_error().decode()}")
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+class AwsemSystem:
+    """One AWSEM system on one GPU (the `fix backbone` + `pair vexcluded` path)."""
+
+    def __init__(self, files: dict, precision: str | int = "fp64", device: int = 0):
+        lib = load_library()
+        self.lib = lib
+        prec = {"fp64": FP64, "mixed": MIXED}.get(precision, precision)
+        h = C.c_void_p()
+        rc = lib.awsem_create_from_files(files["workdir"].encode(), files["data"].encode(), files["coeff"].encode(),
+                                         files["seq"].encode(), files["pair_style"].encode(),
+                                         files.get("pair_coeffs", "").encode(), int(prec), int(device), C.byref(h))
+        _check(lib, rc, "awsem_create_from_files")
+        self.h = h
+        self.natoms = lib.awsem_natoms(h)
+        self.nres = lib.awsem_nres(h)
+        self.precision = prec
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.awsem_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def step(self) -> int:
+        return int(self.lib.awsem_step(self.h))
+
+    def compute(self, x: np.ndarray, step: int = 0, terms: int = TERMS_ALL, f: np.ndarray | None = None):
+        """Forces at x added into f (zeros when not given) and the energy vector."""
+        x = np.ascontiguousarray(x, dtype=np.float64).reshape(self.natoms, 3)
+        if f is None:
+            f = np.zeros((self.natoms, 3))
+        e = np.zeros(21)
+        _check(self.lib, self.lib.awsem_compute(self.h, step, _ptr(x), _ptr(f), _ptr(e), terms), "awsem_compute")
+        return f, e
+
+    def set_state(self, x: np.ndarray | None = None, v: np.ndarray | None = None):
+        xa = None if x is None else np.ascontiguousarray(x, dtype=np.float64).reshape(self.natoms, 3)
+        va = None if v is None else np.ascontiguousarray(v, dtype=np.float64).reshape(self.natoms, 3)
+        _check(self.lib, self.lib.awsem_set_state(self.h, None if xa is None else _ptr(xa),
+                                                  None if va is None else _ptr(va)), "awsem_set_state")
+
+    def get_state(self):
+        x = np.zeros((self.natoms, 3))
+        v = np.zeros((self.natoms, 3))
+        _check(self.lib, self.lib.awsem_get_state(self.h, _ptr(x), _ptr(v)), "awsem_get_state")
+        return x, v
+
+    def run(self, nsteps: int, dt=2.0, langevin=True, t_start=300.0, t_stop=300.0, damp=500.0, seed=1,
+            skin=2.0, neigh_every=0, thermo=False):
+        rp = RunParams(dt, int(langevin), t_start, t_stop, damp, seed, skin, neigh_every)
+        rows = np.zeros((nsteps + 1, 4)) if thermo else None
+        _check(self.lib, self.lib.awsem_run(self.h, nsteps, C.byref(rp), None if rows is None else _ptr(rows)),
+               "awsem_run")
+        return rows
+
+    def energies(self) -> np.ndarray:
+        e = np.zeros(21)
+        _check(self.lib, self.lib.awsem_energies(self.h, _ptr(e)), "awsem_energies")
+        return e
+
+    def forces(self) -> np.ndarray:
+        f = np.zeros((self.natoms, 3))
+        _check(self.lib, self.lib.awsem_forces(self.h, _ptr(f)), "awsem_forces")
+        return f
+
+    def residue_arrays(self) -> np.ndarray:
+        out = np.zeros((self.nres, 8))
+        _check(self.lib, self.lib.awsem_residue_arrays(self.h, _ptr(out)), "awsem_residue_arrays")
+        return out
+
+    def neighbor_stats(self) -> dict:
+        nb, mc, ov = C.c_int(), C.c_int(), C.c_int()
+        rad = C.c_double()
+        _check(self.lib, self.lib.awsem_neighbor_stats(self.h, C.byref(nb), C.byref(rad), C.byref(mc), C.byref(ov)),
+               "awsem_neighbor_stats")
+        return {"builds": nb.value, "radius": rad.value, "max_count": mc.value, "overflow": ov.value}

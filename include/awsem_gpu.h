@@ -1,0 +1,139 @@
+/* awsem_gpu.h -- C ABI of the B200 AWSEM-MD engine (libawsem_gpu.so).
+ *
+ * Replaces, for one single-GPU system, the per-step force and energy path of
+ * the reference LAMMPS plugins of adavtyan/awsemmd:
+ *   fix backbone      FixBackbone::pre_force -> compute_backbone
+ *                     (src/fix_backbone.cpp:8181-8189, :7047-7673)
+ *   pair vexcluded    PairExcludedVolume::compute (src/pair_excluded_volume.cpp:50-138)
+ * and the LAMMPS pieces the benchmark step needs around them (bond_style
+ * harmonic, fix nve, fix langevin, units real).
+ *
+ * Conventions
+ *   - Every call returns 0 on success and a negative AWSEM_E* code on error;
+ *     awsem_last_error() then holds the message (thread local).  Parse and
+ *     topology errors carry the reference's own error texts.
+ *   - Host arrays of positions, velocities and forces are [natoms][3] doubles
+ *     in the caller's atom order (the data file's atom-id order).
+ *   - energies[21]: [0..17] the reference fix's energy[] vector
+ *     (fix_backbone.h:330-332: total, chain, shake, chi, rama, excluded,
+ *     dssp, p_ap, water, burial, helix, amh-go, frag_mem, vec_fm,
+ *     contact_restraints, membrane, ssb, dh), [18] pair vexcluded,
+ *     [19] harmonic bonds, [20] kinetic energy.  kcal/mol.
+ *   - A handle is used by one host thread at a time; distinct handles are
+ *     independent.  Each handle owns one CUDA stream on its device.
+ */
+#ifndef AWSEM_GPU_H
+#define AWSEM_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define AWSEM_OK 0
+#define AWSEM_EINVAL -1   /* bad argument */
+#define AWSEM_EPARSE -2   /* input file or parameter error */
+#define AWSEM_ECUDA -3    /* CUDA runtime error */
+#define AWSEM_ESTATE -4   /* invalid state (e.g. pair-list overflow detected) */
+#define AWSEM_ENOMEM -5   /* device memory budget exceeded */
+
+/* arithmetic forms */
+#define AWSEM_FP64 0   /* plain form: FP64 throughout */
+#define AWSEM_MIXED 1  /* FP32 pair geometry / Gaussians / switches, FP64 accumulation and integration */
+
+/* term groups for awsem_compute */
+#define AWSEM_TERMS_FIX 1   /* fix backbone terms */
+#define AWSEM_TERMS_PAIR 2  /* pair vexcluded */
+#define AWSEM_TERMS_BOND 4  /* bond_style harmonic */
+#define AWSEM_TERMS_ALL 7
+
+typedef struct awsem_system awsem_system;
+
+typedef struct awsem_run_params {
+  double dt;                 /* fs (units real) */
+  int langevin;              /* 0: fix nve only; 1: fix nve + fix langevin */
+  double t_start, t_stop;    /* K, linear ramp over the run */
+  double damp;               /* fs */
+  unsigned long long seed;   /* Langevin stream seed */
+  double skin;               /* pair-list skin, A (applied at the next rebuild) */
+  int neigh_every;           /* forced rebuild period in steps; 0: displacement check only */
+} awsem_run_params;
+
+const char *awsem_last_error(void);
+int awsem_version(void);
+
+/* Build a system from a run directory laid out like a reference run:
+ * coefficient file (fix_backbone_coeff.data sections), sequence file, the
+ * tables read from the working directory (anti_HB, anti_NHB, para_HB,
+ * para_one, anti_one, ssweight, gamma.dat, burial_gamma.dat), fragment
+ * memories (.mem + .gro + gamma file) and an atom_style awsemmd data file.
+ * pair_style: "p cut_short cut_long"; pair_coeffs: ';'-separated
+ * "itype jtype lambda [cut_short cut_long]" records (pair_style vexcluded).
+ * Replaces the FixBackbone constructor (src/fix_backbone.cpp:86-1072),
+ * PairExcludedVolume::settings/coeff (src/pair_excluded_volume.cpp:175-232)
+ * and read_data. */
+int awsem_create_from_files(const char *workdir, const char *data_file, const char *coeff_file,
+                            const char *seq_file, const char *pair_style, const char *pair_coeffs,
+                            int precision, int device, awsem_system **out);
+void awsem_destroy(awsem_system *sys);
+
+int awsem_natoms(const awsem_system *sys);
+int awsem_nres(const awsem_system *sys);
+
+/* Drop-in force call: forces at the caller's positions x are ADDED into f
+ * (the fix adds into atom->f during pre_force), energies (may be NULL) are
+ * written.  `terms` selects AWSEM_TERMS_* groups.  The residue pair list is
+ * kept between calls and rebuilt when the displacement check requires it.
+ * Replaces FixBackbone::pre_force (src/fix_backbone.cpp:8181) and, with
+ * AWSEM_TERMS_PAIR, PairExcludedVolume::compute. */
+int awsem_compute(awsem_system *sys, long long step, const double *x, double *f, double *energies, int terms);
+
+/* Device-resident state (caller atom order). */
+int awsem_set_state(awsem_system *sys, const double *x, const double *v);
+int awsem_get_state(awsem_system *sys, double *x, double *v);
+
+/* `run nsteps`: velocity Verlet (+ Langevin) with every force evaluated on
+ * the GPU; the step sequence is captured in a CUDA graph.  thermo (may be
+ * NULL) receives (nsteps+1) rows of [fix total, vexcluded, bonds, kinetic].
+ * The first row is the setup evaluation at the current step counter. */
+int awsem_run(awsem_system *sys, long long nsteps, const awsem_run_params *rp, double *thermo);
+
+/* Device time (ms) of the last awsem_run, from CUDA events recorded on the
+ * engine's stream around the launched step graphs. */
+double awsem_last_run_ms(const awsem_system *sys);
+
+/* Energies and total forces (incl. Langevin) of the last evaluation. */
+int awsem_energies(awsem_system *sys, double *energies);
+int awsem_forces(awsem_system *sys, double *f);
+
+/* Per-residue pair-pass intermediates of the last evaluation, [nres][8]:
+ * rho_water, rho_helix, xi_water, xi1_helix, xi2_helix, burial coefficient,
+ * sigma_water, sigma_helix. */
+int awsem_residue_arrays(awsem_system *sys, double *out);
+
+/* Pair-list statistics: builds so far, current list radius (A), largest
+ * neighbour count, overflow marker (0 when the list never overflowed). */
+int awsem_neighbor_stats(awsem_system *sys, int *nbuilds, double *radius, int *max_count, int *overflow);
+
+/* Current MD step counter. */
+long long awsem_step(const awsem_system *sys);
+
+/* Kernels of one MD step, in launch order (names for awsem_profile_step). */
+#define AWSEM_NKERNELS 10
+const char *awsem_kernel_name(int k);
+
+/* Average device time (ms) of each kernel of one MD step, measured with CUDA
+ * events on the engine's stream(s) over `reps` steps launched one kernel at
+ * a time (the step advances; no graph).  Uses the last run's parameters. */
+int awsem_profile_step(awsem_system *sys, int reps, double *ms);
+
+/* Sizes behind the roofline's algorithmic-byte counts:
+ * info[0] residues, [1] atoms, [2] fragment-memory records (4 distances
+ * each), [3] bytes per stored distance (8 FP64, 4 mixed), [4] rows per
+ * residue, [5] pair-list capacity, [6] pair-list entries of the last build,
+ * [7] non-uniform memory coefficients stored (0/1). */
+int awsem_model_info(awsem_system *sys, long long *info);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,102 @@
+"""Regenerate the golden vectors of tests/golden/*.npz from the reference.
+
+The reference FixBackbone / PairExcludedVolume sources are compiled in place
+against the LAMMPS-API shim (``make -C oracle ref``) and run on three inputs:
+
+* ``c0``    -- the 100-residue random-coil chain of benchmark configuration 0
+               (generated by awsemmd_b200.synth, seed 0);
+* ``sheet`` -- a three-chain beta-sheet system that exercises the hydrogen-
+               bond, P_AP and burial branches (synth.sheet_system, seed 7);
+* ``r1r69`` -- the reference's own 1R69 example inputs (63 residues, native
+               coordinates, one 63-residue fragment memory), copied verbatim
+               into tests/golden/r1r69 from
+               examples/examples_new/1R69_single_memory, with the default
+               parameter set plus a [Fragment_Memory] section.
+
+For each it stores the inputs' hash, the step-0 forces and energies, the
+per-residue pair-pass intermediates and a 20-step Langevin trajectory
+(x, v and per-step thermo rows).  Run from the repository root with the
+reference tree present:  python tests/golden/make_golden.py
+"""
+from __future__ import annotations
+
+import hashlib
+import os
+import shutil
+import sys
+import tempfile
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+from awsemmd_b200 import synth  # noqa: E402
+
+GOLDEN = os.path.dirname(os.path.abspath(__file__))
+RUN = dict(nsteps=20, dt=2.0, t_start=300.0, t_stop=300.0, damp=500.0, seed=12345)
+
+
+def dir_hash(d: str) -> str:
+    h = hashlib.sha256()
+    for root, _, files in sorted(os.walk(d)):
+        for f in sorted(files):
+            if f in ("energy.log", "timer.log"):
+                continue
+            p = os.path.join(root, f)
+            h.update(os.path.relpath(p, d).encode())
+            with open(p, "rb") as fh:
+                h.update(fh.read())
+    return h.hexdigest()
+
+
+def write_case(name: str, outdir: str) -> dict:
+    if name == "c0":
+        return synth.write_system(synth.config_system(0), outdir)
+    if name == "sheet":
+        return synth.write_system(synth.sheet_system(), outdir)
+    if name == "r1r69":
+        src = os.path.join(GOLDEN, "r1r69")
+        os.makedirs(outdir, exist_ok=True)
+        for f in os.listdir(src):
+            shutil.copy(os.path.join(src, f), os.path.join(outdir, f))
+            os.chmod(os.path.join(outdir, f), 0o644)
+        for t in synth.PARAM_TABLES:
+            shutil.copy(os.path.join(synth.PARAM_DIR, t), os.path.join(outdir, t))
+        with open(os.path.join(outdir, "fix_backbone_coeff.data"), "w") as fh:
+            fh.write(synth.coeff_text(mem_file="fragsLAMW.mem.single", gamma_file="seq.gamma"))
+        return {"workdir": outdir, "data": "data.1r69", "coeff": "fix_backbone_coeff.data", "seq": "extended.seq",
+                "pair_style": synth.PAIR_STYLE, "pair_coeffs": ";".join(synth.PAIR_COEFFS)}
+    raise KeyError(name)
+
+
+CASES = ["c0", "sheet", "r1r69"]
+
+
+def main():
+    import ref
+
+    for name in CASES:
+        with tempfile.TemporaryDirectory() as tmp:
+            files = write_case(name, os.path.join(tmp, name))
+            h = dir_hash(files["workdir"])
+            r = ref.RefSystem(files)
+            x0, v0 = r.get("x"), r.get("v")
+            f0 = r.compute(0)
+            e0 = r.energies()
+            nres = int(open(os.path.join(files["workdir"], files["seq"])).read().replace("\n", "").__len__())
+            res0 = r.residue_arrays(nres)
+            thermo = r.run(RUN["nsteps"], dt=RUN["dt"], langevin=True, t_start=RUN["t_start"], t_stop=RUN["t_stop"],
+                           damp=RUN["damp"], seed=RUN["seed"])
+            xN, vN = r.get("x"), r.get("v")
+            r.close()
+            np.savez_compressed(os.path.join(GOLDEN, f"{name}.npz"), inputs_sha256=np.array(h), x0=x0, v0=v0,
+                                f0=f0, e0=e0, res0=res0, thermo=thermo, xN=xN, vN=vN,
+                                run=np.array([RUN["nsteps"], RUN["dt"], RUN["t_start"], RUN["t_stop"], RUN["damp"],
+                                              RUN["seed"]], dtype=np.float64))
+            print(name, "natoms", len(x0), "E_total", e0[0], "hash", h[:12])
+
+
+if __name__ == "__main__":
+    main()
