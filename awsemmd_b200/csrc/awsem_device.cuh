@@ -89,6 +89,23 @@ template <typename R> struct DevSys {
   unsigned long long *facc;      // [n_res*3][3] fixed-point forces
 };
 
+// The same system viewed with FP64 geometry (the storage is type independent).
+template <typename R> __device__ __forceinline__ DevSys<double> widen(const DevSys<R> &s)
+{
+  DevSys<double> d;
+  d.n_res = s.n_res;
+  d.res_type = s.res_type;
+  d.res_flags = s.res_flags;
+  d.res_chain = s.res_chain;
+  d.chain_start = s.chain_start;
+  d.chain_end = s.chain_end;
+  d.aps = s.aps;
+  d.tables = s.tables;
+  d.pos = s.pos;
+  d.facc = s.facc;
+  return d;
+}
+
 template <typename R> __device__ __forceinline__ V3<double> bead(const DevSys<R> &s, int r, int b)
 {
   double4 q = s.pos[(size_t) r * N_BEADS + b];

@@ -68,17 +68,33 @@ constexpr double BOLTZ = 0.0019872067;
 class EngineBase {
  public:
   virtual ~EngineBase() {}
-  SystemInput in;
+  std::vector<std::unique_ptr<SystemInput>> reps;  // replicas as loaded (until commit)
+  std::vector<unsigned long long> seeds;           // per-replica Langevin seed (0: the run's seed)
+  Batch in;                                        // the committed batch
+  bool committed = false;
   int device = 0;
   long long step = 0;
+  int n_sys() const { return in.n_sys; }
+  int rep_atoms(int r) const { return in.sys_atom_begin[r + 1] - in.sys_atom_begin[r]; }
+  int rep_res(int r) const { return in.sys_res_end[r] - in.sys_res_begin[r]; }
+  void commit()
+  {
+    std::vector<const SystemInput *> v;
+    for (auto &p : reps) v.push_back(p.get());
+    assemble_batch(v, in);
+    seeds.resize(in.n_sys, 0ull);
+    setup();
+    committed = true;
+    reps.clear();  // host copies are no longer needed: state lives on the device
+  }
   virtual void setup() = 0;
   virtual void compute(long long step, const double *x_ext, double *f_ext, double *energies, int groups) = 0;
-  virtual void set_state(const double *x_ext, const double *v_ext) = 0;
-  virtual void get_state(double *x_ext, double *v_ext) = 0;
+  virtual void set_state(int rep, const double *x_ext, const double *v_ext) = 0;
+  virtual void get_state(int rep, double *x_ext, double *v_ext) = 0;
   virtual void run(long long nsteps, const awsem_run_params &rp, double *thermo) = 0;
-  virtual void energies(double *out) = 0;
-  virtual void forces(double *f_ext) = 0;
-  virtual void residue_arrays(double *out) = 0;
+  virtual void energies(int rep, double *out) = 0;
+  virtual void forces(int rep, double *f_ext) = 0;
+  virtual void residue_arrays(int rep, double *out) = 0;
   virtual void nl_stats(int *nbuilds, double *radius, int *maxc, int *overflow) = 0;
   virtual void profile(int reps, double *ms) = 0;
   virtual void model_info(long long *info) = 0;
@@ -107,6 +123,8 @@ template <typename R> class Engine : public EngineBase {
   DBuf<int> fm_row;
   DBuf<R> fm_rf, fm_coef;
   DBuf<double> thermo_rows;
+  DBuf<int> res_sys, sys_begin, sys_end;
+  DBuf<unsigned long long> sys_seed;
   int cap = 0;
   int groups_all = dev::G_FIX | dev::G_PAIR | dev::G_BOND;
   double skin = 2.0;
@@ -182,6 +200,10 @@ template <typename R> class Engine : public EngineBase {
     a.fm_uniform = in.fm.uniform_coef;
     a.groups = groups;
     a.step = dstep.p;
+    a.res_sys = res_sys.p;
+    a.sys_begin = sys_begin.p;
+    a.sys_end = sys_end.p;
+    a.sys_seed = sys_seed.p;
     return a;
   }
 
@@ -194,6 +216,11 @@ template <typename R> class Engine : public EngineBase {
     CK(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
     const Topology &t = in.top;
     int nn = n(), na = natoms();
+    res_sys.upload(in.res_sys, s0);
+    sys_begin.upload(in.sys_res_begin, s0);
+    sys_end.upload(in.sys_res_end, s0);
+    sys_seed.alloc(std::max(in.n_sys, 1));
+    energy.alloc((size_t) E_SLOTS * std::max(in.n_sys, 1));
     res_type.upload(t.res_type, s0);
     res_flags.upload(t.res_flags, s0);
     res_chain.upload(t.res_chain, s0);
@@ -214,7 +241,6 @@ template <typename R> class Engine : public EngineBase {
     work.zero(s0);
     e_res.alloc((size_t) E_SLOTS * nn);
     e_res.zero(s0);
-    energy.alloc(E_SLOTS);
     pos.alloc((size_t) dev::N_BEADS * nn);
     cb_build.alloc(nn);
     cb_build.zero(s0);
@@ -324,7 +350,7 @@ template <typename R> class Engine : public EngineBase {
     int tb = 128, nb = (nn + tb - 1) / tb, wb = (nn * 32 + tb - 1) / tb;
     dev::k_prepare<R><<<nb, tb, 0, s>>>(a, p);
     dev::k_nl_decide<<<1, 1, 0, s>>>(nl.p, force ? 1 : 0, advance ? dstep.p : nullptr);
-    dev::k_nl_build<R><<<wb, tb, 0, s>>>(a, 0, nn);
+    dev::k_nl_build<R><<<wb, tb, 0, s>>>(a);
   }
 
   // one force evaluation (everything up to the fixed-point force sums)
@@ -361,16 +387,23 @@ template <typename R> class Engine : public EngineBase {
 
   void reduce_energies()
   {
-    dev::k_energy_reduce<<<E_SLOTS, 256, 0, s0>>>(e_res.p, n(), 0, n(), energy.p);
+    dim3 grid(E_SLOTS, n_sys());
+    dev::k_energy_reduce<<<grid, 256, 0, s0>>>(e_res.p, n(), sys_begin.p, sys_end.p, energy.p);
+  }
+
+  void need_single(const char *what)
+  {
+    if (n_sys() != 1) throw std::invalid_argument(std::string(what) + " needs a single-system handle");
   }
 
   void compute(long long st, const double *x_ext, double *f_ext, double *energies_out, int groups) override
   {
-    const Topology &t = in.top;
+    need_single("awsem_compute");
+    const std::vector<int> &ext = in.ext_of[0];
     int na = natoms();
     hx.resize((size_t) 3 * na);
     for (int a = 0; a < na; a++)
-      for (int k = 0; k < 3; k++) hx[3 * a + k] = x_ext[3 * t.ext_of[a] + k];
+      for (int k = 0; k < 3; k++) hx[3 * a + k] = x_ext[3 * ext[a] + k];
     CK(cudaMemcpyAsync(x.p, hx.data(), sizeof(double) * 3 * na, cudaMemcpyHostToDevice, s0));
     CK(cudaMemcpyAsync(dstep.p, &st, sizeof st, cudaMemcpyHostToDevice, s0));
     step = st;
@@ -388,7 +421,7 @@ template <typename R> class Engine : public EngineBase {
     CK(cudaStreamSynchronize(s0));
     check_list();
     for (int at = 0; at < na; at++)
-      for (int k = 0; k < 3; k++) f_ext[3 * t.ext_of[at] + k] += f[3 * at + k];
+      for (int k = 0; k < 3; k++) f_ext[3 * ext[at] + k] += f[3 * at + k];
     if (energies_out) finish_energies(e, energies_out, false);
   }
 
@@ -409,32 +442,40 @@ template <typename R> class Engine : public EngineBase {
                                std::to_string(st.overflow) + "); results of this call are invalid");
   }
 
-  void set_state(const double *x_ext, const double *v_ext) override
+  void check_rep(int rep)
   {
-    const Topology &t = in.top;
-    int na = natoms();
+    if (rep < 0 || rep >= n_sys()) throw std::invalid_argument("replica index out of range");
+  }
+
+  void set_state(int rep, const double *x_ext, const double *v_ext) override
+  {
+    check_rep(rep);
+    const std::vector<int> &ext = in.ext_of[rep];
+    int a0 = in.sys_atom_begin[rep], na = rep_atoms(rep);
+    std::vector<double> bx((size_t) 3 * na), bv((size_t) 3 * na);
     for (int a = 0; a < na; a++)
       for (int k = 0; k < 3; k++) {
-        if (x_ext) in.x[3 * a + k] = x_ext[3 * t.ext_of[a] + k];
-        if (v_ext) in.v[3 * a + k] = v_ext[3 * t.ext_of[a] + k];
+        if (x_ext) bx[3 * a + k] = x_ext[3 * ext[a] + k];
+        if (v_ext) bv[3 * a + k] = v_ext[3 * ext[a] + k];
       }
-    if (x_ext) CK(cudaMemcpyAsync(x.p, in.x.data(), sizeof(double) * 3 * na, cudaMemcpyHostToDevice, s0));
-    if (v_ext) CK(cudaMemcpyAsync(v.p, in.v.data(), sizeof(double) * 3 * na, cudaMemcpyHostToDevice, s0));
+    if (x_ext) CK(cudaMemcpyAsync(x.p + 3 * (size_t) a0, bx.data(), sizeof(double) * 3 * na, cudaMemcpyHostToDevice, s0));
+    if (v_ext) CK(cudaMemcpyAsync(v.p + 3 * (size_t) a0, bv.data(), sizeof(double) * 3 * na, cudaMemcpyHostToDevice, s0));
     CK(cudaStreamSynchronize(s0));
   }
 
-  void get_state(double *x_ext, double *v_ext) override
+  void get_state(int rep, double *x_ext, double *v_ext) override
   {
-    const Topology &t = in.top;
-    int na = natoms();
+    check_rep(rep);
+    const std::vector<int> &ext = in.ext_of[rep];
+    int a0 = in.sys_atom_begin[rep], na = rep_atoms(rep);
     std::vector<double> hx2((size_t) 3 * na), hv2((size_t) 3 * na);
-    CK(cudaMemcpyAsync(hx2.data(), x.p, sizeof(double) * 3 * na, cudaMemcpyDeviceToHost, s0));
-    CK(cudaMemcpyAsync(hv2.data(), v.p, sizeof(double) * 3 * na, cudaMemcpyDeviceToHost, s0));
+    CK(cudaMemcpyAsync(hx2.data(), x.p + 3 * (size_t) a0, sizeof(double) * 3 * na, cudaMemcpyDeviceToHost, s0));
+    CK(cudaMemcpyAsync(hv2.data(), v.p + 3 * (size_t) a0, sizeof(double) * 3 * na, cudaMemcpyDeviceToHost, s0));
     CK(cudaStreamSynchronize(s0));
     for (int a = 0; a < na; a++)
       for (int k = 0; k < 3; k++) {
-        if (x_ext) x_ext[3 * t.ext_of[a] + k] = hx2[3 * a + k];
-        if (v_ext) v_ext[3 * t.ext_of[a] + k] = hv2[3 * a + k];
+        if (x_ext) x_ext[3 * ext[a] + k] = hx2[3 * a + k];
+        if (v_ext) v_ext[3 * ext[a] + k] = hv2[3 * a + k];
       }
   }
 
@@ -444,7 +485,7 @@ template <typename R> class Engine : public EngineBase {
   cudaGraphExec_t graphs[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [thermo][chunk]
   static constexpr int kChunk = 25;
   DBuf<dev::Integrator> d_integ;
-  DBuf<double *> d_thermo_ptr;
+  long long thermo_nrows = 1;
   cudaEvent_t ev_run0 = nullptr, ev_run1 = nullptr;
   double last_run_ms = 0.0;
 
@@ -457,7 +498,9 @@ template <typename R> class Engine : public EngineBase {
     for (int c = 0; c < count; c++) {
       launch_eval(a, true);
       dev::k_finish<R><<<nb, tb, 0, s0>>>(a, d_integ.p, g1.p, g2.p, ftot.p, x.p);
-      if (thermo) dev::k_thermo<<<1, 256, 0, s0>>>(e_res.p, nn, dstep.p, d_integ.p, thermo_rows.p);
+      if (thermo)
+        dev::k_thermo<<<n_sys(), 256, 0, s0>>>(e_res.p, nn, dstep.p, d_integ.p, sys_begin.p, sys_end.p,
+                                               thermo_nrows, thermo_rows.p);
     }
     CK(cudaStreamEndCapture(s0, &graph));
     CK(cudaGraphInstantiate(&exec, graph, 0));
@@ -502,7 +545,7 @@ template <typename R> class Engine : public EngineBase {
         switch (k) {
           case 0: dev::k_prepare<R><<<nb, tb, 0, s0>>>(a, p); break;
           case 1: dev::k_nl_decide<<<1, 1, 0, s0>>>(nl.p, 0, dstep.p); break;
-          case 2: dev::k_nl_build<R><<<wb, tb, 0, s0>>>(a, 0, nn); break;
+          case 2: dev::k_nl_build<R><<<wb, tb, 0, s0>>>(a); break;
           case 3: dev::k_density<R><<<wb, tb, 0, s0>>>(a, p); break;
           case 4: dev::k_residue<R><<<nb, tb, 0, s0>>>(a, p); break;
           case 5: dev::k_water_xi<R><<<wb, tb, 0, s0>>>(a, p); break;
@@ -594,13 +637,18 @@ template <typename R> class Engine : public EngineBase {
       set_nl_field(&dev::NLState::every, neigh_every);
     }
     upload_integrator(make_integrator(rp, step, step + nsteps));
+    // Langevin seed of each replica: its own when set, else the run's
+    std::vector<unsigned long long> sd(n_sys());
+    for (int k = 0; k < n_sys(); k++) sd[k] = seeds[k] ? seeds[k] : rp.seed;
+    CK(cudaMemcpyAsync(sys_seed.p, sd.data(), sizeof(unsigned long long) * sd.size(), cudaMemcpyHostToDevice, s0));
     long long pre = step - 1;  // the setup evaluation advances the counter to `step`
     CK(cudaMemcpyAsync(dstep.p, &pre, sizeof pre, cudaMemcpyHostToDevice, s0));
     bool want_thermo = thermo != nullptr;
     int tv = want_thermo ? 1 : 0;
     if (want_thermo) {
-      // thermo graphs bake the row buffer's address: rebuilt per run
-      thermo_rows.alloc((size_t) 4 * (nsteps + 1));
+      // thermo graphs bake the row buffer's address and row count: rebuilt per run
+      thermo_nrows = nsteps + 1;
+      thermo_rows.alloc((size_t) 4 * (nsteps + 1) * n_sys());
       for (auto &g : graphs[1])
         if (g) {
           cudaGraphExecDestroy(g);
@@ -632,7 +680,7 @@ template <typename R> class Engine : public EngineBase {
     step += nsteps;
     check_list();
     if (want_thermo)
-      CK(cudaMemcpy(thermo, thermo_rows.p, sizeof(double) * 4 * (nsteps + 1), cudaMemcpyDeviceToHost));
+      CK(cudaMemcpy(thermo, thermo_rows.p, sizeof(double) * 4 * (nsteps + 1) * n_sys(), cudaMemcpyDeviceToHost));
   }
 
   template <typename F> void set_nl_field(F dev::NLState::*field, F value)
@@ -644,36 +692,39 @@ template <typename R> class Engine : public EngineBase {
     CK(cudaMemcpyAsync(nl.p, &st, sizeof st, cudaMemcpyHostToDevice, s0));
   }
 
-  void energies(double *out) override
+  void energies(int rep, double *out) override
   {
+    check_rep(rep);
     reduce_energies();
     double e[E_SLOTS];
-    CK(cudaMemcpyAsync(e, energy.p, sizeof e, cudaMemcpyDeviceToHost, s0));
+    CK(cudaMemcpyAsync(e, energy.p + (size_t) rep * E_SLOTS, sizeof e, cudaMemcpyDeviceToHost, s0));
     CK(cudaStreamSynchronize(s0));
     finish_energies(e, out, true);
   }
 
-  void forces(double *f_ext) override
+  void forces(int rep, double *f_ext) override
   {
-    const Topology &t = in.top;
-    int na = natoms();
+    check_rep(rep);
+    const std::vector<int> &ext = in.ext_of[rep];
+    int a0 = in.sys_atom_begin[rep], na = rep_atoms(rep);
     std::vector<double> f((size_t) 3 * na);
-    CK(cudaMemcpyAsync(f.data(), ftot.p, sizeof(double) * 3 * na, cudaMemcpyDeviceToHost, s0));
+    CK(cudaMemcpyAsync(f.data(), ftot.p + 3 * (size_t) a0, sizeof(double) * 3 * na, cudaMemcpyDeviceToHost, s0));
     CK(cudaStreamSynchronize(s0));
     for (int at = 0; at < na; at++)
-      for (int k = 0; k < 3; k++) f_ext[3 * t.ext_of[at] + k] = f[3 * at + k];
+      for (int k = 0; k < 3; k++) f_ext[3 * ext[at] + k] = f[3 * at + k];
   }
 
-  void residue_arrays(double *out) override
+  void residue_arrays(int rep, double *out) override
   {
-    int nn = n();
+    check_rep(rep);
+    int nn = n(), r0 = in.sys_res_begin[rep], nr = rep_res(rep);
     std::vector<double> w((size_t) 10 * nn);
     CK(cudaMemcpyAsync(w.data(), work.p, sizeof(double) * 10 * nn, cudaMemcpyDeviceToHost, s0));
     CK(cudaStreamSynchronize(s0));
     // device order: rho_w rho_h sig_w sigp_w sig_h sigp_h xi_w xi1 xi2 bur
     const int src[8] = {0, 1, 6, 7, 8, 9, 2, 4};
-    for (int r = 0; r < nn; r++)
-      for (int c = 0; c < 8; c++) out[8 * r + c] = w[(size_t) src[c] * nn + r];
+    for (int r = 0; r < nr; r++)
+      for (int c = 0; c < 8; c++) out[8 * r + c] = w[(size_t) src[c] * nn + r0 + r];
   }
 
   void nl_stats(int *nbuilds, double *radius, int *maxc, int *overflow) override
@@ -694,6 +745,7 @@ using namespace awsem;
 
 struct awsem_system {
   std::unique_ptr<EngineBase> eng;
+  std::unique_ptr<SharedForceField> shared;  // force field of array-described replicas
 };
 
 template <typename Fn> static int guarded(Fn fn)
@@ -726,46 +778,149 @@ const char *awsem_last_error(void) { return g_last_error.c_str(); }
 
 int awsem_version(void) { return 1; }
 
-int awsem_create_from_files(const char *workdir, const char *data_file, const char *coeff_file, const char *seq_file,
-                            const char *pair_style, const char *pair_coeffs, int precision, int device,
-                            awsem_system **out)
+int awsem_batch_create(int precision, int device, awsem_system **out)
 {
-  if (!out || !data_file || !coeff_file || !seq_file || !pair_style) {
-    g_last_error = "awsem_create_from_files: null argument";
-    return AWSEM_EINVAL;
-  }
-  if (precision != AWSEM_FP64 && precision != AWSEM_MIXED) {
-    g_last_error = "awsem_create_from_files: precision must be AWSEM_FP64 or AWSEM_MIXED";
+  if (!out) {
+    g_last_error = "awsem_batch_create: null argument";
     return AWSEM_EINVAL;
   }
   *out = nullptr;
-  auto *sys = new awsem_system();
-  int rc = guarded([&] {
-    if (precision == AWSEM_FP64) sys->eng.reset(new Engine<double>());
-    else sys->eng.reset(new Engine<float>());
-    sys->eng->device = device;
-    load_system_dir(workdir ? workdir : "", data_file, coeff_file, seq_file, pair_style, pair_coeffs ? pair_coeffs : "",
-                    sys->eng->in);
-    sys->eng->setup();
-  });
-  if (rc != AWSEM_OK) {
-    delete sys;
-    return rc;
+  if (precision != AWSEM_FP64 && precision != AWSEM_MIXED) {
+    g_last_error = "precision must be AWSEM_FP64 or AWSEM_MIXED";
+    return AWSEM_EINVAL;
   }
+  auto *sys = new awsem_system();
+  if (precision == AWSEM_FP64) sys->eng.reset(new Engine<double>());
+  else sys->eng.reset(new Engine<float>());
+  sys->eng->device = device;
   *out = sys;
   return AWSEM_OK;
 }
 
+int awsem_batch_add_files(awsem_system *sys, const char *workdir, const char *data_file, const char *coeff_file,
+                          const char *seq_file, const char *pair_style, const char *pair_coeffs,
+                          unsigned long long seed, int *replica)
+{
+  if (!sys || !data_file || !coeff_file || !seq_file || !pair_style) {
+    g_last_error = "awsem_batch_add_files: null argument";
+    return AWSEM_EINVAL;
+  }
+  if (sys->eng->committed) {
+    g_last_error = "awsem_batch_add_files: the batch is already committed";
+    return AWSEM_ESTATE;
+  }
+  return guarded([&] {
+    std::unique_ptr<SystemInput> S(new SystemInput());
+    load_system_dir(workdir ? workdir : "", data_file, coeff_file, seq_file, pair_style,
+                    pair_coeffs ? pair_coeffs : "", *S);
+    sys->eng->reps.push_back(std::move(S));
+    sys->eng->seeds.push_back(seed);
+    if (replica) *replica = (int) sys->eng->reps.size() - 1;
+  });
+}
+
+int awsem_batch_set_forcefield(awsem_system *sys, const char *workdir, const char *coeff_file,
+                               const char *pair_style, const char *pair_coeffs)
+{
+  if (!sys || !coeff_file || !pair_style) {
+    g_last_error = "awsem_batch_set_forcefield: null argument";
+    return AWSEM_EINVAL;
+  }
+  return guarded([&] {
+    sys->shared.reset(new SharedForceField());
+    load_shared_forcefield(workdir ? workdir : "", coeff_file, pair_style, pair_coeffs ? pair_coeffs : "",
+                           *sys->shared);
+  });
+}
+
+int awsem_batch_add_replica(awsem_system *sys, const awsem_replica_desc *d, int *replica)
+{
+  if (!sys || !d) {
+    g_last_error = "awsem_batch_add_replica: null argument";
+    return AWSEM_EINVAL;
+  }
+  if (!sys->shared) {
+    g_last_error = "awsem_batch_add_replica: call awsem_batch_set_forcefield first";
+    return AWSEM_ESTATE;
+  }
+  if (sys->eng->committed) {
+    g_last_error = "awsem_batch_add_replica: the batch is already committed";
+    return AWSEM_ESTATE;
+  }
+  return guarded([&] {
+    ReplicaArrays ra{d->n_res, d->n_chains, d->chain_len, d->seq, d->ssweight, d->x, d->v, d->n_mem,
+                     d->mem_pos, d->mem_len, d->mem_weight, d->mem_seq, d->mem_ca, d->mem_cb};
+    std::unique_ptr<SystemInput> S(new SystemInput());
+    load_system_arrays(*sys->shared, ra, *S);
+    sys->eng->reps.push_back(std::move(S));
+    sys->eng->seeds.push_back(d->seed);
+    if (replica) *replica = (int) sys->eng->reps.size() - 1;
+  });
+}
+
+int awsem_batch_commit(awsem_system *sys)
+{
+  if (!sys) return AWSEM_EINVAL;
+  if (sys->eng->committed) {
+    g_last_error = "awsem_batch_commit: already committed";
+    return AWSEM_ESTATE;
+  }
+  if (sys->eng->reps.empty()) {
+    g_last_error = "awsem_batch_commit: no replicas";
+    return AWSEM_EINVAL;
+  }
+  return guarded([&] {
+    std::vector<unsigned long long> sd = sys->eng->seeds;
+    sys->eng->commit();
+    sys->eng->seeds = sd;
+  });
+}
+
+int awsem_create_from_files(const char *workdir, const char *data_file, const char *coeff_file, const char *seq_file,
+                            const char *pair_style, const char *pair_coeffs, int precision, int device,
+                            awsem_system **out)
+{
+  int rc = awsem_batch_create(precision, device, out);
+  if (rc != AWSEM_OK) return rc;
+  rc = awsem_batch_add_files(*out, workdir, data_file, coeff_file, seq_file, pair_style, pair_coeffs, 0ull, nullptr);
+  if (rc == AWSEM_OK) rc = awsem_batch_commit(*out);
+  if (rc != AWSEM_OK) {
+    std::string msg = g_last_error;
+    delete *out;
+    *out = nullptr;
+    g_last_error = msg;
+  }
+  return rc;
+}
+
 void awsem_destroy(awsem_system *sys) { delete sys; }
 
-int awsem_natoms(const awsem_system *sys) { return sys ? sys->eng->in.top.n_atoms : 0; }
-int awsem_nres(const awsem_system *sys) { return sys ? sys->eng->in.top.n_res : 0; }
+static bool ready(const awsem_system *sys)
+{
+  if (!sys || !sys->eng->committed) {
+    g_last_error = "handle is null or not committed";
+    return false;
+  }
+  return true;
+}
+
+int awsem_natoms(const awsem_system *sys) { return ready(sys) ? sys->eng->in.top.n_atoms : 0; }
+int awsem_nres(const awsem_system *sys) { return ready(sys) ? sys->eng->in.top.n_res : 0; }
+int awsem_nreplicas(const awsem_system *sys) { return ready(sys) ? sys->eng->in.n_sys : 0; }
+int awsem_replica_natoms(const awsem_system *sys, int r)
+{
+  return ready(sys) && r >= 0 && r < sys->eng->in.n_sys ? sys->eng->rep_atoms(r) : 0;
+}
+int awsem_replica_nres(const awsem_system *sys, int r)
+{
+  return ready(sys) && r >= 0 && r < sys->eng->in.n_sys ? sys->eng->rep_res(r) : 0;
+}
 long long awsem_step(const awsem_system *sys) { return sys ? sys->eng->step : 0; }
 
 int awsem_compute(awsem_system *sys, long long step, const double *x, double *f, double *energies, int terms)
 {
-  if (!sys || !x || !f) {
-    g_last_error = "awsem_compute: null argument";
+  if (!ready(sys) || !x || !f) {
+    g_last_error = "awsem_compute: null argument or uncommitted handle";
     return AWSEM_EINVAL;
   }
   if (terms <= 0 || terms > AWSEM_TERMS_ALL) {
@@ -775,22 +930,39 @@ int awsem_compute(awsem_system *sys, long long step, const double *x, double *f,
   return guarded([&] { sys->eng->compute(step, x, f, energies, terms); });
 }
 
-int awsem_set_state(awsem_system *sys, const double *x, const double *v)
+int awsem_replica_set_state(awsem_system *sys, int r, const double *x, const double *v)
 {
-  if (!sys) return AWSEM_EINVAL;
-  return guarded([&] { sys->eng->set_state(x, v); });
+  if (!ready(sys)) return AWSEM_EINVAL;
+  return guarded([&] { sys->eng->set_state(r, x, v); });
 }
 
-int awsem_get_state(awsem_system *sys, double *x, double *v)
+int awsem_replica_get_state(awsem_system *sys, int r, double *x, double *v)
 {
-  if (!sys) return AWSEM_EINVAL;
-  return guarded([&] { sys->eng->get_state(x, v); });
+  if (!ready(sys)) return AWSEM_EINVAL;
+  return guarded([&] { sys->eng->get_state(r, x, v); });
 }
+
+int awsem_replica_energies(awsem_system *sys, int r, double *energies)
+{
+  if (!ready(sys) || !energies) return AWSEM_EINVAL;
+  return guarded([&] { sys->eng->energies(r, energies); });
+}
+
+int awsem_replica_forces(awsem_system *sys, int r, double *f)
+{
+  if (!ready(sys) || !f) return AWSEM_EINVAL;
+  return guarded([&] { sys->eng->forces(r, f); });
+}
+
+int awsem_set_state(awsem_system *sys, const double *x, const double *v) { return awsem_replica_set_state(sys, 0, x, v); }
+int awsem_get_state(awsem_system *sys, double *x, double *v) { return awsem_replica_get_state(sys, 0, x, v); }
+int awsem_energies(awsem_system *sys, double *energies) { return awsem_replica_energies(sys, 0, energies); }
+int awsem_forces(awsem_system *sys, double *f) { return awsem_replica_forces(sys, 0, f); }
 
 int awsem_run(awsem_system *sys, long long nsteps, const awsem_run_params *rp, double *thermo)
 {
-  if (!sys || !rp) {
-    g_last_error = "awsem_run: null argument";
+  if (!ready(sys) || !rp) {
+    g_last_error = "awsem_run: null argument or uncommitted handle";
     return AWSEM_EINVAL;
   }
   if (rp->dt <= 0 || rp->damp <= 0 || (rp->langevin && (rp->t_start < 0 || rp->t_stop < 0))) {
@@ -800,27 +972,15 @@ int awsem_run(awsem_system *sys, long long nsteps, const awsem_run_params *rp, d
   return guarded([&] { sys->eng->run(nsteps, *rp, thermo); });
 }
 
-int awsem_energies(awsem_system *sys, double *energies)
-{
-  if (!sys || !energies) return AWSEM_EINVAL;
-  return guarded([&] { sys->eng->energies(energies); });
-}
-
-int awsem_forces(awsem_system *sys, double *f)
-{
-  if (!sys || !f) return AWSEM_EINVAL;
-  return guarded([&] { sys->eng->forces(f); });
-}
-
 int awsem_residue_arrays(awsem_system *sys, double *out)
 {
-  if (!sys || !out) return AWSEM_EINVAL;
-  return guarded([&] { sys->eng->residue_arrays(out); });
+  if (!ready(sys) || !out) return AWSEM_EINVAL;
+  return guarded([&] { sys->eng->residue_arrays(0, out); });
 }
 
 int awsem_neighbor_stats(awsem_system *sys, int *nbuilds, double *radius, int *max_count, int *overflow)
 {
-  if (!sys) return AWSEM_EINVAL;
+  if (!ready(sys)) return AWSEM_EINVAL;
   return guarded([&] { sys->eng->nl_stats(nbuilds, radius, max_count, overflow); });
 }
 
@@ -830,13 +990,13 @@ const char *awsem_kernel_name(int k) { return (k >= 0 && k < AWSEM_NKERNELS) ? k
 
 int awsem_profile_step(awsem_system *sys, int reps, double *ms)
 {
-  if (!sys || !ms) return AWSEM_EINVAL;
+  if (!ready(sys) || !ms) return AWSEM_EINVAL;
   return guarded([&] { sys->eng->profile(reps, ms); });
 }
 
 int awsem_model_info(awsem_system *sys, long long *info)
 {
-  if (!sys || !info) return AWSEM_EINVAL;
+  if (!ready(sys) || !info) return AWSEM_EINVAL;
   return guarded([&] { sys->eng->model_info(info); });
 }
 

@@ -66,6 +66,9 @@ template <typename R> struct StepArgs {
   double fm_uniform;
   int groups;        // AWSEM_TERMS_* bits: 1 fix backbone, 2 pair vexcluded, 4 bonds
   long long *step;   // device step counter (advanced by k_nl_decide)
+  // replicas: residue -> replica, replica residue ranges, Langevin seeds
+  const int *res_sys, *sys_begin, *sys_end;
+  const unsigned long long *sys_seed;
 };
 
 enum Group { G_FIX = 1, G_PAIR = 2, G_BOND = 4 };
@@ -171,13 +174,16 @@ template <typename R> __device__ __forceinline__ V3<double> contact(const DevSys
 }
 
 // Full residue pair list (both directions) over contact beads within r_list,
-// written in ascending j.  Brute force over the system, one warp per residue.
-template <typename R> __global__ void k_nl_build(StepArgs<R> a, int sys_begin, int sys_end)
+// written in ascending j.  Brute force over the residue's own replica, one
+// warp per residue.
+template <typename R> __global__ void k_nl_build(StepArgs<R> a)
 {
   if (!a.nl->rebuild) return;
   int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-  int i = sys_begin + warp;
-  if (i >= sys_end) return;
+  int i = warp;
+  if (i >= a.s.n_res) return;
+  int rep = a.res_sys[i];
+  const int sys_begin = a.sys_begin[rep], sys_end = a.sys_end[rep];
   const DevSys<R> &s = a.s;
   V3<double> ci = contact(s, i);
   R rl = (R) a.nl->r_list, rl2 = rl * rl;
@@ -215,21 +221,22 @@ template <typename R> __global__ void k_density(StepArgs<R> a, FFParams p)
   int cnt = fix ? a.ncount[i] : 0;
   const int *nb = a.nbr + (size_t) i * a.cap;
   bool water = p.terms & T_WATER, helix = p.terms & T_HELIX;
+  // FP64 in both forms: the densities feed the burial and switching
+  // functions, and the well selection is then the reference's exactly
   for (int k = lane; k < cnt; k += 32) {
     int j = nb[k];
     if (s.res_chain[j] == chi && abs(i - j) <= 1) continue;
-    V3<R> d = diff<R>(ci, contact(s, j));
-    R rsq = norm2(d);
-    if (water && rsq > R(p.w_rmin_sq[0]) && rsq < R(p.w_rmax_sq[0])) {
-      R th, pr;
-      well_theta(m_sqrt(rsq), R(p.w_rmin_th[0]), R(p.w_rmax_th[0]), R(p.water_kappa), R(p.well_rmin[0]),
-                 R(p.well_rmax[0]), th, pr);
-      aw += fix_dens((double) th);
+    V3<double> d = diff<double>(ci, contact(s, j));
+    double rsq = norm2(d);
+    if (water && rsq > p.w_rmin_sq[0] && rsq < p.w_rmax_sq[0]) {
+      double th, pr;
+      well_theta(sqrt(rsq), p.w_rmin_th[0], p.w_rmax_th[0], p.water_kappa, p.well_rmin[0], p.well_rmax[0], th, pr);
+      aw += fix_dens(th);
     }
-    if (helix && rsq > R(p.h_rmin_sq) && rsq < R(p.h_rmax_sq)) {
-      R th, pr;
-      well_theta(m_sqrt(rsq), R(p.h_rmin_th), R(p.h_rmax_th), R(p.helix_kappa), R(p.helix_rmin), R(p.helix_rmax), th, pr);
-      ah += fix_dens((double) th);
+    if (helix && rsq > p.h_rmin_sq && rsq < p.h_rmax_sq) {
+      double th, pr;
+      well_theta(sqrt(rsq), p.h_rmin_th, p.h_rmax_th, p.helix_kappa, p.helix_rmin, p.helix_rmax, th, pr);
+      ah += fix_dens(th);
     }
   }
   aw = warp_sum(aw);
@@ -275,6 +282,10 @@ template <typename R> __global__ void k_residue(StepArgs<R> a, FFParams p)
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   const DevSys<R> &s = a.s;
   if (i >= s.n_res) return;
+  // the per-residue backbone terms (chain, chi, rama, helical pair) are a
+  // small share of the work and some are sums of steep Gaussians: FP64 in
+  // both forms
+  const DevSys<double> sd = widen(s);
   int n = s.n_res, fl = s.res_flags[i];
   double *E = a.e_res;
   const bool fix = a.groups & G_FIX;
@@ -311,17 +322,17 @@ template <typename R> __global__ void k_residue(StepArgs<R> a, FFParams p)
     if (norm2(d) < R(p.helix_cutoff_sq)) {
       double shj, shpj;
       switching(a.rho_h[j], p.helix_kappa_sigma, p.helix_treshold, shj, shpj);
-      eh = (double) helix_pair(s, p, i, j, sh, shp, shj, shpj, x1, x2);
+      eh = (double) helix_pair(sd, p, i, j, sh, shp, shj, shpj, x1, x2);
     }
   }
   a.xi1[i] = x1;
   a.xi2[i] = x2;
   E[(size_t) E_HELIX * n + i] = eh;
   double ec = 0.0, ex = 0.0, er = 0.0;
-  if (fix && (p.terms & T_CHAIN)) ec = (double) chain_term(s, p, i);
+  if (fix && (p.terms & T_CHAIN)) ec = (double) chain_term(sd, p, i);
   bool inner = fix && !(fl & (R_FIRST | R_LAST | R_GLY));
-  if (inner && (p.terms & T_CHI)) ex = (double) chi_term(s, p, i);
-  if (inner && (p.terms & T_RAMA)) er = (double) rama_term(s, p, i);
+  if (inner && (p.terms & T_CHI)) ex = (double) chi_term(sd, p, i);
+  if (inner && (p.terms & T_RAMA)) er = (double) rama_term(sd, p, i);
   E[(size_t) E_CHAIN * n + i] = ec;
   E[(size_t) E_CHI * n + i] = ex;
   E[(size_t) E_RAMA * n + i] = er;
@@ -655,6 +666,7 @@ __global__ void k_finish(StepArgs<R> a, const Integrator *inp, const double *g1,
   const Integrator in = *inp;
   const long long step = *a.step;
   const bool final_kick = step > in.begin, next = step < in.end;
+  const unsigned long long seed = a.sys_seed[a.res_sys[r]];
   double tsqrt = 0.0;
   if (in.langevin) {
     double delta = in.end != in.begin ? (double) (step - in.begin) / (double) (in.end - in.begin) : 0.0;
@@ -669,7 +681,7 @@ __global__ void k_finish(StepArgs<R> a, const Integrator *inp, const double *g1,
     for (int c = 0; c < 3; c++) {
       double f = (double) (long long) fa[c] * F_UNSCALE;
       double v = a.v[3 * at + c];
-      if (in.langevin) f += g1[at] * v + g2[at] * tsqrt * (uniform01(in.seed, step, a.atom_tag[at], c) - 0.5);
+      if (in.langevin) f += g1[at] * v + g2[at] * tsqrt * (uniform01(seed, step, a.atom_tag[at], c) - 0.5);
       if (ftot) ftot[3 * at + c] = f;
       if (final_kick) v += dtfm * f;
       ke += m * v * v;
@@ -694,12 +706,14 @@ template <typename R> __global__ void k_total_force(StepArgs<R> a, double *ftot)
 
 // Thermo row of the current step: [fix total, vexcluded, bonds, kinetic],
 // residue sums in a fixed tree order (one block of 256 threads).
-__global__ void k_thermo(const double *e_res, int n_res, const long long *step, const Integrator *inp, double *rows)
+__global__ void k_thermo(const double *e_res, int n_res, const long long *step, const Integrator *inp,
+                         const int *sys_begin, const int *sys_end, long long nrows, double *rows)
 {
   const long long begin = inp->begin;
+  const int rep = blockIdx.x;
   __shared__ double sh[4][256];
   double acc[4] = {0, 0, 0, 0};
-  for (int r = threadIdx.x; r < n_res; r += blockDim.x) {
+  for (int r = sys_begin[rep] + threadIdx.x; r < sys_end[rep]; r += blockDim.x) {
     double fx = 0.0;
     for (int t = 1; t < E_FIX_TERMS; t++) fx += e_res[(size_t) t * n_res + r];
     acc[0] += fx;
@@ -716,24 +730,25 @@ __global__ void k_thermo(const double *e_res, int n_res, const long long *step, 
   }
   if (threadIdx.x == 0) {
     long long row = *step - begin;
-    for (int c = 0; c < 4; c++) rows[4 * row + c] = sh[c][0];
+    for (int c = 0; c < 4; c++) rows[((size_t) rep * nrows + row) * 4 + c] = sh[c][0];
   }
 }
 
-// Per-term sums over residues [begin, end) in a fixed tree order (one block per term)
-__global__ void k_energy_reduce(const double *e_res, int n_res, int begin, int end, double *out)
+// Per-term sums of each replica's residues in a fixed tree order
+// (block (t, rep) sums energy slot t of replica rep)
+__global__ void k_energy_reduce(const double *e_res, int n_res, const int *sys_begin, const int *sys_end, double *out)
 {
-  int t = blockIdx.x;
+  const int t = blockIdx.x, rep = blockIdx.y;
   __shared__ double sh[256];
   double acc = 0.0;
-  for (int r = begin + threadIdx.x; r < end; r += blockDim.x) acc += e_res[(size_t) t * n_res + r];
+  for (int r = sys_begin[rep] + threadIdx.x; r < sys_end[rep]; r += blockDim.x) acc += e_res[(size_t) t * n_res + r];
   sh[threadIdx.x] = acc;
   __syncthreads();
   for (int w = blockDim.x / 2; w > 0; w >>= 1) {
     if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
     __syncthreads();
   }
-  if (threadIdx.x == 0) out[t] = sh[0];
+  if (threadIdx.x == 0) out[(size_t) rep * E_SLOTS + t] = sh[0];
 }
 
 }  // namespace dev

@@ -668,6 +668,233 @@ void build_fm_table(const ForceField &ff, const Topology &top, const GammaTable 
   if (out.uniform) out.coef.clear();
 }
 
+void load_shared_forcefield(const std::string &dir, const std::string &coeff_file, const std::string &pair_style,
+                            const std::string &pair_coeffs, SharedForceField &out)
+{
+  read_coeff_file(path_in(dir, coeff_file), out.ff);
+  Topology none;  // ssweight is per replica: read the residue-independent tables only
+  FFParams &p = out.ff.p;
+  uint32_t ssw = p.terms & T_SSW;
+  p.terms &= ~T_SSW;
+  read_tables(dir, out.ff, none);
+  p.terms |= ssw;
+  if (p.terms & T_FM) {
+    read_gamma_table(path_in(dir, out.ff.fm_gamma_file), out.gamma);
+    p.fm_min_sep = out.gamma.min_sep();
+    p.fm_max_sep = out.gamma.max_sep();
+    for (int d = 0; d < 64; d++) p.fm_sigma_sq[d] = pow((double) d, 2 * p.fm_sigma_exp);
+  }
+  out.pair_style = pair_style;
+  out.pair_coeffs = pair_coeffs;
+}
+
+void load_system_arrays(const SharedForceField &sf, const ReplicaArrays &ra, SystemInput &S)
+{
+  if (ra.n_res <= 0 || ra.n_chains <= 0 || !ra.chain_len || !ra.seq || !ra.x) fail("replica: empty description");
+  S.ff = sf.ff;
+  Topology &t = S.top;
+  t.seq.assign(ra.seq, ra.seq + ra.n_res);
+  int at = 0;
+  for (int c = 0; c < ra.n_chains; c++) {
+    if (ra.chain_len[c] <= 0) fail("replica: chain lengths must be positive");
+    t.chain_start.push_back(at);
+    at += ra.chain_len[c];
+    t.chain_end.push_back(at - 1);
+  }
+  if (at != ra.n_res) fail("replica: chain lengths do not add up to n_res");
+  t.n_chains = ra.n_chains;
+  t.n_res = ra.n_res;
+  // atoms in data-file order per residue: CA, O, CB/H-beta; ids 1..3n
+  int na = 3 * ra.n_res;
+  std::vector<int> role(na), res(na), mol(na), typ(na), tag(na);
+  for (int r = 0, c = 0; r < ra.n_res; r++) {
+    while (r > t.chain_end[c]) c++;
+    const int roles[3] = {0, 2, 1};
+    for (int k = 0; k < 3; k++) {
+      int a = 3 * r + k;
+      role[a] = roles[k];
+      res[a] = r + 1;
+      mol[a] = c + 1;
+      typ[a] = k == 0 ? 1 : k == 1 ? 3 : (ra.seq[r] == 'G' ? 5 : 4);
+      tag[a] = a + 1;
+    }
+  }
+  build_topology(t, na, role.data(), res.data(), mol.data(), typ.data(), tag.data(), sf.mass, 5);
+  // harmonic bonds of the AWSEM topology: CA-O, CA-CB/HB, CA-CA(+1), O-CA(+1)
+  std::vector<int> bi, bj;
+  std::vector<double> bk, br;
+  auto add = [&](int i, int j, int type) {
+    bi.push_back(i);
+    bj.push_back(j);
+    bk.push_back(sf.bond_k[type]);
+    br.push_back(sf.bond_r0[type]);
+  };
+  for (int r = 0; r < ra.n_res; r++) {
+    add(3 * r, 3 * r + 1, 2);
+    add(3 * r, 3 * r + 2, ra.seq[r] == 'G' ? 5 : 4);
+    if (!(t.res_flags[r] & R_LAST)) {
+      add(3 * r, 3 * (r + 1), 1);
+      add(3 * r + 1, 3 * (r + 1), 3);
+    }
+  }
+  std::vector<int> ext_to_int(na);
+  for (int s = 0; s < t.n_atoms; s++) ext_to_int[t.ext_of[s]] = s;
+  set_bonds(t, (int) bi.size(), bi.data(), bj.data(), bk.data(), br.data(), ext_to_int.data());
+  set_pair_coeffs(t, sf.pair_style, sf.pair_coeffs);
+  // secondary-structure weights of the enabled [SSWeight] columns, in order
+  t.aps.assign((size_t) 12 * ra.n_res, 0.0);
+  if ((S.ff.p.terms & T_SSW) && ra.ssweight) {
+    int ncol = 0;
+    for (int k = 0; k < 12; k++) ncol += S.ff.p.ssweight[k] ? 1 : 0;
+    for (int r = 0; r < ra.n_res; r++)
+      for (int k = 0, c = 0; k < 12; k++)
+        if (S.ff.p.ssweight[k]) t.aps[(size_t) k * ra.n_res + r] = ra.ssweight[(size_t) r * ncol + c++];
+  }
+  // fragment memories
+  if (S.ff.p.terms & T_FM) {
+    S.gamma = sf.gamma;
+    size_t off = 0;
+    for (int m = 0; m < ra.n_mem; m++) {
+      Memory mm;
+      mm.pos = ra.mem_pos[m];
+      mm.len = ra.mem_len[m];
+      mm.weight = ra.mem_weight[m];
+      if (mm.len <= 0 || mm.pos < 0 || mm.pos + mm.len > ra.n_res)
+        fail("Fragment_Memory: Incorrectly defined memory fragment");
+      mm.se.assign(ra.mem_seq + off, ra.mem_seq + off + mm.len);
+      mm.xca.assign(ra.mem_ca + 3 * off, ra.mem_ca + 3 * (off + mm.len));
+      mm.xcb.assign(ra.mem_cb + 3 * off, ra.mem_cb + 3 * (off + mm.len));
+      off += mm.len;
+      S.mems.push_back(std::move(mm));
+    }
+    build_fm_table(S.ff, t, S.gamma, S.mems, S.fm);
+    S.ff.p.fm_nd = S.fm.nd;
+    S.mems.clear();
+    S.mems.shrink_to_fit();
+  }
+  S.x.assign(3 * t.n_atoms, 0.0);
+  S.v.assign(3 * t.n_atoms, 0.0);
+  for (int s = 0; s < t.n_atoms; s++)
+    for (int k = 0; k < 3; k++) {
+      S.x[3 * s + k] = ra.x[3 * t.ext_of[s] + k];
+      if (ra.v) S.v[3 * s + k] = ra.v[3 * t.ext_of[s] + k];
+    }
+}
+
+void assemble_batch(const std::vector<const SystemInput *> &reps, Batch &B)
+{
+  if (reps.empty()) fail("empty batch");
+  const SystemInput &r0 = *reps[0];
+  B = Batch();
+  B.ff = r0.ff;
+  B.n_sys = (int) reps.size();
+  Topology &T = B.top;
+  T.ntypes = r0.top.ntypes;
+  T.ev_p = r0.top.ev_p;
+  T.ev_pref = r0.top.ev_pref;
+  T.ev_cs = r0.top.ev_cs;
+  T.ev_cl = r0.top.ev_cl;
+  int nd = 0;
+  long long nres = 0, nrec = 0;
+  auto same_ff = [](const FFParams &a, const FFParams &b) {
+    FFParams x = a, y = b;  // rows per residue may differ; everything else must match
+    x.fm_nd = y.fm_nd = 0;
+    return memcmp(&x, &y, sizeof x) == 0;
+  };
+  for (auto *r : reps) {
+    if (!same_ff(r->ff.p, r0.ff.p) || r->ff.tables != r0.ff.tables)
+      fail("batch replicas must share one force field (coefficient file and tables)");
+    if (r->top.ntypes != T.ntypes || r->top.ev_p != T.ev_p || r->top.ev_pref != T.ev_pref ||
+        r->top.ev_cs != T.ev_cs || r->top.ev_cl != T.ev_cl)
+      fail("batch replicas must share one pair_style vexcluded setup");
+    nd = std::max(nd, r->fm.nd);
+    nres += r->top.n_res;
+    nrec += r->fm.records();
+  }
+  if (nres > 0x3fffffff || nrec > 0x7fffffffLL) fail("batch too large");
+  int N = (int) nres;
+  T.n_res = N;
+  T.n_atoms = 3 * N;
+  T.aps.assign((size_t) 12 * N, 0.0);
+  B.fm.nd = nd;
+  B.fm.row_start.assign((size_t) N * nd + 1, 0);
+  bool uniform = true;
+  double ucoef = 0.0;
+  bool have = false;
+  for (auto *r : reps)
+    if (r->fm.records() > 0) {
+      if (!r->fm.uniform) uniform = false;
+      else if (!have) {
+        ucoef = r->fm.uniform_coef;
+        have = true;
+      } else if (r->fm.uniform_coef != ucoef) uniform = false;
+    }
+  B.fm.uniform = uniform;
+  B.fm.uniform_coef = ucoef;
+  B.sys_atom_begin.push_back(0);
+  int roff = 0, coff = 0;
+  long long rec_off = 0;
+  for (int k = 0; k < B.n_sys; k++) {
+    const SystemInput &S = *reps[k];
+    const Topology &t = S.top;
+    int n = t.n_res;
+    B.sys_res_begin.push_back(roff);
+    B.sys_res_end.push_back(roff + n);
+    B.sys_atom_begin.push_back(3 * (roff + n));
+    B.ext_of.push_back(t.ext_of);
+    T.seq += t.seq;
+    for (int i = 0; i < n; i++) {
+      T.res_type.push_back(t.res_type[i]);
+      T.res_flags.push_back(t.res_flags[i]);
+      T.res_chain.push_back(t.res_chain[i] + coff);
+      B.res_sys.push_back(k);
+      T.excl_self.push_back(t.excl_self[i]);
+      T.excl_next.push_back(t.excl_next[i]);
+      for (int q = 0; q < 12; q++) T.aps[(size_t) q * N + roff + i] = t.aps[(size_t) q * n + i];
+    }
+    for (int c = 0; c < t.n_chains; c++) {
+      T.chain_start.push_back(t.chain_start[c] + roff);
+      T.chain_end.push_back(t.chain_end[c] + roff);
+    }
+    for (int a = 0; a < t.n_atoms; a++) {
+      T.atom_type.push_back(t.atom_type[a]);
+      T.atom_tag.push_back(t.atom_tag[a]);
+      T.mass.push_back(t.mass[a]);
+    }
+    for (size_t b = 0; b < t.bond_i.size(); b++) {
+      T.bond_i.push_back(t.bond_i[b] + 3 * roff);
+      T.bond_j.push_back(t.bond_j[b] + 3 * roff);
+      T.bond_k.push_back(t.bond_k[b]);
+      T.bond_r0.push_back(t.bond_r0[b]);
+    }
+    B.x.insert(B.x.end(), S.x.begin(), S.x.end());
+    B.v.insert(B.v.end(), S.v.begin(), S.v.end());
+    // fragment-memory rows, re-laid to the batch's rows per residue
+    const FMTable &f = S.fm;
+    for (int i = 0; i < n; i++)
+      for (int d = 0; d < nd; d++) {
+        size_t dst = (size_t) (roff + i) * nd + d;
+        long long cnt = 0, src0 = 0;
+        if (d < f.nd && f.records() > 0) {
+          src0 = f.row_start[(size_t) i * f.nd + d];
+          cnt = f.row_start[(size_t) i * f.nd + d + 1] - src0;
+        }
+        B.fm.row_start[dst] = (int) rec_off;
+        for (long long q = 0; q < cnt; q++) {
+          for (int c = 0; c < 4; c++) B.fm.rf.push_back(f.rf[(size_t) (src0 + q) * 4 + c]);
+          if (!uniform) B.fm.coef.push_back(f.uniform ? f.uniform_coef : f.coef[src0 + q]);
+        }
+        rec_off += cnt;
+      }
+    roff += n;
+    coff += t.n_chains;
+  }
+  B.fm.row_start[(size_t) N * nd] = (int) rec_off;
+  T.n_chains = coff;
+  B.ff.p.fm_nd = nd;
+  if (!(B.ff.p.terms & T_FM)) B.ff.p.fm_nd = 0;
+}
+
 void load_system_dir(const std::string &dir, const std::string &data_file, const std::string &coeff_file,
                      const std::string &seq_file, const std::string &pair_style, const std::string &pair_coeffs,
                      SystemInput &S)

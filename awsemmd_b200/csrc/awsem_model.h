@@ -151,4 +151,53 @@ void load_system_dir(const std::string &dir, const std::string &data_file, const
                      const std::string &seq_file, const std::string &pair_style, const std::string &pair_coeffs,
                      SystemInput &out);
 
+// A batch of independent replicas concatenated for the device: residues,
+// chains and atoms of replica k follow those of replica k-1; chain ids are
+// global so different replicas never count as the same chain.  All replicas
+// share one force field (same coefficient file, tables and pair_style).
+struct Batch {
+  ForceField ff;
+  Topology top;       // concatenated topology (ext_of is per replica, see below)
+  FMTable fm;         // concatenated fragment-memory rows
+  std::vector<double> x, v;
+  std::vector<int> res_sys;              // residue -> replica
+  std::vector<int> sys_res_begin, sys_res_end;    // [n_sys]
+  std::vector<int> sys_atom_begin;       // [n_sys + 1]
+  std::vector<std::vector<int>> ext_of;  // per replica: local internal atom -> caller index
+  int n_sys = 0;
+};
+
+// Concatenate replicas (each already loaded); throws if their force fields differ.
+void assemble_batch(const std::vector<const SystemInput *> &reps, Batch &out);
+
+// Force field shared by replicas given as arrays: coefficient file and the
+// tables of a run directory, the fragment-memory gamma file, pair_style
+// vexcluded settings, and the data-file conventions of the atom types
+// (1 CA, 3 O, 4 CB, 5 H-beta), their masses and the five bond types.
+struct SharedForceField {
+  ForceField ff;
+  GammaTable gamma;
+  std::string pair_style, pair_coeffs;
+  double mass[6] = {0, 27.0, 14.0, 28.0, 60.0, 2.0};
+  double bond_k[6] = {0, 60, 60, 60, 60, 60}, bond_r0[6] = {0, 3.816, 2.40, 2.76, 1.53, 1.09};
+};
+
+void load_shared_forcefield(const std::string &dir, const std::string &coeff_file, const std::string &pair_style,
+                            const std::string &pair_coeffs, SharedForceField &out);
+
+// One replica from arrays (see awsem_replica_desc in awsem_gpu.h).
+struct ReplicaArrays {
+  int n_res, n_chains;
+  const int *chain_len;
+  const char *seq;
+  const double *ssweight;  // [n_res][number of enabled SSWeight columns] or null
+  const double *x, *v;     // [n_res][3 beads: CA, O, CB/HB][3] (data-file order)
+  int n_mem;
+  const int *mem_pos, *mem_len;
+  const double *mem_weight;
+  const char *mem_seq;
+  const double *mem_ca, *mem_cb;
+};
+void load_system_arrays(const SharedForceField &sf, const ReplicaArrays &ra, SystemInput &out);
+
 }  // namespace awsem

@@ -39,6 +39,14 @@ class RunParams(C.Structure):
                 ("damp", C.c_double), ("seed", C.c_ulonglong), ("skin", C.c_double), ("neigh_every", C.c_int)]
 
 
+class ReplicaDesc(C.Structure):
+    _fields_ = [("n_res", C.c_int), ("n_chains", C.c_int), ("chain_len", C.c_void_p), ("seq", C.c_char_p),
+                ("ssweight", C.c_void_p), ("x", C.c_void_p), ("v", C.c_void_p), ("n_mem", C.c_int),
+                ("mem_pos", C.c_void_p), ("mem_len", C.c_void_p), ("mem_weight", C.c_void_p),
+                ("mem_seq", C.c_char_p), ("mem_ca", C.c_void_p), ("mem_cb", C.c_void_p),
+                ("seed", C.c_ulonglong)]
+
+
 class AwsemError(RuntimeError):
     pass
 
@@ -73,6 +81,24 @@ def load_library(path: str = LIB_PATH):
     lib.awsem_residue_arrays.argtypes = [vp, vp]
     lib.awsem_neighbor_stats.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_double), C.POINTER(C.c_int),
                                          C.POINTER(C.c_int)]
+    lib.awsem_last_run_ms.argtypes = [vp]
+    lib.awsem_last_run_ms.restype = C.c_double
+    lib.awsem_kernel_name.argtypes = [ip]
+    lib.awsem_kernel_name.restype = cp
+    lib.awsem_profile_step.argtypes = [vp, ip, vp]
+    lib.awsem_model_info.argtypes = [vp, vp]
+    lib.awsem_batch_create.argtypes = [ip, ip, C.POINTER(vp)]
+    lib.awsem_batch_add_files.argtypes = [vp, cp, cp, cp, cp, cp, cp, C.c_ulonglong, C.POINTER(ip)]
+    lib.awsem_batch_commit.argtypes = [vp]
+    lib.awsem_nreplicas.argtypes = [vp]
+    lib.awsem_replica_natoms.argtypes = [vp, ip]
+    lib.awsem_replica_nres.argtypes = [vp, ip]
+    lib.awsem_replica_set_state.argtypes = [vp, ip, vp, vp]
+    lib.awsem_replica_get_state.argtypes = [vp, ip, vp, vp]
+    lib.awsem_replica_energies.argtypes = [vp, ip, vp]
+    lib.awsem_replica_forces.argtypes = [vp, ip, vp]
+    lib.awsem_batch_set_forcefield.argtypes = [vp, cp, cp, cp, cp]
+    lib.awsem_batch_add_replica.argtypes = [vp, C.POINTER(ReplicaDesc), C.POINTER(ip)]
     _lib = lib
     return lib
 
@@ -171,3 +197,128 @@ class AwsemSystem:
         _check(self.lib, self.lib.awsem_neighbor_stats(self.h, C.byref(nb), C.byref(rad), C.byref(mc), C.byref(ov)),
                "awsem_neighbor_stats")
         return {"builds": nb.value, "radius": rad.value, "max_count": mc.value, "overflow": ov.value}
+
+    # ------------------------------------------------------------------
+    # measurement helpers
+    def last_run_ms(self) -> float:
+        return float(self.lib.awsem_last_run_ms(self.h))
+
+    def profile_step(self, reps: int = 20) -> dict:
+        ms = np.zeros(10)
+        _check(self.lib, self.lib.awsem_profile_step(self.h, reps, _ptr(ms)), "awsem_profile_step")
+        return {self.lib.awsem_kernel_name(k).decode(): float(ms[k]) for k in range(10)}
+
+    def model_info(self) -> np.ndarray:
+        info = np.zeros(8, dtype=np.int64)
+        _check(self.lib, self.lib.awsem_model_info(self.h, _ptr(info)), "awsem_model_info")
+        return info
+
+
+class AwsemBatch(AwsemSystem):
+    """Independent replicas advanced together by one launch sequence."""
+
+    def __init__(self, replicas: list, precision: str | int = "mixed", device: int = 0, seeds=None):
+        lib = load_library()
+        self.lib = lib
+        prec = {"fp64": FP64, "mixed": MIXED}.get(precision, precision)
+        h = C.c_void_p()
+        _check(lib, lib.awsem_batch_create(int(prec), int(device), C.byref(h)), "awsem_batch_create")
+        self.h = h
+        try:
+            for k, files in enumerate(replicas):
+                seed = 0 if seeds is None else int(seeds[k])
+                rid = C.c_int()
+                _check(lib, lib.awsem_batch_add_files(h, files["workdir"].encode(), files["data"].encode(),
+                                                      files["coeff"].encode(), files["seq"].encode(),
+                                                      files["pair_style"].encode(),
+                                                      files.get("pair_coeffs", "").encode(), seed, C.byref(rid)),
+                       "awsem_batch_add_files")
+            _check(lib, lib.awsem_batch_commit(h), "awsem_batch_commit")
+        except Exception:
+            self.close()
+            raise
+        self.natoms = lib.awsem_natoms(h)
+        self.nres = lib.awsem_nres(h)
+        self.nreplicas = lib.awsem_nreplicas(h)
+        self.precision = prec
+
+    @classmethod
+    def from_arrays(cls, forcefield: dict, chains, precision: str | int = "mixed", device: int = 0, seeds=None):
+        """Replicas described by arrays (see synth.chain_arrays) sharing the
+        force field of a run directory (synth.forcefield_dir)."""
+        self = cls.__new__(cls)
+        lib = load_library()
+        self.lib = lib
+        prec = {"fp64": FP64, "mixed": MIXED}.get(precision, precision)
+        h = C.c_void_p()
+        _check(lib, lib.awsem_batch_create(int(prec), int(device), C.byref(h)), "awsem_batch_create")
+        self.h = h
+        try:
+            _check(lib, lib.awsem_batch_set_forcefield(h, forcefield["workdir"].encode(),
+                                                       forcefield["coeff"].encode(),
+                                                       forcefield["pair_style"].encode(),
+                                                       forcefield.get("pair_coeffs", "").encode()),
+                   "awsem_batch_set_forcefield")
+            for k, c in enumerate(chains):
+                d = ReplicaDesc()
+                d.n_res = int(c["n_res"])
+                d.n_chains = len(c["chain_len"])
+                d.chain_len = c["chain_len"].ctypes.data
+                d.seq = c["seq"]
+                d.ssweight = c["ssweight"].ctypes.data if c.get("ssweight") is not None else None
+                d.x = c["x"].ctypes.data
+                d.v = c["v"].ctypes.data if c.get("v") is not None else None
+                d.n_mem = int(c["n_mem"])
+                d.mem_pos = c["mem_pos"].ctypes.data
+                d.mem_len = c["mem_len"].ctypes.data
+                d.mem_weight = c["mem_weight"].ctypes.data
+                d.mem_seq = c["mem_seq"]
+                d.mem_ca = c["mem_ca"].ctypes.data
+                d.mem_cb = c["mem_cb"].ctypes.data
+                d.seed = 0 if seeds is None else int(seeds[k])
+                rid = C.c_int()
+                _check(lib, lib.awsem_batch_add_replica(h, C.byref(d), C.byref(rid)), "awsem_batch_add_replica")
+            _check(lib, lib.awsem_batch_commit(h), "awsem_batch_commit")
+        except Exception:
+            self.close()
+            raise
+        self.natoms = lib.awsem_natoms(h)
+        self.nres = lib.awsem_nres(h)
+        self.nreplicas = lib.awsem_nreplicas(h)
+        self.precision = prec
+        return self
+
+    def replica_natoms(self, r: int) -> int:
+        return int(self.lib.awsem_replica_natoms(self.h, r))
+
+    def get_state(self, r: int = 0):
+        n = self.replica_natoms(r)
+        x, v = np.zeros((n, 3)), np.zeros((n, 3))
+        _check(self.lib, self.lib.awsem_replica_get_state(self.h, r, _ptr(x), _ptr(v)), "awsem_replica_get_state")
+        return x, v
+
+    def set_state(self, x=None, v=None, r: int = 0):
+        n = self.replica_natoms(r)
+        xa = None if x is None else np.ascontiguousarray(x, dtype=np.float64).reshape(n, 3)
+        va = None if v is None else np.ascontiguousarray(v, dtype=np.float64).reshape(n, 3)
+        _check(self.lib, self.lib.awsem_replica_set_state(self.h, r, None if xa is None else _ptr(xa),
+                                                          None if va is None else _ptr(va)),
+               "awsem_replica_set_state")
+
+    def energies(self, r: int = 0) -> np.ndarray:
+        e = np.zeros(21)
+        _check(self.lib, self.lib.awsem_replica_energies(self.h, r, _ptr(e)), "awsem_replica_energies")
+        return e
+
+    def forces(self, r: int = 0) -> np.ndarray:
+        f = np.zeros((self.replica_natoms(r), 3))
+        _check(self.lib, self.lib.awsem_replica_forces(self.h, r, _ptr(f)), "awsem_replica_forces")
+        return f
+
+    def run(self, nsteps: int, dt=2.0, langevin=True, t_start=300.0, t_stop=300.0, damp=500.0, seed=1,
+            skin=2.0, neigh_every=0, thermo=False):
+        rp = RunParams(dt, int(langevin), t_start, t_stop, damp, seed, skin, neigh_every)
+        rows = np.zeros((self.nreplicas, nsteps + 1, 4)) if thermo else None
+        _check(self.lib, self.lib.awsem_run(self.h, nsteps, C.byref(rp), None if rows is None else _ptr(rows)),
+               "awsem_run")
+        return rows

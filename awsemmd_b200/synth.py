@@ -524,3 +524,135 @@ def sheet_system(seed=7, T=300.0) -> System:
     _, types, _, _ = atom_arrays(s)
     s.velocities = maxwell_velocities(types, T, rng)
     return s
+
+
+# --------------------------------------------------------------------------
+# array form of a chain (no files): what the batched engine takes for the
+# 1,024-replica and served workloads
+
+def chain_arrays(L: int, seed: int, n_mem_per_window=MEMS_PER_WINDOW, win=WINDOW, sigma=1.0, T=300.0) -> dict:
+    """One chain built as in configuration 0 from its own seed, returned as
+    the arrays of an awsem_replica_desc (atoms in data-file order CA, O, CB)."""
+    rng = np.random.default_rng(seed)
+    seq = "".join(AA[k] for k in rng.integers(0, 20, size=L))
+    ca = ca_trace(L, rng)
+    cb, o = place_beads(ca, seq)
+    cb = _chi_sign_fix(ca, cb, o, seq)
+    com = ca.mean(axis=0)
+    ca, cb, o = ca - com, cb - com, o - com
+    ss = ss_segments(L, rng)
+    x = np.stack([ca, o, cb], axis=1)  # [L][CA, O, CB][3]
+    types = np.array([[1, 3, 5 if s == "G" else 4] for s in seq]).reshape(-1)
+    v = maxwell_velocities(types, T, rng).reshape(L, 3, 3)
+    ssw = np.array([{"H": (1.0, 0.0), "E": (0.0, 1.0), "C": (0.0, 0.0)}[s] for s in ss])
+    W = max(L - win + 1, 0)
+    idx = np.arange(W)[:, None] + np.arange(win)[None, :]            # [W][win]
+    noise_ca = rng.normal(0.0, sigma, size=(W, n_mem_per_window, win, 3))
+    noise_cb = rng.normal(0.0, sigma, size=(W, n_mem_per_window, win, 3))
+    mem_ca = ca[idx][:, None, :, :] + noise_ca                        # [W][m][win][3]
+    mem_cb = cb[idx][:, None, :, :] + noise_cb
+    # the .gro precision (nm, 5 decimals)
+    mem_ca = np.round(mem_ca / 10.0, 5) * 10.0
+    mem_cb = np.round(mem_cb / 10.0, 5) * 10.0
+    n_mem = W * n_mem_per_window
+    seq_b = np.frombuffer(seq.encode(), dtype=np.uint8)
+    mem_seq = np.repeat(seq_b[idx][:, None, :], n_mem_per_window, axis=1).reshape(-1)
+    return {
+        "n_res": L, "chain_len": np.array([L], dtype=np.int32), "seq": seq.encode(),
+        "ssweight": np.ascontiguousarray(ssw, dtype=np.float64),
+        "x": np.ascontiguousarray(x, dtype=np.float64), "v": np.ascontiguousarray(v, dtype=np.float64),
+        "n_mem": n_mem, "mem_pos": np.repeat(np.arange(W, dtype=np.int32), n_mem_per_window),
+        "mem_len": np.full(n_mem, win, dtype=np.int32), "mem_weight": np.ones(n_mem),
+        "mem_seq": mem_seq.tobytes(),
+        "mem_ca": np.ascontiguousarray(mem_ca.reshape(-1, 3)), "mem_cb": np.ascontiguousarray(mem_cb.reshape(-1, 3)),
+    }
+
+
+def forcefield_dir(outdir: str) -> dict:
+    """A run directory holding only the shared force field (default
+    parameters + fragment memory with uniform.gamma)."""
+    os.makedirs(outdir, exist_ok=True)
+    for t in PARAM_TABLES:
+        shutil.copy(os.path.join(PARAM_DIR, t), os.path.join(outdir, t))
+    with open(os.path.join(outdir, "fix_backbone_coeff.data"), "w") as f:
+        f.write(coeff_text(mem_file="none.mem"))
+    return {"workdir": outdir, "coeff": "fix_backbone_coeff.data", "pair_style": PAIR_STYLE,
+            "pair_coeffs": ";".join(PAIR_COEFFS)}
+
+
+def write_chain_arrays(c: dict, outdir: str) -> dict:
+    """The run directory (reference input formats) of a chain given in array
+    form, e.g. to check the array path against the file path or the oracle."""
+    os.makedirs(outdir, exist_ok=True)
+    L = int(c["n_res"])
+    seq = c["seq"].decode()
+    x = c["x"].reshape(L * 3, 3)
+    v = c["v"].reshape(L * 3, 3)
+    lines = ["LAMMPS data file (synthetic AWSEM chain)", "", f"{3 * L} atoms", f"{4 * L - 2} bonds",
+             "5 atom types", "5 bond types", "", "-500.0 500.0 xlo xhi", "-500.0 500.0 ylo yhi",
+             "-500.0 500.0 zlo zhi", "", "Masses", ""]
+    lines += [f"{t} {MASSES[t]}" for t in range(1, 6)]
+    lines += ["", "Atoms", ""]
+    for r in range(L):
+        for k, t in enumerate([1, 3, 5 if seq[r] == "G" else 4]):
+            a = 3 * r + k
+            lines.append(f"{a + 1} 1 {r + 1} {t} 0.0 {float(x[a, 0])!r} {float(x[a, 1])!r} {float(x[a, 2])!r}")
+    lines += ["", "Velocities", ""]
+    for a in range(3 * L):
+        lines.append(f"{a + 1} {float(v[a, 0])!r} {float(v[a, 1])!r} {float(v[a, 2])!r}")
+    lines += ["", "Bond Coeffs", ""] + [f"{t} {BOND_COEFFS[t][0]} {BOND_COEFFS[t][1]}" for t in range(1, 6)]
+    lines += ["", "Bonds", ""]
+    b = 0
+    for r in range(L):
+        pairs = [(2, 3 * r, 3 * r + 1), (5 if seq[r] == "G" else 4, 3 * r, 3 * r + 2)]
+        if r < L - 1:
+            pairs += [(1, 3 * r, 3 * r + 3), (3, 3 * r + 1, 3 * r + 3)]
+        for t, i, j in pairs:
+            b += 1
+            lines.append(f"{b} {t} {i + 1} {j + 1}")
+    with open(os.path.join(outdir, "data.awsem"), "w") as f:
+        f.write("\n".join(lines) + "\n")
+    with open(os.path.join(outdir, "protein.seq"), "w") as f:
+        f.write(seq + "\n")
+    with open(os.path.join(outdir, "ssweight"), "w") as f:
+        for row in c["ssweight"]:
+            f.write(f"{float(row[0])!r} {float(row[1])!r}\n")
+    for t in PARAM_TABLES:
+        shutil.copy(os.path.join(PARAM_DIR, t), os.path.join(outdir, t))
+    with open(os.path.join(outdir, "fix_backbone_coeff.data"), "w") as f:
+        f.write(coeff_text())
+    # memories: one .gro per memory window group, coordinates written so
+    # that float(text) * 10 reproduces the array values to the last bits
+    # memories starting at the same residue share one .gro file (stacked)
+    os.makedirs(os.path.join(outdir, "mems"), exist_ok=True)
+    mem_lines = ["[Target]", "query", "", "[Memories]"]
+    off = 0
+    mseq = c["mem_seq"].decode()
+    groups = {}
+    for m in range(int(c["n_mem"])):
+        n = int(c["mem_len"][m])
+        groups.setdefault(int(c["mem_pos"][m]), []).append((m, off, n))
+        off += n
+    for pos, members in groups.items():
+        fname = f"mems/p{pos:05d}.gro"
+        rows = []
+        atom = 0
+        base = 0
+        for m, off, n in members:
+            for r in range(n):
+                rn = THREE[mseq[off + r]]
+                atom += 1
+                p = c["mem_ca"][off + r]
+                rows.append(f"{base + r + 1} {rn} CA {atom} " + " ".join(repr(float(q) / 10.0) for q in p))
+                if mseq[off + r] != "G":
+                    atom += 1
+                    p = c["mem_cb"][off + r]
+                    rows.append(f"{base + r + 1} {rn} CB {atom} " + " ".join(repr(float(q) / 10.0) for q in p))
+            mem_lines.append(f"{fname} {pos + 1} {base + 1} {n} {float(c['mem_weight'][m])!r}")
+            base += n
+        with open(os.path.join(outdir, fname), "w") as f:
+            f.write(f"memories at residue {pos + 1}\n{len(rows)}\n" + "\n".join(rows) + "\n0 0 0\n")
+    with open(os.path.join(outdir, "frags.mem"), "w") as f:
+        f.write("\n".join(mem_lines) + "\n")
+    return {"workdir": outdir, "data": "data.awsem", "coeff": "fix_backbone_coeff.data", "seq": "protein.seq",
+            "pair_style": PAIR_STYLE, "pair_coeffs": ";".join(PAIR_COEFFS)}

@@ -1,28 +1,35 @@
 #!/usr/bin/env python
-"""AWSEM-MD step benchmark: residue-steps/s on B200.
+"""AWSEM-MD step benchmark: residue-steps/s on one B200.
 
-One bench step = `--md-steps` velocity-Verlet + Langevin MD steps (300 K,
-dt 2 fs, damping 500 fs) of the workload with every force term on the GPU.
-Workload (default): benchmark configuration 1, a single system of 8 chains
-x 250 residues (2,000 residues, 6,000 beads) in a 150 A cube with all
-AWSEM terms and fragment memory on, run in the mixed form.
+Workload (default, `--workload c3`): benchmark configuration 3, 1,024
+independent single-chain replicas with lengths uniform in [40, 500] residues
+(278,062 residues), each built as in configuration 0 from its own seed with
+its own fragment-memory tables (20 memories per 9-residue window), all AWSEM
+terms on, pair vexcluded, harmonic bonds, Langevin 300 K, dt 2 fs, damping
+500 fs.  The batched form advances all replicas with one launch sequence per
+MD step (captured in CUDA graphs), in the mixed arithmetic form.  One bench
+step = `--md-steps` MD steps of every replica.
 
-Timing: W untimed warm-up bench steps, then K timed ones, each bracketed by
-a barrier and a device synchronize, device time from CUDA events on the
-engine's stream; L2 is flushed (a 512 MiB write) before every timed bench
-step.  With N GPUs (torchrun) every rank runs its own replica (replicas
-only: the path has no cross-GPU exchange) and the slowest rank's time sets
-the aggregate.
+`--workload c1`: configuration 1, one system of 8 chains x 250 residues.
 
+Timing: W untimed warm-up bench steps, then K timed ones; L2 is flushed (a
+512 MiB write) before each; device time from CUDA events on the engine's
+stream; with N GPUs every rank runs its own copy of the workload (replicas
+only) and the slowest rank's time sets the aggregate.
+
+Reported beside the headline: the plain single-instance FP64 form on the
+same replicas (one replica at a time, a sample), the end-to-end rate through
+the C ABI with host buffers, the roofline of the dominant kernel, and the
+reference CPU implementation on a bounded sample (`cpu_baseline`).
 `--impl reference` times the reference implementation (FixBackbone +
-PairExcludedVolume compiled unmodified against the LAMMPS-API shim, serial,
-one core) on the same workload and metric.
+PairExcludedVolume compiled unmodified against the LAMMPS-API shim) on the
+box's host cores on the same workload and metric.
 """
 from __future__ import annotations
 
 import argparse
-import ctypes as C
 import json
+import multiprocessing as mp
 import os
 import statistics
 import subprocess
@@ -39,8 +46,17 @@ sys.path.insert(0, os.path.join(ROOT, "oracle"))
 
 PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM = 6650.0
-
 RUN = dict(dt=2.0, t_start=300.0, t_stop=300.0, damp=500.0)
+CACHE = os.path.join(tempfile.gettempdir(), "awsem_chain_cache")
+
+WORKLOADS = {
+    "c3": "config3: 1,024 independent chains, lengths uniform in [40, 500] (278,062 residues), each with its own "
+          "fragment-memory tables (20 memories per 9-residue window), all AWSEM terms, pair vexcluded, harmonic "
+          "bonds, Langevin 300 K, dt 2 fs, damping 500 fs",
+    "c1": "config1: 8 chains x 250 residues (2,000 residues, 6,000 beads), 150 A cube, all AWSEM terms + fragment "
+          "memory (20 memories per 9-residue window), pair vexcluded, harmonic bonds, Langevin 300 K, dt 2 fs, "
+          "damping 500 fs",
+}
 
 
 def parse():
@@ -49,16 +65,22 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--md-steps", type=int, default=100)
+    ap.add_argument("--workload", default="c3", choices=list(WORKLOADS))
+    ap.add_argument("--md-steps", type=int, default=None, help="MD steps per bench step")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--replicas", type=int, default=1024, help="c3: number of replicas")
     ap.add_argument("--no-baseline", action="store_true", help="skip the CPU baseline sample")
-    return ap.parse_args()
+    a = ap.parse_args()
+    if a.md_steps is None:
+        a.md_steps = 20 if a.workload == "c3" else 100
+    return a
 
 
 # --------------------------------------------------------------------------
-# distributed plumbing (one process per GPU, replicas only)
 
 class Dist:
+    """One process per GPU; replicas only (no data-path collective)."""
+
     def __init__(self):
         self.world = int(os.environ.get("WORLD_SIZE", "1"))
         self.rank = int(os.environ.get("RANK", "0"))
@@ -93,20 +115,15 @@ class Dist:
             self.pg.destroy_process_group()
 
 
-# --------------------------------------------------------------------------
-
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+    """nvidia-smi clocks and throttle reasons every 200 ms during the timed region."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
     def __init__(self, gpu: int):
-        self.gpu = gpu
-        self.rows = []
-        self.proc = None
-        self.thread = None
+        self.gpu, self.rows, self.proc, self.thread = gpu, [], None, None
 
     def start(self):
         try:
@@ -114,7 +131,6 @@ class ClockSampler:
                                           "--format=csv,noheader,nounits", "-lms", "200"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except OSError:
-            self.proc = None
             return
         self.thread = threading.Thread(target=self._read, daemon=True)
         self.thread.start()
@@ -152,40 +168,68 @@ class ClockSampler:
 
 
 def flush_l2(buf):
-    buf.fill_(1.0)
     import torch
 
+    buf.fill_(1.0)
     torch.cuda.synchronize()
 
 
 def peaks():
     try:
         with open(PEAKS_FILE) as f:
-            p = json.load(f)
-        return float(p["hbm_gbs"]), "measured"
+            return float(json.load(f)["hbm_gbs"]), "measured"
     except (OSError, KeyError, ValueError):
         return FALLBACK_HBM, "fallback"
 
 
-def make_workload(tmp: str, replica: int):
+# --------------------------------------------------------------------------
+# workloads
+
+def c3_chain(L: int, seed: int) -> dict:
+    """Configuration-3 chain in array form, cached on disk by (L, seed)."""
     from awsemmd_b200 import synth
 
-    s = synth.config_system(1, replica=replica)
-    files = synth.write_system(s, os.path.join(tmp, f"c1_r{replica}"))
-    return files, s.n_res
+    os.makedirs(CACHE, exist_ok=True)
+    path = os.path.join(CACHE, f"chain_{L}_{seed}.npz")
+    if os.path.exists(path):
+        try:
+            z = np.load(path)
+            c = {k: z[k] for k in z.files}
+            for k in ("seq", "mem_seq"):
+                c[k] = bytes(c[k])
+            for k in ("n_res", "n_mem"):
+                c[k] = int(c[k])
+            return c
+        except Exception:
+            pass
+    c = synth.chain_arrays(L, seed)
+    tmp = path + f".{os.getpid()}.npz"
+    np.savez(tmp, **{k: (np.frombuffer(v, dtype=np.uint8) if isinstance(v, bytes) else v) for k, v in c.items()})
+    os.replace(tmp, path)
+    return c
 
 
-# algorithmic bytes per launch of each kernel (see the engine's data layout):
-#   fragmem: every stored memory distance once, the row table, the two target
-#            beads per row and the force accumulators of i and j
-#   pair / density / water_xi: the residue pair list once, every residue's
-#            working coordinates and per-residue scalars once
+def c3_lengths(n: int):
+    from awsemmd_b200 import synth
+
+    return synth.replica_lengths(n=1024)[:n]
+
+
+def c3_seed(k: int, rank: int = 0) -> int:
+    return 3000 + k + 100000 * rank
+
+
 def algorithmic_bytes(kernel: str, info) -> float:
+    """Bytes one launch must move at least (data layout of the engine):
+    fragmem -- every stored memory distance once, the row table, the two
+    target beads per residue and the force accumulators it updates;
+    pair / density / water_xi -- the residue pair list once, every residue's
+    working coordinates and per-residue scalars once."""
     n_res, n_atoms, records, rbytes, nd, cap, entries, nonuni = [int(v) for v in info]
-    bead = 32  # double4 working coordinates
+    bead = 32
     if kernel == "fragmem":
-        return records * 4 * rbytes + records * rbytes * nonuni + (n_res * nd + 1) * 4 + n_res * 2 * bead \
-            + n_res * 2 * 3 * 8 * 2
+        return (records * 4 * rbytes + records * rbytes * nonuni + (n_res * nd + 1) * 4 + n_res * 2 * bead
+                + n_res * 2 * 3 * 8 * 2)
     if kernel in ("pair", "density", "water_xi"):
         return entries * 4 + n_res * 6 * bead + n_res * 10 * 8 + n_res * 4 * 4 + n_atoms * 3 * 8
     if kernel == "prepare":
@@ -195,82 +239,113 @@ def algorithmic_bytes(kernel: str, info) -> float:
     return n_res * 6 * bead
 
 
-def cpu_baseline(files, n_res, seconds_target=12.0):
-    """The reference (shim-hosted, one core) on a bounded sample of the
-    workload; falls back to the FP64 restatement when the reference library
-    was not built."""
-    import ref
+# --------------------------------------------------------------------------
+# CPU reference (the shim-hosted reference FixBackbone + PairExcludedVolume)
 
-    if ref.ref_available():
+def _ref_worker(args):
+    """Runs in a spawned process: reference MD on a few c3 replicas."""
+    lens_seeds, md, tmp = args
+    sys.path.insert(0, ROOT)
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ref
+    from awsemmd_b200 import synth
+
+    done_res_steps, t_total = 0, 0.0
+    for L, seed in lens_seeds:
+        c = c3_chain(L, seed)
+        files = synth.write_chain_arrays(c, os.path.join(tmp, f"r{seed}"))
         r = ref.RefSystem(files)
-        r.run(2, langevin=True, seed=7)  # warm-up (includes the O(n^2) cache reset at setup)
-        steps, t = 5, 0.0
-        while True:
-            t0 = time.perf_counter()
-            r.run(steps, langevin=True, seed=7)
-            t = time.perf_counter() - t0
-            if t * 4 > seconds_target or steps >= 400:
-                break
-            steps *= 2
+        r.run(1, langevin=True, seed=seed)  # warm-up (setup caches)
+        t0 = time.perf_counter()
+        r.run(md, langevin=True, seed=seed)
+        t_total += time.perf_counter() - t0
+        done_res_steps += L * md
         r.close()
-        return {"value": n_res * steps / t, "unit": "residue-steps/s", "cores": 1, "kind": "reference",
-                "sample": f"{steps} MD steps (one `run`, incl. its setup evaluation) of the same 2,000-residue "
-                          f"system, reference FixBackbone+PairExcludedVolume compiled -O2 against the LAMMPS-API "
-                          f"shim, 1 MPI rank, {t:.1f} s"}
-    # the FP64 restatement (all-pairs loops) as the port baseline
-    o = ref.OracleSystem(files)
-    from awsemmd_b200.engine import AwsemSystem  # noqa: F401  (state comes from the data file)
-    x0 = np.zeros((o.natoms, 3))
-    v0 = np.zeros((o.natoms, 3))
-    with open(os.path.join(files["workdir"], files["data"])) as fh:
-        lines = fh.read().split("\n")
-    at = lines.index("Atoms") + 2
-    for k in range(o.natoms):
-        w = lines[at + k].split()
-        x0[int(w[0]) - 1] = [float(w[5]), float(w[6]), float(w[7])]
-    steps = 2
-    t0 = time.perf_counter()
-    o.run(x0, v0, steps, langevin=True, seed=7)
-    t = time.perf_counter() - t0
-    return {"value": n_res * steps / t, "unit": "residue-steps/s", "cores": 1, "kind": "port",
-            "sample": f"{steps} MD steps of the FP64 restatement (all-pairs loops), {t:.1f} s"}
+    return done_res_steps, t_total
+
+
+def reference_c3(n_procs: int, per_proc: int, md: int):
+    """Aggregate residue-steps/s of the reference over `n_procs` host cores,
+    each running `per_proc` replicas of the workload (a bounded sample)."""
+    lens = c3_lengths(1024)
+    rng = np.random.default_rng(1)
+    pick = rng.choice(1024, size=n_procs * per_proc, replace=False)
+    jobs = [[(lens[k], c3_seed(k)) for k in pick[p::n_procs]] for p in range(n_procs)]
+    with tempfile.TemporaryDirectory() as tmp:
+        ctx = mp.get_context("spawn")
+        t0 = time.perf_counter()
+        with ctx.Pool(n_procs) as pool:
+            out = pool.map(_ref_worker, [(j, md, tmp) for j in jobs])
+        wall = time.perf_counter() - t0
+    res_steps = sum(o[0] for o in out)
+    busy = max(o[1] for o in out)
+    # each process times only its MD steps; the slowest sets the aggregate
+    return res_steps / busy, res_steps, busy, wall
+
+
+def reference_c1(md: int, warmup: int, steps: int):
+    import ref
+    from awsemmd_b200 import synth
+
+    with tempfile.TemporaryDirectory() as tmp:
+        files = synth.write_system(synth.config_system(1), os.path.join(tmp, "c1"))
+        r = ref.RefSystem(files)
+        for _ in range(warmup):
+            r.run(md, langevin=True, seed=11)
+        t = []
+        for _ in range(steps):
+            t0 = time.perf_counter()
+            r.run(md, langevin=True, seed=11)
+            t.append(time.perf_counter() - t0)
+        r.close()
+    return 2000 * md * steps / sum(t), sum(t)
 
 
 def reference_arm(args, dist: Dist):
-    """--impl reference: the reference CPU implementation, same workload/metric."""
     if dist.rank != 0:
         return
     import ref
 
-    with tempfile.TemporaryDirectory() as tmp:
-        files, n_res = make_workload(tmp, 0)
-        if not ref.ref_available():
-            print(json.dumps({"impl": "reference", "unavailable": "reference library not built (make -C oracle ref)"}))
-            return
-        r = ref.RefSystem(files)
-        md = 5  # MD steps per bench step (a bounded sample of the workload)
-        for _ in range(args.warmup):
-            r.run(md, langevin=True, seed=11)
-        times = []
-        for _ in range(args.steps):
-            t0 = time.perf_counter()
-            r.run(md, langevin=True, seed=11)
-            times.append(time.perf_counter() - t0)
-        r.close()
-    total = sum(times)
-    value = n_res * md * args.steps / total
+    if not ref.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "reference library not built (make -C oracle ref)"}))
+        return
+    cores = os.cpu_count() or 1
+    if args.workload == "c3":
+        md = 10
+        # a bounded sample: every core runs a few random replicas for md steps
+        value, res_steps, busy, wall = reference_c3(cores, max(2, (args.steps + args.warmup) // 4), md)
+        ms = 1e3 * busy / max(args.steps, 1)
+        sample = (f"{res_steps} residue-steps: {cores} processes (one per host core), each running a random "
+                  f"subset of the 1,024 replicas for {md} MD steps (+1 warm-up step); reference FixBackbone + "
+                  f"PairExcludedVolume compiled -O2 against the LAMMPS-API shim, 1 rank per process")
+    else:
+        md = 5
+        value, busy = reference_c1(md, args.warmup, args.steps)
+        cores = 1
+        ms = 1e3 * busy / args.steps
+        sample = f"{md} MD steps per bench step of the 2,000-residue system, 1 core, 1 rank"
     line = {"metric": "residue-steps/s", "value": value, "unit": "residue-steps/s", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic", "impl": "reference",
-            "config": {"workload": "config1: 8 chains x 250 residues, 2,000 residues, 150 A cube, all terms + "
-                                   "fragment memory, Langevin 300 K dt 2 fs", "md_steps_per_step": md,
-                       "parallelism": "1 MPI rank (serial reference; no MPI in the image)"},
-            "cpu_baseline": {"value": value, "unit": "residue-steps/s", "cores": 1, "kind": "reference",
-                             "sample": f"{md} MD steps per bench step, reference FixBackbone+PairExcludedVolume "
-                                       f"compiled -O2 against the LAMMPS-API shim"},
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": {"workload": WORKLOADS[args.workload], "md_steps_per_step": md,
+                       "parallelism": f"{cores} host processes x 1 MPI rank (serial reference; no MPI in the image)"},
+            "cpu_baseline": {"value": value, "unit": "residue-steps/s", "cores": cores, "kind": "reference",
+                             "sample": sample},
             "e2e": {"value": value, "unit": "residue-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
+
+
+# --------------------------------------------------------------------------
+
+def build_c3(n: int, rank: int, precision: str, dev: int, tmp: str):
+    from awsemmd_b200 import synth
+    from awsemmd_b200.engine import AwsemBatch
+
+    lens = c3_lengths(n)
+    chains = (c3_chain(L, c3_seed(k, rank)) for k, L in enumerate(lens))
+    ff = synth.forcefield_dir(os.path.join(tmp, "ff"))
+    seeds = [c3_seed(k, rank) for k in range(n)]
+    return AwsemBatch.from_arrays(ff, chains, precision=precision, device=dev, seeds=seeds), sum(lens), ff, lens
 
 
 def main():
@@ -283,24 +358,30 @@ def main():
     import torch
 
     from awsemmd_b200 import build
-    from awsemmd_b200.engine import AwsemSystem, load_library
+    from awsemmd_b200.engine import AwsemBatch, AwsemSystem
 
-    if dist.rank == 0 or not os.path.exists(os.path.join(ROOT, "awsemmd_b200", "libawsem_gpu.so")):
+    if dist.rank == 0:
         build.build()
     dist.barrier()
-    lib = load_library()
     dev = dist.local
     torch.cuda.set_device(dev)
     l2buf = torch.empty(128 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{dev}")  # 512 MiB > 126 MB L2
     tmp = tempfile.mkdtemp()
-    files, n_res = make_workload(tmp, dist.rank)
-    sysm = AwsemSystem(files, precision=args.precision, device=dev)
-    x0, v0 = sysm.get_state()
     md = args.md_steps
     run_kw = dict(dt=RUN["dt"], langevin=True, t_start=RUN["t_start"], t_stop=RUN["t_stop"], damp=RUN["damp"],
                   seed=1000 + dist.rank)
+    t_setup = time.perf_counter()
+    if args.workload == "c3":
+        eng, n_res, ff, lens = build_c3(args.replicas, dist.rank, args.precision, dev, tmp)
+    else:
+        from awsemmd_b200 import synth
+
+        files = synth.write_system(synth.config_system(1, replica=dist.rank), os.path.join(tmp, "c1"))
+        eng = AwsemSystem(files, precision=args.precision, device=dev)
+        n_res = eng.nres
+    t_setup = time.perf_counter() - t_setup
     for _ in range(args.warmup):
-        sysm.run(md, **run_kw)
+        eng.run(md, **run_kw)
     clocks = ClockSampler(dev)
     clocks.start()
     dev_ms = []
@@ -308,87 +389,110 @@ def main():
         flush_l2(l2buf)
         dist.barrier()
         torch.cuda.synchronize()
-        sysm.run(md, **run_kw)
+        eng.run(md, **run_kw)
         torch.cuda.synchronize()
-        dev_ms.append(lib.awsem_last_run_ms(sysm.h))
+        dev_ms.append(eng.last_run_ms())
         dist.barrier()
     clk = clocks.stop()
     total_ms = dist.max(sum(dev_ms))
     value = dist.world * n_res * md * args.steps / (total_ms / 1e3)
 
-    # end to end through the public API with host buffers: host state in,
-    # `run`, host state out
-    sysm.set_state(x0, v0)
+    # end to end through the C ABI with host buffers: every replica's state
+    # in from host memory, `run`, every replica's state out
+    nrep = getattr(eng, "nreplicas", 1)
+    host = [eng.get_state(r) if nrep > 1 else eng.get_state() for r in range(nrep)]
     e2e_t = []
     for _ in range(max(2, args.steps // 2)):
         dist.barrier()
         t0 = time.perf_counter()
-        sysm.set_state(x0, v0)
-        sysm.run(md, **run_kw)
-        xh, vh = sysm.get_state()
+        for r in range(nrep):
+            if nrep > 1:
+                eng.set_state(host[r][0], host[r][1], r=r)
+            else:
+                eng.set_state(host[r][0], host[r][1])
+        eng.run(md, **run_kw)
+        for r in range(nrep):
+            host[r] = eng.get_state(r) if nrep > 1 else eng.get_state()
         e2e_t.append(time.perf_counter() - t0)
     e2e_total = dist.max(sum(e2e_t))
     e2e_value = dist.world * n_res * md * len(e2e_t) / e2e_total
-    natoms = sysm.natoms
+    natoms = eng.natoms
 
-    # roofline of the dominant kernel: per-kernel CUDA-event times of the step
-    lib.awsem_kernel_name.restype = C.c_char_p
-    names = [lib.awsem_kernel_name(k).decode() for k in range(10)]
-    ms = np.zeros(10)
-    sysm.run(5, **run_kw)
-    rc = lib.awsem_profile_step(sysm.h, 50, ms.ctypes.data_as(C.c_void_p))
-    info = np.zeros(8, dtype=np.int64)
-    lib.awsem_model_info(sysm.h, info.ctypes.data_as(C.c_void_p))
-    top = int(np.argmax(ms))
+    # roofline of the dominant kernel from per-kernel CUDA-event times
+    eng.run(2, **run_kw)
+    prof = eng.profile_step(20)
+    info = eng.model_info()
+    names = list(prof)
+    top = max(names, key=lambda k: prof[k])
     peak, peak_kind = peaks()
-    abytes = algorithmic_bytes(names[top], info)
-    achieved = abytes / (ms[top] * 1e-3) / 1e9
-    fm_k = names.index("fragmem")
-    fm_bytes = algorithmic_bytes("fragmem", info)
-    roofline = {"bound": "hbm", "kernel": names[top], "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "traffic": None, "peak_source": f"{peak_kind} hbm_gbs",
-                "algorithmic_bytes": abytes, "launch_ms": float(ms[top]),
-                "kernel_ms": {names[k]: round(float(ms[k]), 5) for k in range(10)},
-                "fragmem_gbs": fm_bytes / (ms[fm_k] * 1e-3) / 1e9 if ms[fm_k] > 0 else None}
+    abytes = algorithmic_bytes(top, info)
+    achieved = abytes / (prof[top] * 1e-3) / 1e9
+    fm_gbs = algorithmic_bytes("fragmem", info) / (prof["fragmem"] * 1e-3) / 1e9 if prof["fragmem"] > 0 else None
+    roofline = {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": None, "peak_source": f"{peak_kind} hbm_gbs (burst copy)",
+                "algorithmic_bytes_per_launch": abytes, "launch_ms": prof[top],
+                "kernel_ms": {k: round(v, 5) for k, v in prof.items()}, "fragmem_gbs": fm_gbs}
 
-    # the plain FP64 form on the same workload (the comparison point)
+    # the plain single-instance FP64 form (one replica at a time)
     plain = None
-    if args.precision != "fp64":
+    if args.workload == "c3":
+        sample = np.random.default_rng(7).choice(args.replicas, size=min(24, args.replicas), replace=False)
+        res_steps, ms_sum = 0, 0.0
+        for k in sample:
+            c = c3_chain(lens[k], c3_seed(k, dist.rank))
+            with AwsemBatch.from_arrays(ff, [c], precision="fp64", device=dev, seeds=[c3_seed(k, dist.rank)]) as one:
+                one.run(md, **run_kw)
+                flush_l2(l2buf)
+                one.run(md, **run_kw)
+                ms_sum += one.last_run_ms()
+                res_steps += lens[k] * md
+        pv = res_steps / (ms_sum / 1e3)
+        plain = {"value": pv, "unit": "residue-steps/s", "speedup_of_headline": value / pv / dist.world,
+                 "sample": f"{len(sample)} of the replicas run one at a time, plain FP64 single-system form, "
+                           f"{md} MD steps each after a warm-up run, device time"}
+    elif args.precision != "fp64":
         with AwsemSystem(files, precision="fp64", device=dev) as sp:
             sp.run(md, **run_kw)
             pm = []
             for _ in range(max(2, args.steps // 2)):
                 flush_l2(l2buf)
                 sp.run(md, **run_kw)
-                pm.append(lib.awsem_last_run_ms(sp.h))
-            pms = dist.max(sum(pm))
-            plain = {"value": dist.world * n_res * md * len(pm) / (pms / 1e3), "unit": "residue-steps/s"}
+                pm.append(sp.last_run_ms())
+            plain = {"value": n_res * md * len(pm) / (sum(pm) / 1e3), "unit": "residue-steps/s"}
 
     base = None
     if dist.rank == 0 and dist.world == 1 and not args.no_baseline:
         try:
-            base = cpu_baseline(files, n_res)
-        except Exception as e:  # reported, never silently replaced
+            if args.workload == "c3":
+                v, rs, busy, wall = reference_c3(1, 3, 5)
+                base = {"value": v, "unit": "residue-steps/s", "cores": 1, "kind": "reference",
+                        "sample": f"3 random replicas x 5 MD steps ({rs} residue-steps, {busy:.1f} s) on 1 host "
+                                  f"core; reference FixBackbone + PairExcludedVolume compiled -O2 against the "
+                                  f"LAMMPS-API shim, 1 MPI rank"}
+            else:
+                v, busy = reference_c1(5, 1, 2)
+                base = {"value": v, "unit": "residue-steps/s", "cores": 1, "kind": "reference",
+                        "sample": f"2 x 5 MD steps of the 2,000-residue system ({busy:.1f} s), 1 core, 1 rank"}
+        except Exception as e:  # reported, never replaced by something else
             base = {"value": None, "unit": "residue-steps/s", "cores": 1, "kind": "reference",
                     "sample": f"not measured: {e}"}
-    sysm.close()
+    eng.close()
     launches = 10 * (md + 1) * args.steps
     if dist.rank == 0:
         line = {"metric": "residue-steps/s", "value": value, "unit": "residue-steps/s", "n_gpus": dist.world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "f32/f64" if args.precision == "mixed" else "f64", "data": "synthetic",
-                "config": {"workload": "config1: 8 chains x 250 residues (2,000 residues, 6,000 beads), 150 A cube, "
-                                       "all AWSEM terms + fragment memory (20 memories per 9-residue window), "
-                                       "pair vexcluded, harmonic bonds, Langevin 300 K, dt 2 fs, damping 500 fs",
-                           "form": args.precision, "md_steps_per_step": md, "global_batch": dist.world,
-                           "parallelism": f"replicas x{dist.world} (one independent system per GPU)",
-                           "l2": "flushed (512 MiB write) before every timed bench step; fragment-memory tables "
-                                 "stay L2-resident across the MD steps inside one bench step"},
+                "config": {"workload": WORKLOADS[args.workload], "form": args.precision, "md_steps_per_step": md,
+                           "residues": n_res, "replicas": nrep, "global_batch": dist.world * nrep,
+                           "parallelism": f"replicas x{dist.world} GPUs (independent copies per GPU)",
+                           "l2": "flushed (512 MiB write) before every timed bench step",
+                           "setup_s": round(t_setup, 1)},
                 "roofline": roofline, "cpu_baseline": base,
                 "e2e": {"value": e2e_value, "unit": "residue-steps/s",
                         "h2d_bytes_per_step": 2 * natoms * 3 * 8, "d2h_bytes_per_step": 2 * natoms * 3 * 8,
-                        "path": "awsem_set_state(host x, v) + awsem_run + awsem_get_state per bench step"},
+                        "path": "awsem_replica_set_state (host x, v) for every replica + awsem_run + "
+                                "awsem_replica_get_state for every replica, per bench step"},
                 "plain_fp64": plain, "clocks": clk, "gpu_launches": launches}
         print(json.dumps(line))
     dist.close()

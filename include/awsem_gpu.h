@@ -76,6 +76,57 @@ int awsem_create_from_files(const char *workdir, const char *data_file, const ch
                             int precision, int device, awsem_system **out);
 void awsem_destroy(awsem_system *sys);
 
+/* Batches of independent replicas (one launch sequence advances them all).
+ * Create an empty handle, add replicas (each a reference-style run
+ * directory; all must share one coefficient file, tables and pair_style),
+ * then commit.  `seed` is the replica's own Langevin seed (0: use the run's
+ * seed).  A replica's trajectory does not depend on which other replicas
+ * share the batch: every cross-thread sum is an exact fixed-point sum and
+ * the noise stream is keyed by (seed, step, atom id).  No counterpart in the
+ * reference (it runs one system per LAMMPS process). */
+int awsem_batch_create(int precision, int device, awsem_system **out);
+int awsem_batch_add_files(awsem_system *sys, const char *workdir, const char *data_file, const char *coeff_file,
+                          const char *seq_file, const char *pair_style, const char *pair_coeffs,
+                          unsigned long long seed, int *replica);
+int awsem_batch_commit(awsem_system *sys);
+
+/* Replicas given as arrays instead of files.  The force field (coefficient
+ * file, the tables in `workdir`, the fragment-memory gamma file, pair_style
+ * vexcluded settings) is read once; atoms follow the awsemmd data-file
+ * conventions: per residue CA (type 1), O (type 3), CB (type 4) or H-beta
+ * for glycine (type 5), atom ids 1..3n in that order, masses 27/28/60/2,
+ * harmonic bonds CA-CA 3.816, CA-O 2.40, O-CA 2.76, CA-CB 1.53, CA-HB 1.09
+ * with K = 60 kcal/mol/A^2. */
+typedef struct awsem_replica_desc {
+  int n_res;
+  int n_chains;
+  const int *chain_len;        /* [n_chains] residues per chain */
+  const char *seq;             /* [n_res] one-letter residue codes */
+  const double *ssweight;      /* [n_res][enabled SSWeight columns], or NULL */
+  const double *x;             /* [n_res][3][3]: CA, O, CB/H-beta of each residue (A) */
+  const double *v;             /* same layout (A/fs), or NULL for zero */
+  int n_mem;                   /* fragment memories */
+  const int *mem_pos;          /* [n_mem] first target residue, 0-based */
+  const int *mem_len;          /* [n_mem] */
+  const double *mem_weight;    /* [n_mem] */
+  const char *mem_seq;         /* concatenated memory residue codes */
+  const double *mem_ca;        /* concatenated [len][3] CA coordinates (A) */
+  const double *mem_cb;        /* concatenated [len][3] CB coordinates (A; ignored for glycine) */
+  unsigned long long seed;     /* Langevin seed of the replica (0: the run's) */
+} awsem_replica_desc;
+
+int awsem_batch_set_forcefield(awsem_system *sys, const char *workdir, const char *coeff_file,
+                               const char *pair_style, const char *pair_coeffs);
+int awsem_batch_add_replica(awsem_system *sys, const awsem_replica_desc *desc, int *replica);
+int awsem_nreplicas(const awsem_system *sys);
+int awsem_replica_natoms(const awsem_system *sys, int replica);
+int awsem_replica_nres(const awsem_system *sys, int replica);
+int awsem_replica_set_state(awsem_system *sys, int replica, const double *x, const double *v);
+int awsem_replica_get_state(awsem_system *sys, int replica, double *x, double *v);
+int awsem_replica_energies(awsem_system *sys, int replica, double *energies);
+int awsem_replica_forces(awsem_system *sys, int replica, double *f);
+
+/* totals over the whole batch (one replica: that system) */
 int awsem_natoms(const awsem_system *sys);
 int awsem_nres(const awsem_system *sys);
 
@@ -87,14 +138,16 @@ int awsem_nres(const awsem_system *sys);
  * AWSEM_TERMS_PAIR, PairExcludedVolume::compute. */
 int awsem_compute(awsem_system *sys, long long step, const double *x, double *f, double *energies, int terms);
 
-/* Device-resident state (caller atom order). */
+/* Device-resident state of a single-system handle (caller atom order);
+ * the awsem_replica_* forms address one replica of a batch. */
 int awsem_set_state(awsem_system *sys, const double *x, const double *v);
 int awsem_get_state(awsem_system *sys, double *x, double *v);
 
 /* `run nsteps`: velocity Verlet (+ Langevin) with every force evaluated on
  * the GPU; the step sequence is captured in a CUDA graph.  thermo (may be
- * NULL) receives (nsteps+1) rows of [fix total, vexcluded, bonds, kinetic].
- * The first row is the setup evaluation at the current step counter. */
+ * NULL) receives, per replica, (nsteps+1) rows of [fix total, vexcluded,
+ * bonds, kinetic] (replica-major).  The first row is the setup evaluation
+ * at the current step counter.  Advances every replica of a batch. */
 int awsem_run(awsem_system *sys, long long nsteps, const awsem_run_params *rp, double *thermo);
 
 /* Device time (ms) of the last awsem_run, from CUDA events recorded on the

@@ -1,0 +1,69 @@
+"""Batched replicas: parity per replica, and results independent of the mix."""
+import numpy as np
+import pytest
+
+from conftest import write_case
+
+pytestmark = pytest.mark.gpu
+
+
+def _extra_chain(tmp_path, L=57, seed=777):
+    from awsemmd_b200 import synth
+
+    s = synth.make_system([L], box=200.0, seed=seed)
+    return synth.write_system(s, str(tmp_path / f"chain{L}_{seed}"))
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_batch_replicas_match_golden(prec, tmp_path, gpu_lib):
+    from awsemmd_b200.engine import AwsemBatch
+
+    f0, g0 = write_case("c0", tmp_path)
+    f1, g1 = write_case("sheet", tmp_path)
+    f2 = _extra_chain(tmp_path)
+    etol = 1e-6 if prec == "fp64" else 1e-5
+    ftol = 1e-5 if prec == "fp64" else 1e-4
+    with AwsemBatch([f0, f2, f1], precision=prec, seeds=[11, 12, 13]) as b:
+        assert b.nreplicas == 3
+        b.run(0, langevin=False)  # one evaluation at the loaded coordinates
+        for r, g in [(0, g0), (2, g1)]:
+            e = b.energies(r)
+            f = b.forces(r)
+            for k in range(20):
+                assert abs(e[k] - g["e0"][k]) <= etol * max(abs(g["e0"][k]), 1e-3 * max(1.0, abs(g["e0"][0]) * 1e-6)), \
+                    (r, k, e[k], g["e0"][k])
+            assert np.abs(f - g["f0"]).max() / np.abs(g["f0"]).max() < ftol
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_replica_alone_equals_replica_in_the_mix(prec, tmp_path, gpu_lib):
+    """Bitwise: a replica's trajectory does not depend on its batch mates."""
+    from awsemmd_b200.engine import AwsemBatch
+
+    f0, _ = write_case("c0", tmp_path)
+    f1, _ = write_case("sheet", tmp_path)
+    f2 = _extra_chain(tmp_path)
+    kw = dict(dt=2.0, langevin=True, t_start=400.0, t_stop=300.0, damp=500.0, seed=5)
+    with AwsemBatch([f2], precision=prec, seeds=[99]) as alone:
+        alone.run(150, **kw)
+        xa, va = alone.get_state(0)
+        ea = alone.energies(0)
+    with AwsemBatch([f0, f1, f2, f0], precision=prec, seeds=[1, 2, 99, 3]) as mix:
+        mix.run(150, **kw)
+        xm, vm = mix.get_state(2)
+        em = mix.energies(2)
+        x0, _ = mix.get_state(0)
+        x3, _ = mix.get_state(3)
+    assert np.array_equal(xa, xm) and np.array_equal(va, vm)
+    np.testing.assert_allclose(em, ea, rtol=1e-12, atol=1e-9)
+    # same input, different seeds: different trajectories
+    assert not np.array_equal(x0, x3)
+
+
+def test_batch_rejects_mismatched_force_fields(tmp_path, gpu_lib):
+    from awsemmd_b200.engine import AwsemBatch, AwsemError
+
+    f0, _ = write_case("c0", tmp_path)
+    f1, _ = write_case("r1r69", tmp_path)  # different fragment-memory gamma classes
+    with pytest.raises(AwsemError, match="share one force field"):
+        AwsemBatch([f0, f1])
