@@ -20,7 +20,7 @@ BUILD = os.path.join(HERE, "_build")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
               "--expt-relaxed-constexpr", "-I" + CSRC, "-I" + INCLUDE]
-SOURCES = ["awsem_model.cpp", "awsem_engine.cu"]
+SOURCES = ["awsem_model.cpp", "awsem_engine.cu", "awsem_noalloc.cu"]
 
 
 def nvcc() -> str:

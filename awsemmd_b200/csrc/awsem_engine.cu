@@ -99,7 +99,21 @@ class EngineBase {
   virtual void profile(int reps, double *ms) = 0;
   virtual void model_info(long long *info) = 0;
   virtual double run_ms() const = 0;
+  // device-resident fragment-memory table, for entry points outside the engine
+  struct FMView {
+    const int *row;
+    const void *rf, *coef;  // element type: double (FP64 form) or float (mixed form)
+    double uniform;
+    int nd, min_sep, n_res, is_double;
+    const int *res_flags;
+    const double *sigma_sq;  // host table [64]
+  };
+  virtual FMView fm_view() const = 0;
 };
+
+void fragmem_noalloc(int device, int n_res, const int *row, const void *rf, const void *coef, double uniform, int nd,
+                     int min_sep, const double *sigma_sq, int is_double, const double *d_x, double *d_f,
+                     double *d_energy, cudaStream_t stream);  // awsem_noalloc.cu
 
 static const char *kKernelNames[AWSEM_NKERNELS] = {"prepare", "nl_decide", "nl_build", "density", "residue",
                                                    "water_xi", "pair", "fragmem", "bonds", "finish"};
@@ -571,6 +585,22 @@ template <typename R> class Engine : public EngineBase {
 
   double run_ms() const override { return last_run_ms; }
 
+  FMView fm_view() const override
+  {
+    FMView v;
+    v.row = fm_row.p;
+    v.rf = fm_rf.p;
+    v.coef = in.fm.uniform ? nullptr : fm_coef.p;
+    v.uniform = in.fm.uniform_coef;
+    v.nd = in.ff.p.fm_nd;
+    v.min_sep = in.ff.p.fm_min_sep;
+    v.n_res = n();
+    v.is_double = sizeof(R) == sizeof(double);
+    v.res_flags = res_flags.p;
+    v.sigma_sq = in.ff.p.fm_sigma_sq;
+    return v;
+  }
+
   void model_info(long long *info) override
   {
     info[0] = n();
@@ -998,6 +1028,20 @@ int awsem_model_info(awsem_system *sys, long long *info)
 {
   if (!ready(sys) || !info) return AWSEM_EINVAL;
   return guarded([&] { sys->eng->model_info(info); });
+}
+
+int awsem_fragmem_noalloc(awsem_system *sys, const double *d_x, double *d_f, double *d_energy, void *stream)
+{
+  if (!ready(sys) || !d_x || !d_f || !d_energy) {
+    g_last_error = "awsem_fragmem_noalloc: null argument or uncommitted handle";
+    return AWSEM_EINVAL;
+  }
+  return guarded([&] {
+    CK(cudaSetDevice(sys->eng->device));
+    EngineBase::FMView v = sys->eng->fm_view();
+    fragmem_noalloc(sys->eng->device, v.n_res, v.row, v.rf, v.coef, v.uniform, v.nd, v.min_sep, v.sigma_sq,
+                    v.is_double, d_x, d_f, d_energy, (cudaStream_t) stream);
+  });
 }
 
 }  // extern "C"

@@ -186,6 +186,30 @@ int awsem_profile_step(awsem_system *sys, int reps, double *ms);
  * [7] non-uniform memory coefficients stored (0/1). */
 int awsem_model_info(awsem_system *sys, long long *info);
 
+/* Fragment-memory forces and energy through an entry point that allocates
+ * nothing: for callers that cannot call cudaMalloc when forces are needed
+ * (a host code that owns all device memory through its own pool, a step
+ * being recorded into a CUDA graph, an allocation-free real-time loop).
+ * No counterpart in the reference (its fragment-memory term,
+ * FixBackbone::compute_fragment_memory_potential, only runs inside the fix).
+ *
+ * d_x: device array [natoms][3] in the handle's internal order (per residue
+ * CA, CB or H-beta, O; residues in handle order); d_f: device array
+ * [natoms][3], overwritten with the fragment-memory forces; d_energy: one
+ * device double, overwritten with the fragment-memory energy; stream: a
+ * cudaStream_t (NULL: the default stream); the call is asynchronous on it.
+ * The handle's memory tables are used as they are resident since commit.
+ *
+ * Scratch: a fixed-size __device__ array of AWSEM_NOALLOC_MAX_ATOMS atoms
+ * (576 KiB, held by every GPU that loads the library until exit); larger
+ * handles are rejected with AWSEM_EINVAL.  The first call on a device looks
+ * up that array's device address (cudaGetSymbolAddress); make that first
+ * call before any stream capture.  All calls share the array and each
+ * clears what it uses first; calls whose kernels overlap on the GPU race on
+ * it and must be serialised by the caller. */
+#define AWSEM_NOALLOC_MAX_ATOMS 24576
+int awsem_fragmem_noalloc(awsem_system *sys, const double *d_x, double *d_f, double *d_energy, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
