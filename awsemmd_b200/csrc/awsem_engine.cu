@@ -115,8 +115,9 @@ void fragmem_noalloc(int device, int n_res, const int *row, const void *rf, cons
                      int min_sep, const double *sigma_sq, int is_double, const double *d_x, double *d_f,
                      double *d_energy, cudaStream_t stream);  // awsem_noalloc.cu
 
-static const char *kKernelNames[AWSEM_NKERNELS] = {"prepare", "nl_decide", "nl_build", "density", "residue",
-                                                   "water_xi", "pair", "fragmem", "bonds", "finish"};
+static const char *kKernelNames[AWSEM_NKERNELS] = {"prepare", "nl_decide", "nl_build", "density",
+                                                   "residue", "water_xi", "pair",      "hbond",
+                                                   "fragmem", "bonds",    "finish"};
 
 template <typename R> class Engine : public EngineBase {
 
@@ -127,7 +128,9 @@ template <typename R> class Engine : public EngineBase {
   DBuf<double> aps, tables, x, v, mass, g1, g2, ftot, work, e_res, energy;
   DBuf<double4> pos, cb_build;
   DBuf<unsigned long long> facc;
-  DBuf<int> nbr, ncount;
+  DBuf<int> nbr, ncount, hbq;
+  DBuf<long long> e_hb;
+  int hb_blocks = 1;
   DBuf<dev::NLState> nl;
   DBuf<long long> dstep;
   DBuf<double> ev_pref, ev_cs, ev_cl;
@@ -191,6 +194,8 @@ template <typename R> class Engine : public EngineBase {
     a.bur = w + 9 * nn;
     a.e_res = e_res.p;
     a.nbr = nbr.p;
+    a.hbq = hbq.p;
+    a.e_hb = e_hb.p;
     a.ncount = ncount.p;
     a.cap = cap;
     a.cb_build = cb_build.p;
@@ -317,8 +322,12 @@ template <typename R> class Engine : public EngineBase {
     long long s = step;
     CK(cudaMemcpyAsync(dstep.p, &s, sizeof s, cudaMemcpyHostToDevice, s0));
     // size the pair list from a first build
-    cap = 32;
-    nbr.alloc((size_t) cap * nn);
+    e_hb.alloc((size_t) 2 * nn);
+    e_hb.zero(s0);
+    int sms = 148;
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    hb_blocks = std::max(1, std::min((nn * 8 + 127) / 128, 16 * sms));
+    resize_list(32);
     for (int attempt = 0; attempt < 8; attempt++) {
       launch_prepare_and_list(args(groups_all), s0, true, false);
       dev::NLState got;
@@ -347,8 +356,11 @@ template <typename R> class Engine : public EngineBase {
 
   void resize_list(int newcap)
   {
+    // list slots (residue * cap + k) are int indices in the hydrogen-bond queues
+    if ((long long) newcap * n() >= (1ll << 31)) throw std::invalid_argument("residue pair list exceeds 2^31 slots");
     cap = newcap;
     nbr.alloc((size_t) cap * n());
+    hbq.alloc((size_t) 2 * cap * n());
     dev::NLState st;
     CK(cudaMemcpyAsync(&st, nl.p, sizeof st, cudaMemcpyDeviceToHost, s0));
     CK(cudaStreamSynchronize(s0));
@@ -386,6 +398,7 @@ template <typename R> class Engine : public EngineBase {
     dev::k_residue<R><<<nb, tb, 0, s0>>>(a, p);
     dev::k_water_xi<R><<<wb, tb, 0, s0>>>(a, p);
     dev::k_pair<R><<<wb, tb, 0, s0>>>(a, p);
+    dev::k_hbond<R><<<hb_blocks, 128, 0, s0>>>(a, p);
     if (a.groups & dev::G_BOND) dev::k_bonds<R><<<nb, tb, 0, s0>>>(a);
     if (fm) CK(cudaStreamWaitEvent(s0, ev_join, 0));
   }
@@ -402,7 +415,7 @@ template <typename R> class Engine : public EngineBase {
   void reduce_energies()
   {
     dim3 grid(E_SLOTS, n_sys());
-    dev::k_energy_reduce<<<grid, 256, 0, s0>>>(e_res.p, n(), sys_begin.p, sys_end.p, energy.p);
+    dev::k_energy_reduce<<<grid, 256, 0, s0>>>(e_res.p, e_hb.p, n(), sys_begin.p, sys_end.p, energy.p);
   }
 
   void need_single(const char *what)
@@ -513,7 +526,7 @@ template <typename R> class Engine : public EngineBase {
       launch_eval(a, true);
       dev::k_finish<R><<<nb, tb, 0, s0>>>(a, d_integ.p, g1.p, g2.p, ftot.p, x.p);
       if (thermo)
-        dev::k_thermo<<<n_sys(), 256, 0, s0>>>(e_res.p, nn, dstep.p, d_integ.p, sys_begin.p, sys_end.p,
+        dev::k_thermo<<<n_sys(), 256, 0, s0>>>(e_res.p, e_hb.p, nn, dstep.p, d_integ.p, sys_begin.p, sys_end.p,
                                                thermo_nrows, thermo_rows.p);
     }
     CK(cudaStreamEndCapture(s0, &graph));
@@ -564,9 +577,10 @@ template <typename R> class Engine : public EngineBase {
           case 4: dev::k_residue<R><<<nb, tb, 0, s0>>>(a, p); break;
           case 5: dev::k_water_xi<R><<<wb, tb, 0, s0>>>(a, p); break;
           case 6: dev::k_pair<R><<<wb, tb, 0, s0>>>(a, p); break;
-          case 7: if (fm) dev::k_fragmem<R><<<wb, tb, 0, s0>>>(a, p); break;
-          case 8: dev::k_bonds<R><<<nb, tb, 0, s0>>>(a); break;
-          case 9: dev::k_finish<R><<<nb, tb, 0, s0>>>(a, d_integ.p, g1.p, g2.p, ftot.p, x.p); break;
+          case 7: dev::k_hbond<R><<<hb_blocks, 128, 0, s0>>>(a, p); break;
+          case 8: if (fm) dev::k_fragmem<R><<<wb, tb, 0, s0>>>(a, p); break;
+          case 9: dev::k_bonds<R><<<nb, tb, 0, s0>>>(a); break;
+          case 10: dev::k_finish<R><<<nb, tb, 0, s0>>>(a, d_integ.p, g1.p, g2.p, ftot.p, x.p); break;
         }
         CK(cudaEventRecord(ev[2 * k + 1], s0));
       }

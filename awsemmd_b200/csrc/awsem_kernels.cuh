@@ -35,6 +35,9 @@ struct NLState {
   int overflow;       // max neighbour count seen when it exceeded capacity
   float skin;
   float r_contact, r_dssp, r_pap, r_ev;  // term cutoffs on the bead pairs they test
+  float bCAx;         // max distance of a residue's CB or O from its own CA (this step)
+  float ev_pre_sq;    // CA-CA distance^2 beyond which no bead pair of two residues is in excluded-volume range
+  int n_dssp, n_pap;  // hydrogen-bond queue lengths of the current evaluation
 };
 
 template <typename R> struct StepArgs {
@@ -51,6 +54,11 @@ template <typename R> struct StepArgs {
   int *nbr, *ncount, cap;
   double4 *cb_build;
   NLState *nl;
+  // hydrogen-bond work queues: list slots (residue * cap + k) of the DSSP
+  // candidates in [0, n_res*cap) and of the P_AP candidates after them;
+  // their energies per residue in 2^-32 fixed point, [2][n_res]
+  int *hbq;
+  long long *e_hb;
   // excluded volume
   int ntypes, ev_p;
   const double *ev_pref, *ev_cs, *ev_cl;
@@ -82,7 +90,7 @@ __device__ __forceinline__ void atomic_max_f(float *addr, float v)
 template <typename R> __global__ void k_prepare(StepArgs<R> a, FFParams p)
 {
   int r = blockIdx.x * blockDim.x + threadIdx.x;
-  float d2 = 0.f, oO = 0.f, oN = 0.f, oCA = 0.f, oAll = 0.f;
+  float d2 = 0.f, oO = 0.f, oN = 0.f, oCA = 0.f, oAll = 0.f, oX = 0.f;
   if (r < a.s.n_res) {
     const double *x = a.x;
     int fl = a.s.res_flags[r];
@@ -114,6 +122,14 @@ template <typename R> __global__ void k_prepare(StepArgs<R> a, FFParams p)
     w[B_CP] = make_double4(cp[0], cp[1], cp[2], 0.0);
     unsigned long long *f = a.s.facc + (size_t) 9 * r;
     for (int k = 0; k < 9; k++) f[k] = 0ull;
+    a.e_hb[r] = 0;
+    a.e_hb[(size_t) a.s.n_res + r] = 0;
+    {
+      // reach of the residue's beads around its CA (excluded-volume prefilter)
+      double ux = cb[0] - ca[0], uy = cb[1] - ca[1], uz = cb[2] - ca[2];
+      double wx = o[0] - ca[0], wy = o[1] - ca[1], wz = o[2] - ca[2];
+      oX = (float) sqrt(fmax(ux * ux + uy * uy + uz * uz, wx * wx + wy * wy + wz * wz));
+    }
     // list-validity data: contact-bead displacement and bead offsets
     const double *c = (fl & R_GLY) ? ca : cb;
     double4 b0 = a.cb_build[r];
@@ -135,6 +151,7 @@ template <typename R> __global__ void k_prepare(StepArgs<R> a, FFParams p)
     oN = fmaxf(oN, __shfl_xor_sync(0xffffffffu, oN, s));
     oCA = fmaxf(oCA, __shfl_xor_sync(0xffffffffu, oCA, s));
     oAll = fmaxf(oAll, __shfl_xor_sync(0xffffffffu, oAll, s));
+    oX = fmaxf(oX, __shfl_xor_sync(0xffffffffu, oX, s));
   }
   if ((threadIdx.x & 31) == 0) {
     atomic_max_f(&a.nl->d2max, d2);
@@ -142,6 +159,7 @@ template <typename R> __global__ void k_prepare(StepArgs<R> a, FFParams p)
     atomic_max_f(&a.nl->bN, oN);
     atomic_max_f(&a.nl->bCA, oCA);
     atomic_max_f(&a.nl->bAll, oAll);
+    atomic_max_f(&a.nl->bCAx, oX);
   }
 }
 
@@ -165,7 +183,12 @@ __global__ void k_nl_decide(NLState *nl, int force, long long *step)
     s.steps_since++;
   }
   s.rebuild = rb;
-  s.d2max = s.bO = s.bN = s.bCA = s.bAll = 0.f;
+  // two residues whose CAs are farther apart than r_ev + 2 * reach have no
+  // bead pair inside any excluded-volume cutoff (0.01 A covers rounding)
+  float pre = s.r_ev + 2.f * s.bCAx + 0.01f;
+  s.ev_pre_sq = pre * pre;
+  s.d2max = s.bO = s.bN = s.bCA = s.bAll = s.bCAx = 0.f;
+  s.n_dssp = s.n_pap = 0;
 }
 
 template <typename R> __device__ __forceinline__ V3<double> contact(const DevSys<R> &s, int r)
@@ -394,17 +417,20 @@ template <typename R> __global__ void k_water_xi(StepArgs<R> a, FFParams p)
 
 // DL3: main pair loop (fix_backbone.cpp:7956-8134) plus excluded volume
 // between residues.  Radial contact forces and excluded volume act on the
-// owner's beads only (each pair is visited from both sides); DSSP and P_AP
-// are visited once and scatter.
-template <typename R> __global__ void k_pair(StepArgs<R> a, FFParams p)
+// owner's beads only (each pair is visited from both sides).  DSSP and P_AP
+// pairs are only detected here (cheap distance and index tests) and queued;
+// k_hbond evaluates them one thread per pair, so their long, branchy bodies
+// neither serialise this warp nor inflate its register count.
+template <typename R> __global__ void __launch_bounds__(128) k_pair(StepArgs<R> a, FFParams p)
 {
   int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   const DevSys<R> &s = a.s;
   if (i >= s.n_res) return;
   int n = s.n_res, fli = s.res_flags[i], chi = s.res_chain[i], ti = s.res_type[i];
-  int cbi = (fli & R_GLY) ? B_CA : B_CB;
+  // (arrays below are only indexed by unrolled constants: they stay in registers)
+  const bool gly_i = fli & R_GLY;
   V3<double> bi[3] = {bead(s, i, B_CA), bead(s, i, B_CB), bead(s, i, B_O)};
-  V3<double> ci = bi[cbi];
+  V3<double> ci = gly_i ? bi[0] : bi[1];
   V3<double> oi = bi[2];
   int tat[3] = {a.atom_type[3 * i], a.atom_type[3 * i + 1], a.atom_type[3 * i + 2]};
   double xi_i = a.xi_w[i], bur_i = a.bur[i], x1_i = a.xi1[i];
@@ -412,13 +438,22 @@ template <typename R> __global__ void k_pair(StepArgs<R> a, FFParams p)
   double x2_i = i - dh >= 0 ? a.xi2[i - dh] : 0.0;
   double sw_i = a.sig_w[i];
   long long F[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
-  double e_water = 0.0, e_ev = 0.0, e_dssp = 0.0, e_pap = 0.0;
+  long long Fc[3] = {0, 0, 0};  // contact-bead radial forces
+  double e_water = 0.0, e_ev = 0.0;
   const double *WG = s.tables + TB_WATER;
   const bool fix = a.groups & G_FIX, evon = a.groups & G_PAIR;
   uint32_t T = fix ? p.terms : 0u;
   int cnt = a.ncount[i];
   const int *nb = a.nbr + (size_t) i * a.cap;
-  for (int k = lane; k < cnt; k += 32) {
+  const R ev_pre_sq = R(a.nl->ev_pre_sq);
+  // smallest same-chain separation of any P_AP class (fix_backbone.cpp:3279-3383)
+  const int pap_sep = min(p.i_med_min + 2 * p.i_diff_pap, p.i_med_max + 1);
+  const bool dssp_i = (T & T_DSSP) && !(fli & R_LAST);
+  const size_t qcap = (size_t) n * a.cap;
+  for (int k0 = 0; k0 < cnt; k0 += 32) {
+    const int k = k0 + lane;
+    bool q_dssp = false, q_pap = false;
+    if (k < cnt) {
     int j = nb[k];
     int flj = s.res_flags[j];
     bool other = s.res_chain[j] != chi;
@@ -472,21 +507,24 @@ template <typename R> __global__ void k_pair(StepArgs<R> a, FFParams p)
         }
       }
       if (force != R(0)) {
-        F[cbi][0] += fix_force((double) (force * d.x));
-        F[cbi][1] += fix_force((double) (force * d.y));
-        F[cbi][2] += fix_force((double) (force * d.z));
+        Fc[0] += fix_force((double) (force * d.x));
+        Fc[1] += fix_force((double) (force * d.y));
+        Fc[2] += fix_force((double) (force * d.z));
       }
     }
+    const R rca2 = (evon || (T & T_PAP)) ? norm2(diff<R>(bi[0], bead(s, j, B_CA))) : R(0);
     // excluded volume between beads of i and j (1-2 bonded pairs removed)
-    if (evon) {
+    if (evon && rca2 < ev_pre_sq) {
       unsigned excl = 0;
       if (j == i + 1) excl = a.excl_next[i];
       bool prev = j == i - 1;
       unsigned exclp = prev ? a.excl_next[j] : 0u;
       bool shortr = !other && dij < 5;
+#pragma unroll
       for (int b1 = 0; b1 < 3; b1++) {
         V3<double> bj = bead(s, j, b1);
         int tb = a.atom_type[3 * j + b1];
+#pragma unroll
         for (int b0 = 0; b0 < 3; b0++) {
           if (excl & (1u << (b0 * 3 + b1))) continue;
           if (exclp & (1u << (b1 * 3 + b0))) continue;
@@ -501,32 +539,66 @@ template <typename R> __global__ void k_pair(StepArgs<R> a, FFParams p)
       }
     }
     // DSSP with O(i) as acceptor and N-H(j) as donor (fix_backbone.cpp:8064-8079)
-    if ((T & T_DSSP) && (other || dij > 2) && !(flj & R_PRO) && !(fli & R_LAST) && !(flj & R_FIRST)) {
-      V3<R> d = diff<R>(oi, bead(s, j, B_N));
-      if (norm2(d) < R(p.dssp_cut_sq)) e_dssp += (double) dssp_term(s, p, i, j);
-    }
+    if (dssp_i && (other || dij > 2) && !(flj & R_PRO) && !(flj & R_FIRST))
+      q_dssp = norm2(diff<R>(oi, bead(s, j, B_N))) < R(p.dssp_cut_sq);
     // P_AP on CA pairs, visited from the lower residue (fix_backbone.cpp:8096-8103)
-    if ((T & T_PAP) && upper) {
-      V3<R> d = diff<R>(bi[0], bead(s, j, B_CA));
-      if (norm2(d) < R(p.pap_cutoff_sq)) e_pap += (double) pap_term(s, p, i, j);
+    if ((T & T_PAP) && upper && (other || j - i >= pap_sep)) q_pap = rca2 < R(p.pap_cutoff_sq);
+    }
+    // append this round's candidates to the queues (one atomic per warp and kind)
+    const unsigned md = __ballot_sync(0xffffffffu, q_dssp), mp = __ballot_sync(0xffffffffu, q_pap);
+    if (md | mp) {
+      int bd = 0, bp = 0;
+      if (lane == 0) {
+        if (md) bd = atomicAdd(&a.nl->n_dssp, __popc(md));
+        if (mp) bp = atomicAdd(&a.nl->n_pap, __popc(mp));
+      }
+      bd = __shfl_sync(0xffffffffu, bd, 0);
+      bp = __shfl_sync(0xffffffffu, bp, 0);
+      const unsigned below = (1u << lane) - 1u;
+      const int slot = i * a.cap + k;
+      if (q_dssp) a.hbq[bd + __popc(md & below)] = slot;
+      if (q_pap) a.hbq[qcap + bp + __popc(mp & below)] = slot;
     }
   }
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    F[0][c] += gly_i ? Fc[c] : 0ll;
+    F[1][c] += gly_i ? 0ll : Fc[c];
+  }
+#pragma unroll
   for (int b = 0; b < 3; b++)
+#pragma unroll
     for (int c = 0; c < 3; c++) F[b][c] = warp_sum(F[b][c]);
   e_water = warp_sum(e_water);
   e_ev = warp_sum(e_ev);
-  e_dssp = warp_sum(e_dssp);
-  e_pap = warp_sum(e_pap);
   if (lane == 0) {
     unsigned long long *f = s.facc + (size_t) 9 * i;
+#pragma unroll
     for (int b = 0; b < 3; b++)
+#pragma unroll
       for (int c = 0; c < 3; c++)
         if (F[b][c]) atomicAdd(f + 3 * b + c, (unsigned long long) F[b][c]);
     double *E = a.e_res;
     E[(size_t) E_WATER * n + i] = e_water;
     E[(size_t) E_PAIR * n + i] += e_ev;
-    E[(size_t) E_DSSP * n + i] = e_dssp;
-    E[(size_t) E_PAP * n + i] = e_pap;
+  }
+}
+
+// DSSP hydrogen bonds and P_AP of the queued pairs, one thread per pair
+// (grid-stride over both queues).  Forces scatter with fixed-point atomics;
+// each pair's energy goes to its first residue in fixed point, so the sums
+// do not depend on the queue order.
+template <typename R> __global__ void __launch_bounds__(128) k_hbond(StepArgs<R> a, FFParams p)
+{
+  const DevSys<R> &s = a.s;
+  const int nd = a.nl->n_dssp, np = a.nl->n_pap, n = s.n_res;
+  const size_t qcap = (size_t) n * a.cap;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nd + np; t += gridDim.x * blockDim.x) {
+    const bool d = t < nd;
+    const int slot = d ? a.hbq[t] : a.hbq[qcap + (t - nd)];
+    const int i = slot / a.cap, j = a.nbr[slot];
+    R e = d ? dssp_term(s, p, i, j) : pap_term(s, p, i, j);
+    if (e != R(0)) atomicAdd((unsigned long long *) (a.e_hb + (d ? 0 : (size_t) n) + i), (unsigned long long) fix_force((double) e));
   }
 }
 
@@ -706,8 +778,8 @@ template <typename R> __global__ void k_total_force(StepArgs<R> a, double *ftot)
 
 // Thermo row of the current step: [fix total, vexcluded, bonds, kinetic],
 // residue sums in a fixed tree order (one block of 256 threads).
-__global__ void k_thermo(const double *e_res, int n_res, const long long *step, const Integrator *inp,
-                         const int *sys_begin, const int *sys_end, long long nrows, double *rows)
+__global__ void k_thermo(const double *e_res, const long long *e_hb, int n_res, const long long *step,
+                         const Integrator *inp, const int *sys_begin, const int *sys_end, long long nrows, double *rows)
 {
   const long long begin = inp->begin;
   const int rep = blockIdx.x;
@@ -716,6 +788,7 @@ __global__ void k_thermo(const double *e_res, int n_res, const long long *step, 
   for (int r = sys_begin[rep] + threadIdx.x; r < sys_end[rep]; r += blockDim.x) {
     double fx = 0.0;
     for (int t = 1; t < E_FIX_TERMS; t++) fx += e_res[(size_t) t * n_res + r];
+    fx += (double) (e_hb[r] + e_hb[(size_t) n_res + r]) * F_UNSCALE;
     acc[0] += fx;
     acc[1] += e_res[(size_t) E_PAIR * n_res + r];
     acc[2] += e_res[(size_t) E_BOND * n_res + r];
@@ -736,12 +809,16 @@ __global__ void k_thermo(const double *e_res, int n_res, const long long *step, 
 
 // Per-term sums of each replica's residues in a fixed tree order
 // (block (t, rep) sums energy slot t of replica rep)
-__global__ void k_energy_reduce(const double *e_res, int n_res, const int *sys_begin, const int *sys_end, double *out)
+__global__ void k_energy_reduce(const double *e_res, const long long *e_hb, int n_res, const int *sys_begin,
+                                const int *sys_end, double *out)
 {
   const int t = blockIdx.x, rep = blockIdx.y;
   __shared__ double sh[256];
   double acc = 0.0;
-  for (int r = sys_begin[rep] + threadIdx.x; r < sys_end[rep]; r += blockDim.x) acc += e_res[(size_t) t * n_res + r];
+  // DSSP and P_AP energies are kept in fixed point (queue order independent)
+  const long long *fx = t == E_DSSP ? e_hb : t == E_PAP ? e_hb + n_res : nullptr;
+  for (int r = sys_begin[rep] + threadIdx.x; r < sys_end[rep]; r += blockDim.x)
+    acc += fx ? (double) fx[r] * F_UNSCALE : e_res[(size_t) t * n_res + r];
   sh[threadIdx.x] = acc;
   __syncthreads();
   for (int w = blockDim.x / 2; w > 0; w >>= 1) {

@@ -28,6 +28,7 @@ FP64 = 0
 MIXED = 1
 TERMS_FIX, TERMS_PAIR, TERMS_BOND = 1, 2, 4
 TERMS_ALL = 7
+NKERNELS = 11  # AWSEM_NKERNELS: kernels of one MD step, in launch order
 
 ENERGY_NAMES = ["total", "chain", "shake", "chi", "rama", "excluded", "dssp", "p_ap", "water", "burial",
                 "helix", "amh_go", "frag_mem", "vec_fm", "contact_restraints", "membrane", "ssb", "dh",
@@ -204,9 +205,9 @@ class AwsemSystem:
         return float(self.lib.awsem_last_run_ms(self.h))
 
     def profile_step(self, reps: int = 20) -> dict:
-        ms = np.zeros(10)
+        ms = np.zeros(NKERNELS)
         _check(self.lib, self.lib.awsem_profile_step(self.h, reps, _ptr(ms)), "awsem_profile_step")
-        return {self.lib.awsem_kernel_name(k).decode(): float(ms[k]) for k in range(10)}
+        return {self.lib.awsem_kernel_name(k).decode(): float(ms[k]) for k in range(NKERNELS)}
 
     def model_info(self) -> np.ndarray:
         info = np.zeros(8, dtype=np.int64)
