@@ -100,20 +100,11 @@ class EngineBase {
   virtual void model_info(long long *info) = 0;
   virtual double run_ms() const = 0;
   // device-resident fragment-memory table, for entry points outside the engine
-  struct FMView {
-    const int *row;
-    const void *rf, *coef;  // element type: double (FP64 form) or float (mixed form)
-    double uniform;
-    int nd, min_sep, n_res, is_double;
-    const int *res_flags;
-    const double *sigma_sq;  // host table [64]
-  };
   virtual FMView fm_view() const = 0;
 };
 
-void fragmem_noalloc(int device, int n_res, const int *row, const void *rf, const void *coef, double uniform, int nd,
-                     int min_sep, const double *sigma_sq, int is_double, const double *d_x, double *d_f,
-                     double *d_energy, cudaStream_t stream);  // awsem_noalloc.cu
+void fragmem_noalloc(int device, const FMView &v, const double *d_x, double *d_f, double *d_energy,
+                     cudaStream_t stream);  // awsem_noalloc.cu
 
 static const char *kKernelNames[AWSEM_NKERNELS] = {"prepare", "nl_decide", "nl_build", "density",
                                                    "residue", "water_xi", "pair",      "hbond",
@@ -129,7 +120,7 @@ template <typename R> class Engine : public EngineBase {
   DBuf<double4> pos, cb_build;
   DBuf<unsigned long long> facc;
   DBuf<int> nbr, ncount, hbq;
-  DBuf<long long> e_hb;
+  DBuf<long long> e_fix;
   int hb_blocks = 1;
   DBuf<dev::NLState> nl;
   DBuf<long long> dstep;
@@ -137,8 +128,9 @@ template <typename R> class Engine : public EngineBase {
   DBuf<unsigned> excl_self, excl_next;
   DBuf<int> bond_start, bond_i, bond_j;
   DBuf<double> bond_k, bond_r0;
-  DBuf<int> fm_row;
+  DBuf<int> fm_soff, fm_slen;
   DBuf<R> fm_rf, fm_coef;
+  int fm_groups = 0, fm_dsplit = 1;
   DBuf<double> thermo_rows;
   DBuf<int> res_sys, sys_begin, sys_end;
   DBuf<unsigned long long> sys_seed;
@@ -195,7 +187,7 @@ template <typename R> class Engine : public EngineBase {
     a.e_res = e_res.p;
     a.nbr = nbr.p;
     a.hbq = hbq.p;
-    a.e_hb = e_hb.p;
+    a.e_fix = e_fix.p;
     a.ncount = ncount.p;
     a.cap = cap;
     a.cb_build = cb_build.p;
@@ -213,10 +205,15 @@ template <typename R> class Engine : public EngineBase {
     a.bond_j = bond_j.p;
     a.bond_k = bond_k.p;
     a.bond_r0 = bond_r0.p;
-    a.fm_row = fm_row.p;
-    a.fm_rf = fm_rf.p;
-    a.fm_coef = in.fm.uniform ? nullptr : fm_coef.p;
-    a.fm_uniform = in.fm.uniform_coef;
+    a.fm.soff = fm_soff.p;
+    a.fm.slen = fm_slen.p;
+    a.fm.rf = fm_rf.p;
+    a.fm.coef = in.fm.uniform ? nullptr : fm_coef.p;
+    a.fm.uniform = in.fm.uniform_coef;
+    a.fm.nd = in.ff.p.fm_nd;
+    a.fm.min_sep = in.ff.p.fm_min_sep;
+    a.fm.groups = fm_groups;
+    a.fm.dsplit = fm_dsplit;
     a.groups = groups;
     a.step = dstep.p;
     a.res_sys = res_sys.p;
@@ -293,15 +290,8 @@ template <typename R> class Engine : public EngineBase {
     bond_j.upload(bj, s0);
     bond_k.upload(bk, s0);
     bond_r0.upload(br, s0);
-    // fragment memory in the engine's arithmetic type
-    const FMTable &fm = in.fm;
-    std::vector<int> rows = fm.row_start;
-    if (rows.empty()) rows.assign((size_t) nn * std::max(fm.nd, 1) + 1, 0);
-    fm_row.upload(rows, s0);
-    std::vector<R> rf(fm.rf.begin(), fm.rf.end()), cf(fm.coef.begin(), fm.coef.end());
-    fm_rf.upload(rf, s0);
-    fm_coef.upload(cf, s0);
     if (!(in.ff.p.terms & T_FM)) in.ff.p.fm_nd = 0;
+    upload_fm_slices();
     // pair-list radii of the terms
     dev::NLState st{};
     const FFParams &p = in.ff.p;
@@ -322,8 +312,8 @@ template <typename R> class Engine : public EngineBase {
     long long s = step;
     CK(cudaMemcpyAsync(dstep.p, &s, sizeof s, cudaMemcpyHostToDevice, s0));
     // size the pair list from a first build
-    e_hb.alloc((size_t) 2 * nn);
-    e_hb.zero(s0);
+    e_fix.alloc((size_t) 3 * nn);
+    e_fix.zero(s0);
     int sms = 148;
     CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
     hb_blocks = std::max(1, std::min((nn * 8 + 127) / 128, 16 * sms));
@@ -391,7 +381,7 @@ template <typename R> class Engine : public EngineBase {
       // fragment memory is independent of the pair passes: second stream
       CK(cudaEventRecord(ev_fork, s0));
       CK(cudaStreamWaitEvent(s1, ev_fork, 0));
-      dev::k_fragmem<R><<<wb, tb, 0, s1>>>(a, p);
+      dev::k_fragmem<R><<<fm_blocks(), tb, 0, s1>>>(a, p);
       CK(cudaEventRecord(ev_join, s1));
     }
     dev::k_density<R><<<wb, tb, 0, s0>>>(a, p);
@@ -415,7 +405,7 @@ template <typename R> class Engine : public EngineBase {
   void reduce_energies()
   {
     dim3 grid(E_SLOTS, n_sys());
-    dev::k_energy_reduce<<<grid, 256, 0, s0>>>(e_res.p, e_hb.p, n(), sys_begin.p, sys_end.p, energy.p);
+    dev::k_energy_reduce<<<grid, 256, 0, s0>>>(e_res.p, e_fix.p, n(), sys_begin.p, sys_end.p, energy.p);
   }
 
   void need_single(const char *what)
@@ -526,7 +516,7 @@ template <typename R> class Engine : public EngineBase {
       launch_eval(a, true);
       dev::k_finish<R><<<nb, tb, 0, s0>>>(a, d_integ.p, g1.p, g2.p, ftot.p, x.p);
       if (thermo)
-        dev::k_thermo<<<n_sys(), 256, 0, s0>>>(e_res.p, e_hb.p, nn, dstep.p, d_integ.p, sys_begin.p, sys_end.p,
+        dev::k_thermo<<<n_sys(), 256, 0, s0>>>(e_res.p, e_fix.p, nn, dstep.p, d_integ.p, sys_begin.p, sys_end.p,
                                                thermo_nrows, thermo_rows.p);
     }
     CK(cudaStreamEndCapture(s0, &graph));
@@ -578,7 +568,7 @@ template <typename R> class Engine : public EngineBase {
           case 5: dev::k_water_xi<R><<<wb, tb, 0, s0>>>(a, p); break;
           case 6: dev::k_pair<R><<<wb, tb, 0, s0>>>(a, p); break;
           case 7: dev::k_hbond<R><<<hb_blocks, 128, 0, s0>>>(a, p); break;
-          case 8: if (fm) dev::k_fragmem<R><<<wb, tb, 0, s0>>>(a, p); break;
+          case 8: if (fm) dev::k_fragmem<R><<<fm_blocks(), tb, 0, s0>>>(a, p); break;
           case 9: dev::k_bonds<R><<<nb, tb, 0, s0>>>(a); break;
           case 10: dev::k_finish<R><<<nb, tb, 0, s0>>>(a, d_integ.p, g1.p, g2.p, ftot.p, x.p); break;
         }
@@ -602,18 +592,69 @@ template <typename R> class Engine : public EngineBase {
   FMView fm_view() const override
   {
     FMView v;
-    v.row = fm_row.p;
+    v.soff = fm_soff.p;
+    v.slen = fm_slen.p;
     v.rf = fm_rf.p;
     v.coef = in.fm.uniform ? nullptr : fm_coef.p;
     v.uniform = in.fm.uniform_coef;
     v.nd = in.ff.p.fm_nd;
     v.min_sep = in.ff.p.fm_min_sep;
+    v.groups = fm_groups;
+    v.dsplit = fm_dsplit;
     v.n_res = n();
     v.is_double = sizeof(R) == sizeof(double);
-    v.res_flags = res_flags.p;
     v.sigma_sq = in.ff.p.fm_sigma_sq;
     return v;
   }
+
+  // Fragment-memory table in the sliced, lane-interleaved layout of
+  // awsem_fragmem.cuh, in the engine's arithmetic type.
+  void upload_fm_slices()
+  {
+    const FMTable &fm = in.fm;
+    const int nn = n(), nd = in.ff.p.fm_nd;
+    fm_groups = (nn + 31) / 32;
+    std::vector<int> soff((size_t) fm_groups * std::max(nd, 1), 0), slen(soff.size(), 0);
+    long long stripes = 0;
+    for (int g = 0; g < fm_groups; g++)
+      for (int d = 0; d < nd; d++) {
+        int len = 0;
+        for (int l = 0; l < 32 && 32 * g + l < nn; l++) {
+          size_t row = (size_t) (32 * g + l) * fm.nd + d;
+          len = std::max(len, fm.row_start[row + 1] - fm.row_start[row]);
+        }
+        soff[(size_t) g * nd + d] = (int) stripes;
+        slen[(size_t) g * nd + d] = len;
+        stripes += len;
+      }
+    if (stripes * 32 * 4 >= (1ll << 31)) throw std::invalid_argument("fragment memory table exceeds 2^31 distances");
+    const bool coef = !fm.uniform;
+    std::vector<R> rf((size_t) stripes * 32 * 4, R(FMTable::FM_SKIP)), cf(coef ? (size_t) stripes * 32 : 0, R(0));
+    for (int g = 0; g < fm_groups; g++)
+      for (int d = 0; d < nd; d++) {
+        const size_t s0b = soff[(size_t) g * nd + d];
+        for (int l = 0; l < 32 && 32 * g + l < nn; l++) {
+          size_t row = (size_t) (32 * g + l) * fm.nd + d;
+          for (int m = 0, rec = fm.row_start[row]; rec < fm.row_start[row + 1]; m++, rec++) {
+            size_t at = (s0b + m) * 32 + l;
+            for (int k = 0; k < 4; k++) rf[at * 4 + k] = (R) fm.rf[(size_t) rec * 4 + k];
+            if (coef) cf[at] = (R) fm.coef[rec];
+          }
+        }
+      }
+    fm_soff.upload(soff, s0);
+    fm_slen.upload(slen, s0);
+    fm_rf.upload(rf, s0);
+    fm_coef.upload(cf, s0);
+    // enough warps to fill the GPU on small systems: split each group's
+    // separations over several warps when there are few groups
+    int sms = 148;
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    fm_dsplit = std::max(1, std::min(std::max(nd, 1), (16 * sms + fm_groups - 1) / std::max(fm_groups, 1)));
+    CK(cudaStreamSynchronize(s0));  // host vectors go out of scope
+  }
+
+  int fm_blocks() const { return (fm_groups * fm_dsplit * 32 + 127) / 128; }
 
   void model_info(long long *info) override
   {
@@ -1052,9 +1093,7 @@ int awsem_fragmem_noalloc(awsem_system *sys, const double *d_x, double *d_f, dou
   }
   return guarded([&] {
     CK(cudaSetDevice(sys->eng->device));
-    EngineBase::FMView v = sys->eng->fm_view();
-    fragmem_noalloc(sys->eng->device, v.n_res, v.row, v.rf, v.coef, v.uniform, v.nd, v.min_sep, v.sigma_sq,
-                    v.is_double, d_x, d_f, d_energy, (cudaStream_t) stream);
+    fragmem_noalloc(sys->eng->device, sys->eng->fm_view(), d_x, d_f, d_energy, (cudaStream_t) stream);
   });
 }
 

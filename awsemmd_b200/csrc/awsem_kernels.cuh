@@ -10,8 +10,10 @@
 //                helical (i,i+4) pairs (:7843-7868), chain/chi/rama
 //   water_xi     warp/residue: xi_water (DL2, :7877-7954)
 //   pair         warp/residue: water/burial/helix radial forces, excluded
-//                volume, DSSP hydrogen bonds, P_AP (DL3, :7956-8134)
-//   fragmem      warp/residue: fragment-memory Gaussians (:4079-4177)
+//                volume (DL3, :7956-8134); queues DSSP and P_AP pairs
+//   hbond        thread/queued pair: DSSP hydrogen bonds, P_AP
+//   fragmem      warp/32 residues, lane/residue row: fragment-memory
+//                Gaussians (:4079-4177), on a second stream
 //   bonds        thread/residue: harmonic bonds
 //   finish       thread/residue: fixed-point -> FP64 forces, Langevin,
 //                velocity-Verlet half kicks and drift
@@ -20,6 +22,7 @@
 #pragma once
 
 #include "awsem_device.cuh"
+#include "awsem_fragmem.cuh"
 
 namespace awsem {
 namespace dev {
@@ -55,10 +58,11 @@ template <typename R> struct StepArgs {
   double4 *cb_build;
   NLState *nl;
   // hydrogen-bond work queues: list slots (residue * cap + k) of the DSSP
-  // candidates in [0, n_res*cap) and of the P_AP candidates after them;
-  // their energies per residue in 2^-32 fixed point, [2][n_res]
+  // candidates in [0, n_res*cap) and of the P_AP candidates after them
   int *hbq;
-  long long *e_hb;
+  // energies summed by several threads per residue, in 2^-32 fixed point
+  // (sums independent of order): [0] DSSP, [1] P_AP, [2] fragment memory
+  long long *e_fix;
   // excluded volume
   int ntypes, ev_p;
   const double *ev_pref, *ev_cs, *ev_cl;
@@ -68,11 +72,8 @@ template <typename R> struct StepArgs {
   const int *bond_start, *bond_i, *bond_j;
   const double *bond_k, *bond_r0;
   // fragment memory
-  const int *fm_row;
-  const R *fm_rf;
-  const R *fm_coef;  // nullptr when uniform
-  double fm_uniform;
-  int groups;        // AWSEM_TERMS_* bits: 1 fix backbone, 2 pair vexcluded, 4 bonds
+  FMSlices<R> fm;
+  int groups;       // AWSEM_TERMS_* bits: 1 fix backbone, 2 pair vexcluded, 4 bonds
   long long *step;   // device step counter (advanced by k_nl_decide)
   // replicas: residue -> replica, replica residue ranges, Langevin seeds
   const int *res_sys, *sys_begin, *sys_end;
@@ -122,8 +123,7 @@ template <typename R> __global__ void k_prepare(StepArgs<R> a, FFParams p)
     w[B_CP] = make_double4(cp[0], cp[1], cp[2], 0.0);
     unsigned long long *f = a.s.facc + (size_t) 9 * r;
     for (int k = 0; k < 9; k++) f[k] = 0ull;
-    a.e_hb[r] = 0;
-    a.e_hb[(size_t) a.s.n_res + r] = 0;
+    for (int k = 0; k < 3; k++) a.e_fix[(size_t) k * a.s.n_res + r] = 0;
     {
       // reach of the residue's beads around its CA (excluded-volume prefilter)
       double ux = cb[0] - ca[0], uy = cb[1] - ca[1], uz = cb[2] - ca[2];
@@ -598,85 +598,23 @@ template <typename R> __global__ void __launch_bounds__(128) k_hbond(StepArgs<R>
     const int slot = d ? a.hbq[t] : a.hbq[qcap + (t - nd)];
     const int i = slot / a.cap, j = a.nbr[slot];
     R e = d ? dssp_term(s, p, i, j) : pap_term(s, p, i, j);
-    if (e != R(0)) atomicAdd((unsigned long long *) (a.e_hb + (d ? 0 : (size_t) n) + i), (unsigned long long) fix_force((double) e));
+    if (e != R(0))
+      atomicAdd((unsigned long long *) (a.e_fix + (d ? 0 : (size_t) n) + i), (unsigned long long) fix_force((double) e));
   }
 }
 
-// Fragment memory (fix_backbone.cpp:4079-4177) in pair-major form: for target
-// residue i and separation d, lane l handles atom pair k = l & 3 of every
-// eighth memory record of the row; lanes with equal k are then combined.
-template <typename R> __global__ void k_fragmem(StepArgs<R> a, FFParams p)
+// Fragment memory: sliced lane-interleaved table, lane per residue row
+// (awsem_fragmem.cuh)
+template <typename R> struct BeadPos {
+  const DevSys<R> *s;
+  __device__ __forceinline__ V3<double> operator()(int r, int b) const { return bead(*s, r, b ? B_CB : B_CA); }
+};
+
+template <typename R> __global__ void __launch_bounds__(128) k_fragmem(StepArgs<R> a, FFParams p)
 {
-  int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-  const DevSys<R> &s = a.s;
-  if (i >= s.n_res) return;
-  int n = s.n_res, nd = p.fm_nd;
-  int k = lane & 3;
-  const int ib = (k < 2) ? B_CA : B_CB, jb = (k & 1) ? B_CB : B_CA;
-  V3<double> pi = bead(s, i, ib);
-  long long Fi[3] = {0, 0, 0};
-  double e_tot = 0.0;
-  for (int dd = 0; dd < nd; dd++) {
-    int row = i * nd + dd;
-    int r0 = a.fm_row[row], r1 = a.fm_row[row + 1];
-    if (r1 == r0) continue;
-    int j = i + p.fm_min_sep + dd;
-    V3<R> d = diff<R>(pi, bead(s, j, jb));
-    R r = m_sqrt(norm2(d));
-    R s2 = R(p.fm_sigma_sq[p.fm_min_sep + dd]);
-    R inv2s = R(1) / (R(2) * s2);
-    R esum = 0, fsum = 0;
-    const R *rf = a.fm_rf + (size_t) r0 * 4;
-    int nrec4 = (r1 - r0) * 4;
-    if (a.fm_coef) {
-      for (int e = lane; e < nrec4; e += 32) {
-        R dr = r - rf[e];
-        R g = a.fm_coef[r0 + (e >> 2)] * m_fastexp(-dr * dr * inv2s);
-        esum -= g;
-        fsum -= g * dr;
-      }
-    } else {
-      R c = R(a.fm_uniform);
-      for (int e = lane; e < nrec4; e += 32) {
-        R dr = r - rf[e];
-        R g = c * m_fastexp(-dr * dr * inv2s);
-        esum -= g;
-        fsum -= g * dr;
-      }
-    }
-    // combine lanes with the same atom pair (lane & 3)
-    for (int o = 4; o < 32; o <<= 1) {
-      esum += __shfl_xor_sync(0xffffffffu, esum, o);
-      fsum += __shfl_xor_sync(0xffffffffu, fsum, o);
-    }
-    // row energy: the four atom-pair sums
-    double erow = (double) esum;
-    erow += __shfl_xor_sync(0xffffffffu, erow, 1);
-    erow += __shfl_xor_sync(0xffffffffu, erow, 2);
-    e_tot += erow;
-    if (lane < 4) {
-      R fc = fsum / (s2 * r);
-      if (fsum != R(0)) {
-        long long fx = fix_force((double) (fc * d.x)), fy = fix_force((double) (fc * d.y)),
-                  fz = fix_force((double) (fc * d.z));
-        Fi[0] += fx;
-        Fi[1] += fy;
-        Fi[2] += fz;
-        unsigned long long *fj = s.facc + ((size_t) 3 * j + jb) * 3;
-        atomicAdd(fj + 0, (unsigned long long) (-fx));
-        atomicAdd(fj + 1, (unsigned long long) (-fy));
-        atomicAdd(fj + 2, (unsigned long long) (-fz));
-      }
-    }
-  }
-  // lanes 0,1 act on CA(i), lanes 2,3 on CB(i)
-  for (int c = 0; c < 3; c++) Fi[c] += __shfl_xor_sync(0xffffffffu, Fi[c], 1);
-  if (lane == 0 || lane == 2) {
-    unsigned long long *fi = s.facc + ((size_t) 3 * i + ib) * 3;
-    for (int c = 0; c < 3; c++)
-      if (Fi[c]) atomicAdd(fi + c, (unsigned long long) Fi[c]);
-  }
-  if (lane == 0) a.e_res[(size_t) E_FRAGMEM * n + i] = e_tot;
+  const BeadPos<R> pos{&a.s};
+  fragmem_warp(a.fm, p.fm_sigma_sq, a.s.n_res, pos, a.s.facc,
+               (unsigned long long *) (a.e_fix + (size_t) 2 * a.s.n_res), 1);
 }
 
 // bond_style harmonic, bonds grouped by the residue of their first atom
@@ -778,7 +716,7 @@ template <typename R> __global__ void k_total_force(StepArgs<R> a, double *ftot)
 
 // Thermo row of the current step: [fix total, vexcluded, bonds, kinetic],
 // residue sums in a fixed tree order (one block of 256 threads).
-__global__ void k_thermo(const double *e_res, const long long *e_hb, int n_res, const long long *step,
+__global__ void k_thermo(const double *e_res, const long long *e_fix, int n_res, const long long *step,
                          const Integrator *inp, const int *sys_begin, const int *sys_end, long long nrows, double *rows)
 {
   const long long begin = inp->begin;
@@ -788,7 +726,7 @@ __global__ void k_thermo(const double *e_res, const long long *e_hb, int n_res, 
   for (int r = sys_begin[rep] + threadIdx.x; r < sys_end[rep]; r += blockDim.x) {
     double fx = 0.0;
     for (int t = 1; t < E_FIX_TERMS; t++) fx += e_res[(size_t) t * n_res + r];
-    fx += (double) (e_hb[r] + e_hb[(size_t) n_res + r]) * F_UNSCALE;
+    fx += (double) (e_fix[r] + e_fix[(size_t) n_res + r] + e_fix[(size_t) 2 * n_res + r]) * F_UNSCALE;
     acc[0] += fx;
     acc[1] += e_res[(size_t) E_PAIR * n_res + r];
     acc[2] += e_res[(size_t) E_BOND * n_res + r];
@@ -809,14 +747,14 @@ __global__ void k_thermo(const double *e_res, const long long *e_hb, int n_res, 
 
 // Per-term sums of each replica's residues in a fixed tree order
 // (block (t, rep) sums energy slot t of replica rep)
-__global__ void k_energy_reduce(const double *e_res, const long long *e_hb, int n_res, const int *sys_begin,
+__global__ void k_energy_reduce(const double *e_res, const long long *e_fix, int n_res, const int *sys_begin,
                                 const int *sys_end, double *out)
 {
   const int t = blockIdx.x, rep = blockIdx.y;
   __shared__ double sh[256];
   double acc = 0.0;
-  // DSSP and P_AP energies are kept in fixed point (queue order independent)
-  const long long *fx = t == E_DSSP ? e_hb : t == E_PAP ? e_hb + n_res : nullptr;
+  // DSSP, P_AP and fragment-memory energies are kept in fixed point
+  const long long *fx = t == E_DSSP ? e_fix : t == E_PAP ? e_fix + n_res : t == E_FRAGMEM ? e_fix + 2 * (size_t) n_res : nullptr;
   for (int r = sys_begin[rep] + threadIdx.x; r < sys_end[rep]; r += blockDim.x)
     acc += fx ? (double) fx[r] * F_UNSCALE : e_res[(size_t) t * n_res + r];
   sh[threadIdx.x] = acc;
