@@ -119,7 +119,10 @@ template <typename R> class Engine : public EngineBase {
   DBuf<double> aps, tables, x, v, mass, g1, g2, ftot, work, e_res, energy;
   DBuf<double4> pos, cb_build;
   DBuf<unsigned long long> facc;
-  DBuf<int> nbr, ncount, hbq;
+  DBuf<int2> pairs;
+  DBuf<int> ncount, hbq;
+  DBuf<long long> dacc;
+  int pair_blocks = 1;
   DBuf<long long> e_fix;
   int hb_blocks = 1;
   DBuf<dev::NLState> nl;
@@ -134,7 +137,7 @@ template <typename R> class Engine : public EngineBase {
   DBuf<double> thermo_rows;
   DBuf<int> res_sys, sys_begin, sys_end;
   DBuf<unsigned long long> sys_seed;
-  int cap = 0;
+  int pcap = 0;  // residue pair list capacity (pairs)
   int groups_all = dev::G_FIX | dev::G_PAIR | dev::G_BOND;
   double skin = 2.0;
   int neigh_every = 0;
@@ -185,11 +188,12 @@ template <typename R> class Engine : public EngineBase {
     a.xi2 = w + 8 * nn;
     a.bur = w + 9 * nn;
     a.e_res = e_res.p;
-    a.nbr = nbr.p;
+    a.pairs = pairs.p;
+    a.dacc = dacc.p;
     a.hbq = hbq.p;
     a.e_fix = e_fix.p;
     a.ncount = ncount.p;
-    a.cap = cap;
+    a.pcap = pcap;
     a.cb_build = cb_build.p;
     a.nl = nl.p;
     a.ntypes = in.top.ntypes;
@@ -311,28 +315,31 @@ template <typename R> class Engine : public EngineBase {
     CK(cudaMemcpyAsync(nl.p, &st, sizeof st, cudaMemcpyHostToDevice, s0));
     long long s = step;
     CK(cudaMemcpyAsync(dstep.p, &s, sizeof s, cudaMemcpyHostToDevice, s0));
-    // size the pair list from a first build
-    e_fix.alloc((size_t) 3 * nn);
+    e_fix.alloc((size_t) 5 * nn);
     e_fix.zero(s0);
+    dacc.alloc((size_t) 3 * nn);
+    dacc.zero(s0);
     int sms = 148;
     CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
     hb_blocks = std::max(1, std::min((nn * 8 + 127) / 128, 16 * sms));
-    resize_list(32);
+    // size the pair list from a first build: room for 4x the initial pairs
+    // (chains that collapse gain neighbours), at least 24 per residue
+    resize_pairs(std::max<long long>(64, 16LL * nn));
     for (int attempt = 0; attempt < 8; attempt++) {
       launch_prepare_and_list(args(groups_all), s0, true, false);
       dev::NLState got;
       CK(cudaMemcpyAsync(&got, nl.p, sizeof got, cudaMemcpyDeviceToHost, s0));
       CK(cudaStreamSynchronize(s0));
       if (!got.overflow) {
-        int maxc = max_count();
-        int want = std::max(64, ((2 * maxc + 31) / 32) * 32);
-        if (want > cap) {
-          resize_list(want);
+        long long want = std::max(4LL * got.npairs, 24LL * nn) + 1024;
+        pair_blocks = (int) std::max(1LL, std::min<long long>((3LL * got.npairs / 2 + 127) / 128, 16LL * sms));
+        if (want > pcap) {
+          resize_pairs(want);
           continue;
         }
         break;
       }
-      resize_list(std::max(2 * cap, ((2 * got.overflow + 31) / 32) * 32));
+      resize_pairs(std::max<long long>(2LL * pcap, 2LL * got.overflow));
     }
   }
 
@@ -344,13 +351,13 @@ template <typename R> class Engine : public EngineBase {
     return c.empty() ? 0 : *std::max_element(c.begin(), c.end());
   }
 
-  void resize_list(int newcap)
+  void resize_pairs(long long newcap)
   {
-    // list slots (residue * cap + k) are int indices in the hydrogen-bond queues
-    if ((long long) newcap * n() >= (1ll << 31)) throw std::invalid_argument("residue pair list exceeds 2^31 slots");
-    cap = newcap;
-    nbr.alloc((size_t) cap * n());
-    hbq.alloc((size_t) 2 * cap * n());
+    // pair indices (and their complements in the DSSP queue) are ints
+    if (newcap >= (1ll << 31)) throw std::invalid_argument("residue pair list exceeds 2^31 pairs");
+    pcap = (int) newcap;
+    pairs.alloc((size_t) pcap);
+    hbq.alloc((size_t) 3 * pcap);
     dev::NLState st;
     CK(cudaMemcpyAsync(&st, nl.p, sizeof st, cudaMemcpyDeviceToHost, s0));
     CK(cudaStreamSynchronize(s0));
@@ -374,7 +381,7 @@ template <typename R> class Engine : public EngineBase {
   {
     const FFParams &p = in.ff.p;
     int nn = n();
-    int tb = 128, nb = (nn + tb - 1) / tb, wb = (nn * 32 + tb - 1) / tb;
+    int tb = 128, nb = (nn + tb - 1) / tb;
     launch_prepare_and_list(a, s0, false, advance);
     bool fm = (a.groups & dev::G_FIX) && p.fm_nd > 0;
     if (fm) {
@@ -384,10 +391,10 @@ template <typename R> class Engine : public EngineBase {
       dev::k_fragmem<R><<<fm_blocks(), tb, 0, s1>>>(a, p);
       CK(cudaEventRecord(ev_join, s1));
     }
-    dev::k_density<R><<<wb, tb, 0, s0>>>(a, p);
+    dev::k_density<R><<<pair_blocks, tb, 0, s0>>>(a, p);
     dev::k_residue<R><<<nb, tb, 0, s0>>>(a, p);
-    dev::k_water_xi<R><<<wb, tb, 0, s0>>>(a, p);
-    dev::k_pair<R><<<wb, tb, 0, s0>>>(a, p);
+    dev::k_water_xi<R><<<pair_blocks, tb, 0, s0>>>(a, p);
+    dev::k_pair<R><<<pair_blocks, tb, 0, s0>>>(a, p);
     dev::k_hbond<R><<<hb_blocks, 128, 0, s0>>>(a, p);
     if (a.groups & dev::G_BOND) dev::k_bonds<R><<<nb, tb, 0, s0>>>(a);
     if (fm) CK(cudaStreamWaitEvent(s0, ev_join, 0));
@@ -455,7 +462,7 @@ template <typename R> class Engine : public EngineBase {
     dev::NLState st;
     CK(cudaMemcpy(&st, nl.p, sizeof st, cudaMemcpyDeviceToHost));
     if (st.overflow)
-      throw std::runtime_error("residue pair list overflow (capacity " + std::to_string(cap) + ", needed " +
+      throw std::runtime_error("residue pair list overflow (capacity " + std::to_string(pcap) + " pairs, needed " +
                                std::to_string(st.overflow) + "); results of this call are invalid");
   }
 
@@ -563,10 +570,10 @@ template <typename R> class Engine : public EngineBase {
           case 0: dev::k_prepare<R><<<nb, tb, 0, s0>>>(a, p); break;
           case 1: dev::k_nl_decide<<<1, 1, 0, s0>>>(nl.p, 0, dstep.p); break;
           case 2: dev::k_nl_build<R><<<wb, tb, 0, s0>>>(a); break;
-          case 3: dev::k_density<R><<<wb, tb, 0, s0>>>(a, p); break;
+          case 3: dev::k_density<R><<<pair_blocks, tb, 0, s0>>>(a, p); break;
           case 4: dev::k_residue<R><<<nb, tb, 0, s0>>>(a, p); break;
-          case 5: dev::k_water_xi<R><<<wb, tb, 0, s0>>>(a, p); break;
-          case 6: dev::k_pair<R><<<wb, tb, 0, s0>>>(a, p); break;
+          case 5: dev::k_water_xi<R><<<pair_blocks, tb, 0, s0>>>(a, p); break;
+          case 6: dev::k_pair<R><<<pair_blocks, tb, 0, s0>>>(a, p); break;
           case 7: dev::k_hbond<R><<<hb_blocks, 128, 0, s0>>>(a, p); break;
           case 8: if (fm) dev::k_fragmem<R><<<fm_blocks(), tb, 0, s0>>>(a, p); break;
           case 9: dev::k_bonds<R><<<nb, tb, 0, s0>>>(a); break;
@@ -663,13 +670,11 @@ template <typename R> class Engine : public EngineBase {
     info[2] = in.fm.records();
     info[3] = sizeof(R);
     info[4] = in.ff.p.fm_nd;
-    info[5] = cap;
-    std::vector<int> c(n());
-    CK(cudaMemcpyAsync(c.data(), ncount.p, sizeof(int) * n(), cudaMemcpyDeviceToHost, s0));
+    info[5] = pcap;
+    dev::NLState st;
+    CK(cudaMemcpyAsync(&st, nl.p, sizeof st, cudaMemcpyDeviceToHost, s0));
     CK(cudaStreamSynchronize(s0));
-    long long tot = 0;
-    for (int v2 : c) tot += v2;
-    info[6] = tot;
+    info[6] = st.npairs;
     info[7] = in.fm.uniform ? 0 : 1;
   }
 
@@ -804,8 +809,12 @@ template <typename R> class Engine : public EngineBase {
     check_rep(rep);
     int nn = n(), r0 = in.sys_res_begin[rep], nr = rep_res(rep);
     std::vector<double> w((size_t) 10 * nn);
+    std::vector<long long> raw(nn);
     CK(cudaMemcpyAsync(w.data(), work.p, sizeof(double) * 10 * nn, cudaMemcpyDeviceToHost, s0));
+    CK(cudaMemcpyAsync(raw.data(), dacc.p + (size_t) 2 * nn, sizeof(long long) * nn, cudaMemcpyDeviceToHost, s0));
     CK(cudaStreamSynchronize(s0));
+    // xi_water = raw pair sum (2^-40 fixed point) * sigma_water', as k_pair forms it
+    for (int r = 0; r < nn; r++) w[(size_t) 6 * nn + r] = (double) raw[r] * dev::D_UNSCALE * w[(size_t) 3 * nn + r];
     // device order: rho_w rho_h sig_w sigp_w sig_h sigp_h xi_w xi1 xi2 bur
     const int src[8] = {0, 1, 6, 7, 8, 9, 2, 4};
     for (int r = 0; r < nr; r++)

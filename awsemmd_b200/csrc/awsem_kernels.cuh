@@ -4,12 +4,13 @@
 //   prepare      thread/residue: CA, CB, O -> working copy + virtual N, H, C'
 //                (fix_backbone.cpp:7067-7138); zero forces; list-check data
 //   nl_decide    1 thread: rebuild decision for the residue pair list
-//   nl_build     warp/residue: contact-bead pairs within the list radius
-//   density      warp/residue: rho_water, rho_helix (DL1, :7728-7791)
+//   nl_build     warp/residue: pairs i < j of contact beads within the list
+//                radius, appended to a flat pair array
+//   density      thread/pair: rho_water, rho_helix (DL1, :7728-7791)
 //   residue      thread/residue: switching functions, burial (SL, :7795-7841),
 //                helical (i,i+4) pairs (:7843-7868), chain/chi/rama
-//   water_xi     warp/residue: xi_water (DL2, :7877-7954)
-//   pair         warp/residue: water/burial/helix radial forces, excluded
+//   water_xi     thread/pair: xi_water (DL2, :7877-7954)
+//   pair         thread/pair: water/burial/helix radial forces, excluded
 //                volume (DL3, :7956-8134); queues DSSP and P_AP pairs
 //   hbond        thread/queued pair: DSSP hydrogen bonds, P_AP
 //   fragmem      warp/32 residues, lane/residue row: fragment-memory
@@ -18,7 +19,9 @@
 //   finish       thread/residue: fixed-point -> FP64 forces, Langevin,
 //                velocity-Verlet half kicks and drift
 // Residue-owned quantities are written by their owner without atomics;
-// forces scattered to other residues' beads use 64-bit integer atomics.
+// sums over pairs (forces, densities, pair energies) use 64-bit integer
+// atomics on fixed-point accumulators, which makes them exact and order
+// independent.
 #pragma once
 
 #include "awsem_device.cuh"
@@ -41,6 +44,7 @@ struct NLState {
   float bCAx;         // max distance of a residue's CB or O from its own CA (this step)
   float ev_pre_sq;    // CA-CA distance^2 beyond which no bead pair of two residues is in excluded-volume range
   int n_dssp, n_pap;  // hydrogen-bond queue lengths of the current evaluation
+  int npairs;         // pairs in the residue pair list (may exceed its capacity: overflow)
 };
 
 template <typename R> struct StepArgs {
@@ -53,16 +57,20 @@ template <typename R> struct StepArgs {
   // per-residue pair-pass intermediates
   double *rho_w, *rho_h, *sig_w, *sigp_w, *sig_h, *sigp_h, *xi_w, *xi1, *xi2, *bur;
   double *e_res;  // [E_SLOTS][n_res]
-  // residue pair list
-  int *nbr, *ncount, cap;
+  // residue pair list: pairs (i, j), i < j, capacity pcap; per-residue counts
+  int2 *pairs;
+  int *ncount, pcap;
   double4 *cb_build;
   NLState *nl;
-  // hydrogen-bond work queues: list slots (residue * cap + k) of the DSSP
-  // candidates in [0, n_res*cap) and of the P_AP candidates after them
+  // hydrogen-bond work queues (pair indices): DSSP in [0, 2 pcap) (q: O(i)
+  // acceptor, ~q: O(j) acceptor), P_AP in [2 pcap, 3 pcap)
   int *hbq;
-  // energies summed by several threads per residue, in 2^-32 fixed point
-  // (sums independent of order): [0] DSSP, [1] P_AP, [2] fragment memory
+  // energies summed over pairs, in 2^-32 fixed point (sums independent of
+  // order): [0] DSSP, [1] P_AP, [2] fragment memory, [3] water, [4] excluded
+  // volume between residues; [5][n_res]
   long long *e_fix;
+  // density sums in 2^-40 fixed point: [0] water, [1] helix, [2] raw xi_water; [3][n_res]
+  long long *dacc;
   // excluded volume
   int ntypes, ev_p;
   const double *ev_pref, *ev_cs, *ev_cl;
@@ -123,7 +131,8 @@ template <typename R> __global__ void k_prepare(StepArgs<R> a, FFParams p)
     w[B_CP] = make_double4(cp[0], cp[1], cp[2], 0.0);
     unsigned long long *f = a.s.facc + (size_t) 9 * r;
     for (int k = 0; k < 9; k++) f[k] = 0ull;
-    for (int k = 0; k < 3; k++) a.e_fix[(size_t) k * a.s.n_res + r] = 0;
+    for (int k = 0; k < 5; k++) a.e_fix[(size_t) k * a.s.n_res + r] = 0;
+    for (int k = 0; k < 3; k++) a.dacc[(size_t) k * a.s.n_res + r] = 0;
     {
       // reach of the residue's beads around its CA (excluded-volume prefilter)
       double ux = cb[0] - ca[0], uy = cb[1] - ca[1], uz = cb[2] - ca[2];
@@ -176,6 +185,7 @@ __global__ void k_nl_decide(NLState *nl, int force, long long *step)
   float disp = sqrtf(s.d2max);
   bool rb = force || s.r_list <= 0.f || need + 2.f * disp > s.r_list || (s.every > 0 && s.steps_since + 1 >= s.every);
   if (rb) {
+    s.npairs = 0;  // k_nl_build appends
     s.r_list = need + s.skin;
     s.steps_since = 0;
     s.nbuilds++;
@@ -196,78 +206,89 @@ template <typename R> __device__ __forceinline__ V3<double> contact(const DevSys
   return bead(s, r, (s.res_flags[r] & R_GLY) ? B_CA : B_CB);
 }
 
-// Full residue pair list (both directions) over contact beads within r_list,
-// written in ascending j.  Brute force over the residue's own replica, one
-// warp per residue.
+// Residue pair list: every pair i < j of one replica whose contact beads are
+// closer than r_list, as (i, j) in a flat array.  One warp per residue scans
+// the higher residues of its replica twice (count, then write after one
+// atomic reservation), so a residue's pairs are contiguous and ascending.
+// Every pair pass below runs one thread per listed pair and scatters to both
+// residues with fixed-point atomics: each pair is evaluated once, as in the
+// reference's half neighbour list.
 template <typename R> __global__ void k_nl_build(StepArgs<R> a)
 {
   if (!a.nl->rebuild) return;
-  int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-  int i = warp;
+  const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   if (i >= a.s.n_res) return;
-  int rep = a.res_sys[i];
-  const int sys_begin = a.sys_begin[rep], sys_end = a.sys_end[rep];
+  const int sys_end = a.sys_end[a.res_sys[i]];
   const DevSys<R> &s = a.s;
-  V3<double> ci = contact(s, i);
-  R rl = (R) a.nl->r_list, rl2 = rl * rl;
+  const V3<double> ci = contact(s, i);
+  const R rl = (R) a.nl->r_list, rl2 = rl * rl;
   int count = 0;
-  int *out = a.nbr + (size_t) i * a.cap;
-  for (int j0 = sys_begin; j0 < sys_end; j0 += 32) {
-    int j = j0 + lane;
-    bool take = false;
-    if (j < sys_end && j != i) {
-      V3<R> d = diff<R>(ci, contact(s, j));
-      take = norm2(d) < rl2;
-    }
-    unsigned m = __ballot_sync(0xffffffffu, take);
-    int at = count + __popc(m & ((1u << lane) - 1u));
-    if (take && at < a.cap) out[at] = j;
-    count += __popc(m);
+  for (int j0 = i + 1; j0 < sys_end; j0 += 32) {
+    const int j = j0 + lane;
+    const bool take = j < sys_end && norm2(diff<R>(ci, contact(s, j))) < rl2;
+    count += __popc(__ballot_sync(0xffffffffu, take));
   }
+  int base = 0;
+  if (lane == 0 && count) base = atomicAdd(&a.nl->npairs, count);
+  base = __shfl_sync(0xffffffffu, base, 0);
   if (lane == 0) {
-    a.ncount[i] = min(count, a.cap);
-    if (count > a.cap) atomicMax(&a.nl->overflow, count);
+    if (base + count > a.pcap) atomicMax(&a.nl->overflow, base + count);
+    a.ncount[i] = count;
     a.cb_build[i] = make_double4(ci.x, ci.y, ci.z, 0.0);
+  }
+  int at = base;
+  for (int j0 = i + 1; j0 < sys_end && count; j0 += 32) {
+    const int j = j0 + lane;
+    const bool take = j < sys_end && norm2(diff<R>(ci, contact(s, j))) < rl2;
+    const unsigned m = __ballot_sync(0xffffffffu, take);
+    const int k = at + __popc(m & ((1u << lane) - 1u));
+    if (take && k < a.pcap) a.pairs[k] = make_int2(i, j);
+    at += __popc(m);
   }
 }
 
-// DL1: local densities of contact beads (fix_backbone.cpp:7728-7791)
+// Pairs of the list, grid-stride (the count is known only on the device)
+#define FOR_EACH_PAIR(a, p) \
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x, np_ = min((a).nl->npairs, (a).pcap); p < np_; p += gridDim.x * blockDim.x)
+
+// DL1: local densities of contact beads (fix_backbone.cpp:7728-7791).  FP64
+// in both forms: the densities feed the burial and switching functions, and
+// the well selection is then the reference's exactly.  Sums in 2^-40 fixed
+// point (dacc[0], dacc[1]).
 template <typename R> __global__ void k_density(StepArgs<R> a, FFParams p)
 {
-  int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   const DevSys<R> &s = a.s;
-  if (i >= s.n_res) return;
-  V3<double> ci = contact(s, i);
-  int chi = s.res_chain[i];
-  long long aw = 0, ah = 0;
-  const bool fix = a.groups & G_FIX;
-  int cnt = fix ? a.ncount[i] : 0;
-  const int *nb = a.nbr + (size_t) i * a.cap;
-  bool water = p.terms & T_WATER, helix = p.terms & T_HELIX;
-  // FP64 in both forms: the densities feed the burial and switching
-  // functions, and the well selection is then the reference's exactly
-  for (int k = lane; k < cnt; k += 32) {
-    int j = nb[k];
-    if (s.res_chain[j] == chi && abs(i - j) <= 1) continue;
-    V3<double> d = diff<double>(ci, contact(s, j));
-    double rsq = norm2(d);
+  const int n = s.n_res;
+  if (!(a.groups & G_FIX)) return;
+  const bool water = p.terms & T_WATER, helix = p.terms & T_HELIX;
+  unsigned long long *aw = (unsigned long long *) a.dacc, *ah = aw + n;
+  FOR_EACH_PAIR(a, q)
+  {
+    const int2 ij = a.pairs[q];
+    const int i = ij.x, j = ij.y;
+    if (s.res_chain[j] == s.res_chain[i] && j - i <= 1) continue;
+    const double rsq = norm2(diff<double>(contact(s, i), contact(s, j)));
     if (water && rsq > p.w_rmin_sq[0] && rsq < p.w_rmax_sq[0]) {
       double th, pr;
       well_theta(sqrt(rsq), p.w_rmin_th[0], p.w_rmax_th[0], p.water_kappa, p.well_rmin[0], p.well_rmax[0], th, pr);
-      aw += fix_dens(th);
+      const unsigned long long v = (unsigned long long) fix_dens(th);
+      atomicAdd(aw + i, v);
+      atomicAdd(aw + j, v);
     }
     if (helix && rsq > p.h_rmin_sq && rsq < p.h_rmax_sq) {
       double th, pr;
       well_theta(sqrt(rsq), p.h_rmin_th, p.h_rmax_th, p.helix_kappa, p.helix_rmin, p.helix_rmax, th, pr);
-      ah += fix_dens(th);
+      const unsigned long long v = (unsigned long long) fix_dens(th);
+      atomicAdd(ah + i, v);
+      atomicAdd(ah + j, v);
     }
   }
-  aw = warp_sum(aw);
-  ah = warp_sum(ah);
-  if (lane == 0) {
-    a.rho_w[i] = (double) aw * D_UNSCALE;
-    a.rho_h[i] = (double) ah * D_UNSCALE;
-  }
+}
+
+// density sums -> values: k = 0 water density, 1 helix density
+template <typename R> __device__ __forceinline__ double density(const StepArgs<R> &a, int k, int r)
+{
+  return (double) a.dacc[(size_t) k * a.s.n_res + r] * D_UNSCALE;
 }
 
 __device__ __forceinline__ void switching(double rho, double kappa_sigma, double thr, double &sig, double &sigp)
@@ -314,15 +335,18 @@ template <typename R> __global__ void k_residue(StepArgs<R> a, FFParams p)
   const bool fix = a.groups & G_FIX;
   bool water = fix && (p.terms & T_WATER), helix = fix && (p.terms & T_HELIX);
   double sw = 0, swp = 0, sh = 0, shp = 0;
-  if (water) switching(a.rho_w[i], p.water_kappa_sigma, p.treshold, sw, swp);
-  if (helix) switching(a.rho_h[i], p.helix_kappa_sigma, p.helix_treshold, sh, shp);
+  const double rw = density(a, 0, i), rh = density(a, 1, i);
+  a.rho_w[i] = rw;
+  a.rho_h[i] = rh;
+  if (water) switching(rw, p.water_kappa_sigma, p.treshold, sw, swp);
+  if (helix) switching(rh, p.helix_kappa_sigma, p.helix_treshold, sh, shp);
   a.sig_w[i] = sw;
   a.sigp_w[i] = swp;
   a.sig_h[i] = sh;
   a.sigp_h[i] = shp;
   double eb = 0.0, bc = 0.0;
   if (fix && (p.terms & T_BURIAL)) {
-    double rho = a.rho_w[i];
+    double rho = rw;
     const double *g = s.tables + TB_BURIAL + 3 * s.res_type[i];
     double t[3][2];
     for (int k = 0; k < 3; k++) {
@@ -344,7 +368,7 @@ template <typename R> __global__ void k_residue(StepArgs<R> a, FFParams p)
     V3<R> d = diff<R>(bead(s, i, B_O), bead(s, j, B_N));
     if (norm2(d) < R(p.helix_cutoff_sq)) {
       double shj, shpj;
-      switching(a.rho_h[j], p.helix_kappa_sigma, p.helix_treshold, shj, shpj);
+      switching(density(a, 1, j), p.helix_kappa_sigma, p.helix_treshold, shj, shpj);
       eh = (double) helix_pair(sd, p, i, j, sh, shp, shj, shpj, x1, x2);
     }
   }
@@ -377,107 +401,103 @@ template <typename R> __global__ void k_residue(StepArgs<R> a, FFParams p)
   E[(size_t) E_PAIR * n + i] = ev;
 }
 
-// DL2: water-mediated density derivative coefficients (fix_backbone.cpp:7877-7954)
+// DL2: water-mediated density derivative coefficients (fix_backbone.cpp:
+// 7877-7954): raw sums in dacc[2] (2^-40 fixed point); xi_water(i) is that
+// sum times sigma_water'(i) (water_xi below).
 template <typename R> __global__ void k_water_xi(StepArgs<R> a, FFParams p)
 {
-  int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   const DevSys<R> &s = a.s;
-  if (i >= s.n_res) return;
-  if (!(p.terms & T_WATER) || !(a.groups & G_FIX)) {
-    if (lane == 0) a.xi_w[i] = 0.0;
-    return;
-  }
-  V3<double> ci = contact(s, i);
-  int chi = s.res_chain[i], ti = s.res_type[i];
-  long long acc = 0;
-  int cnt = a.ncount[i];
-  const int *nb = a.nbr + (size_t) i * a.cap;
+  if (!(p.terms & T_WATER) || !(a.groups & G_FIX)) return;
+  unsigned long long *acc = (unsigned long long *) a.dacc + (size_t) 2 * s.n_res;
   const double *WG = s.tables + TB_WATER;
-  for (int k = lane; k < cnt; k += 32) {
-    int j = nb[k];
-    if (s.res_chain[j] == chi && abs(i - j) < p.contact_cutoff) continue;
-    V3<R> d = diff<R>(ci, contact(s, j));
-    R rsq = norm2(d);
-    int tj = s.res_type[j];
+  FOR_EACH_PAIR(a, q)
+  {
+    const int2 ij = a.pairs[q];
+    const int i = ij.x, j = ij.y;
+    if (s.res_chain[j] == s.res_chain[i] && j - i < p.contact_cutoff) continue;
+    const R rsq = norm2(diff<R>(contact(s, i), contact(s, j)));
+    const int ti = s.res_type[i], tj = s.res_type[j];
     for (int w = 0; w < p.n_wells; w++) {
       if (!p.well_flag[w]) continue;
-      double g0 = WG[w * 800 + (ti * 20 + tj) * 2], g1 = WG[w * 800 + (ti * 20 + tj) * 2 + 1];
+      const double g0 = WG[w * 800 + (ti * 20 + tj) * 2], g1 = WG[w * 800 + (ti * 20 + tj) * 2 + 1];
       // the reference's `!fabs(g0 - g1) < delta` holds exactly when g0 != g1
       if (g0 != g1 && rsq > R(p.w_rmin_sq[w]) && rsq < R(p.w_rmax_sq[w])) {
         R th, pr;
         well_theta(m_sqrt(rsq), R(p.w_rmin_th[w]), R(p.w_rmax_th[w]), R(p.water_kappa), R(p.well_rmin[w]),
                    R(p.well_rmax[w]), th, pr);
-        acc += fix_dens((g1 - g0) * (double) th * a.sig_w[j]);
+        const double tg = (g1 - g0) * (double) th;
+        atomicAdd(acc + i, (unsigned long long) fix_dens(tg * a.sig_w[j]));
+        atomicAdd(acc + j, (unsigned long long) fix_dens(tg * a.sig_w[i]));
       }
     }
   }
-  acc = warp_sum(acc);
-  if (lane == 0) a.xi_w[i] = (double) acc * D_UNSCALE * a.sigp_w[i];
+}
+
+template <typename R> __device__ __forceinline__ double water_xi(const StepArgs<R> &a, int r)
+{
+  return (double) a.dacc[(size_t) 2 * a.s.n_res + r] * D_UNSCALE * a.sigp_w[r];
+}
+
+template <typename R> __device__ __forceinline__ void scatter_fix(const DevSys<R> &s, int r, int b, const long long f[3])
+{
+  unsigned long long *q = s.facc + ((size_t) 3 * r + b) * 3;
+#pragma unroll
+  for (int c = 0; c < 3; c++)
+    if (f[c]) atomicAdd(q + c, (unsigned long long) f[c]);
 }
 
 // DL3: main pair loop (fix_backbone.cpp:7956-8134) plus excluded volume
-// between residues.  Radial contact forces and excluded volume act on the
-// owner's beads only (each pair is visited from both sides).  DSSP and P_AP
-// pairs are only detected here (cheap distance and index tests) and queued;
-// k_hbond evaluates them one thread per pair, so their long, branchy bodies
-// neither serialise this warp nor inflate its register count.
+// between residues, one thread per listed pair i < j.  Radial contact forces
+// and excluded volume are applied to both residues.  DSSP and P_AP pairs are
+// only detected here (cheap distance and index tests) and queued: k_hbond
+// evaluates them, so their long, branchy bodies do not slow this pass.
 template <typename R> __global__ void __launch_bounds__(128) k_pair(StepArgs<R> a, FFParams p)
 {
-  int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   const DevSys<R> &s = a.s;
-  if (i >= s.n_res) return;
-  int n = s.n_res, fli = s.res_flags[i], chi = s.res_chain[i], ti = s.res_type[i];
-  // (arrays below are only indexed by unrolled constants: they stay in registers)
-  const bool gly_i = fli & R_GLY;
-  V3<double> bi[3] = {bead(s, i, B_CA), bead(s, i, B_CB), bead(s, i, B_O)};
-  V3<double> ci = gly_i ? bi[0] : bi[1];
-  V3<double> oi = bi[2];
-  int tat[3] = {a.atom_type[3 * i], a.atom_type[3 * i + 1], a.atom_type[3 * i + 2]};
-  double xi_i = a.xi_w[i], bur_i = a.bur[i], x1_i = a.xi1[i];
-  int dh = p.helix_i_diff;
-  double x2_i = i - dh >= 0 ? a.xi2[i - dh] : 0.0;
-  double sw_i = a.sig_w[i];
-  long long F[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
-  long long Fc[3] = {0, 0, 0};  // contact-bead radial forces
-  double e_water = 0.0, e_ev = 0.0;
+  const int n = s.n_res;
   const double *WG = s.tables + TB_WATER;
   const bool fix = a.groups & G_FIX, evon = a.groups & G_PAIR;
-  uint32_t T = fix ? p.terms : 0u;
-  int cnt = a.ncount[i];
-  const int *nb = a.nbr + (size_t) i * a.cap;
+  const uint32_t T = fix ? p.terms : 0u;
   const R ev_pre_sq = R(a.nl->ev_pre_sq);
   // smallest same-chain separation of any P_AP class (fix_backbone.cpp:3279-3383)
   const int pap_sep = min(p.i_med_min + 2 * p.i_diff_pap, p.i_med_max + 1);
-  const bool dssp_i = (T & T_DSSP) && !(fli & R_LAST);
-  const size_t qcap = (size_t) n * a.cap;
-  for (int k0 = 0; k0 < cnt; k0 += 32) {
-    const int k = k0 + lane;
-    bool q_dssp = false, q_pap = false;
-    if (k < cnt) {
-    int j = nb[k];
-    int flj = s.res_flags[j];
-    bool other = s.res_chain[j] != chi;
-    int dij = abs(i - j);
-    bool upper = j > i;
+  const int dh = p.helix_i_diff;
+  const size_t qd = 0, qp = (size_t) 2 * a.pcap;  // queue regions: DSSP (both orientations), P_AP
+  unsigned long long *e_water = (unsigned long long *) a.e_fix + (size_t) 3 * n;
+  unsigned long long *e_ev = (unsigned long long *) a.e_fix + (size_t) 4 * n;
+  const int lane = threadIdx.x & 31, np = min(a.nl->npairs, a.pcap);
+  // warp-uniform trip count: the queue appends below are warp collectives
+  for (int base = blockIdx.x * blockDim.x + threadIdx.x - lane; base < np; base += gridDim.x * blockDim.x) {
+    const int q = base + lane;
+    bool q_d0 = false, q_d1 = false, q_p = false;  // queue: DSSP O(i), DSSP O(j), P_AP
+    if (q < np) {
+    const int2 ij = a.pairs[q];
+    const int i = ij.x, j = ij.y;
+    const int fli = s.res_flags[i], flj = s.res_flags[j];
+    const bool other = s.res_chain[j] != s.res_chain[i];
+    const int dij = j - i;
+    const V3<double> ca_i = bead(s, i, B_CA), ca_j = bead(s, j, B_CA);
     // contact-bead radial terms
     if (fix && (other || dij > 1)) {
-      V3<R> d = diff<R>(ci, contact(s, j));
-      R rsq = norm2(d);
-      R r = m_sqrt(rsq);
+      const bool gi = fli & R_GLY, gj = flj & R_GLY;
+      const V3<R> d = diff<R>(gi ? ca_i : bead(s, i, B_CB), gj ? ca_j : bead(s, j, B_CB));
+      const R rsq = norm2(d);
+      const R r = m_sqrt(rsq);
       R force = 0;
-      bool in0 = rsq > R(p.w_rmin_sq[0]) && rsq < R(p.w_rmax_sq[0]);
+      double ew = 0.0;
+      const bool in0 = rsq > R(p.w_rmin_sq[0]) && rsq < R(p.w_rmax_sq[0]);
       R th0 = 0, pr0 = 0;
       if ((T & (T_WATER | T_BURIAL)) && in0)
         well_theta(r, R(p.w_rmin_th[0]), R(p.w_rmax_th[0]), R(p.water_kappa), R(p.well_rmin[0]), R(p.well_rmax[0]),
                    th0, pr0);
       if (T & T_WATER) {
-        int tj = s.res_type[j];
-        bool sep = other || dij >= p.contact_cutoff;
+        const int ti = s.res_type[i], tj = s.res_type[j];
+        const bool sep = other || dij >= p.contact_cutoff;
         for (int w = 0; w < p.n_wells; w++) {
           if (!p.well_flag[w]) continue;
           if (sep && rsq > R(p.w_rmin_sq[w]) && rsq < R(p.w_rmax_sq[w])) {
-            double g0 = WG[w * 800 + (ti * 20 + tj) * 2], g1 = WG[w * 800 + (ti * 20 + tj) * 2 + 1];
-            double sg = fabs(g0 - g1) < 1e-5 ? 0.5 * (g0 + g1) : g0 + (g1 - g0) * sw_i * a.sig_w[j];
+            const double g0 = WG[w * 800 + (ti * 20 + tj) * 2], g1 = WG[w * 800 + (ti * 20 + tj) * 2 + 1];
+            const double sg = fabs(g0 - g1) < 1e-5 ? 0.5 * (g0 + g1) : g0 + (g1 - g0) * a.sig_w[i] * a.sig_w[j];
             R th, pr;
             if (w == 0) {
               th = th0;
@@ -486,19 +506,20 @@ template <typename R> __global__ void __launch_bounds__(128) k_pair(StepArgs<R> 
               well_theta(r, R(p.w_rmin_th[w]), R(p.w_rmax_th[w]), R(p.water_kappa), R(p.well_rmin[w]),
                          R(p.well_rmax[w]), th, pr);
             }
-            if (upper) e_water += -sg * (double) th;
+            ew += -sg * (double) th;
             force += R(sg) * pr;
           }
         }
         if (in0) {
-          double xj = a.xi_w[j];
+          const double xi_i = water_xi(a, i), xi_j = water_xi(a, j);
           if (fabs(xi_i) > 1e-8) force += pr0 * R(xi_i);
-          if (fabs(xj) > 1e-8) force += pr0 * R(xj);
+          if (fabs(xi_j) > 1e-8) force += pr0 * R(xi_j);
         }
       }
-      if ((T & T_BURIAL) && in0) force += R(bur_i + a.bur[j]) * pr0;
+      if ((T & T_BURIAL) && in0) force += R(a.bur[i] + a.bur[j]) * pr0;
       if ((T & T_HELIX) && rsq > R(p.h_rmin_sq) && rsq < R(p.h_rmax_sq)) {
-        double fac = x1_i + a.xi1[j] + x2_i;
+        double fac = a.xi1[i] + a.xi1[j];
+        if (i - dh >= 0) fac += a.xi2[i - dh];
         if (j - dh >= 0) fac += a.xi2[j - dh];
         if (fabs(fac) > 1e-6) {
           R th, pr;
@@ -506,98 +527,93 @@ template <typename R> __global__ void __launch_bounds__(128) k_pair(StepArgs<R> 
           force += -R(fac) * pr;
         }
       }
+      if (ew != 0.0) atomicAdd(e_water + i, (unsigned long long) fix_force(ew));
       if (force != R(0)) {
-        Fc[0] += fix_force((double) (force * d.x));
-        Fc[1] += fix_force((double) (force * d.y));
-        Fc[2] += fix_force((double) (force * d.z));
+        const long long f[3] = {fix_force((double) (force * d.x)), fix_force((double) (force * d.y)),
+                                fix_force((double) (force * d.z))};
+        const long long g[3] = {-f[0], -f[1], -f[2]};
+        scatter_fix(s, i, gi ? B_CA : B_CB, f);
+        scatter_fix(s, j, gj ? B_CA : B_CB, g);
       }
     }
-    const R rca2 = (evon || (T & T_PAP)) ? norm2(diff<R>(bi[0], bead(s, j, B_CA))) : R(0);
+    const R rca2 = norm2(diff<R>(ca_i, ca_j));
     // excluded volume between beads of i and j (1-2 bonded pairs removed)
     if (evon && rca2 < ev_pre_sq) {
-      unsigned excl = 0;
-      if (j == i + 1) excl = a.excl_next[i];
-      bool prev = j == i - 1;
-      unsigned exclp = prev ? a.excl_next[j] : 0u;
-      bool shortr = !other && dij < 5;
+      const unsigned excl = j == i + 1 ? a.excl_next[i] : 0u;
+      const bool shortr = !other && dij < 5;
+      const V3<double> bi[3] = {ca_i, bead(s, i, B_CB), bead(s, i, B_O)};
+      const int tai[3] = {a.atom_type[3 * i], a.atom_type[3 * i + 1], a.atom_type[3 * i + 2]};
+      long long Fi[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+      double ee = 0.0;
 #pragma unroll
       for (int b1 = 0; b1 < 3; b1++) {
-        V3<double> bj = bead(s, j, b1);
-        int tb = a.atom_type[3 * j + b1];
+        const V3<double> bj = b1 == 0 ? ca_j : bead(s, j, b1);
+        const int tb = a.atom_type[3 * j + b1];
+        long long Fj[3] = {0, 0, 0};
 #pragma unroll
         for (int b0 = 0; b0 < 3; b0++) {
           if (excl & (1u << (b0 * 3 + b1))) continue;
-          if (exclp & (1u << (b1 * 3 + b0))) continue;
           V3<R> f;
-          R e = ev_pair(a, tat[b0], tb, shortr, diff<R>(bi[b0], bj), f);
+          const R e = ev_pair(a, tai[b0], tb, shortr, diff<R>(bi[b0], bj), f);
           if (e == R(0) && f.x == R(0) && f.y == R(0) && f.z == R(0)) continue;
-          if (upper) e_ev += (double) e;
-          F[b0][0] += fix_force((double) f.x);
-          F[b0][1] += fix_force((double) f.y);
-          F[b0][2] += fix_force((double) f.z);
+          ee += (double) e;
+          const long long v[3] = {fix_force((double) f.x), fix_force((double) f.y), fix_force((double) f.z)};
+#pragma unroll
+          for (int c = 0; c < 3; c++) {
+            Fi[b0][c] += v[c];
+            Fj[c] -= v[c];
+          }
         }
+        scatter_fix(s, j, b1, Fj);
       }
+#pragma unroll
+      for (int b0 = 0; b0 < 3; b0++) scatter_fix(s, i, b0, Fi[b0]);
+      if (ee != 0.0) atomicAdd(e_ev + i, (unsigned long long) fix_force(ee));
     }
-    // DSSP with O(i) as acceptor and N-H(j) as donor (fix_backbone.cpp:8064-8079)
-    if (dssp_i && (other || dij > 2) && !(flj & R_PRO) && !(flj & R_FIRST))
-      q_dssp = norm2(diff<R>(oi, bead(s, j, B_N))) < R(p.dssp_cut_sq);
-    // P_AP on CA pairs, visited from the lower residue (fix_backbone.cpp:8096-8103)
-    if ((T & T_PAP) && upper && (other || j - i >= pap_sep)) q_pap = rca2 < R(p.pap_cutoff_sq);
+    // DSSP (fix_backbone.cpp:8064-8094): O(i) with N-H(j), and O(j) with N-H(i)
+    if ((T & T_DSSP) && (other || dij > 2)) {
+      q_d0 = !(flj & (R_PRO | R_FIRST)) && !(fli & R_LAST) &&
+             norm2(diff<R>(bead(s, i, B_O), bead(s, j, B_N))) < R(p.dssp_cut_sq);
+      q_d1 = !(fli & (R_PRO | R_FIRST)) && !(flj & R_LAST) &&
+             norm2(diff<R>(bead(s, j, B_O), bead(s, i, B_N))) < R(p.dssp_cut_sq);
     }
-    // append this round's candidates to the queues (one atomic per warp and kind)
-    const unsigned md = __ballot_sync(0xffffffffu, q_dssp), mp = __ballot_sync(0xffffffffu, q_pap);
-    if (md | mp) {
+    // P_AP on CA pairs (fix_backbone.cpp:8096-8103)
+    q_p = (T & T_PAP) && (other || dij >= pap_sep) && rca2 < R(p.pap_cutoff_sq);
+    }
+    // queue appends: one atomic per warp and queue
+    const unsigned m0 = __ballot_sync(0xffffffffu, q_d0), m1 = __ballot_sync(0xffffffffu, q_d1),
+                   mp = __ballot_sync(0xffffffffu, q_p);
+    if (m0 | m1 | mp) {
       int bd = 0, bp = 0;
       if (lane == 0) {
-        if (md) bd = atomicAdd(&a.nl->n_dssp, __popc(md));
+        if (m0 | m1) bd = atomicAdd(&a.nl->n_dssp, __popc(m0) + __popc(m1));
         if (mp) bp = atomicAdd(&a.nl->n_pap, __popc(mp));
       }
       bd = __shfl_sync(0xffffffffu, bd, 0);
       bp = __shfl_sync(0xffffffffu, bp, 0);
       const unsigned below = (1u << lane) - 1u;
-      const int slot = i * a.cap + k;
-      if (q_dssp) a.hbq[bd + __popc(md & below)] = slot;
-      if (q_pap) a.hbq[qcap + bp + __popc(mp & below)] = slot;
+      if (q_d0) a.hbq[qd + bd + __popc(m0 & below)] = q;
+      if (q_d1) a.hbq[qd + bd + __popc(m0) + __popc(m1 & below)] = ~q;
+      if (q_p) a.hbq[qp + bp + __popc(mp & below)] = q;
     }
-  }
-#pragma unroll
-  for (int c = 0; c < 3; c++) {
-    F[0][c] += gly_i ? Fc[c] : 0ll;
-    F[1][c] += gly_i ? 0ll : Fc[c];
-  }
-#pragma unroll
-  for (int b = 0; b < 3; b++)
-#pragma unroll
-    for (int c = 0; c < 3; c++) F[b][c] = warp_sum(F[b][c]);
-  e_water = warp_sum(e_water);
-  e_ev = warp_sum(e_ev);
-  if (lane == 0) {
-    unsigned long long *f = s.facc + (size_t) 9 * i;
-#pragma unroll
-    for (int b = 0; b < 3; b++)
-#pragma unroll
-      for (int c = 0; c < 3; c++)
-        if (F[b][c]) atomicAdd(f + 3 * b + c, (unsigned long long) F[b][c]);
-    double *E = a.e_res;
-    E[(size_t) E_WATER * n + i] = e_water;
-    E[(size_t) E_PAIR * n + i] += e_ev;
   }
 }
 
-// DSSP hydrogen bonds and P_AP of the queued pairs, one thread per pair
-// (grid-stride over both queues).  Forces scatter with fixed-point atomics;
-// each pair's energy goes to its first residue in fixed point, so the sums
-// do not depend on the queue order.
+// DSSP hydrogen bonds and P_AP of the queued pairs, one thread per entry
+// (grid-stride over both queues).  A DSSP entry q >= 0 is pair q with O(i)
+// as acceptor; ~q is the same pair with O(j).  Forces scatter with
+// fixed-point atomics; each pair's energy goes to its acceptor (DSSP) or
+// lower residue (P_AP) in fixed point, so sums do not depend on the order.
 template <typename R> __global__ void __launch_bounds__(128) k_hbond(StepArgs<R> a, FFParams p)
 {
   const DevSys<R> &s = a.s;
   const int nd = a.nl->n_dssp, np = a.nl->n_pap, n = s.n_res;
-  const size_t qcap = (size_t) n * a.cap;
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nd + np; t += gridDim.x * blockDim.x) {
     const bool d = t < nd;
-    const int slot = d ? a.hbq[t] : a.hbq[qcap + (t - nd)];
-    const int i = slot / a.cap, j = a.nbr[slot];
-    R e = d ? dssp_term(s, p, i, j) : pap_term(s, p, i, j);
+    const int q = d ? a.hbq[t] : a.hbq[(size_t) 2 * a.pcap + (t - nd)];
+    const int2 ij = a.pairs[q < 0 ? ~q : q];
+    const int i = q < 0 ? ij.y : ij.x, j = q < 0 ? ij.x : ij.y;
+    const R e = d ? dssp_term(s, p, i, j) : pap_term(s, p, i, j);
     if (e != R(0))
       atomicAdd((unsigned long long *) (a.e_fix + (d ? 0 : (size_t) n) + i), (unsigned long long) fix_force((double) e));
   }
@@ -726,9 +742,11 @@ __global__ void k_thermo(const double *e_res, const long long *e_fix, int n_res,
   for (int r = sys_begin[rep] + threadIdx.x; r < sys_end[rep]; r += blockDim.x) {
     double fx = 0.0;
     for (int t = 1; t < E_FIX_TERMS; t++) fx += e_res[(size_t) t * n_res + r];
-    fx += (double) (e_fix[r] + e_fix[(size_t) n_res + r] + e_fix[(size_t) 2 * n_res + r]) * F_UNSCALE;
+    fx += (double) (e_fix[r] + e_fix[(size_t) n_res + r] + e_fix[(size_t) 2 * n_res + r] +
+                    e_fix[(size_t) 3 * n_res + r]) *
+          F_UNSCALE;
     acc[0] += fx;
-    acc[1] += e_res[(size_t) E_PAIR * n_res + r];
+    acc[1] += e_res[(size_t) E_PAIR * n_res + r] + (double) e_fix[(size_t) 4 * n_res + r] * F_UNSCALE;
     acc[2] += e_res[(size_t) E_BOND * n_res + r];
     acc[3] += e_res[(size_t) E_KIN * n_res + r];
   }
@@ -753,10 +771,11 @@ __global__ void k_energy_reduce(const double *e_res, const long long *e_fix, int
   const int t = blockIdx.x, rep = blockIdx.y;
   __shared__ double sh[256];
   double acc = 0.0;
-  // DSSP, P_AP and fragment-memory energies are kept in fixed point
-  const long long *fx = t == E_DSSP ? e_fix : t == E_PAP ? e_fix + n_res : t == E_FRAGMEM ? e_fix + 2 * (size_t) n_res : nullptr;
+  // pair-summed energies are kept in fixed point (e_fix slots)
+  const int k = t == E_DSSP ? 0 : t == E_PAP ? 1 : t == E_FRAGMEM ? 2 : t == E_WATER ? 3 : t == E_PAIR ? 4 : -1;
+  const long long *fx = k >= 0 ? e_fix + (size_t) k * n_res : nullptr;
   for (int r = sys_begin[rep] + threadIdx.x; r < sys_end[rep]; r += blockDim.x)
-    acc += fx ? (double) fx[r] * F_UNSCALE : e_res[(size_t) t * n_res + r];
+    acc += e_res[(size_t) t * n_res + r] + (fx ? (double) fx[r] * F_UNSCALE : 0.0);
   sh[threadIdx.x] = acc;
   __syncthreads();
   for (int w = blockDim.x / 2; w > 0; w >>= 1) {

@@ -221,17 +221,18 @@ def c3_seed(k: int, rank: int = 0) -> int:
 
 def algorithmic_bytes(kernel: str, info) -> float:
     """Bytes one launch must move at least (data layout of the engine):
-    fragmem -- every stored memory distance once, the row table, the two
+    fragmem -- every stored memory distance once, the block table, the two
     target beads per residue and the force accumulators it updates;
-    pair / density / water_xi -- the residue pair list once, every residue's
-    working coordinates and per-residue scalars once."""
-    n_res, n_atoms, records, rbytes, nd, cap, entries, nonuni = [int(v) for v in info]
+    pair / density / water_xi -- the residue pair array (8 bytes a pair)
+    once, every residue's working coordinates and per-residue scalars once,
+    the force accumulators once."""
+    n_res, n_atoms, records, rbytes, nd, pcap, npairs, nonuni = [int(v) for v in info]
     bead = 32
     if kernel == "fragmem":
-        return (records * 4 * rbytes + records * rbytes * nonuni + (n_res * nd + 1) * 4 + n_res * 2 * bead
+        return (records * 4 * rbytes + records * rbytes * nonuni + ((n_res + 31) // 32) * nd * 8 + n_res * 2 * bead
                 + n_res * 2 * 3 * 8 * 2)
     if kernel in ("pair", "density", "water_xi"):
-        return entries * 4 + n_res * 6 * bead + n_res * 10 * 8 + n_res * 4 * 4 + n_atoms * 3 * 8
+        return npairs * 8 + n_res * 6 * bead + n_res * 10 * 8 + n_res * 4 * 4 + n_atoms * 3 * 8
     if kernel == "prepare":
         return n_atoms * 3 * 8 + n_res * 6 * bead + n_atoms * 3 * 8 + n_res * 32
     if kernel == "finish":

@@ -164,7 +164,8 @@ int awsem_forces(awsem_system *sys, double *f);
 int awsem_residue_arrays(awsem_system *sys, double *out);
 
 /* Pair-list statistics: builds so far, current list radius (A), largest
- * neighbour count, overflow marker (0 when the list never overflowed). */
+ * number of higher-numbered partners of one residue, overflow marker (0 when
+ * the list never overflowed, else the pair count it needed). */
 int awsem_neighbor_stats(awsem_system *sys, int *nbuilds, double *radius, int *max_count, int *overflow);
 
 /* Current MD step counter. */
@@ -182,8 +183,8 @@ int awsem_profile_step(awsem_system *sys, int reps, double *ms);
 /* Sizes behind the roofline's algorithmic-byte counts:
  * info[0] residues, [1] atoms, [2] fragment-memory records (4 distances
  * each), [3] bytes per stored distance (8 FP64, 4 mixed), [4] rows per
- * residue, [5] pair-list capacity, [6] pair-list entries of the last build,
- * [7] non-uniform memory coefficients stored (0/1). */
+ * residue, [5] pair-list capacity (pairs), [6] residue pairs i < j in the
+ * list of the last build, [7] non-uniform memory coefficients stored (0/1). */
 int awsem_model_info(awsem_system *sys, long long *info);
 
 /* Fragment-memory forces and energy through an entry point that allocates
