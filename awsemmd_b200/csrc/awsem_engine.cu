@@ -6,6 +6,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <memory>
 #include <stdexcept>
 #include <string>
@@ -75,7 +76,9 @@ class EngineBase {
   int device = 0;
   long long step = 0;
   int n_sys() const { return in.n_sys; }
-  int rep_atoms(int r) const { return in.sys_atom_begin[r + 1] - in.sys_atom_begin[r]; }
+  // atoms are 3 per residue in internal order: a replica's atoms follow its residues
+  int rep_atom0(int r) const { return 3 * in.sys_res_begin[r]; }
+  int rep_atoms(int r) const { return 3 * (in.sys_res_end[r] - in.sys_res_begin[r]); }
   int rep_res(int r) const { return in.sys_res_end[r] - in.sys_res_begin[r]; }
   void commit()
   {
@@ -101,6 +104,16 @@ class EngineBase {
   virtual double run_ms() const = 0;
   // device-resident fragment-memory table, for entry points outside the engine
   virtual FMView fm_view() const = 0;
+  // serving handles (fixed capacity, requests admitted and released)
+  bool server = false;
+  virtual void server_setup(const SharedForceField &f, long long cap_res, int max_slots, long long cap_records,
+                            double dt, double damp) = 0;
+  virtual int admit(const ReplicaArrays &ra, unsigned long long seed, long long nsteps, double t_start,
+                    double t_stop) = 0;  // slot, or -1 when the request does not fit now
+  virtual void progress(int slot, long long *done, long long *total) = 0;
+  virtual void advance(long long nsteps) = 0;
+  virtual void release(int slot) = 0;
+  virtual void usage(long long *info) = 0;
 };
 
 void fragmem_noalloc(int device, const FMView &v, const double *d_x, double *d_f, double *d_energy,
@@ -129,8 +142,9 @@ template <typename R> class Engine : public EngineBase {
   DBuf<long long> dstep;
   DBuf<double> ev_pref, ev_cs, ev_cl;
   DBuf<unsigned> excl_self, excl_next;
-  DBuf<int> bond_start, bond_i, bond_j;
+  DBuf<int> bond_i, bond_j;
   DBuf<double> bond_k, bond_r0;
+  int bond_cap = 1;
   DBuf<int> fm_soff, fm_slen;
   DBuf<R> fm_rf, fm_coef;
   int fm_groups = 0, fm_dsplit = 1;
@@ -138,6 +152,10 @@ template <typename R> class Engine : public EngineBase {
   DBuf<int> res_sys, sys_begin, sys_end;
   DBuf<unsigned long long> sys_seed;
   int pcap = 0;  // residue pair list capacity (pairs)
+  // pair-list room per residue: 48 covers a compact globule (about 66
+  // partners within 16 A, half of them higher-numbered) with margin
+  int pairs_per_res = 48;
+  int prio_lo = 0, prio_hi = 0;  // stream priority range (prio_hi: highest)
   int groups_all = dev::G_FIX | dev::G_PAIR | dev::G_BOND;
   double skin = 2.0;
   int neigh_every = 0;
@@ -204,7 +222,7 @@ template <typename R> class Engine : public EngineBase {
     a.atom_type = atom_type.p;
     a.excl_self = excl_self.p;
     a.excl_next = excl_next.p;
-    a.bond_start = bond_start.p;
+    a.bond_cap = bond_cap;
     a.bond_i = bond_i.p;
     a.bond_j = bond_j.p;
     a.bond_k = bond_k.p;
@@ -224,14 +242,19 @@ template <typename R> class Engine : public EngineBase {
     a.sys_begin = sys_begin.p;
     a.sys_end = sys_end.p;
     a.sys_seed = sys_seed.p;
+    a.slot_run = slot_run.p;
     return a;
   }
 
   void setup() override
   {
     CK(cudaSetDevice(device));
-    CK(cudaStreamCreateWithFlags(&s0, cudaStreamNonBlocking));
-    CK(cudaStreamCreateWithFlags(&s1, cudaStreamNonBlocking));
+    // the pair-pass chain (s0) is the critical path: it gets the higher
+    // priority, so the block scheduler serves it first and the bandwidth-bound
+    // fragment-memory kernel (s1) fills the remaining room
+    CK(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
+    CK(cudaStreamCreateWithPriority(&s0, cudaStreamNonBlocking, prio_hi));
+    CK(cudaStreamCreateWithPriority(&s1, cudaStreamNonBlocking, prio_lo));
     CK(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
     CK(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
     const Topology &t = in.top;
@@ -240,6 +263,8 @@ template <typename R> class Engine : public EngineBase {
     sys_begin.upload(in.sys_res_begin, s0);
     sys_end.upload(in.sys_res_end, s0);
     sys_seed.alloc(std::max(in.n_sys, 1));
+    slot_run.alloc(std::max(in.n_sys, 1));
+    slot_run.zero(s0);
     energy.alloc((size_t) E_SLOTS * std::max(in.n_sys, 1));
     res_type.upload(t.res_type, s0);
     res_flags.upload(t.res_flags, s0);
@@ -262,6 +287,7 @@ template <typename R> class Engine : public EngineBase {
     e_res.alloc((size_t) E_SLOTS * nn);
     e_res.zero(s0);
     pos.alloc((size_t) dev::N_BEADS * nn);
+    pos.zero(s0);  // residues of no replica keep finite (zero) working positions
     cb_build.alloc(nn);
     cb_build.zero(s0);
     facc.alloc((size_t) 3 * na);
@@ -275,21 +301,21 @@ template <typename R> class Engine : public EngineBase {
     ev_cl.upload(t.ev_cl, s0);
     excl_self.upload(t.excl_self, s0);
     excl_next.upload(t.excl_next, s0);
-    // bonds grouped by the residue of their first atom (stable)
-    std::vector<int> order(t.bond_i.size());
-    for (size_t b = 0; b < order.size(); b++) order[b] = (int) b;
-    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return t.bond_i[a] / 3 < t.bond_i[b] / 3; });
-    std::vector<int> bs(nn + 1, 0), bi, bj;
-    std::vector<double> bk, br;
-    for (int b : order) {
-      bs[t.bond_i[b] / 3 + 1]++;
-      bi.push_back(t.bond_i[b]);
-      bj.push_back(t.bond_j[b]);
-      bk.push_back(t.bond_k[b]);
-      br.push_back(t.bond_r0[b]);
+    // bonds in fixed slots per residue of their first atom, in input order
+    std::vector<int> cnt(nn, 0);
+    for (size_t b = 0; b < t.bond_i.size(); b++) cnt[t.bond_i[b] / 3]++;
+    bond_cap = std::max(1, nn ? *std::max_element(cnt.begin(), cnt.end()) : 1);
+    std::vector<int> bi((size_t) nn * bond_cap, -1), bj((size_t) nn * bond_cap, -1);
+    std::vector<double> bk((size_t) nn * bond_cap, 0.0), br((size_t) nn * bond_cap, 0.0);
+    std::fill(cnt.begin(), cnt.end(), 0);
+    for (size_t b = 0; b < t.bond_i.size(); b++) {
+      int r = t.bond_i[b] / 3;
+      size_t at = (size_t) r * bond_cap + cnt[r]++;
+      bi[at] = t.bond_i[b];
+      bj[at] = t.bond_j[b];
+      bk[at] = t.bond_k[b];
+      br[at] = t.bond_r0[b];
     }
-    for (int r = 0; r < nn; r++) bs[r + 1] += bs[r];
-    bond_start.upload(bs, s0);
     bond_i.upload(bi, s0);
     bond_j.upload(bj, s0);
     bond_k.upload(bk, s0);
@@ -323,7 +349,7 @@ template <typename R> class Engine : public EngineBase {
     CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
     hb_blocks = std::max(1, std::min((nn * 8 + 127) / 128, 16 * sms));
     // size the pair list from a first build: room for 4x the initial pairs
-    // (chains that collapse gain neighbours), at least 24 per residue
+    // (chains that collapse gain neighbours), at least pairs_per_res per residue
     resize_pairs(std::max<long long>(64, 16LL * nn));
     for (int attempt = 0; attempt < 8; attempt++) {
       launch_prepare_and_list(args(groups_all), s0, true, false);
@@ -331,8 +357,9 @@ template <typename R> class Engine : public EngineBase {
       CK(cudaMemcpyAsync(&got, nl.p, sizeof got, cudaMemcpyDeviceToHost, s0));
       CK(cudaStreamSynchronize(s0));
       if (!got.overflow) {
-        long long want = std::max(4LL * got.npairs, 24LL * nn) + 1024;
-        pair_blocks = (int) std::max(1LL, std::min<long long>((3LL * got.npairs / 2 + 127) / 128, 16LL * sms));
+        long long want = std::max(4LL * got.npairs, (long long) pairs_per_res * nn) + 1024;
+        long long expect = std::max(3LL * got.npairs / 2, 12LL * nn);
+        pair_blocks = (int) std::max(1LL, std::min<long long>((expect + 127) / 128, 16LL * sms));
         if (want > pcap) {
           resize_pairs(want);
           continue;
@@ -475,7 +502,7 @@ template <typename R> class Engine : public EngineBase {
   {
     check_rep(rep);
     const std::vector<int> &ext = in.ext_of[rep];
-    int a0 = in.sys_atom_begin[rep], na = rep_atoms(rep);
+    int a0 = rep_atom0(rep), na = rep_atoms(rep);
     std::vector<double> bx((size_t) 3 * na), bv((size_t) 3 * na);
     for (int a = 0; a < na; a++)
       for (int k = 0; k < 3; k++) {
@@ -491,7 +518,7 @@ template <typename R> class Engine : public EngineBase {
   {
     check_rep(rep);
     const std::vector<int> &ext = in.ext_of[rep];
-    int a0 = in.sys_atom_begin[rep], na = rep_atoms(rep);
+    int a0 = rep_atom0(rep), na = rep_atoms(rep);
     std::vector<double> hx2((size_t) 3 * na), hv2((size_t) 3 * na);
     CK(cudaMemcpyAsync(hx2.data(), x.p + 3 * (size_t) a0, sizeof(double) * 3 * na, cudaMemcpyDeviceToHost, s0));
     CK(cudaMemcpyAsync(hv2.data(), v.p + 3 * (size_t) a0, sizeof(double) * 3 * na, cudaMemcpyDeviceToHost, s0));
@@ -509,6 +536,7 @@ template <typename R> class Engine : public EngineBase {
   cudaGraphExec_t graphs[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [thermo][chunk]
   static constexpr int kChunk = 25;
   DBuf<dev::Integrator> d_integ;
+  DBuf<dev::SlotRun> slot_run;  // [n_sys] run window of each replica
   long long thermo_nrows = 1;
   cudaEvent_t ev_run0 = nullptr, ev_run1 = nullptr;
   double last_run_ms = 0.0;
@@ -527,8 +555,29 @@ template <typename R> class Engine : public EngineBase {
                                                thermo_nrows, thermo_rows.p);
     }
     CK(cudaStreamEndCapture(s0, &graph));
+    set_node_priorities(graph);
     CK(cudaGraphInstantiate(&exec, graph, 0));
     CK(cudaGraphDestroy(graph));
+  }
+
+  // Kernel nodes keep the priority of the stream they were captured from
+  // (fragment memory low, everything else high), set explicitly per node.
+  void set_node_priorities(cudaGraph_t graph)
+  {
+    size_t count = 0;
+    CK(cudaGraphGetNodes(graph, nullptr, &count));
+    std::vector<cudaGraphNode_t> nodes(count);
+    CK(cudaGraphGetNodes(graph, nodes.data(), &count));
+    for (cudaGraphNode_t node : nodes) {
+      cudaGraphNodeType type;
+      CK(cudaGraphNodeGetType(node, &type));
+      if (type != cudaGraphNodeTypeKernel) continue;
+      cudaKernelNodeParams kp;
+      CK(cudaGraphKernelNodeGetParams(node, &kp));
+      cudaLaunchAttributeValue v;
+      v.priority = kp.func == (void *) dev::k_fragmem<R> ? prio_lo : prio_hi;
+      CK(cudaGraphKernelNodeSetAttribute(node, cudaLaunchAttributePriority, &v));
+    }
   }
 
   void release_graphs()
@@ -549,11 +598,21 @@ template <typename R> class Engine : public EngineBase {
     CK(cudaMemcpyAsync(d_integ.p, &integ, sizeof integ, cudaMemcpyHostToDevice, s0));
   }
 
+  // One run window for every replica (a run of the whole batch): steps
+  // begin..end, noise keyed by the absolute step.
+  void upload_runs(const awsem_run_params &rp, long long begin, long long end)
+  {
+    upload_integrator(make_integrator(rp, begin));
+    std::vector<dev::SlotRun> w(n_sys(), dev::SlotRun{begin, end, 0, rp.t_start, rp.t_stop});
+    CK(cudaMemcpyAsync(slot_run.p, w.data(), sizeof(dev::SlotRun) * w.size(), cudaMemcpyHostToDevice, s0));
+    CK(cudaStreamSynchronize(s0));
+  }
+
   void profile(int reps, double *ms) override
   {
     if (reps <= 0) throw std::invalid_argument("reps must be positive");
     set_thermostat(last_rp);
-    upload_integrator(make_integrator(last_rp, step, step + reps + 1));
+    upload_runs(last_rp, step, step + reps + 1);
     long long pre = step;  // profiled steps continue the trajectory
     CK(cudaMemcpyAsync(dstep.p, &pre, sizeof pre, cudaMemcpyHostToDevice, s0));
     const FFParams &p = in.ff.p;
@@ -697,18 +756,14 @@ template <typename R> class Engine : public EngineBase {
     thermostat_rp = rp;
   }
 
-  dev::Integrator make_integrator(const awsem_run_params &rp, long long begin, long long end)
+  dev::Integrator make_integrator(const awsem_run_params &rp, long long begin)
   {
     dev::Integrator integ{};
     integ.dt = rp.dt;
     integ.dtf = 0.5 * rp.dt * FTM2V;
     integ.langevin = rp.langevin;
-    integ.t_start = rp.t_start;
-    integ.t_stop = rp.t_stop;
     integ.begin = begin;
-    integ.end = end;
     integ.damp = rp.damp;
-    integ.seed = rp.seed;
     return integ;
   }
 
@@ -726,7 +781,7 @@ template <typename R> class Engine : public EngineBase {
       neigh_every = rp.neigh_every;
       set_nl_field(&dev::NLState::every, neigh_every);
     }
-    upload_integrator(make_integrator(rp, step, step + nsteps));
+    upload_runs(rp, step, step + nsteps);
     // Langevin seed of each replica: its own when set, else the run's
     std::vector<unsigned long long> sd(n_sys());
     for (int k = 0; k < n_sys(); k++) sd[k] = seeds[k] ? seeds[k] : rp.seed;
@@ -796,7 +851,7 @@ template <typename R> class Engine : public EngineBase {
   {
     check_rep(rep);
     const std::vector<int> &ext = in.ext_of[rep];
-    int a0 = in.sys_atom_begin[rep], na = rep_atoms(rep);
+    int a0 = rep_atom0(rep), na = rep_atoms(rep);
     std::vector<double> f((size_t) 3 * na);
     CK(cudaMemcpyAsync(f.data(), ftot.p + 3 * (size_t) a0, sizeof(double) * 3 * na, cudaMemcpyDeviceToHost, s0));
     CK(cudaStreamSynchronize(s0));
@@ -830,6 +885,405 @@ template <typename R> class Engine : public EngineBase {
     if (radius) *radius = st.r_list;
     if (overflow) *overflow = st.overflow;
     if (maxc) *maxc = max_count();
+  }
+
+  // ----------------------------------------------------------------------
+  // Serving: a fixed-capacity handle whose replicas (requests) come and go.
+  // Residues are handed out in 32-residue groups (one fragment-memory group
+  // never mixes requests) and memory records in 32-record stripes, first
+  // fit; all device arrays are allocated once at creation, so admission
+  // and release only copy a request's data in or out.
+  struct Slot {
+    bool used = false;
+    int base = 0, n_res = 0, groups = 0;
+    long long stripe0 = 0, stripes = 0;
+    long long begin = 0, end = 0;  // run window (device steps)
+  };
+  std::vector<Slot> slots;
+  std::map<long long, long long> free_groups, free_stripes;  // start -> length
+  const SharedForceField *sf = nullptr;
+  awsem_run_params srv_rp{};
+  long long stripe_cap = 0;
+  bool fm_coef_mode = false, fm_uniform_known = false;
+
+  static bool take_range(std::map<long long, long long> &fr, long long want, long long &at)
+  {
+    if (want == 0) {
+      at = 0;
+      return true;
+    }
+    for (auto it = fr.begin(); it != fr.end(); ++it)
+      if (it->second >= want) {
+        at = it->first;
+        long long rest = it->second - want;
+        fr.erase(it);
+        if (rest) fr[at + want] = rest;
+        return true;
+      }
+    return false;
+  }
+
+  static void give_range(std::map<long long, long long> &fr, long long at, long long len)
+  {
+    if (len == 0) return;
+    auto it = fr.emplace(at, len).first;
+    auto nx = std::next(it);
+    if (nx != fr.end() && it->first + it->second == nx->first) {
+      it->second += nx->second;
+      fr.erase(nx);
+    }
+    if (it != fr.begin()) {
+      auto pv = std::prev(it);
+      if (pv->first + pv->second == it->first) {
+        pv->second += it->second;
+        fr.erase(it);
+      }
+    }
+  }
+
+  template <typename T> void put(DBuf<T> &b, size_t at, const T *src, size_t count)
+  {
+    if (count) CK(cudaMemcpyAsync(b.p + at, src, count * sizeof(T), cudaMemcpyHostToDevice, s0));
+  }
+  template <typename T> void fill(DBuf<T> &b, size_t at, size_t count, T value)
+  {
+    std::vector<T> h(count, value);
+    put(b, at, h.data(), count);
+    CK(cudaStreamSynchronize(s0));
+  }
+
+  void server_setup(const SharedForceField &f, long long cap_res, int max_slots, long long cap_records, double dt,
+                    double damp) override
+  {
+    if (cap_res <= 0 || max_slots <= 0 || cap_records < 0) throw std::invalid_argument("server capacities must be positive");
+    if (dt <= 0 || damp <= 0) throw std::invalid_argument("dt and damp must be positive");
+    const long long groups = (cap_res + 31) / 32;
+    if (groups * 32 * pairs_per_res >= (1ll << 31)) throw std::invalid_argument("residue capacity too large");
+    sf = &f;
+    server = true;
+    const int nn = (int) (groups * 32);
+    pairs_per_res = 64;  // requests that anneal collapse: room for the densest packing
+    in = Batch();
+    in.ff = f.ff;
+    FFParams &p = in.ff.p;
+    int nd = 0;
+    if (p.terms & T_FM) {
+      const int ms = f.gamma.min_sep(), xs = f.gamma.max_sep();
+      nd = xs == -1 ? 64 - ms : xs - ms + 1;
+      p.fm_min_sep = ms;
+    }
+    p.fm_nd = nd;
+    Topology &t = in.top;
+    t.n_res = nn;
+    t.n_atoms = 3 * nn;
+    t.n_chains = nn;
+    t.ntypes = 5;
+    set_pair_coeffs(t, f.pair_style, f.pair_coeffs);
+    // residues of no request: flagged chain ends of no chain, fully excluded
+    t.res_type.assign(nn, 0);
+    t.res_flags.assign(nn, R_FIRST | R_LAST);
+    t.res_chain.assign(nn, -1);
+    t.chain_start.assign(nn, 0);  // chain ids are the global index of a chain's first residue
+    t.chain_end.assign(nn, 0);
+    t.aps.assign((size_t) 12 * nn, 0.0);
+    t.atom_type.assign(3 * nn, 1);
+    t.atom_tag.assign(3 * nn, 0);
+    t.mass.assign(3 * nn, 1.0);
+    t.excl_self.assign(nn, 0x1ffu);
+    t.excl_next.assign(nn, 0u);
+    in.x.assign((size_t) 9 * nn, 0.0);
+    in.v.assign((size_t) 9 * nn, 0.0);
+    in.res_sys.assign(nn, -1);
+    in.n_sys = max_slots;
+    in.sys_res_begin.assign(max_slots, 0);
+    in.sys_res_end.assign(max_slots, 0);
+    in.ext_of.assign(max_slots, std::vector<int>());
+    in.fm.nd = nd;
+    in.fm.row_start.assign((size_t) nn * nd + 1, 0);
+    in.fm.uniform = true;
+    seeds.assign(max_slots, 0ull);
+    setup();
+    committed = true;
+    // four bond slots per residue: CA-O, CA-CB/HB, CA-CA(+1), O-CA(+1)
+    bond_cap = 4;
+    bond_i.alloc((size_t) 4 * nn);
+    bond_j.alloc((size_t) 4 * nn);
+    bond_k.alloc((size_t) 4 * nn);
+    bond_r0.alloc((size_t) 4 * nn);
+    fill(bond_i, 0, (size_t) 4 * nn, -1);
+    // memory-record pool (stripes of 32 records)
+    stripe_cap = (cap_records + 31) / 32;
+    fm_rf.alloc((size_t) std::max(stripe_cap, 1LL) * 32 * 4);
+    if (stripe_cap) free_stripes[0] = stripe_cap;
+    free_groups[0] = groups;
+    slots.assign(max_slots, Slot());
+    srv_rp = awsem_run_params{dt, 1, 300.0, 300.0, damp, 1ull, skin, 0};
+    upload_integrator(make_integrator(srv_rp, step + 1));
+    CK(cudaStreamSynchronize(s0));
+    release_graphs();  // buffers were reallocated after setup
+  }
+
+  // Langevin factors (fix langevin, units real) of atoms [a0, a0 + na) with masses m
+  void set_thermostat_factors(int a0, const double *m, int na)
+  {
+    std::vector<double> h1(na), h2(na);
+    for (int a = 0; a < na; a++) {
+      h1[a] = -m[a] / srv_rp.damp / FTM2V;
+      h2[a] = sqrt(m[a]) * sqrt(24.0 * BOLTZ / srv_rp.damp / srv_rp.dt / MVV2E) / FTM2V;
+    }
+    put(g1, a0, h1.data(), na);
+    put(g2, a0, h2.data(), na);
+    CK(cudaStreamSynchronize(s0));
+  }
+
+  int admit(const ReplicaArrays &ra, unsigned long long seed, long long nsteps, double t_start, double t_stop) override
+  {
+    if (nsteps < 0) throw std::invalid_argument("nsteps must be >= 0");
+    if (t_start < 0 || t_stop < 0) throw std::invalid_argument("temperatures must be >= 0");
+    SystemInput S;
+    load_system_arrays(*sf, ra, S);
+    const Topology &t = S.top;
+    const FMTable &fm = S.fm;
+    const int nd = in.ff.p.fm_nd, n = t.n_res, groups = (n + 31) / 32;
+    if ((in.ff.p.terms & T_FM) && fm.nd > nd)
+      throw std::invalid_argument("memory separations exceed the fragment-memory table of this handle");
+    // coefficient mode: a uniform coefficient shared by every request so far,
+    // else a per-record coefficient pool
+    if ((in.ff.p.terms & T_FM) && fm.records() > 0 && !fm_coef_mode) {
+      if (!fm_uniform_known && fm.uniform) {
+        in.fm.uniform_coef = fm.uniform_coef;
+        fm_uniform_known = true;
+        release_graphs();
+      } else if (!fm.uniform || fm.uniform_coef != in.fm.uniform_coef) {
+        fm_coef_mode = true;
+        in.fm.uniform = false;
+        fm_coef.alloc((size_t) std::max(stripe_cap, 1LL) * 32);
+        fill(fm_coef, 0, (size_t) std::max(stripe_cap, 1LL) * 32, (R) in.fm.uniform_coef);
+        release_graphs();
+      }
+    }
+    // slices of the request's rows (local groups)
+    std::vector<int> slen((size_t) groups * std::max(nd, 1), 0);
+    long long stripes = 0;
+    for (int g = 0; g < groups; g++)
+      for (int d = 0; d < fm.nd; d++) {
+        int len = 0;
+        for (int l = 0; l < 32 && 32 * g + l < n; l++) {
+          size_t row = (size_t) (32 * g + l) * fm.nd + d;
+          len = std::max(len, fm.row_start[row + 1] - fm.row_start[row]);
+        }
+        slen[(size_t) g * nd + d] = len;
+        stripes += len;
+      }
+    int slot_id = -1;
+    for (int k = 0; k < (int) slots.size(); k++)
+      if (!slots[k].used) {
+        slot_id = k;
+        break;
+      }
+    long long g0 = 0, st0 = 0;
+    if (slot_id < 0 || !take_range(free_groups, groups, g0)) return -1;
+    if (!take_range(free_stripes, stripes, st0)) {
+      give_range(free_groups, g0, groups);
+      return -1;
+    }
+    const int base = (int) (g0 * 32), N = n_res_cap();
+    // topology at residue offset `base`; chain ids are global first residues
+    std::vector<int> rc(n), cs(t.n_chains), ce(t.n_chains);
+    for (int r = 0; r < n; r++) rc[r] = base + t.chain_start[t.res_chain[r]];
+    put(res_type, base, t.res_type.data(), n);
+    put(res_flags, base, t.res_flags.data(), n);
+    put(res_chain, base, rc.data(), n);
+    for (int c = 0; c < t.n_chains; c++) {
+      int id = base + t.chain_start[c], a = base + t.chain_start[c], b = base + t.chain_end[c];
+      put(chain_start, id, &a, 1);
+      put(chain_end, id, &b, 1);
+      CK(cudaStreamSynchronize(s0));  // a and b are reused
+    }
+    for (int k = 0; k < 12; k++) put(aps, (size_t) k * N + base, t.aps.data() + (size_t) k * n, n);
+    put(atom_tag, 3 * base, t.atom_tag.data(), 3 * n);
+    put(atom_type, 3 * base, t.atom_type.data(), 3 * n);
+    put(mass, 3 * base, t.mass.data(), 3 * n);
+    put(x, (size_t) 9 * base, S.x.data(), (size_t) 9 * n);
+    put(v, (size_t) 9 * base, S.v.data(), (size_t) 9 * n);
+    std::vector<unsigned> es(t.excl_self.begin(), t.excl_self.end()), en(t.excl_next.begin(), t.excl_next.end());
+    put(excl_self, base, es.data(), n);
+    put(excl_next, base, en.data(), n);
+    // bonds: slots of the residue of their first atom
+    std::vector<int> bi((size_t) 4 * n, -1), bj((size_t) 4 * n, -1), cnt(n, 0);
+    std::vector<double> bk((size_t) 4 * n, 0.0), br((size_t) 4 * n, 0.0);
+    for (size_t b = 0; b < t.bond_i.size(); b++) {
+      int r = t.bond_i[b] / 3;
+      if (cnt[r] >= 4) throw std::invalid_argument("more than four bonds start at one residue");
+      size_t at = (size_t) 4 * r + cnt[r]++;
+      bi[at] = t.bond_i[b] + 3 * base;
+      bj[at] = t.bond_j[b] + 3 * base;
+      bk[at] = t.bond_k[b];
+      br[at] = t.bond_r0[b];
+    }
+    put(bond_i, (size_t) 4 * base, bi.data(), 4 * n);
+    put(bond_j, (size_t) 4 * base, bj.data(), 4 * n);
+    put(bond_k, (size_t) 4 * base, bk.data(), 4 * n);
+    put(bond_r0, (size_t) 4 * base, br.data(), 4 * n);
+    // fragment memory: the request's blocks at stripe st0
+    if (nd > 0) {
+      std::vector<int> soff((size_t) groups * nd, 0);
+      std::vector<R> rf((size_t) stripes * 32 * 4, R(FMTable::FM_SKIP)), cf(fm_coef_mode ? (size_t) stripes * 32 : 0, R(0));
+      long long at_stripe = 0;
+      for (int g = 0; g < groups; g++)
+        for (int d = 0; d < nd; d++) {
+          const size_t blk = (size_t) g * nd + d;
+          soff[blk] = (int) (st0 + at_stripe);
+          for (int l = 0; l < 32 && 32 * g + l < n && d < fm.nd; l++) {
+            size_t row = (size_t) (32 * g + l) * fm.nd + d;
+            for (int m = 0, rec = fm.row_start[row]; rec < fm.row_start[row + 1]; m++, rec++) {
+              size_t e = (size_t) (at_stripe + m) * 32 + l;
+              for (int k = 0; k < 4; k++) rf[e * 4 + k] = (R) fm.rf[(size_t) rec * 4 + k];
+              if (fm_coef_mode) cf[e] = (R) (fm.uniform ? fm.uniform_coef : fm.coef[rec]);
+            }
+          }
+          at_stripe += slen[blk];
+        }
+      put(fm_soff, (size_t) g0 * nd, soff.data(), soff.size());
+      put(fm_slen, (size_t) g0 * nd, slen.data(), slen.size());
+      put(fm_rf, (size_t) st0 * 32 * 4, rf.data(), rf.size());
+      if (fm_coef_mode) put(fm_coef, (size_t) st0 * 32, cf.data(), cf.size());
+      CK(cudaStreamSynchronize(s0));
+    }
+    // run window: the next evaluation is this request's setup evaluation
+    Slot &sl = slots[slot_id];
+    sl.used = true;
+    sl.base = base;
+    sl.n_res = n;
+    sl.groups = groups;
+    sl.stripe0 = st0;
+    sl.stripes = stripes;
+    sl.begin = step + 1;
+    sl.end = step + 1 + nsteps;
+    dev::SlotRun w{sl.begin, sl.end, sl.begin, t_start, t_stop};
+    int b0 = base, b1 = base + n;
+    put(slot_run, slot_id, &w, 1);
+    put(sys_begin, slot_id, &b0, 1);
+    put(sys_end, slot_id, &b1, 1);
+    put(sys_seed, slot_id, &seed, 1);
+    std::vector<int> rs(n, slot_id);
+    put(res_sys, base, rs.data(), n);
+    CK(cudaStreamSynchronize(s0));
+    set_thermostat_factors(3 * base, t.mass.data(), 3 * n);
+    in.sys_res_begin[slot_id] = base;
+    in.sys_res_end[slot_id] = base + n;
+    in.ext_of[slot_id] = t.ext_of;
+    seeds[slot_id] = seed;
+    set_nl_field(&dev::NLState::r_list, 0.f);  // the next evaluation rebuilds the pair list
+    return slot_id;
+  }
+
+  int n_res_cap() const { return in.top.n_res; }
+
+  void check_slot(int k) const
+  {
+    if (!server) throw std::invalid_argument("not a serving handle");
+    if (k < 0 || k >= (int) slots.size() || !slots[k].used) throw std::invalid_argument("no request in this slot");
+  }
+
+  void progress(int k, long long *done, long long *total) override
+  {
+    check_slot(k);
+    const Slot &sl = slots[k];
+    if (total) *total = sl.end - sl.begin;
+    if (done) *done = std::max(0LL, std::min(step, sl.end) - sl.begin);
+  }
+
+  void advance(long long nsteps) override
+  {
+    if (!server) throw std::invalid_argument("not a serving handle");
+    if (nsteps <= 0) return;
+    if (!graphs[0][0]) capture_steps(graphs[0][0], 1, false);
+    if (nsteps >= kChunk && !graphs[0][1]) capture_steps(graphs[0][1], kChunk, false);
+    if (!ev_run0) {
+      CK(cudaEventCreate(&ev_run0));
+      CK(cudaEventCreate(&ev_run1));
+    }
+    long long done = 0;
+    CK(cudaEventRecord(ev_run0, s0));
+    while (nsteps - done >= kChunk) {
+      CK(cudaGraphLaunch(graphs[0][1], s0));
+      done += kChunk;
+    }
+    while (done < nsteps) {
+      CK(cudaGraphLaunch(graphs[0][0], s0));
+      done++;
+    }
+    CK(cudaEventRecord(ev_run1, s0));
+    CK(cudaStreamSynchronize(s0));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, ev_run0, ev_run1));
+    last_run_ms = ms;
+    step += nsteps;
+    check_list();
+  }
+
+  void release(int k) override
+  {
+    check_slot(k);
+    Slot &sl = slots[k];
+    const int base = sl.base, n = sl.n_res, N = n_res_cap();
+    (void) N;
+    fill(res_sys, base, n, -1);
+    fill(res_flags, base, n, (int) (R_FIRST | R_LAST));
+    fill(res_chain, base, n, -1);
+    fill(excl_self, base, n, 0x1ffu);
+    fill(excl_next, base, n, 0u);
+    fill(bond_i, (size_t) 4 * base, (size_t) 4 * n, -1);
+    fill(x, (size_t) 9 * base, (size_t) 9 * n, 0.0);
+    fill(v, (size_t) 9 * base, (size_t) 9 * n, 0.0);
+    const int nd = in.ff.p.fm_nd;
+    if (nd > 0) fill(fm_slen, (size_t) (base / 32) * nd, (size_t) sl.groups * nd, 0);
+    int zero = 0;
+    dev::SlotRun w{0, 0, 0, 0.0, 0.0};
+    put(sys_begin, k, &zero, 1);
+    put(sys_end, k, &zero, 1);
+    put(slot_run, k, &w, 1);
+    CK(cudaStreamSynchronize(s0));
+    give_range(free_groups, base / 32, sl.groups);
+    give_range(free_stripes, sl.stripe0, sl.stripes);
+    in.sys_res_begin[k] = in.sys_res_end[k] = 0;
+    in.ext_of[k].clear();
+    sl = Slot();
+    set_nl_field(&dev::NLState::r_list, 0.f);
+  }
+
+  void usage(long long *info) override
+  {
+    if (!server) throw std::invalid_argument("not a serving handle");
+    long long active = 0, res = 0, free_st = 0;
+    for (const Slot &sl : slots)
+      if (sl.used) {
+        active++;
+        res += 32LL * sl.groups;
+      }
+    for (auto &kv : free_stripes) free_st += kv.second;
+    info[0] = active;
+    info[1] = res;
+    info[2] = n_res_cap();
+    info[3] = 32 * (stripe_cap - free_st);
+    info[4] = 32 * stripe_cap;
+    info[5] = device_bytes();
+    info[6] = step;
+    info[7] = (long long) slots.size();
+  }
+
+  long long device_bytes() const
+  {
+    long long b = 0;
+    auto add = [&](const auto &buf) { b += (long long) (buf.n * sizeof(*buf.p)); };
+    add(res_type), add(res_flags), add(res_chain), add(chain_start), add(chain_end), add(atom_tag), add(atom_type);
+    add(aps), add(tables), add(x), add(v), add(mass), add(g1), add(g2), add(ftot), add(work), add(e_res), add(energy);
+    add(pos), add(cb_build), add(facc), add(pairs), add(ncount), add(hbq), add(dacc), add(e_fix), add(nl), add(dstep);
+    add(ev_pref), add(ev_cs), add(ev_cl), add(excl_self), add(excl_next), add(bond_i), add(bond_j), add(bond_k);
+    add(bond_r0), add(fm_soff), add(fm_slen), add(fm_rf), add(fm_coef), add(thermo_rows), add(res_sys), add(sys_begin);
+    add(sys_end), add(sys_seed), add(slot_run), add(d_integ);
+    return b;
   }
 };
 
@@ -1063,7 +1517,109 @@ int awsem_run(awsem_system *sys, long long nsteps, const awsem_run_params *rp, d
     g_last_error = "awsem_run: dt and damp must be positive, temperatures non-negative";
     return AWSEM_EINVAL;
   }
+  if (sys->eng->server) {
+    g_last_error = "awsem_run: a serving handle advances with awsem_server_advance";
+    return AWSEM_EINVAL;
+  }
   return guarded([&] { sys->eng->run(nsteps, *rp, thermo); });
+}
+
+// --------------------------------------------------------------------------
+// Serving
+
+int awsem_server_create(const char *workdir, const char *coeff_file, const char *pair_style, const char *pair_coeffs,
+                        int precision, int device, long long max_residues, int max_requests,
+                        long long max_memory_records, double dt, double damp, awsem_system **out)
+{
+  if (!out || !coeff_file || !pair_style) {
+    g_last_error = "awsem_server_create: null argument";
+    return AWSEM_EINVAL;
+  }
+  int rc = awsem_batch_create(precision, device, out);
+  if (rc != AWSEM_OK) return rc;
+  rc = awsem_batch_set_forcefield(*out, workdir, coeff_file, pair_style, pair_coeffs);
+  if (rc == AWSEM_OK) {
+    awsem_system *sys = *out;
+    rc = guarded([&] {
+      CK(cudaSetDevice(sys->eng->device));
+      sys->eng->server_setup(*sys->shared, max_residues, max_requests, max_memory_records, dt, damp);
+    });
+  }
+  if (rc != AWSEM_OK) {
+    std::string keep = g_last_error;
+    awsem_destroy(*out);
+    *out = nullptr;
+    g_last_error = keep;
+  }
+  return rc;
+}
+
+static bool serving(const awsem_system *sys, const char *what)
+{
+  if (!sys || !sys->eng->server) {
+    g_last_error = std::string(what) + ": not a serving handle";
+    return false;
+  }
+  return true;
+}
+
+int awsem_server_admit(awsem_system *sys, const awsem_replica_desc *d, long long nsteps, double t_start,
+                       double t_stop, int *slot)
+{
+  if (!serving(sys, "awsem_server_admit")) return AWSEM_EINVAL;
+  if (!d) {
+    g_last_error = "awsem_server_admit: null request";
+    return AWSEM_EINVAL;
+  }
+  int got = -1;
+  int rc = guarded([&] {
+    CK(cudaSetDevice(sys->eng->device));
+    ReplicaArrays ra{d->n_res, d->n_chains, d->chain_len, d->seq, d->ssweight, d->x, d->v, d->n_mem,
+                     d->mem_pos, d->mem_len, d->mem_weight, d->mem_seq, d->mem_ca, d->mem_cb};
+    got = sys->eng->admit(ra, d->seed, nsteps, t_start, t_stop);
+  });
+  if (rc != AWSEM_OK) return rc;
+  if (got < 0) {
+    g_last_error = "awsem_server_admit: no free slot, residue range or memory-record room now";
+    return AWSEM_EBUSY;
+  }
+  if (slot) *slot = got;
+  return AWSEM_OK;
+}
+
+int awsem_server_advance(awsem_system *sys, long long nsteps)
+{
+  if (!serving(sys, "awsem_server_advance")) return AWSEM_EINVAL;
+  return guarded([&] {
+    CK(cudaSetDevice(sys->eng->device));
+    sys->eng->advance(nsteps);
+  });
+}
+
+int awsem_server_progress(awsem_system *sys, int slot, long long *done, long long *total)
+{
+  if (!serving(sys, "awsem_server_progress")) return AWSEM_EINVAL;
+  return guarded([&] { sys->eng->progress(slot, done, total); });
+}
+
+int awsem_server_collect(awsem_system *sys, int slot, double *x, double *v, double *energies)
+{
+  if (!serving(sys, "awsem_server_collect")) return AWSEM_EINVAL;
+  return guarded([&] {
+    CK(cudaSetDevice(sys->eng->device));
+    long long done = 0, total = 0;
+    sys->eng->progress(slot, &done, &total);
+    if (done < total) throw std::invalid_argument("awsem_server_collect: the request has not finished");
+    if (x || v) sys->eng->get_state(slot, x, v);
+    if (energies) sys->eng->energies(slot, energies);
+    sys->eng->release(slot);
+  });
+}
+
+int awsem_server_usage(awsem_system *sys, long long *info)
+{
+  if (!serving(sys, "awsem_server_usage") || !info) return AWSEM_EINVAL;
+  return guarded([&] { sys->eng->usage(info); });
 }
 
 int awsem_residue_arrays(awsem_system *sys, double *out)

@@ -47,6 +47,14 @@ struct NLState {
   int npairs;         // pairs in the residue pair list (may exceed its capacity: overflow)
 };
 
+// Run window of one replica: integrated over steps begin..end (the
+// evaluation at `begin` is its setup evaluation), thermostat ramp t_start ->
+// t_stop over the window, Langevin noise keyed by step - step0.
+struct SlotRun {
+  long long begin, end, step0;
+  double t_start, t_stop;
+};
+
 template <typename R> struct StepArgs {
   DevSys<R> s;
   int n_atoms;
@@ -76,16 +84,20 @@ template <typename R> struct StepArgs {
   const double *ev_pref, *ev_cs, *ev_cl;
   const int *atom_type;
   const unsigned *excl_self, *excl_next;
-  // bonds grouped by the residue of their first atom
-  const int *bond_start, *bond_i, *bond_j;
+  // bonds in bond_cap slots per residue of their first atom ([n_res][bond_cap],
+  // internal atom indices; bond_i < 0 ends a residue's slots)
+  int bond_cap;
+  const int *bond_i, *bond_j;
   const double *bond_k, *bond_r0;
   // fragment memory
   FMSlices<R> fm;
   int groups;       // AWSEM_TERMS_* bits: 1 fix backbone, 2 pair vexcluded, 4 bonds
   long long *step;   // device step counter (advanced by k_nl_decide)
   // replicas: residue -> replica, replica residue ranges, Langevin seeds
+  // (res_sys < 0: residue of no replica, skipped)
   const int *res_sys, *sys_begin, *sys_end;
   const unsigned long long *sys_seed;
+  const SlotRun *slot_run;
 };
 
 enum Group { G_FIX = 1, G_PAIR = 2, G_BOND = 4 };
@@ -101,6 +113,12 @@ template <typename R> __global__ void k_prepare(StepArgs<R> a, FFParams p)
   int r = blockIdx.x * blockDim.x + threadIdx.x;
   float d2 = 0.f, oO = 0.f, oN = 0.f, oCA = 0.f, oAll = 0.f, oX = 0.f;
   if (r < a.s.n_res) {
+    unsigned long long *f = a.s.facc + (size_t) 9 * r;
+    for (int k = 0; k < 9; k++) f[k] = 0ull;
+    for (int k = 0; k < 5; k++) a.e_fix[(size_t) k * a.s.n_res + r] = 0;
+    for (int k = 0; k < 3; k++) a.dacc[(size_t) k * a.s.n_res + r] = 0;
+  }
+  if (r < a.s.n_res && a.res_sys[r] >= 0) {
     const double *x = a.x;
     int fl = a.s.res_flags[r];
     double ca[3], cb[3], o[3], n[3] = {0, 0, 0}, h[3] = {0, 0, 0}, cp[3] = {0, 0, 0};
@@ -129,10 +147,6 @@ template <typename R> __global__ void k_prepare(StepArgs<R> a, FFParams p)
     w[B_N] = make_double4(n[0], n[1], n[2], 0.0);
     w[B_H] = make_double4(h[0], h[1], h[2], 0.0);
     w[B_CP] = make_double4(cp[0], cp[1], cp[2], 0.0);
-    unsigned long long *f = a.s.facc + (size_t) 9 * r;
-    for (int k = 0; k < 9; k++) f[k] = 0ull;
-    for (int k = 0; k < 5; k++) a.e_fix[(size_t) k * a.s.n_res + r] = 0;
-    for (int k = 0; k < 3; k++) a.dacc[(size_t) k * a.s.n_res + r] = 0;
     {
       // reach of the residue's beads around its CA (excluded-volume prefilter)
       double ux = cb[0] - ca[0], uy = cb[1] - ca[1], uz = cb[2] - ca[2];
@@ -218,6 +232,10 @@ template <typename R> __global__ void k_nl_build(StepArgs<R> a)
   if (!a.nl->rebuild) return;
   const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   if (i >= a.s.n_res) return;
+  if (a.res_sys[i] < 0) {
+    if (lane == 0) a.ncount[i] = 0;
+    return;
+  }
   const int sys_end = a.sys_end[a.res_sys[i]];
   const DevSys<R> &s = a.s;
   const V3<double> ci = contact(s, i);
@@ -325,7 +343,7 @@ template <typename R> __global__ void k_residue(StepArgs<R> a, FFParams p)
 {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   const DevSys<R> &s = a.s;
-  if (i >= s.n_res) return;
+  if (i >= s.n_res || a.res_sys[i] < 0) return;
   // the per-residue backbone terms (chain, chi, rama, helical pair) are a
   // small share of the work and some are sums of steep Gaussians: FP64 in
   // both forms
@@ -640,7 +658,7 @@ template <typename R> __global__ void k_bonds(StepArgs<R> a)
   const DevSys<R> &s = a.s;
   if (r >= s.n_res) return;
   double e = 0.0;
-  for (int b = a.bond_start[r]; b < a.bond_start[r + 1]; b++) {
+  for (int b = r * a.bond_cap; b < (r + 1) * a.bond_cap && a.bond_i[b] >= 0; b++) {
     int ai = a.bond_i[b], aj = a.bond_j[b];
     V3<R> d = diff<R>(bead(s, ai / 3, ai % 3), bead(s, aj / 3, aj % 3));
     R rr = m_sqrt(norm2(d));
@@ -674,29 +692,34 @@ __device__ __forceinline__ double uniform01(uint64_t seed, long long step, long 
 struct Integrator {
   double dt, dtf;           // dtf = 0.5 * dt * ftm2v
   int langevin;
-  double t_start, t_stop;   // thermostat ramp over [begin, end]
-  long long begin, end;
   double damp;
-  unsigned long long seed;
+  long long begin;          // first step of the current run (thermo row 0)
 };
 
 // Total force (fixed point -> FP64, plus Langevin at `step`), then
 // final_integrate of `step` (half kick) and, if `next`, initial_integrate of
-// step+1 (half kick + drift) -- LAMMPS fix nve / fix langevin order.
+// step+1 (half kick + drift) -- LAMMPS fix nve / fix langevin order.  Each
+// replica follows its own run window (SlotRun); outside it the replica is
+// frozen, and residues of no replica are skipped.
 template <typename R>
 __global__ void k_finish(StepArgs<R> a, const Integrator *inp, const double *g1, const double *g2, double *ftot,
                          double *x_out)
 {
   int r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= a.s.n_res) return;
+  const int rep = a.res_sys[r];
+  if (rep < 0) return;
   const Integrator in = *inp;
+  const SlotRun sr = a.slot_run[rep];
   const long long step = *a.step;
-  const bool final_kick = step > in.begin, next = step < in.end;
-  const unsigned long long seed = a.sys_seed[a.res_sys[r]];
+  if (step < sr.begin || step > sr.end) return;
+  const bool final_kick = step > sr.begin, next = step < sr.end;
+  const unsigned long long seed = a.sys_seed[rep];
+  const long long key = step - sr.step0;  // the replica's own step count keys its noise
   double tsqrt = 0.0;
   if (in.langevin) {
-    double delta = in.end != in.begin ? (double) (step - in.begin) / (double) (in.end - in.begin) : 0.0;
-    tsqrt = sqrt(in.t_start + delta * (in.t_stop - in.t_start));
+    double delta = sr.end != sr.begin ? (double) (step - sr.begin) / (double) (sr.end - sr.begin) : 0.0;
+    tsqrt = sqrt(sr.t_start + delta * (sr.t_stop - sr.t_start));
   }
   double ke = 0.0;
   for (int b = 0; b < 3; b++) {
@@ -707,7 +730,7 @@ __global__ void k_finish(StepArgs<R> a, const Integrator *inp, const double *g1,
     for (int c = 0; c < 3; c++) {
       double f = (double) (long long) fa[c] * F_UNSCALE;
       double v = a.v[3 * at + c];
-      if (in.langevin) f += g1[at] * v + g2[at] * tsqrt * (uniform01(seed, step, a.atom_tag[at], c) - 0.5);
+      if (in.langevin) f += g1[at] * v + g2[at] * tsqrt * (uniform01(seed, key, a.atom_tag[at], c) - 0.5);
       if (ftot) ftot[3 * at + c] = f;
       if (final_kick) v += dtfm * f;
       ke += m * v * v;

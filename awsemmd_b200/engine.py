@@ -52,6 +52,28 @@ class AwsemError(RuntimeError):
     pass
 
 
+def replica_desc(c: dict, seed: int = 0) -> ReplicaDesc:
+    """awsem_replica_desc over the arrays of one chain dict (synth.chain_arrays
+    layout); the arrays must stay alive while the descriptor is in use."""
+    d = ReplicaDesc()
+    d.n_res = int(c["n_res"])
+    d.n_chains = len(c["chain_len"])
+    d.chain_len = c["chain_len"].ctypes.data
+    d.seq = c["seq"]
+    d.ssweight = c["ssweight"].ctypes.data if c.get("ssweight") is not None else None
+    d.x = c["x"].ctypes.data
+    d.v = c["v"].ctypes.data if c.get("v") is not None else None
+    d.n_mem = int(c["n_mem"])
+    d.mem_pos = c["mem_pos"].ctypes.data
+    d.mem_len = c["mem_len"].ctypes.data
+    d.mem_weight = c["mem_weight"].ctypes.data
+    d.mem_seq = c["mem_seq"]
+    d.mem_ca = c["mem_ca"].ctypes.data
+    d.mem_cb = c["mem_cb"].ctypes.data
+    d.seed = int(seed)
+    return d
+
+
 _lib = None
 
 
@@ -100,6 +122,13 @@ def load_library(path: str = LIB_PATH):
     lib.awsem_replica_forces.argtypes = [vp, ip, vp]
     lib.awsem_batch_set_forcefield.argtypes = [vp, cp, cp, cp, cp]
     lib.awsem_batch_add_replica.argtypes = [vp, C.POINTER(ReplicaDesc), C.POINTER(ip)]
+    ll = C.c_longlong
+    lib.awsem_server_create.argtypes = [cp, cp, cp, cp, ip, ip, ll, ip, ll, C.c_double, C.c_double, C.POINTER(vp)]
+    lib.awsem_server_admit.argtypes = [vp, C.POINTER(ReplicaDesc), ll, C.c_double, C.c_double, C.POINTER(ip)]
+    lib.awsem_server_advance.argtypes = [vp, ll]
+    lib.awsem_server_progress.argtypes = [vp, ip, C.POINTER(ll), C.POINTER(ll)]
+    lib.awsem_server_collect.argtypes = [vp, ip, vp, vp, vp]
+    lib.awsem_server_usage.argtypes = [vp, vp]
     _lib = lib
     return lib
 
@@ -261,22 +290,7 @@ class AwsemBatch(AwsemSystem):
                                                        forcefield.get("pair_coeffs", "").encode()),
                    "awsem_batch_set_forcefield")
             for k, c in enumerate(chains):
-                d = ReplicaDesc()
-                d.n_res = int(c["n_res"])
-                d.n_chains = len(c["chain_len"])
-                d.chain_len = c["chain_len"].ctypes.data
-                d.seq = c["seq"]
-                d.ssweight = c["ssweight"].ctypes.data if c.get("ssweight") is not None else None
-                d.x = c["x"].ctypes.data
-                d.v = c["v"].ctypes.data if c.get("v") is not None else None
-                d.n_mem = int(c["n_mem"])
-                d.mem_pos = c["mem_pos"].ctypes.data
-                d.mem_len = c["mem_len"].ctypes.data
-                d.mem_weight = c["mem_weight"].ctypes.data
-                d.mem_seq = c["mem_seq"]
-                d.mem_ca = c["mem_ca"].ctypes.data
-                d.mem_cb = c["mem_cb"].ctypes.data
-                d.seed = 0 if seeds is None else int(seeds[k])
+                d = replica_desc(c, 0 if seeds is None else int(seeds[k]))
                 rid = C.c_int()
                 _check(lib, lib.awsem_batch_add_replica(h, C.byref(d), C.byref(rid)), "awsem_batch_add_replica")
             _check(lib, lib.awsem_batch_commit(h), "awsem_batch_commit")
@@ -323,3 +337,81 @@ class AwsemBatch(AwsemSystem):
         _check(self.lib, self.lib.awsem_run(self.h, nsteps, C.byref(rp), None if rows is None else _ptr(rows)),
                "awsem_run")
         return rows
+
+
+EBUSY = -6
+
+
+class AwsemServer:
+    """Continuous batching of MD requests on one GPU (awsem_server_* C ABI).
+
+    All device memory is allocated at creation from the three capacities;
+    `admit` places a request or returns None when it does not fit now,
+    `advance` runs every admitted request, `collect` returns a finished
+    request's final state and energies and frees its room."""
+
+    def __init__(self, forcefield: dict, max_residues: int, max_requests: int, max_memory_records: int,
+                 precision: str | int = "mixed", device: int = 0, dt: float = 2.0, damp: float = 500.0):
+        lib = load_library()
+        self.lib = lib
+        prec = {"fp64": FP64, "mixed": MIXED}.get(precision, precision)
+        h = C.c_void_p()
+        _check(lib, lib.awsem_server_create(forcefield["workdir"].encode(), forcefield["coeff"].encode(),
+                                            forcefield["pair_style"].encode(),
+                                            forcefield.get("pair_coeffs", "").encode(), int(prec), int(device),
+                                            int(max_residues), int(max_requests), int(max_memory_records),
+                                            float(dt), float(damp), C.byref(h)), "awsem_server_create")
+        self.h = h
+        self.precision = prec
+        self.natoms = {}
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.awsem_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def admit(self, chain: dict, nsteps: int, t_start: float = 300.0, t_stop: float = 300.0, seed: int = 1):
+        d = replica_desc(chain, seed)
+        slot = C.c_int()
+        rc = self.lib.awsem_server_admit(self.h, C.byref(d), int(nsteps), float(t_start), float(t_stop),
+                                         C.byref(slot))
+        if rc == EBUSY:
+            return None
+        _check(self.lib, rc, "awsem_server_admit")
+        self.natoms[slot.value] = 3 * int(chain["n_res"])
+        return slot.value
+
+    def advance(self, nsteps: int):
+        _check(self.lib, self.lib.awsem_server_advance(self.h, int(nsteps)), "awsem_server_advance")
+
+    def progress(self, slot: int):
+        done, total = C.c_longlong(), C.c_longlong()
+        _check(self.lib, self.lib.awsem_server_progress(self.h, slot, C.byref(done), C.byref(total)),
+               "awsem_server_progress")
+        return done.value, total.value
+
+    def collect(self, slot: int):
+        n = self.natoms.pop(slot)
+        x, v, e = np.zeros((n, 3)), np.zeros((n, 3)), np.zeros(21)
+        _check(self.lib, self.lib.awsem_server_collect(self.h, slot, _ptr(x), _ptr(v), _ptr(e)),
+               "awsem_server_collect")
+        return x, v, e
+
+    def usage(self) -> dict:
+        info = np.zeros(8, dtype=np.int64)
+        _check(self.lib, self.lib.awsem_server_usage(self.h, _ptr(info)), "awsem_server_usage")
+        keys = ["requests", "residues", "residue_capacity", "records", "record_capacity", "device_bytes", "step",
+                "request_capacity"]
+        return {k: int(v) for k, v in zip(keys, info)}
+
+    def last_run_ms(self) -> float:
+        return float(self.lib.awsem_last_run_ms(self.h))

@@ -1,0 +1,114 @@
+"""Request loop of the serving mode: MD requests (annealing or structure
+prediction runs) arrive over time, are admitted onto one GPU while earlier
+ones are still running (continuous batching), and return their final
+coordinates and per-term energies.
+
+Admission is by the serving handle's fixed memory: the handle allocates its
+residue, request and memory-record capacities once (the HBM budget) and
+`admit` answers None while a request does not fit; the loop keeps such a
+request (and everything behind it, first come first served) waiting until a
+collect frees room.  Latency of a request = completion time - arrival time,
+both on the loop's wall clock.
+"""
+from __future__ import annotations
+
+import time
+from collections import deque
+from dataclasses import dataclass, field
+
+import numpy as np
+
+
+@dataclass
+class Request:
+    rid: int
+    arrival: float  # seconds after the stream starts
+    chain: dict     # synth.chain_arrays layout
+    nsteps: int
+    t_start: float = 600.0
+    t_stop: float = 300.0
+    seed: int = 1
+
+
+@dataclass
+class Completed:
+    rid: int
+    arrival: float
+    admitted: float
+    finished: float
+    n_res: int
+    nsteps: int
+    x: np.ndarray = field(repr=False, default=None)
+    energies: np.ndarray = field(repr=False, default=None)
+
+    @property
+    def latency(self) -> float:
+        return self.finished - self.arrival
+
+
+def poisson_arrivals(n: int, rate: float, rng: np.random.Generator) -> np.ndarray:
+    """Arrival times of a Poisson process with `rate` requests per second."""
+    return np.cumsum(rng.exponential(1.0 / rate, size=n))
+
+
+def log_uniform_lengths(n: int, lo: int, hi: int, rng: np.random.Generator) -> np.ndarray:
+    """Chain lengths log-uniform in [lo, hi]."""
+    return np.floor(np.exp(rng.uniform(np.log(lo), np.log(hi + 1), size=n))).astype(int).clip(lo, hi)
+
+
+def run_stream(server, requests: list, chunk: int = 50, clock=time.perf_counter, sleep=time.sleep,
+               keep_state: bool = True) -> list:
+    """Serve `requests` in real time on `server` (an AwsemServer or anything
+    with its admit / advance / progress / collect methods).  Between GPU
+    chunks of at most `chunk` steps (shorter when a request is about to
+    finish) the loop admits every arrived request that fits and collects
+    every finished one."""
+    pending = deque(sorted(requests, key=lambda r: r.arrival))
+    active = {}  # slot -> (request, admitted time)
+    done = []
+    t0 = clock()
+    while pending or active:
+        now = clock() - t0
+        while pending and pending[0].arrival <= now:
+            r = pending[0]
+            slot = server.admit(r.chain, r.nsteps, r.t_start, r.t_stop, r.seed)
+            if slot is None:
+                break  # first come first served: later arrivals wait behind it
+            pending.popleft()
+            active[slot] = (r, now)
+        if not active:
+            if pending:
+                sleep(max(0.0, pending[0].arrival - (clock() - t0)))
+            continue
+        left = min(total - got for got, total in (server.progress(s) for s in active))
+        server.advance(max(1, min(chunk, left)))
+        now = clock() - t0
+        for slot in [s for s in active if (lambda p: p[0] >= p[1])(server.progress(s))]:
+            r, adm = active.pop(slot)
+            x, _, e = server.collect(slot)
+            done.append(Completed(r.rid, r.arrival, adm, now, int(r.chain["n_res"]), r.nsteps,
+                                  x if keep_state else None, e if keep_state else None))
+    return done
+
+
+def stream_stats(done: list) -> dict:
+    """p50 / p99 latency, makespan and aggregate residue-steps/s of a served stream."""
+    lat = np.array([d.latency for d in done])
+    t_first = min(d.arrival for d in done)
+    t_last = max(d.finished for d in done)
+    work = float(sum(d.n_res * d.nsteps for d in done))
+    return {"requests": len(done), "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+            "mean_s": float(lat.mean()), "makespan_s": t_last - t_first,
+            "residue_steps": work, "residue_steps_per_s": work / max(t_last - t_first, 1e-9)}
+
+
+def fifo_latencies(arrivals: np.ndarray, service: np.ndarray) -> np.ndarray:
+    """Completion latencies of one-at-a-time service in arrival order (a
+    single FIFO server): start = max(arrival, previous finish)."""
+    out = np.empty(len(arrivals))
+    free = 0.0
+    for k in np.argsort(arrivals, kind="stable"):
+        start = max(arrivals[k], free)
+        free = start + service[k]
+        out[k] = free - arrivals[k]
+    return out

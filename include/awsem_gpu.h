@@ -35,6 +35,7 @@ extern "C" {
 #define AWSEM_ECUDA -3    /* CUDA runtime error */
 #define AWSEM_ESTATE -4   /* invalid state (e.g. pair-list overflow detected) */
 #define AWSEM_ENOMEM -5   /* device memory budget exceeded */
+#define AWSEM_EBUSY -6    /* serving handle: the request does not fit now (retry after a collect) */
 
 /* arithmetic forms */
 #define AWSEM_FP64 0   /* plain form: FP64 throughout */
@@ -186,6 +187,42 @@ int awsem_profile_step(awsem_system *sys, int reps, double *ms);
  * residue, [5] pair-list capacity (pairs), [6] residue pairs i < j in the
  * list of the last build, [7] non-uniform memory coefficients stored (0/1). */
 int awsem_model_info(awsem_system *sys, long long *info);
+
+/* Serving: continuous batching of MD runs (annealing or structure
+ * prediction requests) on one GPU.  No counterpart in the reference (one
+ * system per LAMMPS process); each request runs exactly what `run nsteps`
+ * with fix langevin (ramp t_start -> t_stop) and fix nve would run on it
+ * alone, and its result does not depend on which other requests share the
+ * GPU: forces are exact fixed-point sums and the noise is keyed by the
+ * request's own step count and atom ids.
+ *
+ * A serving handle is created with fixed capacities, all device memory
+ * allocated at creation (the memory budget): max_residues residues (handed
+ * out in 32-residue groups), max_requests requests in flight, and
+ * max_memory_records fragment-memory records (one per memory and target
+ * pair; 16 bytes each in the mixed form, 32 in FP64, plus 4 or 8 when the
+ * memory coefficients differ between records).  The force field is read
+ * once, as in awsem_batch_set_forcefield; requests are array-described
+ * replicas (awsem_replica_desc, `seed` = the request's Langevin seed).
+ *
+ * awsem_server_admit places a request (AWSEM_EBUSY when it does not fit
+ * now); it starts with the next step.  awsem_server_advance runs nsteps
+ * steps of every admitted request (finished requests stay frozen).
+ * awsem_server_progress reports steps done / requested; awsem_server_collect
+ * copies a finished request's final x, v ([natoms][3], the request's atom
+ * order) and energies[21] (either may be NULL) and frees its room.
+ * usage: [0] requests held, [1] residues held (group-rounded), [2] residue
+ * capacity, [3] memory records held (stripe-rounded), [4] record capacity,
+ * [5] device bytes allocated, [6] step counter, [7] request capacity. */
+int awsem_server_create(const char *workdir, const char *coeff_file, const char *pair_style, const char *pair_coeffs,
+                        int precision, int device, long long max_residues, int max_requests,
+                        long long max_memory_records, double dt, double damp, awsem_system **out);
+int awsem_server_admit(awsem_system *srv, const awsem_replica_desc *request, long long nsteps, double t_start,
+                       double t_stop, int *slot);
+int awsem_server_advance(awsem_system *srv, long long nsteps);
+int awsem_server_progress(awsem_system *srv, int slot, long long *done, long long *total);
+int awsem_server_collect(awsem_system *srv, int slot, double *x, double *v, double *energies);
+int awsem_server_usage(awsem_system *srv, long long *info);
 
 /* Fragment-memory forces and energy through an entry point that allocates
  * nothing: for callers that cannot call cudaMalloc when forces are needed
