@@ -219,6 +219,12 @@ def c3_seed(k: int, rank: int = 0) -> int:
     return 3000 + k + 100000 * rank
 
 
+# DRAM bytes (read + write) per algorithmic byte of a launch, from one ncu
+# capture of the kernel on the first 64 replicas of configuration 3
+# (profiles/fragmem_pair_hbond_c3_64replicas.txt: 117.2 MB for 108.9 MB)
+TRAFFIC_PER_ALGORITHMIC_BYTE = {"fragmem": 117.185536 / 108.913648}
+
+
 def algorithmic_bytes(kernel: str, info) -> float:
     """Bytes one launch must move at least (data layout of the engine):
     fragmem -- every stored memory distance once, the block table, the two
@@ -429,8 +435,13 @@ def main():
     abytes = algorithmic_bytes(top, info)
     achieved = abytes / (prof[top] * 1e-3) / 1e9
     fm_gbs = algorithmic_bytes("fragmem", info) / (prof["fragmem"] * 1e-3) / 1e9 if prof["fragmem"] > 0 else None
+    traffic = TRAFFIC_PER_ALGORITHMIC_BYTE[top] * abytes if top in TRAFFIC_PER_ALGORITHMIC_BYTE else None
     roofline = {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "traffic": None, "peak_source": f"{peak_kind} hbm_gbs (burst copy)",
+                "frac": achieved / peak, "traffic": traffic,
+                "traffic_source": "ncu dram read+write of a 64-replica launch per algorithmic byte, times this "
+                                  "launch's algorithmic bytes (profiles/fragmem_pair_hbond_c3_64replicas.txt)"
+                if traffic else None,
+                "peak_source": f"{peak_kind} hbm_gbs (burst copy)",
                 "algorithmic_bytes_per_launch": abytes, "launch_ms": prof[top],
                 "kernel_ms": {k: round(v, 5) for k, v in prof.items()}, "fragmem_gbs": fm_gbs}
 
