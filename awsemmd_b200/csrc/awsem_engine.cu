@@ -152,6 +152,10 @@ template <typename R> class Engine : public EngineBase {
   DBuf<int> res_sys, sys_begin, sys_end;
   DBuf<unsigned long long> sys_seed;
   int pcap = 0;  // residue pair list capacity (pairs)
+  // residues the per-residue kernels cover: all of them, or on a serving
+  // handle the used prefix of its capacity (rounded up to 4,096)
+  int launch_res = 0;
+  int n_run() const { return launch_res > 0 ? launch_res : n(); }
   // pair-list room per residue: 48 covers a compact globule (about 66
   // partners within 16 A, half of them higher-numbered) with margin
   int pairs_per_res = 48;
@@ -396,7 +400,7 @@ template <typename R> class Engine : public EngineBase {
   void launch_prepare_and_list(const dev::StepArgs<R> &a, cudaStream_t s, bool force, bool advance)
   {
     const FFParams &p = in.ff.p;
-    int nn = n();
+    int nn = n_run();
     int tb = 128, nb = (nn + tb - 1) / tb, wb = (nn * 32 + tb - 1) / tb;
     dev::k_prepare<R><<<nb, tb, 0, s>>>(a, p);
     dev::k_nl_decide<<<1, 1, 0, s>>>(nl.p, force ? 1 : 0, advance ? dstep.p : nullptr);
@@ -407,7 +411,7 @@ template <typename R> class Engine : public EngineBase {
   void launch_eval(const dev::StepArgs<R> &a, bool advance)
   {
     const FFParams &p = in.ff.p;
-    int nn = n();
+    int nn = n_run();
     int tb = 128, nb = (nn + tb - 1) / tb;
     launch_prepare_and_list(a, s0, false, advance);
     bool fm = (a.groups & dev::G_FIX) && p.fm_nd > 0;
@@ -436,10 +440,11 @@ template <typename R> class Engine : public EngineBase {
     if (!(groups & dev::G_BOND)) CK(cudaMemsetAsync(e_res.p + (size_t) E_BOND * nn, 0, sizeof(double) * nn, s0));
   }
 
-  void reduce_energies()
+  // energy sums of replicas [rep0, rep0 + count) (all of them by default)
+  void reduce_energies(int rep0 = 0, int count = -1)
   {
-    dim3 grid(E_SLOTS, n_sys());
-    dev::k_energy_reduce<<<grid, 256, 0, s0>>>(e_res.p, e_fix.p, n(), sys_begin.p, sys_end.p, energy.p);
+    dim3 grid(E_SLOTS, count < 0 ? n_sys() : count);
+    dev::k_energy_reduce<<<grid, 256, 0, s0>>>(e_res.p, e_fix.p, n(), sys_begin.p, sys_end.p, energy.p, rep0);
   }
 
   void need_single(const char *what)
@@ -544,7 +549,7 @@ template <typename R> class Engine : public EngineBase {
   void capture_steps(cudaGraphExec_t &exec, int count, bool thermo)
   {
     auto a = args(groups_all);
-    int nn = n(), tb = 128, nb = (nn + tb - 1) / tb;
+    int nn = n(), tb = 128, nb = (n_run() + tb - 1) / tb;
     cudaGraph_t graph;
     CK(cudaStreamBeginCapture(s0, cudaStreamCaptureModeThreadLocal));
     for (int c = 0; c < count; c++) {
@@ -617,7 +622,7 @@ template <typename R> class Engine : public EngineBase {
     CK(cudaMemcpyAsync(dstep.p, &pre, sizeof pre, cudaMemcpyHostToDevice, s0));
     const FFParams &p = in.ff.p;
     auto a = args(groups_all);
-    int nn = n(), tb = 128, nb = (nn + tb - 1) / tb, wb = (nn * 32 + tb - 1) / tb;
+    int nn = n_run(), tb = 128, nb = (nn + tb - 1) / tb, wb = (nn * 32 + tb - 1) / tb;
     std::vector<cudaEvent_t> ev(2 * AWSEM_NKERNELS);
     for (auto &e : ev) CK(cudaEventCreate(&e));
     std::vector<double> acc(AWSEM_NKERNELS, 0.0);
@@ -720,7 +725,7 @@ template <typename R> class Engine : public EngineBase {
     CK(cudaStreamSynchronize(s0));  // host vectors go out of scope
   }
 
-  int fm_blocks() const { return (fm_groups * fm_dsplit * 32 + 127) / 128; }
+  int fm_blocks() const { return (((n_run() + 31) / 32) * fm_dsplit * 32 + 127) / 128; }
 
   void model_info(long long *info) override
   {
@@ -840,7 +845,7 @@ template <typename R> class Engine : public EngineBase {
   void energies(int rep, double *out) override
   {
     check_rep(rep);
-    reduce_energies();
+    reduce_energies(rep, 1);
     double e[E_SLOTS];
     CK(cudaMemcpyAsync(e, energy.p + (size_t) rep * E_SLOTS, sizeof e, cudaMemcpyDeviceToHost, s0));
     CK(cudaStreamSynchronize(s0));
@@ -1018,6 +1023,7 @@ template <typename R> class Engine : public EngineBase {
     free_groups[0] = groups;
     slots.assign(max_slots, Slot());
     srv_rp = awsem_run_params{dt, 1, 300.0, 300.0, damp, 1ull, skin, 0};
+    update_launch_extent();
     upload_integrator(make_integrator(srv_rp, step + 1));
     CK(cudaStreamSynchronize(s0));
     release_graphs();  // buffers were reallocated after setup
@@ -1175,7 +1181,23 @@ template <typename R> class Engine : public EngineBase {
     in.ext_of[slot_id] = t.ext_of;
     seeds[slot_id] = seed;
     set_nl_field(&dev::NLState::r_list, 0.f);  // the next evaluation rebuilds the pair list
+    update_launch_extent();
     return slot_id;
+  }
+
+  // Kernels cover residues [0, high-water mark of the used groups), rounded
+  // up to 4,096 so that admissions rarely change the launch shapes (which
+  // are baked into the step graphs: a change re-captures them).
+  void update_launch_extent()
+  {
+    int hwm = 0;
+    for (const Slot &sl : slots)
+      if (sl.used) hwm = std::max(hwm, sl.base + 32 * sl.groups);
+    int want = std::min(n(), std::max(4096, (hwm + 4095) / 4096 * 4096));
+    if (want != launch_res) {
+      launch_res = want;
+      release_graphs();
+    }
   }
 
   int n_res_cap() const { return in.top.n_res; }
@@ -1251,6 +1273,7 @@ template <typename R> class Engine : public EngineBase {
     in.ext_of[k].clear();
     sl = Slot();
     set_nl_field(&dev::NLState::r_list, 0.f);
+    update_launch_extent();
   }
 
   void usage(long long *info) override

@@ -787,11 +787,11 @@ __global__ void k_thermo(const double *e_res, const long long *e_fix, int n_res,
 }
 
 // Per-term sums of each replica's residues in a fixed tree order
-// (block (t, rep) sums energy slot t of replica rep)
+// (block (t, r) sums energy slot t of replica rep0 + r)
 __global__ void k_energy_reduce(const double *e_res, const long long *e_fix, int n_res, const int *sys_begin,
-                                const int *sys_end, double *out)
+                                const int *sys_end, double *out, int rep0)
 {
-  const int t = blockIdx.x, rep = blockIdx.y;
+  const int t = blockIdx.x, rep = rep0 + blockIdx.y;
   __shared__ double sh[256];
   double acc = 0.0;
   // pair-summed energies are kept in fixed point (e_fix slots)

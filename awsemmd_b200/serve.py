@@ -112,3 +112,30 @@ def fifo_latencies(arrivals: np.ndarray, service: np.ndarray) -> np.ndarray:
         free = start + service[k]
         out[k] = free - arrivals[k]
     return out
+
+
+def plan_capacities(forcefield: dict, budget_bytes: float, precision: str = "mixed", records_per_residue: float = 420.0,
+                    mean_request_residues: float = 277.0, device: int = 0) -> dict:
+    """Capacities of a serving handle whose device allocation fits
+    `budget_bytes`: the cost of a residue and of a memory record are read
+    from the allocations of three small probe handles, and the residue
+    capacity is what the budget holds at `records_per_residue` records each
+    (the uniform-coefficient table; a mixed-coefficient stream needs 25%
+    more per record in the mixed form)."""
+    from .engine import AwsemServer
+
+    def size(res, rec, req):
+        with AwsemServer(forcefield, res, req, rec, precision, device) as s:
+            return s.usage()["device_bytes"]
+
+    b0 = size(8192, 0, 64)
+    per_res = (size(16384, 0, 64) - b0) / 8192.0
+    per_rec = (size(8192, 1 << 20, 64) - b0) / float(1 << 20)
+    per_req = (size(8192, 0, 64 + 4096) - b0) / 4096.0
+    fixed = b0 - 8192 * per_res - 64 * per_req
+    req_per_res = 4.0 / mean_request_residues  # request slots: four times the mean concurrency the residues allow
+    max_res = int((budget_bytes - fixed) / (per_res + records_per_residue * per_rec + req_per_res * per_req))
+    max_res -= max_res % 32
+    return {"max_residues": max_res, "max_memory_records": int(max_res * records_per_residue),
+            "max_requests": max(64, int(req_per_res * max_res)),
+            "bytes_per_residue": per_res, "bytes_per_record": per_rec, "bytes_per_request": per_req}

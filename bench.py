@@ -70,6 +70,10 @@ def parse():
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--replicas", type=int, default=1024, help="c3: number of replicas")
     ap.add_argument("--no-baseline", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--serve-requests", type=int, default=48,
+                    help="configuration-4 stream: requests served after the batched measurement (0: skip)")
+    ap.add_argument("--serve-steps", type=int, default=20000, help="MD steps of each served request")
+    ap.add_argument("--serve-budget-gb", type=float, default=150.0, help="HBM budget of the serving handle")
     a = ap.parse_args()
     if a.md_steps is None:
         a.md_steps = 20 if a.workload == "c3" else 100
@@ -308,6 +312,68 @@ def reference_c1(md: int, warmup: int, steps: int):
     return 2000 * md * steps / sum(t), sum(t)
 
 
+def serving_bench(args, dist: Dist, tmp: str) -> dict:
+    """Configuration 4 on one GPU: requests arrive as a Poisson process at
+    50/s with chain lengths log-uniform in [30, 1000], each an annealing run
+    of --serve-steps steps from 600 K to 300 K, served with continuous
+    batching by a handle whose device memory is the --serve-budget-gb budget.
+    Beside it, the plain FP64 form serving the same stream one request at a
+    time: its service times are measured per request length on a sample
+    (device time of 500 steps, scaled to the request's steps) and the FIFO
+    queue is replayed on the same arrival times."""
+    from awsemmd_b200 import serve, synth
+    from awsemmd_b200.engine import AwsemBatch, AwsemServer
+
+    rng = np.random.default_rng(4000 + dist.rank)
+    n = args.serve_requests
+    lens = serve.log_uniform_lengths(n, 30, 1000, rng)
+    arrivals = serve.poisson_arrivals(n, 50.0, rng)
+    chains = [c3_chain(int(L), 400000 + 1000 * dist.rank + k) for k, L in enumerate(lens)]
+    ff = synth.forcefield_dir(os.path.join(tmp, "ff4"))
+    plan = serve.plan_capacities(ff, args.serve_budget_gb * 1e9, args.precision, device=dist.local)
+    t0 = time.perf_counter()
+    with AwsemServer(ff, plan["max_residues"], plan["max_requests"], plan["max_memory_records"],
+                     precision=args.precision, device=dist.local) as srv:
+        t_create = time.perf_counter() - t0
+        # warm-up request (graph capture, first list build), not part of the stream
+        w = srv.admit(chains[0], 30, 600.0, 300.0, seed=7)
+        while srv.progress(w)[0] < 30:
+            srv.advance(31)
+        srv.collect(w)
+        reqs = [serve.Request(k, float(arrivals[k]), chains[k], args.serve_steps, 600.0, 300.0,
+                              seed=4000 + 1000 * dist.rank + k) for k in range(n)]
+        done = serve.run_stream(srv, reqs, chunk=100, keep_state=False)
+        usage = srv.usage()
+    st = serve.stream_stats(done)
+    # plain FP64, one request at a time: service time per length, FIFO replay
+    probe = sorted({30, 100, 300, 1000, int(np.median(lens))})
+    per_step = []
+    for k, L in enumerate(probe):
+        c = c3_chain(L, 490000 + k)
+        with AwsemBatch.from_arrays(ff, [c], precision="fp64", device=dist.local, seeds=[5]) as one:
+            one.run(50, t_start=600.0, t_stop=300.0)
+            one.run(500, t_start=600.0, t_stop=300.0)
+            per_step.append(one.last_run_ms() / 1e3 / 500)
+    coef = np.polyfit(np.array(probe, dtype=float), np.array(per_step), 1)
+    service = np.polyval(coef, lens.astype(float)) * args.serve_steps
+    lat_plain = serve.fifo_latencies(arrivals, service)
+    work = float(np.sum(lens) * args.serve_steps)
+    makespan_plain = float(np.max(arrivals + lat_plain) - np.min(arrivals))
+    return {"workload": f"config4: {n} requests, Poisson 50/s, lengths log-uniform [30, 1000], "
+                        f"{args.serve_steps} Langevin steps each, 600 -> 300 K ramp, dt 2 fs, damping 500 fs, "
+                        f"{args.precision} form",
+            "p50_s": st["p50_s"], "p99_s": st["p99_s"], "mean_s": st["mean_s"], "makespan_s": st["makespan_s"],
+            "residue_steps_per_s": st["residue_steps_per_s"], "residue_steps": st["residue_steps"],
+            "budget_gb": args.serve_budget_gb, "device_bytes": usage["device_bytes"],
+            "residue_capacity": usage["residue_capacity"], "record_capacity": usage["record_capacity"],
+            "create_s": t_create,
+            "plain_fp64_one_at_a_time": {
+                "p50_s": float(np.percentile(lat_plain, 50)), "p99_s": float(np.percentile(lat_plain, 99)),
+                "residue_steps_per_s": work / makespan_plain,
+                "method": "device time of 500 FP64 steps per probe length " + str(probe) +
+                          ", linear in length, scaled to the request's steps; FIFO replay on the same arrivals"}}
+
+
 def reference_arm(args, dist: Dist):
     if dist.rank != 0:
         return
@@ -489,6 +555,11 @@ def main():
             base = {"value": None, "unit": "residue-steps/s", "cores": 1, "kind": "reference",
                     "sample": f"not measured: {e}"}
     eng.close()
+    served = None
+    if args.workload == "c3" and args.serve_requests > 0:
+        del l2buf
+        torch.cuda.empty_cache()  # the serving handle takes the memory budget
+        served = serving_bench(args, dist, tmp)
     from awsemmd_b200.engine import NKERNELS
     launches = NKERNELS * (md + 1) * args.steps  # every kernel of every MD step (setup evaluation included)
     if dist.rank == 0:
@@ -506,7 +577,7 @@ def main():
                         "h2d_bytes_per_step": 2 * natoms * 3 * 8, "d2h_bytes_per_step": 2 * natoms * 3 * 8,
                         "path": "awsem_replica_set_state (host x, v) for every replica + awsem_run + "
                                 "awsem_replica_get_state for every replica, per bench step"},
-                "plain_fp64": plain, "clocks": clk, "gpu_launches": launches}
+                "plain_fp64": plain, "clocks": clk, "gpu_launches": launches, "served": served}
         print(json.dumps(line))
     dist.close()
 
