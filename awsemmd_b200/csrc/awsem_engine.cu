@@ -24,6 +24,11 @@ struct CudaError : std::runtime_error {
   using std::runtime_error::runtime_error;
 };
 
+// invalid device state detected after a call (AWSEM_ESTATE)
+struct StateError : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+
 #define CK(call)                                                                                 \
   do {                                                                                           \
     cudaError_t e_ = (call);                                                                     \
@@ -326,6 +331,8 @@ template <typename R> class Engine : public EngineBase {
     bond_r0.upload(br, s0);
     if (!(in.ff.p.terms & T_FM)) in.ff.p.fm_nd = 0;
     upload_fm_slices();
+    CK(cudaFuncSetAttribute(dev::k_fragmem<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            4 * dev::fm_warp_smem<R>(true)));
     // pair-list radii of the terms
     dev::NLState st{};
     const FFParams &p = in.ff.p;
@@ -419,7 +426,7 @@ template <typename R> class Engine : public EngineBase {
       // fragment memory is independent of the pair passes: second stream
       CK(cudaEventRecord(ev_fork, s0));
       CK(cudaStreamWaitEvent(s1, ev_fork, 0));
-      dev::k_fragmem<R><<<fm_blocks(), tb, 0, s1>>>(a, p);
+      dev::k_fragmem<R><<<fm_blocks(), tb, fm_smem(), s1>>>(a, p);
       CK(cudaEventRecord(ev_join, s1));
     }
     dev::k_density<R><<<pair_blocks, tb, 0, s0>>>(a, p);
@@ -494,8 +501,10 @@ template <typename R> class Engine : public EngineBase {
     dev::NLState st;
     CK(cudaMemcpy(&st, nl.p, sizeof st, cudaMemcpyDeviceToHost));
     if (st.overflow)
-      throw std::runtime_error("residue pair list overflow (capacity " + std::to_string(pcap) + " pairs, needed " +
-                               std::to_string(st.overflow) + "); results of this call are invalid");
+      throw StateError("residue pair list overflow (capacity " + std::to_string(pcap) + " pairs, needed " +
+                       std::to_string(st.overflow) + "); results of this call are invalid");
+    if (st.fm_timeout)
+      throw StateError("fragment-memory stream: a shared-memory copy wait gave up; results of this call are invalid");
   }
 
   void check_rep(int rep)
@@ -639,7 +648,7 @@ template <typename R> class Engine : public EngineBase {
           case 5: dev::k_water_xi<R><<<pair_blocks, tb, 0, s0>>>(a, p); break;
           case 6: dev::k_pair<R><<<pair_blocks, tb, 0, s0>>>(a, p); break;
           case 7: dev::k_hbond<R><<<hb_blocks, 128, 0, s0>>>(a, p); break;
-          case 8: if (fm) dev::k_fragmem<R><<<fm_blocks(), tb, 0, s0>>>(a, p); break;
+          case 8: if (fm) dev::k_fragmem<R><<<fm_blocks(), tb, fm_smem(), s0>>>(a, p); break;
           case 9: dev::k_bonds<R><<<nb, tb, 0, s0>>>(a); break;
           case 10: dev::k_finish<R><<<nb, tb, 0, s0>>>(a, d_integ.p, g1.p, g2.p, ftot.p, x.p); break;
         }
@@ -726,6 +735,8 @@ template <typename R> class Engine : public EngineBase {
   }
 
   int fm_blocks() const { return (((n_run() + 31) / 32) * fm_dsplit * 32 + 127) / 128; }
+  // dynamic shared memory of a fragment-memory block (4 warps)
+  int fm_smem() const { return 4 * dev::fm_warp_smem<R>(!in.fm.uniform); }
 
   void model_info(long long *info) override
   {
@@ -1260,7 +1271,10 @@ template <typename R> class Engine : public EngineBase {
     fill(x, (size_t) 9 * base, (size_t) 9 * n, 0.0);
     fill(v, (size_t) 9 * base, (size_t) 9 * n, 0.0);
     const int nd = in.ff.p.fm_nd;
-    if (nd > 0) fill(fm_slen, (size_t) (base / 32) * nd, (size_t) sl.groups * nd, 0);
+    if (nd > 0) {
+      fill(fm_slen, (size_t) (base / 32) * nd, (size_t) sl.groups * nd, 0);
+      fill(fm_soff, (size_t) (base / 32) * nd, (size_t) sl.groups * nd, 0);
+    }
     int zero = 0;
     dev::SlotRun w{0, 0, 0, 0.0, 0.0};
     put(sys_begin, k, &zero, 1);
@@ -1327,6 +1341,9 @@ template <typename Fn> static int guarded(Fn fn)
   } catch (CudaError &e) {
     g_last_error = e.what();
     return AWSEM_ECUDA;
+  } catch (StateError &e) {
+    g_last_error = e.what();
+    return AWSEM_ESTATE;
   } catch (std::invalid_argument &e) {
     g_last_error = e.what();
     return AWSEM_EINVAL;

@@ -145,6 +145,226 @@ __device__ __forceinline__ void fragmem_warp(const FMSlices<R> &t, const double 
   }
 }
 
+
+// ---------------------------------------------------------------------------
+// Bulk-copy pipeline.  A group's blocks are contiguous stripes, so a warp's
+// whole share is one contiguous run of stripes: lane 0 streams it into a
+// ring of kFmStages shared-memory stages of kFmStripes stripes with 1-D bulk
+// copies (cp.async.bulk, the TMA engine) completing on one mbarrier per
+// stage, and the 32 lanes read their records from shared memory.  Up to
+// kFmStages stages are in flight per warp with no register cost, which is
+// what the register-load version lacks at full size.  Per lane the records
+// are consumed in the same order, so the sums equal the register version's
+// bit for bit.
+constexpr int kFmStages = 3, kFmStripes = 8;
+
+template <typename R> __host__ __device__ constexpr int fm_stage_bytes(bool coef)
+{
+  return kFmStripes * 32 * (int) sizeof(R) * (coef ? 5 : 4);
+}
+// shared memory of one warp: 128 bytes of mbarriers, then the stages
+template <typename R> __host__ __device__ constexpr int fm_warp_smem(bool coef)
+{
+  return 128 + kFmStages * fm_stage_bytes<R>(coef);
+}
+
+__device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t) __cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count)
+{
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect(uint32_t bar, uint32_t bytes)
+{
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void bulk_load(uint32_t dst, const void *src, uint32_t bytes, uint32_t bar)
+{
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+               "l"(src), "r"(bytes), "r"(bar)
+               : "memory");
+}
+
+// Wait for phase `parity` of an mbarrier, giving up after `limit` clock
+// cycles (false: timed out).
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, long long limit)
+{
+  const long long t0 = clock64();
+  while (true) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (done) return true;
+    if (clock64() - t0 > limit) return false;
+  }
+}
+
+constexpr long long kFmWaitLimit = 4000000000LL;  // about two seconds at 2 GHz
+
+__device__ __forceinline__ void load_record_shared(const float *rf, int rec, float m[4])
+{
+  const float4 v = reinterpret_cast<const float4 *>(rf)[rec];
+  m[0] = v.x, m[1] = v.y, m[2] = v.z, m[3] = v.w;
+}
+__device__ __forceinline__ void load_record_shared(const double *rf, int rec, double m[4])
+{
+  const double2 *q = reinterpret_cast<const double2 *>(rf) + 2 * rec;
+  const double2 u = q[0], v = q[1];
+  m[0] = u.x, m[1] = u.y, m[2] = v.x, m[3] = v.y;
+}
+
+template <typename R, class Pos>
+__device__ __forceinline__ void fragmem_warp_bulk(const FMSlices<R> &t, const double *sig, int n, const Pos &pos,
+                                                  unsigned long long *facc, unsigned long long *e_acc,
+                                                  int e_stride, int *timed_out, unsigned char *wsm)
+{
+  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (w >= t.groups * t.dsplit) return;
+  const int g = w / t.dsplit, c = w - g * t.dsplit;
+  const int d0 = c * t.nd / t.dsplit, d1 = (c + 1) * t.nd / t.dsplit;
+  const int i = g * 32 + lane;
+  const bool live = i < n;
+  const int ii = live ? i : n - 1;
+  const bool coef = t.coef != nullptr;
+  const int stage_bytes = fm_stage_bytes<R>(coef);
+  const uint32_t bars = smem_addr(wsm), data = bars + 128;
+  // the warp's run of stripes: its non-empty blocks, contiguous from the first
+  int first = -1, total = 0;
+  for (int dd = d0; dd < d1; dd++) {
+    const int len = t.slen[g * t.nd + dd];
+    if (len > 0 && first < 0) first = t.soff[g * t.nd + dd];
+    total += len;
+  }
+  if (total <= 0) return;
+  const int last = first + total, nchunks = (total + kFmStripes - 1) / kFmStripes;
+  if (lane == 0)
+    for (int s = 0; s < kFmStages; s++) mbar_init(bars + 8 * s, 1);
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  __syncwarp();
+  auto issue = [&](int k) {  // lane 0: chunk k into stage k % kFmStages
+    const int st = k % kFmStages, s0 = first + k * kFmStripes, ns = min(kFmStripes, last - s0);
+    const uint32_t bar = bars + 8 * st, dst = data + st * stage_bytes;
+    const uint32_t rb = ns * 32 * 4 * sizeof(R), cb = coef ? ns * 32 * sizeof(R) : 0;
+    // the stage was last read through the generic proxy: order that before the async-proxy write
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    mbar_expect(bar, rb + cb);
+    bulk_load(dst, t.rf + (size_t) s0 * 32 * 4, rb, bar);
+    if (coef) bulk_load(dst + kFmStripes * 32 * 4 * sizeof(R), t.coef + (size_t) s0 * 32, cb, bar);
+  };
+  if (lane == 0)
+    for (int k = 0; k < kFmStages && k < nchunks; k++) issue(k);
+
+  const V3<double> ca_i = pos(ii, 0), cb_i = pos(ii, 1);
+  long long fca[3] = {0, 0, 0}, fcb[3] = {0, 0, 0};
+  double e = 0.0;
+  const R cu = R(t.uniform);
+  // current row (block d): geometry and sums
+  int d = d0, blk_end = 0, j = 0;
+  V3<R> dv[4];
+  R r[4], s2 = 1, inv2s = 1, es = 0, fs[4] = {0, 0, 0, 0};
+  auto begin_row = [&]() {  // d: the next non-empty block at or after d
+    while (d < d1 && t.slen[g * t.nd + d] == 0) d++;
+    if (d >= d1) return;
+    blk_end = t.soff[g * t.nd + d] - first + t.slen[g * t.nd + d];
+    j = min(ii + t.min_sep + d, n - 1);
+    const V3<double> ca_j = pos(j, 0), cb_j = pos(j, 1);
+    dv[0] = diff<R>(ca_i, ca_j);
+    dv[1] = diff<R>(ca_i, cb_j);
+    dv[2] = diff<R>(cb_i, ca_j);
+    dv[3] = diff<R>(cb_i, cb_j);
+#pragma unroll
+    for (int k = 0; k < 4; k++) r[k] = m_sqrt(norm2(dv[k]));
+    s2 = R(sig[t.min_sep + d]);
+    inv2s = R(1) / (R(2) * s2);
+    es = 0;
+#pragma unroll
+    for (int k = 0; k < 4; k++) fs[k] = 0;
+  };
+  auto end_row = [&]() {
+    e += (double) es;
+    long long fja[3] = {0, 0, 0}, fjb[3] = {0, 0, 0};
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const R fc = fs[k] != R(0) ? fs[k] / (s2 * r[k]) : R(0);
+      const long long v[3] = {fix_force((double) (fc * dv[k].x)), fix_force((double) (fc * dv[k].y)),
+                              fix_force((double) (fc * dv[k].z))};
+#pragma unroll
+      for (int q = 0; q < 3; q++) {
+        if (k < 2)
+          fca[q] += v[q];
+        else
+          fcb[q] += v[q];
+        if (k & 1)
+          fjb[q] -= v[q];
+        else
+          fja[q] -= v[q];
+      }
+    }
+    red_add3(facc + (size_t) 9 * j, fja);
+    red_add3(facc + (size_t) 9 * j + 3, fjb);
+    d++;
+  };
+  begin_row();
+  bool ok = true;
+  int fail_k = 0;
+  for (int k = 0; k < nchunks; k++) {
+    const int st = k % kFmStages;
+    if (!mbar_wait(bars + 8 * st, (k / kFmStages) & 1, kFmWaitLimit)) {
+      ok = false;
+      fail_k = k;
+      break;
+    }
+    const unsigned char *sd = wsm + 128 + st * stage_bytes;
+    const R *srf = reinterpret_cast<const R *>(sd);
+    const R *scf = reinterpret_cast<const R *>(sd + kFmStripes * 32 * 4 * sizeof(R));
+    const int s0 = k * kFmStripes, ns = min(kFmStripes, total - s0);
+    for (int q = 0; q < ns; q++) {
+      const int s = s0 + q;
+      while (s >= blk_end && d < d1) {  // rows end on stripe boundaries
+        end_row();
+        begin_row();
+      }
+      R rec[4];
+      load_record_shared(srf, q * 32 + lane, rec);
+      const R cc = coef ? scf[q * 32 + lane] : cu;
+#pragma unroll
+      for (int kk = 0; kk < 4; kk++) {
+        const R dr = r[kk] - rec[kk];
+        const R gk = cc * m_fastexp(-dr * dr * inv2s);
+        es -= gk;
+        fs[kk] -= gk * dr;
+      }
+    }
+    __syncwarp();  // every lane has read the stage
+    if (lane == 0 && k + kFmStages < nchunks) issue(k + kFmStages);
+  }
+  if (!ok) {
+    // record the failure, let the copies in flight land (bounded), skip the sums
+    if (lane == 0) atomicExch(timed_out, 1);
+    for (int k = fail_k; k < nchunks && k < fail_k + kFmStages; k++)
+      mbar_wait(bars + 8 * (k % kFmStages), (k / kFmStages) & 1, kFmWaitLimit / 8);
+    return;
+  }
+  end_row();
+  if (live) {
+    red_add3(facc + (size_t) 9 * i, fca);
+    red_add3(facc + (size_t) 9 * i + 3, fcb);
+  }
+  long long ef = live ? fix_force(e) : 0;
+  if (e_stride) {
+    if (ef) atomicAdd(e_acc + (size_t) i * e_stride, (unsigned long long) ef);
+  } else {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) ef += __shfl_xor_sync(0xffffffffu, ef, o);
+    if (lane == 0 && ef) atomicAdd(e_acc, (unsigned long long) ef);
+  }
+}
+
 }  // namespace dev
 
 // A handle's resident fragment-memory table, for entry points outside the

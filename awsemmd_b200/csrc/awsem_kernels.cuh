@@ -45,6 +45,7 @@ struct NLState {
   float ev_pre_sq;    // CA-CA distance^2 beyond which no bead pair of two residues is in excluded-volume range
   int n_dssp, n_pap;  // hydrogen-bond queue lengths of the current evaluation
   int npairs;         // pairs in the residue pair list (may exceed its capacity: overflow)
+  int fm_timeout;     // a fragment-memory stream wait gave up (results invalid)
 };
 
 // Run window of one replica: integrated over steps begin..end (the
@@ -644,11 +645,14 @@ template <typename R> struct BeadPos {
   __device__ __forceinline__ V3<double> operator()(int r, int b) const { return bead(*s, r, b ? B_CB : B_CA); }
 };
 
+// 128 threads, fm_warp_smem<R>(coef) bytes of dynamic shared memory per warp
 template <typename R> __global__ void __launch_bounds__(128) k_fragmem(StepArgs<R> a, FFParams p)
 {
+  extern __shared__ __align__(128) unsigned char fm_smem[];
   const BeadPos<R> pos{&a.s};
-  fragmem_warp(a.fm, p.fm_sigma_sq, a.s.n_res, pos, a.s.facc,
-               (unsigned long long *) (a.e_fix + (size_t) 2 * a.s.n_res), 1);
+  unsigned char *wsm = fm_smem + (threadIdx.x >> 5) * fm_warp_smem<R>(a.fm.coef != nullptr);
+  fragmem_warp_bulk(a.fm, p.fm_sigma_sq, a.s.n_res, pos, a.s.facc,
+                    (unsigned long long *) (a.e_fix + (size_t) 2 * a.s.n_res), 1, &a.nl->fm_timeout, wsm);
 }
 
 // bond_style harmonic, bonds grouped by the residue of their first atom

@@ -134,7 +134,9 @@ def plan_capacities(forcefield: dict, budget_bytes: float, precision: str = "mix
     per_req = (size(8192, 0, 64 + 4096) - b0) / 4096.0
     fixed = b0 - 8192 * per_res - 64 * per_req
     req_per_res = 4.0 / mean_request_residues  # request slots: four times the mean concurrency the residues allow
-    max_res = int((budget_bytes - fixed) / (per_res + records_per_residue * per_rec + req_per_res * per_req))
+    # 0.1% kept back for the rounding of residues to groups and records to stripes
+    usable = 0.999 * budget_bytes - fixed
+    max_res = int(usable / (per_res + records_per_residue * per_rec + req_per_res * per_req))
     max_res -= max_res % 32
     return {"max_residues": max_res, "max_memory_records": int(max_res * records_per_residue),
             "max_requests": max(64, int(req_per_res * max_res)),
