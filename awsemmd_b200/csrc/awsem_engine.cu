@@ -99,6 +99,9 @@ class EngineBase {
   virtual void compute(long long step, const double *x_ext, double *f_ext, double *energies, int groups) = 0;
   virtual void set_state(int rep, const double *x_ext, const double *v_ext) = 0;
   virtual void get_state(int rep, double *x_ext, double *v_ext) = 0;
+  // every replica at once, replicas concatenated in replica order, each in its caller atom order
+  virtual void set_state_all(const double *x_ext, const double *v_ext) = 0;
+  virtual void get_state_all(double *x_ext, double *v_ext) = 0;
   virtual void run(long long nsteps, const awsem_run_params &rp, double *thermo) = 0;
   virtual void energies(int rep, double *out) = 0;
   virtual void forces(int rep, double *f_ext) = 0;
@@ -510,6 +513,50 @@ template <typename R> class Engine : public EngineBase {
   void check_rep(int rep)
   {
     if (rep < 0 || rep >= n_sys()) throw std::invalid_argument("replica index out of range");
+  }
+
+  // Whole-batch state transfer: one copy each way through a device staging
+  // buffer, and a gather/scatter kernel between caller order and internal order.
+  DBuf<int> perm;              // internal atom -> position in the concatenated caller arrays
+  DBuf<double> stage;          // [n_atoms][3]
+
+  void ensure_perm()
+  {
+    if (perm.p) return;
+    if (server) throw std::invalid_argument("whole-batch state transfer is not available on a serving handle");
+    std::vector<int> pm(natoms());
+    for (int r = 0; r < n_sys(); r++) {
+      const int a0 = rep_atom0(r), na = rep_atoms(r);
+      for (int a = 0; a < na; a++) pm[a0 + a] = a0 + in.ext_of[r][a];
+    }
+    perm.upload(pm, s0);
+    stage.alloc((size_t) 3 * natoms());
+  }
+
+  void set_state_all(const double *x_ext, const double *v_ext) override
+  {
+    ensure_perm();
+    const int na = natoms(), tb = 256;
+    for (int k = 0; k < 2; k++) {
+      const double *src = k ? v_ext : x_ext;
+      if (!src) continue;
+      CK(cudaMemcpyAsync(stage.p, src, sizeof(double) * 3 * na, cudaMemcpyHostToDevice, s0));
+      dev::k_gather3<<<(na + tb - 1) / tb, tb, 0, s0>>>(stage.p, perm.p, na, k ? v.p : x.p);
+    }
+    CK(cudaStreamSynchronize(s0));
+  }
+
+  void get_state_all(double *x_ext, double *v_ext) override
+  {
+    ensure_perm();
+    const int na = natoms(), tb = 256;
+    for (int k = 0; k < 2; k++) {
+      double *dst = k ? v_ext : x_ext;
+      if (!dst) continue;
+      dev::k_scatter3<<<(na + tb - 1) / tb, tb, 0, s0>>>(k ? v.p : x.p, perm.p, na, stage.p);
+      CK(cudaMemcpyAsync(dst, stage.p, sizeof(double) * 3 * na, cudaMemcpyDeviceToHost, s0));
+      CK(cudaStreamSynchronize(s0));
+    }
   }
 
   void set_state(int rep, const double *x_ext, const double *v_ext) override
@@ -1528,6 +1575,18 @@ int awsem_replica_get_state(awsem_system *sys, int r, double *x, double *v)
 {
   if (!ready(sys)) return AWSEM_EINVAL;
   return guarded([&] { sys->eng->get_state(r, x, v); });
+}
+
+int awsem_batch_set_state(awsem_system *sys, const double *x, const double *v)
+{
+  if (!ready(sys)) return AWSEM_EINVAL;
+  return guarded([&] { sys->eng->set_state_all(x, v); });
+}
+
+int awsem_batch_get_state(awsem_system *sys, double *x, double *v)
+{
+  if (!ready(sys)) return AWSEM_EINVAL;
+  return guarded([&] { sys->eng->get_state_all(x, v); });
 }
 
 int awsem_replica_energies(awsem_system *sys, int r, double *energies)

@@ -470,7 +470,7 @@ template <typename R> __device__ __forceinline__ void scatter_fix(const DevSys<R
 // and excluded volume are applied to both residues.  DSSP and P_AP pairs are
 // only detected here (cheap distance and index tests) and queued: k_hbond
 // evaluates them, so their long, branchy bodies do not slow this pass.
-template <typename R> __global__ void __launch_bounds__(128) k_pair(StepArgs<R> a, FFParams p)
+template <typename R> __global__ void __launch_bounds__(128, 6) k_pair(StepArgs<R> a, FFParams p)
 {
   const DevSys<R> &s = a.s;
   const int n = s.n_res;
@@ -747,6 +747,23 @@ __global__ void k_finish(StepArgs<R> a, const Integrator *inp, const double *g1,
   }
   // kinetic energy after the final half kick (thermo output of the step)
   a.e_res[(size_t) E_KIN * a.s.n_res + r] = 0.5 * 48.88821291 * 48.88821291 * ke;
+}
+
+// Caller-order staging <-> internal order: out[a] = in[perm[a]] / out[perm[a]] = in[a]
+__global__ void k_gather3(const double *in, const int *perm, int n, double *out)
+{
+  int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= n) return;
+  const int p = perm[a];
+  for (int c = 0; c < 3; c++) out[3 * a + c] = in[3 * p + c];
+}
+
+__global__ void k_scatter3(const double *in, const int *perm, int n, double *out)
+{
+  int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= n) return;
+  const int p = perm[a];
+  for (int c = 0; c < 3; c++) out[3 * p + c] = in[3 * a + c];
 }
 
 // Conservative total force of the last evaluation in FP64 (no Langevin)

@@ -122,6 +122,8 @@ def load_library(path: str = LIB_PATH):
     lib.awsem_replica_forces.argtypes = [vp, ip, vp]
     lib.awsem_batch_set_forcefield.argtypes = [vp, cp, cp, cp, cp]
     lib.awsem_batch_add_replica.argtypes = [vp, C.POINTER(ReplicaDesc), C.POINTER(ip)]
+    lib.awsem_batch_set_state.argtypes = [vp, vp, vp]
+    lib.awsem_batch_get_state.argtypes = [vp, vp, vp]
     ll = C.c_longlong
     lib.awsem_server_create.argtypes = [cp, cp, cp, cp, ip, ip, ll, ip, ll, C.c_double, C.c_double, C.POINTER(vp)]
     lib.awsem_server_admit.argtypes = [vp, C.POINTER(ReplicaDesc), ll, C.c_double, C.c_double, C.POINTER(ip)]
@@ -324,6 +326,22 @@ class AwsemBatch(AwsemSystem):
         e = np.zeros(21)
         _check(self.lib, self.lib.awsem_replica_energies(self.h, r, _ptr(e)), "awsem_replica_energies")
         return e
+
+    def set_state_all(self, x=None, v=None):
+        """Every replica at once: [natoms][3] arrays, replicas concatenated in
+        order, each in its caller atom order (awsem_batch_set_state)."""
+        xa = None if x is None else np.ascontiguousarray(x, dtype=np.float64).reshape(self.natoms, 3)
+        va = None if v is None else np.ascontiguousarray(v, dtype=np.float64).reshape(self.natoms, 3)
+        _check(self.lib, self.lib.awsem_batch_set_state(self.h, None if xa is None else _ptr(xa),
+                                                        None if va is None else _ptr(va)), "awsem_batch_set_state")
+
+    def get_state_all(self, x: np.ndarray | None = None, v: np.ndarray | None = None):
+        """Every replica at once into x, v (allocated when not given)."""
+        x = np.zeros((self.natoms, 3)) if x is None else x
+        v = np.zeros((self.natoms, 3)) if v is None else v
+        assert x.flags.c_contiguous and v.flags.c_contiguous and x.dtype == np.float64 and v.dtype == np.float64
+        _check(self.lib, self.lib.awsem_batch_get_state(self.h, _ptr(x), _ptr(v)), "awsem_batch_get_state")
+        return x, v
 
     def forces(self, r: int = 0) -> np.ndarray:
         f = np.zeros((self.replica_natoms(r), 3))

@@ -471,21 +471,28 @@ def main():
     value = dist.world * n_res * md * args.steps / (total_ms / 1e3)
 
     # end to end through the C ABI with host buffers: every replica's state
-    # in from host memory, `run`, every replica's state out
+    # in from pinned host memory (awsem_batch_set_state), `run`, every
+    # replica's state out (awsem_batch_get_state)
     nrep = getattr(eng, "nreplicas", 1)
-    host = [eng.get_state(r) if nrep > 1 else eng.get_state() for r in range(nrep)]
+    pinned = [torch.empty((eng.natoms, 3), dtype=torch.float64, pin_memory=True) for _ in range(2)]
+    hx, hv = pinned[0].numpy(), pinned[1].numpy()
+    if nrep > 1:
+        eng.get_state_all(hx, hv)
+    else:
+        hx[:], hv[:] = eng.get_state()
     e2e_t = []
     for _ in range(max(2, args.steps // 2)):
         dist.barrier()
         t0 = time.perf_counter()
-        for r in range(nrep):
-            if nrep > 1:
-                eng.set_state(host[r][0], host[r][1], r=r)
-            else:
-                eng.set_state(host[r][0], host[r][1])
-        eng.run(md, **run_kw)
-        for r in range(nrep):
-            host[r] = eng.get_state(r) if nrep > 1 else eng.get_state()
+        if nrep > 1:
+            eng.set_state_all(hx, hv)
+            eng.run(md, **run_kw)
+            eng.get_state_all(hx, hv)
+        else:
+            eng.set_state(hx, hv)
+            eng.run(md, **run_kw)
+            x1, v1 = eng.get_state()
+            hx[:], hv[:] = x1, v1
         e2e_t.append(time.perf_counter() - t0)
     e2e_total = dist.max(sum(e2e_t))
     e2e_value = dist.world * n_res * md * len(e2e_t) / e2e_total
@@ -575,8 +582,8 @@ def main():
                 "roofline": roofline, "cpu_baseline": base,
                 "e2e": {"value": e2e_value, "unit": "residue-steps/s",
                         "h2d_bytes_per_step": 2 * natoms * 3 * 8, "d2h_bytes_per_step": 2 * natoms * 3 * 8,
-                        "path": "awsem_replica_set_state (host x, v) for every replica + awsem_run + "
-                                "awsem_replica_get_state for every replica, per bench step"},
+                        "path": "awsem_batch_set_state (pinned host x, v of every replica) + awsem_run + "
+                                "awsem_batch_get_state, per bench step; wall clock"},
                 "plain_fp64": plain, "clocks": clk, "gpu_launches": launches, "served": served}
         print(json.dumps(line))
     dist.close()

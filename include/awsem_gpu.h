@@ -125,6 +125,13 @@ int awsem_replica_nres(const awsem_system *sys, int replica);
 int awsem_replica_set_state(awsem_system *sys, int replica, const double *x, const double *v);
 int awsem_replica_get_state(awsem_system *sys, int replica, double *x, double *v);
 int awsem_replica_energies(awsem_system *sys, int replica, double *energies);
+/* Every replica's state in one call each way: x and v are [natoms][3] with
+ * the replicas concatenated in replica order, each in its caller atom order
+ * (replica r starts at atom 3 * (residues of replicas before r)).  One
+ * host-device copy per array (pinned host memory makes it a DMA at full
+ * bandwidth) plus a reordering kernel.  Either pointer may be NULL. */
+int awsem_batch_set_state(awsem_system *sys, const double *x, const double *v);
+int awsem_batch_get_state(awsem_system *sys, double *x, double *v);
 int awsem_replica_forces(awsem_system *sys, int replica, double *f);
 
 /* totals over the whole batch (one replica: that system) */

@@ -67,3 +67,28 @@ def test_batch_rejects_mismatched_force_fields(tmp_path, gpu_lib):
     f1, _ = write_case("r1r69", tmp_path)  # different fragment-memory gamma classes
     with pytest.raises(AwsemError, match="share one force field"):
         AwsemBatch([f0, f1])
+
+
+def test_whole_batch_state_transfer(tmp_path, gpu_lib):
+    """awsem_batch_set_state / get_state move every replica in one call and
+    agree with the per-replica calls (caller atom order, replicas concatenated)."""
+    from awsemmd_b200 import synth
+    from awsemmd_b200.engine import AwsemBatch
+
+    ff = synth.forcefield_dir(str(tmp_path / "ff"))
+    chains = [synth.chain_arrays(L, seed=600 + k, n_mem_per_window=2) for k, L in enumerate([40, 77, 33])]
+    with AwsemBatch.from_arrays(ff, chains, precision="mixed", seeds=[1, 2, 3]) as b:
+        per = [b.get_state(r) for r in range(3)]
+        x, v = b.get_state_all()
+        assert np.array_equal(x, np.concatenate([p[0] for p in per]))
+        assert np.array_equal(v, np.concatenate([p[1] for p in per]))
+        rng = np.random.default_rng(5)
+        x2 = x + rng.normal(0, 0.01, x.shape)
+        v2 = rng.normal(0, 0.001, v.shape)
+        b.set_state_all(x2, v2)
+        off = 0
+        for r, c in enumerate(chains):
+            xr, vr = b.get_state(r)
+            n = 3 * c["n_res"]
+            assert np.array_equal(xr, x2[off:off + n]) and np.array_equal(vr, v2[off:off + n])
+            off += n
