@@ -160,6 +160,7 @@ template <typename R> class Engine : public EngineBase {
   DBuf<int> res_sys, sys_begin, sys_end;
   DBuf<unsigned long long> sys_seed;
   int pcap = 0;  // residue pair list capacity (pairs)
+  bool server_pending = false;  // setup() called for a serving handle (no replicas yet)
   // residues the per-residue kernels cover: all of them, or on a serving
   // handle the used prefix of its capacity (rounded up to 4,096)
   int launch_res = 0;
@@ -362,6 +363,7 @@ template <typename R> class Engine : public EngineBase {
     int sms = 148;
     CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
     hb_blocks = std::max(1, std::min((nn * 8 + 127) / 128, 16 * sms));
+    if (!server_pending) setup_grids();
     // size the pair list from a first build: room for 4x the initial pairs
     // (chains that collapse gain neighbours), at least pairs_per_res per residue
     resize_pairs(std::max<long long>(64, 16LL * nn));
@@ -407,14 +409,66 @@ template <typename R> class Engine : public EngineBase {
     CK(cudaMemcpyAsync(nl.p, &st, sizeof st, cudaMemcpyHostToDevice, s0));
   }
 
+  // cell grids of the large replicas (see k_grid_setup)
+  DBuf<int> big_rep, big_of, cell_count, cell_start, cell_fill, res_cell, sorted_res;
+  DBuf<dev::GridDesc> grid_desc;
+  int nbig = 0;
+
+  void setup_grids()
+  {
+    std::vector<int> br, bo(std::max(n_sys(), 1), -1);
+    std::vector<dev::GridDesc> gd;
+    int cells = 0;
+    for (int r = 0; r < n_sys(); r++) {
+      const int nr = rep_res(r);
+      if (nr <= dev::kGridMin) continue;
+      bo[r] = (int) br.size();
+      br.push_back(r);
+      dev::GridDesc d{};
+      d.cell0 = cells;
+      d.cap = std::max(64, 2 * nr);
+      cells += d.cap;
+      gd.push_back(d);
+    }
+    nbig = (int) br.size();
+    if (!nbig) return;
+    big_rep.upload(br, s0);
+    big_of.upload(bo, s0);
+    grid_desc.upload(gd, s0);
+    cell_count.alloc(cells);
+    cell_start.alloc(cells);
+    cell_fill.alloc(cells);
+    res_cell.alloc(n());
+    sorted_res.alloc(n());
+    CK(cudaStreamSynchronize(s0));
+  }
+
+  dev::GridArgs grid_args() const
+  {
+    return dev::GridArgs{nbig, big_rep.p, big_of.p, grid_desc.p, cell_count.p, cell_start.p, cell_fill.p,
+                         res_cell.p, sorted_res.p};
+  }
+
+  void launch_list_build(const dev::StepArgs<R> &a, cudaStream_t s)
+  {
+    const int nn = n_run(), tb = 128, nb = (nn + tb - 1) / tb, wb = (nn * 32 + tb - 1) / tb;
+    const dev::GridArgs g = grid_args();
+    if (nbig) {
+      dev::k_grid_setup<R><<<nbig, 256, 0, s>>>(a, g);
+      dev::k_grid_count<R><<<nb, tb, 0, s>>>(a, g);
+      dev::k_grid_scan<R><<<nbig, 1024, 0, s>>>(a, g);
+      dev::k_grid_fill<R><<<nb, tb, 0, s>>>(a, g);
+    }
+    dev::k_nl_build<R><<<wb, tb, 0, s>>>(a, g);
+  }
+
   void launch_prepare_and_list(const dev::StepArgs<R> &a, cudaStream_t s, bool force, bool advance)
   {
     const FFParams &p = in.ff.p;
-    int nn = n_run();
-    int tb = 128, nb = (nn + tb - 1) / tb, wb = (nn * 32 + tb - 1) / tb;
+    const int nn = n_run(), tb = 128, nb = (nn + tb - 1) / tb;
     dev::k_prepare<R><<<nb, tb, 0, s>>>(a, p);
     dev::k_nl_decide<<<1, 1, 0, s>>>(nl.p, force ? 1 : 0, advance ? dstep.p : nullptr);
-    dev::k_nl_build<R><<<wb, tb, 0, s>>>(a);
+    launch_list_build(a, s);
   }
 
   // one force evaluation (everything up to the fixed-point force sums)
@@ -678,7 +732,7 @@ template <typename R> class Engine : public EngineBase {
     CK(cudaMemcpyAsync(dstep.p, &pre, sizeof pre, cudaMemcpyHostToDevice, s0));
     const FFParams &p = in.ff.p;
     auto a = args(groups_all);
-    int nn = n_run(), tb = 128, nb = (nn + tb - 1) / tb, wb = (nn * 32 + tb - 1) / tb;
+    int nn = n_run(), tb = 128, nb = (nn + tb - 1) / tb;
     std::vector<cudaEvent_t> ev(2 * AWSEM_NKERNELS);
     for (auto &e : ev) CK(cudaEventCreate(&e));
     std::vector<double> acc(AWSEM_NKERNELS, 0.0);
@@ -689,7 +743,7 @@ template <typename R> class Engine : public EngineBase {
         switch (k) {
           case 0: dev::k_prepare<R><<<nb, tb, 0, s0>>>(a, p); break;
           case 1: dev::k_nl_decide<<<1, 1, 0, s0>>>(nl.p, 0, dstep.p); break;
-          case 2: dev::k_nl_build<R><<<wb, tb, 0, s0>>>(a); break;
+          case 2: launch_list_build(a, s0); break;
           case 3: dev::k_density<R><<<pair_blocks, tb, 0, s0>>>(a, p); break;
           case 4: dev::k_residue<R><<<nb, tb, 0, s0>>>(a, p); break;
           case 5: dev::k_water_xi<R><<<pair_blocks, tb, 0, s0>>>(a, p); break;
@@ -1065,7 +1119,9 @@ template <typename R> class Engine : public EngineBase {
     in.fm.row_start.assign((size_t) nn * nd + 1, 0);
     in.fm.uniform = true;
     seeds.assign(max_slots, 0ull);
+    server_pending = true;
     setup();
+    server_pending = false;
     committed = true;
     // four bond slots per residue: CA-O, CA-CB/HB, CA-CA(+1), O-CA(+1)
     bond_cap = 4;

@@ -221,14 +221,162 @@ template <typename R> __device__ __forceinline__ V3<double> contact(const DevSys
   return bead(s, r, (s.res_flags[r] & R_GLY) ? B_CA : B_CB);
 }
 
+// Cell grids for large replicas (more than kGridMin residues): each such
+// replica gets a uniform grid over the bounding box of its contact beads at
+// every list build, cells no smaller than the list radius (grown when the
+// box would need more cells than the replica's cell budget), and residues
+// sorted by cell; its residues then scan the 27 surrounding cells instead of
+// the whole replica.  Smaller replicas scan all their higher residues.
+constexpr int kGridMin = 2048;
+
+struct GridDesc {
+  float ox, oy, oz, inv_cell;
+  int nx, ny, nz;
+  int cell0, cap;  // first cell in the shared cell arrays, cells budgeted
+};
+
+struct GridArgs {
+  int nbig;
+  const int *big_rep;   // [nbig] replica of each gridded replica
+  const int *big_of;    // [n_sys] gridded index of a replica, -1 when scanned directly
+  GridDesc *desc;       // [nbig]
+  int *cell_count, *cell_start, *cell_fill;  // [total cells]
+  int *res_cell;        // [n_res] cell of a gridded residue
+  int *sorted;          // [n_res] residues of each gridded replica, by cell, at the replica's residue range
+};
+
+// one block per gridded replica: bounding box, grid shape, cleared counts
+template <typename R> __global__ void k_grid_setup(StepArgs<R> a, GridArgs g)
+{
+  if (!a.nl->rebuild) return;
+  const int b = blockIdx.x, rep = g.big_rep[b];
+  const int r0 = a.sys_begin[rep], r1 = a.sys_end[rep];
+  float lo[3] = {3e38f, 3e38f, 3e38f}, hi[3] = {-3e38f, -3e38f, -3e38f};
+  for (int r = r0 + threadIdx.x; r < r1; r += blockDim.x) {
+    const V3<double> c = contact(a.s, r);
+    const float p[3] = {(float) c.x, (float) c.y, (float) c.z};
+    for (int k = 0; k < 3; k++) {
+      lo[k] = fminf(lo[k], p[k]);
+      hi[k] = fmaxf(hi[k], p[k]);
+    }
+  }
+  __shared__ float sl[3][32], sh[3][32];
+  for (int k = 0; k < 3; k++) {
+    for (int o = 16; o > 0; o >>= 1) {
+      lo[k] = fminf(lo[k], __shfl_xor_sync(0xffffffffu, lo[k], o));
+      hi[k] = fmaxf(hi[k], __shfl_xor_sync(0xffffffffu, hi[k], o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+      sl[k][threadIdx.x >> 5] = lo[k];
+      sh[k][threadIdx.x >> 5] = hi[k];
+    }
+  }
+  __syncthreads();
+  GridDesc &d = g.desc[b];
+  if (threadIdx.x == 0) {
+    for (int k = 0; k < 3; k++)
+      for (int w = 1; w < (int) (blockDim.x >> 5); w++) {
+        sl[k][0] = fminf(sl[k][0], sl[k][w]);
+        sh[k][0] = fmaxf(sh[k][0], sh[k][w]);
+      }
+    // cells at least the list radius (plus rounding room) wide
+    float cell = a.nl->r_list * 1.0001f + 1e-3f;
+    int n[3];
+    for (int it = 0; it < 64; it++) {
+      long long tot = 1;
+      for (int k = 0; k < 3; k++) {
+        n[k] = max(1, (int) ((sh[k][0] - sl[k][0]) / cell) + 1);
+        tot *= n[k];
+      }
+      if (tot <= d.cap) break;
+      cell *= 1.26f;
+    }
+    d.ox = sl[0][0];
+    d.oy = sl[1][0];
+    d.oz = sl[2][0];
+    d.inv_cell = 1.f / cell;
+    d.nx = n[0];
+    d.ny = n[1];
+    d.nz = n[2];
+  }
+  __syncthreads();
+  for (int c = threadIdx.x; c < d.cap; c += blockDim.x) {
+    g.cell_count[d.cell0 + c] = 0;
+    g.cell_fill[d.cell0 + c] = 0;
+  }
+}
+
+__device__ __forceinline__ int grid_coord(float p, float o, float inv, int n)
+{
+  return min(n - 1, max(0, (int) ((p - o) * inv)));
+}
+
+// thread per residue of a gridded replica: its cell, and the cell counts
+template <typename R> __global__ void k_grid_count(StepArgs<R> a, GridArgs g)
+{
+  if (!a.nl->rebuild) return;
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= a.s.n_res || a.res_sys[r] < 0) return;
+  const int b = g.big_of[a.res_sys[r]];
+  if (b < 0) return;
+  const GridDesc d = g.desc[b];
+  const V3<double> c = contact(a.s, r);
+  const int cx = grid_coord((float) c.x, d.ox, d.inv_cell, d.nx), cy = grid_coord((float) c.y, d.oy, d.inv_cell, d.ny),
+            cz = grid_coord((float) c.z, d.oz, d.inv_cell, d.nz);
+  const int cell = d.cell0 + (cz * d.ny + cy) * d.nx + cx;
+  g.res_cell[r] = cell;
+  atomicAdd(&g.cell_count[cell], 1);
+}
+
+// one block per gridded replica: cell starts (exclusive scan, offset by the
+// replica's first residue) in chunks of blockDim.x cells
+template <typename R> __global__ void k_grid_scan(StepArgs<R> a, GridArgs g)
+{
+  if (!a.nl->rebuild) return;
+  const int b = blockIdx.x;
+  const GridDesc d = g.desc[b];
+  const int ncell = d.nx * d.ny * d.nz;
+  __shared__ int part[1024];
+  __shared__ int carry;
+  if (threadIdx.x == 0) carry = a.sys_begin[g.big_rep[b]];
+  __syncthreads();
+  for (int c0 = 0; c0 < ncell; c0 += blockDim.x) {
+    const int c = c0 + threadIdx.x;
+    const int v = c < ncell ? g.cell_count[d.cell0 + c] : 0;
+    part[threadIdx.x] = v;
+    __syncthreads();
+    for (int o = 1; o < (int) blockDim.x; o <<= 1) {  // inclusive Hillis-Steele scan
+      const int add = threadIdx.x >= (unsigned) o ? part[threadIdx.x - o] : 0;
+      __syncthreads();
+      part[threadIdx.x] += add;
+      __syncthreads();
+    }
+    if (c < ncell) g.cell_start[d.cell0 + c] = carry + part[threadIdx.x] - v;
+    __syncthreads();
+    if (threadIdx.x == blockDim.x - 1) carry += part[threadIdx.x];
+    __syncthreads();
+  }
+}
+
+// thread per residue of a gridded replica: place it in its cell's range
+template <typename R> __global__ void k_grid_fill(StepArgs<R> a, GridArgs g)
+{
+  if (!a.nl->rebuild) return;
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= a.s.n_res || a.res_sys[r] < 0 || g.big_of[a.res_sys[r]] < 0) return;
+  const int cell = g.res_cell[r];
+  g.sorted[g.cell_start[cell] + atomicAdd(&g.cell_fill[cell], 1)] = r;
+}
+
 // Residue pair list: every pair i < j of one replica whose contact beads are
 // closer than r_list, as (i, j) in a flat array.  One warp per residue scans
-// the higher residues of its replica twice (count, then write after one
-// atomic reservation), so a residue's pairs are contiguous and ascending.
-// Every pair pass below runs one thread per listed pair and scatters to both
-// residues with fixed-point atomics: each pair is evaluated once, as in the
-// reference's half neighbour list.
-template <typename R> __global__ void k_nl_build(StepArgs<R> a)
+// the candidates twice (count, then write after one atomic reservation), so
+// a residue's pairs are contiguous.  Candidates: the higher residues of its
+// replica, or for a gridded replica the residues of the 27 cells around its
+// own.  Every pair pass below runs one thread per listed pair and scatters to
+// both residues with fixed-point atomics: each pair is evaluated once, as in
+// the reference's half neighbour list.
+template <typename R> __global__ void k_nl_build(StepArgs<R> a, GridArgs g)
 {
   if (!a.nl->rebuild) return;
   const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
@@ -237,16 +385,43 @@ template <typename R> __global__ void k_nl_build(StepArgs<R> a)
     if (lane == 0) a.ncount[i] = 0;
     return;
   }
-  const int sys_end = a.sys_end[a.res_sys[i]];
+  const int rep = a.res_sys[i], sys_end = a.sys_end[rep];
+  const int b = g.nbig ? g.big_of[rep] : -1;
   const DevSys<R> &s = a.s;
   const V3<double> ci = contact(s, i);
   const R rl = (R) a.nl->r_list, rl2 = rl * rl;
-  int count = 0;
-  for (int j0 = i + 1; j0 < sys_end; j0 += 32) {
-    const int j = j0 + lane;
-    const bool take = j < sys_end && norm2(diff<R>(ci, contact(s, j))) < rl2;
-    count += __popc(__ballot_sync(0xffffffffu, take));
+  // candidate ranges: [lo, hi) of residue indices, or of sorted positions (gridded)
+  GridDesc d{};
+  int cx = 0, cy = 0, cz = 0;
+  if (b >= 0) {
+    d = g.desc[b];
+    const int cell = g.res_cell[i] - d.cell0;
+    cx = cell % d.nx;
+    cy = (cell / d.nx) % d.ny;
+    cz = cell / (d.nx * d.ny);
   }
+  auto scan = [&](auto &&visit) {  // visit(j, take) for every candidate, warp-uniform trip counts
+    if (b < 0) {
+      for (int j0 = i + 1; j0 < sys_end; j0 += 32) {
+        const int j = j0 + lane;
+        visit(j, j < sys_end && norm2(diff<R>(ci, contact(s, j))) < rl2);
+      }
+      return;
+    }
+    for (int z = max(0, cz - 1); z <= min(d.nz - 1, cz + 1); z++)
+      for (int y = max(0, cy - 1); y <= min(d.ny - 1, cy + 1); y++)
+        for (int x = max(0, cx - 1); x <= min(d.nx - 1, cx + 1); x++) {
+          const int c = d.cell0 + (z * d.ny + y) * d.nx + x;
+          const int k0 = g.cell_start[c], k1 = k0 + g.cell_count[c];
+          for (int kb = k0; kb < k1; kb += 32) {
+            const int k = kb + lane;
+            const int j = k < k1 ? g.sorted[k] : -1;
+            visit(j, j > i && norm2(diff<R>(ci, contact(s, j))) < rl2);
+          }
+        }
+  };
+  int count = 0;
+  scan([&](int, bool take) { count += __popc(__ballot_sync(0xffffffffu, take)); });
   int base = 0;
   if (lane == 0 && count) base = atomicAdd(&a.nl->npairs, count);
   base = __shfl_sync(0xffffffffu, base, 0);
@@ -256,14 +431,13 @@ template <typename R> __global__ void k_nl_build(StepArgs<R> a)
     a.cb_build[i] = make_double4(ci.x, ci.y, ci.z, 0.0);
   }
   int at = base;
-  for (int j0 = i + 1; j0 < sys_end && count; j0 += 32) {
-    const int j = j0 + lane;
-    const bool take = j < sys_end && norm2(diff<R>(ci, contact(s, j))) < rl2;
-    const unsigned m = __ballot_sync(0xffffffffu, take);
-    const int k = at + __popc(m & ((1u << lane) - 1u));
-    if (take && k < a.pcap) a.pairs[k] = make_int2(i, j);
-    at += __popc(m);
-  }
+  if (count)
+    scan([&](int j, bool take) {
+      const unsigned m = __ballot_sync(0xffffffffu, take);
+      const int k = at + __popc(m & ((1u << lane) - 1u));
+      if (take && k < a.pcap) a.pairs[k] = make_int2(i, j);
+      at += __popc(m);
+    });
 }
 
 // Pairs of the list, grid-stride (the count is known only on the device)

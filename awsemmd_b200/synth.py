@@ -588,7 +588,10 @@ def write_chain_arrays(c: dict, outdir: str) -> dict:
     seq = c["seq"].decode()
     x = c["x"].reshape(L * 3, 3)
     v = c["v"].reshape(L * 3, 3)
-    lines = ["LAMMPS data file (synthetic AWSEM chain)", "", f"{3 * L} atoms", f"{4 * L - 2} bonds",
+    clen = [int(n) for n in c["chain_len"]]
+    mol = np.repeat(np.arange(1, len(clen) + 1), clen)
+    last = set(np.cumsum(clen) - 1)
+    lines = ["LAMMPS data file (synthetic AWSEM chain)", "", f"{3 * L} atoms", f"{4 * L - 2 * len(clen)} bonds",
              "5 atom types", "5 bond types", "", "-500.0 500.0 xlo xhi", "-500.0 500.0 ylo yhi",
              "-500.0 500.0 zlo zhi", "", "Masses", ""]
     lines += [f"{t} {MASSES[t]}" for t in range(1, 6)]
@@ -596,7 +599,8 @@ def write_chain_arrays(c: dict, outdir: str) -> dict:
     for r in range(L):
         for k, t in enumerate([1, 3, 5 if seq[r] == "G" else 4]):
             a = 3 * r + k
-            lines.append(f"{a + 1} 1 {r + 1} {t} 0.0 {float(x[a, 0])!r} {float(x[a, 1])!r} {float(x[a, 2])!r}")
+            lines.append(f"{a + 1} {mol[r]} {r + 1} {t} 0.0 {float(x[a, 0])!r} {float(x[a, 1])!r} "
+                         f"{float(x[a, 2])!r}")
     lines += ["", "Velocities", ""]
     for a in range(3 * L):
         lines.append(f"{a + 1} {float(v[a, 0])!r} {float(v[a, 1])!r} {float(v[a, 2])!r}")
@@ -605,7 +609,7 @@ def write_chain_arrays(c: dict, outdir: str) -> dict:
     b = 0
     for r in range(L):
         pairs = [(2, 3 * r, 3 * r + 1), (5 if seq[r] == "G" else 4, 3 * r, 3 * r + 2)]
-        if r < L - 1:
+        if r not in last:
             pairs += [(1, 3 * r, 3 * r + 3), (3, 3 * r + 1, 3 * r + 3)]
         for t, i, j in pairs:
             b += 1
@@ -613,7 +617,8 @@ def write_chain_arrays(c: dict, outdir: str) -> dict:
     with open(os.path.join(outdir, "data.awsem"), "w") as f:
         f.write("\n".join(lines) + "\n")
     with open(os.path.join(outdir, "protein.seq"), "w") as f:
-        f.write(seq + "\n")
+        starts = np.concatenate([[0], np.cumsum(clen)])
+        f.write("\n".join(seq[starts[k]:starts[k + 1]] for k in range(len(clen))) + "\n")
     with open(os.path.join(outdir, "ssweight"), "w") as f:
         for row in c["ssweight"]:
             f.write(f"{float(row[0])!r} {float(row[1])!r}\n")
@@ -656,3 +661,48 @@ def write_chain_arrays(c: dict, outdir: str) -> dict:
         f.write("\n".join(mem_lines) + "\n")
     return {"workdir": outdir, "data": "data.awsem", "coeff": "fix_backbone_coeff.data", "seq": "protein.seq",
             "pair_style": PAIR_STYLE, "pair_coeffs": ";".join(PAIR_COEFFS)}
+
+
+def packed_arrays(chain_lengths, box: float, seed: int, n_mem_per_window=MEMS_PER_WINDOW, min_dist=4.0,
+                  tries=5000) -> dict:
+    """One system of several chains, each built as in configuration 0 (see
+    chain_arrays, chain k from seed * 100003 + k), placed by a random rotation
+    and a translation uniform in the box with rejection of any inter-chain CA
+    pair closer than min_dist; returned as the arrays of one awsem_replica_desc.
+    Memories are internal distances, unchanged by the placement."""
+    from scipy.spatial import cKDTree
+
+    rng = np.random.default_rng(seed)
+    parts, placed = [], np.zeros((0, 3))
+    for k, L in enumerate(chain_lengths):
+        c = chain_arrays(int(L), seed * 100003 + k, n_mem_per_window=n_mem_per_window)
+        x = c["x"].reshape(-1, 3)
+        ca = c["x"][:, 0, :]
+        tree = cKDTree(placed) if len(placed) else None
+        for _ in range(tries):
+            R = _random_rotation(rng)
+            shift = rng.uniform(-box / 2, box / 2, size=3)
+            new_ca = ca @ R.T + shift
+            if tree is None or tree.query(new_ca, k=1, distance_upper_bound=min_dist)[0].min() >= min_dist:
+                break
+        else:
+            raise RuntimeError("could not place chain without overlap")
+        c["x"] = np.ascontiguousarray((x @ R.T + shift).reshape(-1, 3, 3))
+        c["v"] = np.ascontiguousarray((c["v"].reshape(-1, 3) @ R.T).reshape(-1, 3, 3))
+        placed = np.vstack([placed, new_ca])
+        parts.append(c)
+    offs = np.cumsum([0] + [p["n_res"] for p in parts])
+    return {
+        "n_res": int(offs[-1]), "chain_len": np.array([p["n_res"] for p in parts], dtype=np.int32),
+        "seq": b"".join(p["seq"] for p in parts),
+        "ssweight": np.ascontiguousarray(np.concatenate([p["ssweight"] for p in parts])),
+        "x": np.ascontiguousarray(np.concatenate([p["x"] for p in parts])),
+        "v": np.ascontiguousarray(np.concatenate([p["v"] for p in parts])),
+        "n_mem": int(sum(p["n_mem"] for p in parts)),
+        "mem_pos": np.concatenate([p["mem_pos"] + o for p, o in zip(parts, offs)]).astype(np.int32),
+        "mem_len": np.concatenate([p["mem_len"] for p in parts]).astype(np.int32),
+        "mem_weight": np.concatenate([p["mem_weight"] for p in parts]),
+        "mem_seq": b"".join(p["mem_seq"] for p in parts),
+        "mem_ca": np.ascontiguousarray(np.concatenate([p["mem_ca"] for p in parts])),
+        "mem_cb": np.ascontiguousarray(np.concatenate([p["mem_cb"] for p in parts])),
+    }

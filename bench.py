@@ -49,6 +49,10 @@ FALLBACK_HBM = 6650.0
 RUN = dict(dt=2.0, t_start=300.0, t_stop=300.0, damp=500.0)
 CACHE = os.path.join(tempfile.gettempdir(), "awsem_chain_cache")
 
+C2_CPU_NOTE = ("the reference keeps n x n pair caches (cR, cWell, cP_AP in smart_matrix_lib.h; about 128 bytes "
+               "per residue pair): about 205 GB at 40,000 residues")
+
+
 WORKLOADS = {
     "c3": "config3: 1,024 independent chains, lengths uniform in [40, 500] (278,062 residues), each with its own "
           "fragment-memory tables (20 memories per 9-residue window), all AWSEM terms, pair vexcluded, harmonic "
@@ -56,6 +60,10 @@ WORKLOADS = {
     "c1": "config1: 8 chains x 250 residues (2,000 residues, 6,000 beads), 150 A cube, all AWSEM terms + fragment "
           "memory (20 memories per 9-residue window), pair vexcluded, harmonic bonds, Langevin 300 K, dt 2 fs, "
           "damping 500 fs",
+    "c2": "config2: one system of 160 chains x 250 residues (40,000 residues) randomly packed in a 320 A cube "
+          "(0.0012 residues/A^3), all AWSEM terms + fragment memory (20 memories per 9-residue window), pair "
+          "vexcluded, harmonic bonds, Langevin 300 K, dt 2 fs, damping 500 fs, skin 2 A, list rebuilt every 10 "
+          "steps (cell grid)",
 }
 
 
@@ -76,7 +84,7 @@ def parse():
     ap.add_argument("--serve-budget-gb", type=float, default=150.0, help="HBM budget of the serving handle")
     a = ap.parse_args()
     if a.md_steps is None:
-        a.md_steps = 20 if a.workload == "c3" else 100
+        a.md_steps = {"c3": 20, "c2": 50}.get(a.workload, 100)
     return a
 
 
@@ -383,6 +391,9 @@ def reference_arm(args, dist: Dist):
         print(json.dumps({"impl": "reference", "unavailable": "reference library not built (make -C oracle ref)"}))
         return
     cores = os.cpu_count() or 1
+    if args.workload == "c2":
+        print(json.dumps({"impl": "reference", "unavailable": "configuration 2 does not fit a host: " + C2_CPU_NOTE}))
+        return
     if args.workload == "c3":
         md = 10
         # a bounded sample: every core runs a few random replicas for md steps
@@ -446,6 +457,14 @@ def main():
     t_setup = time.perf_counter()
     if args.workload == "c3":
         eng, n_res, ff, lens = build_c3(args.replicas, dist.rank, args.precision, dev, tmp)
+    elif args.workload == "c2":
+        from awsemmd_b200 import synth
+
+        ff = synth.forcefield_dir(os.path.join(tmp, "ff2"))
+        c2 = synth.packed_arrays([250] * 160, 320.0, 2000 + dist.rank)
+        eng = AwsemBatch.from_arrays(ff, [c2], precision=args.precision, device=dev, seeds=[2000 + dist.rank])
+        n_res = eng.nres
+        run_kw.update(skin=2.0, neigh_every=10)
     else:
         from awsemmd_b200 import synth
 
@@ -536,7 +555,8 @@ def main():
                  "sample": f"{len(sample)} of the replicas run one at a time, plain FP64 single-system form, "
                            f"{md} MD steps each after a warm-up run, device time"}
     elif args.precision != "fp64":
-        with AwsemSystem(files, precision="fp64", device=dev) as sp:
+        with (AwsemBatch.from_arrays(ff, [c2], precision="fp64", device=dev, seeds=[2000 + dist.rank])
+              if args.workload == "c2" else AwsemSystem(files, precision="fp64", device=dev)) as sp:
             sp.run(md, **run_kw)
             pm = []
             for _ in range(max(2, args.steps // 2)):
@@ -554,6 +574,9 @@ def main():
                         "sample": f"3 random replicas x 5 MD steps ({rs} residue-steps, {busy:.1f} s) on 1 host "
                                   f"core; reference FixBackbone + PairExcludedVolume compiled -O2 against the "
                                   f"LAMMPS-API shim, 1 MPI rank"}
+            elif args.workload == "c2":
+                base = {"value": None, "unit": "residue-steps/s", "cores": 1, "kind": "reference",
+                        "sample": "not runnable: " + C2_CPU_NOTE}
             else:
                 v, busy = reference_c1(5, 1, 2)
                 base = {"value": v, "unit": "residue-steps/s", "cores": 1, "kind": "reference",
