@@ -15,8 +15,10 @@ against the LAMMPS-API shim (``make -C oracle ref``) and run on three inputs:
 
 For each it stores the inputs' hash, the step-0 forces and energies, the
 per-residue pair-pass intermediates and a 20-step Langevin trajectory
-(x, v and per-step thermo rows).  Run from the repository root with the
-reference tree present:  python tests/golden/make_golden.py
+(x, v and per-step thermo rows).  ``c0_nve.npz`` holds the thermo rows of a
+1,000-step constant-energy run (fix nve only, dt 2 fs) of ``c0``: the energy
+drift of the reference.  Run from the repository root with the reference tree
+present:  python tests/golden/make_golden.py
 """
 from __future__ import annotations
 
@@ -36,6 +38,7 @@ from awsemmd_b200 import synth  # noqa: E402
 
 GOLDEN = os.path.dirname(os.path.abspath(__file__))
 RUN = dict(nsteps=20, dt=2.0, t_start=300.0, t_stop=300.0, damp=500.0, seed=12345)
+NVE = dict(nsteps=1000, dt=2.0)
 
 
 def dir_hash(d: str) -> str:
@@ -96,6 +99,14 @@ def main():
                                 run=np.array([RUN["nsteps"], RUN["dt"], RUN["t_start"], RUN["t_stop"], RUN["damp"],
                                               RUN["seed"]], dtype=np.float64))
             print(name, "natoms", len(x0), "E_total", e0[0], "hash", h[:12])
+            if name == "c0":
+                r = ref.RefSystem(files)
+                rows = r.run(NVE["nsteps"], dt=NVE["dt"], langevin=False)
+                r.close()
+                np.savez_compressed(os.path.join(GOLDEN, "c0_nve.npz"), inputs_sha256=np.array(h), thermo=rows,
+                                    run=np.array([NVE["nsteps"], NVE["dt"]], dtype=np.float64))
+                e = rows.sum(axis=1)
+                print("c0 nve: max |E(t) - E(0)| over", NVE["nsteps"], "steps:", np.abs(e - e[0]).max())
 
 
 if __name__ == "__main__":

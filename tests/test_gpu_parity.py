@@ -117,3 +117,22 @@ def test_pair_list_survives_motion(tmp_path, gpu_lib, oracle_built):
     fo, eo = o.compute(x)
     assert np.abs(f - fo).max() / np.abs(fo).max() < 1e-5
     assert abs(e[0] - eo[0]) < 1e-6 * abs(eo[0])
+
+
+def test_nve_energy_drift_matches_reference(tmp_path, gpu_lib):
+    """Plain FP64 form, 1,000 constant-energy steps of configuration 0: the
+    total energy follows the reference's step by step at first and drifts
+    by the reference's amount over the run (golden c0_nve.npz)."""
+    import os
+
+    from awsemmd_b200.engine import AwsemSystem
+
+    files, g = write_case("c0", tmp_path)
+    nve = np.load(os.path.join(os.path.dirname(__file__), "golden", "c0_nve.npz"))
+    with AwsemSystem(files, precision="fp64") as s:
+        s.set_state(g["x0"], g["v0"])
+        rows = s.run(1000, dt=2.0, langevin=False, thermo=True)
+    e, er = rows.sum(axis=1), nve["thermo"].sum(axis=1)
+    assert np.abs(e[:200] - er[:200]).max() < 1e-9 * abs(er[0])
+    d, dr = np.abs(e - e[0]).max(), np.abs(er - er[0]).max()
+    assert abs(d - dr) <= 0.05 * dr, (d, dr)

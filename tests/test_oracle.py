@@ -85,3 +85,20 @@ def test_oracle_matches_reference_on_multichain(tmp_path, oracle_built):
     for k in range(20):
         assert abs(eo[k] - er[k]) <= 1e-11 * max(abs(er[k]), 1e-3), k
     assert rel_err(fo, fr) < 1e-12
+
+
+def test_oracle_nve_drift_matches_reference(tmp_path, oracle_built):
+    """1,000 constant-energy steps of configuration 0: the restated
+    integrator follows the reference's trajectory and energy drift."""
+    import numpy as np
+    import ref
+
+    files, g = write_case("c0", tmp_path)
+    nve = np.load(os.path.join(os.path.dirname(__file__), "golden", "c0_nve.npz"))
+    assert str(nve["inputs_sha256"]) == str(g["inputs_sha256"])
+    o = ref.OracleSystem(files)
+    _, _, rows = o.run(g["x0"], g["v0"], 1000, dt=2.0, langevin=False)
+    e, er = rows.sum(axis=1), nve["thermo"].sum(axis=1)
+    assert np.abs(e[:200] - er[:200]).max() < 1e-9 * abs(er[0])
+    d, dr = np.abs(e - e[0]).max(), np.abs(er - er[0]).max()
+    assert abs(d - dr) <= 0.05 * dr, (d, dr)
