@@ -108,6 +108,7 @@ class EngineBase {
   virtual void residue_arrays(int rep, double *out) = 0;
   virtual void nl_stats(int *nbuilds, double *radius, int *maxc, int *overflow) = 0;
   virtual void profile(int reps, double *ms) = 0;
+  virtual void autotune(int reps, int *chosen) = 0;
   virtual void model_info(long long *info) = 0;
   virtual double run_ms() const = 0;
   // device-resident fragment-memory table, for entry points outside the engine
@@ -721,6 +722,71 @@ template <typename R> class Engine : public EngineBase {
     std::vector<dev::SlotRun> w(n_sys(), dev::SlotRun{begin, end, 0, rp.t_start, rp.t_stop});
     CK(cudaMemcpyAsync(slot_run.p, w.data(), sizeof(dev::SlotRun) * w.size(), cudaMemcpyHostToDevice, s0));
     CK(cudaStreamSynchronize(s0));
+  }
+
+  // Launch-shape autotuner: separations per fragment-memory warp (dsplit),
+  // grid of the pair-parallel passes and of the hydrogen-bond pass.  Each
+  // candidate runs `reps` profiled steps on this handle's own system; the
+  // fastest per knob wins.  The state and step counter are restored after.
+  void autotune(int reps, int *chosen) override
+  {
+    if (server) throw std::invalid_argument("autotune: not available on a serving handle");
+    if (reps <= 0) throw std::invalid_argument("reps must be positive");
+    const int na = natoms();
+    DBuf<double> sx, sv;
+    sx.alloc((size_t) 3 * na);
+    sv.alloc((size_t) 3 * na);
+    CK(cudaMemcpyAsync(sx.p, x.p, sizeof(double) * 3 * na, cudaMemcpyDeviceToDevice, s0));
+    CK(cudaMemcpyAsync(sv.p, v.p, sizeof(double) * 3 * na, cudaMemcpyDeviceToDevice, s0));
+    const long long step_saved = step;
+    int sms = 148;
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    std::vector<double> ms(AWSEM_NKERNELS);
+    auto time_of = [&](std::initializer_list<int> kernels) {
+      release_graphs();
+      profile(1, ms.data());  // warm-up of this shape
+      profile(reps, ms.data());
+      double t = 0;
+      for (int k : kernels) t += ms[k];
+      return t;
+    };
+    // fragment memory: separations per warp
+    const int nd = std::max(in.ff.p.fm_nd, 1);
+    if (in.ff.p.fm_nd > 0) {
+      int best = fm_dsplit;
+      double tbest = 1e30;
+      for (int d : {1, 2, 3, 6, nd}) {
+        if (d > nd) continue;
+        fm_dsplit = d;
+        const double t = time_of({8});
+        if (t < tbest) tbest = t, best = d;
+      }
+      fm_dsplit = best;
+    }
+    // pair-parallel passes (density, water_xi, pair) and the hydrogen-bond pass
+    auto tune_blocks = [&](int &blocks, std::initializer_list<int> kernels) {
+      int best = blocks;
+      double tbest = 1e30;
+      for (int f : {1, 2, 4, 8, 16, 32}) {
+        blocks = f * sms;
+        const double t = time_of(kernels);
+        if (t < tbest) tbest = t, best = blocks;
+      }
+      blocks = best;
+    };
+    tune_blocks(pair_blocks, {3, 5, 6});
+    tune_blocks(hb_blocks, {7});
+    release_graphs();
+    CK(cudaMemcpyAsync(x.p, sx.p, sizeof(double) * 3 * na, cudaMemcpyDeviceToDevice, s0));
+    CK(cudaMemcpyAsync(v.p, sv.p, sizeof(double) * 3 * na, cudaMemcpyDeviceToDevice, s0));
+    CK(cudaStreamSynchronize(s0));
+    step = step_saved;
+    set_nl_field(&dev::NLState::r_list, 0.f);
+    if (chosen) {
+      chosen[0] = fm_dsplit;
+      chosen[1] = pair_blocks;
+      chosen[2] = hb_blocks;
+    }
   }
 
   void profile(int reps, double *ms) override
@@ -1797,6 +1863,15 @@ int awsem_profile_step(awsem_system *sys, int reps, double *ms)
 {
   if (!ready(sys) || !ms) return AWSEM_EINVAL;
   return guarded([&] { sys->eng->profile(reps, ms); });
+}
+
+int awsem_autotune(awsem_system *sys, int reps, int *chosen)
+{
+  if (!ready(sys)) return AWSEM_EINVAL;
+  return guarded([&] {
+    CK(cudaSetDevice(sys->eng->device));
+    sys->eng->autotune(reps, chosen);
+  });
 }
 
 int awsem_model_info(awsem_system *sys, long long *info)

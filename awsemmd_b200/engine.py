@@ -109,6 +109,7 @@ def load_library(path: str = LIB_PATH):
     lib.awsem_kernel_name.argtypes = [ip]
     lib.awsem_kernel_name.restype = cp
     lib.awsem_profile_step.argtypes = [vp, ip, vp]
+    lib.awsem_autotune.argtypes = [vp, ip, vp]
     lib.awsem_model_info.argtypes = [vp, vp]
     lib.awsem_batch_create.argtypes = [ip, ip, C.POINTER(vp)]
     lib.awsem_batch_add_files.argtypes = [vp, cp, cp, cp, cp, cp, cp, C.c_ulonglong, C.POINTER(ip)]
@@ -239,6 +240,13 @@ class AwsemSystem:
         ms = np.zeros(NKERNELS)
         _check(self.lib, self.lib.awsem_profile_step(self.h, reps, _ptr(ms)), "awsem_profile_step")
         return {self.lib.awsem_kernel_name(k).decode(): float(ms[k]) for k in range(NKERNELS)}
+
+    def autotune(self, reps: int = 5) -> dict:
+        """Pick the fastest launch shapes on this system (awsem_autotune)."""
+        got = np.zeros(3, dtype=np.int32)
+        _check(self.lib, self.lib.awsem_autotune(self.h, int(reps), _ptr(got)), "awsem_autotune")
+        return {"fragmem_separations_per_warp": int(got[0]), "pair_pass_blocks": int(got[1]),
+                "hbond_blocks": int(got[2])}
 
     def model_info(self) -> np.ndarray:
         info = np.zeros(8, dtype=np.int64)

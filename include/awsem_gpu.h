@@ -188,6 +188,16 @@ const char *awsem_kernel_name(int k);
  * a time (the step advances; no graph).  Uses the last run's parameters. */
 int awsem_profile_step(awsem_system *sys, int reps, double *ms);
 
+/* Launch-shape autotuner (no counterpart in the reference): times `reps`
+ * profiled steps of this handle's own system for each candidate shape of the
+ * tunable kernels and keeps the fastest -- separations per fragment-memory
+ * warp (1, 2, 3, 6 or all), and the grids of the pair-parallel passes and of
+ * the hydrogen-bond pass (1 to 32 blocks per SM).  The state and the step
+ * counter are restored afterwards; results do not depend on the shapes (all
+ * sums are exact).  chosen (may be NULL): [separations per warp, pair-pass
+ * blocks, hydrogen-bond blocks].  Not available on serving handles. */
+int awsem_autotune(awsem_system *sys, int reps, int *chosen);
+
 /* Sizes behind the roofline's algorithmic-byte counts:
  * info[0] residues, [1] atoms, [2] fragment-memory records (4 distances
  * each), [3] bytes per stored distance (8 FP64, 4 mixed), [4] rows per

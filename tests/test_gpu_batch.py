@@ -92,3 +92,22 @@ def test_whole_batch_state_transfer(tmp_path, gpu_lib):
             n = 3 * c["n_res"]
             assert np.array_equal(xr, x2[off:off + n]) and np.array_equal(vr, v2[off:off + n])
             off += n
+
+
+def test_autotune_keeps_results(tmp_path, gpu_lib):
+    """The autotuner changes launch shapes only: the state is restored and a
+    run afterwards is bitwise the run without tuning."""
+    from awsemmd_b200 import synth
+    from awsemmd_b200.engine import AwsemBatch
+
+    ff = synth.forcefield_dir(str(tmp_path / "ff"))
+    chains = [synth.chain_arrays(L, seed=650 + k, n_mem_per_window=3) for k, L in enumerate([90, 140, 60])]
+    out = []
+    for tune in (False, True):
+        with AwsemBatch.from_arrays(ff, chains, precision="mixed", seeds=[4, 5, 6]) as b:
+            if tune:
+                shapes = b.autotune(2)
+                assert shapes["fragmem_separations_per_warp"] >= 1 and shapes["pair_pass_blocks"] > 0
+            b.run(30)
+            out.append(b.get_state_all())
+    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
