@@ -776,6 +776,19 @@ template <typename R> class Engine : public EngineBase {
     };
     tune_blocks(pair_blocks, {3, 5, 6});
     tune_blocks(hb_blocks, {7});
+    // fragment-memory grid: judged on whole steps (it overlaps the pair passes)
+    if (in.ff.p.fm_nd > 0) {
+      int best = 0;
+      double tbest = 1e30;
+      for (int f : {0, 1, 2, 3, 4}) {
+        fm_grid = f * sms;
+        release_graphs();
+        run(reps, last_rp, nullptr);  // warm-up of this shape (graph capture)
+        run(4 * reps, last_rp, nullptr);
+        if (last_run_ms < tbest) tbest = last_run_ms, best = fm_grid;
+      }
+      fm_grid = best;
+    }
     release_graphs();
     CK(cudaMemcpyAsync(x.p, sx.p, sizeof(double) * 3 * na, cudaMemcpyDeviceToDevice, s0));
     CK(cudaMemcpyAsync(v.p, sv.p, sizeof(double) * 3 * na, cudaMemcpyDeviceToDevice, s0));
@@ -786,6 +799,7 @@ template <typename R> class Engine : public EngineBase {
       chosen[0] = fm_dsplit;
       chosen[1] = pair_blocks;
       chosen[2] = hb_blocks;
+      chosen[3] = fm_grid;
     }
   }
 
@@ -901,7 +915,14 @@ template <typename R> class Engine : public EngineBase {
     CK(cudaStreamSynchronize(s0));  // host vectors go out of scope
   }
 
-  int fm_blocks() const { return (((n_run() + 31) / 32) * fm_dsplit * 32 + 127) / 128; }
+  // one warp per fragment-memory work unit, or a smaller persistent grid
+  // (fm_grid blocks) whose warps loop over the units
+  int fm_grid = 0;
+  int fm_blocks() const
+  {
+    const int all = (((n_run() + 31) / 32) * fm_dsplit * 32 + 127) / 128;
+    return fm_grid > 0 ? std::min(all, fm_grid) : all;
+  }
   // dynamic shared memory of a fragment-memory block (4 warps)
   int fm_smem() const { return 4 * dev::fm_warp_smem<R>(!in.fm.uniform); }
 

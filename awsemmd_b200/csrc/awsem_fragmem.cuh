@@ -218,13 +218,17 @@ __device__ __forceinline__ void load_record_shared(const double *rf, int rec, do
   m[0] = u.x, m[1] = u.y, m[2] = v.x, m[3] = v.y;
 }
 
+// One work unit (group g, chunk c of its separations) of a warp.  The warp's
+// mbarriers keep counting phases across its units: chunk k of this unit is
+// the warp's chunk kbase + k (stage (kbase + k) % kFmStages).  Returns false
+// when a wait gave up.
 template <typename R, class Pos>
-__device__ __forceinline__ void fragmem_warp_bulk(const FMSlices<R> &t, const double *sig, int n, const Pos &pos,
-                                                  unsigned long long *facc, unsigned long long *e_acc,
-                                                  int e_stride, int *timed_out, unsigned char *wsm)
+__device__ __forceinline__ bool fragmem_unit_bulk(int w, const FMSlices<R> &t, const double *sig, int n,
+                                                  const Pos &pos, unsigned long long *facc,
+                                                  unsigned long long *e_acc, int e_stride, int *timed_out,
+                                                  unsigned char *wsm, unsigned &kbase)
 {
-  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-  if (w >= t.groups * t.dsplit) return;
+  const int lane = threadIdx.x & 31;
   const int g = w / t.dsplit, c = w - g * t.dsplit;
   const int d0 = c * t.nd / t.dsplit, d1 = (c + 1) * t.nd / t.dsplit;
   const int i = g * 32 + lane;
@@ -240,14 +244,10 @@ __device__ __forceinline__ void fragmem_warp_bulk(const FMSlices<R> &t, const do
     if (len > 0 && first < 0) first = t.soff[g * t.nd + dd];
     total += len;
   }
-  if (total <= 0) return;
+  if (total <= 0) return true;
   const int last = first + total, nchunks = (total + kFmStripes - 1) / kFmStripes;
-  if (lane == 0)
-    for (int s = 0; s < kFmStages; s++) mbar_init(bars + 8 * s, 1);
-  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-  __syncwarp();
-  auto issue = [&](int k) {  // lane 0: chunk k into stage k % kFmStages
-    const int st = k % kFmStages, s0 = first + k * kFmStripes, ns = min(kFmStripes, last - s0);
+  auto issue = [&](int k) {  // lane 0: chunk k into stage (kbase + k) % kFmStages
+    const int st = (kbase + k) % kFmStages, s0 = first + k * kFmStripes, ns = min(kFmStripes, last - s0);
     const uint32_t bar = bars + 8 * st, dst = data + st * stage_bytes;
     const uint32_t rb = ns * 32 * 4 * sizeof(R), cb = coef ? ns * 32 * sizeof(R) : 0;
     // the stage was last read through the generic proxy: order that before the async-proxy write
@@ -313,8 +313,8 @@ __device__ __forceinline__ void fragmem_warp_bulk(const FMSlices<R> &t, const do
   bool ok = true;
   int fail_k = 0;
   for (int k = 0; k < nchunks; k++) {
-    const int st = k % kFmStages;
-    if (!mbar_wait(bars + 8 * st, (k / kFmStages) & 1, kFmWaitLimit)) {
+    const int st = (kbase + k) % kFmStages;
+    if (!mbar_wait(bars + 8 * st, ((kbase + k) / kFmStages) & 1, kFmWaitLimit)) {
       ok = false;
       fail_k = k;
       break;
@@ -347,9 +347,10 @@ __device__ __forceinline__ void fragmem_warp_bulk(const FMSlices<R> &t, const do
     // record the failure, let the copies in flight land (bounded), skip the sums
     if (lane == 0) atomicExch(timed_out, 1);
     for (int k = fail_k; k < nchunks && k < fail_k + kFmStages; k++)
-      mbar_wait(bars + 8 * (k % kFmStages), (k / kFmStages) & 1, kFmWaitLimit / 8);
-    return;
+      mbar_wait(bars + 8 * ((kbase + k) % kFmStages), ((kbase + k) / kFmStages) & 1, kFmWaitLimit / 8);
+    return false;
   }
+  kbase += nchunks;
   end_row();
   if (live) {
     red_add3(facc + (size_t) 9 * i, fca);
@@ -363,6 +364,28 @@ __device__ __forceinline__ void fragmem_warp_bulk(const FMSlices<R> &t, const do
     for (int o = 16; o > 0; o >>= 1) ef += __shfl_xor_sync(0xffffffffu, ef, o);
     if (lane == 0 && ef) atomicAdd(e_acc, (unsigned long long) ef);
   }
+  return true;
+}
+
+// The kernel body: each warp takes work units w, w + warps, ... so a grid
+// smaller than the number of units (a few blocks per SM) still streams at
+// full bandwidth and leaves the rest of each SM to the concurrent pair passes.
+template <typename R, class Pos>
+__device__ __forceinline__ void fragmem_warp_bulk(const FMSlices<R> &t, const double *sig, int n, const Pos &pos,
+                                                  unsigned long long *facc, unsigned long long *e_acc,
+                                                  int e_stride, int *timed_out, unsigned char *wsm)
+{
+  const int lane = threadIdx.x & 31, units = t.groups * t.dsplit;
+  const int w0 = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
+  if (w0 >= units) return;
+  const uint32_t bars = smem_addr(wsm);
+  if (lane == 0)
+    for (int s = 0; s < kFmStages; s++) mbar_init(bars + 8 * s, 1);
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  __syncwarp();
+  unsigned kbase = 0;
+  for (int w = w0; w < units; w += nw)
+    if (!fragmem_unit_bulk(w, t, sig, n, pos, facc, e_acc, e_stride, timed_out, wsm, kbase)) return;
 }
 
 }  // namespace dev

@@ -243,10 +243,10 @@ class AwsemSystem:
 
     def autotune(self, reps: int = 5) -> dict:
         """Pick the fastest launch shapes on this system (awsem_autotune)."""
-        got = np.zeros(3, dtype=np.int32)
+        got = np.zeros(4, dtype=np.int32)
         _check(self.lib, self.lib.awsem_autotune(self.h, int(reps), _ptr(got)), "awsem_autotune")
         return {"fragmem_separations_per_warp": int(got[0]), "pair_pass_blocks": int(got[1]),
-                "hbond_blocks": int(got[2])}
+                "hbond_blocks": int(got[2]), "fragmem_blocks": int(got[3])}
 
     def model_info(self) -> np.ndarray:
         info = np.zeros(8, dtype=np.int64)

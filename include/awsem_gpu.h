@@ -194,8 +194,12 @@ int awsem_profile_step(awsem_system *sys, int reps, double *ms);
  * warp (1, 2, 3, 6 or all), and the grids of the pair-parallel passes and of
  * the hydrogen-bond pass (1 to 32 blocks per SM).  The state and the step
  * counter are restored afterwards; results do not depend on the shapes (all
- * sums are exact).  chosen (may be NULL): [separations per warp, pair-pass
- * blocks, hydrogen-bond blocks].  Not available on serving handles. */
+ * sums are exact).  The grid of the fragment-memory kernel (1 to 4 blocks
+ * per SM looping over the work, or one warp per unit) is judged on whole
+ * steps, since that kernel overlaps the pair passes.  chosen (may be NULL):
+ * [separations per warp, pair-pass blocks, hydrogen-bond blocks,
+ * fragment-memory blocks (0: one warp per unit)].  Not available on serving
+ * handles. */
 int awsem_autotune(awsem_system *sys, int reps, int *chosen);
 
 /* Sizes behind the roofline's algorithmic-byte counts:
