@@ -128,9 +128,8 @@ class EngineBase {
 void fragmem_noalloc(int device, const FMView &v, const double *d_x, double *d_f, double *d_energy,
                      cudaStream_t stream);  // awsem_noalloc.cu
 
-static const char *kKernelNames[AWSEM_NKERNELS] = {"prepare", "nl_decide", "nl_build", "density",
-                                                   "residue", "water_xi", "pair",      "hbond",
-                                                   "fragmem", "bonds",    "finish"};
+static const char *kKernelNames[AWSEM_NKERNELS] = {"prepare", "nl_decide", "nl_build", "density", "residue",
+                                                   "water_xi", "pair",     "hbond",     "fragmem", "finish"};
 
 template <typename R> class Engine : public EngineBase {
 
@@ -161,6 +160,7 @@ template <typename R> class Engine : public EngineBase {
   DBuf<int> res_sys, sys_begin, sys_end;
   DBuf<unsigned long long> sys_seed;
   int pcap = 0;  // residue pair list capacity (pairs)
+  int sms_ = 148;  // multiprocessors of the device
   bool server_pending = false;  // setup() called for a serving handle (no replicas yet)
   // residues the per-residue kernels cover: all of them, or on a serving
   // handle the used prefix of its capacity (rounded up to 4,096)
@@ -363,6 +363,7 @@ template <typename R> class Engine : public EngineBase {
     dacc.zero(s0);
     int sms = 148;
     CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    sms_ = sms;
     hb_blocks = std::max(1, std::min((nn * 8 + 127) / 128, 16 * sms));
     if (!server_pending) setup_grids();
     // size the pair list from a first build: room for 4x the initial pairs
@@ -452,7 +453,8 @@ template <typename R> class Engine : public EngineBase {
 
   void launch_list_build(const dev::StepArgs<R> &a, cudaStream_t s)
   {
-    const int nn = n_run(), tb = 128, nb = (nn + tb - 1) / tb, wb = (nn * 32 + tb - 1) / tb;
+    const int nn = n_run(), tb = 128, nb = (nn + tb - 1) / tb;
+    const int wb = std::min((nn * 32 + tb - 1) / tb, 8 * sms_);
     const dev::GridArgs g = grid_args();
     if (nbig) {
       dev::k_grid_setup<R><<<nbig, 256, 0, s>>>(a, g);
@@ -460,7 +462,7 @@ template <typename R> class Engine : public EngineBase {
       dev::k_grid_scan<R><<<nbig, 1024, 0, s>>>(a, g);
       dev::k_grid_fill<R><<<nb, tb, 0, s>>>(a, g);
     }
-    dev::k_nl_build<R><<<wb, tb, 0, s>>>(a, g);
+    dev::k_nl_build<R><<<wb, tb, 0, s>>>(a, g, nn);
   }
 
   void launch_prepare_and_list(const dev::StepArgs<R> &a, cudaStream_t s, bool force, bool advance)
@@ -492,7 +494,6 @@ template <typename R> class Engine : public EngineBase {
     dev::k_water_xi<R><<<pair_blocks, tb, 0, s0>>>(a, p);
     dev::k_pair<R><<<pair_blocks, tb, 0, s0>>>(a, p);
     dev::k_hbond<R><<<hb_blocks, 128, 0, s0>>>(a, p);
-    if (a.groups & dev::G_BOND) dev::k_bonds<R><<<nb, tb, 0, s0>>>(a);
     if (fm) CK(cudaStreamWaitEvent(s0, ev_join, 0));
   }
 
@@ -830,8 +831,7 @@ template <typename R> class Engine : public EngineBase {
           case 6: dev::k_pair<R><<<pair_blocks, tb, 0, s0>>>(a, p); break;
           case 7: dev::k_hbond<R><<<hb_blocks, 128, 0, s0>>>(a, p); break;
           case 8: if (fm) dev::k_fragmem<R><<<fm_blocks(), tb, fm_smem(), s0>>>(a, p); break;
-          case 9: dev::k_bonds<R><<<nb, tb, 0, s0>>>(a); break;
-          case 10: dev::k_finish<R><<<nb, tb, 0, s0>>>(a, d_integ.p, g1.p, g2.p, ftot.p, x.p); break;
+          case 9: dev::k_finish<R><<<nb, tb, 0, s0>>>(a, d_integ.p, g1.p, g2.p, ftot.p, x.p); break;
         }
         CK(cudaEventRecord(ev[2 * k + 1], s0));
       }

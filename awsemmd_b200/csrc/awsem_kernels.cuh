@@ -8,14 +8,14 @@
 //                radius, appended to a flat pair array
 //   density      thread/pair: rho_water, rho_helix (DL1, :7728-7791)
 //   residue      thread/residue: switching functions, burial (SL, :7795-7841),
-//                helical (i,i+4) pairs (:7843-7868), chain/chi/rama
+//                helical (i,i+4) pairs (:7843-7868), chain/chi/rama,
+//                harmonic bonds
 //   water_xi     thread/pair: xi_water (DL2, :7877-7954)
 //   pair         thread/pair: water/burial/helix radial forces, excluded
 //                volume (DL3, :7956-8134); queues DSSP and P_AP pairs
 //   hbond        thread/queued pair: DSSP hydrogen bonds, P_AP
 //   fragmem      warp/32 residues, lane/residue row: fragment-memory
 //                Gaussians (:4079-4177), on a second stream
-//   bonds        thread/residue: harmonic bonds
 //   finish       thread/residue: fixed-point -> FP64 forces, Langevin,
 //                velocity-Verlet half kicks and drift
 // Residue-owned quantities are written by their owner without atomics;
@@ -376,11 +376,9 @@ template <typename R> __global__ void k_grid_fill(StepArgs<R> a, GridArgs g)
 // own.  Every pair pass below runs one thread per listed pair and scatters to
 // both residues with fixed-point atomics: each pair is evaluated once, as in
 // the reference's half neighbour list.
-template <typename R> __global__ void k_nl_build(StepArgs<R> a, GridArgs g)
+template <typename R> __device__ __forceinline__ void nl_build_one(const StepArgs<R> &a, const GridArgs &g, int i,
+                                                               int lane)
 {
-  if (!a.nl->rebuild) return;
-  const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-  if (i >= a.s.n_res) return;
   if (a.res_sys[i] < 0) {
     if (lane == 0) a.ncount[i] = 0;
     return;
@@ -438,6 +436,16 @@ template <typename R> __global__ void k_nl_build(StepArgs<R> a, GridArgs g)
       if (take && k < a.pcap) a.pairs[k] = make_int2(i, j);
       at += __popc(m);
     });
+}
+
+// a fixed grid of warps loops over the residues, so the launch costs little
+// on the steps that do not rebuild
+template <typename R> __global__ void k_nl_build(StepArgs<R> a, GridArgs g, int n_launch)
+{
+  if (!a.nl->rebuild) return;
+  const int lane = threadIdx.x & 31;
+  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n_launch; i += (gridDim.x * blockDim.x) >> 5)
+    nl_build_one(a, g, i, lane);
 }
 
 // Pairs of the list, grid-stride (the count is known only on the device)
@@ -511,6 +519,26 @@ __device__ __forceinline__ R ev_pair(const StepArgs<R> &a, int ta, int tb, bool 
   R fp = r > R(0) ? -pr * R(a.ev_p) / r : R(0);
   f = {d.x * fp, d.y * fp, d.z * fp};
   return pr * dr;
+}
+
+// bond_style harmonic, the bonds whose first atom is in residue r (run by
+// k_residue's thread of that residue)
+template <typename R> __device__ __forceinline__ void bonds_of(const StepArgs<R> &a, int r)
+{
+  const DevSys<R> &s = a.s;
+  double e = 0.0;
+  for (int b = r * a.bond_cap; b < (r + 1) * a.bond_cap && a.bond_i[b] >= 0; b++) {
+    int ai = a.bond_i[b], aj = a.bond_j[b];
+    V3<R> d = diff<R>(bead(s, ai / 3, ai % 3), bead(s, aj / 3, aj % 3));
+    R rr = m_sqrt(norm2(d));
+    R dr = rr - R(a.bond_r0[b]);
+    R rk = R(a.bond_k[b]) * dr;
+    R fb = rr > R(0) ? R(-2) * rk / rr : R(0);
+    e += (double) (rk * dr);
+    scatter(s, ai / 3, ai % 3, d.x * fb, d.y * fb, d.z * fb);
+    scatter(s, aj / 3, aj % 3, -d.x * fb, -d.y * fb, -d.z * fb);
+  }
+  a.e_res[(size_t) E_BOND * s.n_res + r] = e;
 }
 
 // SL and the per-residue backbone terms
@@ -592,6 +620,7 @@ template <typename R> __global__ void k_residue(StepArgs<R> a, FFParams p)
       }
     }
   E[(size_t) E_PAIR * n + i] = ev;
+  if (a.groups & G_BOND) bonds_of(a, i);
 }
 
 // DL2: water-mediated density derivative coefficients (fix_backbone.cpp:
@@ -827,27 +856,6 @@ template <typename R> __global__ void __launch_bounds__(128) k_fragmem(StepArgs<
   unsigned char *wsm = fm_smem + (threadIdx.x >> 5) * fm_warp_smem<R>(a.fm.coef != nullptr);
   fragmem_warp_bulk(a.fm, p.fm_sigma_sq, a.s.n_res, pos, a.s.facc,
                     (unsigned long long *) (a.e_fix + (size_t) 2 * a.s.n_res), 1, &a.nl->fm_timeout, wsm);
-}
-
-// bond_style harmonic, bonds grouped by the residue of their first atom
-template <typename R> __global__ void k_bonds(StepArgs<R> a)
-{
-  int r = blockIdx.x * blockDim.x + threadIdx.x;
-  const DevSys<R> &s = a.s;
-  if (r >= s.n_res) return;
-  double e = 0.0;
-  for (int b = r * a.bond_cap; b < (r + 1) * a.bond_cap && a.bond_i[b] >= 0; b++) {
-    int ai = a.bond_i[b], aj = a.bond_j[b];
-    V3<R> d = diff<R>(bead(s, ai / 3, ai % 3), bead(s, aj / 3, aj % 3));
-    R rr = m_sqrt(norm2(d));
-    R dr = rr - R(a.bond_r0[b]);
-    R rk = R(a.bond_k[b]) * dr;
-    R fb = rr > R(0) ? R(-2) * rk / rr : R(0);
-    e += (double) (rk * dr);
-    scatter(s, ai / 3, ai % 3, d.x * fb, d.y * fb, d.z * fb);
-    scatter(s, aj / 3, aj % 3, -d.x * fb, -d.y * fb, -d.z * fb);
-  }
-  a.e_res[(size_t) E_BOND * s.n_res + r] = e;
 }
 
 __device__ __forceinline__ uint64_t mix64(uint64_t z)
