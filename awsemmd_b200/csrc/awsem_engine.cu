@@ -1671,6 +1671,37 @@ int awsem_create_from_files(const char *workdir, const char *data_file, const ch
   return rc;
 }
 
+int awsem_create_from_atoms(const char *workdir, const char *coeff_file, const char *seq_file, int natoms,
+                            const int *role, const int *residue, const int *molecule, const int *type, const int *tag,
+                            const double *mass_by_type, int ntypes, const double *x, int nbonds, const int *bond_a,
+                            const int *bond_b, const double *bond_k, const double *bond_r0, const char *pair_style,
+                            const char *pair_coeffs, int precision, int device, awsem_system **out)
+{
+  if (!out || !coeff_file || !seq_file || natoms <= 0 || !role || !residue || !molecule || !type || !tag ||
+      !mass_by_type || (nbonds > 0 && (!bond_a || !bond_b || !bond_k || !bond_r0))) {
+    g_last_error = "awsem_create_from_atoms: null or empty argument";
+    return AWSEM_EINVAL;
+  }
+  int rc = awsem_batch_create(precision, device, out);
+  if (rc != AWSEM_OK) return rc;
+  rc = guarded([&] {
+    std::unique_ptr<SystemInput> S(new SystemInput());
+    load_system_atoms(workdir ? workdir : "", coeff_file, seq_file, natoms, role, residue, molecule, type, tag,
+                      mass_by_type, ntypes, x, nullptr, std::max(nbonds, 0), bond_a, bond_b, bond_k, bond_r0,
+                      pair_style ? pair_style : "2 3.5 3.5", pair_coeffs ? pair_coeffs : "", *S, true);
+    (*out)->eng->reps.push_back(std::move(S));
+    (*out)->eng->seeds.push_back(0ull);
+  });
+  if (rc == AWSEM_OK) rc = awsem_batch_commit(*out);
+  if (rc != AWSEM_OK) {
+    std::string msg = g_last_error;
+    delete *out;
+    *out = nullptr;
+    g_last_error = msg;
+  }
+  return rc;
+}
+
 void awsem_destroy(awsem_system *sys) { delete sys; }
 
 static bool ready(const awsem_system *sys)

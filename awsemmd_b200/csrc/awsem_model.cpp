@@ -964,9 +964,6 @@ void load_system_dir(const std::string &dir, const std::string &data_file, const
     int a = tag_to_ext.at(atoi(t[0].c_str()));
     for (int k = 0; k < 3; k++) ve[3 * a + k] = atof(t[1 + k].c_str());
   }
-  build_topology(S.top, natoms, role.data(), res.data(), mol.data(), typ.data(), tag.data(), mass.data(), ntypes);
-  std::vector<int> ext_to_int(natoms);
-  for (int s = 0; s < S.top.n_atoms; s++) ext_to_int[S.top.ext_of[s]] = s;
   std::vector<double> bk(nbt + 1, 0.0), br(nbt + 1, 0.0);
   for (auto &l : sec["Bond Coeffs"]) {
     auto t = tokens(l);
@@ -983,7 +980,26 @@ void load_system_dir(const std::string &dir, const std::string &data_file, const
     kk.push_back(bk.at(bt));
     rr.push_back(br.at(bt));
   }
-  set_bonds(S.top, (int) bi.size(), bi.data(), bj.data(), kk.data(), rr.data(), ext_to_int.data());
+  load_system_atoms(dir, coeff_file, seq_file, natoms, role.data(), res.data(), mol.data(), typ.data(), tag.data(),
+                    mass.data(), ntypes, xe.data(), ve.data(), (int) bi.size(), bi.data(), bj.data(), kk.data(),
+                    rr.data(), pair_style, pair_coeffs, S, false);
+}
+
+void load_system_atoms(const std::string &dir, const std::string &coeff_file, const std::string &seq_file,
+                       int natoms, const int *role, const int *res, const int *mol, const int *typ, const int *tag,
+                       const double *mass, int ntypes, const double *xe, const double *ve, int nbonds,
+                       const int *bond_a, const int *bond_b, const double *bond_k, const double *bond_r0,
+                       const std::string &pair_style, const std::string &pair_coeffs, SystemInput &S,
+                       bool read_files)
+{
+  if (read_files) {
+    read_coeff_file(path_in(dir, coeff_file), S.ff);
+    read_sequence(path_in(dir, seq_file), S.top);
+  }
+  build_topology(S.top, natoms, role, res, mol, typ, tag, mass, ntypes);
+  std::vector<int> ext_to_int(natoms);
+  for (int s = 0; s < S.top.n_atoms; s++) ext_to_int[S.top.ext_of[s]] = s;
+  set_bonds(S.top, nbonds, bond_a, bond_b, bond_k, bond_r0, ext_to_int.data());
   set_pair_coeffs(S.top, pair_style, pair_coeffs);
   read_tables(dir, S.ff, S.top);
   if (S.ff.p.terms & T_FM) {
@@ -999,8 +1015,8 @@ void load_system_dir(const std::string &dir, const std::string &data_file, const
   S.v.assign(3 * S.top.n_atoms, 0.0);
   for (int s = 0; s < S.top.n_atoms; s++)
     for (int k = 0; k < 3; k++) {
-      S.x[3 * s + k] = xe[3 * S.top.ext_of[s] + k];
-      S.v[3 * s + k] = ve[3 * S.top.ext_of[s] + k];
+      if (xe) S.x[3 * s + k] = xe[3 * S.top.ext_of[s] + k];
+      if (ve) S.v[3 * s + k] = ve[3 * S.top.ext_of[s] + k];
     }
 }
 

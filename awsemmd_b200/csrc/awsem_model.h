@@ -146,6 +146,18 @@ void set_pair_coeffs(Topology &top, const std::string &style, const std::string 
 void build_fm_table(const ForceField &ff, const Topology &top, const GammaTable &g,
                     const std::vector<Memory> &mems, FMTable &out);
 
+// A system from per-atom arrays in the caller's order (a host code's own
+// atom data: roles 0 CA, 1 CB/H-beta, 2 O, -1 other; residue and molecule
+// ids, types, tags, masses by type, x and v (either may be null), bonds as
+// caller indices), with the coefficient file, sequence and tables of `dir`
+// (read_files: also read the coefficient and sequence files).
+void load_system_atoms(const std::string &dir, const std::string &coeff_file, const std::string &seq_file,
+                       int natoms, const int *role, const int *res, const int *mol, const int *typ, const int *tag,
+                       const double *mass, int ntypes, const double *xe, const double *ve, int nbonds,
+                       const int *bond_a, const int *bond_b, const double *bond_k, const double *bond_r0,
+                       const std::string &pair_style, const std::string &pair_coeffs, SystemInput &S,
+                       bool read_files);
+
 // Whole system from a directory laid out like a reference run directory.
 void load_system_dir(const std::string &dir, const std::string &data_file, const std::string &coeff_file,
                      const std::string &seq_file, const std::string &pair_style, const std::string &pair_coeffs,

@@ -77,6 +77,20 @@ int awsem_create_from_files(const char *workdir, const char *data_file, const ch
                             int precision, int device, awsem_system **out);
 void awsem_destroy(awsem_system *sys);
 
+/* The same system from a host code's own atom arrays instead of a data file
+ * (what a LAMMPS fix has in memory): per atom, in the caller's order, its
+ * role (0 CA, 1 CB or H-beta, 2 O, -1 other: the CA / CB / O groups of
+ * `fix backbone`), residue and molecule ids, type and tag; masses by type
+ * (mass_by_type[1..ntypes]); x (may be NULL); bonds as caller indices
+ * (nbonds may be 0 when the host computes the bonds itself).  The
+ * coefficient and sequence files and the tables are read from `workdir`, as
+ * by the FixBackbone constructor (src/fix_backbone.cpp:86-1072). */
+int awsem_create_from_atoms(const char *workdir, const char *coeff_file, const char *seq_file, int natoms,
+                            const int *role, const int *residue, const int *molecule, const int *type, const int *tag,
+                            const double *mass_by_type, int ntypes, const double *x, int nbonds, const int *bond_a,
+                            const int *bond_b, const double *bond_k, const double *bond_r0, const char *pair_style,
+                            const char *pair_coeffs, int precision, int device, awsem_system **out);
+
 /* Batches of independent replicas (one launch sequence advances them all).
  * Create an empty handle, add replicas (each a reference-style run
  * directory; all must share one coefficient file, tables and pair_style),

@@ -3,6 +3,9 @@
 * ``RefSystem``: the reference FixBackbone + PairExcludedVolume, compiled
   unmodified from the reference sources against the LAMMPS-API shim
   (``oracle/_ref/libawsem_ref.so``, built by ``make -C oracle ref``).
+  ``RefSystem(files, gpu_fix="fp64" | "mixed")`` runs the same host with the
+  GPU adapter ``fix backbone/gpu`` in place of the reference fix
+  (``oracle/_ref/libawsem_ref_gpufix.so``, ``make -C oracle gpufix``).
 """
 from __future__ import annotations
 
@@ -13,18 +16,22 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_LIB = os.path.join(HERE, "_ref", "libawsem_ref.so")
+GPUFIX_LIB = os.path.join(HERE, "_ref", "libawsem_ref_gpufix.so")
 
-_ref = None
+_libs = {}
 
 
 def ref_available() -> bool:
     return os.path.exists(REF_LIB)
 
 
-def _load_ref():
-    global _ref
-    if _ref is None:
-        lib = C.CDLL(REF_LIB)
+def gpufix_available() -> bool:
+    return os.path.exists(GPUFIX_LIB)
+
+
+def _load_ref(path=REF_LIB):
+    if path not in _libs:
+        lib = C.CDLL(path)
         lib.ref_create.restype = C.c_void_p
         lib.ref_create.argtypes = [C.c_char_p] * 6 + [C.c_double, C.c_int, C.c_int, C.c_int]
         lib.ref_destroy.argtypes = [C.c_void_p]
@@ -43,19 +50,25 @@ def _load_ref():
         lib.ref_last_error.restype = C.c_char_p
         lib.ref_uniform.restype = C.c_double
         lib.ref_uniform.argtypes = [C.c_ulonglong, C.c_longlong, C.c_longlong, C.c_int]
-        _ref = lib
-    return _ref
+        if path == GPUFIX_LIB:
+            lib.ref_create_gpufix.restype = C.c_void_p
+            lib.ref_create_gpufix.argtypes = [C.c_char_p] * 6 + [C.c_double, C.c_int, C.c_int, C.c_int, C.c_int]
+        _libs[path] = lib
+    return _libs[path]
 
 
 class RefSystem:
     """One reference FixBackbone system hosted by the shim MD loop."""
 
-    def __init__(self, files: dict, skin=2.0, every=1, delay=0, check=1):
-        lib = _load_ref()
+    def __init__(self, files: dict, skin=2.0, every=1, delay=0, check=1, gpu_fix: str | None = None):
+        lib = _load_ref(GPUFIX_LIB if gpu_fix else REF_LIB)
         self.lib = lib
-        self.h = lib.ref_create(files["workdir"].encode(), files["data"].encode(), files["coeff"].encode(),
-                                files["seq"].encode(), files["pair_style"].encode(),
-                                files["pair_coeffs"].encode(), skin, every, delay, check)
+        args = (files["workdir"].encode(), files["data"].encode(), files["coeff"].encode(), files["seq"].encode(),
+                files["pair_style"].encode(), files["pair_coeffs"].encode(), skin, every, delay, check)
+        if gpu_fix:
+            self.h = lib.ref_create_gpufix(*args, {"fp64": 0, "mixed": 1}[gpu_fix])
+        else:
+            self.h = lib.ref_create(*args)
         if not self.h:
             raise RuntimeError(lib.ref_last_error().decode())
         self.natoms = lib.ref_natoms(self.h)

@@ -20,9 +20,16 @@
        (post_neighbor, pre_force, pair, bond, post_force, final_integrate).
    The one deliberate change: the Langevin noise comes from a counter-based
    generator keyed by (seed, step, atom tag, component) instead of LAMMPS's
-   sequential RanMars stream, so the GPU engine can draw the same numbers. */
+   sequential RanMars stream, so the GPU engine can draw the same numbers.
+
+   Built with AWSEM_GPU_FIX, the host can also run the GPU adapter `fix
+   backbone/gpu` (awsemmd_b200/lammps) in place of the reference fix, through
+   the same LAMMPS fix hooks (ref_create_gpufix). */
 #include "lmp_shim.h"
 #include "fix_backbone.h"
+#ifdef AWSEM_GPU_FIX
+#include "fix_backbone_gpu.h"
+#endif
 #include "pair_excluded_volume.h"
 #include "atom_vec_awsemmd.h"
 
@@ -88,7 +95,8 @@ std::vector<std::string> split_ws(const std::string &s)
 
 struct RefHost {
   LAMMPS *lmp = nullptr;
-  FixBackbone *fix = nullptr;
+  Fix *fix = nullptr;
+  FixBackbone *fb = nullptr;  // the reference fix (null when the GPU adapter is hosted)
   PairExcludedVolume *pair = nullptr;
   std::string workdir;
 
@@ -135,6 +143,9 @@ struct RefHost {
       delete lmp;
     }
   }
+
+  // term k of the fix's energy vector (0: total)
+  double fix_energy(int k) { return fb ? fb->energy[k] : (k ? fix->compute_vector(k - 1) : fix->compute_scalar()); }
 
   void read_data(const std::string &path);
   void build_lists();
@@ -489,9 +500,9 @@ const char *ref_last_error() { return g_ref_err.c_str(); }
 /* Create the host, read the data file, construct the reference fix and pair.
    pair_style: "p cut_short cut_long"; pair_coeffs: ';'-separated
    "i j lambda [cs cl]" records; groups by atom type: CA, CB (and H-beta), O. */
-void *ref_create(const char *workdir, const char *data_file, const char *coeff_file,
-                 const char *seq_file, const char *pair_style, const char *pair_coeffs,
-                 double skin, int every, int delay, int check)
+static void *create_host(const char *workdir, const char *data_file, const char *coeff_file,
+                         const char *seq_file, const char *pair_style, const char *pair_coeffs,
+                         double skin, int every, int delay, int check, int gpu_fix)
 {
   RefHost *h = new RefHost();
   try {
@@ -563,7 +574,15 @@ void *ref_create(const char *workdir, const char *data_file, const char *coeff_f
                                     coeff_file, seq_file};
       std::vector<char *> args;
       for (auto &s : v) args.push_back(strdup(s.c_str()));
-      h->fix = new FixBackbone(lmp, 7, args.data());
+#ifdef AWSEM_GPU_FIX
+      if (gpu_fix >= 0) {
+        free(args[2]);
+        args[2] = strdup("backbone/gpu");
+        args.push_back(strdup(gpu_fix == 1 ? "mixed" : "fp64"));
+        h->fix = new FixBackboneGPU(lmp, (int) args.size(), args.data());
+      } else
+#endif
+        h->fix = h->fb = new FixBackbone(lmp, 7, args.data());
       for (char *c : args) free(c);
     }
     // init: force (pair) first, then fixes, then neighbour lists to requestors
@@ -585,6 +604,26 @@ void *ref_create(const char *workdir, const char *data_file, const char *coeff_f
   }
   return h;
 }
+
+void *ref_create(const char *workdir, const char *data_file, const char *coeff_file,
+                 const char *seq_file, const char *pair_style, const char *pair_coeffs,
+                 double skin, int every, int delay, int check)
+{
+  return create_host(workdir, data_file, coeff_file, seq_file, pair_style, pair_coeffs, skin, every, delay,
+                     check, -1);
+}
+
+#ifdef AWSEM_GPU_FIX
+/* The same host with `fix backbone/gpu` (precision 0 FP64, 1 mixed) in place
+   of the reference fix. */
+void *ref_create_gpufix(const char *workdir, const char *data_file, const char *coeff_file,
+                        const char *seq_file, const char *pair_style, const char *pair_coeffs,
+                        double skin, int every, int delay, int check, int precision)
+{
+  return create_host(workdir, data_file, coeff_file, seq_file, pair_style, pair_coeffs, skin, every, delay,
+                     check, precision);
+}
+#endif
 
 void ref_destroy(void *hp)
 {
@@ -630,7 +669,7 @@ int ref_set(void *hp, const char *what, const double *in)
 int ref_energies(void *hp, double *out)
 {
   RefHost *h = (RefHost *) hp;
-  for (int k = 0; k < 18; k++) out[k] = h->fix->energy[k];
+  for (int k = 0; k < 18; k++) out[k] = h->fix_energy(k);
   out[18] = h->e_pair;
   out[19] = h->e_bond;
   out[20] = h->kinetic();
@@ -665,7 +704,8 @@ int ref_compute(void *hp, long long step, double *f_out)
 int ref_residue_arrays(void *hp, double *out)
 {
   RefHost *h = (RefHost *) hp;
-  FixBackbone *fb = h->fix;
+  FixBackbone *fb = h->fb;
+  if (!fb) return 0;
   int n = fb->n;
   for (int i = 0; i < n; i++) {
     out[6 * i + 0] = fb->water_ro[i];
@@ -703,7 +743,7 @@ int ref_run(void *hp, long long nsteps, double dt, int langevin, double t_start,
     h->forces(true);
     auto thermo = [&](long long row) {
       if (!thermo_out) return;
-      thermo_out[4 * row + 0] = h->fix->energy[0];
+      thermo_out[4 * row + 0] = h->fix_energy(0);
       thermo_out[4 * row + 1] = h->e_pair;
       thermo_out[4 * row + 2] = h->e_bond;
       thermo_out[4 * row + 3] = h->kinetic();
