@@ -91,22 +91,28 @@ def parse():
 # --------------------------------------------------------------------------
 
 class Dist:
-    """One process per GPU; replicas only (no data-path collective)."""
+    """One process per GPU; replicas only (no data-path collective).  NCCL
+    on GPUs; gloo when there is no GPU (the CPU tests of the rank logic)."""
 
     def __init__(self):
         self.world = int(os.environ.get("WORLD_SIZE", "1"))
         self.rank = int(os.environ.get("RANK", "0"))
         self.local = int(os.environ.get("LOCAL_RANK", "0"))
         self.pg = None
+        self.device = "cpu"
         if self.world > 1:
             import datetime
 
             import torch
             import torch.distributed as dist
 
-            torch.cuda.set_device(self.local)
-            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
-                                    device_id=torch.device("cuda", self.local))
+            timeout = datetime.timedelta(seconds=600)
+            if torch.cuda.is_available():
+                torch.cuda.set_device(self.local)
+                self.device = f"cuda:{self.local}"
+                dist.init_process_group("nccl", timeout=timeout, device_id=torch.device("cuda", self.local))
+            else:
+                dist.init_process_group("gloo", timeout=timeout)
             self.pg = dist
 
     def barrier(self):
@@ -114,11 +120,12 @@ class Dist:
             self.pg.barrier()
 
     def max(self, v: float) -> float:
+        """The largest value over the ranks (timings: the slowest rank)."""
         if not self.pg:
             return v
         import torch
 
-        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        t = torch.tensor([v], dtype=torch.float64, device=self.device)
         self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
         return float(t.item())
 
