@@ -681,6 +681,9 @@ template <typename R> __global__ void __launch_bounds__(128, 6) k_pair(StepArgs<
   const bool fix = a.groups & G_FIX, evon = a.groups & G_PAIR;
   const uint32_t T = fix ? p.terms : 0u;
   const R ev_pre_sq = R(a.nl->ev_pre_sq);
+  // the largest excluded-volume cutoff, squared, with room for its rounding
+  // to float and for the rounding of the bead distance
+  const R ev_max_sq = R(a.nl->r_ev) * R(a.nl->r_ev) * R(1.0001);
   // smallest same-chain separation of any P_AP class (fix_backbone.cpp:3279-3383)
   const int pap_sep = min(p.i_med_min + 2 * p.i_diff_pap, p.i_med_max + 1);
   const int dh = p.helix_i_diff;
@@ -775,8 +778,10 @@ template <typename R> __global__ void __launch_bounds__(128, 6) k_pair(StepArgs<
 #pragma unroll
         for (int b0 = 0; b0 < 3; b0++) {
           if (excl & (1u << (b0 * 3 + b1))) continue;
+          const V3<R> dd = diff<R>(bi[b0], bj);
+          if (norm2(dd) > ev_max_sq) continue;  // beyond every cutoff: no table lookups
           V3<R> f;
-          const R e = ev_pair(a, tai[b0], tb, shortr, diff<R>(bi[b0], bj), f);
+          const R e = ev_pair(a, tai[b0], tb, shortr, dd, f);
           if (e == R(0) && f.x == R(0) && f.y == R(0) && f.z == R(0)) continue;
           ee += (double) e;
           const long long v[3] = {fix_force((double) f.x), fix_force((double) f.y), fix_force((double) f.z)};
