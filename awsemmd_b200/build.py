@@ -18,7 +18,13 @@ LIB = os.path.join(HERE, "libawsem_gpu.so")
 BUILD = os.path.join(HERE, "_build")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
+# -fmad=false: no multiply-add contraction left to the compiler.  Every
+# product and sum is then rounded on its own, in source order, as the x86-64
+# CPU build of the reference computes them, and identically in every kernel
+# that inlines the same device code (the per-pass kernels and the persistent
+# step kernel give bit-identical trajectories).  Fused operations are written
+# out where they are wanted (__fmaf_rn / __fma_rn).
+NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-fmad=false", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
               "--expt-relaxed-constexpr", "-I" + CSRC, "-I" + INCLUDE]
 SOURCES = ["awsem_model.cpp", "awsem_engine.cu", "awsem_noalloc.cu"]
 
@@ -41,6 +47,7 @@ def build(verbose: bool = False, force: bool = False) -> str:
     os.makedirs(BUILD, exist_ok=True)
     headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
     headers.append(os.path.join(INCLUDE, "awsem_gpu.h"))
+    headers.append(os.path.abspath(__file__))  # the flags above
     objs = []
     for src in SOURCES:
         path = os.path.join(CSRC, src)

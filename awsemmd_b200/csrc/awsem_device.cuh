@@ -45,13 +45,28 @@ __device__ __forceinline__ double norm2(V3<double> d)
 {
   return __dadd_rn(__dadd_rn(__dmul_rn(d.x, d.x), __dmul_rn(d.y, d.y)), __dmul_rn(d.z, d.z));
 }
-__device__ __forceinline__ float norm2(V3<float> d) { return d.x * d.x + d.y * d.y + d.z * d.z; }
+// FP32: the multiply-adds are spelled out, so every kernel that inlines this
+// (the per-pass kernels and the persistent step kernel) rounds identically.
+__device__ __forceinline__ float norm2(V3<float> d)
+{
+  return __fmaf_rn(d.z, d.z, __fmaf_rn(d.y, d.y, __fmul_rn(d.x, d.x)));
+}
 
 __device__ __forceinline__ double dot(V3<double> a, V3<double> b)
 {
   return __dadd_rn(__dadd_rn(__dmul_rn(a.x, b.x), __dmul_rn(a.y, b.y)), __dmul_rn(a.z, b.z));
 }
-__device__ __forceinline__ float dot(V3<float> a, V3<float> b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ float dot(V3<float> a, V3<float> b)
+{
+  return __fmaf_rn(a.z, b.z, __fmaf_rn(a.y, b.y, __fmul_rn(a.x, b.x)));
+}
+
+// c + a * b with one rounding, in either form: accumulations whose
+// contraction would otherwise be left to the compiler
+__device__ __forceinline__ double madd(double a, double b, double c) { return __fma_rn(a, b, c); }
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float madd(float a, float b, float c) { return __fmaf_rn(a, b, c); }
 
 template <typename R> __device__ __forceinline__ V3<R> cross(V3<R> a, V3<R> b)
 {
@@ -146,6 +161,20 @@ __device__ __forceinline__ void well_theta(R r, R rmin_th, R rmax_th, R kappa, R
   R t_max = m_tanh(kappa * (rmax - r));
   theta = R(0.25) * (R(1) + t_min) * (R(1) + t_max);
   prd = kappa * theta * (t_max - t_min) / r;
+}
+// FP32 with every operation spelled out (no contraction left to the compiler)
+template <>
+__device__ __forceinline__ void well_theta(float r, float rmin_th, float rmax_th, float kappa, float rmin, float rmax,
+                                           float &theta, float &prd)
+{
+  if (r < rmin_th || r > rmax_th) {
+    theta = prd = 0.f;
+    return;
+  }
+  const float t_min = tanhf(__fmul_rn(kappa, __fsub_rn(r, rmin)));
+  const float t_max = tanhf(__fmul_rn(kappa, __fsub_rn(rmax, r)));
+  theta = __fmul_rn(__fmul_rn(0.25f, __fadd_rn(1.f, t_min)), __fadd_rn(1.f, t_max));
+  prd = __fdiv_rn(__fmul_rn(__fmul_rn(kappa, theta), __fsub_rn(t_max, t_min)), r);
 }
 
 // compute_chain_potential(i), fix_backbone.cpp:2062-2170

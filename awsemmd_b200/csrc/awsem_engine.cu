@@ -13,7 +13,7 @@
 #include <vector>
 
 #include "awsem_gpu.h"
-#include "awsem_kernels.cuh"
+#include "awsem_step.cuh"
 #include "awsem_model.h"
 
 namespace awsem {
@@ -109,6 +109,8 @@ class EngineBase {
   virtual void nl_stats(int *nbuilds, double *radius, int *maxc, int *overflow) = 0;
   virtual void profile(int reps, double *ms) = 0;
   virtual void autotune(int reps, int *chosen) = 0;
+  virtual void set_step_form(int form, int blocks, int stream_warps) = 0;
+  virtual void get_step_form(int *out) = 0;
   virtual void model_info(long long *info) = 0;
   virtual double run_ms() const = 0;
   // device-resident fragment-memory table, for entry points outside the engine
@@ -193,6 +195,7 @@ template <typename R> class Engine : public EngineBase {
   {
     dev::StepArgs<R> a{};
     a.s.n_res = n();
+    a.n_run = n_run();
     a.s.res_type = res_type.p;
     a.s.res_flags = res_flags.p;
     a.s.res_chain = res_chain.p;
@@ -564,6 +567,14 @@ template <typename R> class Engine : public EngineBase {
                        std::to_string(st.overflow) + "); results of this call are invalid");
     if (st.fm_timeout)
       throw StateError("fragment-memory stream: a shared-memory copy wait gave up; results of this call are invalid");
+    if (gbar.p) {
+      dev::GridBar gb;
+      CK(cudaMemcpy(&gb, gbar.p, sizeof gb, cudaMemcpyDeviceToHost));
+      if (gb.timeout) {
+        CK(cudaMemset(gbar.p, 0, sizeof gb));
+        throw StateError("persistent step: a grid barrier wait gave up; results of this call are invalid");
+      }
+    }
   }
 
   void check_rep(int rep)
@@ -662,11 +673,17 @@ template <typename R> class Engine : public EngineBase {
   {
     auto a = args(groups_all);
     int nn = n(), tb = 128, nb = (n_run() + tb - 1) / tb;
+    const bool persistent = step_form == 1;
+    if (persistent) prepare_persistent(a);
     cudaGraph_t graph;
     CK(cudaStreamBeginCapture(s0, cudaStreamCaptureModeThreadLocal));
     for (int c = 0; c < count; c++) {
-      launch_eval(a, true);
-      dev::k_finish<R><<<nb, tb, 0, s0>>>(a, d_integ.p, g1.p, g2.p, ftot.p, x.p);
+      if (persistent) {
+        launch_step_persistent(a);
+      } else {
+        launch_eval(a, true);
+        dev::k_finish<R><<<nb, tb, 0, s0>>>(a, d_integ.p, g1.p, g2.p, ftot.p, x.p);
+      }
       if (thermo)
         dev::k_thermo<<<n_sys(), 256, 0, s0>>>(e_res.p, e_fix.p, nn, dstep.p, d_integ.p, sys_begin.p, sys_end.p,
                                                thermo_nrows, thermo_rows.p);
@@ -675,6 +692,79 @@ template <typename R> class Engine : public EngineBase {
     set_node_priorities(graph);
     CK(cudaGraphInstantiate(&exec, graph, 0));
     CK(cudaGraphDestroy(graph));
+  }
+
+  // Step form: 0 = the chain of per-pass kernels above (fragment memory on a
+  // second stream), 1 = the persistent step kernel of awsem_step.cuh (one
+  // cooperative launch per step; replicas without cell grids only).
+  int step_form = 0;
+  int ps_blocks = 0;  // persistent grid requested (0: every block that fits)
+  int ps_stream = 2;  // fragment-memory stream warps per block
+  int ps_grid_now = 0, ps_smem_now = 0;
+  DBuf<dev::GridBar> gbar;
+
+  bool fm_on(const dev::StepArgs<R> &a) const { return (a.groups & dev::G_FIX) && in.ff.p.fm_nd > 0; }
+  // warps with a shared-memory copy ring: as many as fit in about half an SM's shared memory
+  int ps_ring_warps() const
+  {
+    return std::min(dev::kStepThreads / 32, (112 * 1024) / dev::fm_warp_smem<R>(!in.fm.uniform));
+  }
+
+  // grid and shared memory of the persistent kernel (outside stream capture)
+  void prepare_persistent(const dev::StepArgs<R> &a)
+  {
+    if (nbig) throw std::invalid_argument("the persistent step kernel does not build cell grids (replicas above 2,048 residues)");
+    // fresh barrier state for the graphs about to be captured (nothing is in flight on s0)
+    if (!gbar.p) gbar.alloc(1);
+    CK(cudaMemsetAsync(gbar.p, 0, sizeof(dev::GridBar), s0));
+    CK(cudaStreamSynchronize(s0));
+    ps_smem_now = fm_on(a) ? ps_ring_warps() * dev::fm_warp_smem<R>(!in.fm.uniform) : 0;
+    CK(cudaFuncSetAttribute(dev::k_step<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, ps_smem_now));
+    int per_sm = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dev::k_step<R>, dev::kStepThreads, ps_smem_now));
+    if (per_sm < 1) throw CudaError("the persistent step kernel does not fit on a multiprocessor");
+    const int most = per_sm * sms_;
+    ps_grid_now = ps_blocks > 0 ? std::min(ps_blocks, most) : most;
+  }
+
+  // one MD step (evaluation, Langevin, velocity Verlet) as one cooperative launch
+  void launch_step_persistent(const dev::StepArgs<R> &a)
+  {
+    const bool fm = fm_on(a);
+    dev::PersistArgs q{d_integ.p, g1.p, g2.p, ftot.p, x.p, gbar.p, n_run(), ps_stream,
+                       fm ? ps_ring_warps() : 0, fm ? std::min(fm_groups, (n_run() + 31) / 32) * fm_dsplit : 0};
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(ps_grid_now);
+    cfg.blockDim = dim3(dev::kStepThreads);
+    cfg.dynamicSmemBytes = ps_smem_now;
+    cfg.stream = s0;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeCooperative;
+    at[0].val.cooperative = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    CK(cudaLaunchKernelEx(&cfg, dev::k_step<R>, a, in.ff.p, q));
+  }
+
+  void set_step_form(int form, int blocks, int stream_warps) override
+  {
+    if (form != 0 && form != 1) throw std::invalid_argument("step form must be 0 (per-pass kernels) or 1 (persistent)");
+    if (blocks < 0) throw std::invalid_argument("blocks must be >= 0 (0: every block that fits)");
+    if (stream_warps < 1 || stream_warps > dev::kStepThreads / 32 - 1)
+      throw std::invalid_argument("stream_warps must be in 1..7");
+    if (form == 1 && nbig)
+      throw std::invalid_argument("the persistent step kernel does not build cell grids (replicas above 2,048 residues)");
+    step_form = form;
+    ps_blocks = blocks;
+    ps_stream = stream_warps;
+    release_graphs();
+  }
+
+  void get_step_form(int *out) override
+  {
+    out[0] = step_form;
+    out[1] = step_form == 1 ? (ps_grid_now ? ps_grid_now : ps_blocks) : 0;
+    out[2] = ps_stream;
   }
 
   // Kernel nodes keep the priority of the stream they were captured from
@@ -789,6 +879,30 @@ template <typename R> class Engine : public EngineBase {
         if (last_run_ms < tbest) tbest = last_run_ms, best = fm_grid;
       }
       fm_grid = best;
+    }
+    // step form: the chain of per-pass kernels against the persistent step
+    // kernel over its grid size and stream-warp count, on whole steps
+    if (!nbig) {
+      auto whole_steps = [&]() {
+        release_graphs();
+        run(reps, last_rp, nullptr);  // warm-up of this shape (graph capture)
+        run(4 * reps, last_rp, nullptr);
+        return last_run_ms;
+      };
+      step_form = 0;
+      double tbest = whole_steps();
+      int bform = 0, bblocks = ps_blocks, bstream = ps_stream;
+      for (int blocks : {0, sms, sms / 2, sms / 4, 8})
+        for (int sw : {1, 2, 3, 4}) {
+          step_form = 1;
+          ps_blocks = blocks;
+          ps_stream = sw;
+          const double t = whole_steps();
+          if (t < tbest) tbest = t, bform = 1, bblocks = blocks, bstream = sw;
+        }
+      step_form = bform;
+      ps_blocks = bblocks;
+      ps_stream = bstream;
     }
     release_graphs();
     CK(cudaMemcpyAsync(x.p, sx.p, sizeof(double) * 3 * na, cudaMemcpyDeviceToDevice, s0));
@@ -1924,6 +2038,21 @@ int awsem_autotune(awsem_system *sys, int reps, int *chosen)
     CK(cudaSetDevice(sys->eng->device));
     sys->eng->autotune(reps, chosen);
   });
+}
+
+int awsem_set_step_form(awsem_system *sys, int form, int blocks, int stream_warps)
+{
+  if (!ready(sys)) return AWSEM_EINVAL;
+  return guarded([&] {
+    CK(cudaSetDevice(sys->eng->device));
+    sys->eng->set_step_form(form, blocks, stream_warps);
+  });
+}
+
+int awsem_get_step_form(awsem_system *sys, int *form)
+{
+  if (!ready(sys) || !form) return AWSEM_EINVAL;
+  return guarded([&] { sys->eng->get_step_form(form); });
 }
 
 int awsem_model_info(awsem_system *sys, long long *info)

@@ -58,18 +58,18 @@ __device__ __forceinline__ void red_add3(unsigned long long *p, const long long 
     if (f[c]) atomicAdd(p + c, (unsigned long long) f[c]);
 }
 
-// The warp's share of the fragment-memory term.  `pos(r, b)` returns the FP64
+// Work unit w (group g, chunk c of its separations) of the fragment-memory
+// term, records loaded into registers.  `pos(r, b)` returns the FP64
 // position of residue r's CA (b = 0) or CB (b = 1); forces go to `facc`
 // ([atom][3], atom = 3 r + b, fixed point).  Energies are added in fixed
 // point to e_acc[i * e_stride] (per residue with e_stride = 1; one total
 // with e_stride = 0).  sig[s] is the Gaussian variance of sequence
 // separation s, |s|^(2 * sigma_exp) (fix_backbone.cpp:4126).
 template <typename R, class Pos>
-__device__ __forceinline__ void fragmem_warp(const FMSlices<R> &t, const double *sig, int n, const Pos &pos,
-                                             unsigned long long *facc, unsigned long long *e_acc, int e_stride)
+__device__ __forceinline__ void fragmem_unit_reg(int w, const FMSlices<R> &t, const double *sig, int n, const Pos &pos,
+                                                 unsigned long long *facc, unsigned long long *e_acc, int e_stride)
 {
-  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-  if (w >= t.groups * t.dsplit) return;
+  const int lane = threadIdx.x & 31;
   const int g = w / t.dsplit, c = w - g * t.dsplit;
   const int d0 = c * t.nd / t.dsplit, d1 = (c + 1) * t.nd / t.dsplit;
   const int i = g * 32 + lane;
@@ -143,6 +143,15 @@ __device__ __forceinline__ void fragmem_warp(const FMSlices<R> &t, const double 
     for (int o = 16; o > 0; o >>= 1) ef += __shfl_xor_sync(0xffffffffu, ef, o);
     if (lane == 0 && ef) atomicAdd(e_acc, (unsigned long long) ef);
   }
+}
+
+// one warp per work unit
+template <typename R, class Pos>
+__device__ __forceinline__ void fragmem_warp(const FMSlices<R> &t, const double *sig, int n, const Pos &pos,
+                                             unsigned long long *facc, unsigned long long *e_acc, int e_stride)
+{
+  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (w < t.groups * t.dsplit) fragmem_unit_reg(w, t, sig, n, pos, facc, e_acc, e_stride);
 }
 
 
@@ -367,6 +376,17 @@ __device__ __forceinline__ bool fragmem_unit_bulk(int w, const FMSlices<R> &t, c
   return true;
 }
 
+// A warp's copy ring: its stage mbarriers, initialised once (the phase
+// count then runs on across the warp's units through kbase).
+__device__ __forceinline__ void fragmem_ring_init(unsigned char *wsm)
+{
+  const uint32_t bars = smem_addr(wsm);
+  if ((threadIdx.x & 31) == 0)
+    for (int s = 0; s < kFmStages; s++) mbar_init(bars + 8 * s, 1);
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  __syncwarp();
+}
+
 // The kernel body: each warp takes work units w, w + warps, ... so a grid
 // smaller than the number of units (a few blocks per SM) still streams at
 // full bandwidth and leaves the rest of each SM to the concurrent pair passes.
@@ -375,14 +395,10 @@ __device__ __forceinline__ void fragmem_warp_bulk(const FMSlices<R> &t, const do
                                                   unsigned long long *facc, unsigned long long *e_acc,
                                                   int e_stride, int *timed_out, unsigned char *wsm)
 {
-  const int lane = threadIdx.x & 31, units = t.groups * t.dsplit;
+  const int units = t.groups * t.dsplit;
   const int w0 = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
   if (w0 >= units) return;
-  const uint32_t bars = smem_addr(wsm);
-  if (lane == 0)
-    for (int s = 0; s < kFmStages; s++) mbar_init(bars + 8 * s, 1);
-  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-  __syncwarp();
+  fragmem_ring_init(wsm);
   unsigned kbase = 0;
   for (int w = w0; w < units; w += nw)
     if (!fragmem_unit_bulk(w, t, sig, n, pos, facc, e_acc, e_stride, timed_out, wsm, kbase)) return;

@@ -58,6 +58,7 @@ struct SlotRun {
 
 template <typename R> struct StepArgs {
   DevSys<R> s;
+  int n_run;  // residues the per-residue passes cover: a prefix of s.n_res (the used part of a serving handle)
   int n_atoms;
   const double *x;  // [n_atoms][3]
   double *v;
@@ -103,23 +104,37 @@ template <typename R> struct StepArgs {
 
 enum Group { G_FIX = 1, G_PAIR = 2, G_BOND = 4 };
 
+// The threads of a pass: thread t of nthr, grid-stride over the pass's items.
+// A standalone kernel gives a pass its whole grid; the persistent step
+// kernel (awsem_step.cuh) gives it the threads it reserves for the pass.
+struct Span {
+  int t, nthr;
+};
+__device__ __forceinline__ Span grid_span()
+{
+  return Span{(int) (blockIdx.x * blockDim.x + threadIdx.x), (int) (gridDim.x * blockDim.x)};
+}
+
 __device__ __forceinline__ void atomic_max_f(float *addr, float v)
 {
   // non-negative floats order like their bit patterns
   atomicMax((int *) addr, __float_as_int(v));
 }
 
-template <typename R> __global__ void k_prepare(StepArgs<R> a, FFParams p)
+template <typename R> __device__ __forceinline__ void prepare_pass(const StepArgs<R> &a, const FFParams &p, Span sp)
 {
-  int r = blockIdx.x * blockDim.x + threadIdx.x;
   float d2 = 0.f, oO = 0.f, oN = 0.f, oCA = 0.f, oAll = 0.f, oX = 0.f;
-  if (r < a.s.n_res) {
+  const int lane = threadIdx.x & 31;
+  // warp-uniform trip count: the maxima are reduced across the warp below
+  for (int r0 = sp.t - lane; r0 < a.n_run; r0 += sp.nthr) {
+  const int r = r0 + lane;
+  if (r < a.n_run) {
     unsigned long long *f = a.s.facc + (size_t) 9 * r;
     for (int k = 0; k < 9; k++) f[k] = 0ull;
     for (int k = 0; k < 5; k++) a.e_fix[(size_t) k * a.s.n_res + r] = 0;
     for (int k = 0; k < 3; k++) a.dacc[(size_t) k * a.s.n_res + r] = 0;
   }
-  if (r < a.s.n_res && a.res_sys[r] >= 0) {
+  if (r < a.n_run && a.res_sys[r] >= 0) {
     const double *x = a.x;
     int fl = a.s.res_flags[r];
     double ca[3], cb[3], o[3], n[3] = {0, 0, 0}, h[3] = {0, 0, 0}, cp[3] = {0, 0, 0};
@@ -152,23 +167,25 @@ template <typename R> __global__ void k_prepare(StepArgs<R> a, FFParams p)
       // reach of the residue's beads around its CA (excluded-volume prefilter)
       double ux = cb[0] - ca[0], uy = cb[1] - ca[1], uz = cb[2] - ca[2];
       double wx = o[0] - ca[0], wy = o[1] - ca[1], wz = o[2] - ca[2];
-      oX = (float) sqrt(fmax(ux * ux + uy * uy + uz * uz, wx * wx + wy * wy + wz * wz));
+      oX = fmaxf(oX, (float) sqrt(fmax(ux * ux + uy * uy + uz * uz, wx * wx + wy * wy + wz * wz)));
     }
     // list-validity data: contact-bead displacement and bead offsets
     const double *c = (fl & R_GLY) ? ca : cb;
     double4 b0 = a.cb_build[r];
     double dx = c[0] - b0.x, dy = c[1] - b0.y, dz = c[2] - b0.z;
-    d2 = (float) (dx * dx + dy * dy + dz * dz);
+    d2 = fmaxf(d2, (float) (dx * dx + dy * dy + dz * dz));
     auto off = [&](const double *q) {
       double ex = q[0] - c[0], ey = q[1] - c[1], ez = q[2] - c[2];
       return (float) sqrt(ex * ex + ey * ey + ez * ez);
     };
-    oO = off(o);
-    oCA = off(ca);
-    oAll = fmaxf(fmaxf(off(ca), off(cb)), off(o));
-    if (!(fl & R_FIRST)) oN = off(n);
+    oO = fmaxf(oO, off(o));
+    oCA = fmaxf(oCA, off(ca));
+    oAll = fmaxf(oAll, fmaxf(fmaxf(off(ca), off(cb)), off(o)));
+    if (!(fl & R_FIRST)) oN = fmaxf(oN, off(n));
   }
-  // block max, then one atomic per block
+  }
+  // warp max, block max, then one atomic per block and quantity (every
+  // thread of the block calls this pass)
   for (int s = 16; s > 0; s >>= 1) {
     d2 = fmaxf(d2, __shfl_xor_sync(0xffffffffu, d2, s));
     oO = fmaxf(oO, __shfl_xor_sync(0xffffffffu, oO, s));
@@ -177,22 +194,30 @@ template <typename R> __global__ void k_prepare(StepArgs<R> a, FFParams p)
     oAll = fmaxf(oAll, __shfl_xor_sync(0xffffffffu, oAll, s));
     oX = fmaxf(oX, __shfl_xor_sync(0xffffffffu, oX, s));
   }
-  if ((threadIdx.x & 31) == 0) {
-    atomic_max_f(&a.nl->d2max, d2);
-    atomic_max_f(&a.nl->bO, oO);
-    atomic_max_f(&a.nl->bN, oN);
-    atomic_max_f(&a.nl->bCA, oCA);
-    atomic_max_f(&a.nl->bAll, oAll);
-    atomic_max_f(&a.nl->bCAx, oX);
+  __shared__ float red[6][32];
+  if (lane == 0) {
+    const int w = threadIdx.x >> 5;
+    red[0][w] = d2, red[1][w] = oO, red[2][w] = oN, red[3][w] = oCA, red[4][w] = oAll, red[5][w] = oX;
+  }
+  __syncthreads();
+  if (threadIdx.x < 6) {
+    const int k = threadIdx.x;
+    float m = 0.f;
+    for (int w = 0; w < (int) (blockDim.x >> 5); w++) m = fmaxf(m, red[k][w]);
+    float *dst = k == 0 ? &a.nl->d2max : k == 1 ? &a.nl->bO : k == 2 ? &a.nl->bN : k == 3 ? &a.nl->bCA
+               : k == 4 ? &a.nl->bAll : &a.nl->bCAx;
+    if (m > 0.f) atomic_max_f(dst, m);  // the maxima start each step at 0
   }
 }
+
+template <typename R> __global__ void k_prepare(StepArgs<R> a, FFParams p) { prepare_pass(a, p, grid_span()); }
 
 // Pair-list rebuild decision.  A residue pair is needed when one of its
 // tested bead pairs is inside that term's cutoff; in contact-bead distance
 // that is at most R_need = max(r_contact, r_dssp + bO + bN, r_pap + 2 bCA,
 // r_ev + 2 bAll).  The list built at t0 with radius R_need(t0) + skin stays
 // complete while R_need(t) + 2 * max displacement <= radius.
-__global__ void k_nl_decide(NLState *nl, int force, long long *step)
+__device__ __forceinline__ void nl_decide(NLState *nl, int force, long long *step)
 {
   if (step) (*step)++;
   NLState &s = *nl;
@@ -215,6 +240,8 @@ __global__ void k_nl_decide(NLState *nl, int force, long long *step)
   s.d2max = s.bO = s.bN = s.bCA = s.bAll = s.bCAx = 0.f;
   s.n_dssp = s.n_pap = 0;
 }
+
+__global__ void k_nl_decide(NLState *nl, int force, long long *step) { nl_decide(nl, force, step); }
 
 template <typename R> __device__ __forceinline__ V3<double> contact(const DevSys<R> &s, int r)
 {
@@ -440,30 +467,35 @@ template <typename R> __device__ __forceinline__ void nl_build_one(const StepArg
 
 // a fixed grid of warps loops over the residues, so the launch costs little
 // on the steps that do not rebuild
+template <typename R>
+__device__ __forceinline__ void nl_build_pass(const StepArgs<R> &a, const GridArgs &g, int n_launch, Span sp)
+{
+  const int lane = threadIdx.x & 31;
+  for (int i = sp.t >> 5; i < n_launch; i += sp.nthr >> 5) nl_build_one(a, g, i, lane);
+}
+
 template <typename R> __global__ void k_nl_build(StepArgs<R> a, GridArgs g, int n_launch)
 {
   if (!a.nl->rebuild) return;
-  const int lane = threadIdx.x & 31;
-  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n_launch; i += (gridDim.x * blockDim.x) >> 5)
-    nl_build_one(a, g, i, lane);
+  nl_build_pass(a, g, n_launch, grid_span());
 }
 
 // Pairs of the list, grid-stride (the count is known only on the device)
-#define FOR_EACH_PAIR(a, p) \
-  for (int p = blockIdx.x * blockDim.x + threadIdx.x, np_ = min((a).nl->npairs, (a).pcap); p < np_; p += gridDim.x * blockDim.x)
+#define FOR_EACH_PAIR(a, p, sp) \
+  for (int p = (sp).t, np_ = min((a).nl->npairs, (a).pcap); p < np_; p += (sp).nthr)
 
 // DL1: local densities of contact beads (fix_backbone.cpp:7728-7791).  FP64
 // in both forms: the densities feed the burial and switching functions, and
 // the well selection is then the reference's exactly.  Sums in 2^-40 fixed
 // point (dacc[0], dacc[1]).
-template <typename R> __global__ void k_density(StepArgs<R> a, FFParams p)
+template <typename R> __device__ __forceinline__ void density_pass(const StepArgs<R> &a, const FFParams &p, Span sp)
 {
   const DevSys<R> &s = a.s;
   const int n = s.n_res;
   if (!(a.groups & G_FIX)) return;
   const bool water = p.terms & T_WATER, helix = p.terms & T_HELIX;
   unsigned long long *aw = (unsigned long long *) a.dacc, *ah = aw + n;
-  FOR_EACH_PAIR(a, q)
+  FOR_EACH_PAIR(a, q, sp)
   {
     const int2 ij = a.pairs[q];
     const int i = ij.x, j = ij.y;
@@ -485,6 +517,8 @@ template <typename R> __global__ void k_density(StepArgs<R> a, FFParams p)
     }
   }
 }
+
+template <typename R> __global__ void k_density(StepArgs<R> a, FFParams p) { density_pass(a, p, grid_span()); }
 
 // density sums -> values: k = 0 water density, 1 helix density
 template <typename R> __device__ __forceinline__ double density(const StepArgs<R> &a, int k, int r)
@@ -534,7 +568,7 @@ template <typename R> __device__ __forceinline__ void bonds_of(const StepArgs<R>
     R dr = rr - R(a.bond_r0[b]);
     R rk = R(a.bond_k[b]) * dr;
     R fb = rr > R(0) ? R(-2) * rk / rr : R(0);
-    e += (double) (rk * dr);
+    e = __dadd_rn(e, (double) mul_rn(rk, dr));
     scatter(s, ai / 3, ai % 3, d.x * fb, d.y * fb, d.z * fb);
     scatter(s, aj / 3, aj % 3, -d.x * fb, -d.y * fb, -d.z * fb);
   }
@@ -542,11 +576,9 @@ template <typename R> __device__ __forceinline__ void bonds_of(const StepArgs<R>
 }
 
 // SL and the per-residue backbone terms
-template <typename R> __global__ void k_residue(StepArgs<R> a, FFParams p)
+template <typename R> __device__ __forceinline__ void residue_one(const StepArgs<R> &a, const FFParams &p, int i)
 {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
   const DevSys<R> &s = a.s;
-  if (i >= s.n_res || a.res_sys[i] < 0) return;
   // the per-residue backbone terms (chain, chi, rama, helical pair) are a
   // small share of the work and some are sums of steep Gaussians: FP64 in
   // both forms
@@ -623,16 +655,24 @@ template <typename R> __global__ void k_residue(StepArgs<R> a, FFParams p)
   if (a.groups & G_BOND) bonds_of(a, i);
 }
 
+template <typename R> __device__ __forceinline__ void residue_pass(const StepArgs<R> &a, const FFParams &p, Span sp)
+{
+  for (int i = sp.t; i < a.n_run; i += sp.nthr)
+    if (a.res_sys[i] >= 0) residue_one(a, p, i);
+}
+
+template <typename R> __global__ void k_residue(StepArgs<R> a, FFParams p) { residue_pass(a, p, grid_span()); }
+
 // DL2: water-mediated density derivative coefficients (fix_backbone.cpp:
 // 7877-7954): raw sums in dacc[2] (2^-40 fixed point); xi_water(i) is that
 // sum times sigma_water'(i) (water_xi below).
-template <typename R> __global__ void k_water_xi(StepArgs<R> a, FFParams p)
+template <typename R> __device__ __forceinline__ void water_xi_pass(const StepArgs<R> &a, const FFParams &p, Span sp)
 {
   const DevSys<R> &s = a.s;
   if (!(p.terms & T_WATER) || !(a.groups & G_FIX)) return;
   unsigned long long *acc = (unsigned long long *) a.dacc + (size_t) 2 * s.n_res;
   const double *WG = s.tables + TB_WATER;
-  FOR_EACH_PAIR(a, q)
+  FOR_EACH_PAIR(a, q, sp)
   {
     const int2 ij = a.pairs[q];
     const int i = ij.x, j = ij.y;
@@ -655,6 +695,8 @@ template <typename R> __global__ void k_water_xi(StepArgs<R> a, FFParams p)
   }
 }
 
+template <typename R> __global__ void k_water_xi(StepArgs<R> a, FFParams p) { water_xi_pass(a, p, grid_span()); }
+
 template <typename R> __device__ __forceinline__ double water_xi(const StepArgs<R> &a, int r)
 {
   return (double) a.dacc[(size_t) 2 * a.s.n_res + r] * D_UNSCALE * a.sigp_w[r];
@@ -673,7 +715,7 @@ template <typename R> __device__ __forceinline__ void scatter_fix(const DevSys<R
 // and excluded volume are applied to both residues.  DSSP and P_AP pairs are
 // only detected here (cheap distance and index tests) and queued: k_hbond
 // evaluates them, so their long, branchy bodies do not slow this pass.
-template <typename R> __global__ void __launch_bounds__(128, 6) k_pair(StepArgs<R> a, FFParams p)
+template <typename R> __device__ __forceinline__ void pair_pass(const StepArgs<R> &a, const FFParams &p, Span sp)
 {
   const DevSys<R> &s = a.s;
   const int n = s.n_res;
@@ -692,7 +734,7 @@ template <typename R> __global__ void __launch_bounds__(128, 6) k_pair(StepArgs<
   unsigned long long *e_ev = (unsigned long long *) a.e_fix + (size_t) 4 * n;
   const int lane = threadIdx.x & 31, np = min(a.nl->npairs, a.pcap);
   // warp-uniform trip count: the queue appends below are warp collectives
-  for (int base = blockIdx.x * blockDim.x + threadIdx.x - lane; base < np; base += gridDim.x * blockDim.x) {
+  for (int base = sp.t - lane; base < np; base += sp.nthr) {
     const int q = base + lane;
     bool q_d0 = false, q_d1 = false, q_p = false;  // queue: DSSP O(i), DSSP O(j), P_AP
     if (q < np) {
@@ -731,17 +773,17 @@ template <typename R> __global__ void __launch_bounds__(128, 6) k_pair(StepArgs<
               well_theta(r, R(p.w_rmin_th[w]), R(p.w_rmax_th[w]), R(p.water_kappa), R(p.well_rmin[w]),
                          R(p.well_rmax[w]), th, pr);
             }
-            ew += -sg * (double) th;
-            force += R(sg) * pr;
+            ew = madd(-sg, (double) th, ew);
+            force = madd(R(sg), pr, force);
           }
         }
         if (in0) {
           const double xi_i = water_xi(a, i), xi_j = water_xi(a, j);
-          if (fabs(xi_i) > 1e-8) force += pr0 * R(xi_i);
-          if (fabs(xi_j) > 1e-8) force += pr0 * R(xi_j);
+          if (fabs(xi_i) > 1e-8) force = madd(pr0, R(xi_i), force);
+          if (fabs(xi_j) > 1e-8) force = madd(pr0, R(xi_j), force);
         }
       }
-      if ((T & T_BURIAL) && in0) force += R(a.bur[i] + a.bur[j]) * pr0;
+      if ((T & T_BURIAL) && in0) force = madd(R(a.bur[i] + a.bur[j]), pr0, force);
       if ((T & T_HELIX) && rsq > R(p.h_rmin_sq) && rsq < R(p.h_rmax_sq)) {
         double fac = a.xi1[i] + a.xi1[j];
         if (i - dh >= 0) fac += a.xi2[i - dh];
@@ -749,7 +791,7 @@ template <typename R> __global__ void __launch_bounds__(128, 6) k_pair(StepArgs<
         if (fabs(fac) > 1e-6) {
           R th, pr;
           well_theta(r, R(p.h_rmin_th), R(p.h_rmax_th), R(p.helix_kappa), R(p.helix_rmin), R(p.helix_rmax), th, pr);
-          force += -R(fac) * pr;
+          force = madd(-R(fac), pr, force);
         }
       }
       if (ew != 0.0) atomicAdd(e_water + i, (unsigned long long) fix_force(ew));
@@ -826,16 +868,21 @@ template <typename R> __global__ void __launch_bounds__(128, 6) k_pair(StepArgs<
   }
 }
 
+template <typename R> __global__ void __launch_bounds__(128, 6) k_pair(StepArgs<R> a, FFParams p)
+{
+  pair_pass(a, p, grid_span());
+}
+
 // DSSP hydrogen bonds and P_AP of the queued pairs, one thread per entry
 // (grid-stride over both queues).  A DSSP entry q >= 0 is pair q with O(i)
 // as acceptor; ~q is the same pair with O(j).  Forces scatter with
 // fixed-point atomics; each pair's energy goes to its acceptor (DSSP) or
 // lower residue (P_AP) in fixed point, so sums do not depend on the order.
-template <typename R> __global__ void __launch_bounds__(128) k_hbond(StepArgs<R> a, FFParams p)
+template <typename R> __device__ __forceinline__ void hbond_pass(const StepArgs<R> &a, const FFParams &p, Span sp)
 {
   const DevSys<R> &s = a.s;
   const int nd = a.nl->n_dssp, np = a.nl->n_pap, n = s.n_res;
-  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nd + np; t += gridDim.x * blockDim.x) {
+  for (int t = sp.t; t < nd + np; t += sp.nthr) {
     const bool d = t < nd;
     const int q = d ? a.hbq[t] : a.hbq[(size_t) 2 * a.pcap + (t - nd)];
     const int2 ij = a.pairs[q < 0 ? ~q : q];
@@ -844,6 +891,11 @@ template <typename R> __global__ void __launch_bounds__(128) k_hbond(StepArgs<R>
     if (e != R(0))
       atomicAdd((unsigned long long *) (a.e_fix + (d ? 0 : (size_t) n) + i), (unsigned long long) fix_force((double) e));
   }
+}
+
+template <typename R> __global__ void __launch_bounds__(128) k_hbond(StepArgs<R> a, FFParams p)
+{
+  hbond_pass(a, p, grid_span());
 }
 
 // Fragment memory: sliced lane-interleaved table, lane per residue row
@@ -893,24 +945,23 @@ struct Integrator {
 // replica follows its own run window (SlotRun); outside it the replica is
 // frozen, and residues of no replica are skipped.
 template <typename R>
-__global__ void k_finish(StepArgs<R> a, const Integrator *inp, const double *g1, const double *g2, double *ftot,
-                         double *x_out)
+__device__ __forceinline__ void finish_one(const StepArgs<R> &a, const Integrator &in, long long step, const double *g1,
+                                           const double *g2, double *ftot, double *x_out, int r)
 {
-  int r = blockIdx.x * blockDim.x + threadIdx.x;
-  if (r >= a.s.n_res) return;
   const int rep = a.res_sys[r];
   if (rep < 0) return;
-  const Integrator in = *inp;
   const SlotRun sr = a.slot_run[rep];
-  const long long step = *a.step;
   if (step < sr.begin || step > sr.end) return;
   const bool final_kick = step > sr.begin, next = step < sr.end;
   const unsigned long long seed = a.sys_seed[rep];
   const long long key = step - sr.step0;  // the replica's own step count keys its noise
+  // Every multiply and add below is rounded on its own (no contraction), as
+  // the x86-64 CPU build computes fix langevin / fix nve, and identically in
+  // every kernel that inlines this.
   double tsqrt = 0.0;
   if (in.langevin) {
     double delta = sr.end != sr.begin ? (double) (step - sr.begin) / (double) (sr.end - sr.begin) : 0.0;
-    tsqrt = sqrt(sr.t_start + delta * (sr.t_stop - sr.t_start));
+    tsqrt = sqrt(__dadd_rn(sr.t_start, __dmul_rn(delta, __dsub_rn(sr.t_stop, sr.t_start))));
   }
   double ke = 0.0;
   for (int b = 0; b < 3; b++) {
@@ -921,19 +972,38 @@ __global__ void k_finish(StepArgs<R> a, const Integrator *inp, const double *g1,
     for (int c = 0; c < 3; c++) {
       double f = (double) (long long) fa[c] * F_UNSCALE;
       double v = a.v[3 * at + c];
-      if (in.langevin) f += g1[at] * v + g2[at] * tsqrt * (uniform01(seed, key, a.atom_tag[at], c) - 0.5);
+      if (in.langevin)
+        f = __dadd_rn(f, __dadd_rn(__dmul_rn(g1[at], v),
+                                   __dmul_rn(__dmul_rn(g2[at], tsqrt),
+                                             __dsub_rn(uniform01(seed, key, a.atom_tag[at], c), 0.5))));
       if (ftot) ftot[3 * at + c] = f;
-      if (final_kick) v += dtfm * f;
-      ke += m * v * v;
+      if (final_kick) v = __dadd_rn(v, __dmul_rn(dtfm, f));
+      ke = __dadd_rn(ke, __dmul_rn(__dmul_rn(m, v), v));
       if (next) {
-        v += dtfm * f;
-        x_out[3 * at + c] += in.dt * v;
+        v = __dadd_rn(v, __dmul_rn(dtfm, f));
+        x_out[3 * at + c] = __dadd_rn(x_out[3 * at + c], __dmul_rn(in.dt, v));
       }
       a.v[3 * at + c] = v;
     }
   }
   // kinetic energy after the final half kick (thermo output of the step)
   a.e_res[(size_t) E_KIN * a.s.n_res + r] = 0.5 * 48.88821291 * 48.88821291 * ke;
+}
+
+template <typename R>
+__device__ __forceinline__ void finish_pass(const StepArgs<R> &a, const Integrator *inp, const double *g1,
+                                            const double *g2, double *ftot, double *x_out, Span sp)
+{
+  const Integrator in = *inp;
+  const long long step = *a.step;
+  for (int r = sp.t; r < a.n_run; r += sp.nthr) finish_one(a, in, step, g1, g2, ftot, x_out, r);
+}
+
+template <typename R>
+__global__ void k_finish(StepArgs<R> a, const Integrator *inp, const double *g1, const double *g2, double *ftot,
+                         double *x_out)
+{
+  finish_pass(a, inp, g1, g2, ftot, x_out, grid_span());
 }
 
 // Caller-order staging <-> internal order: out[a] = in[perm[a]] / out[perm[a]] = in[a]

@@ -110,6 +110,8 @@ def load_library(path: str = LIB_PATH):
     lib.awsem_kernel_name.restype = cp
     lib.awsem_profile_step.argtypes = [vp, ip, vp]
     lib.awsem_autotune.argtypes = [vp, ip, vp]
+    lib.awsem_set_step_form.argtypes = [vp, ip, ip, ip]
+    lib.awsem_get_step_form.argtypes = [vp, vp]
     lib.awsem_model_info.argtypes = [vp, vp]
     lib.awsem_batch_create.argtypes = [ip, ip, C.POINTER(vp)]
     lib.awsem_batch_add_files.argtypes = [vp, cp, cp, cp, cp, cp, cp, C.c_ulonglong, C.POINTER(ip)]
@@ -242,11 +244,24 @@ class AwsemSystem:
         return {self.lib.awsem_kernel_name(k).decode(): float(ms[k]) for k in range(NKERNELS)}
 
     def autotune(self, reps: int = 5) -> dict:
-        """Pick the fastest launch shapes on this system (awsem_autotune)."""
+        """Pick the fastest launch shapes and step form on this system (awsem_autotune)."""
         got = np.zeros(4, dtype=np.int32)
         _check(self.lib, self.lib.awsem_autotune(self.h, int(reps), _ptr(got)), "awsem_autotune")
         return {"fragmem_separations_per_warp": int(got[0]), "pair_pass_blocks": int(got[1]),
-                "hbond_blocks": int(got[2]), "fragmem_blocks": int(got[3])}
+                "hbond_blocks": int(got[2]), "fragmem_blocks": int(got[3]), **self.step_form()}
+
+    def set_step_form(self, form: str, blocks: int = 0, stream_warps: int = 2) -> None:
+        """'kernels': each MD step a graph of per-pass kernels; 'persistent':
+        one cooperative launch per step (awsem_set_step_form)."""
+        f = {"kernels": 0, "persistent": 1}[form]
+        _check(self.lib, self.lib.awsem_set_step_form(self.h, f, int(blocks), int(stream_warps)),
+               "awsem_set_step_form")
+
+    def step_form(self) -> dict:
+        got = np.zeros(3, dtype=np.int32)
+        _check(self.lib, self.lib.awsem_get_step_form(self.h, _ptr(got)), "awsem_get_step_form")
+        return {"step_form": "persistent" if got[0] else "kernels", "persistent_blocks": int(got[1]),
+                "stream_warps": int(got[2])}
 
     def model_info(self) -> np.ndarray:
         info = np.zeros(8, dtype=np.int64)
@@ -431,6 +446,10 @@ class AwsemServer:
         _check(self.lib, self.lib.awsem_server_collect(self.h, slot, _ptr(x), _ptr(v), _ptr(e)),
                "awsem_server_collect")
         return x, v, e
+
+    # step form of `advance` (awsem_set_step_form), as on the batch handles
+    set_step_form = AwsemSystem.set_step_form
+    step_form = AwsemSystem.step_form
 
     def usage(self) -> dict:
         info = np.zeros(8, dtype=np.int64)

@@ -210,11 +210,34 @@ int awsem_profile_step(awsem_system *sys, int reps, double *ms);
  * counter are restored afterwards; results do not depend on the shapes (all
  * sums are exact).  The grid of the fragment-memory kernel (1 to 4 blocks
  * per SM looping over the work, or one warp per unit) is judged on whole
- * steps, since that kernel overlaps the pair passes.  chosen (may be NULL):
- * [separations per warp, pair-pass blocks, hydrogen-bond blocks,
- * fragment-memory blocks (0: one warp per unit)].  Not available on serving
+ * steps, since that kernel overlaps the pair passes.  Last, the step form
+ * (awsem_set_step_form) is chosen on whole steps: the chain of per-pass
+ * kernels with those shapes against the persistent step kernel at several
+ * grid sizes and stream-warp counts (handles without cell-grid replicas).
+ * chosen (may be NULL): [separations per warp, pair-pass blocks,
+ * hydrogen-bond blocks, fragment-memory blocks (0: one warp per unit)]; the
+ * step form is read with awsem_get_step_form.  Not available on serving
  * handles. */
 int awsem_autotune(awsem_system *sys, int reps, int *chosen);
+
+/* Step form of awsem_run / awsem_server_advance (no counterpart in the
+ * reference, which evaluates on the CPU inside LAMMPS's pre_force hook).
+ * form 0: each MD step is a chain of per-pass kernels (prepare, list
+ * decision and build, density, residue, water_xi, pair, hbond, fragment
+ * memory on a second stream, finish), captured in a CUDA graph.  form 1: each
+ * MD step is ONE cooperative launch of a persistent kernel whose blocks pass
+ * through the same passes separated by grid barriers; `stream_warps` (1..7)
+ * of each block's 8 warps stream fragment-memory units concurrently with the
+ * pair passes.  `blocks` is the persistent grid (0: every block that fits on
+ * the device).  Results are identical bit for bit in both forms (all sums
+ * are exact fixed point).  Form 1 is refused (AWSEM_EINVAL) on handles with a
+ * replica above 2,048 residues (those build cell grids).  A barrier wait that
+ * gives up (about one second) makes the call fail with AWSEM_ESTATE. */
+int awsem_set_step_form(awsem_system *sys, int form, int blocks, int stream_warps);
+
+/* form[3] = {form, persistent grid (blocks; 0 until first used when set to
+ * "all that fit"), stream warps per block}. */
+int awsem_get_step_form(awsem_system *sys, int *form);
 
 /* Sizes behind the roofline's algorithmic-byte counts:
  * info[0] residues, [1] atoms, [2] fragment-memory records (4 distances

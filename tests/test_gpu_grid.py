@@ -10,7 +10,7 @@ pytestmark = pytest.mark.gpu
 def test_grid_list_matches_oracle(tmp_path, gpu_lib, oracle_built):
     import ref
     from awsemmd_b200 import synth
-    from awsemmd_b200.engine import AwsemBatch
+    from awsemmd_b200.engine import AwsemBatch, AwsemError
 
     c = synth.packed_arrays([250] * 9, 150.0, 77, n_mem_per_window=1)
     assert c["n_res"] > 2048
@@ -19,6 +19,9 @@ def test_grid_list_matches_oracle(tmp_path, gpu_lib, oracle_built):
     o = ref.OracleSystem(files)
     x0 = c["x"].reshape(-1, 3)
     with AwsemBatch.from_arrays(ff, [c], precision="fp64", seeds=[3]) as b:
+        # the persistent step kernel builds no cell grids: refused on such handles
+        with pytest.raises(AwsemError):
+            b.set_step_form("persistent")
         for stage in range(2):
             x, _ = b.get_state(0)
             f, e = b.compute(x, step=b.step)
