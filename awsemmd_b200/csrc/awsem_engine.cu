@@ -110,6 +110,7 @@ class EngineBase {
   virtual void profile(int reps, double *ms) = 0;
   virtual void autotune(int reps, int *chosen) = 0;
   virtual void set_step_form(int form, int blocks, int stream_warps) = 0;
+  virtual void set_launch_shapes(const int *shapes) = 0;
   virtual void get_step_form(int *out) = 0;
   virtual void model_info(long long *info) = 0;
   virtual double run_ms() const = 0;
@@ -757,6 +758,21 @@ template <typename R> class Engine : public EngineBase {
     step_form = form;
     ps_blocks = blocks;
     ps_stream = stream_warps;
+    release_graphs();
+  }
+
+  // shapes as awsem_autotune reports them: [dsplit, pair blocks, hbond blocks, fragmem blocks]
+  void set_launch_shapes(const int *sh) override
+  {
+    const int nd = std::max(in.ff.p.fm_nd, 1);
+    if (sh[0] < 1 || sh[0] > nd)
+      throw std::invalid_argument("separations per fragment-memory warp must be in 1.." + std::to_string(nd));
+    if (sh[1] < 1 || sh[2] < 1) throw std::invalid_argument("pair and hydrogen-bond grids must be >= 1 block");
+    if (sh[3] < 0) throw std::invalid_argument("fragment-memory grid must be >= 0 (0: one warp per unit)");
+    fm_dsplit = sh[0];
+    pair_blocks = sh[1];
+    hb_blocks = sh[2];
+    fm_grid = sh[3];
     release_graphs();
   }
 
@@ -2047,6 +2063,12 @@ int awsem_set_step_form(awsem_system *sys, int form, int blocks, int stream_warp
     CK(cudaSetDevice(sys->eng->device));
     sys->eng->set_step_form(form, blocks, stream_warps);
   });
+}
+
+int awsem_set_launch_shapes(awsem_system *sys, const int *shapes)
+{
+  if (!ready(sys) || !shapes) return AWSEM_EINVAL;
+  return guarded([&] { sys->eng->set_launch_shapes(shapes); });
 }
 
 int awsem_get_step_form(awsem_system *sys, int *form)

@@ -58,6 +58,37 @@ __device__ __forceinline__ void red_add3(unsigned long long *p, const long long 
     if (f[c]) atomicAdd(p + c, (unsigned long long) f[c]);
 }
 
+// Per-record arithmetic, shared by both load paths (so they agree bit for
+// bit).  The Gaussian of a row with variance s^2 is exp(-dr^2 / (2 s^2)):
+// FP32 evaluates it as 2^(k2 dr^2) with k2 = -log2(e) / (2 s^2) on the ex2
+// unit, FP64 as exp(k2 dr^2) with k2 = -1 / (2 s^2).
+__device__ __forceinline__ float fm_gauss(float x)
+{
+  float y;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ double fm_gauss(double x) { return exp(x); }
+__device__ __forceinline__ float fm_k2(float s2) { return -1.4426950408889634f / (2.f * s2); }
+__device__ __forceinline__ double fm_k2(double s2) { return -1.0 / (2.0 * s2); }
+
+// One record's four Gaussians g_k (times the record's coefficient when the
+// coefficients are not uniform): es += sum g_k, fs_k += g_k dr_k.  The row's
+// energy and radial force sums are scale * es and scale * fs_k, with scale =
+// -coefficient (uniform) or -1.
+template <bool COEF, typename R>
+__device__ __forceinline__ void fm_record(const R rec[4], R cc, const R r[4], R k2, R &es, R fs[4])
+{
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    const R dr = r[k] - rec[k];
+    R g = fm_gauss(dr * dr * k2);
+    if (COEF) g = g * cc;
+    es = es + g;
+    fs[k] = madd(g, dr, fs[k]);
+  }
+}
+
 // Work unit w (group g, chunk c of its separations) of the fragment-memory
 // term, records loaded into registers.  `pos(r, b)` returns the FP64
 // position of residue r's CA (b = 0) or CB (b = 1); forces go to `facc`
@@ -65,9 +96,10 @@ __device__ __forceinline__ void red_add3(unsigned long long *p, const long long 
 // point to e_acc[i * e_stride] (per residue with e_stride = 1; one total
 // with e_stride = 0).  sig[s] is the Gaussian variance of sequence
 // separation s, |s|^(2 * sigma_exp) (fix_backbone.cpp:4126).
-template <typename R, class Pos>
-__device__ __forceinline__ void fragmem_unit_reg(int w, const FMSlices<R> &t, const double *sig, int n, const Pos &pos,
-                                                 unsigned long long *facc, unsigned long long *e_acc, int e_stride)
+template <bool COEF, typename R, class Pos>
+__device__ __forceinline__ void fragmem_unit_reg_t(int w, const FMSlices<R> &t, const double *sig, int n,
+                                                   const Pos &pos, unsigned long long *facc,
+                                                   unsigned long long *e_acc, int e_stride)
 {
   const int lane = threadIdx.x & 31;
   const int g = w / t.dsplit, c = w - g * t.dsplit;
@@ -78,7 +110,7 @@ __device__ __forceinline__ void fragmem_unit_reg(int w, const FMSlices<R> &t, co
   const V3<double> ca_i = pos(ii, 0), cb_i = pos(ii, 1);
   long long fca[3] = {0, 0, 0}, fcb[3] = {0, 0, 0};
   double e = 0.0;
-  const R cu = R(t.uniform);
+  const R scale = COEF ? R(-1) : -R(t.uniform);
   for (int d = d0; d < d1; d++) {
     const int blk = g * t.nd + d;
     const int len = t.slen[blk];
@@ -92,28 +124,21 @@ __device__ __forceinline__ void fragmem_unit_reg(int w, const FMSlices<R> &t, co
 #pragma unroll
     for (int k = 0; k < 4; k++) r[k] = m_sqrt(norm2(dv[k]));
     const R s2 = R(sig[t.min_sep + d]);
-    const R inv2s = R(1) / (R(2) * s2);
+    const R k2 = fm_k2(s2);
     R es = 0, fs[4] = {0, 0, 0, 0};
 #pragma unroll 4
     for (int m = 0; m < len; m++) {
       const size_t at = base + (size_t) m * 32;
       R rec[4];
       load_record(t.rf, at, rec);
-      const R cc = t.coef ? t.coef[at] : cu;
-#pragma unroll
-      for (int k = 0; k < 4; k++) {
-        const R dr = r[k] - rec[k];
-        const R gk = cc * m_fastexp(-dr * dr * inv2s);
-        es -= gk;
-        fs[k] -= gk * dr;
-      }
+      fm_record<COEF>(rec, COEF ? t.coef[at] : R(1), r, k2, es, fs);
     }
-    e += (double) es;
+    e += (double) (scale * es);
     // atom pair k acts on CA(i) (k < 2) or CB(i), and on CA(j) (k even) or CB(j)
     long long fja[3] = {0, 0, 0}, fjb[3] = {0, 0, 0};
 #pragma unroll
     for (int k = 0; k < 4; k++) {
-      const R fc = fs[k] != R(0) ? fs[k] / (s2 * r[k]) : R(0);
+      const R fc = fs[k] != R(0) ? (scale * fs[k]) / (s2 * r[k]) : R(0);
       const long long v[3] = {fix_force((double) (fc * dv[k].x)), fix_force((double) (fc * dv[k].y)),
                               fix_force((double) (fc * dv[k].z))};
 #pragma unroll
@@ -143,6 +168,16 @@ __device__ __forceinline__ void fragmem_unit_reg(int w, const FMSlices<R> &t, co
     for (int o = 16; o > 0; o >>= 1) ef += __shfl_xor_sync(0xffffffffu, ef, o);
     if (lane == 0 && ef) atomicAdd(e_acc, (unsigned long long) ef);
   }
+}
+
+template <typename R, class Pos>
+__device__ __forceinline__ void fragmem_unit_reg(int w, const FMSlices<R> &t, const double *sig, int n, const Pos &pos,
+                                                 unsigned long long *facc, unsigned long long *e_acc, int e_stride)
+{
+  if (t.coef)
+    fragmem_unit_reg_t<true>(w, t, sig, n, pos, facc, e_acc, e_stride);
+  else
+    fragmem_unit_reg_t<false>(w, t, sig, n, pos, facc, e_acc, e_stride);
 }
 
 // one warp per work unit
@@ -231,11 +266,11 @@ __device__ __forceinline__ void load_record_shared(const double *rf, int rec, do
 // mbarriers keep counting phases across its units: chunk k of this unit is
 // the warp's chunk kbase + k (stage (kbase + k) % kFmStages).  Returns false
 // when a wait gave up.
-template <typename R, class Pos>
-__device__ __forceinline__ bool fragmem_unit_bulk(int w, const FMSlices<R> &t, const double *sig, int n,
-                                                  const Pos &pos, unsigned long long *facc,
-                                                  unsigned long long *e_acc, int e_stride, int *timed_out,
-                                                  unsigned char *wsm, unsigned &kbase)
+template <bool COEF, typename R, class Pos>
+__device__ __forceinline__ bool fragmem_unit_bulk_t(int w, const FMSlices<R> &t, const double *sig, int n,
+                                                    const Pos &pos, unsigned long long *facc,
+                                                    unsigned long long *e_acc, int e_stride, int *timed_out,
+                                                    unsigned char *wsm, unsigned &kbase)
 {
   const int lane = threadIdx.x & 31;
   const int g = w / t.dsplit, c = w - g * t.dsplit;
@@ -243,7 +278,7 @@ __device__ __forceinline__ bool fragmem_unit_bulk(int w, const FMSlices<R> &t, c
   const int i = g * 32 + lane;
   const bool live = i < n;
   const int ii = live ? i : n - 1;
-  const bool coef = t.coef != nullptr;
+  const bool coef = COEF;
   const int stage_bytes = fm_stage_bytes<R>(coef);
   const uint32_t bars = smem_addr(wsm), data = bars + 128;
   // the warp's run of stripes: its non-empty blocks, contiguous from the first
@@ -271,11 +306,11 @@ __device__ __forceinline__ bool fragmem_unit_bulk(int w, const FMSlices<R> &t, c
   const V3<double> ca_i = pos(ii, 0), cb_i = pos(ii, 1);
   long long fca[3] = {0, 0, 0}, fcb[3] = {0, 0, 0};
   double e = 0.0;
-  const R cu = R(t.uniform);
+  const R scale = COEF ? R(-1) : -R(t.uniform);
   // current row (block d): geometry and sums
   int d = d0, blk_end = 0, j = 0;
   V3<R> dv[4];
-  R r[4], s2 = 1, inv2s = 1, es = 0, fs[4] = {0, 0, 0, 0};
+  R r[4], s2 = 1, k2 = -1, es = 0, fs[4] = {0, 0, 0, 0};
   auto begin_row = [&]() {  // d: the next non-empty block at or after d
     while (d < d1 && t.slen[g * t.nd + d] == 0) d++;
     if (d >= d1) return;
@@ -289,17 +324,17 @@ __device__ __forceinline__ bool fragmem_unit_bulk(int w, const FMSlices<R> &t, c
 #pragma unroll
     for (int k = 0; k < 4; k++) r[k] = m_sqrt(norm2(dv[k]));
     s2 = R(sig[t.min_sep + d]);
-    inv2s = R(1) / (R(2) * s2);
+    k2 = fm_k2(s2);
     es = 0;
 #pragma unroll
     for (int k = 0; k < 4; k++) fs[k] = 0;
   };
   auto end_row = [&]() {
-    e += (double) es;
+    e += (double) (scale * es);
     long long fja[3] = {0, 0, 0}, fjb[3] = {0, 0, 0};
 #pragma unroll
     for (int k = 0; k < 4; k++) {
-      const R fc = fs[k] != R(0) ? fs[k] / (s2 * r[k]) : R(0);
+      const R fc = fs[k] != R(0) ? (scale * fs[k]) / (s2 * r[k]) : R(0);
       const long long v[3] = {fix_force((double) (fc * dv[k].x)), fix_force((double) (fc * dv[k].y)),
                               fix_force((double) (fc * dv[k].z))};
 #pragma unroll
@@ -332,21 +367,18 @@ __device__ __forceinline__ bool fragmem_unit_bulk(int w, const FMSlices<R> &t, c
     const R *srf = reinterpret_cast<const R *>(sd);
     const R *scf = reinterpret_cast<const R *>(sd + kFmStripes * 32 * 4 * sizeof(R));
     const int s0 = k * kFmStripes, ns = min(kFmStripes, total - s0);
-    for (int q = 0; q < ns; q++) {
-      const int s = s0 + q;
-      while (s >= blk_end && d < d1) {  // rows end on stripe boundaries
+    for (int q = 0; q < ns;) {
+      while (s0 + q >= blk_end && d < d1) {  // rows end on stripe boundaries
         end_row();
         begin_row();
       }
-      R rec[4];
-      load_record_shared(srf, q * 32 + lane, rec);
-      const R cc = coef ? scf[q * 32 + lane] : cu;
-#pragma unroll
-      for (int kk = 0; kk < 4; kk++) {
-        const R dr = r[kk] - rec[kk];
-        const R gk = cc * m_fastexp(-dr * dr * inv2s);
-        es -= gk;
-        fs[kk] -= gk * dr;
+      // the stripes of this chunk that belong to the current row (at least one)
+      const int run = max(q + 1, min(ns, blk_end - s0));
+#pragma unroll(sizeof(R) == 4 ? 2 : 1)
+      for (; q < run; q++) {
+        R rec[4];
+        load_record_shared(srf, q * 32 + lane, rec);
+        fm_record<COEF>(rec, COEF ? scf[q * 32 + lane] : R(1), r, k2, es, fs);
       }
     }
     __syncwarp();  // every lane has read the stage
@@ -374,6 +406,16 @@ __device__ __forceinline__ bool fragmem_unit_bulk(int w, const FMSlices<R> &t, c
     if (lane == 0 && ef) atomicAdd(e_acc, (unsigned long long) ef);
   }
   return true;
+}
+
+template <typename R, class Pos>
+__device__ __forceinline__ bool fragmem_unit_bulk(int w, const FMSlices<R> &t, const double *sig, int n,
+                                                  const Pos &pos, unsigned long long *facc,
+                                                  unsigned long long *e_acc, int e_stride, int *timed_out,
+                                                  unsigned char *wsm, unsigned &kbase)
+{
+  return t.coef ? fragmem_unit_bulk_t<true>(w, t, sig, n, pos, facc, e_acc, e_stride, timed_out, wsm, kbase)
+                : fragmem_unit_bulk_t<false>(w, t, sig, n, pos, facc, e_acc, e_stride, timed_out, wsm, kbase);
 }
 
 // A warp's copy ring: its stage mbarriers, initialised once (the phase

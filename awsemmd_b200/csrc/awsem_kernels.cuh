@@ -733,6 +733,26 @@ template <typename R> __device__ __forceinline__ void pair_pass(const StepArgs<R
   unsigned long long *e_water = (unsigned long long *) a.e_fix + (size_t) 3 * n;
   unsigned long long *e_ev = (unsigned long long *) a.e_fix + (size_t) 4 * n;
   const int lane = threadIdx.x & 31, np = min(a.nl->npairs, a.pcap);
+  // Queue entries are staged per warp in shared memory and written out 32 at
+  // a time with one atomic reservation: one counter update per 32 entries
+  // instead of one per warp iteration (same-address atomics serialise in L2).
+  constexpr int kStageWarps = 8;  // warps per block of any caller
+  __shared__ int stage_d[kStageWarps][96], stage_p[kStageWarps][64];
+  int *const sd = stage_d[threadIdx.x >> 5], *const spp = stage_p[threadIdx.x >> 5];
+  int nsd = 0, nsp = 0;  // staged entries (warp-uniform)
+  // write the first `count` staged entries (count <= 32) to the queue at `region`, move the rest down
+  auto flush = [&](int *buf, int &cnt, int count, int *counter, size_t region) {
+    int at = 0;
+    if (lane == 0) at = atomicAdd(counter, count);
+    at = __shfl_sync(0xffffffffu, at, 0);
+    if (lane < count) a.hbq[region + at + lane] = buf[lane];
+    const int v1 = lane + 32 < cnt ? buf[lane + 32] : 0, v2 = lane + 64 < cnt ? buf[lane + 64] : 0;
+    __syncwarp();
+    buf[lane] = v1;
+    buf[lane + 32] = v2;  // index < 64: inside both buffers
+    __syncwarp();
+    cnt -= count;
+  };
   // warp-uniform trip count: the queue appends below are warp collectives
   for (int base = sp.t - lane; base < np; base += sp.nthr) {
     const int q = base + lane;
@@ -849,23 +869,21 @@ template <typename R> __device__ __forceinline__ void pair_pass(const StepArgs<R
     // P_AP on CA pairs (fix_backbone.cpp:8096-8103)
     q_p = (T & T_PAP) && (other || dij >= pap_sep) && rca2 < R(p.pap_cutoff_sq);
     }
-    // queue appends: one atomic per warp and queue
+    // stage this iteration's queue entries (at most 64 DSSP and 32 P_AP)
     const unsigned m0 = __ballot_sync(0xffffffffu, q_d0), m1 = __ballot_sync(0xffffffffu, q_d1),
                    mp = __ballot_sync(0xffffffffu, q_p);
-    if (m0 | m1 | mp) {
-      int bd = 0, bp = 0;
-      if (lane == 0) {
-        if (m0 | m1) bd = atomicAdd(&a.nl->n_dssp, __popc(m0) + __popc(m1));
-        if (mp) bp = atomicAdd(&a.nl->n_pap, __popc(mp));
-      }
-      bd = __shfl_sync(0xffffffffu, bd, 0);
-      bp = __shfl_sync(0xffffffffu, bp, 0);
-      const unsigned below = (1u << lane) - 1u;
-      if (q_d0) a.hbq[qd + bd + __popc(m0 & below)] = q;
-      if (q_d1) a.hbq[qd + bd + __popc(m0) + __popc(m1 & below)] = ~q;
-      if (q_p) a.hbq[qp + bp + __popc(mp & below)] = q;
-    }
+    const unsigned below = (1u << lane) - 1u;
+    if (q_d0) sd[nsd + __popc(m0 & below)] = q;
+    if (q_d1) sd[nsd + __popc(m0) + __popc(m1 & below)] = ~q;
+    if (q_p) spp[nsp + __popc(mp & below)] = q;
+    nsd += __popc(m0) + __popc(m1);
+    nsp += __popc(mp);
+    __syncwarp();
+    while (nsd >= 32) flush(sd, nsd, 32, &a.nl->n_dssp, qd);
+    if (nsp >= 32) flush(spp, nsp, 32, &a.nl->n_pap, qp);
   }
+  if (nsd > 0) flush(sd, nsd, nsd, &a.nl->n_dssp, qd);
+  if (nsp > 0) flush(spp, nsp, nsp, &a.nl->n_pap, qp);
 }
 
 template <typename R> __global__ void __launch_bounds__(128, 6) k_pair(StepArgs<R> a, FFParams p)

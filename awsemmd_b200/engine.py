@@ -112,6 +112,7 @@ def load_library(path: str = LIB_PATH):
     lib.awsem_autotune.argtypes = [vp, ip, vp]
     lib.awsem_set_step_form.argtypes = [vp, ip, ip, ip]
     lib.awsem_get_step_form.argtypes = [vp, vp]
+    lib.awsem_set_launch_shapes.argtypes = [vp, vp]
     lib.awsem_model_info.argtypes = [vp, vp]
     lib.awsem_batch_create.argtypes = [ip, ip, C.POINTER(vp)]
     lib.awsem_batch_add_files.argtypes = [vp, cp, cp, cp, cp, cp, cp, C.c_ulonglong, C.POINTER(ip)]
@@ -249,6 +250,14 @@ class AwsemSystem:
         _check(self.lib, self.lib.awsem_autotune(self.h, int(reps), _ptr(got)), "awsem_autotune")
         return {"fragmem_separations_per_warp": int(got[0]), "pair_pass_blocks": int(got[1]),
                 "hbond_blocks": int(got[2]), "fragmem_blocks": int(got[3]), **self.step_form()}
+
+    SHAPE_KEYS = ("fragmem_separations_per_warp", "pair_pass_blocks", "hbond_blocks", "fragmem_blocks")
+
+    def set_launch_shapes(self, shapes) -> None:
+        """Apply launch shapes (a dict as `autotune` returns, or four ints in its order)."""
+        v = [shapes[k] for k in self.SHAPE_KEYS] if isinstance(shapes, dict) else list(shapes)
+        arr = np.array(v, dtype=np.int32)
+        _check(self.lib, self.lib.awsem_set_launch_shapes(self.h, _ptr(arr)), "awsem_set_launch_shapes")
 
     def set_step_form(self, form: str, blocks: int = 0, stream_warps: int = 2) -> None:
         """'kernels': each MD step a graph of per-pass kernels; 'persistent':

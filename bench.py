@@ -78,6 +78,8 @@ def parse():
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--replicas", type=int, default=1024, help="c3: number of replicas")
     ap.add_argument("--no-baseline", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--shapes", default=None,
+                    help="launch shapes d,p,h,f (as autotune reports them) instead of autotuning, e.g. for profiling")
     ap.add_argument("--serve-requests", type=int, default=48,
                     help="configuration-4 stream: requests served after the batched measurement (0: skip)")
     ap.add_argument("--serve-steps", type=int, default=20000, help="MD steps of each served request")
@@ -239,9 +241,18 @@ def c3_seed(k: int, rank: int = 0) -> int:
 
 
 # DRAM bytes (read + write) per algorithmic byte of a launch, from one ncu
-# capture of the kernel on the first 64 replicas of configuration 3
-# (profiles/fragmem_pair_hbond_c3_64replicas.txt: 117.2 MB for 108.9 MB)
-TRAFFIC_PER_ALGORITHMIC_BYTE = {"fragmem": 117.185536 / 108.913648}
+# capture of the kernel on the first 256 replicas of configuration 3, whose
+# fragment-memory table (458 MB) is larger than L2
+# (profiles/fragmem_pair_c3_256replicas.txt: 519.6 MB for 458.1 MB)
+TRAFFIC_PER_ALGORITHMIC_BYTE = {"fragmem": 519.551232 / 458.053744}
+TRAFFIC_SOURCE = "ncu dram read+write of a 256-replica launch per algorithmic byte, times this launch's algorithmic " \
+                 "bytes (profiles/fragmem_pair_c3_256replicas.txt)"
+
+
+def workload_text(args) -> str:
+    if args.workload == "c3" and args.replicas != 1024:
+        return (f"first {args.replicas} replicas of " + WORKLOADS["c3"]).replace(" (278,062 residues)", "")
+    return WORKLOADS[args.workload]
 
 
 def algorithmic_bytes(kernel: str, info) -> float:
@@ -418,7 +429,7 @@ def reference_arm(args, dist: Dist):
     line = {"metric": "residue-steps/s", "value": value, "unit": "residue-steps/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
-            "config": {"workload": WORKLOADS[args.workload], "md_steps_per_step": md,
+            "config": {"workload": workload_text(args), "md_steps_per_step": md,
                        "parallelism": f"{cores} host processes x 1 MPI rank (serial reference; no MPI in the image)"},
             "cpu_baseline": {"value": value, "unit": "residue-steps/s", "cores": cores, "kind": "reference",
                              "sample": sample},
@@ -479,7 +490,12 @@ def main():
         eng = AwsemSystem(files, precision=args.precision, device=dev)
         n_res = eng.nres
     t_setup = time.perf_counter() - t_setup
-    shapes = eng.autotune(3)  # launch shapes measured on this workload (results do not depend on them)
+    if args.shapes:
+        eng.set_launch_shapes([int(t) for t in args.shapes.split(",")])
+        shapes = {**dict(zip(eng.SHAPE_KEYS, [int(t) for t in args.shapes.split(",")])), **eng.step_form(),
+                  "source": "--shapes"}
+    else:
+        shapes = eng.autotune(3)  # launch shapes measured on this workload (results do not depend on them)
     for _ in range(args.warmup):
         eng.run(md, **run_kw)
     clocks = ClockSampler(dev)
@@ -536,14 +552,22 @@ def main():
     achieved = abytes / (prof[top] * 1e-3) / 1e9
     fm_gbs = algorithmic_bytes("fragmem", info) / (prof["fragmem"] * 1e-3) / 1e9 if prof["fragmem"] > 0 else None
     traffic = TRAFFIC_PER_ALGORITHMIC_BYTE[top] * abytes if top in TRAFFIC_PER_ALGORITHMIC_BYTE else None
+    # per kernel: algorithmic bytes / CUDA-event time against the same peak
+    per_kernel = {}
+    for k in ("fragmem", "pair", "density", "water_xi", "prepare", "finish"):
+        if prof.get(k, 0) > 0:
+            b = algorithmic_bytes(k, info)
+            per_kernel[k] = {"ms": round(prof[k], 5), "algorithmic_bytes": b,
+                             "achieved_gbs": round(b / (prof[k] * 1e-3) / 1e9, 1),
+                             "frac": round(b / (prof[k] * 1e-3) / 1e9 / peak, 4)}
     roofline = {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": traffic,
-                "traffic_source": "ncu dram read+write of a 64-replica launch per algorithmic byte, times this "
-                                  "launch's algorithmic bytes (profiles/fragmem_pair_hbond_c3_64replicas.txt)"
-                if traffic else None,
+                "traffic_source": TRAFFIC_SOURCE if traffic else None,
                 "peak_source": f"{peak_kind} hbm_gbs (burst copy)",
                 "algorithmic_bytes_per_launch": abytes, "launch_ms": prof[top],
-                "kernel_ms": {k: round(v, 5) for k, v in prof.items()}, "fragmem_gbs": fm_gbs}
+                "kernel_ms": {k: round(v, 5) for k, v in prof.items()}, "fragmem_gbs": fm_gbs,
+                "per_kernel": per_kernel,
+                "model_info": {"residues": int(info[0]), "records": int(info[2]), "pairs": int(info[6])}}
 
     # the plain single-instance FP64 form (one replica at a time)
     plain = None
@@ -605,7 +629,7 @@ def main():
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "f32/f64" if args.precision == "mixed" else "f64", "data": "synthetic",
-                "config": {"workload": WORKLOADS[args.workload], "form": args.precision, "md_steps_per_step": md,
+                "config": {"workload": workload_text(args), "form": args.precision, "md_steps_per_step": md,
                            "residues": n_res, "replicas": nrep, "global_batch": dist.world * nrep,
                            "parallelism": f"replicas x{dist.world} GPUs (independent copies per GPU)",
                            "l2": "flushed (512 MiB write) before every timed bench step",

@@ -220,6 +220,11 @@ int awsem_profile_step(awsem_system *sys, int reps, double *ms);
  * handles. */
 int awsem_autotune(awsem_system *sys, int reps, int *chosen);
 
+/* Launch shapes in awsem_autotune's `chosen` layout, e.g. ones tuned
+ * earlier on the same workload (no counterpart in the reference).  Results
+ * do not depend on them.  AWSEM_EINVAL when a value is out of range. */
+int awsem_set_launch_shapes(awsem_system *sys, const int *shapes);
+
 /* Step form of awsem_run / awsem_server_advance (no counterpart in the
  * reference, which evaluates on the CPU inside LAMMPS's pre_force hook).
  * form 0: each MD step is a chain of per-pass kernels (prepare, list

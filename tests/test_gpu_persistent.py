@@ -106,3 +106,22 @@ def test_step_form_arguments(ff, gpu_lib):
         assert f["step_form"] == "persistent" and f["persistent_blocks"] == 5 and f["stream_warps"] == 3
         b.set_step_form("kernels")
         assert b.step_form()["step_form"] == "kernels"
+
+
+def test_launch_shapes_do_not_change_results(ff, gpu_lib):
+    """awsem_set_launch_shapes: any valid shapes give the same trajectory bit
+    for bit; out-of-range shapes are refused."""
+    from awsemmd_b200.engine import AwsemBatch, AwsemError
+
+    out = []
+    for shapes in [(1, 148, 148, 0), (3, 592, 37, 296), (2, 1, 1, 1)]:
+        with AwsemBatch.from_arrays(ff, chains(), precision="mixed", seeds=[5, 6, 7, 8, 9]) as b:
+            b.set_launch_shapes(shapes)
+            b.run(30, t_start=500.0, t_stop=300.0, neigh_every=10)
+            out.append(b.get_state_all())
+    for x, v in out[1:]:
+        assert np.array_equal(out[0][0], x) and np.array_equal(out[0][1], v)
+    with AwsemBatch.from_arrays(ff, chains()[:1], precision="mixed") as b:
+        for bad in [(0, 1, 1, 0), (1, 0, 1, 0), (1, 1, 0, 0), (1, 1, 1, -1), (99, 1, 1, 0)]:
+            with pytest.raises(AwsemError):
+                b.set_launch_shapes(bad)
