@@ -43,6 +43,8 @@ struct NLState {
   float r_contact, r_dssp, r_pap, r_ev;  // term cutoffs on the bead pairs they test
   float bCAx;         // max distance of a residue's CB or O from its own CA (this step)
   float ev_pre_sq;    // CA-CA distance^2 beyond which no bead pair of two residues is in excluded-volume range
+  float bNCA;         // max distance of a residue's virtual N from its own CA (this step)
+  float dssp_pre_sq;  // CA-CA distance^2 beyond which neither O-N pair of two residues is within the DSSP cutoff
   int n_dssp, n_pap;  // hydrogen-bond queue lengths of the current evaluation
   int npairs;         // pairs in the residue pair list (may exceed its capacity: overflow)
   int fm_timeout;     // a fragment-memory stream wait gave up (results invalid)
@@ -123,7 +125,7 @@ __device__ __forceinline__ void atomic_max_f(float *addr, float v)
 
 template <typename R> __device__ __forceinline__ void prepare_pass(const StepArgs<R> &a, const FFParams &p, Span sp)
 {
-  float d2 = 0.f, oO = 0.f, oN = 0.f, oCA = 0.f, oAll = 0.f, oX = 0.f;
+  float d2 = 0.f, oO = 0.f, oN = 0.f, oCA = 0.f, oAll = 0.f, oX = 0.f, oNCA = 0.f;
   const int lane = threadIdx.x & 31;
   // warp-uniform trip count: the maxima are reduced across the warp below
   for (int r0 = sp.t - lane; r0 < a.n_run; r0 += sp.nthr) {
@@ -181,7 +183,11 @@ template <typename R> __device__ __forceinline__ void prepare_pass(const StepArg
     oO = fmaxf(oO, off(o));
     oCA = fmaxf(oCA, off(ca));
     oAll = fmaxf(oAll, fmaxf(fmaxf(off(ca), off(cb)), off(o)));
-    if (!(fl & R_FIRST)) oN = fmaxf(oN, off(n));
+    if (!(fl & R_FIRST)) {
+      oN = fmaxf(oN, off(n));
+      const double ex = n[0] - ca[0], ey = n[1] - ca[1], ez = n[2] - ca[2];
+      oNCA = fmaxf(oNCA, (float) sqrt(ex * ex + ey * ey + ez * ez));
+    }
   }
   }
   // warp max, block max, then one atomic per block and quantity (every
@@ -193,19 +199,21 @@ template <typename R> __device__ __forceinline__ void prepare_pass(const StepArg
     oCA = fmaxf(oCA, __shfl_xor_sync(0xffffffffu, oCA, s));
     oAll = fmaxf(oAll, __shfl_xor_sync(0xffffffffu, oAll, s));
     oX = fmaxf(oX, __shfl_xor_sync(0xffffffffu, oX, s));
+    oNCA = fmaxf(oNCA, __shfl_xor_sync(0xffffffffu, oNCA, s));
   }
-  __shared__ float red[6][32];
+  __shared__ float red[7][32];
   if (lane == 0) {
     const int w = threadIdx.x >> 5;
     red[0][w] = d2, red[1][w] = oO, red[2][w] = oN, red[3][w] = oCA, red[4][w] = oAll, red[5][w] = oX;
+    red[6][w] = oNCA;
   }
   __syncthreads();
-  if (threadIdx.x < 6) {
+  if (threadIdx.x < 7) {
     const int k = threadIdx.x;
     float m = 0.f;
     for (int w = 0; w < (int) (blockDim.x >> 5); w++) m = fmaxf(m, red[k][w]);
     float *dst = k == 0 ? &a.nl->d2max : k == 1 ? &a.nl->bO : k == 2 ? &a.nl->bN : k == 3 ? &a.nl->bCA
-               : k == 4 ? &a.nl->bAll : &a.nl->bCAx;
+               : k == 4 ? &a.nl->bAll : k == 5 ? &a.nl->bCAx : &a.nl->bNCA;
     if (m > 0.f) atomic_max_f(dst, m);  // the maxima start each step at 0
   }
 }
@@ -237,7 +245,10 @@ __device__ __forceinline__ void nl_decide(NLState *nl, int force, long long *ste
   // bead pair inside any excluded-volume cutoff (0.01 A covers rounding)
   float pre = s.r_ev + 2.f * s.bCAx + 0.01f;
   s.ev_pre_sq = pre * pre;
-  s.d2max = s.bO = s.bN = s.bCA = s.bAll = s.bCAx = 0.f;
+  // |O(i) - N(j)| >= |CA(i) - CA(j)| - |O(i) - CA(i)| - |N(j) - CA(j)|, and bCAx bounds |O - CA|
+  const float dpre = s.r_dssp + s.bCAx + s.bNCA + 0.01f;
+  s.dssp_pre_sq = dpre * dpre;
+  s.d2max = s.bO = s.bN = s.bCA = s.bAll = s.bCAx = s.bNCA = 0.f;
   s.n_dssp = s.n_pap = 0;
 }
 
@@ -722,7 +733,7 @@ template <typename R> __device__ __forceinline__ void pair_pass(const StepArgs<R
   const double *WG = s.tables + TB_WATER;
   const bool fix = a.groups & G_FIX, evon = a.groups & G_PAIR;
   const uint32_t T = fix ? p.terms : 0u;
-  const R ev_pre_sq = R(a.nl->ev_pre_sq);
+  const R ev_pre_sq = R(a.nl->ev_pre_sq), dssp_pre_sq = R(a.nl->dssp_pre_sq);
   // the largest excluded-volume cutoff, squared, with room for its rounding
   // to float and for the rounding of the bead distance
   const R ev_max_sq = R(a.nl->r_ev) * R(a.nl->r_ev) * R(1.0001);
@@ -860,7 +871,7 @@ template <typename R> __device__ __forceinline__ void pair_pass(const StepArgs<R
       if (ee != 0.0) atomicAdd(e_ev + i, (unsigned long long) fix_force(ee));
     }
     // DSSP (fix_backbone.cpp:8064-8094): O(i) with N-H(j), and O(j) with N-H(i)
-    if ((T & T_DSSP) && (other || dij > 2)) {
+    if ((T & T_DSSP) && (other || dij > 2) && rca2 < dssp_pre_sq) {
       q_d0 = !(flj & (R_PRO | R_FIRST)) && !(fli & R_LAST) &&
              norm2(diff<R>(bead(s, i, B_O), bead(s, j, B_N))) < R(p.dssp_cut_sq);
       q_d1 = !(fli & (R_PRO | R_FIRST)) && !(flj & R_LAST) &&
