@@ -6,6 +6,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <limits>
 #include <map>
 #include <memory>
 #include <stdexcept>
@@ -103,6 +104,8 @@ class EngineBase {
   virtual void set_state_all(const double *x_ext, const double *v_ext) = 0;
   virtual void get_state_all(double *x_ext, double *v_ext) = 0;
   virtual void run(long long nsteps, const awsem_run_params &rp, double *thermo) = 0;
+  virtual void run_window(long long nsteps, const awsem_run_params &rp, long long wbegin, long long wend, bool cont,
+                          double *thermo) = 0;
   virtual void energies(int rep, double *out) = 0;
   virtual void forces(int rep, double *f_ext) = 0;
   virtual void residue_arrays(int rep, double *out) = 0;
@@ -525,6 +528,7 @@ template <typename R> class Engine : public EngineBase {
   void compute(long long st, const double *x_ext, double *f_ext, double *energies_out, int groups) override
   {
     need_single("awsem_compute");
+    cont_step = -1;
     const std::vector<int> &ext = in.ext_of[0];
     int na = natoms();
     hx.resize((size_t) 3 * na);
@@ -604,6 +608,7 @@ template <typename R> class Engine : public EngineBase {
   void set_state_all(const double *x_ext, const double *v_ext) override
   {
     ensure_perm();
+    cont_step = -1;
     const int na = natoms(), tb = 256;
     for (int k = 0; k < 2; k++) {
       const double *src = k ? v_ext : x_ext;
@@ -630,6 +635,7 @@ template <typename R> class Engine : public EngineBase {
   void set_state(int rep, const double *x_ext, const double *v_ext) override
   {
     check_rep(rep);
+    cont_step = -1;
     const std::vector<int> &ext = in.ext_of[rep];
     int a0 = rep_atom0(rep), na = rep_atoms(rep);
     std::vector<double> bx((size_t) 3 * na), bv((size_t) 3 * na);
@@ -925,6 +931,7 @@ template <typename R> class Engine : public EngineBase {
     CK(cudaMemcpyAsync(v.p, sv.p, sizeof(double) * 3 * na, cudaMemcpyDeviceToDevice, s0));
     CK(cudaStreamSynchronize(s0));
     step = step_saved;
+    cont_step = -1;
     set_nl_field(&dev::NLState::r_list, 0.f);
     if (chosen) {
       chosen[0] = fm_dsplit;
@@ -937,6 +944,7 @@ template <typename R> class Engine : public EngineBase {
   void profile(int reps, double *ms) override
   {
     if (reps <= 0) throw std::invalid_argument("reps must be positive");
+    cont_step = -1;
     set_thermostat(last_rp);
     upload_runs(last_rp, step, step + reps + 1);
     long long pre = step;  // profiled steps continue the trajectory
@@ -1097,13 +1105,42 @@ template <typename R> class Engine : public EngineBase {
     integ.dtf = 0.5 * rp.dt * FTM2V;
     integ.langevin = rp.langevin;
     integ.begin = begin;
+    integ.stop = std::numeric_limits<long long>::max();
     integ.damp = rp.damp;
     return integ;
   }
 
+  // A run that stopped before its window's end leaves the state at the full
+  // step `cont_step`, with that step's total force in ftot; a later call may
+  // continue the window from there.  Anything else that touches the state or
+  // ftot clears it (-1).
+  long long cont_step = -1, cont_wbegin = 0, cont_wend = 0;
+
   void run(long long nsteps, const awsem_run_params &rp, double *thermo) override
   {
+    run_window(nsteps, rp, step, step + nsteps, false, thermo);
+  }
+
+  // Steps step+1 .. step+nsteps of the window [wbegin, wend], whose ends set
+  // the thermostat ramp and the integration window (setup evaluation at
+  // wbegin, no drift after wend).  cont = false: the call begins with the
+  // setup evaluation at the current step, which must be wbegin; cont = true:
+  // it continues a call that stopped at the current step inside the same
+  // window.
+  void run_window(long long nsteps, const awsem_run_params &rp, long long wbegin, long long wend, bool cont,
+                  double *thermo) override
+  {
     if (nsteps < 0) throw std::invalid_argument("nsteps must be >= 0");
+    if (cont) {
+      if (cont_step != step || wbegin != cont_wbegin || wend != cont_wend)
+        throw std::invalid_argument("continue: the previous call on this handle did not stop at step " +
+                                    std::to_string(step) + " inside this window");
+      if (nsteps < 1) throw std::invalid_argument("continue: nsteps must be >= 1");
+    } else if (wbegin != step) {
+      throw std::invalid_argument("the window must begin at the current step " + std::to_string(step));
+    }
+    if (step + nsteps > wend) throw std::invalid_argument("the call runs past the window's end");
+    cont_step = -1;
     last_rp = rp;
     // thermostat factors per atom (fix langevin, units real)
     set_thermostat(rp);
@@ -1115,26 +1152,33 @@ template <typename R> class Engine : public EngineBase {
       neigh_every = rp.neigh_every;
       set_nl_field(&dev::NLState::every, neigh_every);
     }
-    upload_runs(rp, step, step + nsteps);
+    const long long rows = cont ? nsteps : nsteps + 1;  // evaluations of this call
+    dev::Integrator integ = make_integrator(rp, cont ? step + 1 : step);
+    integ.stop = step + nsteps;
+    upload_integrator(integ);
+    std::vector<dev::SlotRun> w(n_sys(), dev::SlotRun{wbegin, wend, 0, rp.t_start, rp.t_stop});
+    CK(cudaMemcpyAsync(slot_run.p, w.data(), sizeof(dev::SlotRun) * w.size(), cudaMemcpyHostToDevice, s0));
     // Langevin seed of each replica: its own when set, else the run's
     std::vector<unsigned long long> sd(n_sys());
     for (int k = 0; k < n_sys(); k++) sd[k] = seeds[k] ? seeds[k] : rp.seed;
     CK(cudaMemcpyAsync(sys_seed.p, sd.data(), sizeof(unsigned long long) * sd.size(), cudaMemcpyHostToDevice, s0));
-    long long pre = step - 1;  // the setup evaluation advances the counter to `step`
+    // a setup evaluation advances the counter to `step`; a continuation starts from it
+    long long pre = cont ? step : step - 1;
     CK(cudaMemcpyAsync(dstep.p, &pre, sizeof pre, cudaMemcpyHostToDevice, s0));
+    CK(cudaStreamSynchronize(s0));
     bool want_thermo = thermo != nullptr;
     int tv = want_thermo ? 1 : 0;
     if (want_thermo) {
       // thermo graphs bake the row buffer's address and row count: rebuilt per run
-      thermo_nrows = nsteps + 1;
-      thermo_rows.alloc((size_t) 4 * (nsteps + 1) * n_sys());
+      thermo_nrows = rows;
+      thermo_rows.alloc((size_t) 4 * rows * n_sys());
       for (auto &g : graphs[1])
         if (g) {
           cudaGraphExecDestroy(g);
           g = nullptr;
         }
     }
-    long long total = nsteps + 1;
+    long long total = rows;
     if (!graphs[tv][0]) capture_steps(graphs[tv][0], 1, want_thermo);
     if (total >= kChunk && !graphs[tv][1]) capture_steps(graphs[tv][1], kChunk, want_thermo);
     if (!ev_run0) {
@@ -1143,6 +1187,11 @@ template <typename R> class Engine : public EngineBase {
     }
     long long done = 0;
     CK(cudaEventRecord(ev_run0, s0));
+    if (cont) {
+      const int tb = 128;
+      dev::k_continue<R><<<(n_run() + tb - 1) / tb, tb, 0, s0>>>(args(groups_all), d_integ.p, ftot.p, x.p);
+      CK(cudaGetLastError());
+    }
     while (total - done >= kChunk) {
       CK(cudaGraphLaunch(graphs[tv][1], s0));
       done += kChunk;
@@ -1159,7 +1208,12 @@ template <typename R> class Engine : public EngineBase {
     step += nsteps;
     check_list();
     if (want_thermo)
-      CK(cudaMemcpy(thermo, thermo_rows.p, sizeof(double) * 4 * (nsteps + 1) * n_sys(), cudaMemcpyDeviceToHost));
+      CK(cudaMemcpy(thermo, thermo_rows.p, sizeof(double) * 4 * rows * n_sys(), cudaMemcpyDeviceToHost));
+    if (step < wend) {
+      cont_step = step;
+      cont_wbegin = wbegin;
+      cont_wend = wend;
+    }
   }
 
   template <typename F> void set_nl_field(F dev::NLState::*field, F value)
@@ -1909,6 +1963,24 @@ int awsem_set_state(awsem_system *sys, const double *x, const double *v) { retur
 int awsem_get_state(awsem_system *sys, double *x, double *v) { return awsem_replica_get_state(sys, 0, x, v); }
 int awsem_energies(awsem_system *sys, double *energies) { return awsem_replica_energies(sys, 0, energies); }
 int awsem_forces(awsem_system *sys, double *f) { return awsem_replica_forces(sys, 0, f); }
+
+int awsem_run_window(awsem_system *sys, long long nsteps, const awsem_run_params *rp, long long window_begin,
+                     long long window_end, int cont, double *thermo)
+{
+  if (!ready(sys) || !rp) {
+    g_last_error = "awsem_run_window: null argument or uncommitted handle";
+    return AWSEM_EINVAL;
+  }
+  if (rp->dt <= 0 || rp->damp <= 0 || (rp->langevin && (rp->t_start < 0 || rp->t_stop < 0))) {
+    g_last_error = "awsem_run_window: dt and damp must be positive, temperatures non-negative";
+    return AWSEM_EINVAL;
+  }
+  if (sys->eng->server) {
+    g_last_error = "awsem_run_window: a serving handle advances with awsem_server_advance";
+    return AWSEM_EINVAL;
+  }
+  return guarded([&] { sys->eng->run_window(nsteps, *rp, window_begin, window_end, cont != 0, thermo); });
+}
 
 int awsem_run(awsem_system *sys, long long nsteps, const awsem_run_params *rp, double *thermo)
 {

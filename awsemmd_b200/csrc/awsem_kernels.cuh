@@ -965,7 +965,8 @@ struct Integrator {
   double dt, dtf;           // dtf = 0.5 * dt * ftm2v
   int langevin;
   double damp;
-  long long begin;          // first step of the current run (thermo row 0)
+  long long begin;          // first evaluated step of the current call (thermo row 0)
+  long long stop;           // last step of the current call: its state stays at the full step (no drift after it)
 };
 
 // Total force (fixed point -> FP64, plus Langevin at `step`), then
@@ -981,7 +982,7 @@ __device__ __forceinline__ void finish_one(const StepArgs<R> &a, const Integrato
   if (rep < 0) return;
   const SlotRun sr = a.slot_run[rep];
   if (step < sr.begin || step > sr.end) return;
-  const bool final_kick = step > sr.begin, next = step < sr.end;
+  const bool final_kick = step > sr.begin, next = step < sr.end && step < in.stop;
   const unsigned long long seed = a.sys_seed[rep];
   const long long key = step - sr.step0;  // the replica's own step count keys its noise
   // Every multiply and add below is rounded on its own (no contraction), as
@@ -1033,6 +1034,32 @@ __global__ void k_finish(StepArgs<R> a, const Integrator *inp, const double *g1,
                          double *x_out)
 {
   finish_pass(a, inp, g1, g2, ftot, x_out, grid_span());
+}
+
+// Continuation of a run that stopped at step `*a.step` before its window's
+// end: the initial integration (half kick and drift) finish_one would have
+// done there, from the total force it stored in ftot -- the same operations
+// in the same order, so a run split into calls equals the run in one call.
+template <typename R>
+__global__ void k_continue(StepArgs<R> a, const Integrator *inp, const double *ftot, double *x_out)
+{
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= a.n_run) return;
+  const int rep = a.res_sys[r];
+  if (rep < 0) return;
+  const Integrator in = *inp;
+  const SlotRun sr = a.slot_run[rep];
+  const long long step = *a.step;
+  if (step < sr.begin || step >= sr.end) return;
+  for (int b = 0; b < 3; b++) {
+    const int at = 3 * r + b;
+    const double dtfm = in.dtf / a.mass[at];
+    for (int c = 0; c < 3; c++) {
+      const double v = __dadd_rn(a.v[3 * at + c], __dmul_rn(dtfm, ftot[3 * at + c]));
+      x_out[3 * at + c] = __dadd_rn(x_out[3 * at + c], __dmul_rn(in.dt, v));
+      a.v[3 * at + c] = v;
+    }
+  }
 }
 
 // Caller-order staging <-> internal order: out[a] = in[perm[a]] / out[perm[a]] = in[a]

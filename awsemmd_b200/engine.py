@@ -113,6 +113,9 @@ def load_library(path: str = LIB_PATH):
     lib.awsem_set_step_form.argtypes = [vp, ip, ip, ip]
     lib.awsem_get_step_form.argtypes = [vp, vp]
     lib.awsem_set_launch_shapes.argtypes = [vp, vp]
+    lib.awsem_run_window.argtypes = [vp, C.c_longlong, C.POINTER(RunParams), C.c_longlong, C.c_longlong, ip, vp]
+    lib.awsem_create_from_atoms.argtypes = [cp, cp, cp, ip, vp, vp, vp, vp, vp, vp, ip, vp, ip, vp, vp, vp, vp, cp, cp,
+                                            ip, ip, C.POINTER(vp)]
     lib.awsem_model_info.argtypes = [vp, vp]
     lib.awsem_batch_create.argtypes = [ip, ip, C.POINTER(vp)]
     lib.awsem_batch_add_files.argtypes = [vp, cp, cp, cp, cp, cp, cp, C.c_ulonglong, C.POINTER(ip)]
@@ -165,6 +168,38 @@ class AwsemSystem:
         self.nres = lib.awsem_nres(h)
         self.precision = prec
 
+    @classmethod
+    def from_atoms(cls, workdir: str, coeff: str, seq: str, role, residue, molecule, atom_type, tag, mass_by_type,
+                   x=None, bonds=None, pair_style: str = "2 3.5 3.5", pair_coeffs: str = "",
+                   precision: str | int = "fp64", device: int = 0):
+        """A system from per-atom arrays in the caller's order (awsem_create_from_atoms):
+        role 0 CA, 1 CB / H-beta, 2 O; mass_by_type[t] for t = 1..ntypes (index 0 unused);
+        bonds = (a, b, K, r0) with 0-based caller indices, or None."""
+        self = cls.__new__(cls)
+        lib = load_library()
+        self.lib = lib
+        prec = {"fp64": FP64, "mixed": MIXED}.get(precision, precision)
+        ints = [np.ascontiguousarray(v, dtype=np.int32) for v in (role, residue, molecule, atom_type, tag)]
+        n = len(ints[0])
+        mass = np.ascontiguousarray(mass_by_type, dtype=np.float64)
+        xa = None if x is None else np.ascontiguousarray(x, dtype=np.float64).reshape(n, 3)
+        if bonds is not None and len(bonds[0]):
+            ba, bb = (np.ascontiguousarray(v, dtype=np.int32) for v in bonds[:2])
+            bk, br = (np.ascontiguousarray(v, dtype=np.float64) for v in bonds[2:])
+            nb, bp = len(ba), [_ptr(ba), _ptr(bb), _ptr(bk), _ptr(br)]
+        else:
+            nb, bp = 0, [None] * 4
+        h = C.c_void_p()
+        rc = lib.awsem_create_from_atoms(workdir.encode(), coeff.encode(), seq.encode(), n, *[_ptr(v) for v in ints],
+                                         _ptr(mass), len(mass) - 1, None if xa is None else _ptr(xa), nb, *bp,
+                                         pair_style.encode(), pair_coeffs.encode(), int(prec), int(device), C.byref(h))
+        _check(lib, rc, "awsem_create_from_atoms")
+        self.h = h
+        self.natoms = lib.awsem_natoms(h)
+        self.nres = lib.awsem_nres(h)
+        self.precision = prec
+        return self
+
     def close(self):
         if getattr(self, "h", None):
             self.lib.awsem_destroy(self.h)
@@ -178,6 +213,17 @@ class AwsemSystem:
 
     def __exit__(self, *exc):
         self.close()
+
+    def run_window(self, nsteps: int, window: tuple, cont: bool, dt=2.0, langevin=True, t_start=300.0,
+                   t_stop=300.0, damp=500.0, seed=1, skin=2.0, neigh_every=0, thermo=False):
+        """nsteps of the run window (begin, end) (awsem_run_window); cont continues the previous call."""
+        rp = RunParams(dt, int(langevin), t_start, t_stop, damp, seed, skin, neigh_every)
+        nrep = getattr(self, "nreplicas", 1)
+        rows = np.zeros((nrep, nsteps + (0 if cont else 1), 4)) if thermo else None
+        _check(self.lib, self.lib.awsem_run_window(self.h, nsteps, C.byref(rp), int(window[0]), int(window[1]),
+                                                   int(bool(cont)), None if rows is None else _ptr(rows)),
+               "awsem_run_window")
+        return rows if rows is None or nrep > 1 else rows[0]
 
     @property
     def step(self) -> int:

@@ -172,6 +172,23 @@ int awsem_get_state(awsem_system *sys, double *x, double *v);
  * at the current step counter.  Advances every replica of a batch. */
 int awsem_run(awsem_system *sys, long long nsteps, const awsem_run_params *rp, double *thermo);
 
+/* One part of a LAMMPS `run` whose output (thermo, dumps, fix print) falls
+ * between its steps: the window [window_begin, window_end] (absolute steps)
+ * is the whole run -- the fix langevin ramp t_start -> t_stop spans it, as
+ * LAMMPS's fix langevin interpolates over beginstep..endstep, the setup
+ * evaluation is at window_begin and nothing drifts after window_end -- and
+ * this call advances nsteps of it.  cont = 0: the call starts the window with
+ * its setup evaluation (the current step must be window_begin); cont = 1: it
+ * continues a call on this handle that stopped at the current step inside the
+ * same window, so that the parts together are the single call bit for bit.
+ * After each call the state (awsem_get_state) and energies are those of the
+ * full step reached, as LAMMPS has them at end_of_step.  thermo rows: nsteps
+ * + 1 (cont = 0) or nsteps (cont = 1) per replica.  awsem_run(n) is the
+ * window [step, step + n] in one call.  A set_state, compute or profile call
+ * in between ends the possibility to continue (AWSEM_EINVAL). */
+int awsem_run_window(awsem_system *sys, long long nsteps, const awsem_run_params *rp, long long window_begin,
+                     long long window_end, int cont, double *thermo);
+
 /* Device time (ms) of the last awsem_run, from CUDA events recorded on the
  * engine's stream around the launched step graphs. */
 double awsem_last_run_ms(const awsem_system *sys);

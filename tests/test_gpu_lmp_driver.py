@@ -1,0 +1,143 @@
+"""Input-script driver on the GPU: a LAMMPS deck in the style of the
+reference's examples (folding.in) run on the reference's own 1R69 inputs
+must reproduce the reference's 20-step Langevin run (the golden vectors made
+by the shim-hosted reference, tests/golden/make_golden.py) at every output
+step; and a run cut into calls at the output steps (awsem_run_window) must be
+the run in one call bit for bit."""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import write_case
+
+pytestmark = pytest.mark.gpu
+
+DECK = """
+units real
+timestep {dt}
+dimension 3
+boundary s s s
+neighbor 5 bin
+neigh_modify delay 5
+atom_modify sort 0 0.0
+special_bonds fene
+atom_style awsemmd
+bond_style harmonic
+pair_style vexcluded 2 3.5 3.5
+read_data data.1r69
+pair_coeff * * 0.0
+pair_coeff 1 1 20.0 3.5 4.5
+pair_coeff 1 4 20.0 3.5 4.5
+pair_coeff 4 4 20.0 3.5 4.5
+pair_coeff 3 3 20.0 3.5 3.5
+group alpha_carbons type 1
+group beta_atoms type 4 5
+group oxygens type 3
+fix 1 all nve
+fix 11 all langevin {t0} {t1} {damp} {seed}
+fix 2 alpha_carbons backbone beta_atoms oxygens fix_backbone_coeff.data extended.seq
+thermo {thermo}
+dump 1 all atom 10 run.dump
+dump_modify 1 sort id
+variable E_chain equal f_2[1]
+variable E_pot equal pe
+variable E_kin equal ke
+variable Step equal step
+fix energy all print 5 "${{Step}} ${{E_pot}} ${{E_kin}} ${{E_chain}}" file energy screen no
+reset_timestep 0
+run {nsteps}
+write_restart restart.end
+"""
+
+
+def run_deck(workdir, g, thermo):
+    from awsemmd_b200 import lmp
+
+    nsteps, dt, t0, t1, damp, seed = g["run"]
+    deck = DECK.format(dt=dt, t0=t0, t1=t1, damp=damp, seed=int(seed), nsteps=int(nsteps), thermo=thermo)
+    cwd = os.getcwd()
+    os.chdir(workdir)
+    try:
+        d = lmp.Driver(precision="fp64", screen=None, logfile="log.test")
+        try:
+            d.lines(deck.split("\n"))
+        finally:
+            d.close()
+    finally:
+        os.chdir(cwd)
+
+
+def test_deck_reproduces_the_reference_run(tmp_path, gpu_lib):
+    from awsemmd_b200 import lmp
+
+    files, g = write_case("r1r69", tmp_path)
+    wd = files["workdir"]
+    run_deck(wd, g, thermo=5)
+    rows = g["thermo"]  # per step: fix total, vexcluded, bonds, kinetic (reference, 20 Langevin steps)
+    pe_ref, ke_ref = rows[:, 0] + rows[:, 1] + rows[:, 2], rows[:, 3]
+    # fix print at steps 0, 5, 10, 15, 20
+    out = np.array([[float(t) for t in l.split()] for l in open(os.path.join(wd, "energy")).read().splitlines()[1:]])
+    assert list(out[:, 0]) == [0, 5, 10, 15, 20]
+    steps = out[:, 0].astype(int)
+    np.testing.assert_allclose(out[:, 1], pe_ref[steps], rtol=1e-6, atol=1e-6)
+    np.testing.assert_allclose(out[:, 2], ke_ref[steps], rtol=1e-6, atol=1e-6)
+    assert abs(out[0, 3] - g["e0"][1]) <= 1e-6 * abs(g["e0"][1])
+    # energy.log of fix backbone at the thermo steps: step 0 is the reference's energy vector
+    log = open(os.path.join(wd, "energy.log")).read().splitlines()
+    assert log[0].startswith("Step") and [int(l.split()[0]) for l in log[1:]] == [0, 5, 10, 15, 20]
+    e0 = [float(t) for t in log[1].split()[1:]]
+    for k in range(1, 18):
+        assert abs(e0[k - 1] - g["e0"][k]) <= 1e-6 * max(abs(g["e0"][k]), 1.0), k
+    assert abs(e0[17] - g["e0"][0]) <= 1e-6 * abs(g["e0"][0])
+    # the final state (restart file) is the reference's after 20 steps
+    r = lmp.read_data(os.path.join(wd, "restart.end"))
+    assert r.timestep == 20
+    assert np.abs(r.x - g["xN"]).max() < 1e-6 and np.abs(r.v - g["vN"]).max() < 1e-6
+    # dump frames at 0, 10, 20
+    assert open(os.path.join(wd, "run.dump")).read().count("ITEM: TIMESTEP") == 3
+
+
+def test_output_cadence_does_not_change_the_trajectory(tmp_path, gpu_lib):
+    """thermo 1 (a call per step) and thermo 20 (calls at 5, 10, 15, 20 only for
+    fix print and dumps): the restart files are identical."""
+    files, g = write_case("r1r69", tmp_path)
+    texts = []
+    for thermo in (1, 20):
+        run_deck(files["workdir"], g, thermo=thermo)
+        texts.append(open(os.path.join(files["workdir"], "restart.end")).read())
+    assert texts[0] == texts[1]
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_run_window_parts_equal_one_call(prec, tmp_path, gpu_lib):
+    from awsemmd_b200.engine import AwsemError, AwsemSystem
+
+    files, g = write_case("c0", tmp_path)
+    kw = dict(dt=2.0, langevin=True, t_start=450.0, t_stop=250.0, damp=500.0, seed=99, neigh_every=10)
+    with AwsemSystem(files, precision=prec) as s:
+        s.set_state(g["x0"], g["v0"])
+        rows_one = s.run(30, thermo=True, **kw)
+        x1, v1 = s.get_state()
+        e1 = s.energies()
+    with AwsemSystem(files, precision=prec) as s:
+        s.set_state(g["x0"], g["v0"])
+        r0 = s.run_window(0, (0, 30), False, thermo=True, **kw)
+        e_setup = s.energies()
+        r1 = s.run_window(7, (0, 30), True, thermo=True, **kw)
+        r2 = s.run_window(23, (0, 30), True, thermo=True, **kw)
+        x2, v2 = s.get_state()
+        e2 = s.energies()
+        with pytest.raises(AwsemError):  # the window has ended
+            s.run_window(1, (0, 30), True, **kw)
+    assert np.array_equal(x1, x2) and np.array_equal(v1, v2)
+    assert np.array_equal(e1, e2)
+    assert np.array_equal(np.concatenate([r0, r1, r2]), rows_one)
+    assert np.array_equal(e_setup[:20], rows_one[0, 0] * 0 + e_setup[:20])  # setup call: energies at step 0
+    assert e_setup[20] == rows_one[0, 3]
+    # a state change ends the possibility to continue
+    with AwsemSystem(files, precision=prec) as s:
+        s.run_window(3, (0, 10), False, **kw)
+        s.set_state(g["x0"], g["v0"])
+        with pytest.raises(AwsemError):
+            s.run_window(3, (0, 10), True, **kw)
