@@ -161,6 +161,8 @@ template <typename R> class Engine : public EngineBase {
   int bond_cap = 1;
   DBuf<int> fm_soff, fm_slen;
   DBuf<R> fm_rf, fm_coef;
+  DBuf<double> tb_data;            // table fragment memory (energy, force pairs)
+  DBuf<unsigned char> tb_present;
   int fm_groups = 0, fm_dsplit = 1;
   DBuf<double> thermo_rows;
   DBuf<int> res_sys, sys_begin, sys_end;
@@ -257,6 +259,8 @@ template <typename R> class Engine : public EngineBase {
     a.fm.min_sep = in.ff.p.fm_min_sep;
     a.fm.groups = fm_groups;
     a.fm.dsplit = fm_dsplit;
+    a.tb_data = reinterpret_cast<const double2 *>(tb_data.p);
+    a.tb_present = tb_present.p;
     a.groups = groups;
     a.step = dstep.p;
     a.res_sys = res_sys.p;
@@ -343,6 +347,13 @@ template <typename R> class Engine : public EngineBase {
     bond_r0.upload(br, s0);
     if (!(in.ff.p.terms & T_FM)) in.ff.p.fm_nd = 0;
     upload_fm_slices();
+    if (in.ff.p.terms & T_FM_TABLE) {
+      tb_data.upload(in.tb.data, s0);
+      std::vector<unsigned char> pr(in.tb.present.begin(), in.tb.present.end());
+      tb_present.upload(pr, s0);
+      CK(cudaStreamSynchronize(s0));
+      std::vector<double>().swap(in.tb.data);  // the device holds the tables now
+    }
     CK(cudaFuncSetAttribute(dev::k_fragmem<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             4 * dev::fm_warp_smem<R>(true)));
     // pair-list radii of the terms
@@ -489,11 +500,13 @@ template <typename R> class Engine : public EngineBase {
     int tb = 128, nb = (nn + tb - 1) / tb;
     launch_prepare_and_list(a, s0, false, advance);
     bool fm = (a.groups & dev::G_FIX) && p.fm_nd > 0;
-    if (fm) {
+    const bool fmt = (a.groups & dev::G_FIX) && (p.terms & T_FM_TABLE);
+    if (fm || fmt) {
       // fragment memory is independent of the pair passes: second stream
       CK(cudaEventRecord(ev_fork, s0));
       CK(cudaStreamWaitEvent(s1, ev_fork, 0));
-      dev::k_fragmem<R><<<fm_blocks(), tb, fm_smem(), s1>>>(a, p);
+      if (fm) dev::k_fragmem<R><<<fm_blocks(), tb, fm_smem(), s1>>>(a, p);
+      if (fmt) dev::k_fm_table<R><<<fm_table_blocks(), tb, 0, s1>>>(a, p);
       CK(cudaEventRecord(ev_join, s1));
     }
     dev::k_density<R><<<pair_blocks, tb, 0, s0>>>(a, p);
@@ -501,7 +514,13 @@ template <typename R> class Engine : public EngineBase {
     dev::k_water_xi<R><<<pair_blocks, tb, 0, s0>>>(a, p);
     dev::k_pair<R><<<pair_blocks, tb, 0, s0>>>(a, p);
     dev::k_hbond<R><<<hb_blocks, 128, 0, s0>>>(a, p);
-    if (fm) CK(cudaStreamWaitEvent(s0, ev_join, 0));
+    if (fm || fmt) CK(cudaStreamWaitEvent(s0, ev_join, 0));
+  }
+
+  int fm_table_blocks() const
+  {
+    const long long items = (long long) n_run() * std::max(in.ff.p.tb_nbrs, 1);
+    return (int) std::min<long long>((items + 127) / 128, 64LL * sms_);
   }
 
   void zero_unwritten_energies(int groups)
@@ -572,6 +591,13 @@ template <typename R> class Engine : public EngineBase {
                        std::to_string(st.overflow) + "); results of this call are invalid");
     if (st.fm_timeout)
       throw StateError("fragment-memory stream: a shared-memory copy wait gave up; results of this call are invalid");
+    if (st.tb_error) {
+      // the reference stops the run with these messages (fix_backbone.cpp:4400, :4423)
+      const int code = st.tb_error;
+      set_nl_field(&dev::NLState::tb_error, 0);
+      throw StateError(code == 1 ? "Table Fragment Memory: r is out of computed range."
+                                 : "Table Fragment Memory: ir is out of range.");
+    }
     if (gbar.p) {
       dev::GridBar gb;
       CK(cudaMemcpy(&gb, gbar.p, sizeof gb, cudaMemcpyDeviceToHost));
@@ -739,7 +765,8 @@ template <typename R> class Engine : public EngineBase {
   {
     const bool fm = fm_on(a);
     dev::PersistArgs q{d_integ.p, g1.p, g2.p, ftot.p, x.p, gbar.p, n_run(), ps_stream,
-                       fm ? ps_ring_warps() : 0, fm ? std::min(fm_groups, (n_run() + 31) / 32) * fm_dsplit : 0};
+                       fm ? ps_ring_warps() : 0, fm ? std::min(fm_groups, (n_run() + 31) / 32) * fm_dsplit : 0,
+                       (a.groups & dev::G_FIX) && (in.ff.p.terms & T_FM_TABLE) ? 1 : 0};
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(ps_grid_now);
     cfg.blockDim = dim3(dev::kStepThreads);
@@ -968,7 +995,10 @@ template <typename R> class Engine : public EngineBase {
           case 5: dev::k_water_xi<R><<<pair_blocks, tb, 0, s0>>>(a, p); break;
           case 6: dev::k_pair<R><<<pair_blocks, tb, 0, s0>>>(a, p); break;
           case 7: dev::k_hbond<R><<<hb_blocks, 128, 0, s0>>>(a, p); break;
-          case 8: if (fm) dev::k_fragmem<R><<<fm_blocks(), tb, fm_smem(), s0>>>(a, p); break;
+          case 8:
+            if (fm) dev::k_fragmem<R><<<fm_blocks(), tb, fm_smem(), s0>>>(a, p);
+            if (p.terms & T_FM_TABLE) dev::k_fm_table<R><<<fm_table_blocks(), tb, 0, s0>>>(a, p);
+            break;
           case 9: dev::k_finish<R><<<nb, tb, 0, s0>>>(a, d_integ.p, g1.p, g2.p, ftot.p, x.p); break;
         }
         CK(cudaEventRecord(ev[2 * k + 1], s0));
@@ -1345,6 +1375,8 @@ template <typename R> class Engine : public EngineBase {
   {
     if (cap_res <= 0 || max_slots <= 0 || cap_records < 0) throw std::invalid_argument("server capacities must be positive");
     if (dt <= 0 || damp <= 0) throw std::invalid_argument("dt and damp must be positive");
+    if (f.ff.p.terms & T_FM_TABLE)
+      throw std::invalid_argument("serving handles do not support [Fragment_Memory_Table] (use [Fragment_Memory])");
     const long long groups = (cap_res + 31) / 32;
     if (groups * 32 * pairs_per_res >= (1ll << 31)) throw std::invalid_argument("residue capacity too large");
     sf = &f;
@@ -1692,7 +1724,8 @@ template <typename R> class Engine : public EngineBase {
     add(aps), add(tables), add(x), add(v), add(mass), add(g1), add(g2), add(ftot), add(work), add(e_res), add(energy);
     add(pos), add(cb_build), add(facc), add(pairs), add(ncount), add(hbq), add(dacc), add(e_fix), add(nl), add(dstep);
     add(ev_pref), add(ev_cs), add(ev_cl), add(excl_self), add(excl_next), add(bond_i), add(bond_j), add(bond_k);
-    add(bond_r0), add(fm_soff), add(fm_slen), add(fm_rf), add(fm_coef), add(thermo_rows), add(res_sys), add(sys_begin);
+    add(bond_r0), add(fm_soff), add(fm_slen), add(fm_rf), add(fm_coef), add(tb_data), add(tb_present);
+    add(thermo_rows), add(res_sys), add(sys_begin);
     add(sys_end), add(sys_seed), add(slot_run), add(d_integ);
     return b;
   }

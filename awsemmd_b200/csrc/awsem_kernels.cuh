@@ -48,6 +48,7 @@ struct NLState {
   int n_dssp, n_pap;  // hydrogen-bond queue lengths of the current evaluation
   int npairs;         // pairs in the residue pair list (may exceed its capacity: overflow)
   int fm_timeout;     // a fragment-memory stream wait gave up (results invalid)
+  int tb_error;       // table fragment memory: 1 a distance outside the table's range, 2 a grid index outside it
 };
 
 // Run window of one replica: integrated over steps begin..end (the
@@ -95,6 +96,9 @@ template <typename R> struct StepArgs {
   const double *bond_k, *bond_r0;
   // fragment memory
   FMSlices<R> fm;
+  // table fragment memory: [n_res][tb_nbrs][4][tb_size] (energy, force) and the tables present
+  const double2 *tb_data;
+  const unsigned char *tb_present;
   int groups;       // AWSEM_TERMS_* bits: 1 fix backbone, 2 pair vexcluded, 4 bonds
   long long *step;   // device step counter (advanced by k_nl_decide)
   // replicas: residue -> replica, replica residue ranges, Langevin seeds
@@ -943,6 +947,68 @@ template <typename R> __global__ void __launch_bounds__(128) k_fragmem(StepArgs<
   fragmem_warp_bulk(a.fm, p.fm_sigma_sq, a.s.n_res, pos, a.s.facc,
                     (unsigned long long *) (a.e_fix + (size_t) 2 * a.s.n_res), 1, &a.nl->fm_timeout, wsm);
 }
+
+// Table fragment memory of residue i and separation slot jo
+// (FixBackbone::table_fragment_memory, fix_backbone.cpp:4325-4429, called
+// for j = i + min_sep .. min(i + max_sep, the chain's last residue) at
+// :7513-7527): energy and force factor interpolated linearly between the two
+// grid points around r, for the atom pairs CA-CA, CA-CB, CB-CA, CB-CB in that
+// order.  As in the reference, a pair without a CA-CA table is skipped, the
+// first atom pair without a table ends the pair, and a distance outside the
+// table's range is an error (flagged; the host reports it).  FP64 in both
+// forms; energy and forces to fixed point.
+template <typename R> __device__ __forceinline__ void fm_table_pair(const StepArgs<R> &a, const FFParams &p, int i, int jo)
+{
+  const DevSys<R> &s = a.s;
+  const int j = i + p.fm_min_sep + jo;
+  if (a.res_sys[i] < 0 || j > s.chain_end[s.res_chain[i]]) return;
+  const size_t t0 = ((size_t) i * p.tb_nbrs + jo) * 4;
+  if (!a.tb_present[t0]) return;
+  const bool gi = s.res_flags[i] & R_GLY, gj = s.res_flags[j] & R_GLY;
+  double e = 0.0;
+  long long fi[2][3] = {{0, 0, 0}, {0, 0, 0}}, fj[2][3] = {{0, 0, 0}, {0, 0, 0}};
+  for (int k = 0; k < 4; k++) {
+    const int bi = k >= 2 ? 1 : 0, bj = k & 1;  // 0 CA, 1 CB
+    if ((bi && gi) || (bj && gj)) continue;
+    const V3<double> xi = bead(s, i, bi ? B_CB : B_CA), xj = bead(s, j, bj ? B_CB : B_CA);
+    const V3<double> dx = {xi.x - xj.x, xi.y - xj.y, xi.z - xj.z};
+    const double r = sqrt(norm2(dx));
+    if (!(r >= p.tb_rmin && r <= p.tb_rmax)) {
+      atomicMax(&a.nl->tb_error, 1);
+      break;
+    }
+    const int ir = (int) ((r - p.tb_rmin) / p.tb_dr);
+    if (!a.tb_present[t0 + k]) break;
+    if (ir < 0 || ir + 1 >= p.tb_size) {
+      atomicMax(&a.nl->tb_error, 2);
+      break;
+    }
+    const double r1 = p.tb_rmin + (double) ir * p.tb_dr, r2 = p.tb_rmin + (double) (ir + 1) * p.tb_dr;
+    const double2 *T = a.tb_data + (t0 + k) * p.tb_size;
+    const double2 q1 = T[ir], q2 = T[ir + 1];
+    e += ((q2.x - q1.x) * r + q1.x * r2 - q2.x * r1) / (r2 - r1);
+    const double ff = ((q2.y - q1.y) * r + q1.y * r2 - q2.y * r1) / (r2 - r1);
+    const long long v[3] = {fix_force(ff * dx.x), fix_force(ff * dx.y), fix_force(ff * dx.z)};
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      fi[bi][c] += v[c];
+      fj[bj][c] -= v[c];
+    }
+  }
+  scatter_fix(s, i, B_CA, fi[0]);
+  if (!gi) scatter_fix(s, i, B_CB, fi[1]);
+  scatter_fix(s, j, B_CA, fj[0]);
+  if (!gj) scatter_fix(s, j, B_CB, fj[1]);
+  if (e != 0.0) atomicAdd((unsigned long long *) (a.e_fix + (size_t) 2 * s.n_res + i), (unsigned long long) fix_force(e));
+}
+
+template <typename R> __device__ __forceinline__ void fm_table_pass(const StepArgs<R> &a, const FFParams &p, Span sp)
+{
+  const long long items = (long long) a.n_run * p.tb_nbrs;
+  for (long long t = sp.t; t < items; t += sp.nthr) fm_table_pair(a, p, (int) (t / p.tb_nbrs), (int) (t % p.tb_nbrs));
+}
+
+template <typename R> __global__ void k_fm_table(StepArgs<R> a, FFParams p) { fm_table_pass(a, p, grid_span()); }
 
 __device__ __forceinline__ uint64_t mix64(uint64_t z)
 {

@@ -82,7 +82,7 @@ void read_coeff_file(const std::string &path, ForceField &ff)
   const int i_rp = 6;  // first proline Ramachandran well
   double k_rama = 0.0, k_water = 0.0;
   static const char *outside[] = {
-      "[Shake]", "[Excluded]", "[Excluded_P]", "[Excluded_R6]", "[AMH-Go]", "[Fragment_Memory_Table]",
+      "[Shake]", "[Excluded]", "[Excluded_P]", "[Excluded_R6]", "[AMH-Go]",
       "[Contact_Restraints]", "[Vector_Fragment_Memory]", "[Solvent_Barrier]", "[Membrane]",
       "[Fragment_Frustratometer]", "[Tertiary_Frustratometer]", "[Nmer_Frustratometer]", "[Phosphorylation]",
       "[Amylometer]", "[Selection_Temperature]", "[Monte_Carlo_Seq_Opt]", "[Optimization]",
@@ -159,6 +159,13 @@ void read_coeff_file(const std::string &path, ForceField &ff)
     } else if (s == "[Fragment_Memory]") {
       p.terms |= T_FM;
       in >> ff.k_fm_raw >> ff.fm_file >> ff.fm_gamma_file;
+    } else if (s == "[Fragment_Memory_Table]") {
+      // fix_backbone.cpp:310-321
+      p.terms |= T_FM_TABLE;
+      in >> ff.k_fm_raw >> ff.fm_file >> ff.fm_gamma_file;
+      in >> p.tb_rmin >> p.tb_rmax >> p.tb_dr;
+      p.tb_size = (int) ((p.tb_rmax - p.tb_rmin) / p.tb_dr) + 2;
+      in >> ff.tb_width >> ff.tb_use_file >> p.fm_sigma_exp;
     } else if (s == "[Epsilon]") {
       in >> p.epsilon;
     } else {
@@ -668,6 +675,116 @@ void build_fm_table(const ForceField &ff, const Topology &top, const GammaTable 
   if (out.uniform) out.coef.clear();
 }
 
+static bool file_exists(const std::string &path)
+{
+  std::ifstream f(path);
+  return (bool) f;
+}
+
+// FixBackbone::compute_fragment_memory_table (fix_backbone.cpp:4238-4322),
+// read_fragment_memory_table (:4179-4236) and output_fragment_memory_table
+// (:6062-6105), in the reference's loop order and FP64 arithmetic.
+void build_fm_table_tb(const ForceField &ff, const Topology &top, const GammaTable &G,
+                       const std::vector<Memory> &mems, const std::string &dir, FMTableTB &out)
+{
+  const FFParams &p = ff.p;
+  const int n = top.n_res, min_sep = G.min_sep(), max_sep = G.max_sep();
+  out.nbrs = max_sep != -1 ? max_sep - min_sep + 1 : n - min_sep;  // fix_backbone.cpp:999-1002
+  out.size = p.tb_size;
+  if (out.nbrs <= 0 || out.size < 2 || !(p.tb_dr > 0.0))
+    fail("Fragment_Memory_Table: empty table (check rmin, rmax, dr and the gamma file's separations)");
+  const size_t ntb = (size_t) n * out.nbrs * 4;
+  const double bytes = (double) ntb * out.size * 16.0;
+  if (bytes > 96e9)
+    fail("Fragment_Memory_Table: the tables would take " + std::to_string(bytes / 1e9) +
+         " GB; use a coarser dr or a gamma file with a maximum separation");
+  out.data.assign(ntb * out.size * 2, 0.0);
+  out.present.assign(ntb, 0);
+  const std::string fe = path_in(dir, "fm_table.energy"), ff_ = path_in(dir, "fm_table.force");
+  if (ff.tb_use_file && file_exists(fe) && file_exists(ff_)) {
+    // tables listed itb-major, tb_size values each (energies, then forces)
+    for (int pass = 0; pass < 2; pass++) {
+      std::ifstream in(pass ? ff_ : fe);
+      size_t ir = 0, itb = 0;
+      double val;
+      while (in >> val) {
+        if (ir != 0 && ir % out.size == 0) {
+          ir = 0;
+          itb++;
+        }
+        if (itb >= ntb) fail("Fragment memory table file format error!");
+        out.data[(itb * out.size + ir) * 2 + pass] = val;
+        out.present[itb] = 1;
+        ir++;
+      }
+      if (itb != ntb - 1 && ir != (size_t) out.size) fail("Fragment memory table file format error!");
+    }
+    return;
+  }
+  // memories listing residue i, in memory order (fix_backbone.cpp:772-789)
+  std::vector<std::vector<int>> listed(n);
+  for (int k = 0; k < (int) mems.size(); k++)
+    for (int i = mems[k].pos; i < mems[k].pos + mems[k].len - min_sep; i++) listed[i].push_back(k);
+  auto dist = [](const double *a, const double *b) {
+    return sqrt((a[0] - b[0]) * (a[0] - b[0]) + (a[1] - b[1]) * (a[1] - b[1]) + (a[2] - b[2]) * (a[2] - b[2]));
+  };
+  const double w = ff.tb_width;
+  for (int i = 0; i < n; i++)
+    for (int km : listed[i]) {
+      const Memory &m = mems[km];
+      const double ekw = p.epsilon * p.k_fm * m.weight;
+      const int js = i + min_sep;
+      int je = m.pos + m.len - 1;
+      if (max_sep != -1) je = std::min(je, i + max_sep);
+      if (je >= n) fail("Missing residues in memory potential");
+      for (int j = js; j <= je; j++) {
+        double sig_sq = pow((double) abs(i - j), 2 * p.fm_sigma_exp);
+        sig_sq = sig_sq * w * w;
+        const int li = i - m.pos, lj = j - m.pos;
+        const char mi = m.se[li], mj = m.se[lj];
+        const double ekwg = ekw * G.get(top.res_type[i], top.res_type[j], residue_code(mi), residue_code(mj), i, j);
+        // atom pairs CA-CA, CA-CB, CB-CA, CB-CB and their memory distances
+        const double rf[4] = {dist(&m.xca[3 * li], &m.xca[3 * lj]), dist(&m.xca[3 * li], &m.xcb[3 * lj]),
+                              dist(&m.xca[3 * lj], &m.xcb[3 * li]), dist(&m.xcb[3 * lj], &m.xcb[3 * li])};
+        const bool gi = top.seq[i] == 'G' || mi == 'G', gj = top.seq[j] == 'G' || mj == 'G';
+        for (int k = 0; k < 4; k++) {
+          if (k >= 2 && gi) continue;
+          if ((k & 1) && gj) continue;
+          const size_t itb = ((size_t) i * out.nbrs + (j - js)) * 4 + k;
+          out.present[itb] = 1;
+          double *t = &out.data[itb * out.size * 2];
+          for (int ir = 0; ir < out.size; ir++) {
+            const double r = p.tb_rmin + ir * p.tb_dr;
+            const double dr = r - rf[k];
+            const double drsq = dr * dr;
+            const double V = -ekwg * exp(-drsq / (2 * sig_sq));
+            t[2 * ir] += V;
+            t[2 * ir + 1] += V * dr / (sig_sq * r);
+          }
+        }
+      }
+    }
+  if (ff.tb_use_file) {
+    // saved for later runs; absent tables as zero rows, infinities as 0
+    FILE *e = fopen(fe.c_str(), "w"), *f = fopen(ff_.c_str(), "w");
+    if (!e || !f) fail("Fragment memory table files not found!");
+    for (size_t itb = 0; itb < ntb; itb++) {
+      for (int ir = 0; ir < out.size; ir++) {
+        double ev = out.present[itb] ? out.data[(itb * out.size + ir) * 2] : 0.0;
+        double fv = out.present[itb] ? out.data[(itb * out.size + ir) * 2 + 1] : 0.0;
+        if (std::isinf(ev)) ev = 0.0;
+        if (std::isinf(fv)) fv = 0.0;
+        fprintf(e, "%.12f ", ev);
+        fprintf(f, "%.12f ", fv);
+      }
+      fprintf(e, "\n");
+      fprintf(f, "\n");
+    }
+    fclose(e);
+    fclose(f);
+  }
+}
+
 void load_shared_forcefield(const std::string &dir, const std::string &coeff_file, const std::string &pair_style,
                             const std::string &pair_coeffs, SharedForceField &out)
 {
@@ -678,12 +795,14 @@ void load_shared_forcefield(const std::string &dir, const std::string &coeff_fil
   p.terms &= ~T_SSW;
   read_tables(dir, out.ff, none);
   p.terms |= ssw;
-  if (p.terms & T_FM) {
+  if (p.terms & (T_FM | T_FM_TABLE)) {
     read_gamma_table(path_in(dir, out.ff.fm_gamma_file), out.gamma);
     p.fm_min_sep = out.gamma.min_sep();
     p.fm_max_sep = out.gamma.max_sep();
     for (int d = 0; d < 64; d++) p.fm_sigma_sq[d] = pow((double) d, 2 * p.fm_sigma_exp);
   }
+  if ((p.terms & T_FM_TABLE) && p.fm_max_sep == -1)
+    fail("Fragment_Memory_Table: replicas given as arrays need a gamma file with a maximum separation");
   out.pair_style = pair_style;
   out.pair_coeffs = pair_coeffs;
 }
@@ -751,7 +870,7 @@ void load_system_arrays(const SharedForceField &sf, const ReplicaArrays &ra, Sys
         if (S.ff.p.ssweight[k]) t.aps[(size_t) k * ra.n_res + r] = ra.ssweight[(size_t) r * ncol + c++];
   }
   // fragment memories
-  if (S.ff.p.terms & T_FM) {
+  if (S.ff.p.terms & (T_FM | T_FM_TABLE)) {
     S.gamma = sf.gamma;
     size_t off = 0;
     for (int m = 0; m < ra.n_mem; m++) {
@@ -767,8 +886,14 @@ void load_system_arrays(const SharedForceField &sf, const ReplicaArrays &ra, Sys
       off += mm.len;
       S.mems.push_back(std::move(mm));
     }
-    build_fm_table(S.ff, t, S.gamma, S.mems, S.fm);
-    S.ff.p.fm_nd = S.fm.nd;
+    if (S.ff.p.terms & T_FM) {
+      build_fm_table(S.ff, t, S.gamma, S.mems, S.fm);
+      S.ff.p.fm_nd = S.fm.nd;
+    }
+    if (S.ff.p.terms & T_FM_TABLE) {
+      build_fm_table_tb(S.ff, t, S.gamma, S.mems, "", S.tb);
+      S.ff.p.tb_nbrs = S.tb.nbrs;
+    }
     S.mems.clear();
     S.mems.shrink_to_fit();
   }
@@ -799,6 +924,7 @@ void assemble_batch(const std::vector<const SystemInput *> &reps, Batch &B)
   auto same_ff = [](const FFParams &a, const FFParams &b) {
     FFParams x = a, y = b;  // rows per residue may differ; everything else must match
     x.fm_nd = y.fm_nd = 0;
+    x.tb_nbrs = y.tb_nbrs = 0;
     return memcmp(&x, &y, sizeof x) == 0;
   };
   for (auto *r : reps) {
@@ -890,6 +1016,16 @@ void assemble_batch(const std::vector<const SystemInput *> &reps, Batch &B)
     coff += t.n_chains;
   }
   B.fm.row_start[(size_t) N * nd] = (int) rec_off;
+  if (B.ff.p.terms & T_FM_TABLE) {
+    B.tb.nbrs = r0.tb.nbrs;
+    B.tb.size = r0.tb.size;
+    for (auto *r : reps) {
+      if (r->tb.nbrs != B.tb.nbrs || r->tb.size != B.tb.size)
+        fail("batch replicas must share one fragment-memory table shape (a gamma file with a maximum separation)");
+      B.tb.data.insert(B.tb.data.end(), r->tb.data.begin(), r->tb.data.end());
+      B.tb.present.insert(B.tb.present.end(), r->tb.present.begin(), r->tb.present.end());
+    }
+  }
   T.n_chains = coff;
   B.ff.p.fm_nd = nd;
   if (!(B.ff.p.terms & T_FM)) B.ff.p.fm_nd = 0;
@@ -1002,14 +1138,24 @@ void load_system_atoms(const std::string &dir, const std::string &coeff_file, co
   set_bonds(S.top, nbonds, bond_a, bond_b, bond_k, bond_r0, ext_to_int.data());
   set_pair_coeffs(S.top, pair_style, pair_coeffs);
   read_tables(dir, S.ff, S.top);
-  if (S.ff.p.terms & T_FM) {
+  if (S.ff.p.terms & (T_FM | T_FM_TABLE)) {
     read_gamma_table(path_in(dir, S.ff.fm_gamma_file), S.gamma);
-    read_memories(dir, S.ff.fm_file, S.top.n_res, S.mems);
+    const bool tb_from_file = (S.ff.p.terms & T_FM_TABLE) && S.ff.tb_use_file && !(S.ff.p.terms & T_FM) &&
+                              file_exists(path_in(dir, "fm_table.energy")) &&
+                              file_exists(path_in(dir, "fm_table.force"));
+    // the reference reads the memories unless the tables come from files (fix_backbone.cpp:758)
+    if (!tb_from_file) read_memories(dir, S.ff.fm_file, S.top.n_res, S.mems);
     S.ff.p.fm_min_sep = S.gamma.min_sep();
     S.ff.p.fm_max_sep = S.gamma.max_sep();
     for (int d = 0; d < 64; d++) S.ff.p.fm_sigma_sq[d] = pow((double) d, 2 * S.ff.p.fm_sigma_exp);
-    build_fm_table(S.ff, S.top, S.gamma, S.mems, S.fm);
-    S.ff.p.fm_nd = S.fm.nd;
+    if (S.ff.p.terms & T_FM) {
+      build_fm_table(S.ff, S.top, S.gamma, S.mems, S.fm);
+      S.ff.p.fm_nd = S.fm.nd;
+    }
+    if (S.ff.p.terms & T_FM_TABLE) {
+      build_fm_table_tb(S.ff, S.top, S.gamma, S.mems, dir, S.tb);
+      S.ff.p.tb_nbrs = S.tb.nbrs;
+    }
   }
   S.x.assign(3 * S.top.n_atoms, 0.0);
   S.v.assign(3 * S.top.n_atoms, 0.0);

@@ -22,7 +22,7 @@ enum Energy {
 enum TermFlag : uint32_t {
   T_CHAIN = 1u << 0, T_CHI = 1u << 1, T_RAMA = 1u << 2, T_RAMA_P = 1u << 3, T_SSW = 1u << 4,
   T_DSSP = 1u << 5, T_PAP = 1u << 6, T_WATER = 1u << 7, T_BURIAL = 1u << 8, T_HELIX = 1u << 9,
-  T_FM = 1u << 10
+  T_FM = 1u << 10, T_FM_TABLE = 1u << 11
 };
 
 // Residue flags
@@ -57,13 +57,20 @@ struct FFParams {
   double h4prob[20], h4prob_pro, helix_sigma_HO_sqinv, helix_sigma_NO_sqinv, helix_HO_zero, helix_NO_zero;
   double k_fm, fm_sigma_exp;
   double fm_sigma_sq[64];  // |i-j|^(2 * fm_sigma_exp) by separation
+  // table fragment memory ([Fragment_Memory_Table]): grid tb_rmin + ir * tb_dr, ir < tb_size
+  double tb_rmin, tb_rmax, tb_dr;
+  int tb_size, tb_nbrs;
 };
 
 struct ForceField {
   FFParams p{};
   std::vector<double> tables;  // TB_SIZE doubles
+  // one memory file, gamma file and strength serve both [Fragment_Memory] and
+  // [Fragment_Memory_Table] (the reference reads them into the same variables)
   std::string fm_file, fm_gamma_file;
   double k_fm_raw = 0.0;
+  double tb_width = 0.0;  // [Fragment_Memory_Table] well width (scales the Gaussian variance)
+  int tb_use_file = 0;    // read the tables from fm_table.energy/.force when present, else write them
   double k_water = 0.0;  // epsilon-scaled [Water] strength, applied to gamma.dat
 };
 
@@ -121,12 +128,25 @@ struct FMTable {
   long long records() const { return row_start.empty() ? 0 : row_start.back(); }
 };
 
+// Table fragment memory (FixBackbone::compute_fragment_memory_table,
+// fix_backbone.cpp:4238-4322): for target residue i, separation slot
+// jo = j - i - min_sep (< nbrs) and atom pair k, the energy and radial-force
+// factor of every memory covering (i, j) summed on the grid r = tb_rmin +
+// ir * tb_dr.  `present` marks the tables the reference allocates (some
+// memory has the atom pair; a table read from files is always present).
+struct FMTableTB {
+  int nbrs = 0, size = 0;
+  std::vector<double> data;      // [n_res][nbrs][4][size][2]: energy, force
+  std::vector<uint8_t> present;  // [n_res][nbrs][4]
+};
+
 struct SystemInput {
   ForceField ff;
   Topology top;
   GammaTable gamma;
   std::vector<Memory> mems;
   FMTable fm;
+  FMTableTB tb;
   std::vector<double> x, v;  // internal order [n_atoms*3]
 };
 
@@ -145,6 +165,9 @@ void set_bonds(Topology &top, int nb, const int *bi, const int *bj, const double
 void set_pair_coeffs(Topology &top, const std::string &style, const std::string &coeffs);
 void build_fm_table(const ForceField &ff, const Topology &top, const GammaTable &g,
                     const std::vector<Memory> &mems, FMTable &out);
+// `dir`: where fm_table.energy / fm_table.force are read or written
+void build_fm_table_tb(const ForceField &ff, const Topology &top, const GammaTable &g,
+                       const std::vector<Memory> &mems, const std::string &dir, FMTableTB &out);
 
 // A system from per-atom arrays in the caller's order (a host code's own
 // atom data: roles 0 CA, 1 CB/H-beta, 2 O, -1 other; residue and molecule
@@ -171,6 +194,7 @@ struct Batch {
   ForceField ff;
   Topology top;       // concatenated topology (ext_of is per replica, see below)
   FMTable fm;         // concatenated fragment-memory rows
+  FMTableTB tb;       // concatenated fragment-memory tables (per residue)
   std::vector<double> x, v;
   std::vector<int> res_sys;              // residue -> replica
   std::vector<int> sys_res_begin, sys_res_end;    // [n_sys]

@@ -128,6 +128,7 @@ struct PersistArgs {
   int stream_warps;  // fragment-memory stream warps per block (the last ones); 1..7
   int ring_warps;    // warps with a shared-memory copy ring (the last ones); the others load into registers
   int fm_units;      // fragment-memory work units of the step (0: term off)
+  int fm_table;      // table fragment memory on
 };
 
 // Fragment-memory units taken from the step's counter until none is left
@@ -204,6 +205,7 @@ template <typename R> __global__ void __launch_bounds__(kStepThreads, 2) k_step(
     ok = grid_sync(b, 5, seen[5], 1, pass_threads, ok, NoSerial{});
     if (ok) {
       hbond_pass(a, p, sp);
+      if (q.fm_table) fm_table_pass(a, p, sp);
       fragmem_take_units(a, p, q, ring, wsm, kbase);
     }
   }

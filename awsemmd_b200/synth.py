@@ -378,10 +378,17 @@ def replica_lengths(n=1024, lo=40, hi=500, seed=3000):
 # --------------------------------------------------------------------------
 # writers (the reference's input formats)
 
-def coeff_text(k_fm=1.0, mem_file="frags.mem", gamma_file="uniform.gamma") -> str:
+def coeff_text(k_fm=1.0, mem_file="frags.mem", gamma_file="uniform.gamma", table=None) -> str:
+    """The repository's parameter file plus a [Fragment_Memory] section, or with
+    table = (rmin, rmax, dr, well_width, use_table_files, sigma_exp) a
+    [Fragment_Memory_Table] section instead."""
     with open(os.path.join(PARAM_DIR, "fix_backbone_coeff.data")) as f:
         base = f.read()
-    return base.rstrip("\n") + f"\n\n[Fragment_Memory]\n{k_fm}\n{mem_file}\n{gamma_file}\n"
+    if table is None:
+        return base.rstrip("\n") + f"\n\n[Fragment_Memory]\n{k_fm}\n{mem_file}\n{gamma_file}\n"
+    rmin, rmax, dr, width, use, sexp = table
+    return base.rstrip("\n") + (f"\n\n[Fragment_Memory_Table]\n{k_fm}\n{mem_file}\n{gamma_file}\n"
+                                 f"{rmin} {rmax} {dr}\n{width}\n{use}\n{sexp}\n")
 
 
 def write_system(sys_: System, outdir: str, with_fm=True) -> dict:

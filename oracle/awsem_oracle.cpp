@@ -92,7 +92,7 @@ enum { ET_TOTAL = 0, ET_CHAIN, ET_SHAKE, ET_CHI, ET_RAMA, ET_VEXCLUDED, ET_DSSP,
 struct Params {
   double epsilon = 1.0;
   bool abc = 0, chain = 0, chi = 0, rama = 0, rama_p = 0, ssw = 0, dssp = 0, pap = 0, water = 0,
-       burial = 0, helix = 0, fm = 0;
+       burial = 0, helix = 0, fm = 0, fm_tb = 0;
   // defaults of fix_backbone.cpp:136-143
   double an = 0.4831806, bn = 0.7032820, cn = -0.1864262;
   double ap = 0.4436538, bp = 0.2352006, cp = 0.3211455;
@@ -122,6 +122,9 @@ struct Params {
          helix_sigma_HO_sqinv = 0, helix_sigma_NO_sqinv = 0;
   double k_fm = 0, fm_sigma_exp = 0.15;
   std::string fm_file, fm_gamma_file;
+  // [Fragment_Memory_Table] (fix_backbone.cpp:310-321)
+  double tb_rmin = 0, tb_rmax = 0, tb_dr = 0, tb_width = 0;
+  int tb_size = 0, tb_use_file = 0;
   double m_anti_HB[20][20][2], m_anti_NHB[20][20][2], m_para_HB[20][20][2], m_para_one[20], m_anti_one[20];
   double water_gamma[5][20][20][2];
   double burial_gamma[20][3];
@@ -290,6 +293,12 @@ struct System {
   GammaArray G;
   std::vector<Memory> mems;
   std::vector<std::vector<int>> fm_map;  // per residue: memories listing it
+  // table fragment memory: [4 * n * tb_nbrs] tables of tb_size points (empty: not allocated)
+  int tb_nbrs = 0;
+  std::vector<std::vector<double>> tb_e, tb_f;
+  bool tb_files() const;
+  void build_tb();
+  void tb_term(int i, double *f);
 
   // topology
   int natoms = 0, n = 0, nch = 0;
@@ -354,7 +363,7 @@ void System::read_coeff(const std::string &path)
   Params &p = P;
   std::string s;
   static const char *unsupported[] = {"[Shake]", "[Excluded]", "[Excluded_P]", "[Excluded_R6]", "[AMH-Go]",
-                                      "[Fragment_Memory_Table]", "[Contact_Restraints]",
+                                      "[Contact_Restraints]",
                                       "[Vector_Fragment_Memory]", "[Solvent_Barrier]", "[Membrane]",
                                       "[Fragment_Frustratometer]", "[Tertiary_Frustratometer]",
                                       "[Nmer_Frustratometer]", "[Phosphorylation]", "[Amylometer]",
@@ -434,6 +443,12 @@ void System::read_coeff(const std::string &path)
     } else if (s == "[Fragment_Memory]") {
       p.fm = 1;
       in >> p.k_fm >> p.fm_file >> p.fm_gamma_file;
+    } else if (s == "[Fragment_Memory_Table]") {
+      p.fm_tb = 1;
+      in >> p.k_fm >> p.fm_file >> p.fm_gamma_file;
+      in >> p.tb_rmin >> p.tb_rmax >> p.tb_dr;
+      p.tb_size = (int) ((p.tb_rmax - p.tb_rmin) / p.tb_dr) + 2;
+      in >> p.tb_width >> p.tb_use_file >> p.fm_sigma_exp;
     } else if (s == "[Epsilon]") {
       in >> p.epsilon;
     } else {
@@ -695,9 +710,82 @@ void System::read_mems()
   }
   G.load(join(workdir, P.fm_gamma_file));
   fm_map.assign(n, {});
+  if (P.fm_tb && !P.fm && tb_files()) return;  // the tables come from files (fix_backbone.cpp:758)
   int min_sep = G.min_sep();
   for (int k = 0; k < (int) mems.size(); k++)
     for (int i = mems[k].pos; i < mems[k].pos + mems[k].len - min_sep; i++) fm_map[i].push_back(k);
+}
+
+bool System::tb_files() const
+{
+  return P.tb_use_file && std::ifstream(join(workdir, "fm_table.energy")).good() &&
+         std::ifstream(join(workdir, "fm_table.force")).good();
+}
+
+/* the FM tables: read_fragment_memory_table (fix_backbone.cpp:4179-4236) or
+   compute_fragment_memory_table (:4238-4322) */
+void System::build_tb()
+{
+  const Params &p = P;
+  if (!fm_map.size()) fm_map.assign(n, {});
+  if (G.min_sep() == 0 && G.max_sep() == 0) G.load(join(workdir, p.fm_gamma_file));
+  tb_nbrs = G.max_sep() != -1 ? G.max_sep() - G.min_sep() + 1 : n - G.min_sep();
+  const size_t ntb = (size_t) 4 * n * tb_nbrs;
+  tb_e.assign(ntb, {});
+  tb_f.assign(ntb, {});
+  if (tb_files()) {
+    for (int pass = 0; pass < 2; pass++) {
+      std::ifstream in(join(workdir, pass ? "fm_table.force" : "fm_table.energy"));
+      size_t ir = 0, itb = 0;
+      double val;
+      while (in >> val) {
+        if (ir != 0 && ir % p.tb_size == 0) {
+          ir = 0;
+          itb++;
+        }
+        if (itb >= ntb) throw std::runtime_error("Fragment memory table file format error!");
+        std::vector<double> &t = pass ? tb_f[itb] : tb_e[itb];
+        if (t.empty()) t.assign(p.tb_size, 0.0);
+        if (pass && tb_e[itb].empty()) tb_e[itb].assign(p.tb_size, 0.0);
+        t[ir++] = val;
+      }
+    }
+    return;
+  }
+  static const int it[4] = {1, 1, 2, 2}, jt[4] = {1, 2, 1, 2};
+  for (int i = 0; i < n; i++)
+    for (int km : fm_map[i]) {
+      const Memory &m = mems[km];
+      double ekw = p.epsilon * p.k_fm * m.weight;
+      int js = i + G.min_sep();
+      int je = m.pos + m.len - 1;
+      if (G.max_sep() != -1) je = std::min(je, i + G.max_sep());
+      if (je >= n) throw std::runtime_error("Missing residues in memory potential");
+      for (int j = js; j <= je; j++) {
+        double sig_sq = pow(abs(i - j), 2 * p.fm_sigma_exp);
+        sig_sq = sig_sq * p.tb_width * p.tb_width;
+        double gam = G.get(type_of(i), type_of(j), aa_index(m.se[i - m.pos]), aa_index(m.se[j - m.pos]), i, j);
+        double ekwg = ekw * gam;
+        for (int k = 0; k < 4; k++) {
+          if (it[k] == 2 && (se[i] == 'G' || m.se[i - m.pos] == 'G')) continue;
+          if (jt[k] == 2 && (se[j] == 'G' || m.se[j - m.pos] == 'G')) continue;
+          size_t itb = (size_t) 4 * tb_nbrs * i + 4 * (j - js) + k;
+          if (tb_e[itb].empty()) {
+            tb_e[itb].assign(p.tb_size, 0.0);
+            tb_f[itb].assign(p.tb_size, 0.0);
+          }
+          double rf = m.rf(i, it[k], j, jt[k]);
+          for (int ir = 0; ir < p.tb_size; ir++) {
+            double r = p.tb_rmin + ir * p.tb_dr;
+            double dr = r - rf;
+            double drsq = dr * dr;
+            double V = -ekwg * exp(-drsq / (2 * sig_sq));
+            tb_e[itb][ir] += V;
+            tb_f[itb][ir] += V * dr / (sig_sq * r);
+          }
+        }
+      }
+    }
 }
 
 /* pair_style vexcluded settings/coeff/init_one (pair_excluded_volume.cpp:175-265) */
@@ -1298,6 +1386,44 @@ void System::fm_term(int i, double *f)
   }
 }
 
+/* table_fragment_memory(i, j) for j = i + min_sep .. min(i + max_sep, the
+   chain's last residue) (fix_backbone.cpp:4325-4429, :7513-7527) */
+void System::tb_term(int i, double *f)
+{
+  const Params &p = P;
+  int jr0 = i + G.min_sep();
+  int jrn = ch_pos1[chain_of[i]] + ch_len[chain_of[i]] - 2;
+  if (G.max_sep() != -1) jrn = std::min(i + G.max_sep(), jrn);
+  static const int it[4] = {1, 1, 2, 2}, jt[4] = {1, 2, 1, 2};
+  for (int j = jr0; j <= jrn; j++) {
+    int tb_j = j - i - G.min_sep();
+    size_t itb0 = (size_t) 4 * tb_nbrs * i + 4 * tb_j;
+    if (tb_e[itb0].empty()) continue;
+    int ia[4] = {ca[i], ca[i], cb[i], cb[i]}, ja[4] = {ca[j], cb[j], ca[j], cb[j]};
+    const double *xi[4] = {&xca[3 * i], &xca[3 * i], &xcb[3 * i], &xcb[3 * i]};
+    const double *xj[4] = {&xca[3 * j], &xcb[3 * j], &xca[3 * j], &xcb[3 * j]};
+    for (int k = 0; k < 4; k++) {
+      if (se[i] == 'G' && it[k] == 2) continue;
+      if (se[j] == 'G' && jt[k] == 2) continue;
+      double dx[3] = {xi[k][0] - xj[k][0], xi[k][1] - xj[k][1], xi[k][2] - xj[k][2]};
+      double r = sqrt(dx[0] * dx[0] + dx[1] * dx[1] + dx[2] * dx[2]);
+      if (!(r >= p.tb_rmin && r <= p.tb_rmax)) throw std::runtime_error("Table Fragment Memory: r is out of computed range.");
+      int ir = int((r - p.tb_rmin) / p.tb_dr);
+      size_t itb = itb0 + k;
+      if (tb_e[itb].empty()) break;
+      if (ir < 0 || ir >= p.tb_size) throw std::runtime_error("Table Fragment Memory: ir is out of range.");
+      double r1 = p.tb_rmin + (double) ir * p.tb_dr, r2 = p.tb_rmin + (double) (ir + 1) * p.tb_dr;
+      double v1 = tb_e[itb][ir], v2 = tb_e[itb][ir + 1];
+      double V = ((v2 - v1) * r + v1 * r2 - v2 * r1) / (r2 - r1);
+      double f1 = tb_f[itb][ir], f2 = tb_f[itb][ir + 1];
+      double ff = ((f2 - f1) * r + f1 * r2 - f2 * r1) / (r2 - r1);
+      E[ET_FRAGMEM] += V;
+      addf(f, ia[k], ff * dx[0], ff * dx[1], ff * dx[2]);
+      addf(f, ja[k], -ff * dx[0], -ff * dx[1], -ff * dx[2]);
+    }
+  }
+}
+
 /* theta of a density well and its radial derivative over r
    (cWell::compute_theta_pair, smart_matrix_lib.h:612-628) */
 inline void well_theta(double r, double rmin_th, double rmax_th, double kappa, double rmin, double rmax,
@@ -1545,6 +1671,7 @@ void System::compute(const double *x, double *f)
     if (!first(i) && !last(i) && p.chi && se[i] != 'G') chi_term(i, f);
     if (!first(i) && !last(i) && p.rama && se[i] != 'G') rama_term(i, f);
     if (p.fm) fm_term(i, f);
+    if (p.fm_tb) tb_term(i, f);
   }
   pair_terms(x, f);
   for (int k = 1; k < NET; k++) E[ET_TOTAL] += E[k];
@@ -1571,7 +1698,8 @@ void *oracle_create(const char *workdir, const char *data_file, const char *coef
     S->read_data(join(S->workdir, data_file));
     build_residues(*S);
     S->read_tables();
-    if (S->P.fm) S->read_mems();
+    if (S->P.fm || S->P.fm_tb) S->read_mems();
+    if (S->P.fm_tb) S->build_tb();
     S->pair_setup(pair_style, pair_coeffs ? pair_coeffs : "");
   } catch (std::exception &e) {
     g_err = e.what();

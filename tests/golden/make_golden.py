@@ -1,7 +1,7 @@
 """Regenerate the golden vectors of tests/golden/*.npz from the reference.
 
 The reference FixBackbone / PairExcludedVolume sources are compiled in place
-against the LAMMPS-API shim (``make -C oracle ref``) and run on three inputs:
+against the LAMMPS-API shim (``make -C oracle ref``) and run on four inputs:
 
 * ``c0``    -- the 100-residue random-coil chain of benchmark configuration 0
                (generated by awsemmd_b200.synth, seed 0);
@@ -11,14 +11,17 @@ against the LAMMPS-API shim (``make -C oracle ref``) and run on three inputs:
                coordinates, one 63-residue fragment memory), copied verbatim
                into tests/golden/r1r69 from
                examples/examples_new/1R69_single_memory, with the default
-               parameter set plus a [Fragment_Memory] section.
+               parameter set plus a [Fragment_Memory] section;
+* ``r1r69tb`` -- the same inputs with fragment memory in its table form
+               ([Fragment_Memory_Table] with that example's settings: k 0.2,
+               grid 0-50 A by 0.01 A, well width 0.1, sigma exponent 0.15).
 
 For each it stores the inputs' hash, the step-0 forces and energies, the
 per-residue pair-pass intermediates and a 20-step Langevin trajectory
 (x, v and per-step thermo rows).  ``c0_nve.npz`` holds the thermo rows of a
 1,000-step constant-energy run (fix nve only, dt 2 fs) of ``c0``: the energy
 drift of the reference.  Run from the repository root with the reference tree
-present:  python tests/golden/make_golden.py
+present:  python tests/golden/make_golden.py [case ...]
 """
 from __future__ import annotations
 
@@ -59,7 +62,7 @@ def write_case(name: str, outdir: str) -> dict:
         return synth.write_system(synth.config_system(0), outdir)
     if name == "sheet":
         return synth.write_system(synth.sheet_system(), outdir)
-    if name == "r1r69":
+    if name in ("r1r69", "r1r69tb"):
         src = os.path.join(GOLDEN, "r1r69")
         os.makedirs(outdir, exist_ok=True)
         for f in os.listdir(src):
@@ -68,19 +71,23 @@ def write_case(name: str, outdir: str) -> dict:
         for t in synth.PARAM_TABLES:
             shutil.copy(os.path.join(synth.PARAM_DIR, t), os.path.join(outdir, t))
         with open(os.path.join(outdir, "fix_backbone_coeff.data"), "w") as fh:
-            fh.write(synth.coeff_text(mem_file="fragsLAMW.mem.single", gamma_file="seq.gamma"))
+            if name == "r1r69":
+                fh.write(synth.coeff_text(mem_file="fragsLAMW.mem.single", gamma_file="seq.gamma"))
+            else:  # the table form and settings of the reference's 1R69 example coefficient file
+                fh.write(synth.coeff_text(k_fm=0.2, mem_file="fragsLAMW.mem.single", gamma_file="seq.gamma",
+                                          table=(0, 50, 0.01, 0.1, 0, 0.15)))
         return {"workdir": outdir, "data": "data.1r69", "coeff": "fix_backbone_coeff.data", "seq": "extended.seq",
                 "pair_style": synth.PAIR_STYLE, "pair_coeffs": ";".join(synth.PAIR_COEFFS)}
     raise KeyError(name)
 
 
-CASES = ["c0", "sheet", "r1r69"]
+CASES = ["c0", "sheet", "r1r69", "r1r69tb"]
 
 
-def main():
+def main(cases=None):
     import ref
 
-    for name in CASES:
+    for name in cases or CASES:
         with tempfile.TemporaryDirectory() as tmp:
             files = write_case(name, os.path.join(tmp, name))
             h = dir_hash(files["workdir"])
@@ -110,4 +117,4 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:] or None)

@@ -12,7 +12,7 @@ from conftest import write_case
 
 pytestmark = pytest.mark.gpu
 
-CASES = ["c0", "sheet", "r1r69"]
+CASES = ["c0", "sheet", "r1r69", "r1r69tb"]
 TOL = {"fp64": (1e-6, 1e-5), "mixed": (1e-5, 1e-4)}
 
 

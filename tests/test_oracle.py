@@ -6,7 +6,7 @@ import pytest
 
 from conftest import REFERENCE_SRC, write_case
 
-CASES = ["c0", "sheet", "r1r69"]
+CASES = ["c0", "sheet", "r1r69", "r1r69tb"]
 
 
 def rel_err(a, b):
