@@ -114,6 +114,8 @@ class EngineBase {
   virtual void autotune(int reps, int *chosen) = 0;
   virtual void set_step_form(int form, int blocks, int stream_warps) = 0;
   virtual void set_launch_shapes(const int *shapes) = 0;
+  virtual void set_neighbor(double skin, int delay, int every, int check) = 0;
+  virtual void set_list_built(int built) = 0;
   virtual void get_step_form(int *out) = 0;
   virtual void model_info(long long *info) = 0;
   virtual double run_ms() const = 0;
@@ -163,6 +165,11 @@ template <typename R> class Engine : public EngineBase {
   DBuf<R> fm_rf, fm_coef;
   DBuf<double> tb_data;            // table fragment memory (energy, force pairs)
   DBuf<unsigned char> tb_present;
+  DBuf<int> go_start, go_partner;  // AMH-Go native contacts
+  DBuf<double> go_rnat, go_gamma, go_sig_sq, go_norm;
+  DBuf<double> go_x0;              // AMH-Go list emulation: positions at the last build
+  DBuf<unsigned char> go_in;       // contacts in that list
+  DBuf<int> go_ago, go_over;       // per replica: steps since the build, half-skin flag
   int fm_groups = 0, fm_dsplit = 1;
   DBuf<double> thermo_rows;
   DBuf<int> res_sys, sys_begin, sys_end;
@@ -261,6 +268,17 @@ template <typename R> class Engine : public EngineBase {
     a.fm.dsplit = fm_dsplit;
     a.tb_data = reinterpret_cast<const double2 *>(tb_data.p);
     a.tb_present = tb_present.p;
+    a.go_start = go_start.p;
+    a.go_partner = go_partner.p;
+    a.go_rnat = go_rnat.p;
+    a.go_gamma = go_gamma.p;
+    a.go_sig_sq = go_sig_sq.p;
+    a.go_norm = go_norm.p;
+    const bool go_on = in.ff.p.terms & T_AMHGO;
+    a.go_x0 = go_on ? go_x0.p : nullptr;
+    a.go_in = go_on ? go_in.p : nullptr;
+    a.go_ago = go_on ? go_ago.p : nullptr;
+    a.go_over = go_on ? go_over.p : nullptr;
     a.groups = groups;
     a.step = dstep.p;
     a.res_sys = res_sys.p;
@@ -354,6 +372,22 @@ template <typename R> class Engine : public EngineBase {
       CK(cudaStreamSynchronize(s0));
       std::vector<double>().swap(in.tb.data);  // the device holds the tables now
     }
+    if (in.ff.p.terms & T_AMHGO) {
+      go_start.upload(in.go.start, s0);
+      go_partner.upload(in.go.partner.empty() ? std::vector<int>{0} : in.go.partner, s0);
+      go_rnat.upload(in.go.rnat.empty() ? std::vector<double>{0.0} : in.go.rnat, s0);
+      go_gamma.upload(in.go.gamma.empty() ? std::vector<double>{0.0} : in.go.gamma, s0);
+      go_sig_sq.upload(in.go.sig_sq.empty() ? std::vector<double>{1.0} : in.go.sig_sq, s0);
+      go_norm.upload(in.go.norm, s0);
+      go_x0.alloc((size_t) 9 * nn);
+      go_x0.zero(s0);
+      go_in.alloc(std::max<size_t>(in.go.partner.size(), 1));
+      go_in.zero(s0);
+      go_ago.alloc((size_t) std::max(n_sys(), 1));
+      go_ago.zero(s0);
+      go_over.alloc((size_t) std::max(n_sys(), 1));
+      go_over.zero(s0);
+    }
     CK(cudaFuncSetAttribute(dev::k_fragmem<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             4 * dev::fm_warp_smem<R>(true)));
     // pair-list radii of the terms
@@ -372,6 +406,12 @@ template <typename R> class Engine : public EngineBase {
         if (t.ev_pref[a * N + b] != 0.0) evmax = std::max(evmax, std::max(t.ev_cl[a * N + b], t.ev_cs[a * N + b]));
     st.r_ev = (float) evmax;
     st.skin = (float) skin;
+    // LAMMPS defaults: neigh_modify delay 0 every 1 check yes
+    st.go_skin = skin;
+    st.go_delay = 0;
+    st.go_every = 1;
+    st.go_check = 1;
+    st.go_force = 1;
     CK(cudaMemcpyAsync(nl.p, &st, sizeof st, cudaMemcpyHostToDevice, s0));
     long long s = step;
     CK(cudaMemcpyAsync(dstep.p, &s, sizeof s, cudaMemcpyHostToDevice, s0));
@@ -501,12 +541,14 @@ template <typename R> class Engine : public EngineBase {
     launch_prepare_and_list(a, s0, false, advance);
     bool fm = (a.groups & dev::G_FIX) && p.fm_nd > 0;
     const bool fmt = (a.groups & dev::G_FIX) && (p.terms & T_FM_TABLE);
-    if (fm || fmt) {
+    const bool go = (a.groups & dev::G_FIX) && (p.terms & T_AMHGO);
+    if (fm || fmt || go) {
       // fragment memory is independent of the pair passes: second stream
       CK(cudaEventRecord(ev_fork, s0));
       CK(cudaStreamWaitEvent(s1, ev_fork, 0));
       if (fm) dev::k_fragmem<R><<<fm_blocks(), tb, fm_smem(), s1>>>(a, p);
       if (fmt) dev::k_fm_table<R><<<fm_table_blocks(), tb, 0, s1>>>(a, p);
+      if (go) dev::k_amh_go<R><<<nb, tb, 0, s1>>>(a, p);
       CK(cudaEventRecord(ev_join, s1));
     }
     dev::k_density<R><<<pair_blocks, tb, 0, s0>>>(a, p);
@@ -514,7 +556,7 @@ template <typename R> class Engine : public EngineBase {
     dev::k_water_xi<R><<<pair_blocks, tb, 0, s0>>>(a, p);
     dev::k_pair<R><<<pair_blocks, tb, 0, s0>>>(a, p);
     dev::k_hbond<R><<<hb_blocks, 128, 0, s0>>>(a, p);
-    if (fm || fmt) CK(cudaStreamWaitEvent(s0, ev_join, 0));
+    if (fm || fmt || go) CK(cudaStreamWaitEvent(s0, ev_join, 0));
   }
 
   int fm_table_blocks() const
@@ -530,6 +572,8 @@ template <typename R> class Engine : public EngineBase {
     if (!(groups & dev::G_FIX) || !(in.ff.p.terms & T_FM) || in.ff.p.fm_nd == 0)
       CK(cudaMemsetAsync(e_res.p + (size_t) E_FRAGMEM * nn, 0, sizeof(double) * nn, s0));
     if (!(groups & dev::G_BOND)) CK(cudaMemsetAsync(e_res.p + (size_t) E_BOND * nn, 0, sizeof(double) * nn, s0));
+    if (!(groups & dev::G_FIX) || !(in.ff.p.terms & T_AMHGO))
+      CK(cudaMemsetAsync(e_res.p + (size_t) E_AMHGO * nn, 0, sizeof(double) * nn, s0));
   }
 
   // energy sums of replicas [rep0, rep0 + count) (all of them by default)
@@ -557,6 +601,11 @@ template <typename R> class Engine : public EngineBase {
     CK(cudaMemcpyAsync(dstep.p, &st, sizeof st, cudaMemcpyHostToDevice, s0));
     step = st;
     zero_unwritten_energies(groups);
+    if (in.ff.p.terms & T_AMHGO) {
+      // the host's MD loop decides whether this evaluation's list is new
+      set_go_flags(next_compute_built, 1);
+      next_compute_built = 1;
+    }
     auto a = args(groups);
     launch_eval(a, false);
     int tb = 256;
@@ -766,7 +815,8 @@ template <typename R> class Engine : public EngineBase {
     const bool fm = fm_on(a);
     dev::PersistArgs q{d_integ.p, g1.p, g2.p, ftot.p, x.p, gbar.p, n_run(), ps_stream,
                        fm ? ps_ring_warps() : 0, fm ? std::min(fm_groups, (n_run() + 31) / 32) * fm_dsplit : 0,
-                       (a.groups & dev::G_FIX) && (in.ff.p.terms & T_FM_TABLE) ? 1 : 0};
+                       (a.groups & dev::G_FIX) && (in.ff.p.terms & T_FM_TABLE) ? 1 : 0,
+                       (a.groups & dev::G_FIX) && (in.ff.p.terms & T_AMHGO) ? 1 : 0};
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(ps_grid_now);
     cfg.blockDim = dim3(dev::kStepThreads);
@@ -795,6 +845,22 @@ template <typename R> class Engine : public EngineBase {
   }
 
   // shapes as awsem_autotune reports them: [dsplit, pair blocks, hbond blocks, fragmem blocks]
+  void set_neighbor(double skin_, int delay, int every, int check) override
+  {
+    if (delay < 0 || every < 1 || (check != 0 && check != 1))
+      throw std::invalid_argument("neigh_modify: delay >= 0, every >= 1, check 0 or 1");
+    if (skin_ > 0 && skin_ != skin) {
+      skin = skin_;
+      set_nl_field(&dev::NLState::skin, (float) skin);
+      set_nl_field(&dev::NLState::go_skin, skin);
+      set_nl_field(&dev::NLState::r_list, 0.f);  // the next evaluation rebuilds the pair list
+    }
+    set_nl_field(&dev::NLState::go_delay, delay);
+    set_nl_field(&dev::NLState::go_every, every);
+    set_nl_field(&dev::NLState::go_check, check);
+    CK(cudaStreamSynchronize(s0));
+  }
+
   void set_launch_shapes(const int *sh) override
   {
     const int nd = std::max(in.ff.p.fm_nd, 1);
@@ -998,6 +1064,7 @@ template <typename R> class Engine : public EngineBase {
           case 8:
             if (fm) dev::k_fragmem<R><<<fm_blocks(), tb, fm_smem(), s0>>>(a, p);
             if (p.terms & T_FM_TABLE) dev::k_fm_table<R><<<fm_table_blocks(), tb, 0, s0>>>(a, p);
+            if (p.terms & T_AMHGO) dev::k_amh_go<R><<<nb, tb, 0, s0>>>(a, p);
             break;
           case 9: dev::k_finish<R><<<nb, tb, 0, s0>>>(a, d_integ.p, g1.p, g2.p, ftot.p, x.p); break;
         }
@@ -1177,7 +1244,11 @@ template <typename R> class Engine : public EngineBase {
     if (rp.skin > 0 && rp.skin != skin) {
       skin = rp.skin;
       set_nl_field(&dev::NLState::skin, (float) skin);
+      set_nl_field(&dev::NLState::go_skin, skin);
     }
+    // a run's first evaluation is its setup: LAMMPS builds every list there;
+    // the engine decides the later builds
+    if (!cont && (in.ff.p.terms & T_AMHGO)) set_go_flags(1, 0);
     if (rp.neigh_every != neigh_every) {
       neigh_every = rp.neigh_every;
       set_nl_field(&dev::NLState::every, neigh_every);
@@ -1245,6 +1316,20 @@ template <typename R> class Engine : public EngineBase {
       cont_wend = wend;
     }
   }
+
+  int next_compute_built = 1;  // awsem_set_list_built: the next awsem_compute's list is new
+
+  void set_go_flags(int force, int host)
+  {
+    dev::NLState st;
+    CK(cudaMemcpyAsync(&st, nl.p, sizeof st, cudaMemcpyDeviceToHost, s0));
+    CK(cudaStreamSynchronize(s0));
+    st.go_force = force;
+    st.go_host = host;
+    CK(cudaMemcpyAsync(nl.p, &st, sizeof st, cudaMemcpyHostToDevice, s0));
+  }
+
+  void set_list_built(int built) override { next_compute_built = built ? 1 : 0; }
 
   template <typename F> void set_nl_field(F dev::NLState::*field, F value)
   {
@@ -1377,6 +1462,7 @@ template <typename R> class Engine : public EngineBase {
     if (dt <= 0 || damp <= 0) throw std::invalid_argument("dt and damp must be positive");
     if (f.ff.p.terms & T_FM_TABLE)
       throw std::invalid_argument("serving handles do not support [Fragment_Memory_Table] (use [Fragment_Memory])");
+    if (f.ff.p.terms & T_AMHGO) throw std::invalid_argument("serving handles do not support [AMH-Go]");
     const long long groups = (cap_res + 31) / 32;
     if (groups * 32 * pairs_per_res >= (1ll << 31)) throw std::invalid_argument("residue capacity too large");
     sf = &f;
@@ -1725,6 +1811,8 @@ template <typename R> class Engine : public EngineBase {
     add(pos), add(cb_build), add(facc), add(pairs), add(ncount), add(hbq), add(dacc), add(e_fix), add(nl), add(dstep);
     add(ev_pref), add(ev_cs), add(ev_cl), add(excl_self), add(excl_next), add(bond_i), add(bond_j), add(bond_k);
     add(bond_r0), add(fm_soff), add(fm_slen), add(fm_rf), add(fm_coef), add(tb_data), add(tb_present);
+    add(go_start), add(go_partner), add(go_rnat), add(go_gamma), add(go_sig_sq), add(go_norm);
+    add(go_x0), add(go_in), add(go_ago), add(go_over);
     add(thermo_rows), add(res_sys), add(sys_begin);
     add(sys_end), add(sys_seed), add(slot_run), add(d_integ);
     return b;
@@ -2168,6 +2256,18 @@ int awsem_set_step_form(awsem_system *sys, int form, int blocks, int stream_warp
     CK(cudaSetDevice(sys->eng->device));
     sys->eng->set_step_form(form, blocks, stream_warps);
   });
+}
+
+int awsem_set_neighbor(awsem_system *sys, double skin, int delay, int every, int check)
+{
+  if (!ready(sys)) return AWSEM_EINVAL;
+  return guarded([&] { sys->eng->set_neighbor(skin, delay, every, check); });
+}
+
+int awsem_set_list_built(awsem_system *sys, int built)
+{
+  if (!ready(sys) || (built != 0 && built != 1)) return AWSEM_EINVAL;
+  return guarded([&] { sys->eng->set_list_built(built); });
 }
 
 int awsem_set_launch_shapes(awsem_system *sys, const int *shapes)

@@ -49,6 +49,13 @@ struct NLState {
   int npairs;         // pairs in the residue pair list (may exceed its capacity: overflow)
   int fm_timeout;     // a fragment-memory stream wait gave up (results invalid)
   int tb_error;       // table fragment memory: 1 a distance outside the table's range, 2 a grid index outside it
+  // AMH-Go reads the fix's full neighbour list, whose membership is fixed at
+  // each LAMMPS list build: that list's rebuild rule is emulated per replica
+  double go_skin;     // neighbor skin (A)
+  int go_delay, go_every, go_check;  // neigh_modify delay / every / check
+  int go_force;       // host: the next evaluation is a run setup (the list is built)
+  int go_setup;       // this evaluation is a run setup
+  int go_host;        // the host decides the builds (awsem_compute): go_setup alone
 };
 
 // Run window of one replica: integrated over steps begin..end (the
@@ -99,6 +106,12 @@ template <typename R> struct StepArgs {
   // table fragment memory: [n_res][tb_nbrs][4][tb_size] (energy, force) and the tables present
   const double2 *tb_data;
   const unsigned char *tb_present;
+  // AMH-Go native contacts per CA / CB atom slot 2 r + b ([2 n_res + 1] offsets), per residue normalisation
+  const int *go_start, *go_partner;
+  const double *go_rnat, *go_gamma, *go_sig_sq, *go_norm;
+  double *go_x0;                 // [9 n]: positions at the replica's last list build
+  unsigned char *go_in;          // per contact: in the list since that build
+  int *go_ago, *go_over;         // per replica: steps since the build; an atom moved over half the skin
   int groups;       // AWSEM_TERMS_* bits: 1 fix backbone, 2 pair vexcluded, 4 bonds
   long long *step;   // device step counter (advanced by k_nl_decide)
   // replicas: residue -> replica, replica residue ranges, Langevin seeds
@@ -161,6 +174,19 @@ template <typename R> __device__ __forceinline__ void prepare_pass(const StepArg
         double ca1 = x[(3 * (r + 1) + 0) * 3 + k];
         cp[k] = __dadd_rn(__dadd_rn(__dmul_rn(p.ap, ca[k]), __dmul_rn(p.bp, ca1)), __dmul_rn(p.cp, o[k]));
       }
+    }
+    if (a.go_x0) {
+      // LAMMPS check_distance for the AMH-Go list: an atom farther than half
+      // the skin from where it was at the last build
+      const double trig = 0.25 * a.nl->go_skin * a.nl->go_skin;
+      const double *h = a.go_x0 + (size_t) 9 * r;
+      bool over = false;
+      for (int b = 0; b < 3; b++) {
+        const double *q = b == 0 ? ca : b == 1 ? cb : o;
+        const double dx = q[0] - h[3 * b], dy = q[1] - h[3 * b + 1], dz = q[2] - h[3 * b + 2];
+        if (dx * dx + dy * dy + dz * dz > trig) over = true;
+      }
+      if (over) a.go_over[a.res_sys[r]] = 1;
     }
     double4 *w = const_cast<double4 *>(a.s.pos) + (size_t) r * N_BEADS;
     w[B_CA] = make_double4(ca[0], ca[1], ca[2], 0.0);
@@ -254,6 +280,8 @@ __device__ __forceinline__ void nl_decide(NLState *nl, int force, long long *ste
   s.dssp_pre_sq = dpre * dpre;
   s.d2max = s.bO = s.bN = s.bCA = s.bAll = s.bCAx = s.bNCA = 0.f;
   s.n_dssp = s.n_pap = 0;
+  s.go_setup = s.go_force;
+  s.go_force = 0;
 }
 
 __global__ void k_nl_decide(NLState *nl, int force, long long *step) { nl_decide(nl, force, step); }
@@ -1010,6 +1038,87 @@ template <typename R> __device__ __forceinline__ void fm_table_pass(const StepAr
 
 template <typename R> __global__ void k_fm_table(StepArgs<R> a, FFParams p) { fm_table_pass(a, p, grid_span()); }
 
+// LAMMPS Neighbor::decide() for the fix's full list of replica `rep`: the
+// list is built at a run setup; otherwise `ago` counts the steps since the
+// last build and the list is rebuilt once ago >= delay and ago % every == 0,
+// unconditionally without check, with check only if an atom has moved more
+// than half the skin since that build.  Read by the AMH-Go pass and by the
+// replica's first residue in the finish pass, which then advances the state.
+template <typename R> __device__ __forceinline__ bool go_list_build(const StepArgs<R> &a, int rep)
+{
+  const NLState &nl = *a.nl;
+  if (nl.go_setup) return true;
+  if (nl.go_host) return false;
+  const int ago = a.go_ago[rep] + 1;
+  if (ago < nl.go_delay || ago % nl.go_every != 0) return false;
+  return !nl.go_check || a.go_over[rep] != 0;
+}
+
+// AMH-Go (FixBackbone::compute_amh_go_model, fix_backbone.cpp:3856-3992) of
+// residue r's CA and CB: over each atom's native contacts (the full-list
+// partners with a native distance below rc) that are in the fix's full
+// neighbour list -- pairs within the pair-list cutoff plus the skin at the
+// list's last build, which a build step records -- and whose deviation passes
+// dr^2 < 27.6 sigma^2, E_i = sum gamma exp(-dr^2 / 2 sigma^2); the atom's
+// energy is -k E_i^p / (2 a) and each contact's force is scaled by
+// -k p E_i^(p-1) / (2 a) (a: the normalisation).  FP64 in both forms; forces
+// to fixed point, the energy to the residue's slot.
+template <typename R> __device__ __forceinline__ void amh_go_residue(const StepArgs<R> &a, const FFParams &p, int r)
+{
+  const DevSys<R> &s = a.s;
+  const bool build = go_list_build(a, a.res_sys[r]);
+  const double cut = p.pair_list_cutoff + a.nl->go_skin, cutsq = cut * cut;
+  if (build)
+    for (int k = 0; k < 9; k++) a.go_x0[(size_t) 9 * r + k] = a.x[(size_t) 9 * r + k];
+  double E = 0.0;
+  for (int b = 0; b < 2; b++) {
+    const int c0 = a.go_start[2 * r + b], c1 = a.go_start[2 * r + b + 1];
+    if (c0 == c1) continue;
+    const V3<double> xi = bead(s, r, b ? B_CB : B_CA);
+    double Ei = 0.0;
+    for (int c = c0; c < c1; c++) {
+      const int q = a.go_partner[c];
+      const V3<double> xj = bead(s, q / 3, (q % 3) ? B_CB : B_CA);
+      const V3<double> dx = {xi.x - xj.x, xi.y - xj.y, xi.z - xj.z};
+      const double rsq = norm2(dx);
+      if (build) a.go_in[c] = rsq < cutsq;
+      if (!a.go_in[c]) continue;
+      const double dr = sqrt(rsq) - a.go_rnat[c], drsq = dr * dr, sig_sq = a.go_sig_sq[c];
+      if (drsq < 27.6 * sig_sq) Ei += a.go_gamma[c] * exp(-drsq / (2.0 * sig_sq));
+    }
+    const double factor = -0.5 * p.k_amh_go * p.amh_go_p * pow(Ei, p.amh_go_p - 1) / a.go_norm[r];
+    double fi[3] = {0.0, 0.0, 0.0};
+    for (int c = c0; c < c1; c++) {
+      if (!a.go_in[c]) continue;
+      const int q = a.go_partner[c];
+      const V3<double> xj = bead(s, q / 3, (q % 3) ? B_CB : B_CA);
+      const V3<double> dx = {xi.x - xj.x, xi.y - xj.y, xi.z - xj.z};
+      const double rr = sqrt(norm2(dx)), dr = rr - a.go_rnat[c], drsq = dr * dr, sig_sq = a.go_sig_sq[c];
+      if (!(drsq < 27.6 * sig_sq)) continue;
+      const double Eij = a.go_gamma[c] * exp(-drsq / (2.0 * sig_sq));
+      const double force = Eij * dr / (sig_sq * rr);
+      fi[0] += force * dx.x;
+      fi[1] += force * dx.y;
+      fi[2] += force * dx.z;
+      const long long fj[3] = {fix_force(factor * (-force * dx.x)), fix_force(factor * (-force * dx.y)),
+                               fix_force(factor * (-force * dx.z))};
+      scatter_fix(s, q / 3, (q % 3) ? B_CB : B_CA, fj);
+    }
+    const long long fq[3] = {fix_force(factor * fi[0]), fix_force(factor * fi[1]), fix_force(factor * fi[2])};
+    scatter_fix(s, r, b ? B_CB : B_CA, fq);
+    E += -0.5 * p.k_amh_go * pow(Ei, p.amh_go_p) / a.go_norm[r];
+  }
+  a.e_res[(size_t) E_AMHGO * s.n_res + r] = E;
+}
+
+template <typename R> __device__ __forceinline__ void amh_go_pass(const StepArgs<R> &a, const FFParams &p, Span sp)
+{
+  for (int r = sp.t; r < a.n_run; r += sp.nthr)
+    if (a.res_sys[r] >= 0) amh_go_residue(a, p, r);
+}
+
+template <typename R> __global__ void k_amh_go(StepArgs<R> a, FFParams p) { amh_go_pass(a, p, grid_span()); }
+
 __device__ __forceinline__ uint64_t mix64(uint64_t z)
 {
   z += 0x9E3779B97F4A7C15ULL;
@@ -1049,6 +1158,12 @@ __device__ __forceinline__ void finish_one(const StepArgs<R> &a, const Integrato
   const SlotRun sr = a.slot_run[rep];
   if (step < sr.begin || step > sr.end) return;
   const bool final_kick = step > sr.begin, next = step < sr.end && step < in.stop;
+  if (a.go_ago && r == a.sys_begin[rep]) {
+    // the AMH-Go list state moves on once every reader of this step is done
+    const bool built = go_list_build(a, rep);
+    a.go_ago[rep] = built ? 0 : a.go_ago[rep] + 1;
+    a.go_over[rep] = 0;
+  }
   const unsigned long long seed = a.sys_seed[rep];
   const long long key = step - sr.step0;  // the replica's own step count keys its noise
   // Every multiply and add below is rounded on its own (no contraction), as

@@ -19,6 +19,7 @@
 #include <cstring>
 #include <fstream>
 #include <map>
+#include <set>
 #include <sstream>
 #include <stdexcept>
 
@@ -82,13 +83,15 @@ void read_coeff_file(const std::string &path, ForceField &ff)
   const int i_rp = 6;  // first proline Ramachandran well
   double k_rama = 0.0, k_water = 0.0;
   static const char *outside[] = {
-      "[Shake]", "[Excluded]", "[Excluded_P]", "[Excluded_R6]", "[AMH-Go]",
+      "[Shake]", "[Excluded]", "[Excluded_P]", "[Excluded_R6]",
       "[Contact_Restraints]", "[Vector_Fragment_Memory]", "[Solvent_Barrier]", "[Membrane]",
       "[Fragment_Frustratometer]", "[Tertiary_Frustratometer]", "[Nmer_Frustratometer]", "[Phosphorylation]",
       "[Amylometer]", "[Selection_Temperature]", "[Monte_Carlo_Seq_Opt]", "[Optimization]",
       "[Burial_Optimization]", "[DebyeHuckel]", "[DebyeHuckel_Optimization]", "[Shuffler]", "[Mutate_Sequence]"};
-  std::string s;
-  while (in >> s) {
+  std::string s, pending;
+  // a section that omits a trailing value leaves its successor's header as the
+  // next token (`pending`)
+  while (!pending.empty() ? (s = pending, pending.clear(), true) : (bool) (in >> s)) {
     if (s == "[ABC]") {
       in >> p.an >> p.bn >> p.cn >> p.ap >> p.bp >> p.cp >> p.ah >> p.bh >> p.ch;
     } else if (s == "[Chain]") {
@@ -153,9 +156,23 @@ void read_coeff_file(const std::string &path, ForceField &ff)
           p.helix_treshold >> p.helix_i_diff >> p.helix_cutoff >> p.helix_rmin >> p.helix_rmax;
       for (int j = 0; j < 20; j++) in >> p.h4prob[j];
       in >> p.pro_acc_flag >> p.h4prob_pro >> sHO >> sNO >> p.helix_HO_zero >> p.helix_NO_zero;
+      p.helix_sigma_HO = sHO;
+      p.helix_sigma_NO = sNO;
       p.helix_cutoff_sq = p.helix_cutoff * p.helix_cutoff;
       p.helix_sigma_HO_sqinv = 1.0 / (sHO * sHO);
       p.helix_sigma_NO_sqinv = 1.0 / (sNO * sNO);
+    } else if (s == "[AMH-Go]") {
+      // fix_backbone.cpp:297-303
+      p.terms |= T_AMHGO;
+      in >> p.k_amh_go >> p.amh_go_p >> p.amh_go_rc;
+      std::string t;
+      ff.amh_go_censor = 0;
+      if (in >> t) {
+        if (t[0] == '[') pending = t;  // the censoring flag is absent (older coefficient files)
+        else ff.amh_go_censor = atoi(t.c_str());
+      }
+      if (ff.amh_go_censor == 2)
+        fail("AMH-Go: frustration censoring 2 (native distances from go_rnative*.dat) is not supported");
     } else if (s == "[Fragment_Memory]") {
       p.terms |= T_FM;
       in >> ff.k_fm_raw >> ff.fm_file >> ff.fm_gamma_file;
@@ -185,6 +202,7 @@ void read_coeff_file(const std::string &path, ForceField &ff)
   for (int j = 0; j < p.n_rama; j++) p.w[j] *= k_rama;
   for (int j = 0; j < p.n_rama_p; j++) p.w[j + i_rp] *= k_rama;
   p.k_fm = ff.k_fm_raw;
+  p.k_amh_go *= p.epsilon;
   // density-well supports (smart_matrix_lib.h:363-368) and P_AP saturation (:110-115)
   for (int k = 0; k < p.n_wells; k++) {
     p.w_rmin_th[k] = p.well_rmin[k] - 8.0 * 2.302585 / p.water_kappa;
@@ -205,6 +223,34 @@ void read_coeff_file(const std::string &path, ForceField &ff)
   }
   ff.k_water = k_water;
   ff.tables.assign(TB_SIZE, 0.0);
+  p.pair_list_cutoff = pair_list_cutoff(p);
+}
+
+double pair_list_cutoff(const FFParams &p)
+{
+  double cut = 8.0;  // fix_backbone.cpp:1051-1057
+  if (p.terms & T_DSSP) cut = std::max(cut, p.dssp_cut);
+  if (p.terms & T_PAP) cut = std::max(cut, sqrt(p.pap_cutoff_sq));
+  if (p.terms & T_WATER)
+    for (int k = 0; k < p.n_wells; k++) cut = std::max(cut, p.w_rmax_th[k]);
+  if (p.terms & T_HELIX) {
+    cut = std::max(cut, p.h_rmax_th);
+    // calc_exp_helix_cutoff (:1074-1103): O(i) to the atoms behind the virtual N(j) and H(j)
+    const double r0[3] = {3.77, 2.5, 2.41};
+    double r1[3], r2[3];
+    r1[0] = sqrt(pow(p.an * r0[0], 2) + pow(p.cn * r0[1], 2) + p.an * p.cn * (r0[0] * r0[0] + r0[1] * r0[1] - r0[2] * r0[2]));
+    r1[1] = sqrt(pow(p.an * r0[2], 2) + pow(p.bn * r0[1], 2) + p.an * p.bn * (r0[2] * r0[2] + r0[1] * r0[1] - r0[0] * r0[0]));
+    r1[2] = sqrt(pow(p.bn * r0[0], 2) + pow(p.cn * r0[2], 2) + p.bn * p.cn * (r0[0] * r0[0] + r0[2] * r0[2] - r0[1] * r0[1]));
+    r2[0] = sqrt(pow(p.ah * r0[0], 2) + pow(p.ch * r0[1], 2) + p.ah * p.ch * (r0[0] * r0[0] + r0[1] * r0[1] - r0[2] * r0[2]));
+    r2[1] = sqrt(pow(p.ah * r0[2], 2) + pow(p.bh * r0[1], 2) + p.ah * p.bh * (r0[2] * r0[2] + r0[1] * r0[1] - r0[0] * r0[0]));
+    r2[2] = sqrt(pow(p.bh * r0[0], 2) + pow(p.ch * r0[2], 2) + p.bh * p.ch * (r0[0] * r0[0] + r0[2] * r0[2] - r0[1] * r0[1]));
+    double r1_max = std::max(r1[0], std::max(r1[1], r1[2])), r2_max = std::max(r2[0], std::max(r2[1], r2[2]));
+    r1_max = 1.1 * r1_max + p.helix_NO_zero + p.helix_sigma_NO * sqrt(6.0 * log(10.0));
+    r2_max = 1.1 * r2_max + p.helix_HO_zero + p.helix_sigma_HO * sqrt(6.0 * log(10.0));
+    cut = std::max(cut, std::max(r1_max, r2_max));
+    cut = std::max(cut, p.helix_cutoff);
+  }
+  return cut;
 }
 
 void read_sequence(const std::string &path, Topology &top)
@@ -391,6 +437,53 @@ void read_gamma_table(const std::string &path, GammaTable &G)
   }
 }
 
+// CA / CB coordinates (nm -> A) and residue names of residues fpos+1 ..
+// fpos+len of a .gro file (Fragment_Memory::loadGro, fragment_memory.cpp:
+// 34-176); m.len and m.pos are set by the caller.
+static void load_gro(const std::string &path, int fpos, Memory &m, const std::string &open_msg,
+                     const std::string &who)
+{
+  m.se.assign(m.len, '-');
+  m.xca.assign((size_t) m.len * 3, 0.0);
+  m.xcb.assign((size_t) m.len * 3, 0.0);
+  FILE *g = fopen(path.c_str(), "r");
+  if (!g) fail(open_msg);
+  char title[256];
+  int nat = 0, nca = 0;
+  if (!fgets(title, sizeof title, g) || fscanf(g, "%d", &nat) != 1) {
+    fclose(g);
+    fail(who + ": Wrong atom count in memory structure file");
+  }
+  for (int a = 0; a < nat; a++) {
+    int ires, iat;
+    char rn[32], an[32];
+    double x, y, z;
+    if (fscanf(g, "%d %31s %31s %d %lf %lf %lf", &ires, rn, an, &iat, &x, &y, &z) != 7) break;
+    if (ires > fpos + m.len) break;
+    if (ires <= fpos) continue;
+    int r = ires - fpos - 1;
+    double *dst = nullptr;
+    if (!strcmp(an, "CA")) {
+      m.se[r] = residue_from_three(rn);
+      if (m.se[r] == '?') {
+        fclose(g);
+        fail(who + ": Unknown residue");
+      }
+      dst = &m.xca[3 * r];
+      nca++;
+    } else if (!strcmp(an, "CB")) {
+      dst = &m.xcb[3 * r];
+    }
+    if (dst) {
+      dst[0] = x * 10;
+      dst[1] = y * 10;
+      dst[2] = z * 10;
+    }
+  }
+  fclose(g);
+  if (nca != m.len) fail(who + ": Wrong atom count in memory structure file");
+}
+
 void read_memories(const std::string &dir, const std::string &mem_file, int n_res, std::vector<Memory> &mems)
 {
   FILE *f = fopen(path_in(dir, mem_file).c_str(), "r");
@@ -414,45 +507,7 @@ void read_memories(const std::string &dir, const std::string &mem_file, int n_re
       m.len = atoi(t[3].c_str());
       m.weight = atof(t[4].c_str());
       if (m.len <= 0) fail("Fragment_Memory: Incorrectly defined memory fragment");
-      m.se.assign(m.len, '-');
-      m.xca.assign((size_t) m.len * 3, 0.0);
-      m.xcb.assign((size_t) m.len * 3, 0.0);
-      FILE *g = fopen(path_in(dir, t[0]).c_str(), "r");
-      if (!g) fail("Fragment_Memory: Cannot read the file");
-      char title[256];
-      int nat = 0, nca = 0;
-      if (!fgets(title, sizeof title, g) || fscanf(g, "%d", &nat) != 1) {
-        fclose(g);
-        fail("Fragment_Memory: Wrong atom count in memory structure file");
-      }
-      for (int a = 0; a < nat; a++) {
-        int ires, iat;
-        char rn[32], an[32];
-        double x, y, z;
-        if (fscanf(g, "%d %31s %31s %d %lf %lf %lf", &ires, rn, an, &iat, &x, &y, &z) != 7) break;
-        if (ires > fpos + m.len) break;
-        if (ires <= fpos) continue;
-        int r = ires - fpos - 1;
-        double *dst = nullptr;
-        if (!strcmp(an, "CA")) {
-          m.se[r] = residue_from_three(rn);
-          if (m.se[r] == '?') {
-            fclose(g);
-            fail("Fragment_Memory: Unknown residue");
-          }
-          dst = &m.xca[3 * r];
-          nca++;
-        } else if (!strcmp(an, "CB")) {
-          dst = &m.xcb[3 * r];
-        }
-        if (dst) {
-          dst[0] = x * 10;
-          dst[1] = y * 10;
-          dst[2] = z * 10;
-        }
-      }
-      fclose(g);
-      if (nca != m.len) fail("Fragment_Memory: Wrong atom count in memory structure file");
+      load_gro(path_in(dir, t[0]), fpos, m, "Fragment_Memory: Cannot read the file", "Fragment_Memory");
       if (m.pos + m.len > n_res) fail("read_mems: Fragment_Memory: Incorrectly defined memory fragment");
       mems.push_back(std::move(m));
     } else if (state == NONE) {
@@ -785,6 +840,94 @@ void build_fm_table_tb(const ForceField &ff, const Topology &top, const GammaTab
   }
 }
 
+// FixBackbone::compute_amhgo_normalization (fix_backbone.cpp:3787-3848) and
+// the contact selection of compute_amh_go_model (:3850-3992), with the
+// native structure Fragment_Memory(0, 0, n, 1.0, "amh-go.gro") (:695-742).
+void build_amh_go(const ForceField &ff, const Topology &top, const std::string &dir, AmhGoContacts &out)
+{
+  const FFParams &p = ff.p;
+  const int n = top.n_res;
+  GammaTable G;
+  try {
+    read_gamma_table(path_in(dir, "amh-go.gamma"), G);
+  } catch (std::exception &e) {
+    std::string m = e.what();
+    fail(m.find("Cannot read") != std::string::npos ? std::string("Cannot read file amh-go.gamma")
+                                                     : "AMH_Go" + m.substr(m.find(':')));
+  }
+  if (G.frag_resty) fail("AMH-Go: Wrong call of getGamma() function");
+  Memory nat;
+  nat.pos = 0;
+  nat.len = n;
+  load_gro(path_in(dir, "amh-go.gro"), 0, nat, "Cannot read file amh-go.gro", "AMH_Go");
+  std::vector<uint8_t> censored;
+  if (ff.amh_go_censor == 1) {
+    censored.assign((size_t) n * n, 0);
+    std::ifstream cf(path_in(dir, "frustration_censored_contacts.dat"));
+    int a, b;
+    while (cf >> a >> b)
+      if (a >= 1 && a <= n && b >= 1 && b <= n) censored[(size_t) (a - 1) * n + (b - 1)] = 1;
+  }
+  // native distance of atom ia (0 CA, 1 CB) of residue i and atom ja of j
+  // (Fragment_Memory::Rf: CA-CA, CB-CB, CA-CB distances of the structure)
+  auto rnative = [&](int i, int ia, int j, int ja) {
+    const double *a = ia ? &nat.xcb[3 * i] : &nat.xca[3 * i];
+    const double *b = ja ? &nat.xcb[3 * j] : &nat.xca[3 * j];
+    if (ia == ja && i > j) std::swap(a, b);
+    if (ia != ja && ia == 1) std::swap(a, b);  // the CA-CB table is indexed (CA residue, CB residue)
+    return sqrt((a[0] - b[0]) * (a[0] - b[0]) + (a[1] - b[1]) * (a[1] - b[1]) + (a[2] - b[2]) * (a[2] - b[2]));
+  };
+  const int min_sep = G.min_sep();
+  // normalisation a = (1 / 8N) sum over atoms i of |sum over native contacts
+  // of gamma|^p; the power is taken after each partner chain, of the running
+  // sum (the reference's loop nesting), and N is the last chain's last residue
+  double norm = 0.0;
+  for (int i = 0; i < n; i++)
+    for (int ia = 0; ia <= (top.seq[i] == 'G' ? 0 : 1); ia++) {
+      double normi = 0.0;
+      for (int jc = 0; jc < top.n_chains; jc++) {
+        for (int j = top.chain_start[jc]; j <= top.chain_end[jc]; j++)
+          for (int ja = 0; ja <= (top.seq[j] == 'G' ? 0 : 1); ja++) {
+            if (abs(i - j) < min_sep) continue;
+            if (rnative(i, ia, j, ja) < p.amh_go_rc) normi += G.get(top.res_type[i], top.res_type[j], 0, 0, i, j);
+          }
+        norm += pow(fabs(normi), p.amh_go_p);
+      }
+    }
+  norm /= 8 * (top.chain_end.back() + 1);
+  out.norm.assign(n, norm);
+  // 1-2 bonded atom pairs: absent from the full neighbour list (special_bonds fene)
+  std::set<std::pair<int, int>> bonded;
+  for (size_t b = 0; b < top.bond_i.size(); b++)
+    bonded.insert({std::min(top.bond_i[b], top.bond_j[b]), std::max(top.bond_i[b], top.bond_j[b])});
+  // contacts of each CA / CB atom (the full list's partners, in atom order)
+  out.start.assign((size_t) 2 * n + 1, 0);
+  out.partner.clear();
+  out.rnat.clear();
+  out.gamma.clear();
+  out.sig_sq.clear();
+  for (int i = 0; i < n; i++)
+    for (int ia = 0; ia < 2; ia++) {
+      out.start[2 * i + ia] = (int) out.partner.size();
+      if (ia == 1 && top.seq[i] == 'G') continue;
+      for (int j = 0; j < n; j++)
+        for (int ja = 0; ja < 2; ja++) {
+          if ((ja == 1 && top.seq[j] == 'G') || (i == j && ia == ja)) continue;
+          const bool other = top.res_chain[i] != top.res_chain[j];
+          if (!(abs(i - j) >= min_sep || other)) continue;
+          if (!censored.empty() && (censored[(size_t) i * n + j] || censored[(size_t) j * n + i])) continue;
+          if (bonded.count({std::min(3 * i + ia, 3 * j + ja), std::max(3 * i + ia, 3 * j + ja)})) continue;
+          const double rn = rnative(i, ia, j, ja);
+          if (!(rn < p.amh_go_rc)) continue;
+          out.partner.push_back(3 * j + ja);
+          out.rnat.push_back(rn);
+          out.gamma.push_back(G.get(top.res_type[i], top.res_type[j], 0, 0, i, j));
+          out.sig_sq.push_back(pow(abs(i - j), 0.3));
+        }
+    }
+  out.start[(size_t) 2 * n] = (int) out.partner.size();
+}
+
 void load_shared_forcefield(const std::string &dir, const std::string &coeff_file, const std::string &pair_style,
                             const std::string &pair_coeffs, SharedForceField &out)
 {
@@ -809,6 +952,7 @@ void load_shared_forcefield(const std::string &dir, const std::string &coeff_fil
 
 void load_system_arrays(const SharedForceField &sf, const ReplicaArrays &ra, SystemInput &S)
 {
+  if (sf.ff.p.terms & T_AMHGO) fail("AMH-Go needs a run directory (amh-go.gro, amh-go.gamma): load the replica from files");
   if (ra.n_res <= 0 || ra.n_chains <= 0 || !ra.chain_len || !ra.seq || !ra.x) fail("replica: empty description");
   S.ff = sf.ff;
   Topology &t = S.top;
@@ -1016,6 +1160,21 @@ void assemble_batch(const std::vector<const SystemInput *> &reps, Batch &B)
     coff += t.n_chains;
   }
   B.fm.row_start[(size_t) N * nd] = (int) rec_off;
+  if (B.ff.p.terms & T_AMHGO) {
+    B.go.start.push_back(0);
+    int res_off = 0;
+    for (auto *r : reps) {
+      const AmhGoContacts &g = r->go;
+      const int base = (int) B.go.partner.size();
+      for (size_t k = 1; k < g.start.size(); k++) B.go.start.push_back(base + g.start[k]);
+      for (int q : g.partner) B.go.partner.push_back(q + 3 * res_off);
+      B.go.rnat.insert(B.go.rnat.end(), g.rnat.begin(), g.rnat.end());
+      B.go.gamma.insert(B.go.gamma.end(), g.gamma.begin(), g.gamma.end());
+      B.go.sig_sq.insert(B.go.sig_sq.end(), g.sig_sq.begin(), g.sig_sq.end());
+      B.go.norm.insert(B.go.norm.end(), g.norm.begin(), g.norm.end());
+      res_off += r->top.n_res;
+    }
+  }
   if (B.ff.p.terms & T_FM_TABLE) {
     B.tb.nbrs = r0.tb.nbrs;
     B.tb.size = r0.tb.size;
@@ -1157,6 +1316,7 @@ void load_system_atoms(const std::string &dir, const std::string &coeff_file, co
       S.ff.p.tb_nbrs = S.tb.nbrs;
     }
   }
+  if (S.ff.p.terms & T_AMHGO) build_amh_go(S.ff, S.top, dir, S.go);
   S.x.assign(3 * S.top.n_atoms, 0.0);
   S.v.assign(3 * S.top.n_atoms, 0.0);
   for (int s = 0; s < S.top.n_atoms; s++)

@@ -22,7 +22,7 @@ enum Energy {
 enum TermFlag : uint32_t {
   T_CHAIN = 1u << 0, T_CHI = 1u << 1, T_RAMA = 1u << 2, T_RAMA_P = 1u << 3, T_SSW = 1u << 4,
   T_DSSP = 1u << 5, T_PAP = 1u << 6, T_WATER = 1u << 7, T_BURIAL = 1u << 8, T_HELIX = 1u << 9,
-  T_FM = 1u << 10, T_FM_TABLE = 1u << 11
+  T_FM = 1u << 10, T_FM_TABLE = 1u << 11, T_AMHGO = 1u << 12
 };
 
 // Residue flags
@@ -60,6 +60,10 @@ struct FFParams {
   // table fragment memory ([Fragment_Memory_Table]): grid tb_rmin + ir * tb_dr, ir < tb_size
   double tb_rmin, tb_rmax, tb_dr;
   int tb_size, tb_nbrs;
+  // AMH-Go ([AMH-Go], fix_backbone.cpp:297-303): strength (epsilon-scaled), power, native cutoff;
+  // pairs count only within the reference's fix pair-list cutoff plus the neighbour skin
+  double k_amh_go, amh_go_p, amh_go_rc, pair_list_cutoff;
+  double helix_sigma_HO, helix_sigma_NO;  // as read (the pair-list cutoff uses them)
 };
 
 struct ForceField {
@@ -71,6 +75,7 @@ struct ForceField {
   double k_fm_raw = 0.0;
   double tb_width = 0.0;  // [Fragment_Memory_Table] well width (scales the Gaussian variance)
   int tb_use_file = 0;    // read the tables from fm_table.energy/.force when present, else write them
+  int amh_go_censor = 0;  // [AMH-Go] frustration censoring flag (0 or 1)
   double k_water = 0.0;  // epsilon-scaled [Water] strength, applied to gamma.dat
 };
 
@@ -140,6 +145,19 @@ struct FMTableTB {
   std::vector<uint8_t> present;  // [n_res][nbrs][4]
 };
 
+// AMH-Go (FixBackbone::compute_amh_go_model, fix_backbone.cpp:3850-3992):
+// for atom slot 2 r + b (b = 0 CA, 1 CB) of target residue r, the native
+// contacts it interacts with (the full list's partners j with
+// |r - res(j)| >= min_sep or another molecule, not censored, native distance
+// below rc), each with its native distance, gamma and Gaussian variance
+// |r - res(j)|^0.3; and per residue the system's normalisation (:3787-3848).
+struct AmhGoContacts {
+  std::vector<int> start;                    // [2 n_res + 1]
+  std::vector<int> partner;                  // internal atom 3 j + b
+  std::vector<double> rnat, gamma, sig_sq;   // per contact
+  std::vector<double> norm;                  // [n_res]: normalisation of the residue's system
+};
+
 struct SystemInput {
   ForceField ff;
   Topology top;
@@ -147,6 +165,7 @@ struct SystemInput {
   std::vector<Memory> mems;
   FMTable fm;
   FMTableTB tb;
+  AmhGoContacts go;
   std::vector<double> x, v;  // internal order [n_atoms*3]
 };
 
@@ -168,6 +187,11 @@ void build_fm_table(const ForceField &ff, const Topology &top, const GammaTable 
 // `dir`: where fm_table.energy / fm_table.force are read or written
 void build_fm_table_tb(const ForceField &ff, const Topology &top, const GammaTable &g,
                        const std::vector<Memory> &mems, const std::string &dir, FMTableTB &out);
+// AMH-Go native contacts and normalisation from `dir`'s amh-go.gamma, amh-go.gro
+// (and frustration_censored_contacts.dat with censoring 1)
+void build_amh_go(const ForceField &ff, const Topology &top, const std::string &dir, AmhGoContacts &out);
+// FixBackbone's pair-list cutoff (fix_backbone.cpp:1051-1067) for the enabled terms
+double pair_list_cutoff(const FFParams &p);
 
 // A system from per-atom arrays in the caller's order (a host code's own
 // atom data: roles 0 CA, 1 CB/H-beta, 2 O, -1 other; residue and molecule
@@ -195,6 +219,7 @@ struct Batch {
   Topology top;       // concatenated topology (ext_of is per replica, see below)
   FMTable fm;         // concatenated fragment-memory rows
   FMTableTB tb;       // concatenated fragment-memory tables (per residue)
+  AmhGoContacts go;   // concatenated AMH-Go contacts (partners offset to batch atoms)
   std::vector<double> x, v;
   std::vector<int> res_sys;              // residue -> replica
   std::vector<int> sys_res_begin, sys_res_end;    // [n_sys]

@@ -129,6 +129,7 @@ struct PersistArgs {
   int ring_warps;    // warps with a shared-memory copy ring (the last ones); the others load into registers
   int fm_units;      // fragment-memory work units of the step (0: term off)
   int fm_table;      // table fragment memory on
+  int amh_go;        // AMH-Go on
 };
 
 // Fragment-memory units taken from the step's counter until none is left
@@ -206,6 +207,7 @@ template <typename R> __global__ void __launch_bounds__(kStepThreads, 2) k_step(
     if (ok) {
       hbond_pass(a, p, sp);
       if (q.fm_table) fm_table_pass(a, p, sp);
+      if (q.amh_go) amh_go_pass(a, p, sp);
       fragmem_take_units(a, p, q, ring, wsm, kbase);
     }
   }

@@ -113,6 +113,7 @@ def load_library(path: str = LIB_PATH):
     lib.awsem_set_step_form.argtypes = [vp, ip, ip, ip]
     lib.awsem_get_step_form.argtypes = [vp, vp]
     lib.awsem_set_launch_shapes.argtypes = [vp, vp]
+    lib.awsem_set_neighbor.argtypes = [vp, C.c_double, ip, ip, ip]
     lib.awsem_run_window.argtypes = [vp, C.c_longlong, C.POINTER(RunParams), C.c_longlong, C.c_longlong, ip, vp]
     lib.awsem_create_from_atoms.argtypes = [cp, cp, cp, ip, vp, vp, vp, vp, vp, vp, ip, vp, ip, vp, vp, vp, vp, cp, cp,
                                             ip, ip, C.POINTER(vp)]
@@ -304,6 +305,14 @@ class AwsemSystem:
         v = [shapes[k] for k in self.SHAPE_KEYS] if isinstance(shapes, dict) else list(shapes)
         arr = np.array(v, dtype=np.int32)
         _check(self.lib, self.lib.awsem_set_launch_shapes(self.h, _ptr(arr)), "awsem_set_launch_shapes")
+
+    def set_neighbor(self, skin: float = 0.0, delay: int = 0, every: int = 1, check: bool = True) -> None:
+        """LAMMPS `neighbor` skin (> 0 sets it) and neigh_modify delay/every/check
+        of the neighbour list [AMH-Go] reads (awsem_set_neighbor); LAMMPS's
+        defaults until called."""
+        chk = int(check) if not isinstance(check, bool) else int(check is True)
+        _check(self.lib, self.lib.awsem_set_neighbor(self.h, float(skin), int(delay), int(every), chk),
+               "awsem_set_neighbor")
 
     def set_step_form(self, form: str, blocks: int = 0, stream_warps: int = 2) -> None:
         """'kernels': each MD step a graph of per-pass kernels; 'persistent':

@@ -9,6 +9,7 @@
 #include "domain.h"
 #include "error.h"
 #include "group.h"
+#include "neighbor.h"
 #include "update.h"
 
 using namespace LAMMPS_NS;
@@ -80,6 +81,8 @@ void FixBackboneGPU::create_handle()
                                          nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, precision, device,
                                          &handle);
   if (rc != AWSEM_OK) error->all(FLERR, awsem_last_error());
+  // the reach of the fix's neighbour lists: pair-list cutoff + LAMMPS's skin
+  if (awsem_set_neighbor(handle, neighbor->skin, 0, 1, 1) != AWSEM_OK) error->all(FLERR, awsem_last_error());
   xg.assign(3 * (size_t) n, 0.0);
   fg.assign(3 * (size_t) n, 0.0);
 }
@@ -100,6 +103,8 @@ void FixBackboneGPU::evaluate()
     for (int d = 0; d < 3; d++) xg[k + d] = x[i][d] + (per[d] ? box[d] * prd[d] : 0.0);
   }
   std::fill(fg.begin(), fg.end(), 0.0);
+  // [AMH-Go] reads the fix's full neighbour list: new only on build steps
+  if (awsem_set_list_built(handle, neighbor->ago == 0 ? 1 : 0) != AWSEM_OK) error->all(FLERR, awsem_last_error());
   const int rc = awsem_compute(handle, (long long) update->ntimestep, xg.data(), fg.data(), energy, AWSEM_TERMS_FIX);
   if (rc != AWSEM_OK) error->all(FLERR, awsem_last_error());
   for (int i = 0; i < n; i++) {

@@ -348,6 +348,7 @@ class Driver:
         self.boundary = ["p", "p", "p"]
         self.dt = None
         self.skin, self.neigh_every = 2.0, 0
+        self.neigh = {"delay": 0, "every": 1, "check": True}  # LAMMPS's neigh_modify defaults
         self.special_fene = False
         self.atom_style = None
         self.bond_style = None
@@ -527,21 +528,30 @@ class Driver:
             raise LammpsError(f"neighbor: unknown style {a[1]}")
 
     def c_neigh_modify(self, a):
-        k, every, check = 0, 1, True
+        # keywords not given keep their values, as in LAMMPS
+        k = 0
         while k < len(a):
             if a[k] in ("every", "delay", "check", "once", "page", "one", "binsize", "cluster", "include", "exclude"):
-                if a[k] == "every":
-                    every = int(a[k + 1])
+                if a[k] in ("every", "delay"):
+                    v = int(a[k + 1])
+                    if v < (1 if a[k] == "every" else 0):
+                        raise LammpsError(f"neigh_modify: illegal {a[k]} {a[k + 1]}")
+                    self.neigh[a[k]] = v
                 elif a[k] == "check":
-                    check = a[k + 1] == "yes"
+                    if a[k + 1] not in ("yes", "no"):
+                        raise LammpsError(f"neigh_modify: check {a[k + 1]}")
+                    self.neigh["check"] = a[k + 1] == "yes"
+                elif a[k] == "once" and a[k + 1] == "yes":
+                    raise LammpsError("neigh_modify once yes is not supported")
                 elif a[k] == "exclude":
                     raise LammpsError("neigh_modify exclude is not supported")
                 k += 2
             else:
                 raise LammpsError(f"neigh_modify: unknown keyword {a[k]}")
-        # the engine's list is rebuilt whenever a displacement check fails;
-        # `check no` asks for a rebuild every `every` steps on top of it
-        self.neigh_every = 0 if check else every
+        # the engine's own pair list is rebuilt whenever its displacement check
+        # fails; `check no` asks for a rebuild every `every` steps on top of it.
+        # The list [AMH-Go] reads follows delay/every/check exactly.
+        self.neigh_every = 0 if self.neigh["check"] else self.neigh["every"]
 
     def c_special_bonds(self, a):
         if a == ["fene"] or a == ["lj", "0.0", "1.0", "1.0"] or a == ["lj/coul", "0.0", "1.0", "1.0"]:
@@ -899,6 +909,7 @@ class Driver:
             raise LammpsError("this driver integrates with fix nve (+ fix langevin): fix nve is missing")
         lang = [f[2] for f in self.fixes.values() if f[0] == "langevin"]
         eng = self._engine()
+        eng.set_neighbor(self.skin, **self.neigh)
         eng.set_state(self.x, self.v)
         if eng.step != self.step:
             eng.compute(self.x, step=self.step)  # moves the engine's step counter (reset_timestep, read_restart)

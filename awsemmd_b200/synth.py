@@ -308,6 +308,27 @@ def atom_arrays(sys_: System):
     return np.array(xs, dtype=np.float64), np.array(types, np.int32), np.array(mols, np.int32), np.array(ress, np.int32)
 
 
+def write_native_gro(sys_: System, path: str, scale: float = 1.0) -> None:
+    """A native structure for [AMH-Go] (amh-go.gro): the system's CA and CB
+    atoms (no CB for glycine), residues numbered 1..n over all chains,
+    coordinates scaled by `scale` about the CA centroid (scale < 1 makes the
+    native structure more compact than the system), in nm."""
+    ca = np.concatenate([ch.ca for ch in sys_.chains])
+    c0 = ca.mean(axis=0)
+    lines, r, k = [], 0, 0
+    for ch in sys_.chains:
+        for i in range(ch.length):
+            r += 1
+            beads = [("CA", ch.ca[i])] + ([] if ch.seq[i] == "G" else [("CB", ch.cb[i])])
+            for name, x in beads:
+                k += 1
+                y = c0 + scale * (np.asarray(x) - c0)
+                lines.append(f"{r:5d}{THREE[ch.seq[i]]:>5s}{name:>5s}{k:5d} "
+                             + " ".join(_fmt_nm(float(v)) for v in y))
+    with open(path, "w") as f:
+        f.write(f"native structure (synthetic, scale {scale})\n{len(lines)}\n" + "\n".join(lines) + "\n   0.0 0.0 0.0\n")
+
+
 def bond_list(sys_: System):
     """(type, atom_i, atom_j) with 0-based atom indices in data-file order."""
     bonds = []
@@ -378,17 +399,23 @@ def replica_lengths(n=1024, lo=40, hi=500, seed=3000):
 # --------------------------------------------------------------------------
 # writers (the reference's input formats)
 
-def coeff_text(k_fm=1.0, mem_file="frags.mem", gamma_file="uniform.gamma", table=None) -> str:
+def coeff_text(k_fm=1.0, mem_file="frags.mem", gamma_file="uniform.gamma", table=None, amh_go=None) -> str:
     """The repository's parameter file plus a [Fragment_Memory] section, or with
     table = (rmin, rmax, dr, well_width, use_table_files, sigma_exp) a
-    [Fragment_Memory_Table] section instead."""
+    [Fragment_Memory_Table] section instead; amh_go = (k, p, rc, censoring)
+    adds an [AMH-Go] section (inputs amh-go.gro and amh-go.gamma)."""
     with open(os.path.join(PARAM_DIR, "fix_backbone_coeff.data")) as f:
         base = f.read()
     if table is None:
-        return base.rstrip("\n") + f"\n\n[Fragment_Memory]\n{k_fm}\n{mem_file}\n{gamma_file}\n"
-    rmin, rmax, dr, width, use, sexp = table
-    return base.rstrip("\n") + (f"\n\n[Fragment_Memory_Table]\n{k_fm}\n{mem_file}\n{gamma_file}\n"
-                                 f"{rmin} {rmax} {dr}\n{width}\n{use}\n{sexp}\n")
+        text = base.rstrip("\n") + f"\n\n[Fragment_Memory]\n{k_fm}\n{mem_file}\n{gamma_file}\n"
+    else:
+        rmin, rmax, dr, width, use, sexp = table
+        text = base.rstrip("\n") + (f"\n\n[Fragment_Memory_Table]\n{k_fm}\n{mem_file}\n{gamma_file}\n"
+                                     f"{rmin} {rmax} {dr}\n{width}\n{use}\n{sexp}\n")
+    if amh_go is not None:
+        k, pw, rc, cens = amh_go
+        text += f"\n[AMH-Go]\n{k}\n{pw}\n{rc}\n{cens}\n"
+    return text
 
 
 def write_system(sys_: System, outdir: str, with_fm=True) -> dict:

@@ -242,6 +242,30 @@ int awsem_autotune(awsem_system *sys, int reps, int *chosen);
  * do not depend on them.  AWSEM_EINVAL when a value is out of range. */
 int awsem_set_launch_shapes(awsem_system *sys, const int *shapes);
 
+/* LAMMPS `neighbor SKIN bin` and `neigh_modify delay D every E check
+ * yes|no`.  skin > 0 sets the skin of the engine's lists (as
+ * awsem_run_params.skin does for a run; <= 0 keeps it); the rest applies to
+ * the neighbour list that [AMH-Go] reads.  The reference evaluates AMH-Go over the fix's full
+ * neighbour list (fix_backbone.cpp:1809-1813 requests it, :3874-3972 walks
+ * it), whose pairs are those within the pair-list cutoff plus the skin when
+ * LAMMPS last rebuilt it; the engine keeps that membership per replica and
+ * rebuilds it by LAMMPS's rule: at each run setup (and each awsem_compute),
+ * then once at least `delay` steps have passed, on multiples of `every`, and
+ * with check=1 only after some atom moved more than half the skin.
+ * Defaults: skin 2.0, delay 0, every 1, check 1 (LAMMPS's).  AWSEM_EINVAL
+ * for delay < 0, every < 1 or check not 0/1. */
+int awsem_set_neighbor(awsem_system *sys, double skin, int delay, int every, int check);
+
+/* For a host that runs the MD loop itself and calls awsem_compute once per
+ * step (LAMMPS with `fix backbone/gpu`): whether the host rebuilt its
+ * neighbour lists on the step of the next awsem_compute (LAMMPS:
+ * neighbor->ago == 0).  With [AMH-Go] that evaluation then records a new
+ * list (built = 1) or keeps the one recorded at the last build (built = 0),
+ * as the reference fix reads LAMMPS's list (fix_backbone.cpp:3874-3880).
+ * Applies to the next awsem_compute only; without a call every
+ * awsem_compute builds.  AWSEM_EINVAL unless built is 0 or 1. */
+int awsem_set_list_built(awsem_system *sys, int built);
+
 /* Step form of awsem_run / awsem_server_advance (no counterpart in the
  * reference, which evaluates on the CPU inside LAMMPS's pre_force hook).
  * form 0: each MD step is a chain of per-pass kernels (prepare, list

@@ -122,6 +122,10 @@ struct Params {
          helix_sigma_HO_sqinv = 0, helix_sigma_NO_sqinv = 0;
   double k_fm = 0, fm_sigma_exp = 0.15;
   std::string fm_file, fm_gamma_file;
+  // [AMH-Go] (fix_backbone.cpp:297-303)
+  bool amhgo = 0;
+  double k_amh_go = 0, amh_go_p = 0, amh_go_rc = 0;
+  int censoring = 0;
   // [Fragment_Memory_Table] (fix_backbone.cpp:310-321)
   double tb_rmin = 0, tb_rmax = 0, tb_dr = 0, tb_width = 0;
   int tb_size = 0, tb_use_file = 0;
@@ -300,6 +304,23 @@ struct System {
   void build_tb();
   void tb_term(int i, double *f);
 
+  // AMH-Go: native structure, gamma, normalisation, censored residue pairs
+  GammaArray go_gamma;
+  Memory go_mem;                   // the native structure, amh-go.gro (all n residues)
+  std::vector<char> go_censored;   // [n*n]
+  double go_norm = 0.0;
+  double plc = 0.0;  // the fix's pair-list cutoff (fix_backbone.cpp:1048-1066)
+  // The fix's full neighbour list (cut plc + skin) and LAMMPS's rebuild rule
+  // (Neighbor::decide with delay / every / check, the half-skin trigger).
+  double nb_skin = 2.0;
+  int nb_delay = 0, nb_every = 1, nb_check = 1;
+  bool list_setup = true;  // the next compute is a run setup: the list is built
+  long long list_ago = 0;
+  std::vector<double> xhold;  // positions at the last build
+  void read_amh_go();
+  void amhgo_normalization();
+  void amhgo_term(const double *x, double *f);
+
   // topology
   int natoms = 0, n = 0, nch = 0;
   std::vector<int> ch_pos1, ch_len;  // 1-based first residue, length
@@ -362,7 +383,7 @@ void System::read_coeff(const std::string &path)
   if (!in) throw std::runtime_error("Coefficient file was not found!");
   Params &p = P;
   std::string s;
-  static const char *unsupported[] = {"[Shake]", "[Excluded]", "[Excluded_P]", "[Excluded_R6]", "[AMH-Go]",
+  static const char *unsupported[] = {"[Shake]", "[Excluded]", "[Excluded_P]", "[Excluded_R6]",
                                       "[Contact_Restraints]",
                                       "[Vector_Fragment_Memory]", "[Solvent_Barrier]", "[Membrane]",
                                       "[Fragment_Frustratometer]", "[Tertiary_Frustratometer]",
@@ -449,6 +470,13 @@ void System::read_coeff(const std::string &path)
       in >> p.tb_rmin >> p.tb_rmax >> p.tb_dr;
       p.tb_size = (int) ((p.tb_rmax - p.tb_rmin) / p.tb_dr) + 2;
       in >> p.tb_width >> p.tb_use_file >> p.fm_sigma_exp;
+    } else if (s == "[AMH-Go]") {
+      p.amhgo = 1;
+      in >> p.k_amh_go >> p.amh_go_p >> p.amh_go_rc;
+      // the reference reads the censoring flag unconditionally; a file without
+      // it leaves its stream failed, so the oracle asks for it
+      if (!(in >> p.censoring)) throw std::runtime_error("[AMH-Go]: the frustration censoring flag is missing");
+      if (p.censoring == 2) throw std::runtime_error("oracle: [AMH-Go] censoring 2 is not part of the restated path");
     } else if (s == "[Epsilon]") {
       in >> p.epsilon;
     } else {
@@ -465,6 +493,7 @@ void System::read_coeff(const std::string &path)
   p.k_helix *= p.epsilon;
   p.k_dssp *= p.epsilon;
   p.k_global_pap *= p.epsilon;
+  p.k_amh_go *= p.epsilon;
   for (int j = 0; j < p.n_rama; j++) p.w[j] *= p.k_rama;
   for (int j = 0; j < p.n_rama_p; j++) p.w[j + Params::i_rp] *= p.k_rama;
   // well supports: rmin - 8 ln10/kappa, rmax + 8 ln10/kappa (smart_matrix_lib.h:363-368)
@@ -635,6 +664,59 @@ void System::read_data(const std::string &path)
   (void) nbonds;
 }
 
+/* a .gro structure read as Fragment_Memory's constructor does
+   (fragment_memory.cpp:60-172): residues fpos+1..fpos+len, CA and CB
+   coordinates (nm -> A), then the CA-CA / CB-CB and CA-CB distance tables */
+void load_gro(const std::string &path, int fpos, Memory &m, const std::string &open_msg, const std::string &who)
+{
+  m.se.assign(m.len, '?');
+  std::vector<double> xa((size_t) m.len * 3, 0.0), xb((size_t) m.len * 3, 0.0);
+  FILE *fg = fopen(path.c_str(), "r");
+  if (!fg) throw std::runtime_error(open_msg);
+  char buf[256];
+  if (!fgets(buf, sizeof buf, fg)) throw std::runtime_error("bad gro");
+  int nat = 0;
+  if (fscanf(fg, "%d", &nat) != 1) throw std::runtime_error("bad gro");
+  int nca = 0;
+  for (int a = 0; a < nat; a++) {
+    int ires, iatom;
+    char resty[16], atomty[16];
+    double x, y, z;
+    if (fscanf(fg, "%d %15s %15s %d %lf %lf %lf", &ires, resty, atomty, &iatom, &x, &y, &z) != 7) break;
+    if (ires > fpos + m.len) break;
+    if (ires > fpos && ires <= fpos + m.len) {
+      int r = ires - fpos - 1;
+      x *= 10;
+      y *= 10;
+      z *= 10;
+      if (!strcmp(atomty, "CA")) {
+        m.se[r] = three_to_one(resty);
+        if (m.se[r] == '?') {
+          fclose(fg);
+          throw std::runtime_error(who + ": Unknown residue");
+        }
+        xa[3 * r] = x;
+        xa[3 * r + 1] = y;
+        xa[3 * r + 2] = z;
+        nca++;
+      } else if (!strcmp(atomty, "CB")) {
+        xb[3 * r] = x;
+        xb[3 * r + 1] = y;
+        xb[3 * r + 2] = z;
+      }
+    }
+  }
+  fclose(fg);
+  if (nca != m.len) throw std::runtime_error(who + ": Wrong atom count in memory structure file");
+  m.rf0.assign((size_t) m.len * m.len, 0.0);
+  m.rf1.assign((size_t) m.len * m.len, 0.0);
+  for (int i = 0; i < m.len; i++)
+    for (int j = 0; j < m.len; j++) {
+      m.rf0[i * m.len + j] = i < j ? m.R(&xa[3 * i], &xa[3 * j]) : (i > j ? m.R(&xb[3 * i], &xb[3 * j]) : 0.0);
+      m.rf1[i * m.len + j] = m.R(&xa[3 * i], &xb[3 * j]);
+    }
+}
+
 /* .mem list and .gro memories (fix_backbone.cpp:1966-2042,
    fragment_memory.cpp:34-176) and the residue -> memory map (:749-791) */
 void System::read_mems()
@@ -659,48 +741,7 @@ void System::read_mems()
       int fpos = atoi(v[2].c_str()) - 1;
       m.len = atoi(v[3].c_str());
       m.weight = atof(v[4].c_str());
-      m.se.assign(m.len, '?');
-      std::vector<double> xa((size_t) m.len * 3, 0.0), xb((size_t) m.len * 3, 0.0);
-      FILE *fg = fopen(join(workdir, v[0]).c_str(), "r");
-      if (!fg) throw std::runtime_error("Fragment_Memory: Cannot read the file " + v[0]);
-      char buf[256];
-      if (!fgets(buf, sizeof buf, fg)) throw std::runtime_error("bad gro");
-      int nat = 0;
-      if (fscanf(fg, "%d", &nat) != 1) throw std::runtime_error("bad gro");
-      int nca = 0;
-      for (int a = 0; a < nat; a++) {
-        int ires, iatom;
-        char resty[16], atomty[16];
-        double x, y, z;
-        if (fscanf(fg, "%d %15s %15s %d %lf %lf %lf", &ires, resty, atomty, &iatom, &x, &y, &z) != 7) break;
-        if (ires > fpos + m.len) break;
-        if (ires > fpos && ires <= fpos + m.len) {
-          int r = ires - fpos - 1;
-          x *= 10;
-          y *= 10;
-          z *= 10;
-          if (!strcmp(atomty, "CA")) {
-            m.se[r] = three_to_one(resty);
-            xa[3 * r] = x;
-            xa[3 * r + 1] = y;
-            xa[3 * r + 2] = z;
-            nca++;
-          } else if (!strcmp(atomty, "CB")) {
-            xb[3 * r] = x;
-            xb[3 * r + 1] = y;
-            xb[3 * r + 2] = z;
-          }
-        }
-      }
-      fclose(fg);
-      if (nca != m.len) throw std::runtime_error("Fragment_Memory: Wrong atom count in memory structure file");
-      m.rf0.assign((size_t) m.len * m.len, 0.0);
-      m.rf1.assign((size_t) m.len * m.len, 0.0);
-      for (int i = 0; i < m.len; i++)
-        for (int j = 0; j < m.len; j++) {
-          m.rf0[i * m.len + j] = i < j ? m.R(&xa[3 * i], &xa[3 * j]) : (i > j ? m.R(&xb[3 * i], &xb[3 * j]) : 0.0);
-          m.rf1[i * m.len + j] = m.R(&xa[3 * i], &xb[3 * j]);
-        }
+      load_gro(join(workdir, v[0]), fpos, m, "Fragment_Memory: Cannot read the file " + v[0], "Fragment_Memory");
       if (m.pos + m.len > n) throw std::runtime_error("Fragment_Memory: Incorrectly defined memory fragment");
       mems.push_back(m);
     } else if (state == 0) {
@@ -1659,6 +1700,173 @@ void System::bonds(const double *x, double *f)
   }
 }
 
+/* The fix's pair-list cutoff, fix_backbone.cpp:1048-1066: 8 A, or the
+   DSSP / P_AP cutoffs, the outer theta radii of the water and helix wells
+   and, with [Helix], calc_exp_helix_cutoff (:1074-1103), if larger. */
+double pair_list_cut(const Params &p)
+{
+  double cut = 8.0;
+  if (p.dssp) cut = std::max(cut, p.dssp_cut);
+  if (p.pap) cut = std::max(cut, sqrt(p.pap_cutoff_sq));
+  if (p.water)
+    for (int k = 0; k < p.n_wells; k++) cut = std::max(cut, p.w_rmax_th[k]);
+  if (p.helix) {
+    cut = std::max(cut, p.h_rmax_th);
+    // O(i) to virtual N(j) / H(j): the farthest of the atoms they are built from
+    const double r0[3] = {3.77, 2.5, 2.41};
+    auto reach = [&](double a, double b, double c) {
+      double r[3];
+      r[0] = sqrt(pow(a * r0[0], 2) + pow(c * r0[1], 2) + a * c * (r0[0] * r0[0] + r0[1] * r0[1] - r0[2] * r0[2]));
+      r[1] = sqrt(pow(a * r0[2], 2) + pow(b * r0[1], 2) + a * b * (r0[2] * r0[2] + r0[1] * r0[1] - r0[0] * r0[0]));
+      r[2] = sqrt(pow(b * r0[0], 2) + pow(c * r0[2], 2) + b * c * (r0[0] * r0[0] + r0[2] * r0[2] - r0[1] * r0[1]));
+      return std::max(r[0], std::max(r[1], r[2]));
+    };
+    double r1 = 1.1 * reach(p.an, p.bn, p.cn) + p.helix_NO_zero + p.helix_sigma_NO * sqrt(6.0 * log(10.0));
+    double r2 = 1.1 * reach(p.ah, p.bh, p.ch) + p.helix_HO_zero + p.helix_sigma_HO * sqrt(6.0 * log(10.0));
+    cut = std::max(cut, std::max(r1, r2));
+    cut = std::max(cut, p.helix_cutoff);
+  }
+  return cut;
+}
+
+/* [AMH-Go] inputs (fix_backbone.cpp:695-742): amh-go.gamma, the native
+   structure amh-go.gro as Fragment_Memory(0, 0, n, 1.0, ...), the censored
+   residue pairs of frustration_censored_contacts.dat (flag 1), the fix's
+   pair-list cutoff, and the normalisation. */
+void System::read_amh_go()
+{
+  go_gamma.load(join(workdir, "amh-go.gamma"));
+  if (go_gamma.frag_resty) throw std::runtime_error("AMH-Go: Wrong call of getGamma() function");
+  go_mem.pos = 0;
+  go_mem.len = n;
+  go_mem.weight = 1.0;
+  load_gro(join(workdir, "amh-go.gro"), 0, go_mem, "Cannot read file amh-go.gro", "AMH_Go");
+  go_censored.assign((size_t) n * n, 0);
+  if (P.censoring == 1) {
+    std::ifstream cf(join(workdir, "frustration_censored_contacts.dat"));
+    int a, b;
+    while (cf >> a >> b)
+      if (a >= 1 && a <= n && b >= 1 && b <= n) go_censored[(size_t) (a - 1) * n + (b - 1)] = 1;
+  }
+  plc = pair_list_cut(P);
+  amhgo_normalization();
+}
+
+/* compute_amhgo_normalization, fix_backbone.cpp:3787-3854:
+   a = (1 / 8N) sum over CA / CB atoms i of |sum over native contacts of gamma|^p,
+   the power taken of the running sum after each partner chain (the
+   reference's loop nesting), N the last chain's last residue number. */
+void System::amhgo_normalization()
+{
+  const Params &p = P;
+  go_norm = 0.0;
+  int iresn = 0;
+  for (int ich = 0; ich < nch; ++ich) {
+    const int ires0 = ch_pos1[ich] - 1;
+    iresn = ch_pos1[ich] + ch_len[ich] - 1;
+    for (int i = ires0; i < iresn; ++i) {
+      const int it = aa_index(se[i]);
+      for (int iatom = 1; iatom <= 2 - (se[i] == 'G' ? 1 : 0); ++iatom) {
+        double normi = 0.0;
+        for (int jch = 0; jch < nch; ++jch) {
+          const int jres0 = ch_pos1[jch] - 1, jresn = ch_pos1[jch] + ch_len[jch] - 1;
+          for (int j = jres0; j < jresn; ++j) {
+            const int jt = aa_index(se[j]);
+            for (int jatom = 1; jatom <= 2 - (se[j] == 'G' ? 1 : 0); ++jatom) {
+              if (abs(i - j) < go_gamma.min_sep()) continue;
+              if (go_mem.rf(i, iatom, j, jatom) < p.amh_go_rc) normi += go_gamma.get(it, jt, 0, 0, i, j);
+            }
+          }
+          go_norm += pow(fabs(normi), p.amh_go_p);
+        }
+      }
+    }
+  }
+  go_norm /= 8 * iresn;
+}
+
+/* compute_amh_go_model, fix_backbone.cpp:3856-3992, over the fix's full
+   neighbour list: for each atom i, every atom j != i that was within
+   plc + skin of i when LAMMPS last built the list, 1-2 bonded pairs removed
+   (special_bonds fene), in atom order.  The list is built at a run setup and
+   then by Neighbor::decide(): after `delay` steps, on multiples of `every`,
+   with `check` only once an atom has moved more than half the skin. */
+void System::amhgo_term(const double *x, double *f)
+{
+  const Params &p = P;
+  bool build = list_setup;
+  list_setup = false;
+  if (!build) {
+    list_ago++;
+    if (list_ago >= nb_delay && list_ago % nb_every == 0) {
+      if (!nb_check) {
+        build = true;
+      } else {
+        const double trigger = 0.25 * nb_skin * nb_skin;
+        for (int a = 0; a < natoms && !build; a++) {
+          double dx = x[3 * a] - xhold[3 * a], dy = x[3 * a + 1] - xhold[3 * a + 1], dz = x[3 * a + 2] - xhold[3 * a + 2];
+          if (dx * dx + dy * dy + dz * dz > trigger) build = true;
+        }
+      }
+    }
+  }
+  if (build) {
+    xhold.assign(x, x + 3 * natoms);
+    list_ago = 0;
+  }
+  const double cut = plc + nb_skin, cutsq = cut * cut;
+  auto in_list = [&](int i, int j) {
+    double dx = xhold[3 * i] - xhold[3 * j], dy = xhold[3 * i + 1] - xhold[3 * j + 1],
+           dz = xhold[3 * i + 2] - xhold[3 * j + 2];
+    if (!(dx * dx + dy * dy + dz * dz < cutsq)) return false;
+    for (int s : special[i])
+      if (s == j) return false;
+    return true;
+  };
+  const int min_sep = go_gamma.min_sep();
+  double Etot = 0.0;
+  std::vector<int> fmap;
+  std::vector<double> fbuf;
+  for (int i = 0; i < natoms; i++) {
+    const int ires = ares[i], ri = ires - 1;
+    const bool i_ca = i == ca[ri], i_cb = i == cb[ri] && se[ri] != 'G';
+    if (!i_ca && !i_cb) continue;
+    const int it = aa_index(se[ri]);
+    fmap.assign(1, i);
+    fbuf.assign(3, 0.0);
+    double Ei = 0.0;
+    for (int j = 0; j < natoms; j++) {
+      if (j == i || !in_list(i, j)) continue;
+      const int jres = ares[j], rj = jres - 1;
+      if (p.censoring == 1 && (go_censored[(size_t) ri * n + rj] || go_censored[(size_t) rj * n + ri])) continue;
+      const bool j_ca = j == ca[rj], j_cb = j == cb[rj] && se[rj] != 'G';
+      if (!(j_ca || j_cb) || !(abs(ires - jres) >= min_sep || amol[i] != amol[j])) continue;
+      const double rnative = go_mem.rf(ri, i_ca ? 1 : 2, rj, j_ca ? 1 : 2);
+      if (!(rnative < p.amh_go_rc)) continue;
+      const double dx[3] = {x[3 * i] - x[3 * j], x[3 * i + 1] - x[3 * j + 1], x[3 * i + 2] - x[3 * j + 2]};
+      const double r = sqrt(dx[0] * dx[0] + dx[1] * dx[1] + dx[2] * dx[2]);
+      const double dr = r - rnative, drsq = dr * dr;
+      const double sigma_sq = pow(abs(ires - jres), 0.3);
+      if (drsq < 27.6 * sigma_sq) {
+        const double gamma = go_gamma.get(it, aa_index(se[rj]), 0, 0, ri, rj);
+        const double Eij = gamma * exp(-drsq / (2.0 * sigma_sq));
+        const double force = Eij * dr / (sigma_sq * r);
+        fmap.push_back(j);
+        for (int k = 0; k < 3; k++) {
+          fbuf[k] += force * dx[k];
+          fbuf.push_back(-force * dx[k]);
+        }
+        Ei += Eij;
+      }
+    }
+    const double factor = -0.5 * p.k_amh_go * p.amh_go_p * pow(Ei, p.amh_go_p - 1) / go_norm;
+    for (size_t k = 0; k < fmap.size(); k++)
+      for (int c = 0; c < 3; c++) f[3 * fmap[k] + c] += factor * fbuf[3 * k + c];
+    Etot += -0.5 * p.k_amh_go * pow(Ei, p.amh_go_p) / go_norm;
+  }
+  E[ET_AMHGO] += Etot;
+}
+
 /* compute_backbone, fix_backbone.cpp:7047-7673, then vexcluded and bonds */
 void System::compute(const double *x, double *f)
 {
@@ -1674,6 +1882,7 @@ void System::compute(const double *x, double *f)
     if (p.fm_tb) tb_term(i, f);
   }
   pair_terms(x, f);
+  if (p.amhgo) amhgo_term(x, f);
   for (int k = 1; k < NET; k++) E[ET_TOTAL] += E[k];
   excluded_volume(x, f);
   bonds(x, f);
@@ -1700,6 +1909,7 @@ void *oracle_create(const char *workdir, const char *data_file, const char *coef
     S->read_tables();
     if (S->P.fm || S->P.fm_tb) S->read_mems();
     if (S->P.fm_tb) S->build_tb();
+    if (S->P.amhgo) S->read_amh_go();
     S->pair_setup(pair_style, pair_coeffs ? pair_coeffs : "");
   } catch (std::exception &e) {
     g_err = e.what();
@@ -1722,6 +1932,7 @@ int oracle_compute(void *h, const double *x, double *f, double *energies)
       tmp.resize(3 * S->natoms);
       f = tmp.data();
     }
+    S->list_setup = true;  // a single evaluation builds its lists
     S->compute(x, f);
     if (energies) {
       for (int k = 0; k < NET; k++) energies[k] = S->E[k];
@@ -1797,6 +2008,7 @@ int oracle_run(void *h, double *x, double *v, long long step0, long long nsteps,
       thermo[4 * r + 2] = S->e_bond;
       thermo[4 * r + 3] = ke();
     };
+    S->list_setup = true;  // the run's setup builds the lists
     S->compute(x, f.data());
     langevin_force(begin);
     row(0);
@@ -1821,6 +2033,20 @@ int oracle_run(void *h, double *x, double *v, long long step0, long long nsteps,
     g_err = e.what();
     return -1;
   }
+  return 0;
+}
+
+int oracle_set_neighbor(void *h, double skin, int delay, int every, int check)
+{
+  System *S = (System *) h;
+  if (!(skin >= 0.0) || delay < 0 || every < 1) {
+    g_err = "oracle_set_neighbor: skin >= 0, delay >= 0, every >= 1";
+    return -1;
+  }
+  S->nb_skin = skin;
+  S->nb_delay = delay;
+  S->nb_every = every;
+  S->nb_check = check ? 1 : 0;
   return 0;
 }
 

@@ -35,6 +35,9 @@ int oracle_selection_digest(void *h, unsigned long long *counts, unsigned long l
 int oracle_run(void *h, double *x, double *v, long long step0, long long nsteps, double dt,
                int langevin, double t_start, double t_stop, double damp,
                unsigned long long seed, double *thermo);
+/* LAMMPS neighbor skin and neigh_modify delay / every / check of the fix's
+   full neighbour list that [AMH-Go] reads (defaults 2.0, 0, 1, 1) */
+int oracle_set_neighbor(void *h, double skin, int delay, int every, int check);
 double oracle_uniform(unsigned long long seed, long long step, long long tag, int comp);
 
 #ifdef __cplusplus

@@ -101,6 +101,10 @@ class RefSystem:
             raise RuntimeError(self.lib.ref_last_error().decode())
         return f
 
+    def nbuilds(self) -> int:
+        """neighbour-list builds so far (run setups included)"""
+        return int(self.lib.ref_nbuilds(self.h))
+
     def residue_arrays(self, n_res: int) -> np.ndarray:
         out = np.zeros((n_res, 6))
         self.lib.ref_residue_arrays(self.h, out.ctypes.data)
@@ -139,6 +143,7 @@ def _load_oracle():
         lib.oracle_selection_digest.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
         lib.oracle_run.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_longlong, C.c_longlong, C.c_double,
                                    C.c_int, C.c_double, C.c_double, C.c_double, C.c_ulonglong, C.c_void_p]
+        lib.oracle_set_neighbor.argtypes = [C.c_void_p, C.c_double, C.c_int, C.c_int, C.c_int]
         lib.oracle_uniform.restype = C.c_double
         lib.oracle_uniform.argtypes = [C.c_ulonglong, C.c_longlong, C.c_longlong, C.c_int]
         _orc = lib
@@ -173,6 +178,11 @@ class OracleSystem:
         if self.lib.oracle_compute(self.h, x.ctypes.data, f.ctypes.data, e.ctypes.data) != 0:
             raise RuntimeError(self.lib.oracle_last_error().decode())
         return f, e
+
+    def set_neighbor(self, skin=2.0, delay=0, every=1, check=True):
+        """neighbor skin and neigh_modify delay/every/check of the list [AMH-Go] reads"""
+        if self.lib.oracle_set_neighbor(self.h, float(skin), int(delay), int(every), 1 if check else 0) != 0:
+            raise RuntimeError(self.lib.oracle_last_error().decode())
 
     def residue_arrays(self) -> np.ndarray:
         out = np.zeros((self.nres, 8))

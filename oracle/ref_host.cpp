@@ -106,8 +106,9 @@ struct RefHost {
   std::vector<double> bond_k, bond_r0;
   std::vector<std::vector<int>> special;  // 1-2 partners (local indices)
 
-  NeighList fixlist, pairlist;
+  NeighList fixlist, pairlist, fixfull;
   double fix_cut = 0.0, pair_cut = 0.0;
+  bool want_full = false;  // the fix asked for a full list too (AMH-Go)
   double skin = 2.0;
   int every = 1, delay = 0, check = 1;
   bigint last_build = 0;
@@ -149,7 +150,7 @@ struct RefHost {
 
   void read_data(const std::string &path);
   void build_lists();
-  void build_one(NeighList &list, double cut);
+  void build_one(NeighList &list, double cut, bool full);
   bool need_rebuild(bigint step);
   void force_clear();
   void compute_bonds();
@@ -306,9 +307,11 @@ void RefHost::read_data(const std::string &path)
 }
 
 /* Half list, newton on, serial: each pair once (i < j in atom order), pairs
-   within cut+skin, 1-2 bonded pairs removed (special_bonds fene).  Binned so
-   that the CPU baseline's list cost stays the O(N) it is in LAMMPS. */
-void RefHost::build_one(NeighList &list, double cut)
+   within cut+skin, 1-2 bonded pairs removed (special_bonds fene); or, with
+   `full`, every other atom within that range for each atom (LAMMPS's full
+   list).  Binned so that the CPU baseline's list cost stays the O(N) it is in
+   LAMMPS. */
+void RefHost::build_one(NeighList &list, double cut, bool full)
 {
   Atom *a = lmp->atom;
   int n = a->nlocal;
@@ -344,7 +347,7 @@ void RefHost::build_one(NeighList &list, double cut)
           int x = cx + dx, y = cy + dy, z = cz + dz;
           if (x < 0 || y < 0 || z < 0 || x >= nb[0] || y >= nb[1] || z >= nb[2]) continue;
           for (int j = head[(z * nb[1] + y) * nb[0] + x]; j != -1; j = next[j]) {
-            if (j <= i) continue;
+            if (full ? j == i : j <= i) continue;
             double ddx = a->x[i][0] - a->x[j][0];
             double ddy = a->x[i][1] - a->x[j][1];
             double ddz = a->x[i][2] - a->x[j][2];
@@ -381,13 +384,15 @@ void RefHost::build_one(NeighList &list, double cut)
 
 void RefHost::build_lists()
 {
-  build_one(fixlist, fix_cut);
-  build_one(pairlist, pair_cut);
+  build_one(fixlist, fix_cut, false);
+  if (want_full) build_one(fixfull, fix_cut, true);
+  build_one(pairlist, pair_cut, false);
   Atom *a = lmp->atom;
   xhold.resize((size_t) a->nlocal * 3);
   for (int i = 0; i < a->nlocal; i++)
     for (int k = 0; k < 3; k++) xhold[3 * i + k] = a->x[i][k];
   last_build = lmp->update->ntimestep;
+  lmp->neighbor->ago = 0;
   nbuilds++;
 }
 
@@ -591,7 +596,12 @@ static void *create_host(const char *workdir, const char *data_file, const char 
     for (NeighRequest *r : lmp->neighbor->requests) {
       if (r->requestor_is_fix) {
         h->fix_cut = r->cut ? r->cutoff : h->pair->cutforce;
-        h->fix->init_list(r->id, &h->fixlist);
+        if (r->flags & NeighConst::REQ_FULL) {
+          h->want_full = true;
+          h->fix->init_list(r->id, &h->fixfull);
+        } else {
+          h->fix->init_list(r->id, &h->fixlist);
+        }
       } else {
         h->pair_cut = h->pair->cutforce;
         h->pair->init_list(0, &h->pairlist);
@@ -762,6 +772,8 @@ int ref_run(void *hp, long long nsteps, double dt, int langevin, double t_start,
       if (h->need_rebuild(u->ntimestep)) {
         h->build_lists();
         h->fix->post_neighbor();
+      } else {
+        h->lmp->neighbor->ago = (int) (u->ntimestep - h->last_build);
       }
       h->forces(false);
       for (int i = 0; i < a->nlocal; i++) {

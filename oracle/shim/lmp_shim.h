@@ -237,6 +237,7 @@ class NeighRequest {
 class Neighbor {
  public:
   double skin;
+  int ago = 0;  // steps since the lists were built
   std::vector<NeighRequest *> requests;
   NeighRequest *add_request(Fix *, int flags = 0);
   NeighRequest *add_request(Pair *, int flags = 0);

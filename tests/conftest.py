@@ -36,6 +36,15 @@ def gpu_lib():
     return engine.load_library()
 
 
+def neigh_of(g):
+    """(skin, delay, every, check) of a golden case's runs: LAMMPS's defaults
+    unless the case was made with other neighbour settings."""
+    if "neigh" not in g.files:
+        return 2.0, 0, 1, 1
+    skin, delay, every, check = (float(v) for v in g["neigh"])
+    return skin, int(delay), int(every), int(check)
+
+
 def write_case(name, tmp_path):
     """Write a golden case's inputs and check they regenerate byte for byte."""
     import numpy as np

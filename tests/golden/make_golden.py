@@ -14,7 +14,20 @@ against the LAMMPS-API shim (``make -C oracle ref``) and run on four inputs:
                parameter set plus a [Fragment_Memory] section;
 * ``r1r69tb`` -- the same inputs with fragment memory in its table form
                ([Fragment_Memory_Table] with that example's settings: k 0.2,
-               grid 0-50 A by 0.01 A, well width 0.1, sigma exponent 0.15).
+               grid 0-50 A by 0.01 A, well width 0.1, sigma exponent 0.15);
+* ``r1r69go`` -- the r1r69 inputs plus an [AMH-Go] section with the settings
+               of the reference's 1R69_AMH-Go example (k 1, p 1, rc 8 A,
+               no censoring) and that example's amh-go.gro native structure
+               and amh-go.gamma, copied verbatim into tests/golden/r1r69go
+               from examples/examples_new/1R69_AMH-Go;
+* ``r1r69go2`` -- the same with k 1.5, p 2, rc 9 A and censoring 1 (four
+               native residue pairs listed in frustration_censored_contacts.dat);
+* ``c0go``    -- ``c0`` with [AMH-Go] (k 200, p 2, rc 10 A) towards a native
+               structure 0.6 times as large as the starting chain
+               (synth.write_native_gro), run with neighbor skin 0.6 A and
+               neigh_modify delay 3 every 2 check yes: the fix's full list is
+               rebuilt during the run and native contacts cross its reach, so
+               the trajectory depends on LAMMPS's rebuild rule.
 
 For each it stores the inputs' hash, the step-0 forces and energies, the
 per-residue pair-pass intermediates and a 20-step Langevin trajectory
@@ -60,19 +73,37 @@ def dir_hash(d: str) -> str:
 def write_case(name: str, outdir: str) -> dict:
     if name == "c0":
         return synth.write_system(synth.config_system(0), outdir)
+    if name == "c0go":
+        sys_ = synth.config_system(0)
+        files = synth.write_system(sys_, outdir)
+        with open(os.path.join(outdir, files["coeff"]), "w") as fh:
+            fh.write(synth.coeff_text(amh_go=(200.0, 2, 10.0, 0)))
+        synth.write_native_gro(sys_, os.path.join(outdir, "amh-go.gro"), scale=0.6)
+        shutil.copy(os.path.join(GOLDEN, "r1r69go", "amh-go.gamma"), os.path.join(outdir, "amh-go.gamma"))
+        os.chmod(os.path.join(outdir, "amh-go.gamma"), 0o644)
+        return files
     if name == "sheet":
         return synth.write_system(synth.sheet_system(), outdir)
-    if name in ("r1r69", "r1r69tb"):
-        src = os.path.join(GOLDEN, "r1r69")
+    if name in ("r1r69", "r1r69tb", "r1r69go", "r1r69go2"):
         os.makedirs(outdir, exist_ok=True)
-        for f in os.listdir(src):
-            shutil.copy(os.path.join(src, f), os.path.join(outdir, f))
-            os.chmod(os.path.join(outdir, f), 0o644)
+        for d in ("r1r69", "r1r69go") if name.startswith("r1r69go") else ("r1r69",):
+            src = os.path.join(GOLDEN, d)
+            for f in os.listdir(src):
+                shutil.copy(os.path.join(src, f), os.path.join(outdir, f))
+                os.chmod(os.path.join(outdir, f), 0o644)
         for t in synth.PARAM_TABLES:
             shutil.copy(os.path.join(synth.PARAM_DIR, t), os.path.join(outdir, t))
         with open(os.path.join(outdir, "fix_backbone_coeff.data"), "w") as fh:
             if name == "r1r69":
                 fh.write(synth.coeff_text(mem_file="fragsLAMW.mem.single", gamma_file="seq.gamma"))
+            elif name == "r1r69go":
+                fh.write(synth.coeff_text(mem_file="fragsLAMW.mem.single", gamma_file="seq.gamma",
+                                          amh_go=(1.0, 1, 8.0, 0)))
+            elif name == "r1r69go2":
+                fh.write(synth.coeff_text(mem_file="fragsLAMW.mem.single", gamma_file="seq.gamma",
+                                          amh_go=(1.5, 2, 9.0, 1)))
+                with open(os.path.join(outdir, "frustration_censored_contacts.dat"), "w") as cf:
+                    cf.write("3 35\n26 21\n33 39\n49 56\n")
             else:  # the table form and settings of the reference's 1R69 example coefficient file
                 fh.write(synth.coeff_text(k_fm=0.2, mem_file="fragsLAMW.mem.single", gamma_file="seq.gamma",
                                           table=(0, 50, 0.01, 0.1, 0, 0.15)))
@@ -81,7 +112,10 @@ def write_case(name: str, outdir: str) -> dict:
     raise KeyError(name)
 
 
-CASES = ["c0", "sheet", "r1r69", "r1r69tb"]
+CASES = ["c0", "sheet", "r1r69", "r1r69tb", "r1r69go", "r1r69go2", "c0go"]
+# LAMMPS neighbor skin and neigh_modify delay / every / check of a case's runs
+# (the others: 2.0, 0, 1, yes -- LAMMPS's defaults)
+NEIGH = {"c0go": (0.6, 3, 2, 1)}
 
 
 def main(cases=None):
@@ -91,7 +125,8 @@ def main(cases=None):
         with tempfile.TemporaryDirectory() as tmp:
             files = write_case(name, os.path.join(tmp, name))
             h = dir_hash(files["workdir"])
-            r = ref.RefSystem(files)
+            skin, delay, every, check = NEIGH.get(name, (2.0, 0, 1, 1))
+            r = ref.RefSystem(files, skin=skin, every=every, delay=delay, check=check)
             x0, v0 = r.get("x"), r.get("v")
             f0 = r.compute(0)
             e0 = r.energies()
@@ -100,12 +135,14 @@ def main(cases=None):
             thermo = r.run(RUN["nsteps"], dt=RUN["dt"], langevin=True, t_start=RUN["t_start"], t_stop=RUN["t_stop"],
                            damp=RUN["damp"], seed=RUN["seed"])
             xN, vN = r.get("x"), r.get("v")
+            builds = r.nbuilds()
             r.close()
             np.savez_compressed(os.path.join(GOLDEN, f"{name}.npz"), inputs_sha256=np.array(h), x0=x0, v0=v0,
                                 f0=f0, e0=e0, res0=res0, thermo=thermo, xN=xN, vN=vN,
                                 run=np.array([RUN["nsteps"], RUN["dt"], RUN["t_start"], RUN["t_stop"], RUN["damp"],
-                                              RUN["seed"]], dtype=np.float64))
-            print(name, "natoms", len(x0), "E_total", e0[0], "hash", h[:12])
+                                              RUN["seed"]], dtype=np.float64),
+                                neigh=np.array([skin, delay, every, check], dtype=np.float64))
+            print(name, "natoms", len(x0), "E_total", e0[0], "list builds", builds, "hash", h[:12])
             if name == "c0":
                 r = ref.RefSystem(files)
                 rows = r.run(NVE["nsteps"], dt=NVE["dt"], langevin=False)

@@ -6,7 +6,7 @@ forces, the energy vector and a 20-step trajectory agree."""
 import numpy as np
 import pytest
 
-from conftest import write_case
+from conftest import neigh_of, write_case
 
 pytestmark = pytest.mark.gpu
 
@@ -28,3 +28,27 @@ def test_fix_backbone_gpu_replaces_the_reference_fix(name, tmp_path, gpu_lib, or
     t_gpu = gpu.run(20, seed=99)
     np.testing.assert_allclose(t_gpu, t_cpu, rtol=1e-6, atol=1e-6)
     assert np.abs(gpu.get("x") - cpu.get("x")).max() < 1e-6
+
+
+@pytest.mark.parametrize("name", ["r1r69go", "c0go"])
+def test_fix_backbone_gpu_follows_the_hosts_list_builds(name, tmp_path, gpu_lib, oracle_built):
+    """[AMH-Go] reads LAMMPS's neighbour list: the adapter tells the engine on
+    which steps the host rebuilt it (neighbor->ago == 0), so with c0go's
+    neighbor 0.6 / delay 3 / every 2 the run matches the reference fix's."""
+    import ref
+
+    assert ref.gpufix_available()
+    files, g = write_case(name, tmp_path)
+    skin, delay, every, check = neigh_of(g)
+    kw = dict(skin=skin, every=every, delay=delay, check=check)
+    cpu = ref.RefSystem(files, **kw)
+    gpu = ref.RefSystem(files, gpu_fix="fp64", **kw)
+    nsteps, dt, t0, t1, damp, seed = g["run"]
+    run = dict(dt=dt, langevin=True, t_start=t0, t_stop=t1, damp=damp, seed=int(seed))
+    t_cpu = cpu.run(int(nsteps), **run)
+    t_gpu = gpu.run(int(nsteps), **run)
+    assert gpu.nbuilds() == cpu.nbuilds() > 1
+    np.testing.assert_allclose(t_gpu, t_cpu, rtol=1e-6, atol=1e-6)
+    assert np.abs(gpu.get("x") - cpu.get("x")).max() < 1e-6
+    np.testing.assert_allclose(t_cpu, g["thermo"], rtol=1e-9, atol=1e-9)
+

@@ -9,7 +9,7 @@ import os
 import numpy as np
 import pytest
 
-from conftest import write_case
+from conftest import neigh_of, write_case
 
 pytestmark = pytest.mark.gpu
 
@@ -18,14 +18,14 @@ units real
 timestep {dt}
 dimension 3
 boundary s s s
-neighbor 5 bin
-neigh_modify delay 5
+neighbor {skin} bin
+neigh_modify delay {delay} every {every} check {check}
 atom_modify sort 0 0.0
 special_bonds fene
 atom_style awsemmd
 bond_style harmonic
 pair_style vexcluded 2 3.5 3.5
-read_data data.1r69
+read_data {data}
 pair_coeff * * 0.0
 pair_coeff 1 1 20.0 3.5 4.5
 pair_coeff 1 4 20.0 3.5 4.5
@@ -36,7 +36,7 @@ group beta_atoms type 4 5
 group oxygens type 3
 fix 1 all nve
 fix 11 all langevin {t0} {t1} {damp} {seed}
-fix 2 alpha_carbons backbone beta_atoms oxygens fix_backbone_coeff.data extended.seq
+fix 2 alpha_carbons backbone beta_atoms oxygens fix_backbone_coeff.data {seq}
 thermo {thermo}
 dump 1 all atom 10 run.dump
 dump_modify 1 sort id
@@ -51,11 +51,15 @@ write_restart restart.end
 """
 
 
-def run_deck(workdir, g, thermo):
+def run_deck(files, g, thermo):
     from awsemmd_b200 import lmp
 
+    workdir = files["workdir"]
     nsteps, dt, t0, t1, damp, seed = g["run"]
-    deck = DECK.format(dt=dt, t0=t0, t1=t1, damp=damp, seed=int(seed), nsteps=int(nsteps), thermo=thermo)
+    skin, delay, every, check = neigh_of(g)
+    deck = DECK.format(dt=dt, t0=t0, t1=t1, damp=damp, seed=int(seed), nsteps=int(nsteps), thermo=thermo,
+                       skin=skin, delay=delay, every=every, check="yes" if check else "no", data=files["data"],
+                       seq=files["seq"])
     cwd = os.getcwd()
     os.chdir(workdir)
     try:
@@ -68,14 +72,17 @@ def run_deck(workdir, g, thermo):
         os.chdir(cwd)
 
 
-@pytest.mark.parametrize("case", ["r1r69", "r1r69tb"])
+@pytest.mark.parametrize("case", ["r1r69", "r1r69tb", "r1r69go", "c0go"])
 def test_deck_reproduces_the_reference_run(case, tmp_path, gpu_lib):
-    """r1r69tb: fragment memory in the table form, as the shipped 1R69 decks use it."""
+    """r1r69tb: fragment memory in the table form, as the shipped 1R69 decks
+    use it; r1r69go and c0go: [AMH-Go], c0go with neighbor 0.6 and
+    neigh_modify delay 3 every 2 (the deck's settings decide when the list
+    AMH-Go reads is rebuilt)."""
     from awsemmd_b200 import lmp
 
     files, g = write_case(case, tmp_path)
     wd = files["workdir"]
-    run_deck(wd, g, thermo=5)
+    run_deck(files, g, thermo=5)
     rows = g["thermo"]  # per step: fix total, vexcluded, bonds, kinetic (reference, 20 Langevin steps)
     pe_ref, ke_ref = rows[:, 0] + rows[:, 1] + rows[:, 2], rows[:, 3]
     # fix print at steps 0, 5, 10, 15, 20
@@ -106,7 +113,7 @@ def test_output_cadence_does_not_change_the_trajectory(tmp_path, gpu_lib):
     files, g = write_case("r1r69", tmp_path)
     texts = []
     for thermo in (1, 20):
-        run_deck(files["workdir"], g, thermo=thermo)
+        run_deck(files, g, thermo=thermo)
         texts.append(open(os.path.join(files["workdir"], "restart.end")).read())
     assert texts[0] == texts[1]
 

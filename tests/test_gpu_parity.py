@@ -8,11 +8,11 @@ floor for terms that are ~0 on a given input):
 import numpy as np
 import pytest
 
-from conftest import write_case
+from conftest import neigh_of, write_case
 
 pytestmark = pytest.mark.gpu
 
-CASES = ["c0", "sheet", "r1r69", "r1r69tb"]
+CASES = ["c0", "sheet", "r1r69", "r1r69tb", "r1r69go", "r1r69go2", "c0go"]
 TOL = {"fp64": (1e-6, 1e-5), "mixed": (1e-5, 1e-4)}
 
 
@@ -35,6 +35,7 @@ def test_single_point_matches_reference(name, prec, tmp_path, gpu_lib):
     files, g = write_case(name, tmp_path)
     etol, ftol = TOL[prec]
     with AwsemSystem(files, precision=prec) as s:
+        s.set_neighbor(*neigh_of(g))
         f, e = s.compute(g["x0"], step=0)
         # energy floor: a term that is ~0 must stay ~0 relative to the total
         floor = 1e-3 * max(1.0, abs(g["e0"][0]) * 1e-6)
@@ -52,6 +53,7 @@ def test_term_groups_partition_the_forces(name, tmp_path, gpu_lib):
 
     files, g = write_case(name, tmp_path)
     with AwsemSystem(files, precision="fp64") as s:
+        s.set_neighbor(*neigh_of(g))
         fa, ea = s.compute(g["x0"])
         f1, e1 = s.compute(g["x0"], terms=TERMS_FIX)
         f2, e2 = s.compute(g["x0"], terms=TERMS_PAIR)
@@ -68,10 +70,12 @@ def test_trajectory_matches_reference(name, tmp_path, gpu_lib):
 
     files, g = write_case(name, tmp_path)
     nsteps, dt, t0, t1, damp, seed = g["run"]
+    skin, delay, every, check = neigh_of(g)
     with AwsemSystem(files, precision="fp64") as s:
+        s.set_neighbor(skin, delay, every, check)
         s.set_state(g["x0"], g["v0"])
         rows = s.run(int(nsteps), dt=dt, langevin=True, t_start=t0, t_stop=t1, damp=damp, seed=int(seed),
-                     thermo=True)
+                     skin=skin, thermo=True)
         x, v = s.get_state()
     assert np.abs(x - g["xN"]).max() < 1e-6
     assert np.abs(v - g["vN"]).max() < 1e-6

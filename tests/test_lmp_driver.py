@@ -76,6 +76,9 @@ class FakeEngine:
     def set_state(self, x, v):
         self.x, self.v = np.array(x, dtype=float), np.array(v, dtype=float)
 
+    def set_neighbor(self, skin, delay, every, check):
+        self.calls.append(("neighbor", skin, delay, every, check))
+
     def get_state(self):
         return self.x.copy(), self.v.copy()
 
@@ -164,6 +167,8 @@ def test_run_is_cut_at_output_steps(tmp_path):
     assert [(c[1], c[2], c[3]) for c in runs] == [(0, (0, 12), False), (5, (0, 12), True), (5, (0, 12), True),
                                                    (2, (0, 12), True)]
     assert all(c[4:] == (500.0, 300.0, True) for c in runs)  # the ramp spans the whole run
+    # `neigh_modify delay 5` reaches the engine with LAMMPS's defaults for the rest
+    assert ("neighbor", 5.0, 5, 1, True) in eng.calls
     # roles from the fix's groups, bonds as 0-based indices with the Bond Coeffs
     assert list(eng.kw["role"]) == [0, 2, 1, 0, 2, 1]
     assert list(eng.kw["bonds"][0]) == [0, 0, 0, 3] and list(eng.kw["bonds"][1]) == [3, 1, 2, 5]

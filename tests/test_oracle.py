@@ -4,9 +4,9 @@ import os
 import numpy as np
 import pytest
 
-from conftest import REFERENCE_SRC, write_case
+from conftest import REFERENCE_SRC, neigh_of, write_case
 
-CASES = ["c0", "sheet", "r1r69", "r1r69tb"]
+CASES = ["c0", "sheet", "r1r69", "r1r69tb", "r1r69go", "r1r69go2", "c0go"]
 
 
 def rel_err(a, b):
@@ -19,6 +19,7 @@ def test_oracle_forces_energies_match_reference(name, tmp_path, oracle_built):
 
     files, g = write_case(name, tmp_path)
     o = ref.OracleSystem(files)
+    o.set_neighbor(*neigh_of(g))
     f, e = o.compute(g["x0"])
     # the restatement follows the reference operation order: agreement is at
     # the last bits (energies) and 1e-13 of the largest force
@@ -35,6 +36,7 @@ def test_oracle_trajectory_matches_reference(name, tmp_path, oracle_built):
 
     files, g = write_case(name, tmp_path)
     o = ref.OracleSystem(files)
+    o.set_neighbor(*neigh_of(g))
     nsteps, dt, t0, t1, damp, seed = g["run"]
     x, v, thermo = o.run(g["x0"], g["v0"], int(nsteps), dt=dt, langevin=True, t_start=t0, t_stop=t1, damp=damp,
                          seed=int(seed))
@@ -47,9 +49,28 @@ def test_terms_exercised():
     """The fixtures between them exercise every term on the path."""
     e = {n: np.load(os.path.join(os.path.dirname(__file__), "golden", f"{n}.npz"))["e0"] for n in CASES}
     for k, name in [(1, "chain"), (3, "chi"), (4, "rama"), (6, "dssp"), (7, "p_ap"), (8, "water"), (9, "burial"),
-                    (10, "helix"), (12, "frag_mem"), (19, "bond")]:
+                    (10, "helix"), (11, "amh-go"), (12, "frag_mem"), (19, "bond")]:
         assert max(abs(e[c][k]) for c in CASES) > 1e-2, name
     assert max(abs(e[c][18]) for c in CASES) > 1.0  # vexcluded
+
+
+def test_amh_go_list_rule_is_pinned(tmp_path, oracle_built):
+    """c0go's trajectory depends on when LAMMPS rebuilds the fix's full list:
+    the oracle run with another rebuild rule, or another skin, leaves the
+    reference's trajectory by far more than the parity tolerance."""
+    import ref
+
+    files, g = write_case("c0go", tmp_path)
+    nsteps, dt, t0, t1, damp, seed = g["run"]
+    skin, delay, every, check = neigh_of(g)
+    assert (delay, every, check) != (0, 1, 1)
+    for wrong in [(skin, 0, 1, 0), (skin, delay, every, 0), (2.0, delay, every, check)]:
+        o = ref.OracleSystem(files)
+        o.set_neighbor(*wrong)
+        _, _, thermo = o.run(g["x0"], g["v0"], int(nsteps), dt=dt, langevin=True, t_start=t0, t_stop=t1,
+                             damp=damp, seed=int(seed))
+        o.close()
+        assert np.abs(thermo - g["thermo"]).max() > 1e-3, wrong
 
 
 def test_langevin_stream_shared(oracle_built):
