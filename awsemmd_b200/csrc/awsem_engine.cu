@@ -167,9 +167,13 @@ template <typename R> class Engine : public EngineBase {
   DBuf<unsigned char> tb_present;
   DBuf<int> go_start, go_partner;  // AMH-Go native contacts
   DBuf<double> go_rnat, go_gamma, go_sig_sq, go_norm;
-  DBuf<double> go_x0;              // AMH-Go list emulation: positions at the last build
-  DBuf<unsigned char> go_in;       // contacts in that list
-  DBuf<int> go_ago, go_over;       // per replica: steps since the build, half-skin flag
+  DBuf<unsigned char> go_in;       // AMH-Go contacts in the emulated full list
+  DBuf<double> lst_x0;             // emulated LAMMPS lists: positions at the last build
+  DBuf<int> lst_ago, lst_over, lst_build;  // per replica: steps since the build, half-skin flag, built now
+  DBuf<double> charge;             // Debye-Hueckel charges
+  DBuf<int> cr_start, cr_j;        // contact restraints
+  DBuf<double> cr_w, cr_r0;
+  int efix_slots = 5;
   int fm_groups = 0, fm_dsplit = 1;
   DBuf<double> thermo_rows;
   DBuf<int> res_sys, sys_begin, sys_end;
@@ -274,11 +278,18 @@ template <typename R> class Engine : public EngineBase {
     a.go_gamma = go_gamma.p;
     a.go_sig_sq = go_sig_sq.p;
     a.go_norm = go_norm.p;
-    const bool go_on = in.ff.p.terms & T_AMHGO;
-    a.go_x0 = go_on ? go_x0.p : nullptr;
-    a.go_in = go_on ? go_in.p : nullptr;
-    a.go_ago = go_on ? go_ago.p : nullptr;
-    a.go_over = go_on ? go_over.p : nullptr;
+    const bool lst_on = lists_emulated();
+    a.go_in = go_in.p;
+    a.lst_x0 = lst_on ? lst_x0.p : nullptr;
+    a.lst_ago = lst_on ? lst_ago.p : nullptr;
+    a.lst_over = lst_on ? lst_over.p : nullptr;
+    a.lst_build = lst_on ? lst_build.p : nullptr;
+    a.charge = charge.p;
+    a.cr_start = cr_start.p;
+    a.cr_j = cr_j.p;
+    a.cr_w = cr_w.p;
+    a.cr_r0 = cr_r0.p;
+    a.efix_slots = efix_slots;
     a.groups = groups;
     a.step = dstep.p;
     a.res_sys = res_sys.p;
@@ -379,15 +390,31 @@ template <typename R> class Engine : public EngineBase {
       go_gamma.upload(in.go.gamma.empty() ? std::vector<double>{0.0} : in.go.gamma, s0);
       go_sig_sq.upload(in.go.sig_sq.empty() ? std::vector<double>{1.0} : in.go.sig_sq, s0);
       go_norm.upload(in.go.norm, s0);
-      go_x0.alloc((size_t) 9 * nn);
-      go_x0.zero(s0);
       go_in.alloc(std::max<size_t>(in.go.partner.size(), 1));
       go_in.zero(s0);
-      go_ago.alloc((size_t) std::max(n_sys(), 1));
-      go_ago.zero(s0);
-      go_over.alloc((size_t) std::max(n_sys(), 1));
-      go_over.zero(s0);
     }
+    if (lists_emulated()) {
+      lst_x0.alloc((size_t) 9 * nn);
+      lst_x0.zero(s0);
+      for (DBuf<int> *b : {&lst_ago, &lst_over, &lst_build}) {
+        b->alloc((size_t) std::max(n_sys(), 1));
+        b->zero(s0);
+      }
+    }
+    if (in.ff.p.terms & T_DH) {
+      std::vector<double> q(in.charge);
+      q.resize((size_t) nn, 0.0);
+      charge.upload(q, s0);
+    }
+    if (in.ff.p.terms & T_CONTREST) {
+      std::vector<int> st(in.cr.start);
+      st.resize((size_t) nn + 1, st.empty() ? 0 : st.back());
+      cr_start.upload(st, s0);
+      cr_j.upload(in.cr.j.empty() ? std::vector<int>{0} : in.cr.j, s0);
+      cr_w.upload(in.cr.w.empty() ? std::vector<double>{0.0} : in.cr.w, s0);
+      cr_r0.upload(in.cr.r0.empty() ? std::vector<double>{0.0} : in.cr.r0, s0);
+    }
+    efix_slots = (in.ff.p.terms & (T_SSB | T_DH | T_CONTREST)) ? 8 : 5;
     CK(cudaFuncSetAttribute(dev::k_fragmem<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             4 * dev::fm_warp_smem<R>(true)));
     // pair-list radii of the terms
@@ -396,6 +423,7 @@ template <typename R> class Engine : public EngineBase {
     float rc = 0.f;
     for (int w = 0; w < p.n_wells; w++) rc = std::max(rc, (float) p.w_rmax_th[w]);
     if (p.terms & T_HELIX) rc = std::max(rc, (float) p.h_rmax_th);
+    if (p.terms & T_CONTREST) rc = std::max(rc, (float) sqrt(p.cr_cut_sq) * 1.0001f);
     st.r_contact = rc;
     st.r_dssp = (p.terms & T_DSSP) ? (float) p.dssp_cut : 0.f;
     st.r_pap = (p.terms & T_PAP) ? (float) sqrt(p.pap_cutoff_sq) : 0.f;
@@ -407,15 +435,16 @@ template <typename R> class Engine : public EngineBase {
     st.r_ev = (float) evmax;
     st.skin = (float) skin;
     // LAMMPS defaults: neigh_modify delay 0 every 1 check yes
-    st.go_skin = skin;
-    st.go_delay = 0;
-    st.go_every = 1;
-    st.go_check = 1;
-    st.go_force = 1;
+    st.lst_skin = skin;
+    st.lst_delay = 0;
+    st.lst_every = 1;
+    st.lst_check = 1;
+    st.lst_force = 1;
+    st.lst_pair_cut = pair_cut_now();
     CK(cudaMemcpyAsync(nl.p, &st, sizeof st, cudaMemcpyHostToDevice, s0));
     long long s = step;
     CK(cudaMemcpyAsync(dstep.p, &s, sizeof s, cudaMemcpyHostToDevice, s0));
-    e_fix.alloc((size_t) 5 * nn);
+    e_fix.alloc((size_t) efix_slots * nn);
     e_fix.zero(s0);
     dacc.alloc((size_t) 3 * nn);
     dacc.zero(s0);
@@ -542,13 +571,18 @@ template <typename R> class Engine : public EngineBase {
     bool fm = (a.groups & dev::G_FIX) && p.fm_nd > 0;
     const bool fmt = (a.groups & dev::G_FIX) && (p.terms & T_FM_TABLE);
     const bool go = (a.groups & dev::G_FIX) && (p.terms & T_AMHGO);
-    if (fm || fmt || go) {
+    const bool px = (a.groups & dev::G_FIX) && (p.terms & (T_SSB | T_DH | T_CONTREST));
+    // the emulated lists' decision for this step, before anything reads it
+    if (lists_emulated())
+      dev::k_list_decide<<<(n_sys() + 127) / 128, 128, 0, s0>>>(nl.p, n_sys(), lst_ago.p, lst_over.p, lst_build.p);
+    if (fm || fmt || go || px) {
       // fragment memory is independent of the pair passes: second stream
       CK(cudaEventRecord(ev_fork, s0));
       CK(cudaStreamWaitEvent(s1, ev_fork, 0));
       if (fm) dev::k_fragmem<R><<<fm_blocks(), tb, fm_smem(), s1>>>(a, p);
       if (fmt) dev::k_fm_table<R><<<fm_table_blocks(), tb, 0, s1>>>(a, p);
       if (go) dev::k_amh_go<R><<<nb, tb, 0, s1>>>(a, p);
+      if (px) dev::k_pair_extra<R><<<pair_blocks, tb, 0, s1>>>(a, p);
       CK(cudaEventRecord(ev_join, s1));
     }
     dev::k_density<R><<<pair_blocks, tb, 0, s0>>>(a, p);
@@ -556,7 +590,7 @@ template <typename R> class Engine : public EngineBase {
     dev::k_water_xi<R><<<pair_blocks, tb, 0, s0>>>(a, p);
     dev::k_pair<R><<<pair_blocks, tb, 0, s0>>>(a, p);
     dev::k_hbond<R><<<hb_blocks, 128, 0, s0>>>(a, p);
-    if (fm || fmt || go) CK(cudaStreamWaitEvent(s0, ev_join, 0));
+    if (fm || fmt || go || px) CK(cudaStreamWaitEvent(s0, ev_join, 0));
   }
 
   int fm_table_blocks() const
@@ -580,7 +614,8 @@ template <typename R> class Engine : public EngineBase {
   void reduce_energies(int rep0 = 0, int count = -1)
   {
     dim3 grid(E_SLOTS, count < 0 ? n_sys() : count);
-    dev::k_energy_reduce<<<grid, 256, 0, s0>>>(e_res.p, e_fix.p, n(), sys_begin.p, sys_end.p, energy.p, rep0);
+    dev::k_energy_reduce<<<grid, 256, 0, s0>>>(e_res.p, e_fix.p, efix_slots, n(), sys_begin.p, sys_end.p, energy.p,
+                                               rep0);
   }
 
   void need_single(const char *what)
@@ -601,13 +636,14 @@ template <typename R> class Engine : public EngineBase {
     CK(cudaMemcpyAsync(dstep.p, &st, sizeof st, cudaMemcpyHostToDevice, s0));
     step = st;
     zero_unwritten_energies(groups);
-    if (in.ff.p.terms & T_AMHGO) {
-      // the host's MD loop decides whether this evaluation's list is new
-      set_go_flags(next_compute_built, 1);
+    if (lists_emulated()) {
+      // the host's MD loop decides whether this evaluation's lists are new
+      set_list_flags(next_compute_built, 1);
       next_compute_built = 1;
     }
     auto a = args(groups);
     launch_eval(a, false);
+    if (lists_emulated()) dev::k_list_hold<R><<<(n_run() + 127) / 128, 128, 0, s0>>>(a);
     int tb = 256;
     dev::k_total_force<R><<<(3 * na + tb - 1) / tb, tb, 0, s0>>>(a, ftot.p);
     reduce_energies();
@@ -767,7 +803,7 @@ template <typename R> class Engine : public EngineBase {
         dev::k_finish<R><<<nb, tb, 0, s0>>>(a, d_integ.p, g1.p, g2.p, ftot.p, x.p);
       }
       if (thermo)
-        dev::k_thermo<<<n_sys(), 256, 0, s0>>>(e_res.p, e_fix.p, nn, dstep.p, d_integ.p, sys_begin.p, sys_end.p,
+        dev::k_thermo<<<n_sys(), 256, 0, s0>>>(e_res.p, e_fix.p, efix_slots, nn, dstep.p, d_integ.p, sys_begin.p, sys_end.p,
                                                thermo_nrows, thermo_rows.p);
     }
     CK(cudaStreamEndCapture(s0, &graph));
@@ -816,7 +852,9 @@ template <typename R> class Engine : public EngineBase {
     dev::PersistArgs q{d_integ.p, g1.p, g2.p, ftot.p, x.p, gbar.p, n_run(), ps_stream,
                        fm ? ps_ring_warps() : 0, fm ? std::min(fm_groups, (n_run() + 31) / 32) * fm_dsplit : 0,
                        (a.groups & dev::G_FIX) && (in.ff.p.terms & T_FM_TABLE) ? 1 : 0,
-                       (a.groups & dev::G_FIX) && (in.ff.p.terms & T_AMHGO) ? 1 : 0};
+                       (a.groups & dev::G_FIX) && (in.ff.p.terms & T_AMHGO) ? 1 : 0,
+                       (a.groups & dev::G_FIX) && (in.ff.p.terms & (T_SSB | T_DH | T_CONTREST)) ? 1 : 0,
+                       lists_emulated() ? n_sys() : 0};
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(ps_grid_now);
     cfg.blockDim = dim3(dev::kStepThreads);
@@ -852,12 +890,13 @@ template <typename R> class Engine : public EngineBase {
     if (skin_ > 0 && skin_ != skin) {
       skin = skin_;
       set_nl_field(&dev::NLState::skin, (float) skin);
-      set_nl_field(&dev::NLState::go_skin, skin);
+      set_nl_field(&dev::NLState::lst_skin, skin);
+      set_nl_field(&dev::NLState::lst_pair_cut, pair_cut_now());
       set_nl_field(&dev::NLState::r_list, 0.f);  // the next evaluation rebuilds the pair list
     }
-    set_nl_field(&dev::NLState::go_delay, delay);
-    set_nl_field(&dev::NLState::go_every, every);
-    set_nl_field(&dev::NLState::go_check, check);
+    set_nl_field(&dev::NLState::lst_delay, delay);
+    set_nl_field(&dev::NLState::lst_every, every);
+    set_nl_field(&dev::NLState::lst_check, check);
     CK(cudaStreamSynchronize(s0));
   }
 
@@ -1065,6 +1104,7 @@ template <typename R> class Engine : public EngineBase {
             if (fm) dev::k_fragmem<R><<<fm_blocks(), tb, fm_smem(), s0>>>(a, p);
             if (p.terms & T_FM_TABLE) dev::k_fm_table<R><<<fm_table_blocks(), tb, 0, s0>>>(a, p);
             if (p.terms & T_AMHGO) dev::k_amh_go<R><<<nb, tb, 0, s0>>>(a, p);
+            if (p.terms & (T_SSB | T_DH | T_CONTREST)) dev::k_pair_extra<R><<<pair_blocks, tb, 0, s0>>>(a, p);
             break;
           case 9: dev::k_finish<R><<<nb, tb, 0, s0>>>(a, d_integ.p, g1.p, g2.p, ftot.p, x.p); break;
         }
@@ -1244,11 +1284,12 @@ template <typename R> class Engine : public EngineBase {
     if (rp.skin > 0 && rp.skin != skin) {
       skin = rp.skin;
       set_nl_field(&dev::NLState::skin, (float) skin);
-      set_nl_field(&dev::NLState::go_skin, skin);
+      set_nl_field(&dev::NLState::lst_skin, skin);
+      set_nl_field(&dev::NLState::lst_pair_cut, pair_cut_now());
     }
     // a run's first evaluation is its setup: LAMMPS builds every list there;
     // the engine decides the later builds
-    if (!cont && (in.ff.p.terms & T_AMHGO)) set_go_flags(1, 0);
+    if (!cont && lists_emulated()) set_list_flags(1, 0);
     if (rp.neigh_every != neigh_every) {
       neigh_every = rp.neigh_every;
       set_nl_field(&dev::NLState::every, neigh_every);
@@ -1319,13 +1360,21 @@ template <typename R> class Engine : public EngineBase {
 
   int next_compute_built = 1;  // awsem_set_list_built: the next awsem_compute's list is new
 
-  void set_go_flags(int force, int host)
+  // terms that read list membership itself: LAMMPS's lists are emulated
+  bool lists_emulated() const { return in.ff.p.terms & (T_AMHGO | T_SSB | T_DH | T_CONTREST); }
+  // the CA-CA reach of the fix's half list the residue pair list must cover (0: no term needs it)
+  float pair_cut_now() const
+  {
+    return (in.ff.p.terms & (T_SSB | T_DH)) ? (float) (in.ff.p.pair_list_cutoff + skin) * 1.0001f : 0.f;
+  }
+
+  void set_list_flags(int force, int host)
   {
     dev::NLState st;
     CK(cudaMemcpyAsync(&st, nl.p, sizeof st, cudaMemcpyDeviceToHost, s0));
     CK(cudaStreamSynchronize(s0));
-    st.go_force = force;
-    st.go_host = host;
+    st.lst_force = force;
+    st.lst_host = host;
     CK(cudaMemcpyAsync(nl.p, &st, sizeof st, cudaMemcpyHostToDevice, s0));
   }
 
@@ -1463,6 +1512,8 @@ template <typename R> class Engine : public EngineBase {
     if (f.ff.p.terms & T_FM_TABLE)
       throw std::invalid_argument("serving handles do not support [Fragment_Memory_Table] (use [Fragment_Memory])");
     if (f.ff.p.terms & T_AMHGO) throw std::invalid_argument("serving handles do not support [AMH-Go]");
+    if (f.ff.p.terms & (T_SSB | T_DH | T_CONTREST))
+      throw std::invalid_argument("serving handles do not support [Solvent_Barrier], [DebyeHuckel] or [Contact_Restraints]");
     const long long groups = (cap_res + 31) / 32;
     if (groups * 32 * pairs_per_res >= (1ll << 31)) throw std::invalid_argument("residue capacity too large");
     sf = &f;
@@ -1812,7 +1863,8 @@ template <typename R> class Engine : public EngineBase {
     add(ev_pref), add(ev_cs), add(ev_cl), add(excl_self), add(excl_next), add(bond_i), add(bond_j), add(bond_k);
     add(bond_r0), add(fm_soff), add(fm_slen), add(fm_rf), add(fm_coef), add(tb_data), add(tb_present);
     add(go_start), add(go_partner), add(go_rnat), add(go_gamma), add(go_sig_sq), add(go_norm);
-    add(go_x0), add(go_in), add(go_ago), add(go_over);
+    add(go_in), add(lst_x0), add(lst_ago), add(lst_over), add(lst_build), add(charge), add(cr_start), add(cr_j),
+        add(cr_w), add(cr_r0);
     add(thermo_rows), add(res_sys), add(sys_begin);
     add(sys_end), add(sys_seed), add(slot_run), add(d_integ);
     return b;

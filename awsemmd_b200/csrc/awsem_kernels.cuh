@@ -49,13 +49,18 @@ struct NLState {
   int npairs;         // pairs in the residue pair list (may exceed its capacity: overflow)
   int fm_timeout;     // a fragment-memory stream wait gave up (results invalid)
   int tb_error;       // table fragment memory: 1 a distance outside the table's range, 2 a grid index outside it
-  // AMH-Go reads the fix's full neighbour list, whose membership is fixed at
-  // each LAMMPS list build: that list's rebuild rule is emulated per replica
-  double go_skin;     // neighbor skin (A)
-  int go_delay, go_every, go_check;  // neigh_modify delay / every / check
-  int go_force;       // host: the next evaluation is a run setup (the list is built)
-  int go_setup;       // this evaluation is a run setup
-  int go_host;        // the host decides the builds (awsem_compute): go_setup alone
+  // The reference fix reads LAMMPS's neighbour lists, whose membership is
+  // fixed at each list build.  Terms that use list membership itself (AMH-Go;
+  // Debye-Hueckel and the solvent barrier on the CA pairs of the half list)
+  // follow LAMMPS's rebuild rule, emulated per replica (k_list_decide).
+  double lst_skin;    // neighbor skin (A)
+  int lst_delay, lst_every, lst_check;  // neigh_modify delay / every / check
+  int lst_force;      // host: the next evaluation is a run setup (the lists are built)
+  int lst_setup;      // this evaluation is a run setup
+  int lst_host;       // the host decides the builds (awsem_compute): lst_setup alone
+  float lst_pair_cut; // CA-CA reach of the half list (pair-list cutoff + skin) the
+                      // CA-pair terms need covered by the residue pair list (0: none)
+  float lst_d2max;    // max CA displacement^2 since the last emulated build (this step)
 };
 
 // Run window of one replica: integrated over steps begin..end (the
@@ -109,9 +114,15 @@ template <typename R> struct StepArgs {
   // AMH-Go native contacts per CA / CB atom slot 2 r + b ([2 n_res + 1] offsets), per residue normalisation
   const int *go_start, *go_partner;
   const double *go_rnat, *go_gamma, *go_sig_sq, *go_norm;
-  double *go_x0;                 // [9 n]: positions at the replica's last list build
-  unsigned char *go_in;          // per contact: in the list since that build
-  int *go_ago, *go_over;         // per replica: steps since the build; an atom moved over half the skin
+  unsigned char *go_in;          // per AMH-Go contact: in the list since the last build
+  double *lst_x0;                // [9 n]: positions at the replica's last list build
+  int *lst_ago, *lst_over;       // per replica: steps since the build; an atom moved over half the skin
+  const int *lst_build;          // per replica: this evaluation builds the lists
+  // Debye-Hueckel, solvent barrier, contact restraints (k_pair_extra)
+  const double *charge;          // [n]: charge of the residue
+  const int *cr_start, *cr_j;    // contact restraints of residue i (i < j): [cr_start[i], cr_start[i+1])
+  const double *cr_w, *cr_r0;
+  int efix_slots;                // fixed-point energy slots in use (5, or 8 with the pair terms above)
   int groups;       // AWSEM_TERMS_* bits: 1 fix backbone, 2 pair vexcluded, 4 bonds
   long long *step;   // device step counter (advanced by k_nl_decide)
   // replicas: residue -> replica, replica residue ranges, Langevin seeds
@@ -142,7 +153,7 @@ __device__ __forceinline__ void atomic_max_f(float *addr, float v)
 
 template <typename R> __device__ __forceinline__ void prepare_pass(const StepArgs<R> &a, const FFParams &p, Span sp)
 {
-  float d2 = 0.f, oO = 0.f, oN = 0.f, oCA = 0.f, oAll = 0.f, oX = 0.f, oNCA = 0.f;
+  float d2 = 0.f, oO = 0.f, oN = 0.f, oCA = 0.f, oAll = 0.f, oX = 0.f, oNCA = 0.f, dl = 0.f;
   const int lane = threadIdx.x & 31;
   // warp-uniform trip count: the maxima are reduced across the warp below
   for (int r0 = sp.t - lane; r0 < a.n_run; r0 += sp.nthr) {
@@ -150,7 +161,7 @@ template <typename R> __device__ __forceinline__ void prepare_pass(const StepArg
   if (r < a.n_run) {
     unsigned long long *f = a.s.facc + (size_t) 9 * r;
     for (int k = 0; k < 9; k++) f[k] = 0ull;
-    for (int k = 0; k < 5; k++) a.e_fix[(size_t) k * a.s.n_res + r] = 0;
+    for (int k = 0; k < a.efix_slots; k++) a.e_fix[(size_t) k * a.s.n_res + r] = 0;
     for (int k = 0; k < 3; k++) a.dacc[(size_t) k * a.s.n_res + r] = 0;
   }
   if (r < a.n_run && a.res_sys[r] >= 0) {
@@ -175,18 +186,20 @@ template <typename R> __device__ __forceinline__ void prepare_pass(const StepArg
         cp[k] = __dadd_rn(__dadd_rn(__dmul_rn(p.ap, ca[k]), __dmul_rn(p.bp, ca1)), __dmul_rn(p.cp, o[k]));
       }
     }
-    if (a.go_x0) {
-      // LAMMPS check_distance for the AMH-Go list: an atom farther than half
-      // the skin from where it was at the last build
-      const double trig = 0.25 * a.nl->go_skin * a.nl->go_skin;
-      const double *h = a.go_x0 + (size_t) 9 * r;
+    if (a.lst_x0) {
+      // LAMMPS check_distance for the emulated lists: an atom farther than
+      // half the skin from where it was at the last build
+      const double trig = 0.25 * a.nl->lst_skin * a.nl->lst_skin;
+      const double *h = a.lst_x0 + (size_t) 9 * r;
       bool over = false;
       for (int b = 0; b < 3; b++) {
         const double *q = b == 0 ? ca : b == 1 ? cb : o;
         const double dx = q[0] - h[3 * b], dy = q[1] - h[3 * b + 1], dz = q[2] - h[3 * b + 2];
-        if (dx * dx + dy * dy + dz * dz > trig) over = true;
+        const double d2b = dx * dx + dy * dy + dz * dz;
+        if (d2b > trig) over = true;
+        if (b == 0) dl = fmaxf(dl, (float) d2b * 1.0001f);
       }
-      if (over) a.go_over[a.res_sys[r]] = 1;
+      if (over) a.lst_over[a.res_sys[r]] = 1;
     }
     double4 *w = const_cast<double4 *>(a.s.pos) + (size_t) r * N_BEADS;
     w[B_CA] = make_double4(ca[0], ca[1], ca[2], 0.0);
@@ -230,20 +243,21 @@ template <typename R> __device__ __forceinline__ void prepare_pass(const StepArg
     oAll = fmaxf(oAll, __shfl_xor_sync(0xffffffffu, oAll, s));
     oX = fmaxf(oX, __shfl_xor_sync(0xffffffffu, oX, s));
     oNCA = fmaxf(oNCA, __shfl_xor_sync(0xffffffffu, oNCA, s));
+    dl = fmaxf(dl, __shfl_xor_sync(0xffffffffu, dl, s));
   }
-  __shared__ float red[7][32];
+  __shared__ float red[8][32];
   if (lane == 0) {
     const int w = threadIdx.x >> 5;
     red[0][w] = d2, red[1][w] = oO, red[2][w] = oN, red[3][w] = oCA, red[4][w] = oAll, red[5][w] = oX;
-    red[6][w] = oNCA;
+    red[6][w] = oNCA, red[7][w] = dl;
   }
   __syncthreads();
-  if (threadIdx.x < 7) {
+  if (threadIdx.x < 8) {
     const int k = threadIdx.x;
     float m = 0.f;
     for (int w = 0; w < (int) (blockDim.x >> 5); w++) m = fmaxf(m, red[k][w]);
     float *dst = k == 0 ? &a.nl->d2max : k == 1 ? &a.nl->bO : k == 2 ? &a.nl->bN : k == 3 ? &a.nl->bCA
-               : k == 4 ? &a.nl->bAll : k == 5 ? &a.nl->bCAx : &a.nl->bNCA;
+               : k == 4 ? &a.nl->bAll : k == 5 ? &a.nl->bCAx : k == 6 ? &a.nl->bNCA : &a.nl->lst_d2max;
     if (m > 0.f) atomic_max_f(dst, m);  // the maxima start each step at 0
   }
 }
@@ -260,6 +274,10 @@ __device__ __forceinline__ void nl_decide(NLState *nl, int force, long long *ste
   if (step) (*step)++;
   NLState &s = *nl;
   float need = fmaxf(fmaxf(s.r_contact, s.r_dssp + s.bO + s.bN), fmaxf(s.r_pap + 2.f * s.bCA, s.r_ev + 2.f * s.bAll));
+  // residue pairs whose CAs were within the half list's reach at the last
+  // emulated build: their contact beads are at most that reach + twice the
+  // CA displacement since then + twice the CA-to-contact-bead offset apart
+  if (s.lst_pair_cut > 0.f) need = fmaxf(need, s.lst_pair_cut + 2.f * sqrtf(s.lst_d2max) + 2.f * s.bCA + 0.01f);
   float disp = sqrtf(s.d2max);
   bool rb = force || s.r_list <= 0.f || need + 2.f * disp > s.r_list || (s.every > 0 && s.steps_since + 1 >= s.every);
   if (rb) {
@@ -280,8 +298,9 @@ __device__ __forceinline__ void nl_decide(NLState *nl, int force, long long *ste
   s.dssp_pre_sq = dpre * dpre;
   s.d2max = s.bO = s.bN = s.bCA = s.bAll = s.bCAx = s.bNCA = 0.f;
   s.n_dssp = s.n_pap = 0;
-  s.go_setup = s.go_force;
-  s.go_force = 0;
+  s.lst_setup = s.lst_force;
+  s.lst_force = 0;
+  s.lst_d2max = 0.f;
 }
 
 __global__ void k_nl_decide(NLState *nl, int force, long long *step) { nl_decide(nl, force, step); }
@@ -1038,27 +1057,154 @@ template <typename R> __device__ __forceinline__ void fm_table_pass(const StepAr
 
 template <typename R> __global__ void k_fm_table(StepArgs<R> a, FFParams p) { fm_table_pass(a, p, grid_span()); }
 
-// LAMMPS Neighbor::decide() for the fix's full list of replica `rep`: the
-// list is built at a run setup; otherwise `ago` counts the steps since the
-// last build and the list is rebuilt once ago >= delay and ago % every == 0,
-// unconditionally without check, with check only if an atom has moved more
-// than half the skin since that build.  Read by the AMH-Go pass and by the
-// replica's first residue in the finish pass, which then advances the state.
-template <typename R> __device__ __forceinline__ bool go_list_build(const StepArgs<R> &a, int rep)
+// LAMMPS Neighbor::decide() per replica, for the emulated lists: built at a
+// run setup; otherwise `ago` counts the steps since the last build and the
+// lists are rebuilt once ago >= delay and ago % every == 0, unconditionally
+// without check, with check only if an atom has moved more than half the
+// skin since that build (lst_over, set by the prepare pass).  On a handle
+// driven by awsem_compute the host decides (lst_setup alone).  Runs between
+// the prepare pass and the passes that read lst_build; the finish pass then
+// records the positions of a build.
+__device__ __forceinline__ void list_decide_one(const NLState &nl, int *ago, int *over, int *built, int rep)
 {
-  const NLState &nl = *a.nl;
-  if (nl.go_setup) return true;
-  if (nl.go_host) return false;
-  const int ago = a.go_ago[rep] + 1;
-  if (ago < nl.go_delay || ago % nl.go_every != 0) return false;
-  return !nl.go_check || a.go_over[rep] != 0;
+  bool b;
+  if (nl.lst_setup) {
+    b = true;
+  } else if (nl.lst_host) {
+    b = false;
+  } else {
+    const int g = ago[rep] + 1;
+    b = g >= nl.lst_delay && g % nl.lst_every == 0 && (!nl.lst_check || over[rep] != 0);
+  }
+  built[rep] = b;
+  ago[rep] = b ? 0 : ago[rep] + 1;
+  over[rep] = 0;
 }
+
+__global__ void k_list_decide(const NLState *nl, int n_sys, int *ago, int *over, int *built)
+{
+  const int rep = blockIdx.x * blockDim.x + threadIdx.x;
+  if (rep < n_sys) list_decide_one(*nl, ago, over, built, rep);
+}
+
+// awsem_compute has no finish pass: record the positions of a build here
+template <typename R> __global__ void k_list_hold(StepArgs<R> a)
+{
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= a.n_run || a.res_sys[r] < 0 || !a.lst_build[a.res_sys[r]]) return;
+  for (int k = 0; k < 9; k++) a.lst_x0[(size_t) 9 * r + k] = a.x[(size_t) 9 * r + k];
+}
+
+// Terms of the reference's DL3 loop (fix_backbone.cpp:7956-8134) that the
+// benchmark force field leaves off, one thread per listed residue pair i < j,
+// on the second stream beside the pair passes:
+//   contact restraints (:8058-8060, :8152-8177) on the contact beads, for
+//     restrained pairs closer than the global cutoff that are in the fix's
+//     half list (contact beads within the pair-list cutoff plus the skin at
+//     the last list build);
+//   solvent-separated barrier (:8109-8110, :6237-6305) and Debye-Hueckel
+//     (:8112-8113, :6307-6363), evaluated for every CA pair of the fix's half
+//     list -- CAs within the pair-list cutoff plus the skin at the replica's
+//     last list build, 1-2 bonded pairs removed -- on the contact beads.
+// Forces to the fixed-point accumulators; energies to fixed-point slots 5-7.
+template <typename R> __device__ __forceinline__ void pair_extra_pass(const StepArgs<R> &a, const FFParams &p, Span sp)
+{
+  const DevSys<R> &s = a.s;
+  const int n = s.n_res;
+  if (!(a.groups & G_FIX)) return;
+  const uint32_t T = p.terms;
+  unsigned long long *e_ssb = (unsigned long long *) a.e_fix + (size_t) 5 * n;
+  unsigned long long *e_dh = (unsigned long long *) a.e_fix + (size_t) 6 * n;
+  unsigned long long *e_cr = (unsigned long long *) a.e_fix + (size_t) 7 * n;
+  const double cut = p.pair_list_cutoff + a.nl->lst_skin, cutsq = cut * cut;
+  const int np = min(a.nl->npairs, a.pcap);
+  for (int q = sp.t; q < np; q += sp.nthr) {
+    const int2 ij = a.pairs[q];
+    const int i = ij.x, j = ij.y;
+    const bool other = s.res_chain[j] != s.res_chain[i];
+    const int dij = j - i;
+    if (!other && dij <= 1) continue;  // the contact-bead branch and every CA-pair term need more
+    const bool gi = s.res_flags[i] & R_GLY, gj = s.res_flags[j] & R_GLY;
+    const V3<double> ci = bead(s, i, gi ? B_CA : B_CB), cj = bead(s, j, gj ? B_CA : B_CB);
+    const V3<double> d = {ci.x - cj.x, ci.y - cj.y, ci.z - cj.z};
+    const double rsq = norm2(d);
+    double force = 0.0;
+    const bool build = a.lst_build[a.res_sys[i]];
+    const double *h = a.lst_x0;
+    // contact restraints: the restraint listed for (i, j), if any
+    bool cr_on = (T & T_CONTREST) && a.cr_start[i] < a.cr_start[i + 1] && rsq < p.cr_cut_sq;
+    if (cr_on && !build) {  // on a build step the bead pair is within reach (rsq < cr_cut_sq <= cutsq)
+      const int bi = 9 * i + 3 * (gi ? 0 : 1), bj = 9 * j + 3 * (gj ? 0 : 1);
+      cr_on = norm2(V3<double>{h[bi] - h[bj], h[bi + 1] - h[bj + 1], h[bi + 2] - h[bj + 2]}) < cutsq;
+    }
+    if (cr_on) {
+      for (int k = a.cr_start[i]; k < a.cr_start[i + 1]; k++) {
+        if (a.cr_j[k] != j) continue;
+        const double r = sqrt(rsq), dr = r - a.cr_r0[k];
+        if (fabs(dr) < p.cr_dr_cut) {
+          const double V = -a.cr_w[k] * exp(-0.5 * (dr * dr) * p.cr_sigma_sq_inv);
+          force += V * dr * p.cr_sigma_sq_inv / r;
+          atomicAdd(e_cr + i, (unsigned long long) fix_force(V));
+        }
+        break;
+      }
+    }
+    // CA pair of the fix's half list?
+    if (T & (T_SSB | T_DH)) {
+      const double *c = build ? a.x : h;
+      bool in_list = norm2(V3<double>{c[9 * i] - c[9 * j], c[9 * i + 1] - c[9 * j + 1], c[9 * i + 2] - c[9 * j + 2]}) < cutsq;
+      if (in_list && dij == 1 && (a.excl_next[i] & 1u)) in_list = false;  // CA(i)-CA(i+1) bonded
+      if (in_list) {
+        const double r = sqrt(rsq);
+        if ((T & T_SSB) && (other || dij >= p.ssb_ij_sep)) {
+          double rmin1 = p.ssb_rmin1, rmax1 = p.ssb_rmax1, rmin2 = p.ssb_rmin2, rmax2 = p.ssb_rmax2;
+          if (p.ssb_rad_cor) {
+            const double sh = p.ssb_rshift[s.res_type[i]] + p.ssb_rshift[s.res_type[j]];
+            rmin1 += sh;
+            rmax1 += sh;
+            rmin2 += sh;
+            rmax2 += sh;
+          }
+          if (!(r > rmax1 + 10 / p.ssb_kappa && r > rmax2 + 10 / p.ssb_kappa)) {
+            const double tn1 = tanh(p.ssb_kappa * (r - rmin1)), tx1 = tanh(p.ssb_kappa * (rmax1 - r));
+            const double tn2 = tanh(p.ssb_kappa * (r - rmin2)), tx2 = tanh(p.ssb_kappa * (rmax2 - r));
+            const double th1 = 0.5 * (tn1 + tx1), th2 = 0.5 * (tn2 + tx2);
+            const double e = p.epsilon * p.k_ssb1 * th1 + p.epsilon * p.k_ssb2 * th2;
+            atomicAdd(e_ssb + i, (unsigned long long) fix_force(e));
+            force += -p.epsilon * p.k_ssb1 * p.ssb_kappa * th1 * (tx1 - tn1) / r;
+            force += -p.epsilon * p.k_ssb2 * p.ssb_kappa * th2 * (tx2 - tn2) / r;
+          }
+        }
+        if ((T & T_DH) && dij > 1 && dij >= p.dh_min_sep) {
+          const double qi = a.charge[i], qj = a.charge[j];
+          double qq = 0.0;
+          if (qi > 0.0 && qj > 0.0) qq = p.k_plusplus * qi * qj / r;
+          else if (qi < 0.0 && qj < 0.0) qq = p.k_minusminus * qi * qj / r;
+          else if ((qi < 0.0 && qj > 0.0) || (qi > 0.0 && qj < 0.0)) qq = p.k_plusminus * qi * qj / r;
+          if (qq != 0.0) {
+            const double e = p.epsilon * qq * exp(-p.k_screening * r / p.screening_length);
+            atomicAdd(e_dh + i, (unsigned long long) fix_force(e));
+            force += (e / r) * (1.0 / r + p.k_screening / p.screening_length);
+          }
+        }
+      }
+    }
+    if (force != 0.0) {
+      const long long f[3] = {fix_force(force * d.x), fix_force(force * d.y), fix_force(force * d.z)};
+      const long long g[3] = {-f[0], -f[1], -f[2]};
+      scatter_fix(s, i, gi ? B_CA : B_CB, f);
+      scatter_fix(s, j, gj ? B_CA : B_CB, g);
+    }
+  }
+}
+
+template <typename R> __global__ void k_pair_extra(StepArgs<R> a, FFParams p) { pair_extra_pass(a, p, grid_span()); }
 
 // AMH-Go (FixBackbone::compute_amh_go_model, fix_backbone.cpp:3856-3992) of
 // residue r's CA and CB: over each atom's native contacts (the full-list
 // partners with a native distance below rc) that are in the fix's full
 // neighbour list -- pairs within the pair-list cutoff plus the skin at the
-// list's last build, which a build step records -- and whose deviation passes
+// list's last build (k_list_decide), which a build step records -- and whose deviation passes
 // dr^2 < 27.6 sigma^2, E_i = sum gamma exp(-dr^2 / 2 sigma^2); the atom's
 // energy is -k E_i^p / (2 a) and each contact's force is scaled by
 // -k p E_i^(p-1) / (2 a) (a: the normalisation).  FP64 in both forms; forces
@@ -1066,10 +1212,8 @@ template <typename R> __device__ __forceinline__ bool go_list_build(const StepAr
 template <typename R> __device__ __forceinline__ void amh_go_residue(const StepArgs<R> &a, const FFParams &p, int r)
 {
   const DevSys<R> &s = a.s;
-  const bool build = go_list_build(a, a.res_sys[r]);
-  const double cut = p.pair_list_cutoff + a.nl->go_skin, cutsq = cut * cut;
-  if (build)
-    for (int k = 0; k < 9; k++) a.go_x0[(size_t) 9 * r + k] = a.x[(size_t) 9 * r + k];
+  const bool build = a.lst_build[a.res_sys[r]];
+  const double cut = p.pair_list_cutoff + a.nl->lst_skin, cutsq = cut * cut;
   double E = 0.0;
   for (int b = 0; b < 2; b++) {
     const int c0 = a.go_start[2 * r + b], c1 = a.go_start[2 * r + b + 1];
@@ -1158,12 +1302,8 @@ __device__ __forceinline__ void finish_one(const StepArgs<R> &a, const Integrato
   const SlotRun sr = a.slot_run[rep];
   if (step < sr.begin || step > sr.end) return;
   const bool final_kick = step > sr.begin, next = step < sr.end && step < in.stop;
-  if (a.go_ago && r == a.sys_begin[rep]) {
-    // the AMH-Go list state moves on once every reader of this step is done
-    const bool built = go_list_build(a, rep);
-    a.go_ago[rep] = built ? 0 : a.go_ago[rep] + 1;
-    a.go_over[rep] = 0;
-  }
+  if (a.lst_x0 && a.lst_build[rep])  // the emulated lists were built at these positions
+    for (int k = 0; k < 9; k++) a.lst_x0[(size_t) 9 * r + k] = x_out[(size_t) 9 * r + k];
   const unsigned long long seed = a.sys_seed[rep];
   const long long key = step - sr.step0;  // the replica's own step count keys its noise
   // Every multiply and add below is rounded on its own (no contraction), as
@@ -1270,7 +1410,7 @@ template <typename R> __global__ void k_total_force(StepArgs<R> a, double *ftot)
 
 // Thermo row of the current step: [fix total, vexcluded, bonds, kinetic],
 // residue sums in a fixed tree order (one block of 256 threads).
-__global__ void k_thermo(const double *e_res, const long long *e_fix, int n_res, const long long *step,
+__global__ void k_thermo(const double *e_res, const long long *e_fix, int efix_slots, int n_res, const long long *step,
                          const Integrator *inp, const int *sys_begin, const int *sys_end, long long nrows, double *rows)
 {
   const long long begin = inp->begin;
@@ -1280,9 +1420,9 @@ __global__ void k_thermo(const double *e_res, const long long *e_fix, int n_res,
   for (int r = sys_begin[rep] + threadIdx.x; r < sys_end[rep]; r += blockDim.x) {
     double fx = 0.0;
     for (int t = 1; t < E_FIX_TERMS; t++) fx += e_res[(size_t) t * n_res + r];
-    fx += (double) (e_fix[r] + e_fix[(size_t) n_res + r] + e_fix[(size_t) 2 * n_res + r] +
-                    e_fix[(size_t) 3 * n_res + r]) *
-          F_UNSCALE;
+    long long fq = e_fix[r] + e_fix[(size_t) n_res + r] + e_fix[(size_t) 2 * n_res + r] + e_fix[(size_t) 3 * n_res + r];
+    for (int k = 5; k < efix_slots; k++) fq += e_fix[(size_t) k * n_res + r];
+    fx += (double) fq * F_UNSCALE;
     acc[0] += fx;
     acc[1] += e_res[(size_t) E_PAIR * n_res + r] + (double) e_fix[(size_t) 4 * n_res + r] * F_UNSCALE;
     acc[2] += e_res[(size_t) E_BOND * n_res + r];
@@ -1303,14 +1443,16 @@ __global__ void k_thermo(const double *e_res, const long long *e_fix, int n_res,
 
 // Per-term sums of each replica's residues in a fixed tree order
 // (block (t, r) sums energy slot t of replica rep0 + r)
-__global__ void k_energy_reduce(const double *e_res, const long long *e_fix, int n_res, const int *sys_begin,
-                                const int *sys_end, double *out, int rep0)
+__global__ void k_energy_reduce(const double *e_res, const long long *e_fix, int efix_slots, int n_res,
+                                const int *sys_begin, const int *sys_end, double *out, int rep0)
 {
   const int t = blockIdx.x, rep = rep0 + blockIdx.y;
   __shared__ double sh[256];
   double acc = 0.0;
   // pair-summed energies are kept in fixed point (e_fix slots)
-  const int k = t == E_DSSP ? 0 : t == E_PAP ? 1 : t == E_FRAGMEM ? 2 : t == E_WATER ? 3 : t == E_PAIR ? 4 : -1;
+  int k = t == E_DSSP ? 0 : t == E_PAP ? 1 : t == E_FRAGMEM ? 2 : t == E_WATER ? 3 : t == E_PAIR ? 4
+              : t == E_SSB ? 5 : t == E_DH ? 6 : t == E_CONT_REST ? 7 : -1;
+  if (k >= efix_slots) k = -1;
   const long long *fx = k >= 0 ? e_fix + (size_t) k * n_res : nullptr;
   for (int r = sys_begin[rep] + threadIdx.x; r < sys_end[rep]; r += blockDim.x)
     acc += e_res[(size_t) t * n_res + r] + (fx ? (double) fx[r] * F_UNSCALE : 0.0);

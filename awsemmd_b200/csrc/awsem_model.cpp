@@ -84,10 +84,10 @@ void read_coeff_file(const std::string &path, ForceField &ff)
   double k_rama = 0.0, k_water = 0.0;
   static const char *outside[] = {
       "[Shake]", "[Excluded]", "[Excluded_P]", "[Excluded_R6]",
-      "[Contact_Restraints]", "[Vector_Fragment_Memory]", "[Solvent_Barrier]", "[Membrane]",
+      "[Vector_Fragment_Memory]", "[Membrane]",
       "[Fragment_Frustratometer]", "[Tertiary_Frustratometer]", "[Nmer_Frustratometer]", "[Phosphorylation]",
       "[Amylometer]", "[Selection_Temperature]", "[Monte_Carlo_Seq_Opt]", "[Optimization]",
-      "[Burial_Optimization]", "[DebyeHuckel]", "[DebyeHuckel_Optimization]", "[Shuffler]", "[Mutate_Sequence]"};
+      "[Burial_Optimization]", "[DebyeHuckel_Optimization]", "[Shuffler]", "[Mutate_Sequence]"};
   std::string s, pending;
   // a section that omits a trailing value leaves its successor's header as the
   // next token (`pending`)
@@ -173,6 +173,21 @@ void read_coeff_file(const std::string &path, ForceField &ff)
       }
       if (ff.amh_go_censor == 2)
         fail("AMH-Go: frustration censoring 2 (native distances from go_rnative*.dat) is not supported");
+    } else if (s == "[Solvent_Barrier]") {
+      // fix_backbone.cpp:334-345 (the 20 radius shifts are read whatever the correction flag)
+      p.terms |= T_SSB;
+      in >> p.k_ssb1 >> p.ssb_rmin1 >> p.ssb_rmax1 >> p.k_ssb2 >> p.ssb_rmin2 >> p.ssb_rmax2 >> p.ssb_kappa >>
+          p.ssb_ij_sep >> p.ssb_rad_cor;
+      for (int j = 0; j < 20; j++) in >> p.ssb_rshift[j];
+    } else if (s == "[DebyeHuckel]") {
+      // fix_backbone.cpp:467-477
+      p.terms |= T_DH;
+      in >> p.k_plusplus >> p.k_minusminus >> p.k_plusminus >> p.k_screening >> p.screening_length >> p.dh_min_sep;
+    } else if (s == "[Contact_Restraints]") {
+      // fix_backbone.cpp:321-327
+      p.terms |= T_CONTREST;
+      in >> p.k_cont_rest >> p.cr_sigma >> ff.cr_file;
+      p.cr_sigma_sq_inv = pow(p.cr_sigma, -2);
     } else if (s == "[Fragment_Memory]") {
       p.terms |= T_FM;
       in >> ff.k_fm_raw >> ff.fm_file >> ff.fm_gamma_file;
@@ -203,6 +218,7 @@ void read_coeff_file(const std::string &path, ForceField &ff)
   for (int j = 0; j < p.n_rama_p; j++) p.w[j + i_rp] *= k_rama;
   p.k_fm = ff.k_fm_raw;
   p.k_amh_go *= p.epsilon;
+  p.k_cont_rest *= p.epsilon;
   // density-well supports (smart_matrix_lib.h:363-368) and P_AP saturation (:110-115)
   for (int k = 0; k < p.n_wells; k++) {
     p.w_rmin_th[k] = p.well_rmin[k] - 8.0 * 2.302585 / p.water_kappa;
@@ -249,6 +265,15 @@ double pair_list_cutoff(const FFParams &p)
     r2_max = 1.1 * r2_max + p.helix_HO_zero + p.helix_sigma_HO * sqrt(6.0 * log(10.0));
     cut = std::max(cut, std::max(r1_max, r2_max));
     cut = std::max(cut, p.helix_cutoff);
+  }
+  if (p.terms & T_CONTREST) cut = std::max(cut, sqrt(p.cr_cut_sq));
+  if (p.terms & T_DH) cut = std::max(cut, 2.0 * p.screening_length / p.k_screening);
+  if (p.terms & T_SSB) {
+    double c = 0.0;
+    if (p.ssb_rad_cor)
+      for (int k = 0; k < 20; k++) c = std::max(c, 2.0 * p.ssb_rshift[k]);
+    c += std::max(p.ssb_rmax1, p.ssb_rmax2) + 10.0 / p.ssb_kappa;
+    cut = std::max(cut, c);
   }
   return cut;
 }
@@ -840,6 +865,56 @@ void build_fm_table_tb(const ForceField &ff, const Topology &top, const GammaTab
   }
 }
 
+// charge_on_residues.dat (fix_backbone.cpp:1022-1045): a count, then that
+// many (residue number, charge) records; residues not listed carry no charge
+void read_charges(const std::string &path, int n_res, std::vector<double> &q)
+{
+  std::ifstream in(path);
+  if (!in) fail("File charge_on_residues.dat doesn't exist");
+  int count = 0;
+  in >> count;
+  q.assign(n_res, 0.0);
+  for (int k = 0; k < count; k++) {
+    int r;
+    double c;
+    if (!(in >> r >> c)) fail("DebyeHuckel: charge_on_residues.dat has fewer records than its count");
+    if (r < 1 || r > n_res) fail("DebyeHuckel: residue number out of range in charge_on_residues.dat");
+    q[r - 1] = c;
+  }
+}
+
+// read_contact_restraints_file (fix_backbone.cpp:1106-1171): records
+// "i1 i2 w r0" (residue numbers from 1), w scaled by the epsilon-scaled
+// strength; the global cutoff r0_max + 4.29 sigma; per residue min(i1, i2) the
+// restraints sorted by the other residue (a pair listed twice: the first record)
+void read_contact_restraints(const std::string &path, FFParams &p, int n_res, ContactRestraints &out)
+{
+  std::ifstream in(path);
+  if (!in) fail("File for Contact Restraints potential doesn't exist");
+  struct Rec { int i, j, order; double w, r0; };
+  std::vector<Rec> recs;
+  int i1, i2;
+  double w, r0, r0_max = 0.0;
+  while (in >> i1 >> i2 >> w >> r0) {
+    const int j1 = std::min(i1, i2) - 1, j2 = std::max(i1, i2) - 1;
+    if (j1 < 0 || j1 >= n_res || j2 < 0 || j2 >= n_res) fail("Indices out of range in Contact Restraints potential file");
+    recs.push_back({j1, j2, (int) recs.size(), w * p.k_cont_rest, r0});
+    if (r0 > r0_max) r0_max = r0;
+  }
+  p.cr_dr_cut = p.cr_sigma * 4.29;
+  p.cr_cut_sq = pow(r0_max + p.cr_dr_cut, 2);
+  std::stable_sort(recs.begin(), recs.end(), [](const Rec &a, const Rec &b) { return a.i != b.i ? a.i < b.i : a.j < b.j; });
+  out = ContactRestraints();
+  out.start.assign(n_res + 1, 0);
+  for (const Rec &r : recs) {
+    out.start[r.i + 1]++;
+    out.j.push_back(r.j);
+    out.w.push_back(r.w);
+    out.r0.push_back(r.r0);
+  }
+  for (int k = 0; k < n_res; k++) out.start[k + 1] += out.start[k];
+}
+
 // FixBackbone::compute_amhgo_normalization (fix_backbone.cpp:3787-3848) and
 // the contact selection of compute_amh_go_model (:3850-3992), with the
 // native structure Fragment_Memory(0, 0, n, 1.0, "amh-go.gro") (:695-742).
@@ -953,6 +1028,9 @@ void load_shared_forcefield(const std::string &dir, const std::string &coeff_fil
 void load_system_arrays(const SharedForceField &sf, const ReplicaArrays &ra, SystemInput &S)
 {
   if (sf.ff.p.terms & T_AMHGO) fail("AMH-Go needs a run directory (amh-go.gro, amh-go.gamma): load the replica from files");
+  if (sf.ff.p.terms & T_DH) fail("DebyeHuckel needs a run directory (charge_on_residues.dat): load the replica from files");
+  if (sf.ff.p.terms & T_CONTREST)
+    fail("Contact_Restraints needs a run directory (the restraints file): load the replica from files");
   if (ra.n_res <= 0 || ra.n_chains <= 0 || !ra.chain_len || !ra.seq || !ra.x) fail("replica: empty description");
   S.ff = sf.ff;
   Topology &t = S.top;
@@ -1175,6 +1253,20 @@ void assemble_batch(const std::vector<const SystemInput *> &reps, Batch &B)
       res_off += r->top.n_res;
     }
   }
+  if (B.ff.p.terms & T_DH)
+    for (auto *r : reps) B.charge.insert(B.charge.end(), r->charge.begin(), r->charge.end());
+  if (B.ff.p.terms & T_CONTREST) {
+    B.cr.start.push_back(0);
+    int res_off = 0;
+    for (auto *r : reps) {
+      const int base = (int) B.cr.j.size();
+      for (size_t k = 1; k < r->cr.start.size(); k++) B.cr.start.push_back(base + r->cr.start[k]);
+      for (int q : r->cr.j) B.cr.j.push_back(q + res_off);
+      B.cr.w.insert(B.cr.w.end(), r->cr.w.begin(), r->cr.w.end());
+      B.cr.r0.insert(B.cr.r0.end(), r->cr.r0.begin(), r->cr.r0.end());
+      res_off += r->top.n_res;
+    }
+  }
   if (B.ff.p.terms & T_FM_TABLE) {
     B.tb.nbrs = r0.tb.nbrs;
     B.tb.size = r0.tb.size;
@@ -1315,6 +1407,11 @@ void load_system_atoms(const std::string &dir, const std::string &coeff_file, co
       build_fm_table_tb(S.ff, S.top, S.gamma, S.mems, dir, S.tb);
       S.ff.p.tb_nbrs = S.tb.nbrs;
     }
+  }
+  if (S.ff.p.terms & T_DH) read_charges(path_in(dir, "charge_on_residues.dat"), S.top.n_res, S.charge);
+  if (S.ff.p.terms & T_CONTREST) {
+    read_contact_restraints(path_in(dir, S.ff.cr_file), S.ff.p, S.top.n_res, S.cr);
+    S.ff.p.pair_list_cutoff = pair_list_cutoff(S.ff.p);  // the restraints set their cutoff
   }
   if (S.ff.p.terms & T_AMHGO) build_amh_go(S.ff, S.top, dir, S.go);
   S.x.assign(3 * S.top.n_atoms, 0.0);

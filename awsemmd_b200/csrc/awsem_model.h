@@ -22,7 +22,8 @@ enum Energy {
 enum TermFlag : uint32_t {
   T_CHAIN = 1u << 0, T_CHI = 1u << 1, T_RAMA = 1u << 2, T_RAMA_P = 1u << 3, T_SSW = 1u << 4,
   T_DSSP = 1u << 5, T_PAP = 1u << 6, T_WATER = 1u << 7, T_BURIAL = 1u << 8, T_HELIX = 1u << 9,
-  T_FM = 1u << 10, T_FM_TABLE = 1u << 11, T_AMHGO = 1u << 12
+  T_FM = 1u << 10, T_FM_TABLE = 1u << 11, T_AMHGO = 1u << 12, T_SSB = 1u << 13, T_DH = 1u << 14,
+  T_CONTREST = 1u << 15
 };
 
 // Residue flags
@@ -64,6 +65,13 @@ struct FFParams {
   // pairs count only within the reference's fix pair-list cutoff plus the neighbour skin
   double k_amh_go, amh_go_p, amh_go_rc, pair_list_cutoff;
   double helix_sigma_HO, helix_sigma_NO;  // as read (the pair-list cutoff uses them)
+  // [Solvent_Barrier] (fix_backbone.cpp:334-345): two wells, kappa, separation, radius correction
+  double k_ssb1, k_ssb2, ssb_rmin1, ssb_rmax1, ssb_rmin2, ssb_rmax2, ssb_kappa, ssb_rshift[20];
+  int ssb_ij_sep, ssb_rad_cor, dh_min_sep;
+  // [DebyeHuckel] (:467-477): strengths by charge signs, screening, minimum separation
+  double k_plusplus, k_minusminus, k_plusminus, k_screening, screening_length;
+  // [Contact_Restraints] (:321-327, :1106-1150): epsilon-scaled strength, width and its cutoffs
+  double k_cont_rest, cr_sigma, cr_sigma_sq_inv, cr_dr_cut, cr_cut_sq;
 };
 
 struct ForceField {
@@ -76,6 +84,7 @@ struct ForceField {
   double tb_width = 0.0;  // [Fragment_Memory_Table] well width (scales the Gaussian variance)
   int tb_use_file = 0;    // read the tables from fm_table.energy/.force when present, else write them
   int amh_go_censor = 0;  // [AMH-Go] frustration censoring flag (0 or 1)
+  std::string cr_file;    // [Contact_Restraints] restraints file
   double k_water = 0.0;  // epsilon-scaled [Water] strength, applied to gamma.dat
 };
 
@@ -158,6 +167,13 @@ struct AmhGoContacts {
   std::vector<double> norm;                  // [n_res]: normalisation of the residue's system
 };
 
+// Contact restraints in residue-pair order: restraints of residue i (with a
+// partner j > i) at [start[i], start[i+1]), sorted by j (fix_backbone.cpp:1106-1171)
+struct ContactRestraints {
+  std::vector<int> start, j;
+  std::vector<double> w, r0;
+};
+
 struct SystemInput {
   ForceField ff;
   Topology top;
@@ -166,6 +182,8 @@ struct SystemInput {
   FMTable fm;
   FMTableTB tb;
   AmhGoContacts go;
+  std::vector<double> charge;  // [n_res] Debye-Hueckel charges (charge_on_residues.dat)
+  ContactRestraints cr;
   std::vector<double> x, v;  // internal order [n_atoms*3]
 };
 
@@ -220,6 +238,8 @@ struct Batch {
   FMTable fm;         // concatenated fragment-memory rows
   FMTableTB tb;       // concatenated fragment-memory tables (per residue)
   AmhGoContacts go;   // concatenated AMH-Go contacts (partners offset to batch atoms)
+  std::vector<double> charge;  // concatenated Debye-Hueckel charges
+  ContactRestraints cr;        // concatenated contact restraints (residues offset)
   std::vector<double> x, v;
   std::vector<int> res_sys;              // residue -> replica
   std::vector<int> sys_res_begin, sys_res_end;    // [n_sys]

@@ -130,6 +130,8 @@ struct PersistArgs {
   int fm_units;      // fragment-memory work units of the step (0: term off)
   int fm_table;      // table fragment memory on
   int amh_go;        // AMH-Go on
+  int pair_extra;    // solvent barrier, Debye-Hueckel or contact restraints on
+  int list_reps;     // replicas whose LAMMPS lists are emulated (0: none)
 };
 
 // Fragment-memory units taken from the step's counter until none is left
@@ -192,6 +194,10 @@ template <typename R> __global__ void __launch_bounds__(kStepThreads, 2) k_step(
     if (ok) fragmem_take_units(a, p, q, ring, wsm, kbase);
   } else {
     const Span sp{(int) (blockIdx.x * pass_threads + threadIdx.x), (int) (gridDim.x * pass_threads)};
+    // the emulated lists' decision (read after the next barrier)
+    if (ok)
+      for (int r = sp.t; r < q.list_reps; r += sp.nthr)
+        list_decide_one(*a.nl, a.lst_ago, a.lst_over, const_cast<int *>(a.lst_build), r);
     if (a.nl->rebuild) {
       if (ok) nl_build_pass(a, GridArgs{}, q.n_launch, sp);
       ok = grid_sync(b, 1, seen[1], 1, pass_threads, ok, NoSerial{});
@@ -208,6 +214,7 @@ template <typename R> __global__ void __launch_bounds__(kStepThreads, 2) k_step(
       hbond_pass(a, p, sp);
       if (q.fm_table) fm_table_pass(a, p, sp);
       if (q.amh_go) amh_go_pass(a, p, sp);
+      if (q.pair_extra) pair_extra_pass(a, p, sp);
       fragmem_take_units(a, p, q, ring, wsm, kbase);
     }
   }

@@ -329,6 +329,60 @@ def write_native_gro(sys_: System, path: str, scale: float = 1.0) -> None:
         f.write(f"native structure (synthetic, scale {scale})\n{len(lines)}\n" + "\n".join(lines) + "\n   0.0 0.0 0.0\n")
 
 
+# [Solvent_Barrier] settings of the synthetic pair-term cases: well 1 (barrier)
+# and well 2 strengths and ranges (A), kappa, minimum same-chain separation,
+# radius correction on, and per residue type radius shifts (A)
+SSB_PARAMS = (0.35, 6.0, 7.0, -0.2, 7.5, 9.0, 5.0, 10, 1,
+              (0.00, 0.20, 0.06, 0.06, 0.04, 0.11, 0.12, -0.15, 0.09, 0.07,
+               0.08, 0.15, 0.10, 0.10, -0.01, 0.03, 0.04, 0.12, 0.12, 0.04))
+# [DebyeHuckel]: strengths ++, --, +- (strong, so that which pairs the fix's list holds
+# shows in a short trajectory); screening constant; screening length (A); minimum separation
+DH_PARAMS = (40.0, 40.0, 40.0, 1.0, 5.0, 10)
+
+
+def pair_terms_text(k_cont_rest=1.0, cr_sigma=1.0, cr_file="contact_restraints.dat") -> str:
+    """[Solvent_Barrier], [DebyeHuckel] and [Contact_Restraints] sections."""
+    k1, a1, b1, k2, a2, b2, kap, sep, cor, shifts = SSB_PARAMS
+    kpp, kmm, kpm, ks, L, msep = DH_PARAMS
+    return (f"\n[Solvent_Barrier]\n{k1}\n{a1} {b1}\n{k2}\n{a2} {b2}\n{kap}\n{sep}\n{cor}\n"
+            + " ".join(str(v) for v in shifts) + "\n"
+            + f"\n[DebyeHuckel]\n{kpp} {kmm} {kpm}\n{ks}\n{L}\n{msep}\n"
+            + f"\n[Contact_Restraints]\n{k_cont_rest}\n{cr_sigma}\n{cr_file}\n")
+
+
+def write_charges(sys_: System, path: str) -> None:
+    """charge_on_residues.dat: +1 on K and R, -1 on D and E (residues numbered over all chains)."""
+    seq = "".join(ch.seq for ch in sys_.chains)
+    rec = [(k + 1, 1.0 if a in "KR" else -1.0) for k, a in enumerate(seq) if a in "KRDE"]
+    with open(path, "w") as f:
+        f.write(f"{len(rec)}\n" + "".join(f"{r} {q}\n" for r, q in rec))
+
+
+def write_contact_restraints(sys_: System, path: str, n: int = 24, seed: int = 5) -> None:
+    """Restraints "i j w r0" on residue pairs whose contact beads are within
+    12 A (separation > 2), r0 the current distance shifted by up to 2 A; plus
+    a pair listed twice (the first record counts) and an adjacent pair (never
+    evaluated: the fix skips |i - j| <= 1 on one chain)."""
+    rng = np.random.default_rng(seed)
+    beads = np.concatenate([np.where(np.array([a == "G" for a in ch.seq])[:, None], ch.ca, ch.cb)
+                            for ch in sys_.chains])
+    nres = len(beads)
+    d = np.linalg.norm(beads[:, None, :] - beads[None, :, :], axis=-1)
+    cand = [(i, j) for i in range(nres) for j in range(i + 3, nres) if d[i, j] < 12.0]
+    pick = rng.choice(len(cand), size=min(n, len(cand)), replace=False)
+    lines = []
+    for k in pick:
+        i, j = cand[k]
+        w = round(float(rng.uniform(1.0, 2.0)), 3)
+        r0 = round(float(max(3.5, d[i, j] + rng.uniform(-2.0, 2.0))), 3)
+        lines.append(f"{j + 1} {i + 1} {w} {r0}" if rng.random() < 0.3 else f"{i + 1} {j + 1} {w} {r0}")
+    i, j = cand[pick[0]]
+    lines.append(f"{i + 1} {j + 1} 5.0 {round(float(d[i, j]), 3)}")  # duplicate: ignored
+    lines.append(f"4 5 3.0 {round(float(d[3, 4]), 3)}")  # adjacent: ignored
+    with open(path, "w") as f:
+        f.write("\n".join(lines) + "\n")
+
+
 def bond_list(sys_: System):
     """(type, atom_i, atom_j) with 0-based atom indices in data-file order."""
     bonds = []

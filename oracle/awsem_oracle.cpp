@@ -126,6 +126,14 @@ struct Params {
   bool amhgo = 0;
   double k_amh_go = 0, amh_go_p = 0, amh_go_rc = 0;
   int censoring = 0;
+  // [Solvent_Barrier] (:334-345), [DebyeHuckel] (:467-477), [Contact_Restraints] (:321-327)
+  bool ssb = 0, huckel = 0, cont_rest = 0;
+  double k_solventb1 = 0, k_solventb2 = 0, ssb_rmin1 = 0, ssb_rmax1 = 0, ssb_rmin2 = 0, ssb_rmax2 = 0, ssb_kappa = 0;
+  double ssb_rshift[20] = {0};
+  int ssb_ij_sep = 0, ssb_rad_cor = 0, debye_huckel_min_sep = 0;
+  double k_PlusPlus = 0, k_MinusMinus = 0, k_PlusMinus = 0, k_screening = 0, screening_length = 0;
+  double k_cont_rest = 0, cr_sigma = 0, cr_sigma_sq_inv = 0, cr_dr_cutoff = 0, cr_glob_cutoff_sq = 0;
+  std::string cr_file;
   // [Fragment_Memory_Table] (fix_backbone.cpp:310-321)
   double tb_rmin = 0, tb_rmax = 0, tb_dr = 0, tb_width = 0;
   int tb_size = 0, tb_use_file = 0;
@@ -317,6 +325,17 @@ struct System {
   bool list_setup = true;  // the next compute is a run setup: the list is built
   long long list_ago = 0;
   std::vector<double> xhold;  // positions at the last build
+  bool lists_used() const { return P.amhgo || P.ssb || P.huckel || P.cont_rest; }
+  void list_update(const double *x);
+  bool in_list(int a, int b) const;
+  // Debye-Hueckel charges and contact restraints (per residue min(i1, i2), sorted by the other)
+  std::vector<double> charge;
+  struct Restraint { int i2; double w, r0; };
+  std::vector<std::vector<Restraint>> cr_map;
+  void read_pair_extras();
+  void pair_extras(const double *x, double *f);
+  void solvent_barrier(int i, int j, const double *x, double *f);
+  void debye_huckel(int i, int j, const double *x, double *f);
   void read_amh_go();
   void amhgo_normalization();
   void amhgo_term(const double *x, double *f);
@@ -384,12 +403,11 @@ void System::read_coeff(const std::string &path)
   Params &p = P;
   std::string s;
   static const char *unsupported[] = {"[Shake]", "[Excluded]", "[Excluded_P]", "[Excluded_R6]",
-                                      "[Contact_Restraints]",
-                                      "[Vector_Fragment_Memory]", "[Solvent_Barrier]", "[Membrane]",
+                                      "[Vector_Fragment_Memory]", "[Membrane]",
                                       "[Fragment_Frustratometer]", "[Tertiary_Frustratometer]",
                                       "[Nmer_Frustratometer]", "[Phosphorylation]", "[Amylometer]",
                                       "[Selection_Temperature]", "[Monte_Carlo_Seq_Opt]", "[Optimization]",
-                                      "[Burial_Optimization]", "[DebyeHuckel]", "[DebyeHuckel_Optimization]",
+                                      "[Burial_Optimization]", "[DebyeHuckel_Optimization]",
                                       "[Shuffler]", "[Mutate_Sequence]"};
   while (in >> s) {
     if (s == "[ABC]") {
@@ -477,6 +495,19 @@ void System::read_coeff(const std::string &path)
       // it leaves its stream failed, so the oracle asks for it
       if (!(in >> p.censoring)) throw std::runtime_error("[AMH-Go]: the frustration censoring flag is missing");
       if (p.censoring == 2) throw std::runtime_error("oracle: [AMH-Go] censoring 2 is not part of the restated path");
+    } else if (s == "[Solvent_Barrier]") {
+      p.ssb = 1;
+      in >> p.k_solventb1 >> p.ssb_rmin1 >> p.ssb_rmax1 >> p.k_solventb2 >> p.ssb_rmin2 >> p.ssb_rmax2 >> p.ssb_kappa >>
+          p.ssb_ij_sep >> p.ssb_rad_cor;
+      for (int j = 0; j < 20; ++j) in >> p.ssb_rshift[j];
+    } else if (s == "[DebyeHuckel]") {
+      p.huckel = 1;
+      in >> p.k_PlusPlus >> p.k_MinusMinus >> p.k_PlusMinus >> p.k_screening >> p.screening_length >>
+          p.debye_huckel_min_sep;
+    } else if (s == "[Contact_Restraints]") {
+      p.cont_rest = 1;
+      in >> p.k_cont_rest >> p.cr_sigma >> p.cr_file;
+      p.cr_sigma_sq_inv = pow(p.cr_sigma, -2);
     } else if (s == "[Epsilon]") {
       in >> p.epsilon;
     } else {
@@ -494,6 +525,7 @@ void System::read_coeff(const std::string &path)
   p.k_dssp *= p.epsilon;
   p.k_global_pap *= p.epsilon;
   p.k_amh_go *= p.epsilon;
+  p.k_cont_rest *= p.epsilon;
   for (int j = 0; j < p.n_rama; j++) p.w[j] *= p.k_rama;
   for (int j = 0; j < p.n_rama_p; j++) p.w[j + Params::i_rp] *= p.k_rama;
   // well supports: rmin - 8 ln10/kappa, rmax + 8 ln10/kappa (smart_matrix_lib.h:363-368)
@@ -1726,6 +1758,15 @@ double pair_list_cut(const Params &p)
     cut = std::max(cut, std::max(r1, r2));
     cut = std::max(cut, p.helix_cutoff);
   }
+  if (p.cont_rest) cut = std::max(cut, sqrt(p.cr_glob_cutoff_sq));
+  if (p.huckel) cut = std::max(cut, 2.0 * p.screening_length / p.k_screening);
+  if (p.ssb) {
+    double c = 0.0;
+    if (p.ssb_rad_cor)
+      for (int i = 0; i < 20; ++i) c = std::max(c, 2.0 * p.ssb_rshift[i]);
+    c += std::max(p.ssb_rmax1, p.ssb_rmax2) + 10.0 / p.ssb_kappa;
+    cut = std::max(cut, c);
+  }
   return cut;
 }
 
@@ -1748,7 +1789,6 @@ void System::read_amh_go()
     while (cf >> a >> b)
       if (a >= 1 && a <= n && b >= 1 && b <= n) go_censored[(size_t) (a - 1) * n + (b - 1)] = 1;
   }
-  plc = pair_list_cut(P);
   amhgo_normalization();
 }
 
@@ -1786,43 +1826,11 @@ void System::amhgo_normalization()
 }
 
 /* compute_amh_go_model, fix_backbone.cpp:3856-3992, over the fix's full
-   neighbour list: for each atom i, every atom j != i that was within
-   plc + skin of i when LAMMPS last built the list, 1-2 bonded pairs removed
-   (special_bonds fene), in atom order.  The list is built at a run setup and
-   then by Neighbor::decide(): after `delay` steps, on multiples of `every`,
-   with `check` only once an atom has moved more than half the skin. */
+   neighbour list: for each atom i, every atom j != i in the list (in_list),
+   in atom order. */
 void System::amhgo_term(const double *x, double *f)
 {
   const Params &p = P;
-  bool build = list_setup;
-  list_setup = false;
-  if (!build) {
-    list_ago++;
-    if (list_ago >= nb_delay && list_ago % nb_every == 0) {
-      if (!nb_check) {
-        build = true;
-      } else {
-        const double trigger = 0.25 * nb_skin * nb_skin;
-        for (int a = 0; a < natoms && !build; a++) {
-          double dx = x[3 * a] - xhold[3 * a], dy = x[3 * a + 1] - xhold[3 * a + 1], dz = x[3 * a + 2] - xhold[3 * a + 2];
-          if (dx * dx + dy * dy + dz * dz > trigger) build = true;
-        }
-      }
-    }
-  }
-  if (build) {
-    xhold.assign(x, x + 3 * natoms);
-    list_ago = 0;
-  }
-  const double cut = plc + nb_skin, cutsq = cut * cut;
-  auto in_list = [&](int i, int j) {
-    double dx = xhold[3 * i] - xhold[3 * j], dy = xhold[3 * i + 1] - xhold[3 * j + 1],
-           dz = xhold[3 * i + 2] - xhold[3 * j + 2];
-    if (!(dx * dx + dy * dy + dz * dz < cutsq)) return false;
-    for (int s : special[i])
-      if (s == j) return false;
-    return true;
-  };
   const int min_sep = go_gamma.min_sep();
   double Etot = 0.0;
   std::vector<int> fmap;
@@ -1867,12 +1875,184 @@ void System::amhgo_term(const double *x, double *f)
   E[ET_AMHGO] += Etot;
 }
 
+/* The fix's neighbour lists (cut plc + skin; fix_backbone.cpp:1805-1813)
+   as LAMMPS keeps them: built at a run setup, then by Neighbor::decide() --
+   after `delay` steps, on multiples of `every`, and with `check` only once an
+   atom has moved more than half the skin since the last build. */
+void System::list_update(const double *x)
+{
+  bool build = list_setup;
+  list_setup = false;
+  if (!build) {
+    list_ago++;
+    if (list_ago >= nb_delay && list_ago % nb_every == 0) {
+      if (!nb_check) {
+        build = true;
+      } else {
+        const double trigger = 0.25 * nb_skin * nb_skin;
+        for (int a = 0; a < natoms && !build; a++) {
+          double dx = x[3 * a] - xhold[3 * a], dy = x[3 * a + 1] - xhold[3 * a + 1], dz = x[3 * a + 2] - xhold[3 * a + 2];
+          if (dx * dx + dy * dy + dz * dz > trigger) build = true;
+        }
+      }
+    }
+  }
+  if (build) {
+    xhold.assign(x, x + 3 * natoms);
+    list_ago = 0;
+  }
+}
+
+/* atoms a and b are neighbours in those lists: within plc + skin at the last
+   build, not 1-2 bonded (special_bonds fene) */
+bool System::in_list(int a, int b) const
+{
+  const double cut = plc + nb_skin, cutsq = cut * cut;
+  double dx = xhold[3 * a] - xhold[3 * b], dy = xhold[3 * a + 1] - xhold[3 * b + 1], dz = xhold[3 * a + 2] - xhold[3 * b + 2];
+  if (!(dx * dx + dy * dy + dz * dz < cutsq)) return false;
+  for (int s : special[a])
+    if (s == b) return false;
+  return true;
+}
+
+/* charge_on_residues.dat (fix_backbone.cpp:1022-1045) and the contact
+   restraints file (read_contact_restraints_file, :1106-1171) */
+void System::read_pair_extras()
+{
+  Params &p = P;
+  if (p.huckel) {
+    charge.assign(n, 0.0);
+    std::ifstream in(join(workdir, "charge_on_residues.dat"));
+    if (!in) throw std::runtime_error("File charge_on_residues.dat doesn't exist");
+    int total = 0;
+    in >> total;
+    for (int k = 0; k < total; k++) {
+      int r;
+      double q;
+      in >> r >> q;
+      if (r < 1 || r > n) throw std::runtime_error("oracle: charge_on_residues.dat residue out of range");
+      charge[r - 1] = q;
+    }
+  }
+  if (p.cont_rest) {
+    std::ifstream in(join(workdir, p.cr_file));
+    if (!in) throw std::runtime_error("File for Contact Restraints potential doesn't exist");
+    cr_map.assign(n, {});
+    int i1, i2;
+    double ww, r0, r0_max = 0.0;
+    while (in >> i1 >> i2 >> ww >> r0) {
+      if (in.eof()) throw std::runtime_error("Contact Restraints potential parameter file format error");
+      int j1 = std::min(i1, i2) - 1, j2 = std::max(i1, i2) - 1;
+      if (j1 < 0 || j1 >= n || j2 < 0 || j2 >= n)
+        throw std::runtime_error("Indices out of range in Contact Restraints potential file");
+      cr_map[j1].push_back({j2, ww * p.k_cont_rest, r0});
+      if (r0 > r0_max) r0_max = r0;
+    }
+    p.cr_dr_cutoff = p.cr_sigma * 4.29;
+    p.cr_glob_cutoff_sq = pow(r0_max + p.cr_dr_cutoff, 2);
+    for (auto &m : cr_map)
+      std::stable_sort(m.begin(), m.end(), [](const Restraint &a, const Restraint &b) { return a.i2 < b.i2; });
+  }
+}
+
+/* compute_solvent_barrier, fix_backbone.cpp:6237-6305 (residues i < j) */
+void System::solvent_barrier(int i, int j, const double *x, double *f)
+{
+  const Params &p = P;
+  if (chain_of[i] == chain_of[j] && j - i < p.ssb_ij_sep) return;
+  const int iatom = contact_atom(i), jatom = contact_atom(j);
+  double dx[3] = {x[3 * iatom] - x[3 * jatom], x[3 * iatom + 1] - x[3 * jatom + 1], x[3 * iatom + 2] - x[3 * jatom + 2]};
+  double r = sqrt(dx[0] * dx[0] + dx[1] * dx[1] + dx[2] * dx[2]);
+  double rmin1 = p.ssb_rmin1, rmax1 = p.ssb_rmax1, rmin2 = p.ssb_rmin2, rmax2 = p.ssb_rmax2;
+  if (p.ssb_rad_cor) {
+    double rshift = p.ssb_rshift[type_of(i)] + p.ssb_rshift[type_of(j)];
+    rmin1 += rshift;
+    rmax1 += rshift;
+    rmin2 += rshift;
+    rmax2 += rshift;
+  }
+  if (r > rmax1 + 10 / p.ssb_kappa && r > rmax2 + 10 / p.ssb_kappa) return;
+  double t_min1 = tanh(p.ssb_kappa * (r - rmin1)), t_max1 = tanh(p.ssb_kappa * (rmax1 - r));
+  double t_min2 = tanh(p.ssb_kappa * (r - rmin2)), t_max2 = tanh(p.ssb_kappa * (rmax2 - r));
+  double theta1 = 0.5 * (t_min1 + t_max1), theta2 = 0.5 * (t_min2 + t_max2);
+  E[ET_SSB] += p.epsilon * p.k_solventb1 * theta1;
+  E[ET_SSB] += p.epsilon * p.k_solventb2 * theta2;
+  double force1 = -p.epsilon * p.k_solventb1 * p.ssb_kappa * theta1 * (t_max1 - t_min1) / r;
+  double force2 = -p.epsilon * p.k_solventb2 * p.ssb_kappa * theta2 * (t_max2 - t_min2) / r;
+  for (int k = 0; k < 3; k++) {
+    f[3 * iatom + k] += force1 * dx[k];
+    f[3 * iatom + k] += force2 * dx[k];
+    f[3 * jatom + k] += -force1 * dx[k];
+    f[3 * jatom + k] += -force2 * dx[k];
+  }
+}
+
+/* compute_DebyeHuckel_Interaction, fix_backbone.cpp:6307-6363 (residues i < j) */
+void System::debye_huckel(int i, int j, const double *x, double *f)
+{
+  const Params &p = P;
+  if (abs(i - j) < p.debye_huckel_min_sep) return;
+  double qi = charge[i], qj = charge[j];
+  if (qi == 0 && qj == 0) return;
+  const int iatom = contact_atom(i), jatom = contact_atom(j);
+  double dx[3] = {x[3 * iatom] - x[3 * jatom], x[3 * iatom + 1] - x[3 * jatom + 1], x[3 * iatom + 2] - x[3 * jatom + 2]};
+  double r = sqrt(dx[0] * dx[0] + dx[1] * dx[1] + dx[2] * dx[2]);
+  double qq = 0.0;
+  if (qi > 0.0 && qj > 0.0) qq = p.k_PlusPlus * qi * qj / r;
+  else if (qi < 0.0 && qj < 0.0) qq = p.k_MinusMinus * qi * qj / r;
+  else if ((qi < 0.0 && qj > 0.0) || (qi > 0.0 && qj < 0.0)) qq = p.k_PlusMinus * qi * qj / r;
+  double e = p.epsilon * qq * exp(-p.k_screening * r / p.screening_length);
+  E[ET_DH] += e;
+  double force = (e / r) * (1.0 / r + p.k_screening / p.screening_length);
+  for (int k = 0; k < 3; k++) {
+    f[3 * iatom + k] += force * dx[k];
+    f[3 * jatom + k] += -force * dx[k];
+  }
+}
+
+/* The DL3 loop's contact restraints (fix_backbone.cpp:8058-8060, :8137-8177)
+   on contact-bead pairs, solvent barrier and Debye-Hueckel (:8105-8114) on
+   CA pairs, each pair as the fix's half list holds it. */
+void System::pair_extras(const double *x, double *f)
+{
+  const Params &p = P;
+  for (int i = 0; i < n; i++)
+    for (int j = i + 1; j < n; j++) {
+      const int ci = contact_atom(i), cj = contact_atom(j);
+      if (p.cont_rest && (amol[ci] != amol[cj] || j - i > 1) && !cr_map[i].empty()) {
+        double dx[3] = {x[3 * ci] - x[3 * cj], x[3 * ci + 1] - x[3 * cj + 1], x[3 * ci + 2] - x[3 * cj + 2]};
+        double rsq = dx[0] * dx[0] + dx[1] * dx[1] + dx[2] * dx[2];
+        if (rsq < p.cr_glob_cutoff_sq && in_list(ci, cj)) {
+          for (const Restraint &c : cr_map[i]) {
+            if (c.i2 != j) continue;
+            double r = sqrt(rsq), dr = r - c.r0;
+            if (fabs(dr) < p.cr_dr_cutoff) {
+              double V = -c.w * exp(-0.5 * (dr * dr) * p.cr_sigma_sq_inv);
+              double force = V * dr * p.cr_sigma_sq_inv / r;
+              E[ET_CONT_REST] += V;
+              for (int k = 0; k < 3; k++) {
+                f[3 * ci + k] += force * dx[k];
+                f[3 * cj + k] -= force * dx[k];
+              }
+            }
+            break;
+          }
+        }
+      }
+      if ((p.ssb || p.huckel) && in_list(ca[i], ca[j])) {
+        if (p.ssb && (amol[ca[i]] != amol[ca[j]] || j - i >= p.ssb_ij_sep)) solvent_barrier(i, j, x, f);
+        if (p.huckel && j - i > 1) debye_huckel(i, j, x, f);
+      }
+    }
+}
+
 /* compute_backbone, fix_backbone.cpp:7047-7673, then vexcluded and bonds */
 void System::compute(const double *x, double *f)
 {
   const Params &p = P;
   for (double &e : E) e = 0.0;
   for (int k = 0; k < 3 * natoms; k++) f[k] = 0.0;
+  if (lists_used()) list_update(x);
   backbone_atoms(x);
   for (int i = 0; i < n; i++) {
     if (p.chain) chain_term(i, f);
@@ -1882,6 +2062,7 @@ void System::compute(const double *x, double *f)
     if (p.fm_tb) tb_term(i, f);
   }
   pair_terms(x, f);
+  if (p.ssb || p.huckel || p.cont_rest) pair_extras(x, f);
   if (p.amhgo) amhgo_term(x, f);
   for (int k = 1; k < NET; k++) E[ET_TOTAL] += E[k];
   excluded_volume(x, f);
@@ -1909,6 +2090,8 @@ void *oracle_create(const char *workdir, const char *data_file, const char *coef
     S->read_tables();
     if (S->P.fm || S->P.fm_tb) S->read_mems();
     if (S->P.fm_tb) S->build_tb();
+    if (S->P.ssb || S->P.huckel || S->P.cont_rest) S->read_pair_extras();
+    if (S->lists_used()) S->plc = pair_list_cut(S->P);
     if (S->P.amhgo) S->read_amh_go();
     S->pair_setup(pair_style, pair_coeffs ? pair_coeffs : "");
   } catch (std::exception &e) {

@@ -22,6 +22,12 @@ against the LAMMPS-API shim (``make -C oracle ref``) and run on four inputs:
                from examples/examples_new/1R69_AMH-Go;
 * ``r1r69go2`` -- the same with k 1.5, p 2, rc 9 A and censoring 1 (four
                native residue pairs listed in frustration_censored_contacts.dat);
+* ``c0x``     -- ``c0`` with [Solvent_Barrier], [DebyeHuckel] (charges +1 on
+               K/R, -1 on D/E) and [Contact_Restraints] (synth.pair_terms_text,
+               write_charges, write_contact_restraints), run with neighbor 0.6
+               and neigh_modify delay 3 every 2: the barrier and Debye-Hueckel
+               sum over the CA pairs of the fix's half list as last built;
+* ``sheetx``  -- ``sheet`` (three chains) with the same three sections;
 * ``c0go``    -- ``c0`` with [AMH-Go] (k 200, p 2, rc 10 A) towards a native
                structure 0.6 times as large as the starting chain
                (synth.write_native_gro), run with neighbor skin 0.6 A and
@@ -73,6 +79,14 @@ def dir_hash(d: str) -> str:
 def write_case(name: str, outdir: str) -> dict:
     if name == "c0":
         return synth.write_system(synth.config_system(0), outdir)
+    if name in ("c0x", "sheetx"):
+        sys_ = synth.config_system(0) if name == "c0x" else synth.sheet_system()
+        files = synth.write_system(sys_, outdir)
+        with open(os.path.join(outdir, files["coeff"]), "w") as fh:
+            fh.write(synth.coeff_text() + synth.pair_terms_text())
+        synth.write_charges(sys_, os.path.join(outdir, "charge_on_residues.dat"))
+        synth.write_contact_restraints(sys_, os.path.join(outdir, "contact_restraints.dat"))
+        return files
     if name == "c0go":
         sys_ = synth.config_system(0)
         files = synth.write_system(sys_, outdir)
@@ -112,10 +126,10 @@ def write_case(name: str, outdir: str) -> dict:
     raise KeyError(name)
 
 
-CASES = ["c0", "sheet", "r1r69", "r1r69tb", "r1r69go", "r1r69go2", "c0go"]
+CASES = ["c0", "sheet", "r1r69", "r1r69tb", "r1r69go", "r1r69go2", "c0go", "c0x", "sheetx"]
 # LAMMPS neighbor skin and neigh_modify delay / every / check of a case's runs
 # (the others: 2.0, 0, 1, yes -- LAMMPS's defaults)
-NEIGH = {"c0go": (0.6, 3, 2, 1)}
+NEIGH = {"c0go": (0.6, 3, 2, 1), "c0x": (0.6, 3, 2, 1)}
 
 
 def main(cases=None):

@@ -30,11 +30,12 @@ def test_fix_backbone_gpu_replaces_the_reference_fix(name, tmp_path, gpu_lib, or
     assert np.abs(gpu.get("x") - cpu.get("x")).max() < 1e-6
 
 
-@pytest.mark.parametrize("name", ["r1r69go", "c0go"])
+@pytest.mark.parametrize("name", ["r1r69go", "c0go", "c0x"])
 def test_fix_backbone_gpu_follows_the_hosts_list_builds(name, tmp_path, gpu_lib, oracle_built):
-    """[AMH-Go] reads LAMMPS's neighbour list: the adapter tells the engine on
-    which steps the host rebuilt it (neighbor->ago == 0), so with c0go's
-    neighbor 0.6 / delay 3 / every 2 the run matches the reference fix's."""
+    """[AMH-Go], the solvent barrier and Debye-Hueckel read LAMMPS's
+    neighbour lists: the adapter tells the engine on which steps the host
+    rebuilt them (neighbor->ago == 0), so with neighbor 0.6 / delay 3 /
+    every 2 the run matches the reference fix's."""
     import ref
 
     assert ref.gpufix_available()

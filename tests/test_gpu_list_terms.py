@@ -1,9 +1,11 @@
-"""[AMH-Go] on the GPU beyond the single-system golden runs: the neighbour
-list it reads is kept per replica, so a replica in a batch, a run cut into
-continuation calls, and the persistent step form all follow the reference's
-list rebuilds exactly.  c0go: the 100-residue chain with a compact native
-structure, run with neighbor 0.6 and neigh_modify delay 3 every 2 check yes
-(its list is rebuilt during the run and native contacts cross its reach)."""
+"""Terms that read the fix's neighbour lists themselves ([AMH-Go]; the
+solvent barrier and Debye-Hueckel on the CA pairs of the half list) on the
+GPU beyond the single-system golden runs: the lists are kept per replica, so a
+replica in a batch, a run cut into continuation calls, and the persistent step
+form all follow the reference's list rebuilds exactly.  c0go: the 100-residue
+chain with a compact native structure; c0x: the same chain with the three
+pair terms; both run with neighbor 0.6 and neigh_modify delay 3 every 2 check
+yes (the lists are rebuilt during the run and pairs cross their reach)."""
 import numpy as np
 import pytest
 
@@ -18,13 +20,14 @@ def _kw(g, seed=None):
                              seed=int(gseed if seed is None else seed), skin=neigh_of(g)[0])
 
 
-def test_batch_replicas_keep_their_own_lists(tmp_path, gpu_lib):
-    """Two c0go replicas with different seeds rebuild at different steps: the
+@pytest.mark.parametrize("case", ["c0go", "c0x"])
+def test_batch_replicas_keep_their_own_lists(case, tmp_path, gpu_lib):
+    """Two replicas with different seeds rebuild at different steps: the
     one with the reference's seed reproduces the reference's trajectory, the
     other equals its single-system run bit for bit."""
     from awsemmd_b200.engine import AwsemBatch, AwsemSystem
 
-    files, g = write_case("c0go", tmp_path)
+    files, g = write_case(case, tmp_path)
     nsteps, kw = _kw(g)
     skin, delay, every, check = neigh_of(g)
     with AwsemSystem(files, precision="fp64") as s:
@@ -44,13 +47,14 @@ def test_batch_replicas_keep_their_own_lists(tmp_path, gpu_lib):
     assert not np.array_equal(x0, x1)
 
 
+@pytest.mark.parametrize("case", ["c0go", "c0x"])
 @pytest.mark.parametrize("prec", ["fp64", "mixed"])
-def test_continuation_calls_keep_the_list(prec, tmp_path, gpu_lib):
+def test_continuation_calls_keep_the_list(case, prec, tmp_path, gpu_lib):
     """A run cut into continuation calls (awsem_run_window) is the run in one
     call: the list state carries over between the calls."""
     from awsemmd_b200.engine import AwsemSystem
 
-    files, g = write_case("c0go", tmp_path)
+    files, g = write_case(case, tmp_path)
     nsteps, kw = _kw(g)
     skin, delay, every, check = neigh_of(g)
     with AwsemSystem(files, precision=prec) as s:
@@ -69,10 +73,11 @@ def test_continuation_calls_keep_the_list(prec, tmp_path, gpu_lib):
     assert np.array_equal(np.concatenate([r0, r1, r2]), rows_one)
 
 
-def test_persistent_form_equals_kernel_chain(tmp_path, gpu_lib):
+@pytest.mark.parametrize("case", ["c0go", "c0x"])
+def test_persistent_form_equals_kernel_chain(case, tmp_path, gpu_lib):
     from awsemmd_b200.engine import AwsemSystem
 
-    files, g = write_case("c0go", tmp_path)
+    files, g = write_case(case, tmp_path)
     nsteps, kw = _kw(g)
     out = {}
     for form in ["kernels", "persistent"]:

@@ -72,7 +72,7 @@ def run_deck(files, g, thermo):
         os.chdir(cwd)
 
 
-@pytest.mark.parametrize("case", ["r1r69", "r1r69tb", "r1r69go", "c0go"])
+@pytest.mark.parametrize("case", ["r1r69", "r1r69tb", "r1r69go", "c0go", "c0x"])
 def test_deck_reproduces_the_reference_run(case, tmp_path, gpu_lib):
     """r1r69tb: fragment memory in the table form, as the shipped 1R69 decks
     use it; r1r69go and c0go: [AMH-Go], c0go with neighbor 0.6 and

@@ -6,7 +6,7 @@ import pytest
 
 from conftest import REFERENCE_SRC, neigh_of, write_case
 
-CASES = ["c0", "sheet", "r1r69", "r1r69tb", "r1r69go", "r1r69go2", "c0go"]
+CASES = ["c0", "sheet", "r1r69", "r1r69tb", "r1r69go", "r1r69go2", "c0go", "c0x", "sheetx"]
 
 
 def rel_err(a, b):
@@ -49,28 +49,34 @@ def test_terms_exercised():
     """The fixtures between them exercise every term on the path."""
     e = {n: np.load(os.path.join(os.path.dirname(__file__), "golden", f"{n}.npz"))["e0"] for n in CASES}
     for k, name in [(1, "chain"), (3, "chi"), (4, "rama"), (6, "dssp"), (7, "p_ap"), (8, "water"), (9, "burial"),
-                    (10, "helix"), (11, "amh-go"), (12, "frag_mem"), (19, "bond")]:
+                    (10, "helix"), (11, "amh-go"), (12, "frag_mem"), (14, "contact restraints"), (16, "ssb"),
+                    (17, "debye-hueckel"), (19, "bond")]:
         assert max(abs(e[c][k]) for c in CASES) > 1e-2, name
     assert max(abs(e[c][18]) for c in CASES) > 1.0  # vexcluded
 
 
-def test_amh_go_list_rule_is_pinned(tmp_path, oracle_built):
-    """c0go's trajectory depends on when LAMMPS rebuilds the fix's full list:
-    the oracle run with another rebuild rule, or another skin, leaves the
-    reference's trajectory by far more than the parity tolerance."""
+@pytest.mark.parametrize("name", ["c0go", "c0x"])
+def test_list_rule_is_pinned(name, tmp_path, oracle_built):
+    """c0go's (AMH-Go) and c0x's (Debye-Hueckel on the CA pairs of the half
+    list) trajectories depend on when LAMMPS rebuilds the fix's lists: the
+    oracle run with another rebuild rule, or another skin, leaves the
+    reference's final positions by more than the parity tolerance (1e-6 A)."""
     import ref
 
-    files, g = write_case("c0go", tmp_path)
+    files, g = write_case(name, tmp_path)
     nsteps, dt, t0, t1, damp, seed = g["run"]
     skin, delay, every, check = neigh_of(g)
     assert (delay, every, check) != (0, 1, 1)
-    for wrong in [(skin, 0, 1, 0), (skin, delay, every, 0), (2.0, delay, every, check)]:
+    wrongs = [(skin, 0, 1, 0), (2.0, delay, every, check)]
+    if name == "c0go":
+        wrongs.append((skin, delay, every, 0))
+    for wrong in wrongs:
         o = ref.OracleSystem(files)
         o.set_neighbor(*wrong)
-        _, _, thermo = o.run(g["x0"], g["v0"], int(nsteps), dt=dt, langevin=True, t_start=t0, t_stop=t1,
-                             damp=damp, seed=int(seed))
+        x, _, _ = o.run(g["x0"], g["v0"], int(nsteps), dt=dt, langevin=True, t_start=t0, t_stop=t1, damp=damp,
+                        seed=int(seed))
         o.close()
-        assert np.abs(thermo - g["thermo"]).max() > 1e-3, wrong
+        assert np.abs(x - g["xN"]).max() > 2e-6, wrong
 
 
 def test_langevin_stream_shared(oracle_built):
