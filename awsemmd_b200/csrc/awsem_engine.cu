@@ -173,6 +173,7 @@ template <typename R> class Engine : public EngineBase {
   DBuf<double> charge;             // Debye-Hueckel charges
   DBuf<int> cr_start, cr_j;        // contact restraints
   DBuf<double> cr_w, cr_r0;
+  DBuf<int> zim;                   // membrane zones
   int efix_slots = 5;
   int fm_groups = 0, fm_dsplit = 1;
   DBuf<double> thermo_rows;
@@ -290,6 +291,7 @@ template <typename R> class Engine : public EngineBase {
     a.cr_w = cr_w.p;
     a.cr_r0 = cr_r0.p;
     a.efix_slots = efix_slots;
+    a.zim = zim.p;
     a.groups = groups;
     a.step = dstep.p;
     a.res_sys = res_sys.p;
@@ -415,6 +417,11 @@ template <typename R> class Engine : public EngineBase {
       cr_r0.upload(in.cr.r0.empty() ? std::vector<double>{0.0} : in.cr.r0, s0);
     }
     efix_slots = (in.ff.p.terms & (T_SSB | T_DH | T_CONTREST)) ? 8 : 5;
+    if (in.ff.p.terms & T_MEMB) {
+      std::vector<int> z(in.zim);
+      z.resize((size_t) nn, 1);
+      zim.upload(z, s0);
+    }
     CK(cudaFuncSetAttribute(dev::k_fragmem<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             4 * dev::fm_warp_smem<R>(true)));
     // pair-list radii of the terms
@@ -572,10 +579,11 @@ template <typename R> class Engine : public EngineBase {
     const bool fmt = (a.groups & dev::G_FIX) && (p.terms & T_FM_TABLE);
     const bool go = (a.groups & dev::G_FIX) && (p.terms & T_AMHGO);
     const bool px = (a.groups & dev::G_FIX) && (p.terms & (T_SSB | T_DH | T_CONTREST));
+    const bool rx = (a.groups & dev::G_FIX) && (p.terms & (T_SHAKE | T_MEMB));
     // the emulated lists' decision for this step, before anything reads it
     if (lists_emulated())
       dev::k_list_decide<<<(n_sys() + 127) / 128, 128, 0, s0>>>(nl.p, n_sys(), lst_ago.p, lst_over.p, lst_build.p);
-    if (fm || fmt || go || px) {
+    if (fm || fmt || go || px || rx) {
       // fragment memory is independent of the pair passes: second stream
       CK(cudaEventRecord(ev_fork, s0));
       CK(cudaStreamWaitEvent(s1, ev_fork, 0));
@@ -583,6 +591,7 @@ template <typename R> class Engine : public EngineBase {
       if (fmt) dev::k_fm_table<R><<<fm_table_blocks(), tb, 0, s1>>>(a, p);
       if (go) dev::k_amh_go<R><<<nb, tb, 0, s1>>>(a, p);
       if (px) dev::k_pair_extra<R><<<pair_blocks, tb, 0, s1>>>(a, p);
+      if (rx) dev::k_residue_extra<R><<<nb, tb, 0, s1>>>(a, p);
       CK(cudaEventRecord(ev_join, s1));
     }
     dev::k_density<R><<<pair_blocks, tb, 0, s0>>>(a, p);
@@ -590,7 +599,7 @@ template <typename R> class Engine : public EngineBase {
     dev::k_water_xi<R><<<pair_blocks, tb, 0, s0>>>(a, p);
     dev::k_pair<R><<<pair_blocks, tb, 0, s0>>>(a, p);
     dev::k_hbond<R><<<hb_blocks, 128, 0, s0>>>(a, p);
-    if (fm || fmt || go || px) CK(cudaStreamWaitEvent(s0, ev_join, 0));
+    if (fm || fmt || go || px || rx) CK(cudaStreamWaitEvent(s0, ev_join, 0));
   }
 
   int fm_table_blocks() const
@@ -608,6 +617,8 @@ template <typename R> class Engine : public EngineBase {
     if (!(groups & dev::G_BOND)) CK(cudaMemsetAsync(e_res.p + (size_t) E_BOND * nn, 0, sizeof(double) * nn, s0));
     if (!(groups & dev::G_FIX) || !(in.ff.p.terms & T_AMHGO))
       CK(cudaMemsetAsync(e_res.p + (size_t) E_AMHGO * nn, 0, sizeof(double) * nn, s0));
+    if (!(groups & dev::G_FIX))
+      for (int t : {E_SHAKE, E_MEMB}) CK(cudaMemsetAsync(e_res.p + (size_t) t * nn, 0, sizeof(double) * nn, s0));
   }
 
   // energy sums of replicas [rep0, rep0 + count) (all of them by default)
@@ -854,7 +865,8 @@ template <typename R> class Engine : public EngineBase {
                        (a.groups & dev::G_FIX) && (in.ff.p.terms & T_FM_TABLE) ? 1 : 0,
                        (a.groups & dev::G_FIX) && (in.ff.p.terms & T_AMHGO) ? 1 : 0,
                        (a.groups & dev::G_FIX) && (in.ff.p.terms & (T_SSB | T_DH | T_CONTREST)) ? 1 : 0,
-                       lists_emulated() ? n_sys() : 0};
+                       lists_emulated() ? n_sys() : 0,
+                       (a.groups & dev::G_FIX) && (in.ff.p.terms & (T_SHAKE | T_MEMB)) ? 1 : 0};
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(ps_grid_now);
     cfg.blockDim = dim3(dev::kStepThreads);
@@ -1105,6 +1117,7 @@ template <typename R> class Engine : public EngineBase {
             if (p.terms & T_FM_TABLE) dev::k_fm_table<R><<<fm_table_blocks(), tb, 0, s0>>>(a, p);
             if (p.terms & T_AMHGO) dev::k_amh_go<R><<<nb, tb, 0, s0>>>(a, p);
             if (p.terms & (T_SSB | T_DH | T_CONTREST)) dev::k_pair_extra<R><<<pair_blocks, tb, 0, s0>>>(a, p);
+            if (p.terms & (T_SHAKE | T_MEMB)) dev::k_residue_extra<R><<<nb, tb, 0, s0>>>(a, p);
             break;
           case 9: dev::k_finish<R><<<nb, tb, 0, s0>>>(a, d_integ.p, g1.p, g2.p, ftot.p, x.p); break;
         }
@@ -1512,8 +1525,9 @@ template <typename R> class Engine : public EngineBase {
     if (f.ff.p.terms & T_FM_TABLE)
       throw std::invalid_argument("serving handles do not support [Fragment_Memory_Table] (use [Fragment_Memory])");
     if (f.ff.p.terms & T_AMHGO) throw std::invalid_argument("serving handles do not support [AMH-Go]");
-    if (f.ff.p.terms & (T_SSB | T_DH | T_CONTREST))
-      throw std::invalid_argument("serving handles do not support [Solvent_Barrier], [DebyeHuckel] or [Contact_Restraints]");
+    if (f.ff.p.terms & (T_SSB | T_DH | T_CONTREST | T_MEMB))
+      throw std::invalid_argument(
+          "serving handles do not support [Solvent_Barrier], [DebyeHuckel], [Contact_Restraints] or [Membrane]");
     const long long groups = (cap_res + 31) / 32;
     if (groups * 32 * pairs_per_res >= (1ll << 31)) throw std::invalid_argument("residue capacity too large");
     sf = &f;
@@ -1864,7 +1878,7 @@ template <typename R> class Engine : public EngineBase {
     add(bond_r0), add(fm_soff), add(fm_slen), add(fm_rf), add(fm_coef), add(tb_data), add(tb_present);
     add(go_start), add(go_partner), add(go_rnat), add(go_gamma), add(go_sig_sq), add(go_norm);
     add(go_in), add(lst_x0), add(lst_ago), add(lst_over), add(lst_build), add(charge), add(cr_start), add(cr_j),
-        add(cr_w), add(cr_r0);
+        add(cr_w), add(cr_r0), add(zim);
     add(thermo_rows), add(res_sys), add(sys_begin);
     add(sys_end), add(sys_seed), add(slot_run), add(d_integ);
     return b;

@@ -123,6 +123,7 @@ template <typename R> struct StepArgs {
   const int *cr_start, *cr_j;    // contact restraints of residue i (i < j): [cr_start[i], cr_start[i+1])
   const double *cr_w, *cr_r0;
   int efix_slots;                // fixed-point energy slots in use (5, or 8 with the pair terms above)
+  const int *zim;                // [n]: membrane zone (1, 2, 3) of the residue
   int groups;       // AWSEM_TERMS_* bits: 1 fix backbone, 2 pair vexcluded, 4 bonds
   long long *step;   // device step counter (advanced by k_nl_decide)
   // replicas: residue -> replica, replica residue ranges, Langevin seeds
@@ -662,7 +663,8 @@ template <typename R> __device__ __forceinline__ void residue_one(const StepArgs
   double eb = 0.0, bc = 0.0;
   if (fix && (p.terms & T_BURIAL)) {
     double rho = rw;
-    const double *g = s.tables + TB_BURIAL + 3 * s.res_type[i];
+    // a phosphorylated residue takes glutamate's burial gammas (fix_backbone.cpp:2887-2899)
+    const double *g = s.tables + TB_BURIAL + 3 * ((fl & R_PHOSPH) ? 6 : s.res_type[i]);
     double t[3][2];
     for (int k = 0; k < 3; k++) {
       t[k][0] = tanh(p.burial_kappa * (rho - p.burial_ro_min[k]));
@@ -741,9 +743,12 @@ template <typename R> __device__ __forceinline__ void water_xi_pass(const StepAr
     if (s.res_chain[j] == s.res_chain[i] && j - i < p.contact_cutoff) continue;
     const R rsq = norm2(diff<R>(contact(s, i), contact(s, j)));
     const int ti = s.res_type[i], tj = s.res_type[j];
+    // pairs with a phosphorylated residue use the phosphorylation gammas (fix_backbone.cpp:2872-2885)
+    const double *W = ((p.terms & T_PHOSPH) && ((s.res_flags[i] | s.res_flags[j]) & R_PHOSPH))
+                          ? s.tables + TB_WATER_PHOSPH : WG;
     for (int w = 0; w < p.n_wells; w++) {
       if (!p.well_flag[w]) continue;
-      const double g0 = WG[w * 800 + (ti * 20 + tj) * 2], g1 = WG[w * 800 + (ti * 20 + tj) * 2 + 1];
+      const double g0 = W[w * 800 + (ti * 20 + tj) * 2], g1 = W[w * 800 + (ti * 20 + tj) * 2 + 1];
       // the reference's `!fabs(g0 - g1) < delta` holds exactly when g0 != g1
       if (g0 != g1 && rsq > R(p.w_rmin_sq[w]) && rsq < R(p.w_rmax_sq[w])) {
         R th, pr;
@@ -842,10 +847,11 @@ template <typename R> __device__ __forceinline__ void pair_pass(const StepArgs<R
       if (T & T_WATER) {
         const int ti = s.res_type[i], tj = s.res_type[j];
         const bool sep = other || dij >= p.contact_cutoff;
+        const double *W = ((fli | flj) & R_PHOSPH) ? s.tables + TB_WATER_PHOSPH : WG;
         for (int w = 0; w < p.n_wells; w++) {
           if (!p.well_flag[w]) continue;
           if (sep && rsq > R(p.w_rmin_sq[w]) && rsq < R(p.w_rmax_sq[w])) {
-            const double g0 = WG[w * 800 + (ti * 20 + tj) * 2], g1 = WG[w * 800 + (ti * 20 + tj) * 2 + 1];
+            const double g0 = W[w * 800 + (ti * 20 + tj) * 2], g1 = W[w * 800 + (ti * 20 + tj) * 2 + 1];
             const double sg = fabs(g0 - g1) < 1e-5 ? 0.5 * (g0 + g1) : g0 + (g1 - g0) * a.sig_w[i] * a.sig_w[j];
             R th, pr;
             if (w == 0) {
@@ -1199,6 +1205,87 @@ template <typename R> __device__ __forceinline__ void pair_extra_pass(const Step
 }
 
 template <typename R> __global__ void k_pair_extra(StepArgs<R> a, FFParams p) { pair_extra_pass(a, p, grid_span()); }
+
+// Per-residue terms the benchmark force field leaves off, thread per residue,
+// FP64 in both forms, on the second stream: Shake (compute_shake,
+// fix_backbone.cpp:2172-2237) and the membrane potential
+// (compute_membrane_potential, :6107-6235) on the contact bead.
+template <typename R> __device__ __forceinline__ void residue_extra_one(const StepArgs<R> &a, const FFParams &p, int i)
+{
+  const DevSys<R> &s = a.s;
+  const int n = s.n_res, fl = s.res_flags[i];
+  if (p.terms & T_SHAKE) {
+    // harmonic CA(i)-CA(i+1), CA(i)-O(i), O(i)-CA(i+1) (the first and last not at a chain end)
+    double e = 0.0;
+    long long fca[3] = {0, 0, 0}, fo[3] = {0, 0, 0}, fnx[3] = {0, 0, 0};
+    const V3<double> ca = bead(s, i, B_CA), o = bead(s, i, B_O);
+    auto spring = [&](V3<double> u, V3<double> v, double r0, long long *fu, long long *fv) {
+      const double dx[3] = {u.x - v.x, u.y - v.y, u.z - v.z};
+      const double r = sqrt(dx[0] * dx[0] + dx[1] * dx[1] + dx[2] * dx[2]), dr = r - r0;
+      const double force = 2 * p.epsilon * p.k_shake * dr / r;
+      e += p.epsilon * p.k_shake * dr * dr;
+      for (int c = 0; c < 3; c++) {
+        fu[c] += fix_force(-dx[c] * force);
+        fv[c] += fix_force(dx[c] * force);
+      }
+    };
+    const bool last = fl & R_LAST;
+    V3<double> ca1{0, 0, 0};
+    if (!last) {
+      ca1 = bead(s, i + 1, B_CA);
+      spring(ca, ca1, p.r_sh1, fca, fnx);
+    }
+    spring(ca, o, p.r_sh2, fca, fo);
+    if (!last) spring(o, ca1, p.r_sh3, fo, fnx);
+    scatter_fix(s, i, B_CA, fca);
+    scatter_fix(s, i, B_O, fo);
+    if (!last) scatter_fix(s, i + 1, B_CA, fnx);
+    a.e_res[(size_t) E_SHAKE * n + i] = e;
+  }
+  if (p.terms & T_MEMB) {
+    const bool gly = fl & R_GLY;
+    const V3<double> xi = bead(s, i, gly ? B_CA : B_CB);
+    const double dx = xi.x - p.memb_xo[0], dy = xi.y - p.memb_xo[1], dz = xi.z - p.memb_xo[2];
+    const double ma = p.rho0_distor * p.rho0_max, mb = p.memb_len / 2;
+    const double rho = sqrt(dx * dx + dy * dy);
+    const double rho0 = (p.rho0_max - ma) + (ma / p.memb_len) * (dz + mb);
+    const double kb = p.k_bin;
+    const double t_per = tanh(kb * (dz - mb)), t_m1 = tanh(kb * (dz + mb)), t_m2 = tanh(kb * (mb - dz));
+    const double t_cyt = tanh(kb * (-mb - dz)), t_por = tanh(kb * (rho - rho0));
+    const double s_per = 0.5 * (1 + t_per), s_mem = 0.5 * (t_m1 + t_m2), s_cyt = 0.5 * (1 + t_cyt);
+    const double s_por = 0.5 * (1 - t_por), s_nopor = 1 - s_por;
+    const double dz_per = 0.5 * kb * (1 - t_per * t_per);
+    const double dz_mem = -0.5 * kb * (t_m1 * t_m1) + 0.5 * kb * (t_m2 * t_m2);
+    const double dz_cyt = -0.5 * kb * (1 - t_cyt * t_cyt);
+    const double dr1_dz = ma / p.memb_len;
+    const double dz_s_por = 0.5 * kb * (1 - t_por * t_por) * dr1_dz;
+    const double dx_s_por = ((-0.5 * kb * dx) / rho) * (1 - t_por * t_por);
+    const double dy_s_por = ((-0.5 * kb * dy) / rho) * (1 - t_por * t_por);
+    const double dz_s_por_smem = s_mem * dz_s_por + dz_mem * s_por;
+    const double dz_s_nopor_smem = s_mem * -dz_s_por + dz_mem * s_nopor;
+    // zones 1 and 3 share one sign pattern, zone 2 the opposite one
+    const int z = a.zim[i] - 1;
+    const double *g = p.g_memb[z];
+    const double sg = z == 1 ? -1.0 : 1.0;
+    const double V = sg * ((-g[0] * s_per) + (-g[1] * s_cyt) + (g[2] * s_mem * s_nopor) + (-g[3] * s_mem * s_por));
+    const double dVx = sg * (g[2] * s_mem * -dx_s_por + (-g[3]) * s_mem * dx_s_por);
+    const double dVy = sg * (g[2] * s_mem * -dy_s_por + (-g[3]) * s_mem * dy_s_por);
+    const double dVz = sg * (-g[0] * dz_per + (-g[1]) * dz_cyt + g[2] * dz_s_nopor_smem + (-g[3]) * dz_s_por_smem);
+    const double k = p.epsilon * p.k_overall_memb;
+    const long long f[3] = {fix_force(-k * dVx), fix_force(-k * dVy), fix_force(-k * dVz)};
+    scatter_fix(s, i, gly ? B_CA : B_CB, f);
+    a.e_res[(size_t) E_MEMB * n + i] = k * V;
+  }
+}
+
+template <typename R> __device__ __forceinline__ void residue_extra_pass(const StepArgs<R> &a, const FFParams &p, Span sp)
+{
+  if (!(a.groups & G_FIX)) return;
+  for (int r = sp.t; r < a.n_run; r += sp.nthr)
+    if (a.res_sys[r] >= 0) residue_extra_one(a, p, r);
+}
+
+template <typename R> __global__ void k_residue_extra(StepArgs<R> a, FFParams p) { residue_extra_pass(a, p, grid_span()); }
 
 // AMH-Go (FixBackbone::compute_amh_go_model, fix_backbone.cpp:3856-3992) of
 // residue r's CA and CB: over each atom's native contacts (the full-list

@@ -83,9 +83,8 @@ void read_coeff_file(const std::string &path, ForceField &ff)
   const int i_rp = 6;  // first proline Ramachandran well
   double k_rama = 0.0, k_water = 0.0;
   static const char *outside[] = {
-      "[Shake]", "[Excluded]", "[Excluded_P]", "[Excluded_R6]",
-      "[Vector_Fragment_Memory]", "[Membrane]",
-      "[Fragment_Frustratometer]", "[Tertiary_Frustratometer]", "[Nmer_Frustratometer]", "[Phosphorylation]",
+      "[Excluded]", "[Excluded_P]", "[Excluded_R6]", "[Vector_Fragment_Memory]",
+      "[Fragment_Frustratometer]", "[Tertiary_Frustratometer]", "[Nmer_Frustratometer]",
       "[Amylometer]", "[Selection_Temperature]", "[Monte_Carlo_Seq_Opt]", "[Optimization]",
       "[Burial_Optimization]", "[DebyeHuckel_Optimization]", "[Shuffler]", "[Mutate_Sequence]"};
   std::string s, pending;
@@ -173,6 +172,24 @@ void read_coeff_file(const std::string &path, ForceField &ff)
       }
       if (ff.amh_go_censor == 2)
         fail("AMH-Go: frustration censoring 2 (native distances from go_rnative*.dat) is not supported");
+    } else if (s == "[Shake]") {
+      // fix_backbone.cpp:180-183
+      p.terms |= T_SHAKE;
+      in >> p.k_shake >> p.r_sh1 >> p.r_sh2 >> p.r_sh3;
+    } else if (s == "[Membrane]") {
+      // fix_backbone.cpp:346-358
+      p.terms |= T_MEMB;
+      in >> p.k_overall_memb >> p.k_bin >> p.memb_xo[0] >> p.memb_xo[1] >> p.memb_xo[2] >> p.memb_pore_type >>
+          p.memb_len >> p.rho0_max >> p.rho0_distor;
+      for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 4; j++) in >> p.g_memb[i][j];
+    } else if (s == "[Phosphorylation]") {
+      // fix_backbone.cpp:413-421 (the water section must come first)
+      if (!(p.terms & T_WATER)) fail("Cannot run phosphorylation without water potential");
+      p.terms |= T_PHOSPH;
+      in >> p.k_hypercharge >> p.n_phosph_res;
+      if (p.n_phosph_res > 20) fail("Number of phosphorylated residues may not exceed 20");
+      for (int i = 0; i < p.n_phosph_res; i++) in >> p.phosph_res[i];
     } else if (s == "[Solvent_Barrier]") {
       // fix_backbone.cpp:334-345 (the 20 radius shifts are read whatever the correction flag)
       p.terms |= T_SSB;
@@ -349,6 +366,25 @@ void read_tables(const std::string &dir, ForceField &ff, Topology &top)
             T[TB_WATER + w * 800 + (a * 20 + b) * 2 + 1] = g1;
           }
         }
+  }
+  if (p.terms & T_PHOSPH) {
+    // fix_backbone.cpp:643-670: pairs with a phosphorylated residue take the
+    // serine (15) rows and columns from glutamate (6), scaled by the
+    // hypercharge factor once (partner class 1) or twice (classes 2, 3), in the
+    // reference's loop order
+    static const int bb_class[20] = {1, 3, 2, 2, 4, 2, 2, 1, 3, 4, 4, 3, 4, 4, 1, 1, 1, 4, 4, 4};
+    for (int w = 0; w < p.n_wells; w++) {
+      double *P = &T[TB_WATER_PHOSPH + w * 800];
+      std::copy(&T[TB_WATER + w * 800], &T[TB_WATER + w * 800] + 800, P);
+      for (int i = 0; i < 20; i++) {
+        const double fac = bb_class[i] == 1 ? p.k_hypercharge
+                         : (bb_class[i] == 2 || bb_class[i] == 3) ? pow(p.k_hypercharge, 2) : 1.0;
+        for (int c = 0; c < 2; c++) {
+          const double g = bb_class[i] == 4 ? P[(i * 20 + 6) * 2 + c] : P[(i * 20 + 6) * 2 + c] * fac;
+          P[(i * 20 + 15) * 2 + c] = P[(15 * 20 + i) * 2 + c] = g;
+        }
+      }
+    }
   }
   if (p.terms & T_BURIAL) {
     if (!(p.terms & T_WATER)) fail("Cannot use burial without water potential");
@@ -865,6 +901,31 @@ void build_fm_table_tb(const ForceField &ff, const Topology &top, const GammaTab
   }
 }
 
+// zim (fix_backbone.cpp:611-619): the membrane zone (1, 2 or 3) of each
+// residue; the reference leaves the potential undefined for other values
+void read_zim(const std::string &path, int n_res, std::vector<int> &z)
+{
+  std::ifstream in(path);
+  if (!in) fail("File zim doesn't exist");
+  z.assign(n_res, 0);
+  for (int i = 0; i < n_res; i++) {
+    in >> z[i];
+    if (!in || in.eof()) fail("Membrane potential parameter file format error");
+    if (z[i] < 1 || z[i] > 3) fail("Membrane: zim values must be 1, 2 or 3");
+  }
+}
+
+// phosph_map (fix_backbone.cpp:671-681): residue numbers from 1; 0 entries are ignored
+void flag_phosphorylated(const FFParams &p, Topology &top)
+{
+  for (int k = 0; k < p.n_phosph_res; k++) {
+    const int r = p.phosph_res[k];
+    if (r == 0) continue;
+    if (r < 1 || r > top.n_res) fail("Phosphorylation: residue number out of range");
+    top.res_flags[r - 1] |= R_PHOSPH;
+  }
+}
+
 // charge_on_residues.dat (fix_backbone.cpp:1022-1045): a count, then that
 // many (residue number, charge) records; residues not listed carry no charge
 void read_charges(const std::string &path, int n_res, std::vector<double> &q)
@@ -1029,6 +1090,7 @@ void load_system_arrays(const SharedForceField &sf, const ReplicaArrays &ra, Sys
 {
   if (sf.ff.p.terms & T_AMHGO) fail("AMH-Go needs a run directory (amh-go.gro, amh-go.gamma): load the replica from files");
   if (sf.ff.p.terms & T_DH) fail("DebyeHuckel needs a run directory (charge_on_residues.dat): load the replica from files");
+  if (sf.ff.p.terms & T_MEMB) fail("Membrane needs a run directory (zim): load the replica from files");
   if (sf.ff.p.terms & T_CONTREST)
     fail("Contact_Restraints needs a run directory (the restraints file): load the replica from files");
   if (ra.n_res <= 0 || ra.n_chains <= 0 || !ra.chain_len || !ra.seq || !ra.x) fail("replica: empty description");
@@ -1119,6 +1181,7 @@ void load_system_arrays(const SharedForceField &sf, const ReplicaArrays &ra, Sys
     S.mems.clear();
     S.mems.shrink_to_fit();
   }
+  if (S.ff.p.terms & T_PHOSPH) flag_phosphorylated(S.ff.p, t);
   S.x.assign(3 * t.n_atoms, 0.0);
   S.v.assign(3 * t.n_atoms, 0.0);
   for (int s = 0; s < t.n_atoms; s++)
@@ -1255,6 +1318,8 @@ void assemble_batch(const std::vector<const SystemInput *> &reps, Batch &B)
   }
   if (B.ff.p.terms & T_DH)
     for (auto *r : reps) B.charge.insert(B.charge.end(), r->charge.begin(), r->charge.end());
+  if (B.ff.p.terms & T_MEMB)
+    for (auto *r : reps) B.zim.insert(B.zim.end(), r->zim.begin(), r->zim.end());
   if (B.ff.p.terms & T_CONTREST) {
     B.cr.start.push_back(0);
     int res_off = 0;
@@ -1409,6 +1474,8 @@ void load_system_atoms(const std::string &dir, const std::string &coeff_file, co
     }
   }
   if (S.ff.p.terms & T_DH) read_charges(path_in(dir, "charge_on_residues.dat"), S.top.n_res, S.charge);
+  if (S.ff.p.terms & T_MEMB) read_zim(path_in(dir, "zim"), S.top.n_res, S.zim);
+  if (S.ff.p.terms & T_PHOSPH) flag_phosphorylated(S.ff.p, S.top);
   if (S.ff.p.terms & T_CONTREST) {
     read_contact_restraints(path_in(dir, S.ff.cr_file), S.ff.p, S.top.n_res, S.cr);
     S.ff.p.pair_list_cutoff = pair_list_cutoff(S.ff.p);  // the restraints set their cutoff

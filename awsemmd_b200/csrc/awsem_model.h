@@ -23,16 +23,16 @@ enum TermFlag : uint32_t {
   T_CHAIN = 1u << 0, T_CHI = 1u << 1, T_RAMA = 1u << 2, T_RAMA_P = 1u << 3, T_SSW = 1u << 4,
   T_DSSP = 1u << 5, T_PAP = 1u << 6, T_WATER = 1u << 7, T_BURIAL = 1u << 8, T_HELIX = 1u << 9,
   T_FM = 1u << 10, T_FM_TABLE = 1u << 11, T_AMHGO = 1u << 12, T_SSB = 1u << 13, T_DH = 1u << 14,
-  T_CONTREST = 1u << 15
+  T_CONTREST = 1u << 15, T_SHAKE = 1u << 16, T_MEMB = 1u << 17, T_PHOSPH = 1u << 18
 };
 
 // Residue flags
-enum ResFlag : uint32_t { R_GLY = 1u, R_PRO = 2u, R_FIRST = 4u, R_LAST = 8u };
+enum ResFlag : uint32_t { R_GLY = 1u, R_PRO = 2u, R_FIRST = 4u, R_LAST = 8u, R_PHOSPH = 16u };
 
 // Offsets of the lookup tables inside the device table buffer (doubles)
 enum TableOffset {
   TB_ANTI_HB = 0, TB_ANTI_NHB = 800, TB_PARA_HB = 1600, TB_PARA_ONE = 2400, TB_ANTI_ONE = 2420,
-  TB_BURIAL = 2440, TB_WATER = 2500, TB_SIZE = 2500 + 5 * 800
+  TB_BURIAL = 2440, TB_WATER = 2500, TB_WATER_PHOSPH = 2500 + 5 * 800, TB_SIZE = 2500 + 10 * 800
 };
 
 // Scalar parameters, passed to kernels by value.  Names follow the reference.
@@ -72,6 +72,14 @@ struct FFParams {
   double k_plusplus, k_minusminus, k_plusminus, k_screening, screening_length;
   // [Contact_Restraints] (:321-327, :1106-1150): epsilon-scaled strength, width and its cutoffs
   double k_cont_rest, cr_sigma, cr_sigma_sq_inv, cr_dr_cut, cr_cut_sq;
+  // [Shake] (:180-183): strength and the CA(i)-CA(i+1), CA(i)-O(i), O(i)-CA(i+1) lengths
+  double k_shake, r_sh1, r_sh2, r_sh3;
+  // [Membrane] (:346-358): strength, switching steepness, centre, pore, thickness, radii, gammas
+  double k_overall_memb, k_bin, memb_xo[3], memb_len, rho0_max, rho0_distor, g_memb[3][4];
+  int memb_pore_type;
+  // [Phosphorylation] (:413-421): hypercharge factor; the residues are flagged R_PHOSPH
+  double k_hypercharge;
+  int n_phosph_res, phosph_res[20];
 };
 
 struct ForceField {
@@ -184,6 +192,7 @@ struct SystemInput {
   AmhGoContacts go;
   std::vector<double> charge;  // [n_res] Debye-Hueckel charges (charge_on_residues.dat)
   ContactRestraints cr;
+  std::vector<int> zim;        // [n_res] membrane zone of each residue (file zim: 1, 2 or 3)
   std::vector<double> x, v;  // internal order [n_atoms*3]
 };
 
@@ -240,6 +249,7 @@ struct Batch {
   AmhGoContacts go;   // concatenated AMH-Go contacts (partners offset to batch atoms)
   std::vector<double> charge;  // concatenated Debye-Hueckel charges
   ContactRestraints cr;        // concatenated contact restraints (residues offset)
+  std::vector<int> zim;        // concatenated membrane zones
   std::vector<double> x, v;
   std::vector<int> res_sys;              // residue -> replica
   std::vector<int> sys_res_begin, sys_res_end;    // [n_sys]

@@ -132,6 +132,7 @@ struct PersistArgs {
   int amh_go;        // AMH-Go on
   int pair_extra;    // solvent barrier, Debye-Hueckel or contact restraints on
   int list_reps;     // replicas whose LAMMPS lists are emulated (0: none)
+  int residue_extra; // Shake or the membrane potential on
 };
 
 // Fragment-memory units taken from the step's counter until none is left
@@ -215,6 +216,7 @@ template <typename R> __global__ void __launch_bounds__(kStepThreads, 2) k_step(
       if (q.fm_table) fm_table_pass(a, p, sp);
       if (q.amh_go) amh_go_pass(a, p, sp);
       if (q.pair_extra) pair_extra_pass(a, p, sp);
+      if (q.residue_extra) residue_extra_pass(a, p, sp);
       fragmem_take_units(a, p, q, ring, wsm, kbase);
     }
   }

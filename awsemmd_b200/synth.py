@@ -350,6 +350,29 @@ def pair_terms_text(k_cont_rest=1.0, cr_sigma=1.0, cr_file="contact_restraints.d
             + f"\n[Contact_Restraints]\n{k_cont_rest}\n{cr_sigma}\n{cr_file}\n")
 
 
+def residue_terms_text(sys_: System, phosph=None) -> str:
+    """[Shake] (the reference examples' lengths), [Membrane] centred on the
+    system's CA centroid (30 A slab, distorted pore, per-zone gammas) and
+    [Phosphorylation] of the given residue numbers (hypercharge 1.2)."""
+    ca = np.concatenate([ch.ca for ch in sys_.chains])
+    c = ca.mean(axis=0)
+    gm = ((1.0, 0.8, 1.2, 0.5), (0.7, 0.9, 1.1, 0.6), (0.4, 1.3, 0.9, 0.8))
+    text = "\n[Shake]\n10.0 3.83 2.36 2.71\n"
+    text += (f"\n[Membrane]\n1.0\n0.5\n{c[0]:.3f} {c[1]:.3f} {c[2]:.3f}\n0\n30.0\n5.0\n0.3\n"
+             + "".join(" ".join(str(v) for v in row) + "\n" for row in gm))
+    if phosph:
+        text += f"\n[Phosphorylation]\n1.2\n{len(phosph)}\n" + " ".join(str(r) for r in phosph) + "\n"
+    return text
+
+
+def write_zim(sys_: System, path: str, seed: int = 11) -> None:
+    """zim: a membrane zone (1, 2 or 3) per residue, seeded."""
+    n = sum(ch.length for ch in sys_.chains)
+    z = np.random.default_rng(seed).integers(1, 4, size=n)
+    with open(path, "w") as f:
+        f.write("\n".join(str(int(v)) for v in z) + "\n")
+
+
 def write_charges(sys_: System, path: str) -> None:
     """charge_on_residues.dat: +1 on K and R, -1 on D and E (residues numbered over all chains)."""
     seq = "".join(ch.seq for ch in sys_.chains)

@@ -134,6 +134,15 @@ struct Params {
   double k_PlusPlus = 0, k_MinusMinus = 0, k_PlusMinus = 0, k_screening = 0, screening_length = 0;
   double k_cont_rest = 0, cr_sigma = 0, cr_sigma_sq_inv = 0, cr_dr_cutoff = 0, cr_glob_cutoff_sq = 0;
   std::string cr_file;
+  // [Shake] (:180-183), [Membrane] (:346-358), [Phosphorylation] (:413-421)
+  bool shake = 0, memb = 0, phosph = 0;
+  double k_shake = 0, r_sh1 = 0, r_sh2 = 0, r_sh3 = 0;
+  double k_overall_memb = 0, k_bin = 0, memb_xo[3] = {0, 0, 0}, memb_len = 0, rho0_max = 0, rho0_distor = 0;
+  double g_memb[3][4] = {{0}};
+  int memb_pore_type = 0;
+  double k_hypercharge = 0;
+  int n_phosph_res = 0, phosph_res[20] = {0};
+  double phosph_water_gamma[5][20][20][2];
   // [Fragment_Memory_Table] (fix_backbone.cpp:310-321)
   double tb_rmin = 0, tb_rmax = 0, tb_dr = 0, tb_width = 0;
   int tb_size = 0, tb_use_file = 0;
@@ -329,6 +338,16 @@ struct System {
   void list_update(const double *x);
   bool in_list(int a, int b) const;
   // Debye-Hueckel charges and contact restraints (per residue min(i1, i2), sorted by the other)
+  std::vector<int> phosph_map;  // [n]: phosphorylated residues
+  std::vector<int> z_res;       // [n]: membrane zones (zim)
+  /* get_water_gamma, fix_backbone.cpp:2872-2885 */
+  double water_gamma(int i, int j, int w, int ti, int tj, int c) const
+  {
+    if (P.phosph && (phosph_map[i] || phosph_map[j])) return P.phosph_water_gamma[w][ti][tj][c];
+    return P.water_gamma[w][ti][tj][c];
+  }
+  void shake_term(int i, double *f);
+  void membrane_term(int i, double *f);
   std::vector<double> charge;
   struct Restraint { int i2; double w, r0; };
   std::vector<std::vector<Restraint>> cr_map;
@@ -402,10 +421,10 @@ void System::read_coeff(const std::string &path)
   if (!in) throw std::runtime_error("Coefficient file was not found!");
   Params &p = P;
   std::string s;
-  static const char *unsupported[] = {"[Shake]", "[Excluded]", "[Excluded_P]", "[Excluded_R6]",
-                                      "[Vector_Fragment_Memory]", "[Membrane]",
+  static const char *unsupported[] = {"[Excluded]", "[Excluded_P]", "[Excluded_R6]",
+                                      "[Vector_Fragment_Memory]",
                                       "[Fragment_Frustratometer]", "[Tertiary_Frustratometer]",
-                                      "[Nmer_Frustratometer]", "[Phosphorylation]", "[Amylometer]",
+                                      "[Nmer_Frustratometer]", "[Amylometer]",
                                       "[Selection_Temperature]", "[Monte_Carlo_Seq_Opt]", "[Optimization]",
                                       "[Burial_Optimization]", "[DebyeHuckel_Optimization]",
                                       "[Shuffler]", "[Mutate_Sequence]"};
@@ -495,6 +514,21 @@ void System::read_coeff(const std::string &path)
       // it leaves its stream failed, so the oracle asks for it
       if (!(in >> p.censoring)) throw std::runtime_error("[AMH-Go]: the frustration censoring flag is missing");
       if (p.censoring == 2) throw std::runtime_error("oracle: [AMH-Go] censoring 2 is not part of the restated path");
+    } else if (s == "[Shake]") {
+      p.shake = 1;
+      in >> p.k_shake >> p.r_sh1 >> p.r_sh2 >> p.r_sh3;
+    } else if (s == "[Membrane]") {
+      p.memb = 1;
+      in >> p.k_overall_memb >> p.k_bin >> p.memb_xo[0] >> p.memb_xo[1] >> p.memb_xo[2] >> p.memb_pore_type >>
+          p.memb_len >> p.rho0_max >> p.rho0_distor;
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 4; ++j) in >> p.g_memb[i][j];
+    } else if (s == "[Phosphorylation]") {
+      if (!p.water) throw std::runtime_error("Cannot run phosphorylation without water potential");
+      p.phosph = 1;
+      in >> p.k_hypercharge >> p.n_phosph_res;
+      if (p.n_phosph_res > 20) throw std::runtime_error("Number of phosphorylated residues may not exceed 20");
+      for (int i = 0; i < p.n_phosph_res; ++i) in >> p.phosph_res[i];
     } else if (s == "[Solvent_Barrier]") {
       p.ssb = 1;
       in >> p.k_solventb1 >> p.ssb_rmin1 >> p.ssb_rmax1 >> p.k_solventb2 >> p.ssb_rmin2 >> p.ssb_rmax2 >> p.ssb_kappa >>
@@ -596,6 +630,29 @@ void System::read_tables()
           p.water_gamma[w][j][i][0] = p.water_gamma[w][i][j][0];
           p.water_gamma[w][j][i][1] = p.water_gamma[w][i][j][1];
         }
+  }
+  if (p.phosph) {
+    // fix_backbone.cpp:643-670
+    static const int bb_four_letter_map[20] = {1, 3, 2, 2, 4, 2, 2, 1, 3, 4, 4, 3, 4, 4, 1, 1, 1, 4, 4, 4};
+    for (int w = 0; w < p.n_wells; ++w)
+      for (int i = 0; i < 20; ++i)
+        for (int j = i; j < 20; ++j)
+          for (int c = 0; c < 2; c++)
+            p.phosph_water_gamma[w][i][j][c] = p.phosph_water_gamma[w][j][i][c] = p.water_gamma[w][i][j][c];
+    for (int w = 0; w < p.n_wells; ++w)
+      for (int i = 0; i < 20; ++i)
+        for (int c = 0; c < 2; c++) {
+          double g = p.phosph_water_gamma[w][i][6][c];
+          if (bb_four_letter_map[i] == 1) g *= p.k_hypercharge;
+          else if (bb_four_letter_map[i] == 2 || bb_four_letter_map[i] == 3) g *= pow(p.k_hypercharge, 2);
+          p.phosph_water_gamma[w][i][15][c] = p.phosph_water_gamma[w][15][i][c] = g;
+        }
+    phosph_map.assign(n, 0);
+    for (int j = 0; j < p.n_phosph_res; ++j)
+      if (p.phosph_res[j] != 0) {
+        if (p.phosph_res[j] < 1 || p.phosph_res[j] > n) throw std::runtime_error("oracle: phosphorylated residue out of range");
+        phosph_map[p.phosph_res[j] - 1] = 1;
+      }
   }
   if (p.burial) {
     std::ifstream in(join(workdir, "burial_gamma.dat"));
@@ -1572,7 +1629,8 @@ void System::pair_terms(const double *x, double *f)
         t[k][0] = tanh(p.burial_kappa * (rho_w[i] - p.burial_ro_min[k]));
         t[k][1] = tanh(p.burial_kappa * (p.burial_ro_max[k] - rho_w[i]));
       }
-      int ty = type_of(i);
+      // get_burial_gamma (fix_backbone.cpp:2887-2899): glutamate's gammas for a phosphorylated residue
+      int ty = (p.phosph && phosph_map[i]) ? 6 : type_of(i);
       for (int k = 0; k < 3; k++) E[ET_BURIAL] += -0.5 * p.k_burial * p.burial_gamma[ty][k] * (t[k][0] + t[k][1]);
       bur[i] = p.burial_gamma[ty][0] * (t[0][1] * t[0][1] - t[0][0] * t[0][0]);
       bur[i] += p.burial_gamma[ty][1] * (t[1][1] * t[1][1] - t[1][0] * t[1][0]);
@@ -1601,7 +1659,7 @@ void System::pair_terms(const double *x, double *f)
         int ti = type_of(i), tj = type_of(j);
         for (int w = 0; w < p.n_wells; w++) {
           if (!p.well_flag[w]) continue;
-          double g0 = p.water_gamma[w][ti][tj][0], g1 = p.water_gamma[w][ti][tj][1];
+          double g0 = water_gamma(i, j, w, ti, tj, 0), g1 = water_gamma(i, j, w, ti, tj, 1);
           // `!fabs(g0 - g1) < delta` in the reference is true exactly when g0 != g1
           if (g0 != g1 && rsq > p.w_rmin_sq[w] && rsq < p.w_rmax_sq[w]) {
             double th, pr;
@@ -1630,7 +1688,7 @@ void System::pair_terms(const double *x, double *f)
         for (int w = 0; w < p.n_wells; w++) {
           if (!p.well_flag[w]) continue;
           if ((other || abs(j - i) >= p.contact_cutoff) && rsq > p.w_rmin_sq[w] && rsq < p.w_rmax_sq[w]) {
-            double g0 = p.water_gamma[w][ti][tj][0], g1 = p.water_gamma[w][ti][tj][1];
+            double g0 = water_gamma(i, j, w, ti, tj, 0), g1 = water_gamma(i, j, w, ti, tj, 1);
             double sg = fabs(g0 - g1) < 1e-5 ? 0.5 * (g0 + g1) : g0 + (g1 - g0) * sig_w[i] * sig_w[j];
             double th, pr;
             well_theta(r, p.w_rmin_th[w], p.w_rmax_th[w], p.water_kappa, p.well_rmin[w], p.well_rmax[w], th, pr);
@@ -2046,6 +2104,77 @@ void System::pair_extras(const double *x, double *f)
     }
 }
 
+/* compute_shake, fix_backbone.cpp:2172-2237 */
+void System::shake_term(int i, double *f)
+{
+  const Params &p = P;
+  auto bond = [&](const double *u, const double *v, int au, int av, double r0) {
+    double dx[3] = {u[0] - v[0], u[1] - v[1], u[2] - v[2]};
+    double r = sqrt(dx[0] * dx[0] + dx[1] * dx[1] + dx[2] * dx[2]);
+    double dr = r - r0;
+    double force = 2 * p.epsilon * p.k_shake * dr / r;
+    E[ET_SHAKE] += p.epsilon * p.k_shake * dr * dr;
+    for (int k = 0; k < 3; k++) {
+      f[3 * au + k] -= dx[k] * force;
+      f[3 * av + k] -= -dx[k] * force;
+    }
+  };
+  if (!last(i)) bond(&xca[3 * i], &xca[3 * (i + 1)], ca[i], ca[i + 1], p.r_sh1);
+  bond(&xca[3 * i], &xo[3 * i], ca[i], o[i], p.r_sh2);
+  if (!last(i)) bond(&xo[3 * i], &xca[3 * (i + 1)], o[i], ca[i + 1], p.r_sh3);
+}
+
+/* compute_membrane_potential, fix_backbone.cpp:6107-6235 (pore type 0) */
+void System::membrane_term(int i, double *f)
+{
+  const Params &p = P;
+  const double *xi = se[i] == 'G' ? &xca[3 * i] : &xcb[3 * i];
+  const int iatom = contact_atom(i);
+  double dx = xi[0] - p.memb_xo[0], dy = xi[1] - p.memb_xo[1], dz = xi[2] - p.memb_xo[2];
+  double memb_a = p.rho0_distor * p.rho0_max, memb_b = p.memb_len / 2;
+  double rho_actual = sqrt(dx * dx + dy * dy);
+  double rho0 = (p.rho0_max - memb_a) + ((memb_a) / (p.memb_len)) * (dz + memb_b);
+  const double kb = p.k_bin;
+  double s_per = 0.5 * (1 + tanh(kb * (dz - memb_b)));
+  double s_mem = 0.5 * ((tanh(kb * (dz + memb_b))) + (tanh(kb * (memb_b - dz))));
+  double s_cyt = 0.5 * (1 + tanh(kb * (-memb_b - dz)));
+  double s_por = 0.5 * (1 - (tanh(kb * (rho_actual - rho0))));
+  double s_nopor = (1 - s_por);
+  const double(*g)[4] = p.g_memb;
+  double V = 0.0;
+  if (z_res[i] == 1) V = (-g[0][0] * s_per) + (-g[0][1] * s_cyt) + (g[0][2] * s_mem * s_nopor) + (-g[0][3] * s_mem * s_por);
+  else if (z_res[i] == 2) V = (g[1][0] * s_per) + (g[1][1] * s_cyt) + (-g[1][2] * s_mem * s_nopor) + (g[1][3] * s_mem * s_por);
+  else V = (-g[2][0] * s_per) + (-g[2][1] * s_cyt) + (g[2][2] * s_mem * s_nopor) + (-g[2][3] * s_mem * s_por);
+  E[ET_MEMB] += p.epsilon * p.k_overall_memb * V;
+  double dz_per = 0.5 * kb * (1 - pow((tanh(kb * (dz - memb_b))), 2));
+  double dz_mem = -0.5 * kb * pow(tanh(kb * (dz + memb_b)), 2) + 0.5 * kb * pow(tanh(kb * (memb_b - dz)), 2);
+  double dz_cyt = -0.5 * kb * (1 - pow((tanh(kb * (-memb_b - dz))), 2));
+  double dr1_dz = ((memb_a) / (p.memb_len));
+  double dz_s_por = 0.5 * kb * (1 - pow(tanh(kb * (rho_actual - rho0)), 2)) * dr1_dz;
+  double dx_s_por = ((-0.5 * kb * dx) / rho_actual) * (1 - pow(tanh(kb * (rho_actual - rho0)), 2));
+  double dy_s_por = ((-0.5 * kb * dy) / rho_actual) * (1 - pow(tanh(kb * (rho_actual - rho0)), 2));
+  double dx_s_nopor = -dx_s_por, dy_s_nopor = -dy_s_por, dz_s_nopor = -dz_s_por;
+  double dz_s_por_smem = s_mem * dz_s_por + dz_mem * s_por;
+  double dz_s_nopor_smem = s_mem * dz_s_nopor + dz_mem * s_nopor;
+  double dV_dx, dV_dy, dV_dz;
+  if (z_res[i] == 1) {
+    dV_dx = g[0][2] * s_mem * dx_s_nopor + (-g[0][3]) * s_mem * dx_s_por;
+    dV_dy = g[0][2] * s_mem * dy_s_nopor + (-g[0][3]) * s_mem * dy_s_por;
+    dV_dz = -g[0][0] * dz_per + (-g[0][1]) * dz_cyt + g[0][2] * dz_s_nopor_smem + (-g[0][3]) * dz_s_por_smem;
+  } else if (z_res[i] == 2) {
+    dV_dx = -g[1][2] * s_mem * dx_s_nopor + g[1][3] * s_mem * dx_s_por;
+    dV_dy = -g[1][2] * s_mem * dy_s_nopor + g[1][3] * s_mem * dy_s_por;
+    dV_dz = g[1][0] * dz_per + g[1][1] * dz_cyt + (-g[1][2]) * dz_s_nopor_smem + g[1][3] * dz_s_por_smem;
+  } else {
+    dV_dx = g[2][2] * s_mem * dx_s_nopor + (-g[2][3]) * s_mem * dx_s_por;
+    dV_dy = g[2][2] * s_mem * dy_s_nopor + (-g[2][3]) * s_mem * dy_s_por;
+    dV_dz = -g[2][0] * dz_per + (-g[2][1]) * dz_cyt + g[2][2] * dz_s_nopor_smem + (-g[2][3]) * dz_s_por_smem;
+  }
+  f[3 * iatom + 0] += -p.epsilon * p.k_overall_memb * dV_dx;
+  f[3 * iatom + 1] += -p.epsilon * p.k_overall_memb * dV_dy;
+  f[3 * iatom + 2] += -p.epsilon * p.k_overall_memb * dV_dz;
+}
+
 /* compute_backbone, fix_backbone.cpp:7047-7673, then vexcluded and bonds */
 void System::compute(const double *x, double *f)
 {
@@ -2058,6 +2187,8 @@ void System::compute(const double *x, double *f)
     if (p.chain) chain_term(i, f);
     if (!first(i) && !last(i) && p.chi && se[i] != 'G') chi_term(i, f);
     if (!first(i) && !last(i) && p.rama && se[i] != 'G') rama_term(i, f);
+    if (p.shake) shake_term(i, f);
+    if (p.memb) membrane_term(i, f);
     if (p.fm) fm_term(i, f);
     if (p.fm_tb) tb_term(i, f);
   }
@@ -2091,6 +2222,17 @@ void *oracle_create(const char *workdir, const char *data_file, const char *coef
     if (S->P.fm || S->P.fm_tb) S->read_mems();
     if (S->P.fm_tb) S->build_tb();
     if (S->P.ssb || S->P.huckel || S->P.cont_rest) S->read_pair_extras();
+    if (S->P.memb) {
+      // zim (fix_backbone.cpp:611-619)
+      std::ifstream in(join(S->workdir, "zim"));
+      if (!in) throw std::runtime_error("File zim doesn't exist");
+      S->z_res.assign(S->n, 0);
+      for (int i = 0; i < S->n; ++i) {
+        in >> S->z_res[i];
+        if (in.eof()) throw std::runtime_error("Membrane potential parameter file format error");
+        if (S->z_res[i] < 1 || S->z_res[i] > 3) throw std::runtime_error("oracle: zim values must be 1, 2 or 3");
+      }
+    }
     if (S->lists_used()) S->plc = pair_list_cut(S->P);
     if (S->P.amhgo) S->read_amh_go();
     S->pair_setup(pair_style, pair_coeffs ? pair_coeffs : "");

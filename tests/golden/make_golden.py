@@ -28,6 +28,11 @@ against the LAMMPS-API shim (``make -C oracle ref``) and run on four inputs:
                and neigh_modify delay 3 every 2: the barrier and Debye-Hueckel
                sum over the CA pairs of the fix's half list as last built;
 * ``sheetx``  -- ``sheet`` (three chains) with the same three sections;
+* ``c0s``     -- ``c0`` with [Shake], [Membrane] (zones from a seeded zim)
+               and [Phosphorylation] of two serines and one other residue
+               (synth.residue_terms_text, write_zim);
+* ``sheets``  -- ``sheet`` with the same sections, its serines phosphorylated
+               (water contacts of phosphorylated residues);
 * ``c0go``    -- ``c0`` with [AMH-Go] (k 200, p 2, rc 10 A) towards a native
                structure 0.6 times as large as the starting chain
                (synth.write_native_gro), run with neighbor skin 0.6 A and
@@ -87,6 +92,18 @@ def write_case(name: str, outdir: str) -> dict:
         synth.write_charges(sys_, os.path.join(outdir, "charge_on_residues.dat"))
         synth.write_contact_restraints(sys_, os.path.join(outdir, "contact_restraints.dat"))
         return files
+    if name in ("c0s", "sheets"):
+        sys_ = synth.config_system(0) if name == "c0s" else synth.sheet_system()
+        files = synth.write_system(sys_, outdir)
+        seq = "".join(ch.seq for ch in sys_.chains)
+        if name == "c0s":
+            phosph = [k + 1 for k, a in enumerate(seq) if a == "S"][:2] + [next(k + 1 for k, a in enumerate(seq) if a not in "SG")]
+        else:
+            phosph = ([k + 1 for k, a in enumerate(seq) if a == "S"] + [k + 1 for k, a in enumerate(seq) if a == "T"])[:20]
+        with open(os.path.join(outdir, files["coeff"]), "w") as fh:
+            fh.write(synth.coeff_text() + synth.residue_terms_text(sys_, phosph))
+        synth.write_zim(sys_, os.path.join(outdir, "zim"))
+        return files
     if name == "c0go":
         sys_ = synth.config_system(0)
         files = synth.write_system(sys_, outdir)
@@ -126,7 +143,7 @@ def write_case(name: str, outdir: str) -> dict:
     raise KeyError(name)
 
 
-CASES = ["c0", "sheet", "r1r69", "r1r69tb", "r1r69go", "r1r69go2", "c0go", "c0x", "sheetx"]
+CASES = ["c0", "sheet", "r1r69", "r1r69tb", "r1r69go", "r1r69go2", "c0go", "c0x", "sheetx", "c0s", "sheets"]
 # LAMMPS neighbor skin and neigh_modify delay / every / check of a case's runs
 # (the others: 2.0, 0, 1, yes -- LAMMPS's defaults)
 NEIGH = {"c0go": (0.6, 3, 2, 1), "c0x": (0.6, 3, 2, 1)}
