@@ -174,6 +174,8 @@ template <typename R> class Engine : public EngineBase {
   DBuf<int> cr_start, cr_j;        // contact restraints
   DBuf<double> cr_w, cr_r0;
   DBuf<int> zim;                   // membrane zones
+  DBuf<int> vfm_start, vfm_j;      // vector fragment memory records
+  DBuf<double> vfm_angle;
   int efix_slots = 5;
   int fm_groups = 0, fm_dsplit = 1;
   DBuf<double> thermo_rows;
@@ -292,6 +294,9 @@ template <typename R> class Engine : public EngineBase {
     a.cr_r0 = cr_r0.p;
     a.efix_slots = efix_slots;
     a.zim = zim.p;
+    a.vfm_start = vfm_start.p;
+    a.vfm_j = vfm_j.p;
+    a.vfm_angle = vfm_angle.p;
     a.groups = groups;
     a.step = dstep.p;
     a.res_sys = res_sys.p;
@@ -417,6 +422,13 @@ template <typename R> class Engine : public EngineBase {
       cr_r0.upload(in.cr.r0.empty() ? std::vector<double>{0.0} : in.cr.r0, s0);
     }
     efix_slots = (in.ff.p.terms & (T_SSB | T_DH | T_CONTREST)) ? 8 : 5;
+    if (in.ff.p.terms & T_VFM) {
+      std::vector<int> st(in.vfm.start);
+      st.resize((size_t) nn + 1, st.empty() ? 0 : st.back());
+      vfm_start.upload(st, s0);
+      vfm_j.upload(in.vfm.j.empty() ? std::vector<int>{0} : in.vfm.j, s0);
+      vfm_angle.upload(in.vfm.angle.empty() ? std::vector<double>{0.0} : in.vfm.angle, s0);
+    }
     if (in.ff.p.terms & T_MEMB) {
       std::vector<int> z(in.zim);
       z.resize((size_t) nn, 1);
@@ -579,7 +591,7 @@ template <typename R> class Engine : public EngineBase {
     const bool fmt = (a.groups & dev::G_FIX) && (p.terms & T_FM_TABLE);
     const bool go = (a.groups & dev::G_FIX) && (p.terms & T_AMHGO);
     const bool px = (a.groups & dev::G_FIX) && (p.terms & (T_SSB | T_DH | T_CONTREST));
-    const bool rx = (a.groups & dev::G_FIX) && (p.terms & (T_SHAKE | T_MEMB));
+    const bool rx = (a.groups & dev::G_FIX) && (p.terms & (T_SHAKE | T_MEMB | T_VFM));
     // the emulated lists' decision for this step, before anything reads it
     if (lists_emulated())
       dev::k_list_decide<<<(n_sys() + 127) / 128, 128, 0, s0>>>(nl.p, n_sys(), lst_ago.p, lst_over.p, lst_build.p);
@@ -618,7 +630,7 @@ template <typename R> class Engine : public EngineBase {
     if (!(groups & dev::G_FIX) || !(in.ff.p.terms & T_AMHGO))
       CK(cudaMemsetAsync(e_res.p + (size_t) E_AMHGO * nn, 0, sizeof(double) * nn, s0));
     if (!(groups & dev::G_FIX))
-      for (int t : {E_SHAKE, E_MEMB}) CK(cudaMemsetAsync(e_res.p + (size_t) t * nn, 0, sizeof(double) * nn, s0));
+      for (int t : {E_SHAKE, E_MEMB, E_VFRAGMEM}) CK(cudaMemsetAsync(e_res.p + (size_t) t * nn, 0, sizeof(double) * nn, s0));
   }
 
   // energy sums of replicas [rep0, rep0 + count) (all of them by default)
@@ -866,7 +878,7 @@ template <typename R> class Engine : public EngineBase {
                        (a.groups & dev::G_FIX) && (in.ff.p.terms & T_AMHGO) ? 1 : 0,
                        (a.groups & dev::G_FIX) && (in.ff.p.terms & (T_SSB | T_DH | T_CONTREST)) ? 1 : 0,
                        lists_emulated() ? n_sys() : 0,
-                       (a.groups & dev::G_FIX) && (in.ff.p.terms & (T_SHAKE | T_MEMB)) ? 1 : 0};
+                       (a.groups & dev::G_FIX) && (in.ff.p.terms & (T_SHAKE | T_MEMB | T_VFM)) ? 1 : 0};
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(ps_grid_now);
     cfg.blockDim = dim3(dev::kStepThreads);
@@ -1117,7 +1129,7 @@ template <typename R> class Engine : public EngineBase {
             if (p.terms & T_FM_TABLE) dev::k_fm_table<R><<<fm_table_blocks(), tb, 0, s0>>>(a, p);
             if (p.terms & T_AMHGO) dev::k_amh_go<R><<<nb, tb, 0, s0>>>(a, p);
             if (p.terms & (T_SSB | T_DH | T_CONTREST)) dev::k_pair_extra<R><<<pair_blocks, tb, 0, s0>>>(a, p);
-            if (p.terms & (T_SHAKE | T_MEMB)) dev::k_residue_extra<R><<<nb, tb, 0, s0>>>(a, p);
+            if (p.terms & (T_SHAKE | T_MEMB | T_VFM)) dev::k_residue_extra<R><<<nb, tb, 0, s0>>>(a, p);
             break;
           case 9: dev::k_finish<R><<<nb, tb, 0, s0>>>(a, d_integ.p, g1.p, g2.p, ftot.p, x.p); break;
         }
@@ -1878,7 +1890,7 @@ template <typename R> class Engine : public EngineBase {
     add(bond_r0), add(fm_soff), add(fm_slen), add(fm_rf), add(fm_coef), add(tb_data), add(tb_present);
     add(go_start), add(go_partner), add(go_rnat), add(go_gamma), add(go_sig_sq), add(go_norm);
     add(go_in), add(lst_x0), add(lst_ago), add(lst_over), add(lst_build), add(charge), add(cr_start), add(cr_j),
-        add(cr_w), add(cr_r0), add(zim);
+        add(cr_w), add(cr_r0), add(zim), add(vfm_start), add(vfm_j), add(vfm_angle);
     add(thermo_rows), add(res_sys), add(sys_begin);
     add(sys_end), add(sys_seed), add(slot_run), add(d_integ);
     return b;

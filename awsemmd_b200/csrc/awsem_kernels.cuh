@@ -124,6 +124,8 @@ template <typename R> struct StepArgs {
   const double *cr_w, *cr_r0;
   int efix_slots;                // fixed-point energy slots in use (5, or 8 with the pair terms above)
   const int *zim;                // [n]: membrane zone (1, 2, 3) of the residue
+  const int *vfm_start, *vfm_j;  // vector fragment memory records of residue i (i < j)
+  const double *vfm_angle;
   int groups;       // AWSEM_TERMS_* bits: 1 fix backbone, 2 pair vexcluded, 4 bonds
   long long *step;   // device step counter (advanced by k_nl_decide)
   // replicas: residue -> replica, replica residue ranges, Langevin seeds
@@ -1278,11 +1280,57 @@ template <typename R> __device__ __forceinline__ void residue_extra_one(const St
   }
 }
 
+// Vector fragment memory (compute_vector_fragment_memory_potential,
+// fix_backbone.cpp:3994-4077) of residue i: per record (partner j, the
+// memory's CA->CB angle), V = -eps k exp(-(theta - theta_mem)^2 / 2 sigma^2)
+// with theta the angle between the CA->CB vectors of i and j.
+template <typename R> __device__ __forceinline__ void vfm_one(const StepArgs<R> &a, const FFParams &p, int i)
+{
+  const DevSys<R> &s = a.s;
+  const int c0 = a.vfm_start[i], c1 = a.vfm_start[i + 1];
+  double E = 0.0;
+  if (c0 < c1) {
+    const V3<double> cai = bead(s, i, B_CA), cbi = bead(s, i, B_CB);
+    const double vi[3] = {cbi.x - cai.x, cbi.y - cai.y, cbi.z - cai.z};
+    const double vmsqi = vi[0] * vi[0] + vi[1] * vi[1] + vi[2] * vi[2], vmi = sqrt(vmsqi);
+    const double ek = p.epsilon * p.k_vfm;
+    long long fi[3] = {0, 0, 0};
+    for (int c = c0; c < c1; c++) {
+      const int j = a.vfm_j[c];
+      const V3<double> caj = bead(s, j, B_CA), cbj = bead(s, j, B_CB);
+      const double vj[3] = {cbj.x - caj.x, cbj.y - caj.y, cbj.z - caj.z};
+      const double vmsqj = vj[0] * vj[0] + vj[1] * vj[1] + vj[2] * vj[2], vmj = sqrt(vmsqj);
+      const double vp = vi[0] * vj[0] + vi[1] * vj[1] + vi[2] * vj[2];
+      const double vpn = vp / (vmi * vmj);
+      const double dg = acos(vpn) - a.vfm_angle[c];
+      const double V = -ek * exp(-dg * dg / (2 * p.vfm_sigma_sq));
+      E += V;
+      const double force = -V * dg / (p.vfm_sigma_sq * vmi * vmj * sqrt(1 - vpn * vpn));
+      long long fj[3], mfj[3];
+      for (int k = 0; k < 3; k++) {
+        const long long v = fix_force(force * (vj[k] - vi[k] * vp / vmsqi));
+        fi[k] += v;
+        fj[k] = fix_force(force * (vi[k] - vj[k] * vp / vmsqj));
+        mfj[k] = -fj[k];
+      }
+      scatter_fix(s, j, B_CA, mfj);
+      scatter_fix(s, j, B_CB, fj);
+    }
+    const long long mfi[3] = {-fi[0], -fi[1], -fi[2]};
+    scatter_fix(s, i, B_CA, mfi);
+    scatter_fix(s, i, B_CB, fi);
+  }
+  a.e_res[(size_t) E_VFRAGMEM * s.n_res + i] = E;
+}
+
 template <typename R> __device__ __forceinline__ void residue_extra_pass(const StepArgs<R> &a, const FFParams &p, Span sp)
 {
   if (!(a.groups & G_FIX)) return;
   for (int r = sp.t; r < a.n_run; r += sp.nthr)
-    if (a.res_sys[r] >= 0) residue_extra_one(a, p, r);
+    if (a.res_sys[r] >= 0) {
+      if (p.terms & (T_SHAKE | T_MEMB)) residue_extra_one(a, p, r);
+      if (p.terms & T_VFM) vfm_one(a, p, r);
+    }
 }
 
 template <typename R> __global__ void k_residue_extra(StepArgs<R> a, FFParams p) { residue_extra_pass(a, p, grid_span()); }

@@ -83,7 +83,7 @@ void read_coeff_file(const std::string &path, ForceField &ff)
   const int i_rp = 6;  // first proline Ramachandran well
   double k_rama = 0.0, k_water = 0.0;
   static const char *outside[] = {
-      "[Excluded]", "[Excluded_P]", "[Excluded_R6]", "[Vector_Fragment_Memory]",
+      "[Excluded]", "[Excluded_P]", "[Excluded_R6]",
       "[Fragment_Frustratometer]", "[Tertiary_Frustratometer]", "[Nmer_Frustratometer]",
       "[Amylometer]", "[Selection_Temperature]", "[Monte_Carlo_Seq_Opt]", "[Optimization]",
       "[Burial_Optimization]", "[DebyeHuckel_Optimization]", "[Shuffler]", "[Mutate_Sequence]"};
@@ -172,6 +172,12 @@ void read_coeff_file(const std::string &path, ForceField &ff)
       }
       if (ff.amh_go_censor == 2)
         fail("AMH-Go: frustration censoring 2 (native distances from go_rnative*.dat) is not supported");
+    } else if (s == "[Vector_Fragment_Memory]") {
+      // fix_backbone.cpp:328-333
+      p.terms |= T_VFM;
+      double sigma;
+      in >> p.k_vfm >> sigma;
+      p.vfm_sigma_sq = sigma * sigma;
     } else if (s == "[Shake]") {
       // fix_backbone.cpp:180-183
       p.terms |= T_SHAKE;
@@ -901,6 +907,47 @@ void build_fm_table_tb(const ForceField &ff, const Topology &top, const GammaTab
   }
 }
 
+// compute_vector_fragment_memory_potential's pairs (fix_backbone.cpp:
+// 3994-4077): for residue i, each memory covering it (the fragment-memory
+// map, :765-790, memories in file order), partners j from i + min_sep to the
+// memory's end (and i + max_sep), neither residue nor its memory residue a
+// glycine; the memory's angle between the CA->CB vectors of i and j
+// (Fragment_Memory::VM, fragment_memory.cpp:240-243)
+void build_vfm(const Topology &top, const GammaTable &G, const std::vector<Memory> &mems, VfmRecords &out)
+{
+  const int n = top.n_res, min_sep = G.min_sep(), max_sep = G.max_sep();
+  std::vector<std::vector<std::pair<int, double>>> per(n);
+  for (const Memory &m : mems) {
+    if (m.pos + m.len > n) fail("Fragment_Memory: Incorrectly defined memory fragment");
+    auto vec = [&](int r, double *v) {
+      for (int c = 0; c < 3; c++) v[c] = m.xcb[3 * r + c] - m.xca[3 * r + c];
+    };
+    for (int i = m.pos; i < m.pos + m.len - min_sep; i++) {
+      int je = m.pos + m.len - 1;
+      if (max_sep != -1) je = std::min(je, i + max_sep);
+      for (int j = i + min_sep; j <= je; j++) {
+        if (top.res_chain[i] != top.res_chain[j])
+          fail("Fragment Memory: Interaction between residues of different chains");
+        if (top.seq[i] == 'G' || top.seq[j] == 'G' || m.se[i - m.pos] == 'G' || m.se[j - m.pos] == 'G') continue;
+        double u[3], v[3];
+        vec(i - m.pos, u);
+        vec(j - m.pos, v);
+        const double nu = sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]), nv = sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+        per[i].push_back({j, acos((u[0] * v[0] + u[1] * v[1] + u[2] * v[2]) / (nu * nv))});
+      }
+    }
+  }
+  out = VfmRecords();
+  out.start.assign(n + 1, 0);
+  for (int i = 0; i < n; i++) {
+    out.start[i + 1] = out.start[i] + (int) per[i].size();
+    for (auto &e : per[i]) {
+      out.j.push_back(e.first);
+      out.angle.push_back(e.second);
+    }
+  }
+}
+
 // zim (fix_backbone.cpp:611-619): the membrane zone (1, 2 or 3) of each
 // residue; the reference leaves the potential undefined for other values
 void read_zim(const std::string &path, int n_res, std::vector<int> &z)
@@ -1178,6 +1225,7 @@ void load_system_arrays(const SharedForceField &sf, const ReplicaArrays &ra, Sys
       build_fm_table_tb(S.ff, t, S.gamma, S.mems, "", S.tb);
       S.ff.p.tb_nbrs = S.tb.nbrs;
     }
+    if (S.ff.p.terms & T_VFM) build_vfm(t, S.gamma, S.mems, S.vfm);
     S.mems.clear();
     S.mems.shrink_to_fit();
   }
@@ -1320,6 +1368,17 @@ void assemble_batch(const std::vector<const SystemInput *> &reps, Batch &B)
     for (auto *r : reps) B.charge.insert(B.charge.end(), r->charge.begin(), r->charge.end());
   if (B.ff.p.terms & T_MEMB)
     for (auto *r : reps) B.zim.insert(B.zim.end(), r->zim.begin(), r->zim.end());
+  if (B.ff.p.terms & T_VFM) {
+    B.vfm.start.push_back(0);
+    int res_off = 0;
+    for (auto *r : reps) {
+      const int base = (int) B.vfm.j.size();
+      for (size_t k = 1; k < r->vfm.start.size(); k++) B.vfm.start.push_back(base + r->vfm.start[k]);
+      for (int q : r->vfm.j) B.vfm.j.push_back(q + res_off);
+      B.vfm.angle.insert(B.vfm.angle.end(), r->vfm.angle.begin(), r->vfm.angle.end());
+      res_off += r->top.n_res;
+    }
+  }
   if (B.ff.p.terms & T_CONTREST) {
     B.cr.start.push_back(0);
     int res_off = 0;
@@ -1472,7 +1531,13 @@ void load_system_atoms(const std::string &dir, const std::string &coeff_file, co
       build_fm_table_tb(S.ff, S.top, S.gamma, S.mems, dir, S.tb);
       S.ff.p.tb_nbrs = S.tb.nbrs;
     }
+    if (S.ff.p.terms & T_VFM) {
+      if (tb_from_file) fail("Vector_Fragment_Memory needs the memories (the fragment-memory tables came from files)");
+      build_vfm(S.top, S.gamma, S.mems, S.vfm);
+    }
   }
+  if ((S.ff.p.terms & T_VFM) && !(S.ff.p.terms & (T_FM | T_FM_TABLE)))
+    fail("Vector_Fragment_Memory needs the memories of [Fragment_Memory] or [Fragment_Memory_Table]");
   if (S.ff.p.terms & T_DH) read_charges(path_in(dir, "charge_on_residues.dat"), S.top.n_res, S.charge);
   if (S.ff.p.terms & T_MEMB) read_zim(path_in(dir, "zim"), S.top.n_res, S.zim);
   if (S.ff.p.terms & T_PHOSPH) flag_phosphorylated(S.ff.p, S.top);

@@ -23,7 +23,7 @@ enum TermFlag : uint32_t {
   T_CHAIN = 1u << 0, T_CHI = 1u << 1, T_RAMA = 1u << 2, T_RAMA_P = 1u << 3, T_SSW = 1u << 4,
   T_DSSP = 1u << 5, T_PAP = 1u << 6, T_WATER = 1u << 7, T_BURIAL = 1u << 8, T_HELIX = 1u << 9,
   T_FM = 1u << 10, T_FM_TABLE = 1u << 11, T_AMHGO = 1u << 12, T_SSB = 1u << 13, T_DH = 1u << 14,
-  T_CONTREST = 1u << 15, T_SHAKE = 1u << 16, T_MEMB = 1u << 17, T_PHOSPH = 1u << 18
+  T_CONTREST = 1u << 15, T_SHAKE = 1u << 16, T_MEMB = 1u << 17, T_PHOSPH = 1u << 18, T_VFM = 1u << 19
 };
 
 // Residue flags
@@ -80,6 +80,8 @@ struct FFParams {
   // [Phosphorylation] (:413-421): hypercharge factor; the residues are flagged R_PHOSPH
   double k_hypercharge;
   int n_phosph_res, phosph_res[20];
+  // [Vector_Fragment_Memory] (:328-333): strength and angle width (rad)
+  double k_vfm, vfm_sigma_sq;
 };
 
 struct ForceField {
@@ -182,6 +184,13 @@ struct ContactRestraints {
   std::vector<double> w, r0;
 };
 
+// Vector fragment memory records of residue i: [start[i], start[i+1]), each
+// a partner j and the memory's CA-CB angle between i and j (radians)
+struct VfmRecords {
+  std::vector<int> start, j;
+  std::vector<double> angle;
+};
+
 struct SystemInput {
   ForceField ff;
   Topology top;
@@ -193,6 +202,7 @@ struct SystemInput {
   std::vector<double> charge;  // [n_res] Debye-Hueckel charges (charge_on_residues.dat)
   ContactRestraints cr;
   std::vector<int> zim;        // [n_res] membrane zone of each residue (file zim: 1, 2 or 3)
+  VfmRecords vfm;
   std::vector<double> x, v;  // internal order [n_atoms*3]
 };
 
@@ -250,6 +260,7 @@ struct Batch {
   std::vector<double> charge;  // concatenated Debye-Hueckel charges
   ContactRestraints cr;        // concatenated contact restraints (residues offset)
   std::vector<int> zim;        // concatenated membrane zones
+  VfmRecords vfm;              // concatenated vector fragment memory records (residues offset)
   std::vector<double> x, v;
   std::vector<int> res_sys;              // residue -> replica
   std::vector<int> sys_res_begin, sys_res_end;    // [n_sys]

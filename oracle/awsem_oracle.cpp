@@ -143,6 +143,9 @@ struct Params {
   double k_hypercharge = 0;
   int n_phosph_res = 0, phosph_res[20] = {0};
   double phosph_water_gamma[5][20][20][2];
+  // [Vector_Fragment_Memory] (:328-333)
+  bool vfm = 0;
+  double k_vec_frag_mem = 0, vfm_sigma = 0, vfm_sigma_sq = 0;
   // [Fragment_Memory_Table] (fix_backbone.cpp:310-321)
   double tb_rmin = 0, tb_rmax = 0, tb_dr = 0, tb_width = 0;
   int tb_size = 0, tb_use_file = 0;
@@ -282,6 +285,7 @@ struct Memory {
   double weight;
   std::string se;
   std::vector<double> rf0, rf1;  // [len*len]: CA-CA (i<j) / CB-CB (i>j); CA_i-CB_j
+  std::vector<double> vmf;       // [len*len]: angle between the CA->CB vectors of i and j (VM)
 
   double R(const double *a, const double *b) const
   {
@@ -347,6 +351,7 @@ struct System {
     return P.water_gamma[w][ti][tj][c];
   }
   void shake_term(int i, double *f);
+  void vfm_term(int i, double *f);
   void membrane_term(int i, double *f);
   std::vector<double> charge;
   struct Restraint { int i2; double w, r0; };
@@ -422,7 +427,6 @@ void System::read_coeff(const std::string &path)
   Params &p = P;
   std::string s;
   static const char *unsupported[] = {"[Excluded]", "[Excluded_P]", "[Excluded_R6]",
-                                      "[Vector_Fragment_Memory]",
                                       "[Fragment_Frustratometer]", "[Tertiary_Frustratometer]",
                                       "[Nmer_Frustratometer]", "[Amylometer]",
                                       "[Selection_Temperature]", "[Monte_Carlo_Seq_Opt]", "[Optimization]",
@@ -514,6 +518,10 @@ void System::read_coeff(const std::string &path)
       // it leaves its stream failed, so the oracle asks for it
       if (!(in >> p.censoring)) throw std::runtime_error("[AMH-Go]: the frustration censoring flag is missing");
       if (p.censoring == 2) throw std::runtime_error("oracle: [AMH-Go] censoring 2 is not part of the restated path");
+    } else if (s == "[Vector_Fragment_Memory]") {
+      p.vfm = 1;
+      in >> p.k_vec_frag_mem >> p.vfm_sigma;
+      p.vfm_sigma_sq = p.vfm_sigma * p.vfm_sigma;
     } else if (s == "[Shake]") {
       p.shake = 1;
       in >> p.k_shake >> p.r_sh1 >> p.r_sh2 >> p.r_sh3;
@@ -803,6 +811,14 @@ void load_gro(const std::string &path, int fpos, Memory &m, const std::string &o
     for (int j = 0; j < m.len; j++) {
       m.rf0[i * m.len + j] = i < j ? m.R(&xa[3 * i], &xa[3 * j]) : (i > j ? m.R(&xb[3 * i], &xb[3 * j]) : 0.0);
       m.rf1[i * m.len + j] = m.R(&xa[3 * i], &xb[3 * j]);
+    }
+  // Fragment_Memory::VM (fragment_memory.cpp:240-243)
+  m.vmf.assign((size_t) m.len * m.len, 0.0);
+  for (int i = 0; i < m.len; i++)
+    for (int j = 0; j < m.len; j++) {
+      const double *a = &xa[3 * i], *b = &xb[3 * i], *c = &xa[3 * j], *d = &xb[3 * j];
+      m.vmf[i * m.len + j] = acos(((b[0] - a[0]) * (d[0] - c[0]) + (b[1] - a[1]) * (d[1] - c[1]) + (b[2] - a[2]) * (d[2] - c[2])) /
+                                  (m.R(a, b) * m.R(c, d)));
     }
 }
 
@@ -2175,6 +2191,47 @@ void System::membrane_term(int i, double *f)
   f[3 * iatom + 2] += -p.epsilon * p.k_overall_memb * dV_dz;
 }
 
+/* compute_vector_fragment_memory_potential, fix_backbone.cpp:3994-4077 */
+void System::vfm_term(int i, double *f)
+{
+  const Params &p = P;
+  for (int k : fm_map[i]) {
+    const Memory &m = mems[k];
+    const double epsilon_k_weight = p.epsilon * p.k_vec_frag_mem;
+    int js = i + G.min_sep(), je = m.pos + m.len - 1;
+    if (G.max_sep() != -1) je = std::min(je, i + G.max_sep());
+    if (je >= n) throw std::runtime_error("Missing residues in memory potential");
+    for (int j = js; j <= je; ++j) {
+      if (chain_of[i] != chain_of[j])
+        throw std::runtime_error("Fragment Memory: Interaction between residues of different chains");
+      if (se[i] == 'G' || se[j] == 'G' || m.se[i - m.pos] == 'G' || m.se[j - m.pos] == 'G') continue;
+      double vi[3], vj[3];
+      for (int c = 0; c < 3; c++) {
+        vi[c] = xcb[3 * i + c] - xca[3 * i + c];
+        vj[c] = xcb[3 * j + c] - xca[3 * j + c];
+      }
+      double vmsqi = vi[0] * vi[0] + vi[1] * vi[1] + vi[2] * vi[2];
+      double vmsqj = vj[0] * vj[0] + vj[1] * vj[1] + vj[2] * vj[2];
+      double vmi = sqrt(vmsqi), vmj = sqrt(vmsqj);
+      double vp = vi[0] * vj[0] + vi[1] * vj[1] + vi[2] * vj[2];
+      double vpn = vp / (vmi * vmj);
+      double gc = acos(vpn);
+      double gf = m.vmf[(i - m.pos) * m.len + (j - m.pos)];
+      double dg = gc - gf;
+      double V = -epsilon_k_weight * exp(-dg * dg / (2 * p.vfm_sigma_sq));
+      E[ET_VFRAGMEM] += V;
+      double force = -V * dg / (p.vfm_sigma_sq * vmi * vmj * sqrt(1 - vpn * vpn));
+      for (int c = 0; c < 3; c++) {
+        double fi = force * (vj[c] - vi[c] * vp / vmsqi), fj = force * (vi[c] - vj[c] * vp / vmsqj);
+        f[3 * ca[i] + c] += -fi;
+        f[3 * cb[i] + c] += fi;
+        f[3 * ca[j] + c] += -fj;
+        f[3 * cb[j] + c] += fj;
+      }
+    }
+  }
+}
+
 /* compute_backbone, fix_backbone.cpp:7047-7673, then vexcluded and bonds */
 void System::compute(const double *x, double *f)
 {
@@ -2189,6 +2246,7 @@ void System::compute(const double *x, double *f)
     if (!first(i) && !last(i) && p.rama && se[i] != 'G') rama_term(i, f);
     if (p.shake) shake_term(i, f);
     if (p.memb) membrane_term(i, f);
+    if (p.vfm) vfm_term(i, f);
     if (p.fm) fm_term(i, f);
     if (p.fm_tb) tb_term(i, f);
   }
@@ -2219,6 +2277,8 @@ void *oracle_create(const char *workdir, const char *data_file, const char *coef
     S->read_data(join(S->workdir, data_file));
     build_residues(*S);
     S->read_tables();
+    if (S->P.vfm && !S->P.fm && !S->P.fm_tb)
+      throw std::runtime_error("oracle: Vector_Fragment_Memory needs the fragment-memory memories");
     if (S->P.fm || S->P.fm_tb) S->read_mems();
     if (S->P.fm_tb) S->build_tb();
     if (S->P.ssb || S->P.huckel || S->P.cont_rest) S->read_pair_extras();

@@ -33,6 +33,8 @@ against the LAMMPS-API shim (``make -C oracle ref``) and run on four inputs:
                (synth.residue_terms_text, write_zim);
 * ``sheets``  -- ``sheet`` with the same sections, its serines phosphorylated
                (water contacts of phosphorylated residues);
+* ``c0v``     -- ``c0`` with [Vector_Fragment_Memory] (k 1, sigma 0.3 rad)
+               over its fragment memories;
 * ``c0go``    -- ``c0`` with [AMH-Go] (k 200, p 2, rc 10 A) towards a native
                structure 0.6 times as large as the starting chain
                (synth.write_native_gro), run with neighbor skin 0.6 A and
@@ -104,6 +106,11 @@ def write_case(name: str, outdir: str) -> dict:
             fh.write(synth.coeff_text() + synth.residue_terms_text(sys_, phosph))
         synth.write_zim(sys_, os.path.join(outdir, "zim"))
         return files
+    if name == "c0v":
+        files = synth.write_system(synth.config_system(0), outdir)
+        with open(os.path.join(outdir, files["coeff"]), "a") as fh:
+            fh.write("\n[Vector_Fragment_Memory]\n1.0\n0.3\n")
+        return files
     if name == "c0go":
         sys_ = synth.config_system(0)
         files = synth.write_system(sys_, outdir)
@@ -143,7 +150,7 @@ def write_case(name: str, outdir: str) -> dict:
     raise KeyError(name)
 
 
-CASES = ["c0", "sheet", "r1r69", "r1r69tb", "r1r69go", "r1r69go2", "c0go", "c0x", "sheetx", "c0s", "sheets"]
+CASES = ["c0", "sheet", "r1r69", "r1r69tb", "r1r69go", "r1r69go2", "c0go", "c0x", "sheetx", "c0s", "sheets", "c0v"]
 # LAMMPS neighbor skin and neigh_modify delay / every / check of a case's runs
 # (the others: 2.0, 0, 1, yes -- LAMMPS's defaults)
 NEIGH = {"c0go": (0.6, 3, 2, 1), "c0x": (0.6, 3, 2, 1)}

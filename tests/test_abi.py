@@ -44,12 +44,12 @@ def test_parse_errors_carry_reference_messages(gpu_lib, tmp_path):
 
 
 def test_unsupported_sections_are_rejected(gpu_lib, tmp_path):
-    (tmp_path / "c").write_text("[Chain]\n1 1 1\n2 2 2\n\n[Vector_Fragment_Memory]\n1.0\n")
+    (tmp_path / "c").write_text("[Chain]\n1 1 1\n2 2 2\n\n[Excluded]\n5.0 3.0\n5.0 4.0\n")
     h = C.c_void_p()
     rc = gpu_lib.awsem_create_from_files(str(tmp_path).encode(), b"d", b"c", b"s", b"2 3.5 3.5", b"", 0, 0,
                                          C.byref(h))
     assert rc == -2
-    assert b"[Vector_Fragment_Memory]" in gpu_lib.awsem_last_error()
+    assert b"[Excluded]" in gpu_lib.awsem_last_error()
 
 
 def test_disabled_sections_are_ignored(gpu_lib, tmp_path):

@@ -73,10 +73,10 @@ def test_continuation_calls_keep_the_list(case, prec, tmp_path, gpu_lib):
     assert np.array_equal(np.concatenate([r0, r1, r2]), rows_one)
 
 
-@pytest.mark.parametrize("case", ["c0go", "c0x", "c0s"])
+@pytest.mark.parametrize("case", ["c0go", "c0x", "c0s", "c0v"])
 def test_persistent_form_equals_kernel_chain(case, tmp_path, gpu_lib):
-    """c0s: Shake and the membrane potential, whose pass the persistent
-    kernel runs beside the pair passes."""
+    """c0s, c0v: Shake, the membrane potential and vector fragment memory,
+    whose pass the persistent kernel runs beside the pair passes."""
     from awsemmd_b200.engine import AwsemSystem
 
     files, g = write_case(case, tmp_path)

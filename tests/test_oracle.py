@@ -6,7 +6,7 @@ import pytest
 
 from conftest import REFERENCE_SRC, neigh_of, write_case
 
-CASES = ["c0", "sheet", "r1r69", "r1r69tb", "r1r69go", "r1r69go2", "c0go", "c0x", "sheetx", "c0s", "sheets"]
+CASES = ["c0", "sheet", "r1r69", "r1r69tb", "r1r69go", "r1r69go2", "c0go", "c0x", "sheetx", "c0s", "sheets", "c0v"]
 
 
 def rel_err(a, b):
@@ -49,7 +49,7 @@ def test_terms_exercised():
     """The fixtures between them exercise every term on the path."""
     e = {n: np.load(os.path.join(os.path.dirname(__file__), "golden", f"{n}.npz"))["e0"] for n in CASES}
     for k, name in [(1, "chain"), (2, "shake"), (3, "chi"), (4, "rama"), (6, "dssp"), (7, "p_ap"), (8, "water"), (9, "burial"),
-                    (10, "helix"), (11, "amh-go"), (12, "frag_mem"), (14, "contact restraints"), (15, "membrane"), (16, "ssb"),
+                    (10, "helix"), (11, "amh-go"), (12, "frag_mem"), (13, "vector frag_mem"), (14, "contact restraints"), (15, "membrane"), (16, "ssb"),
                     (17, "debye-hueckel"), (19, "bond")]:
         assert max(abs(e[c][k]) for c in CASES) > 1e-2, name
     assert max(abs(e[c][18]) for c in CASES) > 1.0  # vexcluded
