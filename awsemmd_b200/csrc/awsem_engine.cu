@@ -116,6 +116,8 @@ class EngineBase {
   virtual void set_launch_shapes(const int *shapes) = 0;
   virtual void set_neighbor(double skin, int delay, int every, int check) = 0;
   virtual void set_list_built(int built) = 0;
+  virtual int q_create(int rep, const std::string &words) = 0;
+  virtual double q_value(int qid) = 0;
   virtual void get_step_form(int *out) = 0;
   virtual void model_info(long long *info) = 0;
   virtual double run_ms() const = 0;
@@ -1405,6 +1407,46 @@ template <typename R> class Engine : public EngineBase {
 
   void set_list_built(int built) override { next_compute_built = built ? 1 : 0; }
 
+  // Q order parameters (compute qwolynes / qonuchic) of single replicas
+  struct QDev {
+    int rep = 0;
+    QDefinition def;
+    DBuf<double> mat, partial, out;
+  };
+  std::vector<std::unique_ptr<QDev>> qdefs;
+
+  int q_create(int rep, const std::string &words) override
+  {
+    check_rep(rep);
+    std::unique_ptr<QDev> q(new QDev());
+    q->rep = rep;
+    q->def = parse_q_compute(words, rep_res(rep));
+    q->mat.upload(q->def.mat, s0);
+    q->partial.alloc((size_t) std::max(q->def.n, 1));
+    q->out.alloc(1);
+    std::vector<double>().swap(q->def.mat);
+    CK(cudaStreamSynchronize(s0));
+    qdefs.push_back(std::move(q));
+    return (int) qdefs.size() - 1;
+  }
+
+  double q_value(int qid) override
+  {
+    if (qid < 0 || qid >= (int) qdefs.size()) throw std::invalid_argument("no such Q definition");
+    QDev &q = *qdefs[qid];
+    const QDefinition &d = q.def;
+    const double *xr = x.p + (size_t) 3 * rep_atom0(q.rep);
+    if (d.n > 0) {
+      dev::k_q_rows<<<d.n, 256, 0, s0>>>(xr, d.n, d.kind, d.sep, d.sigma_exp, q.mat.p, q.partial.p);
+      dev::k_q_sum<<<1, 256, 0, s0>>>(q.partial.p, d.n, d.qnorm, q.out.p);
+    }
+    CK(cudaGetLastError());
+    double v = 0.0;
+    if (d.n > 0) CK(cudaMemcpyAsync(&v, q.out.p, sizeof v, cudaMemcpyDeviceToHost, s0));
+    CK(cudaStreamSynchronize(s0));
+    return v;
+  }
+
   template <typename F> void set_nl_field(F dev::NLState::*field, F value)
   {
     dev::NLState st;
@@ -2340,6 +2382,18 @@ int awsem_set_neighbor(awsem_system *sys, double skin, int delay, int every, int
 {
   if (!ready(sys)) return AWSEM_EINVAL;
   return guarded([&] { sys->eng->set_neighbor(skin, delay, every, check); });
+}
+
+int awsem_q_create(awsem_system *sys, int rep, const char *words, int *qid)
+{
+  if (!ready(sys) || !words || !qid) return AWSEM_EINVAL;
+  return guarded([&] { *qid = sys->eng->q_create(rep, words); });
+}
+
+int awsem_q_value(awsem_system *sys, int qid, double *value)
+{
+  if (!ready(sys) || !value) return AWSEM_EINVAL;
+  return guarded([&] { *value = sys->eng->q_value(qid); });
 }
 
 int awsem_set_list_built(awsem_system *sys, int built)

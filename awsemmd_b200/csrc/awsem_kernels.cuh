@@ -1576,6 +1576,59 @@ __global__ void k_thermo(const double *e_res, const long long *e_fix, int efix_s
   }
 }
 
+// Q order parameters (compute qwolynes / qonuchic; QDefinition): block i
+// sums row i of the pair terms over j > i, in a fixed tree order; k_q_sum
+// adds the rows in a fixed order and normalises.  x: the replica's atoms
+// from its first (CA, O, CB per residue).
+__global__ void k_q_rows(const double *x, int n, int kind, int sep, double sigma_exp, const double *mat,
+                         double *partial)
+{
+  const int i = blockIdx.x;
+  __shared__ double sh[256];
+  double acc = 0.0;
+  const double xi0 = x[9 * i], xi1 = x[9 * i + 1], xi2 = x[9 * i + 2];
+  for (int j = i + 1 + threadIdx.x; j < n; j += blockDim.x) {
+    const int d = j - i;
+    const double m = mat[(size_t) i * n + j];
+    const double dx = xi0 - x[9 * j], dy = xi1 - x[9 * j + 1], dz = xi2 - x[9 * j + 2];
+    const double rsq = dx * dx + dy * dy + dz * dz;
+    if (kind == 0) {
+      if (d <= sep) continue;
+      const double sg = pow(1.0 + d, sigma_exp), dr = sqrt(rsq) - m;
+      acc += exp(-(dr * dr) / (2.0 * (sg * sg)));
+    } else {
+      if (d <= 3 || m < 0.0) continue;
+      if (kind == 1) {
+        if (rsq < m) acc += 1.0;
+      } else {
+        const double s2 = pow(1.0 + d, 2.0 * sigma_exp), dr = sqrt(rsq) - sqrt(m);
+        acc += exp(-(dr * dr) / (2.0 * s2));
+      }
+    }
+  }
+  sh[threadIdx.x] = acc;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) partial[i] = sh[0];
+}
+
+__global__ void k_q_sum(const double *partial, int n, double qnorm, double *out)
+{
+  __shared__ double sh[256];
+  double acc = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) acc += partial[i];
+  sh[threadIdx.x] = acc;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *out = sh[0] * qnorm;
+}
+
 // Per-term sums of each replica's residues in a fixed tree order
 // (block (t, r) sums energy slot t of replica rep0 + r)
 __global__ void k_energy_reduce(const double *e_res, const long long *e_fix, int efix_slots, int n_res,

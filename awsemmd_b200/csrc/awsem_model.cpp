@@ -948,6 +948,87 @@ void build_vfm(const Topology &top, const GammaTable &G, const std::vector<Memor
   }
 }
 
+// The constructors of compute qwolynes (compute_q_wolynes.cpp:50-110, file
+// read :135-152) and compute qonuchic (compute_q_onuchic.cpp:27-85, contact
+// arrays :124-186): argument counts, the native data and the normalisation.
+// The group is the replica's CA atoms (n_res of them).
+QDefinition parse_q_compute(const std::string &words, int n_res)
+{
+  auto w = tokens(words);
+  QDefinition q;
+  q.n = n_res;
+  q.mat.assign((size_t) n_res * n_res, 0.0);
+  if (w.size() >= 3 && w[2] == "qwolynes") {
+    if (w.size() != 6) fail("Illegal compute qwolynes command");
+    q.kind = 0;
+    q.sep = atoi(w[4].c_str());
+    q.sigma_exp = atof(w[5].c_str());
+    std::ifstream in(w[3]);
+    if (!in) fail("Native distance file can't be read");
+    for (size_t k = 0; k < q.mat.size(); k++)
+      if (!(in >> q.mat[k])) fail("compute qwolynes: the native distance file holds fewer than n x n values");
+    q.qnorm = 2.0 / (((double) n_res - (double) q.sep) * ((double) n_res - ((double) q.sep + 1.0)));
+    return q;
+  }
+  if (w.size() < 3 || w[2] != "qonuchic") fail("compute: only the qwolynes and qonuchic styles are supported");
+  const int narg = (int) w.size();
+  if (narg != 5 && narg != 6 && narg != 7) fail("Illegal compute qonuchic command");
+  const std::string type = w[3];
+  q.sigma_exp = 0.15;
+  double count = 0.0;
+  for (double &m : q.mat) m = -1.0;  // not native
+  if (type == "cutoff" || type == "cutoff/gauss") {
+    const bool hard = type == "cutoff";
+    if (hard ? narg != 7 : narg != 6) fail("Illegal compute qonuchic command");
+    q.kind = hard ? 1 : 2;
+    const double r_contact = atof(w[4].c_str()), r_consq = r_contact * r_contact;
+    const double factor = hard ? atof(w[6].c_str()) : 1.0;
+    FILE *f = fopen(w[5].c_str(), "r");
+    if (!f) fail("Compute qonuchic: can't read native coordinates");
+    int na = 0;
+    if (fscanf(f, "%d", &na) != 1) na = -1;
+    std::vector<double> xn((size_t) 3 * std::max(na, 0));
+    for (int i = 0; i < na; i++)
+      if (fscanf(f, "%lf %lf %lf", &xn[3 * i], &xn[3 * i + 1], &xn[3 * i + 2]) != 3) na = -1;
+    fclose(f);
+    if (na != n_res) fail("Compute qonuchic: atom number mismatch");
+    for (int i = 0; i < na; i++)
+      for (int j = 0; j < na; j++) {
+        const double dx = xn[3 * j] - xn[3 * i], dy = xn[3 * j + 1] - xn[3 * i + 1], dz = xn[3 * j + 2] - xn[3 * i + 2];
+        double rsq = dx * dx + dy * dy + dz * dz;
+        if (rsq < r_consq && j - i > 3) {
+          count += 1.0;
+          if (hard) rsq *= factor * factor;
+          q.mat[(size_t) i * n_res + j] = rsq;
+        }
+      }
+  } else if (type == "shadow" || type == "shadow/gauss") {
+    const bool hard = type == "shadow";
+    if (hard ? narg != 6 : narg != 5) fail("Illegal compute qonuchic command");
+    q.kind = hard ? 1 : 2;
+    const double factor = hard ? atof(w[5].c_str()) : 1.0;
+    FILE *f = fopen(w[4].c_str(), "r");
+    if (!f) fail("Compute qonuchic: can't read contact map file");
+    int ires, jres;
+    double rn;
+    while (fscanf(f, "%d %d %lf", &ires, &jres, &rn) == 3) {
+      ires--;
+      jres--;
+      if (ires >= n_res || jres >= n_res || ires < 0 || jres < 0 || abs(jres - ires) <= 3) {
+        fclose(f);
+        fail("Compute qonuchic: wrong residue index in shadow contact map file");
+      }
+      q.mat[(size_t) ires * n_res + jres] = hard ? rn * rn * (factor * factor) : rn * rn;
+      count += 1.0;
+    }
+    fclose(f);
+  } else {
+    fail("Wrong type for compute qonuchic");
+  }
+  q.qnorm = 1 / count;
+  return q;
+}
+
 // zim (fix_backbone.cpp:611-619): the membrane zone (1, 2 or 3) of each
 // residue; the reference leaves the potential undefined for other values
 void read_zim(const std::string &path, int n_res, std::vector<int> &z)

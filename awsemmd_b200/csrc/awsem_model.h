@@ -269,6 +269,20 @@ struct Batch {
   int n_sys = 0;
 };
 
+// A Q order parameter over the CA atoms of one replica: compute qwolynes
+// (src/compute_q_wolynes.cpp) or compute qonuchic (src/compute_q_onuchic.cpp)
+// from the words after LAMMPS's `compute`.  kind 0: Q_W, sum over |i-j| > sep
+// of exp(-(r - mat)^2 / 2 sigma^2), sigma = (1 + |i-j|)^sigma_exp; kind 1:
+// count of native pairs (mat >= 0, |i-j| > 3) with r^2 < mat; kind 2: sum over
+// them of exp(-(r - sqrt(mat))^2 / 2 sigma^2), sigma^2 = (1 + |i-j|)^(2 sigma_exp).
+// The value is the sum times qnorm; only entries i < j of mat are read.
+struct QDefinition {
+  int kind = 0, n = 0, sep = 0;
+  double sigma_exp = 0.15, qnorm = 0.0;
+  std::vector<double> mat;  // [n*n]
+};
+QDefinition parse_q_compute(const std::string &words, int n_res);
+
 // Concatenate replicas (each already loaded); throws if their force fields differ.
 void assemble_batch(const std::vector<const SystemInput *> &reps, Batch &out);
 

@@ -114,6 +114,9 @@ def load_library(path: str = LIB_PATH):
     lib.awsem_get_step_form.argtypes = [vp, vp]
     lib.awsem_set_launch_shapes.argtypes = [vp, vp]
     lib.awsem_set_neighbor.argtypes = [vp, C.c_double, ip, ip, ip]
+    lib.awsem_set_list_built.argtypes = [vp, ip]
+    lib.awsem_q_create.argtypes = [vp, ip, cp, vp]
+    lib.awsem_q_value.argtypes = [vp, ip, vp]
     lib.awsem_run_window.argtypes = [vp, C.c_longlong, C.POINTER(RunParams), C.c_longlong, C.c_longlong, ip, vp]
     lib.awsem_create_from_atoms.argtypes = [cp, cp, cp, ip, vp, vp, vp, vp, vp, vp, ip, vp, ip, vp, vp, vp, vp, cp, cp,
                                             ip, ip, C.POINTER(vp)]
@@ -313,6 +316,19 @@ class AwsemSystem:
         chk = int(check) if not isinstance(check, bool) else int(check is True)
         _check(self.lib, self.lib.awsem_set_neighbor(self.h, float(skin), int(delay), int(every), chk),
                "awsem_set_neighbor")
+
+    def q_create(self, words: str, rep: int = 0) -> int:
+        """A Q order parameter (awsem_q_create): `words` as after LAMMPS's
+        `compute` (ID group qwolynes ... / qonuchic ...)."""
+        qid = C.c_int()
+        _check(self.lib, self.lib.awsem_q_create(self.h, int(rep), words.encode(), C.byref(qid)), "awsem_q_create")
+        return qid.value
+
+    def q_value(self, qid: int) -> float:
+        """The Q order parameter on the replica's current positions (awsem_q_value)."""
+        v = C.c_double()
+        _check(self.lib, self.lib.awsem_q_value(self.h, int(qid), C.byref(v)), "awsem_q_value")
+        return v.value
 
     def set_step_form(self, form: str, blocks: int = 0, stream_warps: int = 2) -> None:
         """'kernels': each MD step a graph of per-pass kernels; 'persistent':

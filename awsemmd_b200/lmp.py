@@ -22,9 +22,11 @@ velocity <group> create|set|zero|scale (all atoms); group (id, type,
 molecule: lists, ranges a:b[:c], `<>`, `<`, `>` ... ; union, subtract,
 intersect, delete); fix nve / langevin / backbone / print; unfix; thermo;
 thermo_style custom; dump atom; dump_modify sort id; undump; variable
-equal|string|index|loop; print; reset_timestep; run N [upto]; log; echo.
-Anything else (clear, minimize, fix nvt, computes, ...) is an error naming
-the command.
+equal|string|index|loop; print; reset_timestep; run N [upto]; log; echo;
+compute qwolynes / qonuchic on the fix's CA group, c_ID in formulas and
+thermo columns (awsem_q_create / awsem_q_value); uncompute.
+Anything else (clear, minimize, fix nvt, other computes, ...) is an error
+naming the command.
 
 Differences from LAMMPS, by design of the engine: the Langevin noise is the
 engine's counter-based stream keyed by (seed, step, atom id) instead of
@@ -366,6 +368,8 @@ class Driver:
         self.step = 0
         self.eng = None
         self.eng_key = None
+        self.computes = {}   # ID -> the words after `compute`
+        self.qids = {}       # ID -> (engine, Q definition id)
         self.x = self.v = None   # host state (between runs)
         self.energies = None
         self.energy_log = None
@@ -682,6 +686,38 @@ class Driver:
         return 2.0 * ke / (self._dof() * BOLTZ)
 
     # -- fixes, output -------------------------------------------------------
+    def c_compute(self, a):
+        if len(a) < 3:
+            raise LammpsError("Illegal compute command")
+        if a[2] not in ("qwolynes", "qonuchic"):
+            raise LammpsError(f"compute style {a[2]} is not supported by this driver")
+        if a[1] not in self.groups:
+            raise LammpsError(f"Could not find compute group ID {a[1]}")
+        self.computes[a[0]] = " ".join(a)
+        self.qids.pop(a[0], None)
+
+    def c_uncompute(self, a):
+        if a[0] not in self.computes:
+            raise LammpsError(f"Could not find uncompute ID {a[0]}")
+        del self.computes[a[0]]
+        self.qids.pop(a[0], None)
+
+    def _compute_value(self, cid: str) -> float:
+        """c_ID of a Q compute on the engine's current positions"""
+        if cid not in self.computes:
+            raise LammpsError(f"Invalid compute ID c_{cid} in variable formula")
+        if self.eng is None:
+            raise LammpsError(f"compute {cid} used before the first run")
+        words = self.computes[cid]
+        fb = [f for f in self.fixes.values() if f[0] == "backbone"]
+        if not fb or words.split()[1] != fb[0][1]:
+            raise LammpsError(f"compute {cid}: its group must be the CA group of fix backbone")
+        held = self.qids.get(cid)
+        if held is None or held[0] is not self.eng:
+            held = (self.eng, self.eng.q_create(words))
+            self.qids[cid] = held
+        return float(self.eng.q_value(held[1]))
+
     def c_fix(self, a):
         fid, group, style, rest = a[0], a[1], a[2], a[3:]
         if group not in self.groups:
@@ -811,6 +847,8 @@ class Driver:
             return self.step * float(self.dt or 1.0)
         if name == "atoms":
             return float(len(self.data.ids))
+        if name.startswith("c_"):
+            return self._compute_value(name[2:])
         e = self.energies
         if e is None:
             raise LammpsError(f"energy keyword {name} used before the first run")
@@ -976,7 +1014,7 @@ class Driver:
     def thermo_row(self):
         vals = []
         for k in self.thermo_keys:
-            if k == "press" or k == "vol" or k.startswith("c_"):
+            if k == "press" or k == "vol" or (k.startswith("c_") and k[2:] not in self.computes):
                 vals.append(f"{'n/a':>14s}")
             elif k == "step":
                 vals.append(f"{self.step:>14d}")

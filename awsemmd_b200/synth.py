@@ -373,6 +373,27 @@ def write_zim(sys_: System, path: str, seed: int = 11) -> None:
         f.write("\n".join(str(int(v)) for v in z) + "\n")
 
 
+def write_q_files(ca_native: np.ndarray, outdir: str, r_contact: float = 9.5) -> None:
+    """Inputs of the Q order parameters for a native CA trace [n][3] (A):
+    rnative.dat (compute qwolynes: the n x n CA-CA distance matrix),
+    native_ca.dat (compute qonuchic cutoff: the count, then CA coordinates)
+    and shadow.dat (compute qonuchic shadow: "i j r" for the native pairs
+    with |i - j| > 3 closer than r_contact)."""
+    ca = np.asarray(ca_native, dtype=np.float64)
+    n = len(ca)
+    d = np.linalg.norm(ca[:, None, :] - ca[None, :, :], axis=-1)
+    with open(os.path.join(outdir, "rnative.dat"), "w") as f:
+        for i in range(n):
+            f.write(" ".join(f"{float(v):.6f}" for v in d[i]) + "\n")
+    with open(os.path.join(outdir, "native_ca.dat"), "w") as f:
+        f.write(f"{n}\n" + "".join(f"{float(p[0]):.6f} {float(p[1]):.6f} {float(p[2]):.6f}\n" for p in ca))
+    with open(os.path.join(outdir, "shadow.dat"), "w") as f:
+        for i in range(n):
+            for j in range(i + 4, n):
+                if d[i, j] < r_contact:
+                    f.write(f"{i + 1} {j + 1} {float(d[i, j]):.6f}\n")
+
+
 def write_charges(sys_: System, path: str) -> None:
     """charge_on_residues.dat: +1 on K and R, -1 on D and E (residues numbered over all chains)."""
     seq = "".join(ch.seq for ch in sys_.chains)

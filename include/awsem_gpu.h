@@ -266,6 +266,19 @@ int awsem_set_neighbor(awsem_system *sys, double skin, int delay, int every, int
  * awsem_compute builds.  AWSEM_EINVAL unless built is 0 or 1. */
 int awsem_set_list_built(awsem_system *sys, int built);
 
+/* Q order parameters, as LAMMPS's `compute ID group qwolynes datafile sep
+ * exp` (src/compute_q_wolynes.cpp:50-238) and `compute ID group qonuchic
+ * cutoff r_contact datafile factor | cutoff/gauss r_contact datafile |
+ * shadow datafile factor | shadow/gauss datafile` (src/compute_q_onuchic.cpp:
+ * 27-317) define them: `words` are the words after `compute`, the group is
+ * the CA atoms of replica `rep` (the fix's first group), data files are
+ * opened as named (relative to the process's working directory).  Errors
+ * carry the reference's messages.  awsem_q_value evaluates a definition on
+ * the replica's current positions (its compute_scalar): pair sums in FP64 in
+ * a fixed order on the device. */
+int awsem_q_create(awsem_system *sys, int rep, const char *words, int *qid);
+int awsem_q_value(awsem_system *sys, int qid, double *value);
+
 /* Step form of awsem_run / awsem_server_advance (no counterpart in the
  * reference, which evaluates on the CPU inside LAMMPS's pre_force hook).
  * form 0: each MD step is a chain of per-pass kernels (prepare, list

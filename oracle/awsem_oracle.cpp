@@ -2435,6 +2435,131 @@ int oracle_set_neighbor(void *h, double skin, int delay, int every, int check)
   return 0;
 }
 
+/* compute qwolynes (compute_q_wolynes.cpp:50-238) and compute qonuchic
+   (compute_q_onuchic.cpp:27-317) over the CA atoms (group alpha_carbons),
+   `words` as after LAMMPS's `compute`, data files opened as named. */
+int oracle_q(void *h, const double *x, const char *words_c, double *out)
+{
+  System *S = (System *) h;
+  try {
+    std::vector<std::string> w = words(words_c);
+    if (w.size() < 3) throw std::runtime_error("compute: ID group style ...");
+    if (w[1] != "alpha_carbons") throw std::runtime_error("oracle: Q over the group alpha_carbons only");
+    const int n = S->n;
+    auto xca = [&](int r, int k) { return x[3 * S->ca[r] + k]; };
+    double q = 0.0;
+    if (w[2] == "qwolynes") {
+      if (w.size() != 6) throw std::runtime_error("Illegal compute qwolynes command");
+      int sep = atoi(w[4].c_str());
+      double sigmaexp = atof(w[5].c_str());
+      std::vector<double> r_native((size_t) n * n);
+      std::ifstream in(w[3]);
+      if (!in) throw std::runtime_error("Native distance file can't be read");
+      for (int i = 0; i < n; ++i)
+        for (int j = 0; j < n; ++j) in >> r_native[(size_t) i * n + j];
+      for (int i = 0; i < n; i++)
+        for (int j = i + 1; j < n; j++) {
+          if (!(abs(j - i) > sep)) continue;
+          double sigmaij = pow(1 + abs(i - j), sigmaexp);
+          double rijn = r_native[(size_t) i * n + j];
+          double rij = sqrt(pow(xca(i, 0) - xca(j, 0), 2) + pow(xca(i, 1) - xca(j, 1), 2) + pow(xca(i, 2) - xca(j, 2), 2));
+          q += exp(-pow(rij - rijn, 2) / (2.0 * pow(sigmaij, 2)));
+        }
+      *out = q * (2.0 / (((double) n - (double) sep) * ((double) n - ((double) sep + 1.0))));
+      return 0;
+    }
+    if (w[2] != "qonuchic") throw std::runtime_error("oracle: compute style " + w[2]);
+    int narg = (int) w.size();
+    if (narg != 5 && narg != 6 && narg != 7) throw std::runtime_error("Illegal compute qonuchic command");
+    enum { T_CUTOFF = 0, T_SHADOW = 1, T_CUTOFF_GAUSS = 2, T_SHADOW_GAUSS = 3 };
+    int cp_type;
+    double factor = 1.0, r_consq = 0.0;
+    std::string datafile;
+    if (w[3] == "cutoff" || w[3] == "cutoff/gauss") {
+      cp_type = w[3] == "cutoff" ? T_CUTOFF : T_CUTOFF_GAUSS;
+      if (narg != (cp_type == T_CUTOFF ? 7 : 6)) throw std::runtime_error("Illegal compute qonuchic command");
+      double r_contact = atof(w[4].c_str());
+      r_consq = r_contact * r_contact;
+      datafile = w[5];
+      if (cp_type == T_CUTOFF) factor = atof(w[6].c_str());
+    } else if (w[3] == "shadow" || w[3] == "shadow/gauss") {
+      cp_type = w[3] == "shadow" ? T_SHADOW : T_SHADOW_GAUSS;
+      if (narg != (cp_type == T_SHADOW ? 6 : 5)) throw std::runtime_error("Illegal compute qonuchic command");
+      datafile = w[4];
+      if (cp_type == T_SHADOW) factor = atof(w[5].c_str());
+    } else {
+      throw std::runtime_error("Wrong type for compute qonuchic");
+    }
+    const double sigmaexp = 0.15;
+    std::vector<double> rsq_native((size_t) n * n, 0.0);
+    std::vector<char> is_native((size_t) n * n, 0);
+    double qnorm = 0.0;
+    if (cp_type == T_CUTOFF || cp_type == T_CUTOFF_GAUSS) {
+      FILE *f = fopen(datafile.c_str(), "r");
+      if (!f) throw std::runtime_error("Compute qonuchic: can't read native coordinates");
+      int nAtoms = 0;
+      if (fscanf(f, "%d", &nAtoms) != 1 || nAtoms != n) {
+        fclose(f);
+        throw std::runtime_error("Compute qonuchic: atom number mismatch");
+      }
+      std::vector<double> xn((size_t) 3 * n);
+      for (int i = 0; i < n; ++i)
+        if (fscanf(f, "%lf %lf %lf", &xn[3 * i], &xn[3 * i + 1], &xn[3 * i + 2]) != 3) {
+          fclose(f);
+          throw std::runtime_error("Compute qonuchic: can't read native coordinates");
+        }
+      fclose(f);
+      for (int i = 0; i < n; ++i)
+        for (int j = 0; j < n; ++j) {
+          double dx0 = xn[3 * j] - xn[3 * i], dx1 = xn[3 * j + 1] - xn[3 * i + 1], dx2 = xn[3 * j + 2] - xn[3 * i + 2];
+          double &r = rsq_native[(size_t) i * n + j];
+          r = dx0 * dx0 + dx1 * dx1 + dx2 * dx2;
+          if (r < r_consq && j - i > 3) {
+            is_native[(size_t) i * n + j] = 1;
+            qnorm += 1.0;
+          }
+          if (cp_type == T_CUTOFF && is_native[(size_t) i * n + j]) r *= factor * factor;
+        }
+    } else {
+      FILE *f = fopen(datafile.c_str(), "r");
+      if (!f) throw std::runtime_error("Compute qonuchic: can't read contact map file");
+      int ires, jres;
+      double rn;
+      while (fscanf(f, "%d %d %lf", &ires, &jres, &rn) == 3) {
+        ires--;
+        jres--;
+        if (ires >= n || jres >= n || ires < 0 || jres < 0 || abs(jres - ires) <= 3) {
+          fclose(f);
+          throw std::runtime_error("Compute qonuchic: wrong residue index in shadow contact map file");
+        }
+        is_native[(size_t) ires * n + jres] = 1;
+        rsq_native[(size_t) ires * n + jres] = rn * rn;
+        if (cp_type == T_SHADOW) rsq_native[(size_t) ires * n + jres] *= factor * factor;
+        qnorm += 1.0;
+      }
+      fclose(f);
+    }
+    qnorm = 1 / qnorm;
+    for (int i = 0; i < n; i++)
+      for (int j = i + 1; j < n; j++) {
+        if (!(is_native[(size_t) i * n + j] && abs(j - i) > 3)) continue;
+        double dx0 = xca(i, 0) - xca(j, 0), dx1 = xca(i, 1) - xca(j, 1), dx2 = xca(i, 2) - xca(j, 2);
+        double rsq = dx0 * dx0 + dx1 * dx1 + dx2 * dx2;
+        if (cp_type == T_CUTOFF || cp_type == T_SHADOW) {
+          if (rsq < rsq_native[(size_t) i * n + j]) q += 1.0;
+        } else {
+          double sigma_sq = pow(1 + abs(i - j), 2.0 * sigmaexp);
+          q += exp(-pow(sqrt(rsq) - sqrt(rsq_native[(size_t) i * n + j]), 2) / (2.0 * sigma_sq));
+        }
+      }
+    *out = q * qnorm;
+  } catch (std::exception &e) {
+    g_err = e.what();
+    return -1;
+  }
+  return 0;
+}
+
 double oracle_uniform(unsigned long long seed, long long step, long long tag, int comp)
 {
   return uniform01(seed, step, tag, comp);

@@ -38,6 +38,9 @@ int oracle_run(void *h, double *x, double *v, long long step0, long long nsteps,
 /* LAMMPS neighbor skin and neigh_modify delay / every / check of the fix's
    full neighbour list that [AMH-Go] reads (defaults 2.0, 0, 1, 1) */
 int oracle_set_neighbor(void *h, double skin, int delay, int every, int check);
+/* compute qwolynes / qonuchic over the CA atoms at positions x ([natoms][3]);
+   `words` as after LAMMPS's `compute`, data files opened as named */
+int oracle_q(void *h, const double *x, const char *words, double *out);
 double oracle_uniform(unsigned long long seed, long long step, long long tag, int comp);
 
 #ifdef __cplusplus

@@ -45,6 +45,7 @@ def _load_ref(path=REF_LIB):
         lib.ref_residue_arrays.argtypes = [C.c_void_p, C.c_void_p]
         lib.ref_run.argtypes = [C.c_void_p, C.c_longlong, C.c_double, C.c_int, C.c_double, C.c_double,
                                 C.c_double, C.c_ulonglong, C.c_void_p]
+        lib.ref_compute_q.argtypes = [C.c_void_p, C.c_char_p, C.c_void_p]
         lib.ref_nbuilds.argtypes = [C.c_void_p]
         lib.ref_nbuilds.restype = C.c_long
         lib.ref_last_error.restype = C.c_char_p
@@ -101,6 +102,13 @@ class RefSystem:
             raise RuntimeError(self.lib.ref_last_error().decode())
         return f
 
+    def compute_q(self, words: str) -> float:
+        """the reference's `compute <words>` (qwolynes / qonuchic) at the current positions"""
+        out = C.c_double()
+        if self.lib.ref_compute_q(self.h, words.encode(), C.byref(out)) != 0:
+            raise RuntimeError(self.lib.ref_last_error().decode())
+        return out.value
+
     def nbuilds(self) -> int:
         """neighbour-list builds so far (run setups included)"""
         return int(self.lib.ref_nbuilds(self.h))
@@ -144,6 +152,7 @@ def _load_oracle():
         lib.oracle_run.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_longlong, C.c_longlong, C.c_double,
                                    C.c_int, C.c_double, C.c_double, C.c_double, C.c_ulonglong, C.c_void_p]
         lib.oracle_set_neighbor.argtypes = [C.c_void_p, C.c_double, C.c_int, C.c_int, C.c_int]
+        lib.oracle_q.argtypes = [C.c_void_p, C.c_void_p, C.c_char_p, C.c_void_p]
         lib.oracle_uniform.restype = C.c_double
         lib.oracle_uniform.argtypes = [C.c_ulonglong, C.c_longlong, C.c_longlong, C.c_int]
         _orc = lib
@@ -178,6 +187,14 @@ class OracleSystem:
         if self.lib.oracle_compute(self.h, x.ctypes.data, f.ctypes.data, e.ctypes.data) != 0:
             raise RuntimeError(self.lib.oracle_last_error().decode())
         return f, e
+
+    def q(self, x: np.ndarray, words: str) -> float:
+        """compute qwolynes / qonuchic (`words` after `compute`) at positions x"""
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        out = C.c_double()
+        if self.lib.oracle_q(self.h, x.ctypes.data, words.encode(), C.byref(out)) != 0:
+            raise RuntimeError(self.lib.oracle_last_error().decode())
+        return out.value
 
     def set_neighbor(self, skin=2.0, delay=0, every=1, check=True):
         """neighbor skin and neigh_modify delay/every/check of the list [AMH-Go] reads"""

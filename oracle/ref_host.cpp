@@ -31,6 +31,8 @@
 #include "fix_backbone_gpu.h"
 #endif
 #include "pair_excluded_volume.h"
+#include "compute_q_onuchic.h"
+#include "compute_q_wolynes.h"
 #include "atom_vec_awsemmd.h"
 
 #include <unistd.h>
@@ -790,6 +792,39 @@ int ref_run(void *hp, long long nsteps, double dt, int langevin, double t_start,
 }
 
 long ref_nbuilds(void *hp) { return ((RefHost *) hp)->nbuilds; }
+
+/* The reference's `compute ID group qwolynes ...` / `compute ID group
+   qonuchic ...` (the whitespace-separated words after `compute`), created in
+   the run directory and evaluated once at the current positions. */
+int ref_compute_q(void *hp, const char *words, double *out)
+{
+  RefHost *h = (RefHost *) hp;
+  try {
+    Cwd cwd(h->workdir);
+    std::vector<std::string> v = split_ws(words);
+    if (v.size() < 3) throw std::runtime_error("compute: ID group style ...");
+    std::vector<char *> args;
+    for (auto &s : v) args.push_back(strdup(s.c_str()));
+    Compute *c = nullptr;
+    try {
+      if (v[2] == "qwolynes") c = new ComputeQWolynes(h->lmp, (int) args.size(), args.data());
+      else if (v[2] == "qonuchic") c = new ComputeQOnuchic(h->lmp, (int) args.size(), args.data());
+      else throw std::runtime_error("compute style " + v[2] + " is not hosted");
+      c->init();
+      *out = c->compute_scalar();
+    } catch (...) {
+      delete c;
+      for (char *a : args) free(a);
+      throw;
+    }
+    delete c;
+    for (char *a : args) free(a);
+  } catch (std::exception &e) {
+    g_ref_err = e.what();
+    return -1;
+  }
+  return 0;
+}
 
 /* Uniform draw of the shared Langevin stream (exported for cross-checks). */
 double ref_uniform(unsigned long long seed, long long step, long long tag, int comp)

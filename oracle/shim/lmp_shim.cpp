@@ -159,6 +159,24 @@ Fix::~Fix()
   free(style);
 }
 
+Compute::Compute(LAMMPS *lmp, int, char **arg) : Pointers(lmp)
+{
+  id = strdup(arg[0]);
+  style = strdup(arg[2]);
+  igroup = lmp->group->find(arg[1]);
+  if (igroup == -1) error->all(FLERR, "Could not find compute group ID");
+  groupbit = lmp->group->bitmask[igroup];
+  scalar_flag = vector_flag = extscalar = 0;
+  scalar = 0.0;
+  invoked_scalar = -1;
+}
+
+Compute::~Compute()
+{
+  free(id);
+  free(style);
+}
+
 Pair::Pair(LAMMPS *lmp) : Pointers(lmp)
 {
   eng_vdwl = eng_coul = 0.0;
@@ -242,6 +260,7 @@ LAMMPS::LAMMPS()
   error = new Error();
   atom = new Atom();
   memset(atom, 0, sizeof(Atom));
+  atom->tag_enable = 1;
   update = new Update();
   memset(update, 0, sizeof(Update));
   neighbor = new Neighbor();

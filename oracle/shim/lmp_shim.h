@@ -142,6 +142,7 @@ class Atom {
   tagint *residue;
   double *mass;
   int molecular;
+  int tag_enable = 1;
   AtomVec *avec;
   AtomVec *style_match(const char *name);
 };
@@ -277,6 +278,20 @@ namespace FixConst {
     MIN_ENERGY = 1 << 22
   };
 }
+
+// LAMMPS's Compute base, as far as the reference computes use it
+class Compute : protected Pointers {
+ public:
+  char *id, *style;
+  int igroup, groupbit;
+  int scalar_flag, vector_flag, extscalar;
+  double scalar;
+  bigint invoked_scalar;
+  Compute(LAMMPS *, int, char **);
+  virtual ~Compute();
+  virtual void init() {}
+  virtual double compute_scalar() { return 0.0; }
+};
 
 class Fix : protected Pointers {
  public:

@@ -42,6 +42,12 @@ against the LAMMPS-API shim (``make -C oracle ref``) and run on four inputs:
                rebuilt during the run and native contacts cross its reach, so
                the trajectory depends on LAMMPS's rebuild rule.
 
+``q_r1r69.npz`` and ``q_c0.npz`` hold the reference's Q order parameters
+(compute qwolynes, compute qonuchic in its four types; Q_DEFS) at the start
+and the end of the 20-step run, with the inputs of synth.write_q_files: the
+native CA trace of r1r69 is its own (crystal) coordinates, that of c0 its
+chain shrunk to 0.8 times its size.
+
 For each it stores the inputs' hash, the step-0 forces and energies, the
 per-residue pair-pass intermediates and a 20-step Langevin trajectory
 (x, v and per-step thermo rows).  ``c0_nve.npz`` holds the thermo rows of a
@@ -156,6 +162,62 @@ CASES = ["c0", "sheet", "r1r69", "r1r69tb", "r1r69go", "r1r69go2", "c0go", "c0x"
 NEIGH = {"c0go": (0.6, 3, 2, 1), "c0x": (0.6, 3, 2, 1)}
 
 
+Q_DEFS = [
+    "q1 alpha_carbons qwolynes rnative.dat 2 0.15",
+    "q2 alpha_carbons qwolynes rnative.dat 3 0.3",
+    "q3 alpha_carbons qonuchic cutoff 9.5 native_ca.dat 1.2",
+    "q4 alpha_carbons qonuchic cutoff/gauss 9.5 native_ca.dat",
+    "q5 alpha_carbons qonuchic shadow shadow.dat 1.2",
+    "q6 alpha_carbons qonuchic shadow/gauss shadow.dat",
+]
+Q_CASES = ["r1r69", "c0"]
+
+
+def write_q_case(name: str, outdir: str) -> dict:
+    """A case's inputs plus the Q inputs (synth.write_q_files) of its native CA trace."""
+    files = write_case(name, outdir)
+    x0 = read_data_x(os.path.join(outdir, files["data"]))
+    ca = x0[::3]  # data files list CA, O, CB per residue
+    if name == "c0":
+        ca = ca.mean(axis=0) + 0.8 * (ca - ca.mean(axis=0))
+    synth.write_q_files(ca, outdir)
+    return files
+
+
+def read_data_x(path: str) -> np.ndarray:
+    """Atom coordinates of a data file in atom-id order."""
+    lines = open(path).read().splitlines()
+    k = next(i for i, l in enumerate(lines) if l.strip().startswith("Atoms"))
+    rows = {}
+    for l in lines[k + 1:]:
+        t = l.split()
+        if not t:
+            if rows:
+                break
+            continue
+        rows[int(t[0])] = [float(v) for v in t[5:8]]
+    return np.array([rows[i] for i in sorted(rows)])
+
+
+def main_q(cases=None):
+    import ref
+
+    for name in cases or Q_CASES:
+        with tempfile.TemporaryDirectory() as tmp:
+            files = write_q_case(name, os.path.join(tmp, name))
+            h = dir_hash(files["workdir"])
+            r = ref.RefSystem(files)
+            q0 = [r.compute_q(w) for w in Q_DEFS]
+            r.run(RUN["nsteps"], dt=RUN["dt"], langevin=True, t_start=RUN["t_start"], t_stop=RUN["t_stop"],
+                  damp=RUN["damp"], seed=RUN["seed"])
+            qN = [r.compute_q(w) for w in Q_DEFS]
+            xN = r.get("x")
+            r.close()
+            np.savez_compressed(os.path.join(GOLDEN, f"q_{name}.npz"), inputs_sha256=np.array(h),
+                                words=np.array(Q_DEFS), q0=np.array(q0), qN=np.array(qN), xN=xN)
+            print("q", name, np.round(q0, 4), np.round(qN, 4))
+
+
 def main(cases=None):
     import ref
 
@@ -192,4 +254,8 @@ def main(cases=None):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1:] or None)
+    args = sys.argv[1:]
+    if args and args[0] == "q":
+        main_q(args[1:] or None)
+    else:
+        main(args or None)

@@ -150,3 +150,38 @@ def test_run_window_parts_equal_one_call(prec, tmp_path, gpu_lib):
         s.set_state(g["x0"], g["v0"])
         with pytest.raises(AwsemError):
             s.run_window(3, (0, 10), True, **kw)
+
+
+def test_deck_q_computes_match_the_reference(tmp_path, gpu_lib):
+    """compute qwolynes / qonuchic (all four types) in a deck on the 1R69
+    inputs: the values fix print writes at steps 0 and 20 of the reference's
+    20-step run are the reference computes' (tests/golden/q_r1r69.npz)."""
+    import make_golden
+
+    files = make_golden.write_q_case("r1r69", str(tmp_path / "r1r69"))
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "r1r69.npz"))
+    q = np.load(os.path.join(os.path.dirname(__file__), "golden", "q_r1r69.npz"))
+    nsteps, dt, t0, t1, damp, seed = g["run"]
+    deck = DECK.format(dt=dt, t0=t0, t1=t1, damp=damp, seed=int(seed), nsteps=int(nsteps), thermo=20, skin=2.0,
+                       delay=0, every=1, check="yes", data=files["data"], seq=files["seq"])
+    comp = "\n".join(f"compute {w}" for w in q["words"])
+    qv = "\n".join(f"variable Q{k + 1} equal c_q{k + 1}" for k in range(len(q["words"])))
+    line = " ".join(f"${{Q{k + 1}}}" for k in range(len(q["words"])))
+    deck = deck.replace("reset_timestep 0", f"{comp}\n{qv}\nfix qprint all print 20 \"{line}\" file qvals screen no\n"
+                                            "reset_timestep 0")
+    from awsemmd_b200 import lmp
+
+    cwd = os.getcwd()
+    os.chdir(files["workdir"])
+    try:
+        d = lmp.Driver(precision="fp64", screen=None, logfile=None)
+        try:
+            d.lines(deck.split("\n"))
+        finally:
+            d.close()
+        rows = [[float(t) for t in l.split()] for l in open("qvals").read().splitlines()[1:]]
+    finally:
+        os.chdir(cwd)
+    assert len(rows) == 2
+    np.testing.assert_allclose(rows[0], q["q0"], rtol=1e-9, atol=1e-12)
+    np.testing.assert_allclose(rows[1], q["qN"], rtol=1e-5, atol=1e-6)

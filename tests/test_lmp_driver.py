@@ -79,6 +79,13 @@ class FakeEngine:
     def set_neighbor(self, skin, delay, every, check):
         self.calls.append(("neighbor", skin, delay, every, check))
 
+    def q_create(self, words):
+        self.calls.append(("q_create", words))
+        return 0
+
+    def q_value(self, qid):
+        return 0.5 + 0.01 * self._step
+
     def get_state(self):
         return self.x.copy(), self.v.copy()
 
@@ -299,3 +306,25 @@ def test_shipped_decks_parse_and_run(deck, tmp_path):
     assert runs[0][3] is False and all(c[3] for c in runs[1:])
     assert sorted(set(eng.kw["role"])) == [0, 1, 2]
     assert (tmp_path / "energy.log").exists()
+
+
+def test_q_compute_in_thermo_and_print(tmp_path):
+    """compute qwolynes on the CA group: c_ID in thermo columns and fix print
+    formulas is the engine's Q at each output step; the definition is made
+    once per engine; another group or style is refused."""
+    deck = DECK.replace("thermo_style custom step pe ke etotal emol epair f_2 v_E_P",
+                        "compute qw alpha_carbons qwolynes rnative.dat 2 0.15\n"
+                        "thermo_style custom step pe c_qw") \
+               .replace('"${Step} ${E_chain} ${E_P}"', '"${Step} ${Q}"') \
+               .replace("variable Step equal step", "variable Step equal step\nvariable Q equal c_qw")
+    d, engines, screen = run_deck(tmp_path, deck)
+    (eng,) = engines
+    assert [c for c in eng.calls if c[0] == "q_create"] == [("q_create", "qw alpha_carbons qwolynes rnative.dat 2 0.15")]
+    rows = [l.split() for l in screen.splitlines() if l.strip() and l.split()[0].isdigit()]
+    assert [(int(r[0]), float(r[2])) for r in rows] == [(s, 0.5 + 0.01 * s) for s in (0, 5, 10, 12)]
+    lines = (tmp_path / "energy").read_text().splitlines()[1:]
+    assert [[float(t) for t in l.split()] for l in lines] == [[s, 0.5 + 0.01 * s] for s in (0, 5, 10)]
+    for bad, msg in [("compute qw oxygens qwolynes rnative.dat 2 0.15", "CA group"),
+                     ("compute qw alpha_carbons rg", "not supported")]:
+        with pytest.raises(lmp.LammpsError, match=msg):
+            run_deck(tmp_path, deck.replace("compute qw alpha_carbons qwolynes rnative.dat 2 0.15", bad))

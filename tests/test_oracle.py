@@ -129,3 +129,27 @@ def test_oracle_nve_drift_matches_reference(tmp_path, oracle_built):
     assert np.abs(e[:200] - er[:200]).max() < 1e-9 * abs(er[0])
     d, dr = np.abs(e - e[0]).max(), np.abs(er - er[0]).max()
     assert abs(d - dr) <= 0.05 * dr, (d, dr)
+
+
+@pytest.mark.parametrize("name", ["r1r69", "c0"])
+def test_oracle_q_matches_reference(name, tmp_path, oracle_built):
+    """compute qwolynes / qonuchic in all four types: the restatement against
+    the reference computes (compiled in the shim) at the start and the end of
+    the 20-step run."""
+    import make_golden
+    import ref
+
+    files = make_golden.write_q_case(name, str(tmp_path / name))
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", f"q_{name}.npz"))
+    assert make_golden.dir_hash(files["workdir"]) == str(g["inputs_sha256"])
+    x0 = np.load(os.path.join(os.path.dirname(__file__), "golden", f"{name}.npz"))["x0"]
+    o = ref.OracleSystem(files)
+    cwd = os.getcwd()
+    os.chdir(files["workdir"])
+    try:
+        for k, words in enumerate(g["words"]):
+            for x, want in ((x0, g["q0"][k]), (g["xN"], g["qN"][k])):
+                got = o.q(x, str(words))
+                assert abs(got - want) <= 1e-12 * max(abs(want), 1e-3), (str(words), got, want)
+    finally:
+        os.chdir(cwd)
