@@ -273,7 +273,9 @@ template <typename R> class Engine : public EngineBase {
     a.fm.uniform = in.fm.uniform_coef;
     a.fm.nd = in.ff.p.fm_nd;
     a.fm.min_sep = in.ff.p.fm_min_sep;
-    a.fm.groups = fm_groups;
+    // residue groups the fragment-memory kernel walks: those of the launch
+    // extent (on a serving handle the used prefix, not the whole capacity)
+    a.fm.groups = std::min(fm_groups, (n_run() + 31) / 32);
     a.fm.dsplit = fm_dsplit;
     a.tb_data = reinterpret_cast<const double2 *>(tb_data.p);
     a.tb_present = tb_present.p;
