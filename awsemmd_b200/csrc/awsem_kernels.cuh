@@ -806,9 +806,10 @@ template <typename R> __device__ __forceinline__ void pair_pass(const StepArgs<R
   // a time with one atomic reservation: one counter update per 32 entries
   // instead of one per warp iteration (same-address atomics serialise in L2).
   constexpr int kStageWarps = 8;  // warps per block of any caller
-  __shared__ int stage_d[kStageWarps][96], stage_p[kStageWarps][64];
+  __shared__ int stage_d[kStageWarps][96], stage_p[kStageWarps][64], stage_e[kStageWarps][64];
   int *const sd = stage_d[threadIdx.x >> 5], *const spp = stage_p[threadIdx.x >> 5];
-  int nsd = 0, nsp = 0;  // staged entries (warp-uniform)
+  int *const se = stage_e[threadIdx.x >> 5];
+  int nsd = 0, nsp = 0, nse = 0;  // staged entries (warp-uniform)
   // write the first `count` staged entries (count <= 32) to the queue at `region`, move the rest down
   auto flush = [&](int *buf, int &cnt, int count, int *counter, size_t region) {
     int at = 0;
@@ -822,10 +823,60 @@ template <typename R> __device__ __forceinline__ void pair_pass(const StepArgs<R
     __syncwarp();
     cnt -= count;
   };
+  // excluded volume between the beads of listed pair q (1-2 bonded pairs removed)
+  auto ev_of_pair = [&](int q) {
+    const int2 ij = a.pairs[q];
+    const int i = ij.x, j = ij.y;
+    const bool other = s.res_chain[j] != s.res_chain[i];
+    const int dij = j - i;
+    const V3<double> ca_i = bead(s, i, B_CA), ca_j = bead(s, j, B_CA);
+    const unsigned excl = j == i + 1 ? a.excl_next[i] : 0u;
+    const bool shortr = !other && dij < 5;
+    const V3<double> bi[3] = {ca_i, bead(s, i, B_CB), bead(s, i, B_O)};
+    const int tai[3] = {a.atom_type[3 * i], a.atom_type[3 * i + 1], a.atom_type[3 * i + 2]};
+    long long Fi[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+    double ee = 0.0;
+#pragma unroll
+    for (int b1 = 0; b1 < 3; b1++) {
+      const V3<double> bj = b1 == 0 ? ca_j : bead(s, j, b1);
+      const int tb = a.atom_type[3 * j + b1];
+      long long Fj[3] = {0, 0, 0};
+#pragma unroll
+      for (int b0 = 0; b0 < 3; b0++) {
+        if (excl & (1u << (b0 * 3 + b1))) continue;
+        const V3<R> dd = diff<R>(bi[b0], bj);
+        if (norm2(dd) > ev_max_sq) continue;  // beyond every cutoff: no table lookups
+        V3<R> f;
+        const R e = ev_pair(a, tai[b0], tb, shortr, dd, f);
+        if (e == R(0) && f.x == R(0) && f.y == R(0) && f.z == R(0)) continue;
+        ee += (double) e;
+        const long long v[3] = {fix_force((double) f.x), fix_force((double) f.y), fix_force((double) f.z)};
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+          Fi[b0][c] += v[c];
+          Fj[c] -= v[c];
+        }
+      }
+      scatter_fix(s, j, b1, Fj);
+    }
+#pragma unroll
+    for (int b0 = 0; b0 < 3; b0++) scatter_fix(s, i, b0, Fi[b0]);
+    if (ee != 0.0) atomicAdd(e_ev + i, (unsigned long long) fix_force(ee));
+  };
+  // run the first `count` staged EV pairs (count <= 32), one per lane; move the rest down
+  auto ev_batch = [&](int count) {
+    const int q = lane < count ? se[lane] : -1;
+    const int v1 = lane + 32 < nse ? se[lane + 32] : 0;
+    __syncwarp();
+    se[lane] = v1;
+    __syncwarp();
+    nse -= count;
+    if (q >= 0) ev_of_pair(q);
+  };
   // warp-uniform trip count: the queue appends below are warp collectives
   for (int base = sp.t - lane; base < np; base += sp.nthr) {
     const int q = base + lane;
-    bool q_d0 = false, q_d1 = false, q_p = false;  // queue: DSSP O(i), DSSP O(j), P_AP
+    bool q_d0 = false, q_d1 = false, q_p = false, q_e = false;  // queue: DSSP O(i), DSSP O(j), P_AP; stage: EV
     if (q < np) {
     const int2 ij = a.pairs[q];
     const int i = ij.x, j = ij.y;
@@ -894,41 +945,9 @@ template <typename R> __device__ __forceinline__ void pair_pass(const StepArgs<R
       }
     }
     const R rca2 = norm2(diff<R>(ca_i, ca_j));
-    // excluded volume between beads of i and j (1-2 bonded pairs removed)
-    if (evon && rca2 < ev_pre_sq) {
-      const unsigned excl = j == i + 1 ? a.excl_next[i] : 0u;
-      const bool shortr = !other && dij < 5;
-      const V3<double> bi[3] = {ca_i, bead(s, i, B_CB), bead(s, i, B_O)};
-      const int tai[3] = {a.atom_type[3 * i], a.atom_type[3 * i + 1], a.atom_type[3 * i + 2]};
-      long long Fi[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
-      double ee = 0.0;
-#pragma unroll
-      for (int b1 = 0; b1 < 3; b1++) {
-        const V3<double> bj = b1 == 0 ? ca_j : bead(s, j, b1);
-        const int tb = a.atom_type[3 * j + b1];
-        long long Fj[3] = {0, 0, 0};
-#pragma unroll
-        for (int b0 = 0; b0 < 3; b0++) {
-          if (excl & (1u << (b0 * 3 + b1))) continue;
-          const V3<R> dd = diff<R>(bi[b0], bj);
-          if (norm2(dd) > ev_max_sq) continue;  // beyond every cutoff: no table lookups
-          V3<R> f;
-          const R e = ev_pair(a, tai[b0], tb, shortr, dd, f);
-          if (e == R(0) && f.x == R(0) && f.y == R(0) && f.z == R(0)) continue;
-          ee += (double) e;
-          const long long v[3] = {fix_force((double) f.x), fix_force((double) f.y), fix_force((double) f.z)};
-#pragma unroll
-          for (int c = 0; c < 3; c++) {
-            Fi[b0][c] += v[c];
-            Fj[c] -= v[c];
-          }
-        }
-        scatter_fix(s, j, b1, Fj);
-      }
-#pragma unroll
-      for (int b0 = 0; b0 < 3; b0++) scatter_fix(s, i, b0, Fi[b0]);
-      if (ee != 0.0) atomicAdd(e_ev + i, (unsigned long long) fix_force(ee));
-    }
+    // excluded volume between beads of i and j: staged (below), so that the
+    // few pairs this close run their 3 x 3 bead loop with full warps
+    q_e = evon && rca2 < ev_pre_sq;
     // DSSP (fix_backbone.cpp:8064-8094): O(i) with N-H(j), and O(j) with N-H(i)
     if ((T & T_DSSP) && (other || dij > 2) && rca2 < dssp_pre_sq) {
       q_d0 = !(flj & (R_PRO | R_FIRST)) && !(fli & R_LAST) &&
@@ -941,19 +960,23 @@ template <typename R> __device__ __forceinline__ void pair_pass(const StepArgs<R
     }
     // stage this iteration's queue entries (at most 64 DSSP and 32 P_AP)
     const unsigned m0 = __ballot_sync(0xffffffffu, q_d0), m1 = __ballot_sync(0xffffffffu, q_d1),
-                   mp = __ballot_sync(0xffffffffu, q_p);
+                   mp = __ballot_sync(0xffffffffu, q_p), me = __ballot_sync(0xffffffffu, q_e);
     const unsigned below = (1u << lane) - 1u;
     if (q_d0) sd[nsd + __popc(m0 & below)] = q;
     if (q_d1) sd[nsd + __popc(m0) + __popc(m1 & below)] = ~q;
     if (q_p) spp[nsp + __popc(mp & below)] = q;
+    if (q_e) se[nse + __popc(me & below)] = q;
     nsd += __popc(m0) + __popc(m1);
     nsp += __popc(mp);
+    nse += __popc(me);
     __syncwarp();
     while (nsd >= 32) flush(sd, nsd, 32, &a.nl->n_dssp, qd);
     if (nsp >= 32) flush(spp, nsp, 32, &a.nl->n_pap, qp);
+    if (nse >= 32) ev_batch(32);
   }
   if (nsd > 0) flush(sd, nsd, nsd, &a.nl->n_dssp, qd);
   if (nsp > 0) flush(spp, nsp, nsp, &a.nl->n_pap, qp);
+  if (nse > 0) ev_batch(nse);
 }
 
 template <typename R> __global__ void __launch_bounds__(128, 6) k_pair(StepArgs<R> a, FFParams p)
