@@ -1004,7 +1004,7 @@ template <typename R> __device__ __forceinline__ void hbond_pass(const StepArgs<
   }
 }
 
-template <typename R> __global__ void __launch_bounds__(128) k_hbond(StepArgs<R> a, FFParams p)
+template <typename R> __global__ void __launch_bounds__(128, 6) k_hbond(StepArgs<R> a, FFParams p)
 {
   hbond_pass(a, p, grid_span());
 }
