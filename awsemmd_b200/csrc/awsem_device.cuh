@@ -361,12 +361,13 @@ template <typename R> __device__ R rama_term(const DevSys<R> &s, const FFParams 
 // Returns the energy; writes the density-derivative coefficients xi1, xi2.
 template <typename R>
 __device__ R helix_pair(const DevSys<R> &s, const FFParams &p, int i, int j, double sh_i, double shp_i, double sh_j,
-                        double shp_j, double &xi1, double &xi2)
+                        double shp_j, double &xi1, double &xi2, unsigned *gate = nullptr)
 {
   V3<double> oi = bead(s, i, B_O);
   V3<R> xNO = diff<R>(oi, bead(s, j, B_N)), xHO = diff<R>(oi, bead(s, j, B_H));
   R R_NO = m_sqrt(norm2(xNO));
   if (R_NO > R(p.helix_cutoff)) return R(0);
+  if (gate) *gate = 1u;
   R R_HO = m_sqrt(norm2(xHO));
   const double *T = s.tables;
   (void) T;
@@ -396,12 +397,16 @@ __device__ R helix_pair(const DevSys<R> &s, const FFParams &p, int i, int j, dou
 }
 
 // compute_dssp_hdrgn(i, j): O of residue i, N-H of residue j.
-// fix_backbone.cpp:2902-3277.  Returns the energy and scatters the forces.
-template <typename R> __device__ R dssp_term(const DevSys<R> &s, const FFParams &p, int i, int j)
+// fix_backbone.cpp:2902-3277.  Returns the energy and scatters the forces;
+// *gate (optional) receives the gates passed: bit 0 r_NO <= cutoff (:2904),
+// bit 1 both nu switches >= 1e-4 (:3052).
+template <typename R> __device__ R dssp_term(const DevSys<R> &s, const FFParams &p, int i, int j,
+                                             unsigned *gate = nullptr)
 {
   V3<double> oi = bead(s, i, B_O);
   R rno = m_sqrt(norm2(diff<R>(oi, bead(s, j, B_N))));
   if (rno > R(p.dssp_cut)) return R(0);
+  if (gate) *gate = 1u;
   const int *fl = s.res_flags, *ty = s.res_type;
   int ic = s.res_chain[i], jc = s.res_chain[j];
   int i_start = s.chain_start[ic], i_end = s.chain_end[ic];
@@ -484,6 +489,7 @@ template <typename R> __device__ R dssp_term(const DevSys<R> &s, const FFParams 
     }
   }
   if (nu[0] < R(1e-4) || nu[1] < R(1e-4)) return R(0);
+  if (gate) *gate = 3u;
   bool on[4] = {true, i_rep, i_AP, i_P};
   const int acc[4] = {i, i, j, j}, don[4] = {j, j + 1, i, i + 2};
   R theta[4], prd[4][2];
@@ -546,8 +552,11 @@ template <typename R> __device__ __forceinline__ void pap_nu(const DevSys<R> &s,
   }
 }
 
-// compute_P_AP_potential(i, j) with i < j, fix_backbone.cpp:3279-3383
-template <typename R> __device__ R pap_term(const DevSys<R> &s, const FFParams &p, int i, int j)
+// compute_P_AP_potential(i, j) with i < j, fix_backbone.cpp:3279-3383.
+// *gate (optional): bit 0 nu(i, j) >= 1e-12 (:3281), bits 1-3 the classes
+// antiparallel medium, antiparallel long, parallel (:3290-3295).
+template <typename R> __device__ R pap_term(const DevSys<R> &s, const FFParams &p, int i, int j,
+                                            unsigned *gate = nullptr)
 {
   R nu_ij, prd_ij;
   V3<R> d0;
@@ -563,6 +572,7 @@ template <typename R> __device__ R pap_term(const DevSys<R> &s, const FFParams &
                  (!same && i + dd < s.n_res && j - dd >= 0 && s.res_chain[i + dd] == ic && s.res_chain[j - dd] == jc);
   bool par = (same && i < ie - (p.i_med_max + 1 + dd) && j >= i + (p.i_med_max + 1) && j < ie - dd) ||
              (!same && i + dd < s.n_res && j + dd < s.n_res && s.res_chain[i + dd] == ic && s.res_chain[j + dd] == jc);
+  if (gate) *gate = 1u | (ap_med ? 2u : 0u) | (ap_long ? 4u : 0u) | (par ? 8u : 0u);
   const double *beta = s.aps + (size_t) (p.n_rama - 1) * s.n_res;
   bool bp = p.n_rama > 0 && beta[i] == 1.0 && beta[j] == 1.0;
   R E = 0;

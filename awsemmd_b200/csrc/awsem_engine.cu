@@ -109,6 +109,7 @@ class EngineBase {
   virtual void energies(int rep, double *out) = 0;
   virtual void forces(int rep, double *f_ext) = 0;
   virtual void residue_arrays(int rep, double *out) = 0;
+  virtual long long debug_selections(long long step, const double *x_ext, unsigned long long *keys, long long cap) = 0;
   virtual void nl_stats(int *nbuilds, double *radius, int *maxc, int *overflow) = 0;
   virtual void profile(int reps, double *ms) = 0;
   virtual void autotune(int reps, int *chosen) = 0;
@@ -308,7 +309,39 @@ template <typename R> class Engine : public EngineBase {
     a.sys_end = sys_end.p;
     a.sys_seed = sys_seed.p;
     a.slot_run = slot_run.p;
+    a.sel = sel_cap > 0 ? sel_keys.p : nullptr;
+    a.sel_n = sel_count.p;
+    a.sel_cap = sel_cap;
     return a;
+  }
+
+  // selection records of one evaluation (awsem_debug_selections)
+  DBuf<unsigned long long> sel_keys, sel_count;
+  long long sel_cap = 0;
+
+  long long debug_selections(long long st, const double *x_ext, unsigned long long *keys, long long cap) override
+  {
+    need_single("awsem_debug_selections");
+    if (cap < 0) throw std::invalid_argument("negative selection capacity");
+    sel_keys.alloc((size_t) std::max<long long>(cap, 1));
+    sel_count.alloc(1);
+    sel_count.zero(s0);
+    std::vector<double> f((size_t) 3 * natoms(), 0.0);
+    sel_cap = std::max<long long>(cap, 1);
+    try {
+      compute(st, x_ext, f.data(), nullptr, groups_all);
+    } catch (...) {
+      sel_cap = 0;
+      throw;
+    }
+    sel_cap = 0;
+    unsigned long long got = 0;
+    CK(cudaMemcpy(&got, sel_count.p, sizeof got, cudaMemcpyDeviceToHost));
+    const long long keep = std::min<long long>((long long) got, cap);
+    if (keep > 0) CK(cudaMemcpy(keys, sel_keys.p, sizeof(unsigned long long) * keep, cudaMemcpyDeviceToHost));
+    sel_keys.release();
+    sel_count.release();
+    return (long long) got;
   }
 
   void setup() override
@@ -2344,6 +2377,21 @@ int awsem_residue_arrays(awsem_system *sys, double *out)
 {
   if (!ready(sys) || !out) return AWSEM_EINVAL;
   return guarded([&] { sys->eng->residue_arrays(0, out); });
+}
+
+int awsem_debug_selections(awsem_system *sys, long long step, const double *x, unsigned long long *keys,
+                           long long cap, long long *count)
+{
+  if (!ready(sys) || !x || (cap > 0 && !keys) || !count) return AWSEM_EINVAL;
+  long long got = 0;
+  int rc = guarded([&] { got = sys->eng->debug_selections(step, x, keys, cap); });
+  *count = got;
+  if (rc == AWSEM_OK && got > cap) {
+    g_last_error = "selection records exceed the capacity given (" + std::to_string(cap) + " < " +
+                   std::to_string(got) + ")";
+    return AWSEM_ESTATE;
+  }
+  return rc;
 }
 
 int awsem_neighbor_stats(awsem_system *sys, int *nbuilds, double *radius, int *max_count, int *overflow)

@@ -26,6 +26,7 @@
 
 #include "awsem_device.cuh"
 #include "awsem_fragmem.cuh"
+#include "awsem_gpu.h"
 
 namespace awsem {
 namespace dev {
@@ -133,6 +134,9 @@ template <typename R> struct StepArgs {
   const int *res_sys, *sys_begin, *sys_end;
   const unsigned long long *sys_seed;
   const SlotRun *slot_run;
+  // selection records (awsem_debug_selections; null in steps): keys, count, capacity
+  unsigned long long *sel, *sel_n;
+  long long sel_cap;
 };
 
 enum Group { G_FIX = 1, G_PAIR = 2, G_BOND = 4 };
@@ -146,6 +150,16 @@ struct Span {
 __device__ __forceinline__ Span grid_span()
 {
   return Span{(int) (blockIdx.x * blockDim.x + threadIdx.x), (int) (gridDim.x * blockDim.x)};
+}
+
+// one selection record (AWSEM_SEL_* key, awsem_gpu.h) when the evaluation records them
+template <typename R> __device__ __forceinline__ void sel_rec(const StepArgs<R> &a, int kind, int aux, int i, int j)
+{
+  if (!a.sel) return;
+  const unsigned long long k = atomicAdd(a.sel_n, 1ull);
+  if (k < (unsigned long long) a.sel_cap)
+    a.sel[k] = (unsigned long long) kind << 56 | (unsigned long long) aux << 44 | (unsigned long long) i << 22 |
+               (unsigned long long) j;
 }
 
 __device__ __forceinline__ void atomic_max_f(float *addr, float v)
@@ -572,6 +586,7 @@ template <typename R> __device__ __forceinline__ void density_pass(const StepArg
       const unsigned long long v = (unsigned long long) fix_dens(th);
       atomicAdd(aw + i, v);
       atomicAdd(aw + j, v);
+      sel_rec(a, AWSEM_SEL_DENS_WATER, 0, i, j);
     }
     if (helix && rsq > p.h_rmin_sq && rsq < p.h_rmax_sq) {
       double th, pr;
@@ -579,6 +594,7 @@ template <typename R> __device__ __forceinline__ void density_pass(const StepArg
       const unsigned long long v = (unsigned long long) fix_dens(th);
       atomicAdd(ah + i, v);
       atomicAdd(ah + j, v);
+      sel_rec(a, AWSEM_SEL_DENS_HELIX, 0, i, j);
     }
   }
 }
@@ -602,7 +618,8 @@ __device__ __forceinline__ void switching(double rho, double kappa_sigma, double
 // pair_excluded_volume.cpp:50-138).  Returns the pair energy and the force
 // on bead a (the force on b is its negative).
 template <typename R>
-__device__ __forceinline__ R ev_pair(const StepArgs<R> &a, int ta, int tb, bool short_range, V3<R> d, V3<R> &f)
+__device__ __forceinline__ R ev_pair(const StepArgs<R> &a, int ta, int tb, bool short_range, V3<R> d, V3<R> &f,
+                                     bool *hit = nullptr)
 {
   int N = a.ntypes + 1;
   double pref = a.ev_pref[ta * N + tb];
@@ -611,6 +628,7 @@ __device__ __forceinline__ R ev_pair(const StepArgs<R> &a, int ta, int tb, bool 
   R rc = (R) (short_range ? a.ev_cs[ta * N + tb] : a.ev_cl[ta * N + tb]);
   R r = m_sqrt(norm2(d));
   if (!(r < rc)) return R(0);
+  if (hit) *hit = true;
   R dr = r - rc;
   R pw = R(1);
   for (int k = 1; k < a.ev_p; k++) pw *= dr;  // dr^(p-1)
@@ -688,7 +706,9 @@ template <typename R> __device__ __forceinline__ void residue_one(const StepArgs
     if (norm2(d) < R(p.helix_cutoff_sq)) {
       double shj, shpj;
       switching(density(a, 1, j), p.helix_kappa_sigma, p.helix_treshold, shj, shpj);
-      eh = (double) helix_pair(sd, p, i, j, sh, shp, shj, shpj, x1, x2);
+      unsigned gate = 0;
+      eh = (double) helix_pair(sd, p, i, j, sh, shp, shj, shpj, x1, x2, &gate);
+      sel_rec(a, AWSEM_SEL_HELIX_PAIR, (int) gate, i, j);
     }
   }
   a.xi1[i] = x1;
@@ -709,8 +729,10 @@ template <typename R> __device__ __forceinline__ void residue_one(const StepArgs
     for (int b1 = b0 + 1; b1 < 3; b1++) {
       if (ex_self & (1u << (b0 * 3 + b1))) continue;
       V3<R> f;
+      bool hit = false;
       R e = ev_pair(a, a.atom_type[3 * i + b0], a.atom_type[3 * i + b1], true,
-                    diff<R>(bead(s, i, b0), bead(s, i, b1)), f);
+                    diff<R>(bead(s, i, b0), bead(s, i, b1)), f, &hit);
+      if (hit) sel_rec(a, AWSEM_SEL_EV, 3 * b0 + b1, i, i);
       if (e != R(0) || f.x != R(0) || f.y != R(0) || f.z != R(0)) {
         ev += (double) e;
         scatter(s, i, b0, f);
@@ -753,6 +775,7 @@ template <typename R> __device__ __forceinline__ void water_xi_pass(const StepAr
       const double g0 = W[w * 800 + (ti * 20 + tj) * 2], g1 = W[w * 800 + (ti * 20 + tj) * 2 + 1];
       // the reference's `!fabs(g0 - g1) < delta` holds exactly when g0 != g1
       if (g0 != g1 && rsq > R(p.w_rmin_sq[w]) && rsq < R(p.w_rmax_sq[w])) {
+        sel_rec(a, AWSEM_SEL_XI_WATER, w, i, j);
         R th, pr;
         well_theta(m_sqrt(rsq), R(p.w_rmin_th[w]), R(p.w_rmax_th[w]), R(p.water_kappa), R(p.well_rmin[w]),
                    R(p.well_rmax[w]), th, pr);
@@ -847,7 +870,9 @@ template <typename R> __device__ __forceinline__ void pair_pass(const StepArgs<R
         const V3<R> dd = diff<R>(bi[b0], bj);
         if (norm2(dd) > ev_max_sq) continue;  // beyond every cutoff: no table lookups
         V3<R> f;
-        const R e = ev_pair(a, tai[b0], tb, shortr, dd, f);
+        bool hit = false;
+        const R e = ev_pair(a, tai[b0], tb, shortr, dd, f, &hit);
+        if (hit) sel_rec(a, AWSEM_SEL_EV, 3 * b0 + b1, i, j);
         if (e == R(0) && f.x == R(0) && f.y == R(0) && f.z == R(0)) continue;
         ee += (double) e;
         const long long v[3] = {fix_force((double) f.x), fix_force((double) f.y), fix_force((double) f.z)};
@@ -904,6 +929,7 @@ template <typename R> __device__ __forceinline__ void pair_pass(const StepArgs<R
         for (int w = 0; w < p.n_wells; w++) {
           if (!p.well_flag[w]) continue;
           if (sep && rsq > R(p.w_rmin_sq[w]) && rsq < R(p.w_rmax_sq[w])) {
+            sel_rec(a, AWSEM_SEL_WATER, w, i, j);
             const double g0 = W[w * 800 + (ti * 20 + tj) * 2], g1 = W[w * 800 + (ti * 20 + tj) * 2 + 1];
             const double sg = fabs(g0 - g1) < 1e-5 ? 0.5 * (g0 + g1) : g0 + (g1 - g0) * a.sig_w[i] * a.sig_w[j];
             R th, pr;
@@ -920,8 +946,10 @@ template <typename R> __device__ __forceinline__ void pair_pass(const StepArgs<R
         }
         if (in0) {
           const double xi_i = water_xi(a, i), xi_j = water_xi(a, j);
-          if (fabs(xi_i) > 1e-8) force = madd(pr0, R(xi_i), force);
-          if (fabs(xi_j) > 1e-8) force = madd(pr0, R(xi_j), force);
+          const int on = (fabs(xi_i) > 1e-8 ? 1 : 0) | (fabs(xi_j) > 1e-8 ? 2 : 0);
+          if (on & 1) force = madd(pr0, R(xi_i), force);
+          if (on & 2) force = madd(pr0, R(xi_j), force);
+          if (on) sel_rec(a, AWSEM_SEL_XI_FORCE, on, i, j);
         }
       }
       if ((T & T_BURIAL) && in0) force = madd(R(a.bur[i] + a.bur[j]), pr0, force);
@@ -930,6 +958,7 @@ template <typename R> __device__ __forceinline__ void pair_pass(const StepArgs<R
         if (i - dh >= 0) fac += a.xi2[i - dh];
         if (j - dh >= 0) fac += a.xi2[j - dh];
         if (fabs(fac) > 1e-6) {
+          sel_rec(a, AWSEM_SEL_HELIX_FORCE, 0, i, j);
           R th, pr;
           well_theta(r, R(p.h_rmin_th), R(p.h_rmax_th), R(p.helix_kappa), R(p.helix_rmin), R(p.helix_rmax), th, pr);
           force = madd(-R(fac), pr, force);
@@ -998,7 +1027,9 @@ template <typename R> __device__ __forceinline__ void hbond_pass(const StepArgs<
     const int q = d ? a.hbq[t] : a.hbq[(size_t) 2 * a.pcap + (t - nd)];
     const int2 ij = a.pairs[q < 0 ? ~q : q];
     const int i = q < 0 ? ij.y : ij.x, j = q < 0 ? ij.x : ij.y;
-    const R e = d ? dssp_term(s, p, i, j) : pap_term(s, p, i, j);
+    unsigned gate = 0;
+    const R e = d ? dssp_term(s, p, i, j, &gate) : pap_term(s, p, i, j, &gate);
+    sel_rec(a, d ? AWSEM_SEL_DSSP : AWSEM_SEL_PAP, (int) gate, i, j);
     if (e != R(0))
       atomicAdd((unsigned long long *) (a.e_fix + (d ? 0 : (size_t) n) + i), (unsigned long long) fix_force((double) e));
   }

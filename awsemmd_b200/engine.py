@@ -102,6 +102,7 @@ def load_library(path: str = LIB_PATH):
     lib.awsem_energies.argtypes = [vp, vp]
     lib.awsem_forces.argtypes = [vp, vp]
     lib.awsem_residue_arrays.argtypes = [vp, vp]
+    lib.awsem_debug_selections.argtypes = [vp, C.c_longlong, vp, vp, C.c_longlong, C.POINTER(C.c_longlong)]
     lib.awsem_neighbor_stats.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_double), C.POINTER(C.c_int),
                                          C.POINTER(C.c_int)]
     lib.awsem_last_run_ms.argtypes = [vp]
@@ -276,6 +277,21 @@ class AwsemSystem:
         out = np.zeros((self.nres, 8))
         _check(self.lib, self.lib.awsem_residue_arrays(self.h, _ptr(out)), "awsem_residue_arrays")
         return out
+
+    def selections(self, x: np.ndarray, step: int = 0) -> np.ndarray:
+        """Sorted AWSEM_SEL_* selection keys of one evaluation at x
+        (awsem_debug_selections; kind << 56 | aux << 44 | i << 22 | j)"""
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        cap = 96 * self.nres + 4096
+        while True:
+            keys = np.zeros(cap, dtype=np.uint64)
+            got = C.c_longlong()
+            rc = self.lib.awsem_debug_selections(self.h, step, _ptr(x), _ptr(keys), cap, C.byref(got))
+            if rc == 0:
+                return np.sort(keys[:got.value])
+            if got.value <= cap:
+                _check(self.lib, rc, "awsem_debug_selections")
+            cap = got.value + 1024
 
     def neighbor_stats(self) -> dict:
         nb, mc, ov = C.c_int(), C.c_int(), C.c_int()

@@ -279,15 +279,41 @@ def algorithmic_bytes(kernel: str, info) -> float:
 # --------------------------------------------------------------------------
 # CPU reference (the shim-hosted reference FixBackbone + PairExcludedVolume)
 
+# categories of the reference's timer.log (final_log_output, fix_backbone.cpp:1186-1206)
+TIMER_NAMES = ["Chain", "Shake", "Chi", "Rama", "Vexcluded", "DSSP", "PAP", "Water", "Burial", "Helix", "AHM-Go",
+               "Frag_Mem", "Vec_FM", "Membrane", "SSB", "DH", "Frust_Analysis", "Pair", "Pair_Double_Loop1",
+               "Pair_Single_Loop", "Pair_Double_Loop2", "Pair_Double_Loop3", "Total"]
+# the GPU kernels that do the work of each timed reference section
+TIMER_TO_KERNELS = {"Chain": "residue", "Chi": "residue", "Rama": "residue", "DSSP": "pair (detection) + hbond",
+                    "PAP": "pair (detection) + hbond", "Frag_Mem": "fragmem", "Pair_Double_Loop1": "density",
+                    "Pair_Single_Loop": "residue (switching, burial, helical pairs)", "Pair_Double_Loop2": "water_xi",
+                    "Pair_Double_Loop3": "pair", "Vexcluded": "pair + residue"}
+
+
+def read_timer_log(path: str) -> dict:
+    out = {}
+    try:
+        for line in open(path):
+            name, _, val = line.partition(" time = ")
+            if val:
+                out[name.strip()] = float(val)
+    except OSError:
+        pass
+    return out
+
+
 def _ref_worker(args):
-    """Runs in a spawned process: reference MD on a few c3 replicas."""
+    """Runs in a spawned process: reference MD on a list of c3 replicas.
+    Returns residue-steps, the seconds of its timed MD steps, and the sum of
+    the replicas' timer.log sections (the reference's own per-term clocks,
+    written when the fix is destroyed)."""
     lens_seeds, md, tmp = args
     sys.path.insert(0, ROOT)
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import ref
     from awsemmd_b200 import synth
 
-    done_res_steps, t_total = 0, 0.0
+    done_res_steps, t_total, timers = 0, 0.0, {}
     for L, seed in lens_seeds:
         c = c3_chain(L, seed)
         files = synth.write_chain_arrays(c, os.path.join(tmp, f"r{seed}"))
@@ -298,26 +324,50 @@ def _ref_worker(args):
         t_total += time.perf_counter() - t0
         done_res_steps += L * md
         r.close()
-    return done_res_steps, t_total
+        for k, v in read_timer_log(os.path.join(files["workdir"], "timer.log")).items():
+            timers[k] = timers.get(k, 0.0) + v
+    return done_res_steps, t_total, timers
 
 
-def reference_c3(n_procs: int, per_proc: int, md: int):
-    """Aggregate residue-steps/s of the reference over `n_procs` host cores,
-    each running `per_proc` replicas of the workload (a bounded sample)."""
-    lens = c3_lengths(1024)
-    rng = np.random.default_rng(1)
-    pick = rng.choice(1024, size=n_procs * per_proc, replace=False)
-    jobs = [[(lens[k], c3_seed(k)) for k in pick[p::n_procs]] for p in range(n_procs)]
+def reference_c3(n_procs: int, md: int, n_replicas: int = 1024, sample: int | None = None):
+    """Aggregate residue-steps/s of the reference over `n_procs` host
+    processes (one per core).  Every replica of the workload (or a random
+    `sample` of them) runs `md` MD steps; replicas are dealt to the processes
+    longest first to the least-loaded one, each process times only its MD
+    steps, and the slowest process sets the aggregate."""
+    lens = c3_lengths(n_replicas)
+    ks = list(range(n_replicas))
+    if sample is not None:
+        ks = [int(k) for k in np.random.default_rng(1).choice(n_replicas, size=sample, replace=False)]
+    jobs, load = [[] for _ in range(n_procs)], [0] * n_procs
+    for k in sorted(ks, key=lambda k: -lens[k]):
+        p = int(np.argmin(load))
+        jobs[p].append((lens[k], c3_seed(k)))
+        load[p] += lens[k]
+    jobs = [j for j in jobs if j]
     with tempfile.TemporaryDirectory() as tmp:
         ctx = mp.get_context("spawn")
         t0 = time.perf_counter()
-        with ctx.Pool(n_procs) as pool:
+        with ctx.Pool(len(jobs)) as pool:
             out = pool.map(_ref_worker, [(j, md, tmp) for j in jobs])
         wall = time.perf_counter() - t0
     res_steps = sum(o[0] for o in out)
     busy = max(o[1] for o in out)
-    # each process times only its MD steps; the slowest sets the aggregate
-    return res_steps / busy, res_steps, busy, wall
+    timers = {}
+    for o in out:
+        for k, v in o[2].items():
+            timers[k] = timers.get(k, 0.0) + v
+    return res_steps / busy, res_steps, busy, wall, timers, len(ks)
+
+
+def timer_breakdown(timers: dict) -> dict:
+    """The reference's timer.log sections as shares of its timed total, each
+    with the GPU kernels that do that work here."""
+    total = timers.get("Total", 0.0)
+    if total <= 0:
+        return {}
+    return {k: {"share": round(timers[k] / total, 4), "gpu": TIMER_TO_KERNELS.get(k, "")}
+            for k in TIMER_NAMES[:-1] if timers.get(k, 0.0) > 0}
 
 
 def reference_c1(md: int, warmup: int, steps: int):
@@ -412,28 +462,36 @@ def reference_arm(args, dist: Dist):
     if args.workload == "c2":
         print(json.dumps({"impl": "reference", "unavailable": "configuration 2 does not fit a host: " + C2_CPU_NOTE}))
         return
+    timers = None
     if args.workload == "c3":
-        md = 10
-        # a bounded sample: every core runs a few random replicas for md steps
-        value, res_steps, busy, wall = reference_c3(cores, max(2, (args.steps + args.warmup) // 4), md)
-        ms = 1e3 * busy / max(args.steps, 1)
-        sample = (f"{res_steps} residue-steps: {cores} processes (one per host core), each running a random "
-                  f"subset of the 1,024 replicas for {md} MD steps (+1 warm-up step); reference FixBackbone + "
-                  f"PairExcludedVolume compiled -O2 against the LAMMPS-API shim, 1 rank per process")
+        md = args.md_steps
+        # the whole workload: every replica for the repo arm's MD steps per bench step
+        value, res_steps, busy, wall, tm, nrep = reference_c3(cores, md, args.replicas)
+        timers = timer_breakdown(tm)
+        ms = 1e3 * busy
+        steps = 1
+        sample = (f"the whole workload once: all {nrep} replicas x {md} MD steps ({res_steps} residue-steps, one "
+                  f"bench step of the repo arm; +1 untimed warm-up step each), dealt longest first over {cores} "
+                  f"processes (one per host core); reference FixBackbone + PairExcludedVolume compiled -O2 "
+                  f"against the LAMMPS-API shim, 1 rank per process; slowest process's MD time {busy:.1f} s, "
+                  f"wall {wall:.1f} s")
     else:
         md = 5
         value, busy = reference_c1(md, args.warmup, args.steps)
         cores = 1
         ms = 1e3 * busy / args.steps
+        steps = args.steps
         sample = f"{md} MD steps per bench step of the 2,000-residue system, 1 core, 1 rank"
     line = {"metric": "residue-steps/s", "value": value, "unit": "residue-steps/s", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "steps": steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
             "config": {"workload": workload_text(args), "md_steps_per_step": md,
                        "parallelism": f"{cores} host processes x 1 MPI rank (serial reference; no MPI in the image)"},
             "cpu_baseline": {"value": value, "unit": "residue-steps/s", "cores": cores, "kind": "reference",
                              "sample": sample},
             "e2e": {"value": value, "unit": "residue-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if timers:
+        line["reference_timer_log"] = timers
     print(json.dumps(line))
 
 
@@ -601,11 +659,12 @@ def main():
     if dist.rank == 0 and dist.world == 1 and not args.no_baseline:
         try:
             if args.workload == "c3":
-                v, rs, busy, wall = reference_c3(1, 3, 5)
+                v, rs, busy, wall, tm, nrep = reference_c3(1, md, args.replicas, sample=16)
                 base = {"value": v, "unit": "residue-steps/s", "cores": 1, "kind": "reference",
-                        "sample": f"3 random replicas x 5 MD steps ({rs} residue-steps, {busy:.1f} s) on 1 host "
-                                  f"core; reference FixBackbone + PairExcludedVolume compiled -O2 against the "
-                                  f"LAMMPS-API shim, 1 MPI rank"}
+                        "sample": f"{nrep} random replicas x {md} MD steps ({rs} residue-steps, {busy:.1f} s) on 1 "
+                                  f"host core; reference FixBackbone + PairExcludedVolume compiled -O2 against the "
+                                  f"LAMMPS-API shim, 1 MPI rank",
+                        "reference_timer_log": timer_breakdown(tm)}
             elif args.workload == "c2":
                 base = {"value": None, "unit": "residue-steps/s", "cores": 1, "kind": "reference",
                         "sample": "not runnable: " + C2_CPU_NOTE}

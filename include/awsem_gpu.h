@@ -49,6 +49,44 @@ extern "C" {
 
 typedef struct awsem_system awsem_system;
 
+/* Selection records (awsem_debug_selections): one 64-bit key per selected
+ * item, key = kind << 56 | aux << 44 | i << 22 | j, with residue indices
+ * i, j (internal order: the data file's residues in id order).  These are
+ * the discrete decisions of the reference's pair passes, each at the line
+ * that takes it in src/fix_backbone.cpp:
+ *   DENS_WATER  (i<j) contact beads inside water well 0's support, |i-j|>1
+ *               or another chain (DL1 :7759)
+ *   DENS_HELIX  the same for the helix well (DL1 :7768)
+ *   XI_WATER    aux = well: gamma0 != gamma1, separated, inside the well's
+ *               support (DL2 :7925)
+ *   WATER       aux = well: separated, inside the well's support (DL3 :8009)
+ *   XI_FORCE    pair inside well 0's support with |xi_water(i)| > 1e-8
+ *               (aux bit 0) or |xi_water(j)| > 1e-8 (bit 1) (:8027, :8033)
+ *   HELIX_FORCE pair inside the helix support with |xi-helix sum| > 1e-6 (:8052)
+ *   HELIX_PAIR  (i, i + helix_i_diff): |O_i - N_j|^2 < cutoff^2 (:7864);
+ *               aux bit 0: |O_i - N_j| <= cutoff as well (:3708)
+ *   DSSP        (acceptor O of i, donor N-H of j): candidate (:8064-8094);
+ *               aux bit 0: r_NO <= cutoff (:2904), bit 1: both nu switches
+ *               >= 1e-4 (:3052)
+ *   PAP         (i<j) CA pair inside the P_AP cutoff (:8096-8103) and
+ *               separated enough for some P_AP class; aux bit 0:
+ *               nu(i, j) >= 1e-12 (:3281), bits 1-3: antiparallel medium,
+ *               antiparallel long, parallel (:3290-3295)
+ *   EV          bead pair (i, b0), (j, b1), i <= j, inside its pair
+ *               vexcluded cutoff with a non-zero prefactor
+ *               (src/pair_excluded_volume.cpp:98-110); aux = 3 b0 + b1
+ *               (beads 0 CA, 1 CB or H-beta, 2 O) */
+#define AWSEM_SEL_DENS_WATER 1
+#define AWSEM_SEL_DENS_HELIX 2
+#define AWSEM_SEL_XI_WATER 3
+#define AWSEM_SEL_WATER 4
+#define AWSEM_SEL_XI_FORCE 5
+#define AWSEM_SEL_HELIX_FORCE 6
+#define AWSEM_SEL_HELIX_PAIR 7
+#define AWSEM_SEL_DSSP 8
+#define AWSEM_SEL_PAP 9
+#define AWSEM_SEL_EV 10
+
 typedef struct awsem_run_params {
   double dt;                 /* fs (units real) */
   int langevin;              /* 0: fix nve only; 1: fix nve + fix langevin */
@@ -201,6 +239,19 @@ int awsem_forces(awsem_system *sys, double *f);
  * rho_water, rho_helix, xi_water, xi1_helix, xi2_helix, burial coefficient,
  * sigma_water, sigma_helix. */
 int awsem_residue_arrays(awsem_system *sys, double *out);
+
+/* One force evaluation of a single-system handle at positions x (as
+ * awsem_compute with AWSEM_TERMS_ALL) that also records its selections
+ * (AWSEM_SEL_* keys above, in no particular order) into keys[cap].  *count
+ * receives the number recorded; when it exceeds cap only the first cap
+ * keys are stored and the call returns AWSEM_ESTATE.  The evaluation
+ * reuses the handle's pair list when it is still valid, as a step does.  A
+ * diagnostic for parity tests: the reference keeps these decisions inside
+ * compute_pair (src/fix_backbone.cpp:7677-8135), compute_dssp_hdrgn (:2902),
+ * compute_P_AP_potential (:3279), compute_helix_dtheta_pair (:3706) and
+ * PairExcludedVolume::compute (src/pair_excluded_volume.cpp:50-138). */
+int awsem_debug_selections(awsem_system *sys, long long step, const double *x, unsigned long long *keys,
+                           long long cap, long long *count);
 
 /* Pair-list statistics: builds so far, current list radius (A), largest
  * number of higher-numbered partners of one residue, overflow marker (0 when

@@ -20,6 +20,7 @@
    The restatement is checked against the reference compiled against the
    LAMMPS-API shim (oracle/_ref) on the same inputs. */
 #include "awsem_oracle.h"
+#include "../include/awsem_gpu.h"
 
 #include <cmath>
 #include <cstdint>
@@ -70,6 +71,16 @@ inline double uniform01(uint64_t seed, int64_t step, int64_t tag, int comp)
   uint64_t r = mix64(key ^ ((uint64_t) tag * 4ULL + (uint64_t) comp));
   return (double) (r >> 11) * (1.0 / 9007199254740992.0);
 }
+
+/* selection keys: kind << 56 | aux << 44 | i << 22 | j (awsem_gpu.h) */
+inline uint64_t sel_key(int kind, int aux, int i, int j)
+{
+  return (uint64_t) kind << 56 | (uint64_t) aux << 44 | (uint64_t) i << 22 | (uint64_t) j;
+}
+/* reference cache entries (oracle and reference host only) */
+enum { TOUCH_WELL = 32, TOUCH_HWELL = 33, TOUCH_RNO = 34, TOUCH_RHO = 35, TOUCH_NU = 36 };
+/* v within 2e-6 (relative) of the threshold t: FP32 geometry may decide otherwise */
+inline bool near_thr(double v, double t) { return fabs(v - t) <= 2e-6 * fabs(t); }
 
 std::vector<std::string> words(const std::string &s)
 {
@@ -389,13 +400,32 @@ struct System {
   std::vector<double> rho_w, rho_h, sig_w, sigp_w, sig_h, sigp_h, xi_w, xi1, xi2, bur;
   double E[NET];
   double e_pair = 0, e_bond = 0;
-  unsigned long long sel_count[2];
-  unsigned long long sel_hash;
+  // Selections of the last compute, recorded when sel_on: sel_keys holds one
+  // AWSEM_SEL_* key per selected item (include/awsem_gpu.h), near_keys the
+  // distance predicates decided within 2e-6 (relative) of their threshold
+  // (where FP32 geometry may decide otherwise), touch_keys the entries of the
+  // reference's n x n caches (cWell, cR, cP_AP, smart_matrix_lib.h) that the
+  // reference evaluation reads or fills, in its own index order.
+  bool sel_on = false;
+  std::vector<uint64_t> sel_keys, near_keys, touch_keys;
+  void sel(int kind, int aux, int i, int j)
+  {
+    if (sel_on) sel_keys.push_back(sel_key(kind, aux, i, j));
+  }
+  void near(int kind, int aux, int i, int j)
+  {
+    if (sel_on) near_keys.push_back(sel_key(kind, aux, i, j));
+  }
+  void touch(int kind, int aux, int i, int j)
+  {
+    if (sel_on) touch_keys.push_back(sel_key(kind, aux, i, j));
+  }
 
   bool first(int i) const { return ch_pos1[chain_of[i]] == i + 1; }
   bool last(int i) const { return ch_pos1[chain_of[i]] + ch_len[chain_of[i]] - 1 == i + 1; }
   int type_of(int i) const { return aa_index(se[i]); }
   int contact_atom(int i) const { return se[i] == 'G' ? ca[i] : cb[i]; }
+  bool bonded(int a, int b) const { return std::find(special[a].begin(), special[a].end(), b) != special[a].end(); }
 
   void read_coeff(const std::string &path);
   void read_tables();
@@ -409,10 +439,10 @@ struct System {
   void chi_term(int i, double *f);
   void rama_term(int i, double *f);
   void dihedral_slopes(int i, int iang, double &angle, double ys[5][3], double xs[5][3]);
-  void dssp_term(int i, int j, double *f);
+  int dssp_term(int i, int j, double *f);
   void pap_nu(int i, int j, double &nu, double &prd);
-  void pap_term(int i, int j, double *f);
-  void helix_pair(int i, int j, double *f);
+  int pap_term(int i, int j, double *f);
+  int helix_pair(int i, int j, double *f);
   void fm_term(int i, double *f);
   void pair_terms(const double *x, double *f);
   void excluded_volume(const double *x, double *f);
@@ -1248,7 +1278,8 @@ void System::rama_term(int i, double *f)
 }
 
 /* compute_dssp_hdrgn(i, j), fix_backbone.cpp:2902-3277 (O of i, N-H of j) */
-void System::dssp_term(int i, int j, double *f)
+/* returns the gates passed: bit 0 r_NO <= cutoff (:2904), bit 1 both nu >= 1e-4 (:3052) */
+int System::dssp_term(int i, int j, double *f)
 {
   const Params &p = P;
   auto rNO = [&](int a, int b) {
@@ -1259,7 +1290,10 @@ void System::dssp_term(int i, int j, double *f)
     return sqrt(pow(xo[3 * a] - xh[3 * b], 2) + pow(xo[3 * a + 1] - xh[3 * b + 1], 2) +
                 pow(xo[3 * a + 2] - xh[3 * b + 2], 2));
   };
-  if (rNO(i, j) > p.dssp_cut) return;
+  touch(TOUCH_RNO, 0, i, j);
+  const double rno0 = rNO(i, j);
+  if (near_thr(rno0, p.dssp_cut)) near(AWSEM_SEL_DSSP, 0, i, j);
+  if (rno0 > p.dssp_cut) return 0;
   int ic = chain_of[i], jc = chain_of[j];
   int i_ch_start = ch_pos1[ic], j_ch_start = ch_pos1[jc];
   int i_ch_end = ch_pos1[ic] + ch_len[ic] - 1, j_ch_end = ch_pos1[jc] + ch_len[jc] - 1;
@@ -1340,7 +1374,7 @@ void System::dssp_term(int i, int j, double *f)
     } else
       nu[s] = 1.0;
   }
-  if (nu[0] < 1e-4 || nu[1] < 1e-4) return;
+  if (nu[0] < 1e-4 || nu[1] < 1e-4) return 1;
   bool i_theta[4] = {true, i_rep, i_AP, i_P};
   // (acceptor O residue, donor N-H residue) of the four Gaussians
   int acc[4] = {i, i, j, j}, don[4] = {j, j + 1, i, i + 2};
@@ -1352,6 +1386,8 @@ void System::dssp_term(int i, int j, double *f)
       continue;
     }
     int a = acc[k], d = don[k];
+    touch(TOUCH_RNO, 0, a, d);
+    touch(TOUCH_RHO, 0, a, d);
     R_NO[k] = rNO(a, d);
     R_HO[k] = rHO(a, d);
     for (int l = 0; l < 3; l++) {
@@ -1397,6 +1433,7 @@ void System::dssp_term(int i, int j, double *f)
       f[3 * o[d - 1] + l] += p.cn * q0 * xNO[k][l] + p.ch * q1 * xHO[k][l];
     }
   }
+  return 3;
 }
 
 /* cP_AP::compute, smart_matrix_lib.h:178-203 */
@@ -1419,13 +1456,16 @@ void System::pap_nu(int i, int j, double &nu, double &prd)
   }
 }
 
-/* compute_P_AP_potential(i, j), i < j, fix_backbone.cpp:3279-3383 */
-void System::pap_term(int i, int j, double *f)
+/* compute_P_AP_potential(i, j), i < j, fix_backbone.cpp:3279-3383; returns
+   bit 0 nu(i, j) >= 1e-12 (:3281), bits 1-3 the classes antiparallel medium,
+   antiparallel long, parallel (:3290-3295) */
+int System::pap_term(int i, int j, double *f)
 {
   const Params &p = P;
   double nu_ij, prd_ij;
+  touch(TOUCH_NU, 0, i, j);
   pap_nu(i, j, nu_ij, prd_ij);
-  if (nu_ij < 1e-12) return;
+  if (nu_ij < 1e-12) return 0;
   int ic = chain_of[i], jc = chain_of[j], d = p.i_diff_pap;
   int i_ch_end = ch_pos1[ic] + ch_len[ic] - 1, j_ch_end = ch_pos1[jc] + ch_len[jc] - 1;
   bool ap_med = ic == jc && i < i_ch_end - (p.i_med_min + 2 * d) && j >= i + (p.i_med_min + 2 * d) &&
@@ -1438,6 +1478,7 @@ void System::pap_term(int i, int j, double *f)
   bool beta = p.n_rama > 0 && aps[p.n_rama - 1][i] == 1.0 && aps[p.n_rama - 1][j] == 1.0;
   auto apply = [&](double K, int i2, int j2) {
     double nu2, prd2;
+    touch(TOUCH_NU, 0, i2, j2);
     pap_nu(i2, j2, nu2, prd2);
     E[ET_PAP] += -p.k_global_pap * K * nu_ij * nu2;
     double f0 = p.k_global_pap * K * prd_ij * nu2;
@@ -1460,10 +1501,12 @@ void System::pap_term(int i, int j, double *f)
     double K = beta ? p.k_pap[2] * p.k_betapred_pap : p.k_pap[2];
     apply(K, i + d, j + d);
   }
+  return 1 | (ap_med ? 2 : 0) | (ap_long ? 4 : 0) | (par ? 8 : 0);
 }
 
-/* compute_helix_dtheta_pair(i, j = i + 4), fix_backbone.cpp:3706-3785 */
-void System::helix_pair(int i, int j, double *f)
+/* compute_helix_dtheta_pair(i, j = i + 4), fix_backbone.cpp:3706-3785;
+   returns 1 when |O_i - N_j| <= cutoff (:3708) */
+int System::helix_pair(int i, int j, double *f)
 {
   const Params &p = P;
   double xNO[3], xHO[3];
@@ -1472,8 +1515,11 @@ void System::helix_pair(int i, int j, double *f)
     xHO[k] = xo[3 * i + k] - xh[3 * j + k];
   }
   double R_NO = sqrt(pow(xNO[0], 2) + pow(xNO[1], 2) + pow(xNO[2], 2));
-  if (R_NO > p.helix_cutoff) return;
-  if (chain_of[i] != chain_of[j]) return;
+  touch(TOUCH_RNO, 0, i, j);
+  if (near_thr(R_NO, p.helix_cutoff)) near(AWSEM_SEL_HELIX_PAIR, 0, i, j);
+  if (R_NO > p.helix_cutoff) return 0;
+  if (chain_of[i] != chain_of[j]) return 1;
+  touch(TOUCH_RHO, 0, i, j);
   double R_HO = sqrt(pow(xHO[0], 2) + pow(xHO[1], 2) + pow(xHO[2], 2));
   double h4i = p.h4prob[type_of(i)];
   if (se[i] == 'P' && p.pro_acc_flag) h4i = p.h4prob_pro;
@@ -1493,6 +1539,7 @@ void System::helix_pair(int i, int j, double *f)
     f[3 * o[j - 1] + k] -= -V * (p.cn * prd0 * xNO[k] + p.ch * prd1 * xHO[k]);
     f[3 * o[i] + k] -= V * (prd0 * xNO[k] + prd1 * xHO[k]);
   }
+  return 1;
 }
 
 /* compute_fragment_memory_potential(i), fix_backbone.cpp:4079-4177 */
@@ -1600,8 +1647,10 @@ void System::pair_terms(const double *x, double *f)
   xi1.assign(n, 0.0);
   xi2.assign(n, 0.0);
   bur.assign(n, 0.0);
-  sel_count[0] = sel_count[1] = 0;
-  sel_hash = 0;
+  auto in_win = [&](double rsq, double lo, double hi, int kind, int aux, int i, int j) {
+    if (near_thr(rsq, lo) || near_thr(rsq, hi)) near(kind, aux, i, j);
+    return rsq > lo && rsq < hi;
+  };
   auto cpos = [&](int i) { return &x[3 * contact_atom(i)]; };
   // DL1
   for (int i = 0; i < n; i++)
@@ -1610,21 +1659,21 @@ void System::pair_terms(const double *x, double *f)
       const double *a = cpos(i), *b = cpos(j);
       double dx0 = a[0] - b[0], dx1 = a[1] - b[1], dx2 = a[2] - b[2];
       double rsq = dx0 * dx0 + dx1 * dx1 + dx2 * dx2;
-      if (p.water && rsq > p.w_rmin_sq[0] && rsq < p.w_rmax_sq[0]) {
+      if (p.water && in_win(rsq, p.w_rmin_sq[0], p.w_rmax_sq[0], AWSEM_SEL_DENS_WATER, 0, i, j)) {
         double th, pr;
         well_theta(sqrt(rsq), p.w_rmin_th[0], p.w_rmax_th[0], p.water_kappa, p.well_rmin[0], p.well_rmax[0], th, pr);
         rho_w[i] += th;
         rho_w[j] += th;
-        sel_count[0]++;
-        sel_hash += mix64(((uint64_t) i << 32) ^ (uint64_t) j ^ (1ULL << 62));
+        sel(AWSEM_SEL_DENS_WATER, 0, i, j);
+        touch(TOUCH_WELL, 0, i, j);
       }
-      if (p.helix && rsq > p.h_rmin_sq && rsq < p.h_rmax_sq) {
+      if (p.helix && in_win(rsq, p.h_rmin_sq, p.h_rmax_sq, AWSEM_SEL_DENS_HELIX, 0, i, j)) {
         double th, pr;
         well_theta(sqrt(rsq), p.h_rmin_th, p.h_rmax_th, p.helix_kappa, p.helix_rmin, p.helix_rmax, th, pr);
         rho_h[i] += th;
         rho_h[j] += th;
-        sel_count[1]++;
-        sel_hash += mix64(((uint64_t) i << 32) ^ (uint64_t) j ^ (2ULL << 62));
+        sel(AWSEM_SEL_DENS_HELIX, 0, i, j);
+        touch(TOUCH_HWELL, 0, i, j);
       }
     }
   // SL: switching functions and burial (:7795-7841)
@@ -1661,7 +1710,9 @@ void System::pair_terms(const double *x, double *f)
       int j = i + d;
       if (j >= n || chain_of[j] != chain_of[i]) continue;
       double dx0 = xo[3 * i] - xn[3 * j], dx1 = xo[3 * i + 1] - xn[3 * j + 1], dx2 = xo[3 * i + 2] - xn[3 * j + 2];
-      if (dx0 * dx0 + dx1 * dx1 + dx2 * dx2 < p.helix_cutoff_sq) helix_pair(i, j, f);
+      const double r2 = dx0 * dx0 + dx1 * dx1 + dx2 * dx2;
+      if (near_thr(r2, p.helix_cutoff_sq)) near(AWSEM_SEL_HELIX_PAIR, 0, i, j);
+      if (r2 < p.helix_cutoff_sq) sel(AWSEM_SEL_HELIX_PAIR, helix_pair(i, j, f), i, j);
     }
   }
   // DL2: water xi (:7877-7954)
@@ -1677,7 +1728,9 @@ void System::pair_terms(const double *x, double *f)
           if (!p.well_flag[w]) continue;
           double g0 = water_gamma(i, j, w, ti, tj, 0), g1 = water_gamma(i, j, w, ti, tj, 1);
           // `!fabs(g0 - g1) < delta` in the reference is true exactly when g0 != g1
-          if (g0 != g1 && rsq > p.w_rmin_sq[w] && rsq < p.w_rmax_sq[w]) {
+          if (g0 != g1 && in_win(rsq, p.w_rmin_sq[w], p.w_rmax_sq[w], AWSEM_SEL_XI_WATER, w, i, j)) {
+            sel(AWSEM_SEL_XI_WATER, w, i, j);
+            touch(TOUCH_WELL, w, i, j);
             double th, pr;
             well_theta(sqrt(rsq), p.w_rmin_th[w], p.w_rmax_th[w], p.water_kappa, p.well_rmin[w], p.well_rmax[w], th, pr);
             double tg = (g1 - g0) * th;
@@ -1703,7 +1756,10 @@ void System::pair_terms(const double *x, double *f)
         int ti = type_of(i), tj = type_of(j);
         for (int w = 0; w < p.n_wells; w++) {
           if (!p.well_flag[w]) continue;
-          if ((other || abs(j - i) >= p.contact_cutoff) && rsq > p.w_rmin_sq[w] && rsq < p.w_rmax_sq[w]) {
+          if ((other || abs(j - i) >= p.contact_cutoff) &&
+              in_win(rsq, p.w_rmin_sq[w], p.w_rmax_sq[w], AWSEM_SEL_WATER, w, i, j)) {
+            sel(AWSEM_SEL_WATER, w, i, j);
+            touch(TOUCH_WELL, w, i, j);
             double g0 = water_gamma(i, j, w, ti, tj, 0), g1 = water_gamma(i, j, w, ti, tj, 1);
             double sg = fabs(g0 - g1) < 1e-5 ? 0.5 * (g0 + g1) : g0 + (g1 - g0) * sig_w[i] * sig_w[j];
             double th, pr;
@@ -1712,24 +1768,32 @@ void System::pair_terms(const double *x, double *f)
             force += sg * pr;
           }
         }
-        if (rsq > p.w_rmin_sq[0] && rsq < p.w_rmax_sq[0]) {
+        if (in_win(rsq, p.w_rmin_sq[0], p.w_rmax_sq[0], AWSEM_SEL_XI_FORCE, 0, i, j)) {
           double th, pr;
           well_theta(r, p.w_rmin_th[0], p.w_rmax_th[0], p.water_kappa, p.well_rmin[0], p.well_rmax[0], th, pr);
-          if (fabs(xi_w[i]) > 1e-8) force += pr * xi_w[i];
-          if (fabs(xi_w[j]) > 1e-8) force += pr * xi_w[j];
+          const int on = (fabs(xi_w[i]) > 1e-8 ? 1 : 0) | (fabs(xi_w[j]) > 1e-8 ? 2 : 0);
+          if (on & 1) force += pr * xi_w[i];
+          if (on & 2) force += pr * xi_w[j];
+          if (on) {
+            sel(AWSEM_SEL_XI_FORCE, on, i, j);
+            touch(TOUCH_WELL, 0, i, j);
+          }
         }
       }
       if (p.burial && rsq > p.w_rmin_sq[0] && rsq < p.w_rmax_sq[0]) {
+        touch(TOUCH_WELL, 0, i, j);
         double th, pr;
         well_theta(r, p.w_rmin_th[0], p.w_rmax_th[0], p.water_kappa, p.well_rmin[0], p.well_rmax[0], th, pr);
         force += (bur[i] + bur[j]) * pr;
       }
-      if (p.helix && rsq > p.h_rmin_sq && rsq < p.h_rmax_sq) {
+      if (p.helix && in_win(rsq, p.h_rmin_sq, p.h_rmax_sq, AWSEM_SEL_HELIX_FORCE, 0, i, j)) {
         int d = p.helix_i_diff;
         double fac = xi1[i] + xi1[j];
         if (i - d >= 0) fac += xi2[i - d];
         if (j - d >= 0) fac += xi2[j - d];
         if (fabs(fac) > 1e-6) {
+          sel(AWSEM_SEL_HELIX_FORCE, 0, i, j);
+          touch(TOUCH_HWELL, 0, i, j);
           double th, pr;
           well_theta(r, p.h_rmin_th, p.h_rmax_th, p.helix_kappa, p.helix_rmin, p.helix_rmax, th, pr);
           force += -fac * pr;
@@ -1749,15 +1813,28 @@ void System::pair_terms(const double *x, double *f)
         if (se[j] == 'P' || last(i) || first(j)) continue;
         if (j == 0) continue;
         double dx0 = xo[3 * i] - xn[3 * j], dx1 = xo[3 * i + 1] - xn[3 * j + 1], dx2 = xo[3 * i + 2] - xn[3 * j + 2];
-        if (dx0 * dx0 + dx1 * dx1 + dx2 * dx2 < p.dssp_cut_sq) dssp_term(i, j, f);
+        const double r2 = dx0 * dx0 + dx1 * dx1 + dx2 * dx2;
+        if (near_thr(r2, p.dssp_cut_sq)) near(AWSEM_SEL_DSSP, 0, i, j);
+        if (r2 < p.dssp_cut_sq) sel(AWSEM_SEL_DSSP, dssp_term(i, j, f), i, j);
       }
   // DL3: P_AP on CA pairs (:8096-8103)
+  // the selection records list the CA pairs separated enough for some P_AP
+  // class (other chains, or at least the smallest class separation)
+  const int pap_sep = std::min(p.i_med_min + 2 * p.i_diff_pap, p.i_med_max + 1);
   if (p.pap)
     for (int i = 0; i < n; i++)
       for (int j = i + 1; j < n; j++) {
         const double *a = &x[3 * ca[i]], *b = &x[3 * ca[j]];
         double dx0 = a[0] - b[0], dx1 = a[1] - b[1], dx2 = a[2] - b[2];
-        if (dx0 * dx0 + dx1 * dx1 + dx2 * dx2 < p.pap_cutoff_sq) pap_term(i, j, f);
+        const double rsq = dx0 * dx0 + dx1 * dx1 + dx2 * dx2;
+        const bool listed = chain_of[i] != chain_of[j] || j - i >= pap_sep;
+        if (listed && near_thr(rsq, p.pap_cutoff_sq)) near(AWSEM_SEL_PAP, 0, i, j);
+        // 1-2 bonded CA pairs are not in LAMMPS's list (special_bonds fene):
+        // the reference never evaluates them (no P_AP class holds them anyway)
+        if (rsq < p.pap_cutoff_sq && !bonded(ca[i], ca[j])) {
+          const int g = pap_term(i, j, f);
+          if (listed) sel(AWSEM_SEL_PAP, g, i, j);
+        }
       }
 }
 
@@ -1765,6 +1842,21 @@ void System::pair_terms(const double *x, double *f)
    atom pairs except 1-2 bonded ones (special_bonds fene) */
 void System::excluded_volume(const double *x, double *f)
 {
+  // a bead pair as (residue, bead) with the lower residue (then bead) first
+  auto ev_sel = [&](int a, int b, bool near_only) {
+    auto bead = [&](int at) {
+      const int r = ares[at] - 1;
+      return at == ca[r] ? 0 : at == cb[r] ? 1 : at == o[r] ? 2 : -1;
+    };
+    int ri = ares[a] - 1, rj = ares[b] - 1, bi = bead(a), bj = bead(b);
+    if (bi < 0 || bj < 0) return;
+    if (ri > rj || (ri == rj && bi > bj)) {
+      std::swap(ri, rj);
+      std::swap(bi, bj);
+    }
+    if (near_only) near(AWSEM_SEL_EV, 3 * bi + bj, ri, rj);
+    else sel(AWSEM_SEL_EV, 3 * bi + bj, ri, rj);
+  };
   int N = ntypes + 1;
   int sign = ev_p % 2 == 0 ? 1 : -1;
   e_pair = 0.0;
@@ -1775,11 +1867,14 @@ void System::excluded_volume(const double *x, double *f)
       double dx = x[3 * i] - x[3 * j], dy = x[3 * i + 1] - x[3 * j + 1], dz = x[3 * i + 2] - x[3 * j + 2];
       double rsq = dx * dx + dy * dy + dz * dz;
       double r = sqrt(rsq);
+      const bool counted = sel_on && ev_lambda[ti * N + tj] != 0.0;
+      if (counted && near_thr(r, rc)) ev_sel(i, j, true);
       if (!(r < rc)) continue;
       bool excl = false;
       for (int s : special[i])
         if (s == j) excl = true;
       if (excl) continue;
+      if (counted) ev_sel(i, j, false);
       double dr = r - rc;
       double pref = ev_lambda[ti * N + tj] * sign * pow(dr, ev_p - 1);
       double fpair = r > 0.0 ? -pref * ev_p / r : 0.0;
@@ -2348,13 +2443,28 @@ int oracle_residue_arrays(void *h, double *out)
   return S->n;
 }
 
-int oracle_selection_digest(void *h, unsigned long long *counts, unsigned long long *hash)
+long long oracle_selections(void *h, const double *x, int which, unsigned long long *out, long long cap)
 {
   System *S = (System *) h;
-  counts[0] = S->sel_count[0];
-  counts[1] = S->sel_count[1];
-  *hash = S->sel_hash;
-  return 0;
+  try {
+    std::vector<double> f((size_t) 3 * S->natoms);
+    S->sel_keys.clear();
+    S->near_keys.clear();
+    S->touch_keys.clear();
+    S->sel_on = true;
+    S->list_setup = true;
+    S->compute(x, f.data());
+    S->sel_on = false;
+  } catch (std::exception &e) {
+    S->sel_on = false;
+    g_err = e.what();
+    return -1;
+  }
+  std::vector<uint64_t> &v = which == 0 ? S->sel_keys : which == 1 ? S->near_keys : S->touch_keys;
+  std::sort(v.begin(), v.end());
+  v.erase(std::unique(v.begin(), v.end()), v.end());
+  for (long long k = 0; k < (long long) v.size() && k < cap; k++) out[k] = v[k];
+  return (long long) v.size();
 }
 
 int oracle_run(void *h, double *x, double *v, long long step0, long long nsteps, double dt, int langevin,

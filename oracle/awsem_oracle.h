@@ -26,10 +26,12 @@ int oracle_compute(void *h, const double *x, double *f, double *energies);
 /* per-residue intermediates of the last compute: rho_w, rho_h, xi_w, xi1_h,
    xi2_h, burial_coefficient, sigma_w, sigma_h ([n][8]) */
 int oracle_residue_arrays(void *h, double *out);
-/* number of (i<j) contact-bead pairs selected into each density well by the
-   last compute: counts[0] water well 0 (DL1), counts[1] helix well (DL1),
-   and a 64-bit order-independent hash of the selected (i, j, well) triples */
-int oracle_selection_digest(void *h, unsigned long long *counts, unsigned long long *hash);
+/* One evaluation at x recording its selections; returns the number of
+   distinct keys of the set `which` (0: AWSEM_SEL_* selection records,
+   include/awsem_gpu.h; 1: distance predicates decided within 2e-6 of their
+   threshold; 2: the reference's n x n cache entries the evaluation touches,
+   kinds 32-36) and stores up to cap of them, sorted, in out; -1 on error */
+long long oracle_selections(void *h, const double *x, int which, unsigned long long *out, long long cap);
 /* nsteps of velocity Verlet (+ Langevin); x and v updated in place.
    thermo (optional): (nsteps+1) x 4 rows of [fix total, vexcluded, bonds, ke]. */
 int oracle_run(void *h, double *x, double *v, long long step0, long long nsteps, double dt,

@@ -46,6 +46,8 @@ def _load_ref(path=REF_LIB):
         lib.ref_run.argtypes = [C.c_void_p, C.c_longlong, C.c_double, C.c_int, C.c_double, C.c_double,
                                 C.c_double, C.c_ulonglong, C.c_void_p]
         lib.ref_compute_q.argtypes = [C.c_void_p, C.c_char_p, C.c_void_p]
+        lib.ref_touches.restype = C.c_longlong
+        lib.ref_touches.argtypes = [C.c_void_p, C.c_void_p, C.c_longlong]
         lib.ref_nbuilds.argtypes = [C.c_void_p]
         lib.ref_nbuilds.restype = C.c_long
         lib.ref_last_error.restype = C.c_char_p
@@ -118,6 +120,16 @@ class RefSystem:
         self.lib.ref_residue_arrays(self.h, out.ctypes.data)
         return out
 
+    def touches(self) -> np.ndarray:
+        """sorted keys of the reference's n x n cache entries that the last
+        evaluation read or filled (kinds 32-36, oracle/ref_host.cpp)"""
+        n = self.lib.ref_touches(self.h, None, 0)
+        if n < 0:
+            raise RuntimeError("no reference fix hosted")
+        out = np.zeros(max(n, 1), dtype=np.uint64)
+        self.lib.ref_touches(self.h, out.ctypes.data, n)
+        return out[:n]
+
     def run(self, nsteps, dt=2.0, langevin=True, t_start=300.0, t_stop=300.0, damp=500.0, seed=1):
         thermo = np.zeros((nsteps + 1, 4))
         if self.lib.ref_run(self.h, nsteps, dt, int(langevin), t_start, t_stop, damp, seed, thermo.ctypes.data) != 0:
@@ -148,7 +160,8 @@ def _load_oracle():
         lib.oracle_nres.argtypes = [C.c_void_p]
         lib.oracle_compute.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         lib.oracle_residue_arrays.argtypes = [C.c_void_p, C.c_void_p]
-        lib.oracle_selection_digest.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        lib.oracle_selections.restype = C.c_longlong
+        lib.oracle_selections.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_longlong]
         lib.oracle_run.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_longlong, C.c_longlong, C.c_double,
                                    C.c_int, C.c_double, C.c_double, C.c_double, C.c_ulonglong, C.c_void_p]
         lib.oracle_set_neighbor.argtypes = [C.c_void_p, C.c_double, C.c_int, C.c_int, C.c_int]
@@ -206,11 +219,19 @@ class OracleSystem:
         self.lib.oracle_residue_arrays(self.h, out.ctypes.data)
         return out
 
-    def selection_digest(self):
-        counts = np.zeros(2, dtype=np.uint64)
-        h = np.zeros(1, dtype=np.uint64)
-        self.lib.oracle_selection_digest(self.h, counts.ctypes.data, h.ctypes.data)
-        return int(counts[0]), int(counts[1]), int(h[0])
+    def selections(self, x: np.ndarray, which: str = "sel") -> np.ndarray:
+        """Sorted keys of one evaluation at x: "sel" the AWSEM_SEL_* selection
+        records (include/awsem_gpu.h), "near" the distance predicates decided
+        within 2e-6 of their threshold, "touch" the reference cache entries the
+        evaluation reads or fills (kinds 32-36, as RefSystem.touches)"""
+        w = {"sel": 0, "near": 1, "touch": 2}[which]
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        n = self.lib.oracle_selections(self.h, x.ctypes.data, w, None, 0)
+        if n < 0:
+            raise RuntimeError(self.lib.oracle_last_error().decode())
+        out = np.zeros(max(n, 1), dtype=np.uint64)
+        self.lib.oracle_selections(self.h, x.ctypes.data, w, out.ctypes.data, n)
+        return out[:n]
 
     def run(self, x, v, nsteps, step0=0, dt=2.0, langevin=True, t_start=300.0, t_stop=300.0, damp=500.0, seed=1):
         x = np.ascontiguousarray(x, dtype=np.float64).copy()
@@ -220,3 +241,49 @@ class OracleSystem:
                                t_stop, damp, seed, thermo.ctypes.data) != 0:
             raise RuntimeError(self.lib.oracle_last_error().decode())
         return x, v, thermo
+
+
+# --------------------------------------------------------------------------
+# selection records (AWSEM_SEL_* keys, include/awsem_gpu.h)
+
+SEL_KINDS = {1: "dens_water", 2: "dens_helix", 3: "xi_water", 4: "water", 5: "xi_force", 6: "helix_force",
+             7: "helix_pair", 8: "dssp", 9: "pap", 10: "ev"}
+# kinds whose aux carries gates on transcendental outputs (not the identity of the predicate)
+_GATED = (5, 7, 8, 9)
+_AUX = np.uint64(0xFFF << 44)
+
+
+def _kind(keys):
+    return (np.asarray(keys, dtype=np.uint64) >> np.uint64(56)).astype(np.int64)
+
+
+def compare_selections(got, want, near=None) -> dict:
+    """Compare two sets of selection keys kind by kind.
+
+    ``cand`` counts items selected by one side only (for the gated kinds
+    XI_FORCE, HELIX_PAIR, DSSP, PAP compared without their gate bits);
+    ``cand_far`` those of them that are not in ``near`` (distance predicates
+    decided within 2e-6 of their threshold by the oracle); ``gate`` counts
+    items both select whose gate bits differ."""
+    got = np.unique(np.asarray(got, dtype=np.uint64))
+    want = np.unique(np.asarray(want, dtype=np.uint64))
+    near = np.unique(np.asarray(near if near is not None else [], dtype=np.uint64))
+    out = {}
+    for k, name in SEL_KINDS.items():
+        g, w = got[_kind(got) == k], want[_kind(want) == k]
+        gated = k in _GATED
+        gb, wb = (g & ~_AUX, w & ~_AUX) if gated else (g, w)
+        nb = near[_kind(near) == k]
+        if gated:
+            nb = nb & ~_AUX
+        diff = np.setxor1d(gb, wb)
+        far = np.setdiff1d(diff, nb)
+        common = np.intersect1d(gb, wb)
+        gate = 0
+        if gated and len(common):
+            gmap = dict(zip((gb).tolist(), g.tolist()))
+            wmap = dict(zip((wb).tolist(), w.tolist()))
+            gate = sum(1 for c in common.tolist() if gmap[c] != wmap[c])
+        out[name] = {"got": int(len(g)), "want": int(len(w)), "cand": int(len(diff)), "cand_far": int(len(far)),
+                     "gate": int(gate)}
+    return out

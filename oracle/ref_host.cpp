@@ -95,6 +95,39 @@ std::vector<std::string> split_ws(const std::string &s)
 
 }  // namespace
 
+/* Read access to private members of the reference's classes, for
+   ref_touches: an explicit instantiation may name a private member
+   ([temp.explicit]: access checking does not apply to the names in an
+   explicit instantiation), so the reference sources stay unmodified. */
+template <typename Tag, typename Tag::type M> struct Expose {
+  friend typename Tag::type get(Tag) { return M; }
+};
+#define EXPOSE(NAME, CLASS, TYPE, MEMBER)         \
+  struct NAME {                                    \
+    typedef TYPE CLASS::*type;                     \
+    friend type get(NAME);                         \
+  };                                               \
+  template struct Expose<NAME, &CLASS::MEMBER>;
+typedef cWell<double, FixBackbone> WellT;
+typedef cR<double, FixBackbone> RT;
+typedef cP_AP<double, FixBackbone> PapT;
+EXPOSE(FbWell, FixBackbone, WellT *, well)
+EXPOSE(FbHWell, FixBackbone, WellT *, helix_well)
+EXPOSE(FbR, FixBackbone, RT *, R)
+EXPOSE(FbPap, FixBackbone, PapT *, p_ap)
+EXPOSE(WellG, WellT, int ***, gTheta)
+EXPOSE(WellN, WellT, int, n)
+EXPOSE(WellM, WellT, int, m)
+EXPOSE(WellNW, WellT, int, nw)
+EXPOSE(RGNO, RT, int **, gNO)
+EXPOSE(RGHO, RT, int **, gHO)
+EXPOSE(RN, RT, int, n)
+EXPOSE(RM, RT, int, m)
+EXPOSE(PapG, PapT, int **, g)
+EXPOSE(PapN, PapT, int, n)
+EXPOSE(PapM, PapT, int, m)
+#undef EXPOSE
+
 struct RefHost {
   LAMMPS *lmp = nullptr;
   Fix *fix = nullptr;
@@ -728,6 +761,56 @@ int ref_residue_arrays(void *hp, double *out)
     out[6 * i + 5] = fb->burial_force[i];
   }
   return n;
+}
+
+/* The entries of the reference's n x n caches (cWell for the water and
+   helix wells, cR for r_NO / r_HO, cP_AP for nu; smart_matrix_lib.h) that
+   the last evaluation read or filled: those whose generation tag equals the
+   fix's current ntimestep.  Keys kind << 56 | aux << 44 | i << 22 | j with
+   kind 32 water well (aux = well, i < j), 33 helix well (i < j), 34 r_NO,
+   35 r_HO, 36 nu (ordered pairs), sorted.  Returns the number of keys (up
+   to cap stored), -1 when no reference fix is hosted. */
+long long ref_touches(void *hp, unsigned long long *out, long long cap)
+{
+  RefHost *h = (RefHost *) hp;
+  FixBackbone *fb = h->fb;
+  if (!fb) return -1;
+  const int t = fb->ntimestep;
+  std::vector<unsigned long long> keys;
+  auto key = [](int kind, int aux, int i, int j) {
+    return (unsigned long long) kind << 56 | (unsigned long long) aux << 44 | (unsigned long long) i << 22 |
+           (unsigned long long) j;
+  };
+  auto wells = [&](WellT *w, int kind) {
+    if (!w) return;
+    int ***g = w->*get(WellG());
+    const int n = w->*get(WellN()), m = w->*get(WellM()), nw = w->*get(WellNW());
+    for (int k = 0; k < nw; k++)
+      for (int i = 0; i < n; i++)
+        for (int j = i + 1; j < m; j++)
+          if (g[k][i][j] == t) keys.push_back(key(kind, k, i, j));
+  };
+  wells(fb->*get(FbWell()), 32);
+  wells(fb->*get(FbHWell()), 33);
+  if (RT *r = fb->*get(FbR())) {
+    int **gno = r->*get(RGNO()), **gho = r->*get(RGHO());
+    const int n = r->*get(RN()), m = r->*get(RM());
+    for (int i = 0; i < n; i++)
+      for (int j = 0; j < m; j++) {
+        if (gno[i][j] == t) keys.push_back(key(34, 0, i, j));
+        if (gho[i][j] == t) keys.push_back(key(35, 0, i, j));
+      }
+  }
+  if (PapT *q = fb->*get(FbPap())) {
+    int **g = q->*get(PapG());
+    const int n = q->*get(PapN()), m = q->*get(PapM());
+    for (int i = 0; i < n; i++)
+      for (int j = 0; j < m; j++)
+        if (g[i][j] == t) keys.push_back(key(36, 0, i, j));
+  }
+  std::sort(keys.begin(), keys.end());
+  for (long long k = 0; k < (long long) keys.size() && k < cap; k++) out[k] = keys[k];
+  return (long long) keys.size();
 }
 
 /* `run nsteps` with fix nve (+ fix langevin when langevin != 0).

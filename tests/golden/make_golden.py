@@ -35,6 +35,10 @@ against the LAMMPS-API shim (``make -C oracle ref``) and run on four inputs:
                (water contacts of phosphorylated residues);
 * ``c0v``     -- ``c0`` with [Vector_Fragment_Memory] (k 1, sigma 0.3 rad)
                over its fragment memories;
+* ``c1``      -- benchmark configuration 1: 8 chains x 250 residues (2,000
+               residues) at seeded non-overlapping positions in a 150 A cube
+               (synth.config_system(1)), all terms of the default parameter
+               set plus fragment memory;
 * ``c0go``    -- ``c0`` with [AMH-Go] (k 200, p 2, rc 10 A) towards a native
                structure 0.6 times as large as the starting chain
                (synth.write_native_gro), run with neighbor skin 0.6 A and
@@ -92,6 +96,8 @@ def dir_hash(d: str) -> str:
 def write_case(name: str, outdir: str) -> dict:
     if name == "c0":
         return synth.write_system(synth.config_system(0), outdir)
+    if name == "c1":
+        return synth.write_system(synth.config_system(1), outdir)
     if name in ("c0x", "sheetx"):
         sys_ = synth.config_system(0) if name == "c0x" else synth.sheet_system()
         files = synth.write_system(sys_, outdir)
@@ -156,7 +162,8 @@ def write_case(name: str, outdir: str) -> dict:
     raise KeyError(name)
 
 
-CASES = ["c0", "sheet", "r1r69", "r1r69tb", "r1r69go", "r1r69go2", "c0go", "c0x", "sheetx", "c0s", "sheets", "c0v"]
+CASES = ["c0", "sheet", "r1r69", "r1r69tb", "r1r69go", "r1r69go2", "c0go", "c0x", "sheetx", "c0s", "sheets", "c0v",
+         "c1"]
 # LAMMPS neighbor skin and neigh_modify delay / every / check of a case's runs
 # (the others: 2.0, 0, 1, yes -- LAMMPS's defaults)
 NEIGH = {"c0go": (0.6, 3, 2, 1), "c0x": (0.6, 3, 2, 1)}

@@ -12,7 +12,9 @@ from conftest import neigh_of, write_case
 
 pytestmark = pytest.mark.gpu
 
-CASES = ["c0", "sheet", "r1r69", "r1r69tb", "r1r69go", "r1r69go2", "c0go", "c0x", "sheetx", "c0s", "sheets", "c0v"]
+# c1: configuration 1 (8 x 250 residues), made by the compiled reference like the others
+CASES = ["c0", "sheet", "r1r69", "r1r69tb", "r1r69go", "r1r69go2", "c0go", "c0x", "sheetx", "c0s", "sheets", "c0v",
+         "c1"]
 TOL = {"fp64": (1e-6, 1e-5), "mixed": (1e-5, 1e-4)}
 
 
