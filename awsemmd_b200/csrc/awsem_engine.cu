@@ -1983,8 +1983,27 @@ struct awsem_system {
   std::unique_ptr<SharedForceField> shared;  // force field of array-described replicas
 };
 
+// The caller's current device, put back when an entry point returns (the
+// engine makes the handle's device current for its work).
+struct DeviceRestore {
+  int prev = -1;
+  DeviceRestore()
+  {
+    if (cudaGetDevice(&prev) != cudaSuccess) {
+      prev = -1;
+      cudaGetLastError();
+    }
+  }
+  ~DeviceRestore()
+  {
+    int now = -1;
+    if (prev >= 0 && cudaGetDevice(&now) == cudaSuccess && now != prev) cudaSetDevice(prev);
+  }
+};
+
 template <typename Fn> static int guarded(Fn fn)
 {
+  DeviceRestore restore;
   try {
     fn();
     return AWSEM_OK;
@@ -2137,7 +2156,7 @@ int awsem_create_from_atoms(const char *workdir, const char *coeff_file, const c
                             const int *bond_b, const double *bond_k, const double *bond_r0, const char *pair_style,
                             const char *pair_coeffs, int precision, int device, awsem_system **out)
 {
-  if (!out || !coeff_file || !seq_file || natoms <= 0 || !role || !residue || !molecule || !type || !tag ||
+  if (!out || (!coeff_file) != (!seq_file) || natoms <= 0 || !role || !residue || !molecule || !type || !tag ||
       !mass_by_type || (nbonds > 0 && (!bond_a || !bond_b || !bond_k || !bond_r0))) {
     g_last_error = "awsem_create_from_atoms: null or empty argument";
     return AWSEM_EINVAL;
@@ -2146,7 +2165,8 @@ int awsem_create_from_atoms(const char *workdir, const char *coeff_file, const c
   if (rc != AWSEM_OK) return rc;
   rc = guarded([&] {
     std::unique_ptr<SystemInput> S(new SystemInput());
-    load_system_atoms(workdir ? workdir : "", coeff_file, seq_file, natoms, role, residue, molecule, type, tag,
+    load_system_atoms(workdir ? workdir : "", coeff_file ? coeff_file : "", seq_file ? seq_file : "", natoms, role,
+                      residue, molecule, type, tag,
                       mass_by_type, ntypes, x, nullptr, std::max(nbonds, 0), bond_a, bond_b, bond_k, bond_r0,
                       pair_style ? pair_style : "2 3.5 3.5", pair_coeffs ? pair_coeffs : "", *S, true);
     (*out)->eng->reps.push_back(std::move(S));

@@ -1584,7 +1584,28 @@ void load_system_atoms(const std::string &dir, const std::string &coeff_file, co
                        const std::string &pair_style, const std::string &pair_coeffs, SystemInput &S,
                        bool read_files)
 {
-  if (read_files) {
+  if (read_files && coeff_file.empty() && seq_file.empty()) {
+    // pair vexcluded (and bonds) only: no fix backbone terms, so no
+    // coefficient or sequence file; residues 1..max id, chains as runs of
+    // equal molecule id along the residues, every residue read as alanine
+    // (residue kinds matter to fix backbone terms only)
+    S.ff.p.terms = 0;
+    int n = 0;
+    for (int a = 0; a < natoms; a++) n = std::max(n, res[a]);
+    if (n <= 0) fail("Residue tag is out of range");
+    std::vector<int> mol_of(n, -1);
+    for (int a = 0; a < natoms; a++)
+      if (role[a] >= 0 && res[a] >= 1) mol_of[res[a] - 1] = mol[a];
+    S.top.seq.assign(n, 'A');
+    S.top.chain_start.clear();
+    S.top.chain_end.clear();
+    for (int r = 0; r < n; r++) {
+      if (r == 0 || mol_of[r] != mol_of[r - 1]) S.top.chain_start.push_back(r);
+      if (r == n - 1 || mol_of[r + 1] != mol_of[r]) S.top.chain_end.push_back(r);
+    }
+    S.top.n_chains = (int) S.top.chain_start.size();
+    S.top.n_res = n;
+  } else if (read_files) {
     read_coeff_file(path_in(dir, coeff_file), S.ff);
     read_sequence(path_in(dir, seq_file), S.top);
   }

@@ -33,23 +33,51 @@ constexpr int kEnergySlot = AWSEM_NOALLOC_MAX_ATOMS * 3;
 static __device__ __align__(256) unsigned long long g_facc[AWSEM_NOALLOC_MAX_ATOMS * 3 + 32];
 
 constexpr int kMaxDevices = 64;
-static unsigned long long *g_facc_addr[kMaxDevices];
+struct ScratchAddr {
+  void *ctx = nullptr;                // the CUDA context the address belongs to
+  unsigned long long *addr = nullptr;
+};
+static ScratchAddr g_facc_addr[kMaxDevices];
 static std::mutex g_mutex;
+
+// The driver's cuCtxGetCurrent, found through the runtime (no link-time
+// dependency on the driver library); CUcontext is an opaque pointer.
+typedef int (*CtxGetCurrentFn)(void **);
+static CtxGetCurrentFn ctx_get_current()
+{
+  static CtxGetCurrentFn fn = [] {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      p = nullptr;
+    return (CtxGetCurrentFn) p;
+  }();
+  return fn;
+}
 
 // Device address of g_facc on `device` (the current device).  In host code
 // the array's name is only a host-side stand-in; the address comes from the
-// runtime, once per device.
+// runtime: at the first call on the device, and again whenever the device's
+// context has changed since (after a cudaDeviceReset the old address is
+// gone).
 static unsigned long long *scratch(int device)
 {
   if (device < 0 || device >= kMaxDevices) throw std::invalid_argument("device index out of range");
   std::lock_guard<std::mutex> lock(g_mutex);
-  if (!g_facc_addr[device]) {
+  void *ctx = nullptr;
+  if (CtxGetCurrentFn get = ctx_get_current()) {
+    if (get(&ctx) != 0) ctx = nullptr;
+  }
+  ScratchAddr &c = g_facc_addr[device];
+  if (!c.addr || ctx != c.ctx) {
     void *p = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&p, g_facc);
     if (e != cudaSuccess) throw std::runtime_error(std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-    g_facc_addr[device] = (unsigned long long *) p;
+    c.addr = (unsigned long long *) p;
+    c.ctx = ctx;
   }
-  return g_facc_addr[device];
+  return c.addr;
 }
 
 __global__ void k_clear(unsigned long long *facc, int n)

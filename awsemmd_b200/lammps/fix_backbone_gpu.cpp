@@ -98,8 +98,8 @@ void FixBackboneGPU::evaluate()
   const int per[3] = {domain->xperiodic, domain->yperiodic, domain->zperiodic};
   for (int i = 0; i < n; i++) {
     const size_t k = 3 * (size_t) (atom->tag[i] - 1);
-    const int box[3] = {(int) (image[i] & 1023) - 512, (int) (image[i] >> 10 & 1023) - 512,
-                        (int) (image[i] >> 20) - 512};
+    const int box[3] = {(int) (image[i] & IMGMASK) - IMGMAX, (int) (image[i] >> IMGBITS & IMGMASK) - IMGMAX,
+                        (int) (image[i] >> IMG2BITS) - IMGMAX};
     for (int d = 0; d < 3; d++) xg[k + d] = x[i][d] + (per[d] ? box[d] * prd[d] : 0.0);
   }
   std::fill(fg.begin(), fg.end(), 0.0);

@@ -122,7 +122,11 @@ void awsem_destroy(awsem_system *sys);
  * (mass_by_type[1..ntypes]); x (may be NULL); bonds as caller indices
  * (nbonds may be 0 when the host computes the bonds itself).  The
  * coefficient and sequence files and the tables are read from `workdir`, as
- * by the FixBackbone constructor (src/fix_backbone.cpp:86-1072). */
+ * by the FixBackbone constructor (src/fix_backbone.cpp:86-1072).  With both
+ * coeff_file and seq_file NULL the handle carries no fix backbone terms: it
+ * evaluates pair vexcluded (AWSEM_TERMS_PAIR) and the given bonds only, its
+ * chains being the runs of equal molecule id along the residues (what
+ * PairExcludedVolume alone needs, src/pair_excluded_volume.cpp:50-138). */
 int awsem_create_from_atoms(const char *workdir, const char *coeff_file, const char *seq_file, int natoms,
                             const int *role, const int *residue, const int *molecule, const int *type, const int *tag,
                             const double *mass_by_type, int ntypes, const double *x, int nbonds, const int *bond_a,
@@ -410,9 +414,13 @@ int awsem_server_usage(awsem_system *srv, long long *info);
  * (576 KiB, held by every GPU that loads the library until exit); larger
  * handles are rejected with AWSEM_EINVAL.  The first call on a device looks
  * up that array's device address (cudaGetSymbolAddress); make that first
- * call before any stream capture.  All calls share the array and each
- * clears what it uses first; calls whose kernels overlap on the GPU race on
- * it and must be serialised by the caller. */
+ * call before any stream capture.  A device reset (cudaDeviceReset) ends the
+ * context that address belongs to: the next call on that device looks it up
+ * again, so it too should come before any capture.  All calls share the
+ * array and each clears what it uses first; calls whose kernels overlap on
+ * the GPU race on it and must be serialised by the caller.  The caller's
+ * buffers and stream belong to the handle's device; like every entry point,
+ * the call leaves the caller's current device as it found it. */
 #define AWSEM_NOALLOC_MAX_ATOMS 24576
 int awsem_fragmem_noalloc(awsem_system *sys, const double *d_x, double *d_f, double *d_energy, void *stream);
 

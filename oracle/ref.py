@@ -4,8 +4,10 @@
   unmodified from the reference sources against the LAMMPS-API shim
   (``oracle/_ref/libawsem_ref.so``, built by ``make -C oracle ref``).
   ``RefSystem(files, gpu_fix="fp64" | "mixed")`` runs the same host with the
-  GPU adapter ``fix backbone/gpu`` in place of the reference fix
-  (``oracle/_ref/libawsem_ref_gpufix.so``, ``make -C oracle gpufix``).
+  GPU adapter ``fix backbone/gpu`` in place of the reference fix, and
+  ``RefSystem(files, gpu_pair=...)`` with ``pair_style vexcluded/gpu`` in place
+  of the reference pair style (``oracle/_ref/libawsem_ref_gpufix.so``,
+  ``make -C oracle gpufix``).
 """
 from __future__ import annotations
 
@@ -15,6 +17,9 @@ import os
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
+# the reference source tree the oracle recipe compiles (oracle/Makefile's REF);
+# AWSEM_REFERENCE_DIR overrides it
+REFERENCE_DIR = os.environ.get("AWSEM_REFERENCE_DIR", "/root/reference")
 REF_LIB = os.path.join(HERE, "_ref", "libawsem_ref.so")
 GPUFIX_LIB = os.path.join(HERE, "_ref", "libawsem_ref_gpufix.so")
 
@@ -54,8 +59,9 @@ def _load_ref(path=REF_LIB):
         lib.ref_uniform.restype = C.c_double
         lib.ref_uniform.argtypes = [C.c_ulonglong, C.c_longlong, C.c_longlong, C.c_int]
         if path == GPUFIX_LIB:
-            lib.ref_create_gpufix.restype = C.c_void_p
-            lib.ref_create_gpufix.argtypes = [C.c_char_p] * 6 + [C.c_double, C.c_int, C.c_int, C.c_int, C.c_int]
+            for fn in (lib.ref_create_gpufix, lib.ref_create_gpupair):
+                fn.restype = C.c_void_p
+                fn.argtypes = [C.c_char_p] * 6 + [C.c_double, C.c_int, C.c_int, C.c_int, C.c_int]
         _libs[path] = lib
     return _libs[path]
 
@@ -63,13 +69,17 @@ def _load_ref(path=REF_LIB):
 class RefSystem:
     """One reference FixBackbone system hosted by the shim MD loop."""
 
-    def __init__(self, files: dict, skin=2.0, every=1, delay=0, check=1, gpu_fix: str | None = None):
-        lib = _load_ref(GPUFIX_LIB if gpu_fix else REF_LIB)
+    def __init__(self, files: dict, skin=2.0, every=1, delay=0, check=1, gpu_fix: str | None = None,
+                 gpu_pair: str | None = None):
+        assert not (gpu_fix and gpu_pair)
+        lib = _load_ref(GPUFIX_LIB if gpu_fix or gpu_pair else REF_LIB)
         self.lib = lib
         args = (files["workdir"].encode(), files["data"].encode(), files["coeff"].encode(), files["seq"].encode(),
                 files["pair_style"].encode(), files["pair_coeffs"].encode(), skin, every, delay, check)
         if gpu_fix:
             self.h = lib.ref_create_gpufix(*args, {"fp64": 0, "mixed": 1}[gpu_fix])
+        elif gpu_pair:
+            self.h = lib.ref_create_gpupair(*args, {"fp64": 0, "mixed": 1}[gpu_pair])
         else:
             self.h = lib.ref_create(*args)
         if not self.h:

@@ -29,6 +29,7 @@
 #include "fix_backbone.h"
 #ifdef AWSEM_GPU_FIX
 #include "fix_backbone_gpu.h"
+#include "pair_excluded_volume_gpu.h"
 #endif
 #include "pair_excluded_volume.h"
 #include "compute_q_onuchic.h"
@@ -132,7 +133,7 @@ struct RefHost {
   LAMMPS *lmp = nullptr;
   Fix *fix = nullptr;
   FixBackbone *fb = nullptr;  // the reference fix (null when the GPU adapter is hosted)
-  PairExcludedVolume *pair = nullptr;
+  Pair *pair = nullptr;
   std::string workdir;
 
   int natoms = 0, ntypes = 0, nbondtypes = 0;
@@ -167,6 +168,8 @@ struct RefHost {
       lmp->memory->destroy(a->x);
       lmp->memory->destroy(a->v);
       lmp->memory->destroy(a->f);
+      if (a->nspecial) lmp->memory->destroy(a->nspecial);
+      if (a->special) lmp->memory->destroy(a->special);
       free(a->tag);
       free(a->type);
       free(a->mask);
@@ -331,6 +334,15 @@ void RefHost::read_data(const std::string &path)
     bond_b.push_back(j);
     special[i].push_back(j);
     special[j].push_back(i);
+  }
+  // LAMMPS's special list of the 1-2 partners (what a pair style reads)
+  size_t maxsp = 1;
+  for (auto &v : special) maxsp = std::max(maxsp, v.size());
+  lmp->memory->create(a->nspecial, natoms, 3, "nspecial");
+  lmp->memory->create(a->special, natoms, (int) maxsp, "special");
+  for (int i = 0; i < natoms; i++) {
+    a->nspecial[i][0] = a->nspecial[i][1] = a->nspecial[i][2] = (int) special[i].size();
+    for (size_t k = 0; k < special[i].size(); k++) a->special[i][k] = a->tag[special[i][k]];
   }
   for (int t = 1; t <= ntypes; t++) a->mass[t] = mass[t];
   for (int k = 0; k < 3; k++) d->periodicity[k] = 0;
@@ -542,7 +554,7 @@ const char *ref_last_error() { return g_ref_err.c_str(); }
    "i j lambda [cs cl]" records; groups by atom type: CA, CB (and H-beta), O. */
 static void *create_host(const char *workdir, const char *data_file, const char *coeff_file,
                          const char *seq_file, const char *pair_style, const char *pair_coeffs,
-                         double skin, int every, int delay, int check, int gpu_fix)
+                         double skin, int every, int delay, int check, int gpu_fix, int gpu_pair = -1)
 {
   RefHost *h = new RefHost();
   try {
@@ -586,10 +598,16 @@ static void *create_host(const char *workdir, const char *data_file, const char 
       if (t == 3) a->mask[i] |= 8;
     }
     // pair vexcluded
-    h->pair = new PairExcludedVolume(lmp);
+#ifdef AWSEM_GPU_FIX
+    if (gpu_pair >= 0)
+      h->pair = new PairExcludedVolumeGPU(lmp);
+    else
+#endif
+      h->pair = new PairExcludedVolume(lmp);
     lmp->force->pair = h->pair;
     {
       auto v = split_ws(pair_style);
+      if (gpu_pair >= 0) v.push_back(gpu_pair == 1 ? "mixed" : "fp64");
       std::vector<char *> args;
       for (auto &s : v) args.push_back(strdup(s.c_str()));
       h->pair->settings((int) args.size(), args.data());
@@ -667,6 +685,16 @@ void *ref_create_gpufix(const char *workdir, const char *data_file, const char *
 {
   return create_host(workdir, data_file, coeff_file, seq_file, pair_style, pair_coeffs, skin, every, delay,
                      check, precision);
+}
+
+/* The same host with the reference fix and `pair_style vexcluded/gpu`
+   (precision 0 FP64, 1 mixed) in place of the reference pair style. */
+void *ref_create_gpupair(const char *workdir, const char *data_file, const char *coeff_file,
+                         const char *seq_file, const char *pair_style, const char *pair_coeffs,
+                         double skin, int every, int delay, int check, int precision)
+{
+  return create_host(workdir, data_file, coeff_file, seq_file, pair_style, pair_coeffs, skin, every, delay,
+                     check, -1, precision);
 }
 #endif
 

@@ -39,6 +39,11 @@ typedef long long bigint;
 
 #define NEIGHMASK 0x1FFFFFFF
 #define SBBITS 30
+// image flags of LAMMPS's default (smallbig) build: three 10-bit fields
+#define IMGMASK 1023
+#define IMGMAX 512
+#define IMGBITS 10
+#define IMG2BITS 20
 static inline int sbmask(int j) { return j >> SBBITS & 3; }
 
 class LAMMPS;
@@ -143,6 +148,10 @@ class Atom {
   double *mass;
   int molecular;
   int tag_enable = 1;
+  // special neighbours: nspecial[i] = cumulative counts of 1-2, 1-3, 1-4
+  // partners, special[i] their atom ids (this host fills the 1-2 ones)
+  int **nspecial = nullptr;
+  tagint **special = nullptr;
   AtomVec *avec;
   AtomVec *style_match(const char *name);
 };

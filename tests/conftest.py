@@ -9,7 +9,9 @@ sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
 
-REFERENCE_SRC = "/root/reference/src"
+from ref import REFERENCE_DIR  # noqa: E402  (oracle/ref.py)
+
+REFERENCE_SRC = os.path.join(REFERENCE_DIR, "src")
 
 
 def pytest_configure(config):
@@ -22,7 +24,7 @@ def oracle_built():
     (only where the reference tree exists)."""
     subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle")], check=True)
     if os.path.isdir(REFERENCE_SRC):
-        subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True)
+        subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref", f"REF={REFERENCE_DIR}"], check=True)
     return True
 
 

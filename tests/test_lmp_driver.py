@@ -9,6 +9,7 @@ import numpy as np
 import pytest
 
 from awsemmd_b200 import lmp
+from ref import REFERENCE_DIR  # oracle/ref.py (on the path via conftest)
 
 DATA = """LAMMPS data file for a test
 
@@ -271,7 +272,7 @@ def test_errors(tmp_path, line, msg):
         run_deck(tmp_path, deck)
 
 
-REF_EXAMPLE = "/root/reference/examples/examples_new/1R69_single_memory"
+REF_EXAMPLE = os.path.join(REFERENCE_DIR, "examples", "examples_new", "1R69_single_memory")
 
 
 @pytest.mark.skipif(not os.path.isdir(REF_EXAMPLE), reason="the reference's example decks are not present")

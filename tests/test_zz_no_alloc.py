@@ -17,7 +17,7 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
-def fm_only_case(tmp_path):
+def fm_only_case(tmp_path, weights="uniform"):
     from awsemmd_b200 import synth
 
     s = synth.make_system([90], box=200.0, seed=515)
@@ -25,18 +25,31 @@ def fm_only_case(tmp_path):
     # a coefficient file whose only term is fragment memory
     with open(os.path.join(files["workdir"], files["coeff"]), "w") as f:
         f.write("[Epsilon]\n1.0\n\n[Fragment_Memory]\n1.0\nfrags.mem\nuniform.gamma\n")
+    if weights == "varied":
+        # memory weights 0.5, 0.75, 1.0, ...: every record carries its own
+        # coefficient (the per-record path of the kernel)
+        path = os.path.join(files["workdir"], "frags.mem")
+        lines = open(path).read().split("\n")
+        k = lines.index("[Memories]") + 1
+        for m in range(k, len(lines)):
+            t = lines[m].split()
+            if len(t) == 5:
+                t[4] = repr(0.5 + 0.25 * ((m - k) % 4))
+                lines[m] = " ".join(t)
+        open(path, "w").write("\n".join(lines))
     return files
 
 
+@pytest.mark.parametrize("weights", ["uniform", "varied"])
 @pytest.mark.parametrize("prec,tol", [("fp64", 1e-12), ("mixed", 1e-12)])
-def test_noalloc_matches_existing_entry_point(prec, tol, tmp_path, gpu_lib):
+def test_noalloc_matches_existing_entry_point(prec, tol, weights, tmp_path, gpu_lib):
     import torch
 
     from awsemmd_b200.engine import TERMS_FIX, AwsemSystem
 
     lib = gpu_lib
     lib.awsem_fragmem_noalloc.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
-    files = fm_only_case(tmp_path)
+    files = fm_only_case(tmp_path, weights)
     with AwsemSystem(files, precision=prec) as s:
         x_ext, _ = s.get_state()
         nat = s.natoms
