@@ -117,6 +117,7 @@ class EngineBase {
   virtual void set_launch_shapes(const int *shapes) = 0;
   virtual void set_neighbor(double skin, int delay, int every, int check) = 0;
   virtual void set_list_built(int built) = 0;
+  virtual void set_wait_limits(long long fm_cycles, long long barrier_cycles, int hold) = 0;
   virtual int q_create(int rep, const std::string &words) = 0;
   virtual double q_value(int qid) = 0;
   virtual void get_step_form(int *out) = 0;
@@ -278,6 +279,8 @@ template <typename R> class Engine : public EngineBase {
     // extent (on a serving handle the used prefix, not the whole capacity)
     a.fm.groups = std::min(fm_groups, (n_run() + 31) / 32);
     a.fm.dsplit = fm_dsplit;
+    a.fm.wait_limit = fm_wait_limit;
+    a.fm.hold_tx = hold_waits ? 16u : 0u;
     a.tb_data = reinterpret_cast<const double2 *>(tb_data.p);
     a.tb_present = tb_present.p;
     a.go_start = go_start.p;
@@ -701,13 +704,23 @@ template <typename R> class Engine : public EngineBase {
       set_list_flags(next_compute_built, 1);
       next_compute_built = 1;
     }
-    auto a = args(groups);
-    launch_eval(a, false);
-    if (lists_emulated()) dev::k_list_hold<R><<<(n_run() + 127) / 128, 128, 0, s0>>>(a);
     int tb = 256;
-    dev::k_total_force<R><<<(3 * na + tb - 1) / tb, tb, 0, s0>>>(a, ftot.p);
-    reduce_energies();
-    CK(cudaGetLastError());
+    for (int attempt = 0; attempt < 2; attempt++) {
+      auto a = args(groups);
+      launch_eval(a, false);
+      if (lists_emulated()) dev::k_list_hold<R><<<(n_run() + 127) / 128, 128, 0, s0>>>(a);
+      dev::k_total_force<R><<<(3 * na + tb - 1) / tb, tb, 0, s0>>>(a, ftot.p);
+      reduce_energies();
+      CK(cudaGetLastError());
+      // an evaluation whose pair list overflowed runs again on a grown list
+      // (it changes no state, unless LAMMPS's lists are emulated, whose
+      // per-step bookkeeping it advances: then the overflow is reported)
+      int ovf = 0;
+      CK(cudaMemcpyAsync(&ovf, &nl.p->overflow, sizeof ovf, cudaMemcpyDeviceToHost, s0));
+      CK(cudaStreamSynchronize(s0));
+      if (!ovf || attempt == 1 || lists_emulated()) break;
+      grow_pairs(ovf);
+    }
     std::vector<double> f((size_t) 3 * na);
     CK(cudaMemcpyAsync(f.data(), ftot.p, sizeof(double) * 3 * na, cudaMemcpyDeviceToHost, s0));
     double e[E_SLOTS];
@@ -727,15 +740,48 @@ template <typename R> class Engine : public EngineBase {
     if (!with_ke) out[E_KIN] = 0.0;
   }
 
+  // Limits of the bounded device waits (SM clock cycles; 0: the defaults).
+  // The graphs carry the old limits as kernel parameters: recaptured.
+  long long fm_wait_limit = dev::kFmWaitLimit, bar_wait_limit = dev::kBarWaitLimit;
+  bool hold_waits = false;  // tests: the waits' conditions are made unreachable, so they run out
+  void set_wait_limits(long long fm_cycles, long long barrier_cycles, int hold) override
+  {
+    if (fm_cycles < 0 || barrier_cycles < 0) throw std::invalid_argument("wait limits must not be negative");
+    fm_wait_limit = fm_cycles ? fm_cycles : dev::kFmWaitLimit;
+    bar_wait_limit = barrier_cycles ? barrier_cycles : dev::kBarWaitLimit;
+    hold_waits = hold != 0;
+    release_graphs();
+  }
+
+  // After a pair-list overflow the list grows to twice what the evaluation
+  // needed (the graphs hold the old buffers and are recaptured), so the next
+  // call runs clean.
+  void grow_pairs(long long needed)
+  {
+    release_graphs();
+    resize_pairs(std::max<long long>(2LL * pcap, 2LL * needed));
+  }
+
   void check_list()
   {
     dev::NLState st;
     CK(cudaMemcpy(&st, nl.p, sizeof st, cudaMemcpyDeviceToHost));
-    if (st.overflow)
-      throw StateError("residue pair list overflow (capacity " + std::to_string(pcap) + " pairs, needed " +
-                       std::to_string(st.overflow) + "); results of this call are invalid");
-    if (st.fm_timeout)
+    if (st.bad_x) {
+      // positions are inputs: the next call with finite ones is clean
+      set_nl_field(&dev::NLState::bad_x, 0);
+      throw StateError("non-finite atom coordinates; results of this call are invalid");
+    }
+    if (st.overflow) {
+      const long long old = pcap;
+      grow_pairs(st.overflow);
+      throw StateError("residue pair list overflow (capacity " + std::to_string(old) + " pairs, needed " +
+                       std::to_string(st.overflow) + "); results of this call are invalid; the capacity is now " +
+                       std::to_string(pcap) + " pairs");
+    }
+    if (st.fm_timeout) {
+      set_nl_field(&dev::NLState::fm_timeout, 0);
       throw StateError("fragment-memory stream: a shared-memory copy wait gave up; results of this call are invalid");
+    }
     if (st.tb_error) {
       // the reference stops the run with these messages (fix_backbone.cpp:4400, :4423)
       const int code = st.tb_error;
@@ -915,7 +961,8 @@ template <typename R> class Engine : public EngineBase {
                        (a.groups & dev::G_FIX) && (in.ff.p.terms & T_AMHGO) ? 1 : 0,
                        (a.groups & dev::G_FIX) && (in.ff.p.terms & (T_SSB | T_DH | T_CONTREST)) ? 1 : 0,
                        lists_emulated() ? n_sys() : 0,
-                       (a.groups & dev::G_FIX) && (in.ff.p.terms & (T_SHAKE | T_MEMB | T_VFM)) ? 1 : 0};
+                       (a.groups & dev::G_FIX) && (in.ff.p.terms & (T_SHAKE | T_MEMB | T_VFM)) ? 1 : 0,
+                       bar_wait_limit, hold_waits ? 1u : 0u};
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(ps_grid_now);
     cfg.blockDim = dim3(dev::kStepThreads);
@@ -2464,6 +2511,13 @@ int awsem_q_value(awsem_system *sys, int qid, double *value)
 {
   if (!ready(sys) || !value) return AWSEM_EINVAL;
   return guarded([&] { *value = sys->eng->q_value(qid); });
+}
+
+int awsem_set_wait_limits(awsem_system *sys, long long fm_copy_wait_cycles, long long grid_barrier_wait_cycles,
+                          int hold)
+{
+  if (!ready(sys)) return AWSEM_EINVAL;
+  return guarded([&] { sys->eng->set_wait_limits(fm_copy_wait_cycles, grid_barrier_wait_cycles, hold); });
 }
 
 int awsem_set_list_built(awsem_system *sys, int built)

@@ -36,6 +36,9 @@ template <typename R> struct FMSlices {
   int nd, min_sep;  // separations min_sep .. min_sep + nd - 1
   int groups;       // G = ceil(n_res / 32)
   int dsplit;       // separation chunks per group (warps per group)
+  long long wait_limit;  // SM clock cycles a warp waits for one stage's copies before it gives up
+  unsigned hold_tx;      // bytes each stage expects beyond its copies: 0, or (tests of the give-up
+                         // path) 16, which never arrive, so every stage wait runs out
 };
 
 // One memory record: 16 bytes (FP32) or 32 bytes (FP64)
@@ -296,7 +299,7 @@ __device__ __forceinline__ bool fragmem_unit_bulk_t(int w, const FMSlices<R> &t,
     const uint32_t rb = ns * 32 * 4 * sizeof(R), cb = coef ? ns * 32 * sizeof(R) : 0;
     // the stage was last read through the generic proxy: order that before the async-proxy write
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    mbar_expect(bar, rb + cb);
+    mbar_expect(bar, rb + cb + t.hold_tx);
     bulk_load(dst, t.rf + (size_t) s0 * 32 * 4, rb, bar);
     if (coef) bulk_load(dst + kFmStripes * 32 * 4 * sizeof(R), t.coef + (size_t) s0 * 32, cb, bar);
   };
@@ -358,7 +361,8 @@ __device__ __forceinline__ bool fragmem_unit_bulk_t(int w, const FMSlices<R> &t,
   int fail_k = 0;
   for (int k = 0; k < nchunks; k++) {
     const int st = (kbase + k) % kFmStages;
-    if (!mbar_wait(bars + 8 * st, ((kbase + k) / kFmStages) & 1, kFmWaitLimit)) {
+    // the warp gives up together (every lane polls the same barrier)
+    if (!__all_sync(0xffffffffu, mbar_wait(bars + 8 * st, ((kbase + k) / kFmStages) & 1, t.wait_limit))) {
       ok = false;
       fail_k = k;
       break;

@@ -62,6 +62,7 @@ struct NLState {
   float lst_pair_cut; // CA-CA reach of the half list (pair-list cutoff + skin) the
                       // CA-pair terms need covered by the residue pair list (0: none)
   float lst_d2max;    // max CA displacement^2 since the last emulated build (this step)
+  int bad_x;          // a position was not finite (results invalid; the host reports and clears it)
 };
 
 // Run window of one replica: integrated over steps begin..end (the
@@ -185,11 +186,14 @@ template <typename R> __device__ __forceinline__ void prepare_pass(const StepArg
     const double *x = a.x;
     int fl = a.s.res_flags[r];
     double ca[3], cb[3], o[3], n[3] = {0, 0, 0}, h[3] = {0, 0, 0}, cp[3] = {0, 0, 0};
+    bool finite = true;
     for (int k = 0; k < 3; k++) {
       ca[k] = x[(3 * r + 0) * 3 + k];
       cb[k] = x[(3 * r + 1) * 3 + k];
       o[k] = x[(3 * r + 2) * 3 + k];
+      finite = finite && isfinite(ca[k]) && isfinite(cb[k]) && isfinite(o[k]);
     }
+    if (!finite) a.nl->bad_x = 1;
     if (!(fl & R_FIRST)) {
       for (int k = 0; k < 3; k++) {
         double ca0 = x[(3 * (r - 1) + 0) * 3 + k], o0 = x[(3 * (r - 1) + 2) * 3 + k];

@@ -130,6 +130,8 @@ template <typename R> dev::FMSlices<R> slices(const FMView &v)
   t.min_sep = v.min_sep;
   t.groups = v.groups;
   t.dsplit = v.dsplit;
+  t.wait_limit = dev::kFmWaitLimit;  // the register-load path used here has no waits
+  t.hold_tx = 0;
   return t;
 }
 

@@ -90,20 +90,20 @@ __device__ __forceinline__ void named_sync(int id, int nthreads)
 // wait gave up) still arrives but does not wait.  Returns the block's ok.
 template <class Serial>
 __device__ __forceinline__ bool grid_sync(GridBar *b, int j, unsigned seen, int id, int nthreads, bool ok,
-                                          Serial serial)
+                                          long long limit, unsigned hold, Serial serial)
 {
   __shared__ int s_ok;
   named_sync(id, nthreads);
   if (threadIdx.x == 0) {
     const unsigned prev = atom_add_acq_rel(&b->arrive[j], 1u);
-    if (prev == gridDim.x - 1) {
+    if (prev == gridDim.x - 1 + hold) {  // hold 1 (tests): no block is the last, every wait runs out
       serial();
       st_relaxed(&b->arrive[j], 0u);  // ordered before the release below
       red_add_release(&b->rel[j], 1u);
     } else if (ok) {
       const long long t0 = clock64();
       for (unsigned it = 1; ld_acquire(&b->rel[j]) == seen; it++)
-        if ((it & 63u) == 0 && clock64() - t0 > kBarWaitLimit) {  // the clock is read every 64th poll
+        if ((it & 63u) == 0 && clock64() - t0 > limit) {  // the clock is read every 64th poll
           atomicExch(&b->timeout, 1);
           ok = false;
           break;
@@ -133,6 +133,8 @@ struct PersistArgs {
   int pair_extra;    // solvent barrier, Debye-Hueckel or contact restraints on
   int list_reps;     // replicas whose LAMMPS lists are emulated (0: none)
   int residue_extra; // Shake or the membrane potential on
+  long long bar_wait_limit;  // SM clock cycles a block waits at a grid barrier before it gives up
+  unsigned hold;             // 0, or 1 (tests of the give-up path): the barriers wait for one block too many
 };
 
 // Fragment-memory units taken from the step's counter until none is left
@@ -190,7 +192,7 @@ template <typename R> __global__ void __launch_bounds__(kStepThreads, 2) k_step(
 
   const Span all{(int) (blockIdx.x * kStepThreads + threadIdx.x), (int) (gridDim.x * kStepThreads)};
   prepare_pass(a, p, all);
-  bool ok = grid_sync(b, 0, seen[0], 0, kStepThreads, true, FirstSerial{a.nl, a.step, b});
+  bool ok = grid_sync(b, 0, seen[0], 0, kStepThreads, true, q.bar_wait_limit, q.hold, FirstSerial{a.nl, a.step, b});
   if ((int) threadIdx.x >= pass_threads) {
     if (ok) fragmem_take_units(a, p, q, ring, wsm, kbase);
   } else {
@@ -201,16 +203,16 @@ template <typename R> __global__ void __launch_bounds__(kStepThreads, 2) k_step(
         list_decide_one(*a.nl, a.lst_ago, a.lst_over, const_cast<int *>(a.lst_build), r);
     if (a.nl->rebuild) {
       if (ok) nl_build_pass(a, GridArgs{}, q.n_launch, sp);
-      ok = grid_sync(b, 1, seen[1], 1, pass_threads, ok, NoSerial{});
+      ok = grid_sync(b, 1, seen[1], 1, pass_threads, ok, q.bar_wait_limit, q.hold, NoSerial{});
     }
     if (ok) density_pass(a, p, sp);
-    ok = grid_sync(b, 2, seen[2], 1, pass_threads, ok, NoSerial{});
+    ok = grid_sync(b, 2, seen[2], 1, pass_threads, ok, q.bar_wait_limit, q.hold, NoSerial{});
     if (ok) residue_pass(a, p, sp);
-    ok = grid_sync(b, 3, seen[3], 1, pass_threads, ok, NoSerial{});
+    ok = grid_sync(b, 3, seen[3], 1, pass_threads, ok, q.bar_wait_limit, q.hold, NoSerial{});
     if (ok) water_xi_pass(a, p, sp);
-    ok = grid_sync(b, 4, seen[4], 1, pass_threads, ok, NoSerial{});
+    ok = grid_sync(b, 4, seen[4], 1, pass_threads, ok, q.bar_wait_limit, q.hold, NoSerial{});
     if (ok) pair_pass(a, p, sp);
-    ok = grid_sync(b, 5, seen[5], 1, pass_threads, ok, NoSerial{});
+    ok = grid_sync(b, 5, seen[5], 1, pass_threads, ok, q.bar_wait_limit, q.hold, NoSerial{});
     if (ok) {
       hbond_pass(a, p, sp);
       if (q.fm_table) fm_table_pass(a, p, sp);
@@ -221,7 +223,7 @@ template <typename R> __global__ void __launch_bounds__(kStepThreads, 2) k_step(
     }
   }
   // thread 0 (a pass thread) carries the block's state into the last barrier
-  ok = grid_sync(b, 6, seen[6], 0, kStepThreads, ok, NoSerial{});
+  ok = grid_sync(b, 6, seen[6], 0, kStepThreads, ok, q.bar_wait_limit, q.hold, NoSerial{});
   if (ok) finish_pass(a, q.integ, q.g1, q.g2, q.ftot, q.x_out, all);
 }
 

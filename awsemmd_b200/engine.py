@@ -103,6 +103,7 @@ def load_library(path: str = LIB_PATH):
     lib.awsem_forces.argtypes = [vp, vp]
     lib.awsem_residue_arrays.argtypes = [vp, vp]
     lib.awsem_debug_selections.argtypes = [vp, C.c_longlong, vp, vp, C.c_longlong, C.POINTER(C.c_longlong)]
+    lib.awsem_set_wait_limits.argtypes = [vp, C.c_longlong, C.c_longlong, ip]
     lib.awsem_neighbor_stats.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_double), C.POINTER(C.c_int),
                                          C.POINTER(C.c_int)]
     lib.awsem_last_run_ms.argtypes = [vp]
@@ -345,6 +346,13 @@ class AwsemSystem:
         v = C.c_double()
         _check(self.lib, self.lib.awsem_q_value(self.h, int(qid), C.byref(v)), "awsem_q_value")
         return v.value
+
+    def set_wait_limits(self, fm_cycles: int = 0, barrier_cycles: int = 0, hold: bool = False) -> None:
+        """Limits of the bounded device waits in SM clock cycles (0: the
+        defaults); hold=True (tests) makes every wait run out
+        (awsem_set_wait_limits)"""
+        _check(self.lib, self.lib.awsem_set_wait_limits(self.h, int(fm_cycles), int(barrier_cycles), int(hold)),
+               "awsem_set_wait_limits")
 
     def set_step_form(self, form: str, blocks: int = 0, stream_warps: int = 2) -> None:
         """'kernels': each MD step a graph of per-pass kernels; 'persistent':

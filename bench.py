@@ -508,13 +508,32 @@ def build_c3(n: int, rank: int, precision: str, dev: int, tmp: str):
     return AwsemBatch.from_arrays(ff, chains, precision=precision, device=dev, seeds=seeds), sum(lens), ff, lens
 
 
+def free_port() -> int:
+    import socket
+
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        return sk.getsockname()[1]
+
+
+def launch_command(argv, n: int, port: int):
+    """The command that runs this benchmark as n ranks, one process per GPU,
+    when it was started plainly with --gpus n (no torchrun around it)."""
+    return [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={n}",
+            "--master-addr", "127.0.0.1", f"--master-port={port}", os.path.abspath(__file__)] + list(argv)
+
+
 def main():
     args = parse()
+    if args.impl == "ours" and args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        sys.exit(subprocess.call(launch_command(sys.argv[1:], args.gpus, free_port())))
     dist = Dist()
     if args.impl == "reference":
         reference_arm(args, dist)
         dist.close()
         return
+    if dist.world != args.gpus:
+        raise SystemExit(f"bench.py: --gpus {args.gpus} but {dist.world} ranks are running")
     import torch
 
     from awsemmd_b200 import build

@@ -197,9 +197,13 @@ int awsem_nres(const awsem_system *sys);
 /* Drop-in force call: forces at the caller's positions x are ADDED into f
  * (the fix adds into atom->f during pre_force), energies (may be NULL) are
  * written.  `terms` selects AWSEM_TERMS_* groups.  The residue pair list is
- * kept between calls and rebuilt when the displacement check requires it.
- * Replaces FixBackbone::pre_force (src/fix_backbone.cpp:8181) and, with
- * AWSEM_TERMS_PAIR, PairExcludedVolume::compute. */
+ * kept between calls and rebuilt when the displacement check requires it;
+ * when it outgrows its capacity it is enlarged and the evaluation repeated
+ * (with LAMMPS's lists emulated the call returns AWSEM_ESTATE instead and
+ * the next one runs on the enlarged list).  Non-finite positions make the
+ * call return AWSEM_ESTATE.  Replaces FixBackbone::pre_force
+ * (src/fix_backbone.cpp:8181) and, with AWSEM_TERMS_PAIR,
+ * PairExcludedVolume::compute. */
 int awsem_compute(awsem_system *sys, long long step, const double *x, double *f, double *energies, int terms);
 
 /* Device-resident state of a single-system handle (caller atom order);
@@ -256,6 +260,20 @@ int awsem_residue_arrays(awsem_system *sys, double *out);
  * PairExcludedVolume::compute (src/pair_excluded_volume.cpp:50-138). */
 int awsem_debug_selections(awsem_system *sys, long long step, const double *x, unsigned long long *keys,
                            long long cap, long long *count);
+
+/* Limits of the bounded waits in device code, in SM clock cycles (0: the
+ * defaults, about two seconds for a fragment-memory warp waiting on its
+ * shared-memory copies and one second for a block of the persistent step
+ * form waiting at a grid barrier).  A wait that runs out gives up, the kernel
+ * ends normally (a fragment-memory warp first lets its copies in flight land,
+ * waiting a fixed quarter second at most) and the call returns AWSEM_ESTATE
+ * ("results of this call are invalid"); the next call runs clean.  hold != 0,
+ * for tests of those paths only, makes the waits' conditions unreachable
+ * (each copy stage expects 16 bytes that never arrive; each grid barrier one
+ * block more than the grid), so every wait runs out; hold 0 restores normal
+ * waits.  No counterpart in the reference (LAMMPS has no device waits). */
+int awsem_set_wait_limits(awsem_system *sys, long long fm_copy_wait_cycles, long long grid_barrier_wait_cycles,
+                          int hold);
 
 /* Pair-list statistics: builds so far, current list radius (A), largest
  * number of higher-numbered partners of one residue, overflow marker (0 when

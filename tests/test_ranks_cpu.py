@@ -43,3 +43,25 @@ def test_two_gloo_ranks_replicas_only():
     assert [g[0] for g in got] == [0, 1] and all(g[1] == 2 for g in got)
     assert all(g[2] == 2.0 for g in got)  # max over ranks
     assert not set(got[0][3]) & set(got[1][3])  # each rank its own replicas
+
+
+def test_plain_launch_with_several_gpus_starts_one_rank_per_gpu():
+    sys.path.insert(0, ROOT)
+    import bench
+
+    cmd = bench.launch_command(["--gpus", "4", "--steps", "3"], 4, 29533)
+    assert cmd[1:3] == ["-m", "torch.distributed.run"]
+    assert "--nproc-per-node=4" in cmd and "--master-addr" in cmd and "127.0.0.1" in cmd
+    assert cmd[-4:] == ["--gpus", "4", "--steps", "3"] and cmd[-5].endswith("bench.py")
+
+
+def test_rank_count_must_match_gpus():
+    """Two ranks started for --gpus 3: every rank stops before any work, and
+    the launcher reports the failure (gloo on the CPU)."""
+    import subprocess
+
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node=2", "--master-addr",
+           "127.0.0.1", f"--master-port={_free_port()}", os.path.join(ROOT, "bench.py"), "--gpus", "3"]
+    p = subprocess.run(cmd, capture_output=True, text=True, timeout=300, env=dict(os.environ, CUDA_VISIBLE_DEVICES=""))
+    assert p.returncode != 0
+    assert "--gpus 3 but 2 ranks" in p.stdout + p.stderr
