@@ -95,6 +95,13 @@ __device__ __forceinline__ long long fix_dens(double v) { return __double2ll_rn(
 // boundaries (res_flags, chain_start/end) keep index arithmetic inside a
 // chain, and `res_chain` is globally unique so different systems never
 // match as "same chain".
+// A block's shared-memory force accumulator over residues [r0, r0 + n) in
+// the facc layout ([residue][bead][3], 2^-32 fixed point); n == 0: none.
+struct ForceWindow {
+  uint32_t addr;  // shared-state-space address
+  int r0, n;
+};
+
 template <typename R> struct DevSys {
   int n_res;
   const int *res_type, *res_flags, *res_chain, *chain_start, *chain_end;
@@ -102,6 +109,7 @@ template <typename R> struct DevSys {
   const double *tables; // TB_SIZE
   const double4 *pos;            // [n_res][6] working coordinates (FP64 in both forms)
   unsigned long long *facc;      // [n_res*3][3] fixed-point forces
+  ForceWindow win;               // residues whose forces the block sums in shared memory first
 };
 
 // The same system viewed with FP64 geometry (the storage is type independent).
@@ -118,6 +126,7 @@ template <typename R> __device__ __forceinline__ DevSys<double> widen(const DevS
   d.tables = s.tables;
   d.pos = s.pos;
   d.facc = s.facc;
+  d.win = s.win;
   return d;
 }
 
@@ -135,12 +144,23 @@ template <typename R> __device__ __forceinline__ V3<R> diff(V3<double> a, V3<dou
   return {(R) (a.x - b.x), (R) (a.y - b.y), (R) (a.z - b.z)};
 }
 
+// Add a force to bead b of residue r: converted to fixed point first, then
+// summed in the block's shared-memory window when r lies in it (flushed to
+// facc by the block), else added to facc directly.
 template <typename R> __device__ __forceinline__ void scatter(const DevSys<R> &s, int r, int b, R fx, R fy, R fz)
 {
+  const long long v[3] = {fix_force((double) fx), fix_force((double) fy), fix_force((double) fz)};
+  if ((unsigned) (r - s.win.r0) < (unsigned) s.win.n) {
+    const uint32_t q = s.win.addr + (uint32_t) (((r - s.win.r0) * 3 + b) * 3) * 8u;
+#pragma unroll
+    for (int c = 0; c < 3; c++)
+      if (v[c]) asm volatile("red.shared.add.u64 [%0], %1;" ::"r"(q + 8u * c), "l"(v[c]) : "memory");
+    return;
+  }
   unsigned long long *p = s.facc + ((size_t) 3 * r + b) * 3;
-  atomicAdd(p + 0, (unsigned long long) fix_force((double) fx));
-  atomicAdd(p + 1, (unsigned long long) fix_force((double) fy));
-  atomicAdd(p + 2, (unsigned long long) fix_force((double) fz));
+#pragma unroll
+  for (int c = 0; c < 3; c++)
+    if (v[c]) atomicAdd(p + c, (unsigned long long) v[c]);
 }
 
 template <typename R> __device__ __forceinline__ void scatter(const DevSys<R> &s, int r, int b, V3<R> f)

@@ -280,7 +280,7 @@ template <typename R> class Engine : public EngineBase {
     a.fm.groups = std::min(fm_groups, (n_run() + 31) / 32);
     a.fm.dsplit = fm_dsplit;
     a.fm.wait_limit = fm_wait_limit;
-    a.fm.hold_tx = hold_waits ? 16u : 0u;
+    a.fm.hold_tx = (hold_waits & 1) ? 16u : 0u;
     a.tb_data = reinterpret_cast<const double2 *>(tb_data.p);
     a.tb_present = tb_present.p;
     a.go_start = go_start.p;
@@ -646,11 +646,19 @@ template <typename R> class Engine : public EngineBase {
       if (rx) dev::k_residue_extra<R><<<nb, tb, 0, s1>>>(a, p);
       CK(cudaEventRecord(ev_join, s1));
     }
-    dev::k_density<R><<<pair_blocks, tb, 0, s0>>>(a, p);
-    dev::k_residue<R><<<nb, tb, 0, s0>>>(a, p);
-    dev::k_water_xi<R><<<pair_blocks, tb, 0, s0>>>(a, p);
-    dev::k_pair<R><<<pair_blocks, tb, 0, s0>>>(a, p);
-    dev::k_hbond<R><<<hb_blocks, 128, 0, s0>>>(a, p);
+    if (a.sel) {  // awsem_debug_selections: the same passes, recording their selections
+      dev::k_density_sel<R><<<pair_blocks, tb, 0, s0>>>(a, p);
+      dev::k_residue_sel<R><<<nb, tb, 0, s0>>>(a, p);
+      dev::k_water_xi_sel<R><<<pair_blocks, tb, 0, s0>>>(a, p);
+      dev::k_pair_sel<R><<<pair_blocks, tb, 0, s0>>>(a, p);
+      dev::k_hbond_sel<R><<<hb_blocks, 128, 0, s0>>>(a, p);
+    } else {
+      dev::k_density<R><<<pair_blocks, tb, 0, s0>>>(a, p);
+      dev::k_residue<R><<<nb, tb, 0, s0>>>(a, p);
+      dev::k_water_xi<R><<<pair_blocks, tb, 0, s0>>>(a, p);
+      dev::k_pair<R><<<pair_blocks, tb, 0, s0>>>(a, p);
+      dev::k_hbond<R><<<hb_blocks, 128, 0, s0>>>(a, p);
+    }
     if (fm || fmt || go || px || rx) CK(cudaStreamWaitEvent(s0, ev_join, 0));
   }
 
@@ -743,13 +751,14 @@ template <typename R> class Engine : public EngineBase {
   // Limits of the bounded device waits (SM clock cycles; 0: the defaults).
   // The graphs carry the old limits as kernel parameters: recaptured.
   long long fm_wait_limit = dev::kFmWaitLimit, bar_wait_limit = dev::kBarWaitLimit;
-  bool hold_waits = false;  // tests: the waits' conditions are made unreachable, so they run out
+  int hold_waits = 0;  // tests: bit 0 copy waits, bit 1 grid barriers made unreachable, so they run out
   void set_wait_limits(long long fm_cycles, long long barrier_cycles, int hold) override
   {
     if (fm_cycles < 0 || barrier_cycles < 0) throw std::invalid_argument("wait limits must not be negative");
     fm_wait_limit = fm_cycles ? fm_cycles : dev::kFmWaitLimit;
     bar_wait_limit = barrier_cycles ? barrier_cycles : dev::kBarWaitLimit;
-    hold_waits = hold != 0;
+    if (hold < 0 || hold > 3) throw std::invalid_argument("hold must be 0..3");
+    hold_waits = hold;
     release_graphs();
   }
 
@@ -962,7 +971,7 @@ template <typename R> class Engine : public EngineBase {
                        (a.groups & dev::G_FIX) && (in.ff.p.terms & (T_SSB | T_DH | T_CONTREST)) ? 1 : 0,
                        lists_emulated() ? n_sys() : 0,
                        (a.groups & dev::G_FIX) && (in.ff.p.terms & (T_SHAKE | T_MEMB | T_VFM)) ? 1 : 0,
-                       bar_wait_limit, hold_waits ? 1u : 0u};
+                       bar_wait_limit, (hold_waits & 2) ? 1u : 0u};
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(ps_grid_now);
     cfg.blockDim = dim3(dev::kStepThreads);

@@ -153,10 +153,13 @@ __device__ __forceinline__ Span grid_span()
   return Span{(int) (blockIdx.x * blockDim.x + threadIdx.x), (int) (gridDim.x * blockDim.x)};
 }
 
-// one selection record (AWSEM_SEL_* key, awsem_gpu.h) when the evaluation records them
-template <typename R> __device__ __forceinline__ void sel_rec(const StepArgs<R> &a, int kind, int aux, int i, int j)
+// one selection record (AWSEM_SEL_* key, awsem_gpu.h).  The passes take SEL
+// as a template flag: the per-step kernels are compiled without recording
+// (SEL false), the diagnostic kernels of awsem_debug_selections with it.
+template <bool SEL, typename R>
+__device__ __forceinline__ void sel_rec(const StepArgs<R> &a, int kind, int aux, int i, int j)
 {
-  if (!a.sel) return;
+  if (!SEL || !a.sel) return;
   const unsigned long long k = atomicAdd(a.sel_n, 1ull);
   if (k < (unsigned long long) a.sel_cap)
     a.sel[k] = (unsigned long long) kind << 56 | (unsigned long long) aux << 44 | (unsigned long long) i << 22 |
@@ -571,7 +574,7 @@ template <typename R> __global__ void k_nl_build(StepArgs<R> a, GridArgs g, int 
 // in both forms: the densities feed the burial and switching functions, and
 // the well selection is then the reference's exactly.  Sums in 2^-40 fixed
 // point (dacc[0], dacc[1]).
-template <typename R> __device__ __forceinline__ void density_pass(const StepArgs<R> &a, const FFParams &p, Span sp)
+template <typename R, bool SEL = false> __device__ __forceinline__ void density_pass(const StepArgs<R> &a, const FFParams &p, Span sp)
 {
   const DevSys<R> &s = a.s;
   const int n = s.n_res;
@@ -590,7 +593,7 @@ template <typename R> __device__ __forceinline__ void density_pass(const StepArg
       const unsigned long long v = (unsigned long long) fix_dens(th);
       atomicAdd(aw + i, v);
       atomicAdd(aw + j, v);
-      sel_rec(a, AWSEM_SEL_DENS_WATER, 0, i, j);
+      sel_rec<SEL>(a, AWSEM_SEL_DENS_WATER, 0, i, j);
     }
     if (helix && rsq > p.h_rmin_sq && rsq < p.h_rmax_sq) {
       double th, pr;
@@ -598,12 +601,16 @@ template <typename R> __device__ __forceinline__ void density_pass(const StepArg
       const unsigned long long v = (unsigned long long) fix_dens(th);
       atomicAdd(ah + i, v);
       atomicAdd(ah + j, v);
-      sel_rec(a, AWSEM_SEL_DENS_HELIX, 0, i, j);
+      sel_rec<SEL>(a, AWSEM_SEL_DENS_HELIX, 0, i, j);
     }
   }
 }
 
 template <typename R> __global__ void k_density(StepArgs<R> a, FFParams p) { density_pass(a, p, grid_span()); }
+template <typename R> __global__ void k_density_sel(StepArgs<R> a, FFParams p)
+{
+  density_pass<R, true>(a, p, grid_span());
+}
 
 // density sums -> values: k = 0 water density, 1 helix density
 template <typename R> __device__ __forceinline__ double density(const StepArgs<R> &a, int k, int r)
@@ -644,9 +651,8 @@ __device__ __forceinline__ R ev_pair(const StepArgs<R> &a, int ta, int tb, bool 
 
 // bond_style harmonic, the bonds whose first atom is in residue r (run by
 // k_residue's thread of that residue)
-template <typename R> __device__ __forceinline__ void bonds_of(const StepArgs<R> &a, int r)
+template <typename R> __device__ __forceinline__ void bonds_of(const StepArgs<R> &a, const DevSys<R> &s, int r)
 {
-  const DevSys<R> &s = a.s;
   double e = 0.0;
   for (int b = r * a.bond_cap; b < (r + 1) * a.bond_cap && a.bond_i[b] >= 0; b++) {
     int ai = a.bond_i[b], aj = a.bond_j[b];
@@ -663,9 +669,11 @@ template <typename R> __device__ __forceinline__ void bonds_of(const StepArgs<R>
 }
 
 // SL and the per-residue backbone terms
-template <typename R> __device__ __forceinline__ void residue_one(const StepArgs<R> &a, const FFParams &p, int i)
+template <typename R, bool SEL = false>
+__device__ __forceinline__ void residue_one(const StepArgs<R> &a, const FFParams &p, int i, ForceWindow win = {})
 {
-  const DevSys<R> &s = a.s;
+  DevSys<R> s = a.s;
+  s.win = win;
   // the per-residue backbone terms (chain, chi, rama, helical pair) are a
   // small share of the work and some are sums of steep Gaussians: FP64 in
   // both forms
@@ -711,8 +719,8 @@ template <typename R> __device__ __forceinline__ void residue_one(const StepArgs
       double shj, shpj;
       switching(density(a, 1, j), p.helix_kappa_sigma, p.helix_treshold, shj, shpj);
       unsigned gate = 0;
-      eh = (double) helix_pair(sd, p, i, j, sh, shp, shj, shpj, x1, x2, &gate);
-      sel_rec(a, AWSEM_SEL_HELIX_PAIR, (int) gate, i, j);
+      eh = (double) helix_pair(sd, p, i, j, sh, shp, shj, shpj, x1, x2, SEL ? &gate : nullptr);
+      sel_rec<SEL>(a, AWSEM_SEL_HELIX_PAIR, (int) gate, i, j);
     }
   }
   a.xi1[i] = x1;
@@ -735,8 +743,8 @@ template <typename R> __device__ __forceinline__ void residue_one(const StepArgs
       V3<R> f;
       bool hit = false;
       R e = ev_pair(a, a.atom_type[3 * i + b0], a.atom_type[3 * i + b1], true,
-                    diff<R>(bead(s, i, b0), bead(s, i, b1)), f, &hit);
-      if (hit) sel_rec(a, AWSEM_SEL_EV, 3 * b0 + b1, i, i);
+                    diff<R>(bead(s, i, b0), bead(s, i, b1)), f, SEL ? &hit : nullptr);
+      if (hit) sel_rec<SEL>(a, AWSEM_SEL_EV, 3 * b0 + b1, i, i);
       if (e != R(0) || f.x != R(0) || f.y != R(0) || f.z != R(0)) {
         ev += (double) e;
         scatter(s, i, b0, f);
@@ -744,21 +752,53 @@ template <typename R> __device__ __forceinline__ void residue_one(const StepArgs
       }
     }
   E[(size_t) E_PAIR * n + i] = ev;
-  if (a.groups & G_BOND) bonds_of(a, i);
+  if (a.groups & G_BOND) bonds_of(a, s, i);
 }
 
-template <typename R> __device__ __forceinline__ void residue_pass(const StepArgs<R> &a, const FFParams &p, Span sp)
+template <typename R, bool SEL = false> __device__ __forceinline__ void residue_pass(const StepArgs<R> &a, const FFParams &p, Span sp)
 {
   for (int i = sp.t; i < a.n_run; i += sp.nthr)
-    if (a.res_sys[i] >= 0) residue_one(a, p, i);
+    if (a.res_sys[i] >= 0) residue_one<R, SEL>(a, p, i);
 }
 
-template <typename R> __global__ void k_residue(StepArgs<R> a, FFParams p) { residue_pass(a, p, grid_span()); }
+// The standalone residue kernel: 128 residues per block and iteration; the
+// forces its terms push to residues r0 - 1 .. r0 + 127 + helix_i_diff (the
+// helical pair reaches i + 4) are summed in shared memory and flushed with
+// one global atomic per non-zero component.  Each contribution is converted
+// to fixed point before it is summed, so the result is the direct scatter's
+// bit for bit.
+constexpr int kResBlock = 128, kResHalo = 5, kResWin = kResBlock + kResHalo;
+template <typename R, bool SEL> __device__ __forceinline__ void residue_pass_window(const StepArgs<R> &a, const FFParams &p)
+{
+  __shared__ unsigned long long acc[kResWin * 9];
+  const uint32_t addr = (uint32_t) __cvta_generic_to_shared(acc);
+  for (int r0 = blockIdx.x * kResBlock; r0 < a.n_run; r0 += gridDim.x * kResBlock) {
+    for (int k = threadIdx.x; k < kResWin * 9; k += kResBlock) acc[k] = 0ull;
+    __syncthreads();
+    const int i = r0 + threadIdx.x;
+    if (i < a.n_run && a.res_sys[i] >= 0) residue_one<R, SEL>(a, p, i, ForceWindow{addr, r0 - 1, kResWin});
+    __syncthreads();
+    for (int k = threadIdx.x; k < kResWin * 9; k += kResBlock) {
+      const unsigned long long v = acc[k];
+      const int r = r0 - 1 + k / 9;
+      if (v && r >= 0 && r < a.s.n_res) atomicAdd(a.s.facc + (size_t) 9 * r + k % 9, v);
+    }
+    __syncthreads();
+  }
+}
+template <typename R> __global__ void __launch_bounds__(kResBlock) k_residue(StepArgs<R> a, FFParams p)
+{
+  residue_pass_window<R, false>(a, p);
+}
+template <typename R> __global__ void __launch_bounds__(kResBlock) k_residue_sel(StepArgs<R> a, FFParams p)
+{
+  residue_pass_window<R, true>(a, p);
+}
 
 // DL2: water-mediated density derivative coefficients (fix_backbone.cpp:
 // 7877-7954): raw sums in dacc[2] (2^-40 fixed point); xi_water(i) is that
 // sum times sigma_water'(i) (water_xi below).
-template <typename R> __device__ __forceinline__ void water_xi_pass(const StepArgs<R> &a, const FFParams &p, Span sp)
+template <typename R, bool SEL = false> __device__ __forceinline__ void water_xi_pass(const StepArgs<R> &a, const FFParams &p, Span sp)
 {
   const DevSys<R> &s = a.s;
   if (!(p.terms & T_WATER) || !(a.groups & G_FIX)) return;
@@ -779,7 +819,7 @@ template <typename R> __device__ __forceinline__ void water_xi_pass(const StepAr
       const double g0 = W[w * 800 + (ti * 20 + tj) * 2], g1 = W[w * 800 + (ti * 20 + tj) * 2 + 1];
       // the reference's `!fabs(g0 - g1) < delta` holds exactly when g0 != g1
       if (g0 != g1 && rsq > R(p.w_rmin_sq[w]) && rsq < R(p.w_rmax_sq[w])) {
-        sel_rec(a, AWSEM_SEL_XI_WATER, w, i, j);
+        sel_rec<SEL>(a, AWSEM_SEL_XI_WATER, w, i, j);
         R th, pr;
         well_theta(m_sqrt(rsq), R(p.w_rmin_th[w]), R(p.w_rmax_th[w]), R(p.water_kappa), R(p.well_rmin[w]),
                    R(p.well_rmax[w]), th, pr);
@@ -792,6 +832,10 @@ template <typename R> __device__ __forceinline__ void water_xi_pass(const StepAr
 }
 
 template <typename R> __global__ void k_water_xi(StepArgs<R> a, FFParams p) { water_xi_pass(a, p, grid_span()); }
+template <typename R> __global__ void k_water_xi_sel(StepArgs<R> a, FFParams p)
+{
+  water_xi_pass<R, true>(a, p, grid_span());
+}
 
 template <typename R> __device__ __forceinline__ double water_xi(const StepArgs<R> &a, int r)
 {
@@ -811,7 +855,7 @@ template <typename R> __device__ __forceinline__ void scatter_fix(const DevSys<R
 // and excluded volume are applied to both residues.  DSSP and P_AP pairs are
 // only detected here (cheap distance and index tests) and queued: k_hbond
 // evaluates them, so their long, branchy bodies do not slow this pass.
-template <typename R> __device__ __forceinline__ void pair_pass(const StepArgs<R> &a, const FFParams &p, Span sp)
+template <typename R, bool SEL = false> __device__ __forceinline__ void pair_pass(const StepArgs<R> &a, const FFParams &p, Span sp)
 {
   const DevSys<R> &s = a.s;
   const int n = s.n_res;
@@ -875,8 +919,8 @@ template <typename R> __device__ __forceinline__ void pair_pass(const StepArgs<R
         if (norm2(dd) > ev_max_sq) continue;  // beyond every cutoff: no table lookups
         V3<R> f;
         bool hit = false;
-        const R e = ev_pair(a, tai[b0], tb, shortr, dd, f, &hit);
-        if (hit) sel_rec(a, AWSEM_SEL_EV, 3 * b0 + b1, i, j);
+        const R e = ev_pair(a, tai[b0], tb, shortr, dd, f, SEL ? &hit : nullptr);
+        if (hit) sel_rec<SEL>(a, AWSEM_SEL_EV, 3 * b0 + b1, i, j);
         if (e == R(0) && f.x == R(0) && f.y == R(0) && f.z == R(0)) continue;
         ee += (double) e;
         const long long v[3] = {fix_force((double) f.x), fix_force((double) f.y), fix_force((double) f.z)};
@@ -933,7 +977,7 @@ template <typename R> __device__ __forceinline__ void pair_pass(const StepArgs<R
         for (int w = 0; w < p.n_wells; w++) {
           if (!p.well_flag[w]) continue;
           if (sep && rsq > R(p.w_rmin_sq[w]) && rsq < R(p.w_rmax_sq[w])) {
-            sel_rec(a, AWSEM_SEL_WATER, w, i, j);
+            sel_rec<SEL>(a, AWSEM_SEL_WATER, w, i, j);
             const double g0 = W[w * 800 + (ti * 20 + tj) * 2], g1 = W[w * 800 + (ti * 20 + tj) * 2 + 1];
             const double sg = fabs(g0 - g1) < 1e-5 ? 0.5 * (g0 + g1) : g0 + (g1 - g0) * a.sig_w[i] * a.sig_w[j];
             R th, pr;
@@ -953,7 +997,7 @@ template <typename R> __device__ __forceinline__ void pair_pass(const StepArgs<R
           const int on = (fabs(xi_i) > 1e-8 ? 1 : 0) | (fabs(xi_j) > 1e-8 ? 2 : 0);
           if (on & 1) force = madd(pr0, R(xi_i), force);
           if (on & 2) force = madd(pr0, R(xi_j), force);
-          if (on) sel_rec(a, AWSEM_SEL_XI_FORCE, on, i, j);
+          if (on) sel_rec<SEL>(a, AWSEM_SEL_XI_FORCE, on, i, j);
         }
       }
       if ((T & T_BURIAL) && in0) force = madd(R(a.bur[i] + a.bur[j]), pr0, force);
@@ -962,7 +1006,7 @@ template <typename R> __device__ __forceinline__ void pair_pass(const StepArgs<R
         if (i - dh >= 0) fac += a.xi2[i - dh];
         if (j - dh >= 0) fac += a.xi2[j - dh];
         if (fabs(fac) > 1e-6) {
-          sel_rec(a, AWSEM_SEL_HELIX_FORCE, 0, i, j);
+          sel_rec<SEL>(a, AWSEM_SEL_HELIX_FORCE, 0, i, j);
           R th, pr;
           well_theta(r, R(p.h_rmin_th), R(p.h_rmax_th), R(p.helix_kappa), R(p.helix_rmin), R(p.helix_rmax), th, pr);
           force = madd(-R(fac), pr, force);
@@ -1016,13 +1060,17 @@ template <typename R> __global__ void __launch_bounds__(128, 6) k_pair(StepArgs<
 {
   pair_pass(a, p, grid_span());
 }
+template <typename R> __global__ void __launch_bounds__(128) k_pair_sel(StepArgs<R> a, FFParams p)
+{
+  pair_pass<R, true>(a, p, grid_span());
+}
 
 // DSSP hydrogen bonds and P_AP of the queued pairs, one thread per entry
 // (grid-stride over both queues).  A DSSP entry q >= 0 is pair q with O(i)
 // as acceptor; ~q is the same pair with O(j).  Forces scatter with
 // fixed-point atomics; each pair's energy goes to its acceptor (DSSP) or
 // lower residue (P_AP) in fixed point, so sums do not depend on the order.
-template <typename R> __device__ __forceinline__ void hbond_pass(const StepArgs<R> &a, const FFParams &p, Span sp)
+template <typename R, bool SEL = false> __device__ __forceinline__ void hbond_pass(const StepArgs<R> &a, const FFParams &p, Span sp)
 {
   const DevSys<R> &s = a.s;
   const int nd = a.nl->n_dssp, np = a.nl->n_pap, n = s.n_res;
@@ -1032,8 +1080,8 @@ template <typename R> __device__ __forceinline__ void hbond_pass(const StepArgs<
     const int2 ij = a.pairs[q < 0 ? ~q : q];
     const int i = q < 0 ? ij.y : ij.x, j = q < 0 ? ij.x : ij.y;
     unsigned gate = 0;
-    const R e = d ? dssp_term(s, p, i, j, &gate) : pap_term(s, p, i, j, &gate);
-    sel_rec(a, d ? AWSEM_SEL_DSSP : AWSEM_SEL_PAP, (int) gate, i, j);
+    const R e = d ? dssp_term(s, p, i, j, SEL ? &gate : nullptr) : pap_term(s, p, i, j, SEL ? &gate : nullptr);
+    sel_rec<SEL>(a, d ? AWSEM_SEL_DSSP : AWSEM_SEL_PAP, (int) gate, i, j);
     if (e != R(0))
       atomicAdd((unsigned long long *) (a.e_fix + (d ? 0 : (size_t) n) + i), (unsigned long long) fix_force((double) e));
   }
@@ -1042,6 +1090,10 @@ template <typename R> __device__ __forceinline__ void hbond_pass(const StepArgs<
 template <typename R> __global__ void __launch_bounds__(128, 6) k_hbond(StepArgs<R> a, FFParams p)
 {
   hbond_pass(a, p, grid_span());
+}
+template <typename R> __global__ void __launch_bounds__(128) k_hbond_sel(StepArgs<R> a, FFParams p)
+{
+  hbond_pass<R, true>(a, p, grid_span());
 }
 
 // Fragment memory: sliced lane-interleaved table, lane per residue row

@@ -347,10 +347,10 @@ class AwsemSystem:
         _check(self.lib, self.lib.awsem_q_value(self.h, int(qid), C.byref(v)), "awsem_q_value")
         return v.value
 
-    def set_wait_limits(self, fm_cycles: int = 0, barrier_cycles: int = 0, hold: bool = False) -> None:
+    def set_wait_limits(self, fm_cycles: int = 0, barrier_cycles: int = 0, hold: int = 0) -> None:
         """Limits of the bounded device waits in SM clock cycles (0: the
-        defaults); hold=True (tests) makes every wait run out
-        (awsem_set_wait_limits)"""
+        defaults); hold (tests) makes waits run out: bit 0 the fragment-memory
+        copy waits, bit 1 the grid barriers (awsem_set_wait_limits)"""
         _check(self.lib, self.lib.awsem_set_wait_limits(self.h, int(fm_cycles), int(barrier_cycles), int(hold)),
                "awsem_set_wait_limits")
 

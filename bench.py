@@ -80,8 +80,12 @@ def parse():
     ap.add_argument("--no-baseline", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--shapes", default=None,
                     help="launch shapes d,p,h,f (as autotune reports them) instead of autotuning, e.g. for profiling")
-    ap.add_argument("--serve-requests", type=int, default=48,
+    ap.add_argument("--serve-requests", type=int, default=750,
                     help="configuration-4 stream: requests served after the batched measurement (0: skip)")
+    ap.add_argument("--serve-plain", type=int, default=8,
+                    help="configuration-4 stream: its first requests also served one at a time in plain FP64")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the error-against-oracle, configuration-1 and configuration-2 measurements")
     ap.add_argument("--serve-steps", type=int, default=20000, help="MD steps of each served request")
     ap.add_argument("--serve-budget-gb", type=float, default=150.0, help="HBM budget of the serving handle")
     a = ap.parse_args()
@@ -228,6 +232,25 @@ def c3_chain(L: int, seed: int) -> dict:
     np.savez(tmp, **{k: (np.frombuffer(v, dtype=np.uint8) if isinstance(v, bytes) else v) for k, v in c.items()})
     os.replace(tmp, path)
     return c
+
+
+def _gen_chain(args):
+    L, seed = args
+    sys.path.insert(0, ROOT)
+    c3_chain(L, seed)
+    return 0
+
+
+def prefetch_chains(pairs):
+    """Generate the (length, seed) chains missing from the on-disk cache,
+    in parallel over the host cores (spawned processes)."""
+    todo = sorted({(int(L), int(s)) for L, s in pairs
+                   if not os.path.exists(os.path.join(CACHE, f"chain_{int(L)}_{int(s)}.npz"))})
+    if len(todo) < 8:
+        return
+    os.makedirs(CACHE, exist_ok=True)
+    with mp.get_context("spawn").Pool(min(os.cpu_count() or 1, 32)) as pool:
+        pool.map(_gen_chain, todo, chunksize=4)
 
 
 def c3_lengths(n: int):
@@ -393,10 +416,11 @@ def serving_bench(args, dist: Dist, tmp: str) -> dict:
     50/s with chain lengths log-uniform in [30, 1000], each an annealing run
     of --serve-steps steps from 600 K to 300 K, served with continuous
     batching by a handle whose device memory is the --serve-budget-gb budget.
-    Beside it, the plain FP64 form serving the same stream one request at a
-    time: its service times are measured per request length on a sample
-    (device time of 500 steps, scaled to the request's steps) and the FIFO
-    queue is replayed on the same arrival times."""
+    Latencies are reported over the whole stream and over the requests that
+    arrive after its first 10 s (the stream once it is full).  Beside it, the
+    plain FP64 form serving the first --serve-plain requests of the same
+    stream for real, one at a time in arrival order on their arrival times
+    (each request its own handle, created when its turn comes)."""
     from awsemmd_b200 import serve, synth
     from awsemmd_b200.engine import AwsemBatch, AwsemServer
 
@@ -404,7 +428,9 @@ def serving_bench(args, dist: Dist, tmp: str) -> dict:
     n = args.serve_requests
     lens = serve.log_uniform_lengths(n, 30, 1000, rng)
     arrivals = serve.poisson_arrivals(n, 50.0, rng)
-    chains = [c3_chain(int(L), 400000 + 1000 * dist.rank + k) for k, L in enumerate(lens)]
+    seeds = [400000 + 1000 * dist.rank + k for k in range(n)]
+    prefetch_chains(zip(lens, seeds))
+    chains = [c3_chain(int(L), seeds[k]) for k, L in enumerate(lens)]
     ff = synth.forcefield_dir(os.path.join(tmp, "ff4"))
     plan = serve.plan_capacities(ff, args.serve_budget_gb * 1e9, args.precision, device=dist.local)
     t0 = time.perf_counter()
@@ -421,33 +447,156 @@ def serving_bench(args, dist: Dist, tmp: str) -> dict:
         done = serve.run_stream(srv, reqs, chunk=100, keep_state=False)
         usage = srv.usage()
     st = serve.stream_stats(done)
-    # plain FP64, one request at a time: service time per length, FIFO replay
-    probe = sorted({30, 100, 300, 1000, int(np.median(lens))})
-    per_step = []
-    for k, L in enumerate(probe):
-        c = c3_chain(L, 490000 + k)
-        with AwsemBatch.from_arrays(ff, [c], precision="fp64", device=dist.local, seeds=[5]) as one:
-            one.run(50, t_start=600.0, t_stop=300.0)
-            one.run(500, t_start=600.0, t_stop=300.0)
-            per_step.append(one.last_run_ms() / 1e3 / 500)
-    coef = np.polyfit(np.array(probe, dtype=float), np.array(per_step), 1)
-    service = np.polyval(coef, lens.astype(float)) * args.serve_steps
-    lat_plain = serve.fifo_latencies(arrivals, service)
-    work = float(np.sum(lens) * args.serve_steps)
-    makespan_plain = float(np.max(arrivals + lat_plain) - np.min(arrivals))
+    late = [d for d in done if d.arrival >= 10.0]
+    steady = serve.stream_stats(late) if len(late) >= 20 else None
+    # plain FP64, one request at a time, for real, on the first requests' arrival times
+    plain = None
+    m = min(args.serve_plain, n)
+    if m > 0:
+        first = sorted(range(n), key=lambda k: arrivals[k])[:m]
+        lat, free, work = [], 0.0, 0.0
+        clock0 = time.perf_counter()
+        for k in first:
+            wait = arrivals[k] - arrivals[first[0]] - (time.perf_counter() - clock0)
+            if wait > 0:
+                time.sleep(wait)
+            with AwsemBatch.from_arrays(ff, [chains[k]], precision="fp64", device=dist.local,
+                                        seeds=[4000 + 1000 * dist.rank + k]) as one:
+                one.run(args.serve_steps, t_start=600.0, t_stop=300.0)
+            lat.append(time.perf_counter() - clock0 - (arrivals[k] - arrivals[first[0]]))
+            work += float(lens[k]) * args.serve_steps
+        span = time.perf_counter() - clock0
+        mine = {d.rid: d.latency for d in done}
+        served_same = [mine[k] for k in first]
+        plain = {"requests": m, "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+                 "residue_steps_per_s": work / span,
+                 "served_p50_s_same_requests": float(np.percentile(served_same, 50)),
+                 "served_p99_s_same_requests": float(np.percentile(served_same, 99)),
+                 "method": f"the stream's first {m} requests run for real, one at a time in arrival order on their "
+                           f"arrival times: each a plain FP64 single-system handle created when its turn comes, "
+                           f"{args.serve_steps} steps, wall clock"}
     return {"workload": f"config4: {n} requests, Poisson 50/s, lengths log-uniform [30, 1000], "
                         f"{args.serve_steps} Langevin steps each, 600 -> 300 K ramp, dt 2 fs, damping 500 fs, "
                         f"{args.precision} form",
             "p50_s": st["p50_s"], "p99_s": st["p99_s"], "mean_s": st["mean_s"], "makespan_s": st["makespan_s"],
             "residue_steps_per_s": st["residue_steps_per_s"], "residue_steps": st["residue_steps"],
+            "after_first_10s": None if steady is None else {
+                "requests": steady["requests"], "p50_s": steady["p50_s"], "p99_s": steady["p99_s"],
+                "mean_s": steady["mean_s"]},
+            "arrivals_span_s": float(arrivals[-1] - arrivals[0]),
             "budget_gb": args.serve_budget_gb, "device_bytes": usage["device_bytes"],
             "residue_capacity": usage["residue_capacity"], "record_capacity": usage["record_capacity"],
-            "create_s": t_create,
-            "plain_fp64_one_at_a_time": {
-                "p50_s": float(np.percentile(lat_plain, 50)), "p99_s": float(np.percentile(lat_plain, 99)),
-                "residue_steps_per_s": work / makespan_plain,
-                "method": "device time of 500 FP64 steps per probe length " + str(probe) +
-                          ", linear in length, scaled to the request's steps; FIFO replay on the same arrivals"}}
+            "create_s": t_create, "plain_fp64_one_at_a_time": plain}
+
+
+TERM_NAMES = ["total", "chain", "shake", "chi", "rama", "excluded", "dssp", "p_ap", "water", "burial", "helix",
+              "amh_go", "frag_mem", "vec_fm", "contact_restraints", "membrane", "ssb", "dh", "vexcluded", "bonds"]
+
+
+def error_vs_oracle(dev: int, tmp: str) -> dict:
+    """Both arithmetic forms against the FP64 oracle on eight of the
+    workload's replicas (its longest, 500 residues, and seven drawn with a
+    fixed seed), run as one batch: per energy term the largest relative error
+    over the replicas (relative to max(|term|, 0.01 kcal/mol)), the largest
+    force error relative to the replica's largest force, and the selections
+    (awsem_debug_selections) of the longest replica against the oracle's."""
+    import ref
+    from awsemmd_b200 import synth
+    from awsemmd_b200.engine import AwsemBatch, AwsemSystem
+
+    lens = c3_lengths(1024)
+    pick = [int(np.argmax(lens))] + [int(k) for k in np.random.default_rng(31).choice(1024, 7, replace=False)]
+    chains = [c3_chain(lens[k], c3_seed(k)) for k in pick]
+    ff = synth.forcefield_dir(os.path.join(tmp, "ffe"))
+    files = [synth.write_chain_arrays(c, os.path.join(tmp, f"err{r}")) for r, c in enumerate(chains)]
+    oracle = []
+    for r, c in enumerate(chains):
+        o = ref.OracleSystem(files[r])
+        x = c["x"].reshape(-1, 3)
+        oracle.append((x,) + o.compute(x))
+        o.close()
+    out = {"sample": f"replicas {pick} of the workload ({sum(lens[k] for k in pick)} residues), step 0"}
+    for prec in ("fp64", "mixed"):
+        with AwsemBatch.from_arrays(ff, chains, precision=prec, device=dev, seeds=[c3_seed(k) for k in pick]) as b:
+            b.run(0, langevin=False)
+            terms = np.zeros(20)
+            ferr = 0.0
+            for r in range(len(chains)):
+                x, fo, eo = oracle[r]
+                f, e = b.forces(r), b.energies(r)
+                terms = np.maximum(terms, np.abs(e[:20] - eo[:20]) / np.maximum(np.abs(eo[:20]), 1e-2))
+                ferr = max(ferr, float(np.abs(f - fo).max() / np.abs(fo).max()))
+        out[prec] = {"energy_rel": {TERM_NAMES[k]: float(terms[k]) for k in range(20)}, "force_rel": ferr}
+    o = ref.OracleSystem(files[0])
+    x = oracle[0][0]
+    want, near = o.selections(x), o.selections(x, "near")
+    o.close()
+    sel = {}
+    for prec in ("fp64", "mixed"):
+        with AwsemSystem(files[0], precision=prec, device=dev) as s:
+            cmp = ref.compare_selections(s.selections(x), want, near)
+        sel[prec] = {k: v for k, v in cmp.items() if v["want"] or v["got"]}
+    out["selections_longest_replica"] = {
+        "fp64_identical": all(v["cand"] == 0 and v["gate"] == 0 for v in sel["fp64"].values()),
+        "mixed": sel["mixed"], "near_threshold_in_oracle": int(len(near)),
+        "note": "cand: items one side selects and the other does not (gated kinds without their gate bits); "
+                "cand_far: of those, not within 2e-6 of a threshold; gate: items both select with other gate bits"}
+    return out
+
+
+def config1_extra(dev: int, tmp: str, run_kw: dict, l2buf) -> dict:
+    """Configuration 1 (8 x 250 residues): the plain FP64 form (and the mixed
+    form) on the GPU against the reference on one host core."""
+    from awsemmd_b200 import synth
+    from awsemmd_b200.engine import AwsemSystem
+
+    files = synth.write_system(synth.config_system(1), os.path.join(tmp, "c1x"))
+    out = {"workload": WORKLOADS["c1"]}
+    for prec in ("fp64", "mixed"):
+        with AwsemSystem(files, precision=prec, device=dev) as s:
+            s.run(100, **run_kw)
+            ms = []
+            for _ in range(3):
+                flush_l2(l2buf)
+                s.run(100, **run_kw)
+                ms.append(s.last_run_ms())
+        t = sum(ms) / 1e3
+        out[prec] = {"steps_per_s": 300 / t, "residue_steps_per_s": 2000 * 300 / t}
+    v, busy = reference_c1(5, 1, 2)
+    out["reference_1_core"] = {"residue_steps_per_s": v, "sample": f"2 x 5 MD steps ({busy:.1f} s), 1 rank"}
+    out["fp64_over_reference"] = out["fp64"]["residue_steps_per_s"] / v
+    return out
+
+
+def config2_extra(dev: int, tmp: str, run_kw: dict, l2buf, peak: float) -> dict:
+    """Configuration 2 (40,000 residues, one system, mixed form): steps/s,
+    residue-steps/s and per-kernel achieved HBM GB/s against the peak."""
+    from awsemmd_b200 import synth
+    from awsemmd_b200.engine import AwsemBatch
+
+    ff = synth.forcefield_dir(os.path.join(tmp, "ff2x"))
+    c2 = synth.packed_arrays([250] * 160, 320.0, 2000)
+    kw = dict(run_kw, skin=2.0, neigh_every=10)
+    with AwsemBatch.from_arrays(ff, [c2], precision="mixed", device=dev, seeds=[2000]) as s:
+        shapes = s.autotune(2)
+        s.run(50, **kw)
+        ms = []
+        for _ in range(3):
+            flush_l2(l2buf)
+            s.run(50, **kw)
+            ms.append(s.last_run_ms())
+        prof = s.profile_step(10)
+        info = s.model_info()
+    t = sum(ms) / 1e3
+    per_kernel = {}
+    for k in ("fragmem", "pair", "density", "water_xi", "prepare", "finish"):
+        if prof.get(k, 0) > 0:
+            b = algorithmic_bytes(k, info)
+            per_kernel[k] = {"ms": round(prof[k], 5), "achieved_gbs": round(b / (prof[k] * 1e-3) / 1e9, 1),
+                             "frac": round(b / (prof[k] * 1e-3) / 1e9 / peak, 4)}
+    return {"workload": WORKLOADS["c2"], "steps_per_s": 150 / t, "residue_steps_per_s": 40000 * 150 / t,
+            "kernel_ms": {k: round(v, 5) for k, v in prof.items()}, "per_kernel": per_kernel,
+            "launch_shapes": shapes, "peak_gbs": peak}
 
 
 def reference_arm(args, dist: Dist):
@@ -502,6 +651,7 @@ def build_c3(n: int, rank: int, precision: str, dev: int, tmp: str):
     from awsemmd_b200.engine import AwsemBatch
 
     lens = c3_lengths(n)
+    prefetch_chains((L, c3_seed(k, rank)) for k, L in enumerate(lens))
     chains = (c3_chain(L, c3_seed(k, rank)) for k, L in enumerate(lens))
     ff = synth.forcefield_dir(os.path.join(tmp, "ff"))
     seeds = [c3_seed(k, rank) for k in range(n)]
@@ -695,6 +845,15 @@ def main():
             base = {"value": None, "unit": "residue-steps/s", "cores": 1, "kind": "reference",
                     "sample": f"not measured: {e}"}
     eng.close()
+    extras = {}
+    if args.workload == "c3" and dist.world == 1 and not args.no_extras:
+        for key, fn in (("error_vs_oracle", lambda: error_vs_oracle(dev, tmp)),
+                        ("config1", lambda: config1_extra(dev, tmp, run_kw, l2buf)),
+                        ("config2", lambda: config2_extra(dev, tmp, run_kw, l2buf, peak))):
+            try:
+                extras[key] = fn()
+            except Exception as e:  # reported, never replaced by something else
+                extras[key] = {"not_measured": f"{type(e).__name__}: {e}"}
     served = None
     if args.workload == "c3" and args.serve_requests > 0:
         del l2buf
@@ -717,7 +876,7 @@ def main():
                         "h2d_bytes_per_step": 2 * natoms * 3 * 8, "d2h_bytes_per_step": 2 * natoms * 3 * 8,
                         "path": "awsem_batch_set_state (pinned host x, v of every replica) + awsem_run + "
                                 "awsem_batch_get_state, per bench step; wall clock"},
-                "plain_fp64": plain, "clocks": clk, "gpu_launches": launches, "served": served}
+                "plain_fp64": plain, "clocks": clk, "gpu_launches": launches, "served": served, **extras}
         print(json.dumps(line))
     dist.close()
 

@@ -267,11 +267,12 @@ int awsem_debug_selections(awsem_system *sys, long long step, const double *x, u
  * form waiting at a grid barrier).  A wait that runs out gives up, the kernel
  * ends normally (a fragment-memory warp first lets its copies in flight land,
  * waiting a fixed quarter second at most) and the call returns AWSEM_ESTATE
- * ("results of this call are invalid"); the next call runs clean.  hold != 0,
- * for tests of those paths only, makes the waits' conditions unreachable
- * (each copy stage expects 16 bytes that never arrive; each grid barrier one
- * block more than the grid), so every wait runs out; hold 0 restores normal
- * waits.  No counterpart in the reference (LAMMPS has no device waits). */
+ * ("results of this call are invalid"); the next call runs clean.  hold, for
+ * tests of those paths only, makes the waits' conditions unreachable so that
+ * every wait runs out: bit 0 the copy waits (each stage expects 16 bytes that
+ * never arrive), bit 1 the grid barriers (each waits for one block more than
+ * the grid); hold 0 restores normal waits.  No counterpart in the reference
+ * (LAMMPS has no device waits). */
 int awsem_set_wait_limits(awsem_system *sys, long long fm_copy_wait_cycles, long long grid_barrier_wait_cycles,
                           int hold);
 

@@ -1,7 +1,7 @@
 """Failure paths, each made to happen without a GPU fault, trap or hang.
 
 * A bounded device wait that runs out: awsem_set_wait_limits(hold) makes the
-  waits' conditions unreachable (a fragment-memory copy stage expects bytes
+  conditions of one kind of wait unreachable (a fragment-memory copy stage expects bytes
   that never arrive; a grid barrier of the persistent step form one block
   more than the grid), so every wait gives up after its limit, the kernels
   end normally and the call reports AWSEM_ESTATE.
@@ -34,7 +34,7 @@ def test_fragment_memory_wait_runs_out_then_next_call_is_clean(prec, tmp_path, g
     with AwsemSystem(files, precision=prec) as s:
         x, _ = s.get_state()
         f0, e0 = s.compute(x)
-        s.set_wait_limits(fm_cycles=SHORT, hold=True)
+        s.set_wait_limits(fm_cycles=SHORT, hold=1)
         with pytest.raises(AwsemError, match="fragment-memory stream"):
             s.compute(x)
         s.set_wait_limits()
@@ -55,7 +55,7 @@ def test_grid_barrier_wait_runs_out_then_next_call_is_clean(tmp_path, gpu_lib):
         x_ref, v_ref = ref.get_state()
     with AwsemSystem(files, precision="mixed") as s:
         s.set_step_form("persistent")
-        s.set_wait_limits(barrier_cycles=SHORT, hold=True)
+        s.set_wait_limits(barrier_cycles=SHORT, hold=2)
         with pytest.raises(AwsemError, match="grid barrier"):
             s.run(3, **kw)
         s.set_wait_limits()
