@@ -182,7 +182,27 @@ __device__ __forceinline__ void well_theta(R r, R rmin_th, R rmax_th, R kappa, R
   theta = R(0.25) * (R(1) + t_min) * (R(1) + t_max);
   prd = kappa * theta * (t_max - t_min) / r;
 }
-// FP32 with every operation spelled out (no contraction left to the compiler)
+// FP32 (mixed form) from two exponentials instead of two tanh.  With
+// e_a = exp(-2 kappa (r - rmin)) and e_b = exp(-2 kappa (rmax - r)), the
+// identity 1 + tanh(x) = 2 / (1 + exp(-2x)) gives
+//   theta = 1 / ((1 + e_a)(1 + e_b)),
+//   tanh(kappa (rmax - r)) - tanh(kappa (r - rmin)) = 2 (e_a - e_b) theta,
+//   prd = kappa theta (t_max - t_min) / r = 2 kappa theta^2 (e_a - e_b) / r.
+// Inside the support (|kappa (r - edge)| <= 8 ln 10) the exponentials stay
+// below 1e17.  Hardware 2^x and reciprocal (relative error ~1e-7); every
+// operation spelled out, no contraction left to the compiler.
+__device__ __forceinline__ float fast_exp2(float x)
+{
+  float y;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float fast_rcp(float x)
+{
+  float y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
 template <>
 __device__ __forceinline__ void well_theta(float r, float rmin_th, float rmax_th, float kappa, float rmin, float rmax,
                                            float &theta, float &prd)
@@ -191,10 +211,12 @@ __device__ __forceinline__ void well_theta(float r, float rmin_th, float rmax_th
     theta = prd = 0.f;
     return;
   }
-  const float t_min = tanhf(__fmul_rn(kappa, __fsub_rn(r, rmin)));
-  const float t_max = tanhf(__fmul_rn(kappa, __fsub_rn(rmax, r)));
-  theta = __fmul_rn(__fmul_rn(0.25f, __fadd_rn(1.f, t_min)), __fadd_rn(1.f, t_max));
-  prd = __fdiv_rn(__fmul_rn(__fmul_rn(kappa, theta), __fsub_rn(t_max, t_min)), r);
+  const float c = __fmul_rn(-2.8853900817779268f, kappa);  // -2 kappa log2(e)
+  const float ea = fast_exp2(__fmul_rn(c, __fsub_rn(r, rmin)));
+  const float eb = fast_exp2(__fmul_rn(c, __fsub_rn(rmax, r)));
+  theta = fast_rcp(__fmul_rn(__fadd_rn(1.f, ea), __fadd_rn(1.f, eb)));
+  prd = __fmul_rn(__fmul_rn(__fmul_rn(__fmul_rn(2.f, kappa), __fmul_rn(theta, theta)), __fsub_rn(ea, eb)),
+                  fast_rcp(r));
 }
 
 // compute_chain_potential(i), fix_backbone.cpp:2062-2170

@@ -79,16 +79,64 @@ __device__ __forceinline__ double fm_k2(double s2) { return -1.0 / (2.0 * s2); }
 // coefficients are not uniform): es += sum g_k, fs_k += g_k dr_k.  The row's
 // energy and radial force sums are scale * es and scale * fs_k, with scale =
 // -coefficient (uniform) or -1.
+// FP32 operand pairs for Blackwell's paired FP32 instructions (f32x2): each
+// element is rounded as the scalar operation rounds it.
+__device__ __forceinline__ unsigned long long f2_pack(float a, float b)
+{
+  unsigned long long d;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(d) : "f"(a), "f"(b));
+  return d;
+}
+__device__ __forceinline__ void f2_unpack(unsigned long long d, float &a, float &b)
+{
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(d));
+}
+__device__ __forceinline__ unsigned long long f2_sub(unsigned long long a, unsigned long long b)
+{
+  unsigned long long d;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ unsigned long long f2_mul(unsigned long long a, unsigned long long b)
+{
+  unsigned long long d;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ unsigned long long f2_fma(unsigned long long a, unsigned long long b, unsigned long long c)
+{
+  unsigned long long d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+  return d;
+}
+
 template <bool COEF, typename R>
 __device__ __forceinline__ void fm_record(const R rec[4], R cc, const R r[4], R k2, R &es, R fs[4])
 {
+  if constexpr (sizeof(R) == 4) {
+    // atom pairs (0, 1) and (2, 3) as f32x2 pairs: the same operations in
+    // the same order as the scalar loop below, half the instructions
+    const unsigned long long k22 = f2_pack(k2, k2);
 #pragma unroll
-  for (int k = 0; k < 4; k++) {
-    const R dr = r[k] - rec[k];
-    R g = fm_gauss(dr * dr * k2);
-    if (COEF) g = g * cc;
-    es = es + g;
-    fs[k] = madd(g, dr, fs[k]);
+    for (int h = 0; h < 4; h += 2) {
+      const unsigned long long dr = f2_sub(f2_pack(r[h], r[h + 1]), f2_pack(rec[h], rec[h + 1]));
+      float x0, x1;
+      f2_unpack(f2_mul(f2_mul(dr, dr), k22), x0, x1);
+      float g0 = fm_gauss(x0), g1 = fm_gauss(x1);
+      if (COEF) f2_unpack(f2_mul(f2_pack(g0, g1), f2_pack(cc, cc)), g0, g1);
+      es = es + g0;
+      es = es + g1;
+      f2_unpack(f2_fma(f2_pack(g0, g1), dr, f2_pack(fs[h], fs[h + 1])), fs[h], fs[h + 1]);
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const R dr = r[k] - rec[k];
+      R g = fm_gauss(dr * dr * k2);
+      if (COEF) g = g * cc;
+      es = es + g;
+      fs[k] = madd(g, dr, fs[k]);
+    }
   }
 }
 

@@ -786,7 +786,7 @@ template <typename R, bool SEL> __device__ __forceinline__ void residue_pass_win
     __syncthreads();
   }
 }
-template <typename R> __global__ void __launch_bounds__(kResBlock) k_residue(StepArgs<R> a, FFParams p)
+template <typename R> __global__ void __launch_bounds__(kResBlock, 4) k_residue(StepArgs<R> a, FFParams p)
 {
   residue_pass_window<R, false>(a, p);
 }
@@ -953,14 +953,22 @@ template <typename R, bool SEL = false> __device__ __forceinline__ void pair_pas
     if (q < np) {
     const int2 ij = a.pairs[q];
     const int i = ij.x, j = ij.y;
+    // every per-residue input of the pair, loaded up front and without
+    // conditions, so that the gathers are in flight together
     const int fli = s.res_flags[i], flj = s.res_flags[j];
     const bool other = s.res_chain[j] != s.res_chain[i];
-    const int dij = j - i;
+    const int ti = s.res_type[i], tj = s.res_type[j];
     const V3<double> ca_i = bead(s, i, B_CA), ca_j = bead(s, j, B_CA);
+    const V3<double> cb_i = bead(s, i, B_CB), cb_j = bead(s, j, B_CB);
+    const double sw_i = a.sig_w[i], sw_j = a.sig_w[j], bur_i = a.bur[i], bur_j = a.bur[j];
+    const double xi_i = water_xi(a, i), xi_j = water_xi(a, j);
+    const double x1_i = a.xi1[i], x1_j = a.xi1[j];
+    const double x2_i = a.xi2[max(i - dh, 0)], x2_j = a.xi2[max(j - dh, 0)];
+    const int dij = j - i;
     // contact-bead radial terms
     if (fix && (other || dij > 1)) {
       const bool gi = fli & R_GLY, gj = flj & R_GLY;
-      const V3<R> d = diff<R>(gi ? ca_i : bead(s, i, B_CB), gj ? ca_j : bead(s, j, B_CB));
+      const V3<R> d = diff<R>(gi ? ca_i : cb_i, gj ? ca_j : cb_j);
       const R rsq = norm2(d);
       const R r = m_sqrt(rsq);
       R force = 0;
@@ -971,7 +979,6 @@ template <typename R, bool SEL = false> __device__ __forceinline__ void pair_pas
         well_theta(r, R(p.w_rmin_th[0]), R(p.w_rmax_th[0]), R(p.water_kappa), R(p.well_rmin[0]), R(p.well_rmax[0]),
                    th0, pr0);
       if (T & T_WATER) {
-        const int ti = s.res_type[i], tj = s.res_type[j];
         const bool sep = other || dij >= p.contact_cutoff;
         const double *W = ((fli | flj) & R_PHOSPH) ? s.tables + TB_WATER_PHOSPH : WG;
         for (int w = 0; w < p.n_wells; w++) {
@@ -979,7 +986,7 @@ template <typename R, bool SEL = false> __device__ __forceinline__ void pair_pas
           if (sep && rsq > R(p.w_rmin_sq[w]) && rsq < R(p.w_rmax_sq[w])) {
             sel_rec<SEL>(a, AWSEM_SEL_WATER, w, i, j);
             const double g0 = W[w * 800 + (ti * 20 + tj) * 2], g1 = W[w * 800 + (ti * 20 + tj) * 2 + 1];
-            const double sg = fabs(g0 - g1) < 1e-5 ? 0.5 * (g0 + g1) : g0 + (g1 - g0) * a.sig_w[i] * a.sig_w[j];
+            const double sg = fabs(g0 - g1) < 1e-5 ? 0.5 * (g0 + g1) : g0 + (g1 - g0) * sw_i * sw_j;
             R th, pr;
             if (w == 0) {
               th = th0;
@@ -993,18 +1000,17 @@ template <typename R, bool SEL = false> __device__ __forceinline__ void pair_pas
           }
         }
         if (in0) {
-          const double xi_i = water_xi(a, i), xi_j = water_xi(a, j);
           const int on = (fabs(xi_i) > 1e-8 ? 1 : 0) | (fabs(xi_j) > 1e-8 ? 2 : 0);
           if (on & 1) force = madd(pr0, R(xi_i), force);
           if (on & 2) force = madd(pr0, R(xi_j), force);
           if (on) sel_rec<SEL>(a, AWSEM_SEL_XI_FORCE, on, i, j);
         }
       }
-      if ((T & T_BURIAL) && in0) force = madd(R(a.bur[i] + a.bur[j]), pr0, force);
+      if ((T & T_BURIAL) && in0) force = madd(R(bur_i + bur_j), pr0, force);
       if ((T & T_HELIX) && rsq > R(p.h_rmin_sq) && rsq < R(p.h_rmax_sq)) {
-        double fac = a.xi1[i] + a.xi1[j];
-        if (i - dh >= 0) fac += a.xi2[i - dh];
-        if (j - dh >= 0) fac += a.xi2[j - dh];
+        double fac = x1_i + x1_j;
+        if (i - dh >= 0) fac += x2_i;
+        if (j - dh >= 0) fac += x2_j;
         if (fabs(fac) > 1e-6) {
           sel_rec<SEL>(a, AWSEM_SEL_HELIX_FORCE, 0, i, j);
           R th, pr;
@@ -1056,7 +1062,10 @@ template <typename R, bool SEL = false> __device__ __forceinline__ void pair_pas
   if (nse > 0) ev_batch(nse);
 }
 
-template <typename R> __global__ void __launch_bounds__(128, 6) k_pair(StepArgs<R> a, FFParams p)
+// blocks per SM the pair pass is compiled for: its up-front gathers need the
+// registers of 5 blocks in FP32; the FP64 form holds twice the data
+template <typename R> constexpr int kPairMinBlocks = sizeof(R) == 4 ? 5 : 4;
+template <typename R> __global__ void __launch_bounds__(128, kPairMinBlocks<R>) k_pair(StepArgs<R> a, FFParams p)
 {
   pair_pass(a, p, grid_span());
 }
