@@ -554,12 +554,21 @@ template <typename R> __device__ R dssp_term(const DevSys<R> &s, const FFParams 
   ff1 *= nu[0] * nu[1];
   for (int k = 0; k < 4; k++) V[k] *= ff1;
   R VT = V[0] + V[1] + V[2] + V[3];
+  // Beads that several contributions reach are summed here first, in this
+  // fixed order, and scattered once: O(i) (acceptor of k = 0, 1), O(j)
+  // (O(d - 1) of k = 1, acceptor of k = 2, 3), CA(j) (CA(d) of k = 0,
+  // CA(d - 1) of k = 1) and CA(i + 2) (CA(d) of k = 3, the nu switch of i).
+  V3<R> fOi = {R(0), R(0), R(0)}, fOj = fOi, fCAj = fOi, fCAi2 = fOi;
+  auto add = [](V3<R> &t, R x, R y, R z) { t = {t.x + x, t.y + y, t.z + z}; };
   for (int q = 0; q < 2; q++) {
     if (!use_nu[q]) continue;
     R g = q == 0 ? theta_sum * prdnu[0] * nu[1] : theta_sum * nu[0] * prdnu[1];
     int c = cen[q];
     scatter(s, c - 2, B_CA, g * dxnu[q].x, g * dxnu[q].y, g * dxnu[q].z);
-    scatter(s, c + 2, B_CA, -g * dxnu[q].x, -g * dxnu[q].y, -g * dxnu[q].z);
+    if (q == 0)
+      add(fCAi2, -g * dxnu[q].x, -g * dxnu[q].y, -g * dxnu[q].z);
+    else
+      scatter(s, c + 2, B_CA, -g * dxnu[q].x, -g * dxnu[q].y, -g * dxnu[q].z);
   }
   const R an = p.an, bn = p.bn, cn = p.cn, ah = p.ah, bh = p.bh, ch = p.ch;
   for (int k = 0; k < 4; k++) {
@@ -568,11 +577,30 @@ template <typename R> __device__ R dssp_term(const DevSys<R> &s, const FFParams 
     R q0 = prd[k][0] * sc, q1 = prd[k][1] * sc;
     V3<R> a = xNO[k], h = xHO[k];
     int d = don[k];
-    scatter(s, acc[k], B_O, -(q0 * a.x + q1 * h.x), -(q0 * a.y + q1 * h.y), -(q0 * a.z + q1 * h.z));
-    scatter(s, d - 1, B_CA, an * q0 * a.x + ah * q1 * h.x, an * q0 * a.y + ah * q1 * h.y, an * q0 * a.z + ah * q1 * h.z);
-    scatter(s, d, B_CA, bn * q0 * a.x + bh * q1 * h.x, bn * q0 * a.y + bh * q1 * h.y, bn * q0 * a.z + bh * q1 * h.z);
-    scatter(s, d - 1, B_O, cn * q0 * a.x + ch * q1 * h.x, cn * q0 * a.y + ch * q1 * h.y, cn * q0 * a.z + ch * q1 * h.z);
+    const R ox = -(q0 * a.x + q1 * h.x), oy = -(q0 * a.y + q1 * h.y), oz = -(q0 * a.z + q1 * h.z);
+    const R px = an * q0 * a.x + ah * q1 * h.x, py = an * q0 * a.y + ah * q1 * h.y, pz = an * q0 * a.z + ah * q1 * h.z;
+    const R cx = bn * q0 * a.x + bh * q1 * h.x, cy = bn * q0 * a.y + bh * q1 * h.y, cz = bn * q0 * a.z + bh * q1 * h.z;
+    const R wx = cn * q0 * a.x + ch * q1 * h.x, wy = cn * q0 * a.y + ch * q1 * h.y, wz = cn * q0 * a.z + ch * q1 * h.z;
+    add(k < 2 ? fOi : fOj, ox, oy, oz);  // O of the acceptor (i for k < 2, j otherwise)
+    if (k == 1)
+      add(fCAj, px, py, pz);  // CA(d - 1) = CA(j)
+    else
+      scatter(s, d - 1, B_CA, px, py, pz);
+    if (k == 0)
+      add(fCAj, cx, cy, cz);  // CA(d) = CA(j)
+    else if (k == 3)
+      add(fCAi2, cx, cy, cz);  // CA(d) = CA(i + 2)
+    else
+      scatter(s, d, B_CA, cx, cy, cz);
+    if (k == 1)
+      add(fOj, wx, wy, wz);  // O(d - 1) = O(j)
+    else
+      scatter(s, d - 1, B_O, wx, wy, wz);
   }
+  scatter(s, i, B_O, fOi);
+  scatter(s, j, B_O, fOj);
+  scatter(s, j, B_CA, fCAj);
+  if (use_nu[0] || on[3]) scatter(s, i + 2, B_CA, fCAi2);
   return VT;
 }
 

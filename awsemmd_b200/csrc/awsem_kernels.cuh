@@ -1527,11 +1527,19 @@ __device__ __forceinline__ uint64_t mix64(uint64_t z)
 
 // Uniform in [0,1) keyed by (seed, step, atom id, component): the Langevin
 // noise stream shared with the CPU oracle.
-__device__ __forceinline__ double uniform01(uint64_t seed, long long step, long long tag, int comp)
+// the stream's key for (seed, step), and the uniform of (key, atom id, component)
+__device__ __forceinline__ uint64_t uniform_key(uint64_t seed, long long step)
 {
-  uint64_t key = mix64(seed ^ mix64((uint64_t) step));
+  return mix64(seed ^ mix64((uint64_t) step));
+}
+__device__ __forceinline__ double uniform01_k(uint64_t key, long long tag, int comp)
+{
   uint64_t r = mix64(key ^ ((uint64_t) tag * 4ULL + (uint64_t) comp));
   return (double) (r >> 11) * (1.0 / 9007199254740992.0);
+}
+__device__ __forceinline__ double uniform01(uint64_t seed, long long step, long long tag, int comp)
+{
+  return uniform01_k(uniform_key(seed, step), tag, comp);
 }
 
 struct Integrator {
@@ -1564,6 +1572,7 @@ __device__ __forceinline__ void finish_one(const StepArgs<R> &a, const Integrato
   // the x86-64 CPU build computes fix langevin / fix nve, and identically in
   // every kernel that inlines this.
   double tsqrt = 0.0;
+  const uint64_t nkey = in.langevin ? uniform_key(seed, key) : 0ull;  // once per residue, not per draw
   if (in.langevin) {
     double delta = sr.end != sr.begin ? (double) (step - sr.begin) / (double) (sr.end - sr.begin) : 0.0;
     tsqrt = sqrt(__dadd_rn(sr.t_start, __dmul_rn(delta, __dsub_rn(sr.t_stop, sr.t_start))));
@@ -1580,7 +1589,7 @@ __device__ __forceinline__ void finish_one(const StepArgs<R> &a, const Integrato
       if (in.langevin)
         f = __dadd_rn(f, __dadd_rn(__dmul_rn(g1[at], v),
                                    __dmul_rn(__dmul_rn(g2[at], tsqrt),
-                                             __dsub_rn(uniform01(seed, key, a.atom_tag[at], c), 0.5))));
+                                             __dsub_rn(uniform01_k(nkey, a.atom_tag[at], c), 0.5))));
       if (ftot) ftot[3 * at + c] = f;
       if (final_kick) v = __dadd_rn(v, __dmul_rn(dtfm, f));
       ke = __dadd_rn(ke, __dmul_rn(__dmul_rn(m, v), v));
