@@ -1138,18 +1138,26 @@ template <typename R> class Engine : public EngineBase {
     };
     tune_blocks(pair_blocks, {3, 5, 6});
     tune_blocks(hb_blocks, {7});
-    // fragment-memory grid: judged on whole steps (it overlaps the pair passes)
+    // fragment-memory grid with the pair-pass grid, judged together on whole
+    // steps: fragment memory (HBM-bound, second stream) can only overlap the
+    // latency-bound pair passes when their grids leave it room on the SMs
     if (in.ff.p.fm_nd > 0) {
-      int best = 0;
+      int best = 0, best_pb = pair_blocks;
       double tbest = 1e30;
-      for (int f : {0, 1, 2, 3, 4}) {
-        fm_grid = f * sms;
-        release_graphs();
-        run(reps, last_rp, nullptr);  // warm-up of this shape (graph capture)
-        run(4 * reps, last_rp, nullptr);
-        if (last_run_ms < tbest) tbest = last_run_ms, best = fm_grid;
+      const int tuned_pb = pair_blocks;
+      for (int pb : {tuned_pb, 2 * sms, 4 * sms, 8 * sms}) {
+        if (pb != tuned_pb && pb == best_pb) continue;
+        for (int f : {0, 1, 2, 3, 4}) {
+          pair_blocks = pb;
+          fm_grid = f * sms;
+          release_graphs();
+          run(reps, last_rp, nullptr);  // warm-up of this shape (graph capture)
+          run(4 * reps, last_rp, nullptr);
+          if (last_run_ms < tbest) tbest = last_run_ms, best = fm_grid, best_pb = pb;
+        }
       }
       fm_grid = best;
+      pair_blocks = best_pb;
     }
     // step form: the chain of per-pass kernels against the persistent step
     // kernel over its grid size and stream-warp count, on whole steps
