@@ -246,9 +246,17 @@ def prefetch_chains(pairs):
     in parallel over the host cores (spawned processes)."""
     todo = sorted({(int(L), int(s)) for L, s in pairs
                    if not os.path.exists(os.path.join(CACHE, f"chain_{int(L)}_{int(s)}.npz"))})
-    if len(todo) < 8:
+    if not todo:
         return
     os.makedirs(CACHE, exist_ok=True)
+    # spawned workers re-import the main module: only bench.py itself (whose
+    # work sits behind its __main__ guard) may start them; other callers
+    # generate in this process
+    main = getattr(sys.modules.get("__main__"), "__file__", None)
+    if len(todo) < 8 or not main or os.path.abspath(main) != os.path.abspath(__file__):
+        for L, seed in todo:
+            c3_chain(L, seed)
+        return
     with mp.get_context("spawn").Pool(min(os.cpu_count() or 1, 32)) as pool:
         pool.map(_gen_chain, todo, chunksize=4)
 
