@@ -863,7 +863,7 @@ def main():
             except Exception as e:  # reported, never replaced by something else
                 extras[key] = {"not_measured": f"{type(e).__name__}: {e}"}
     served = None
-    if args.workload == "c3" and args.serve_requests > 0:
+    if args.workload == "c3" and args.serve_requests > 0 and dist.world == 1:
         del l2buf
         torch.cuda.empty_cache()  # the serving handle takes the memory budget
         served = serving_bench(args, dist, tmp)
