@@ -152,7 +152,7 @@ template <typename R> class Engine : public EngineBase {
   DBuf<double> aps, tables, x, v, mass, g1, g2, ftot, work, e_res, energy;
   DBuf<double4> pos, cb_build;
   DBuf<unsigned long long> facc;
-  DBuf<int2> pairs;
+  DBuf<int2> pairs, cpairs;  // residue pair list; the near list of an evaluation
   DBuf<int> ncount, hbq;
   DBuf<long long> dacc;
   int pair_blocks = 1;
@@ -248,6 +248,7 @@ template <typename R> class Engine : public EngineBase {
     a.bur = w + 9 * nn;
     a.e_res = e_res.p;
     a.pairs = pairs.p;
+    a.cpairs = cpairs.p;
     a.dacc = dacc.p;
     a.hbq = hbq.p;
     a.e_fix = e_fix.p;
@@ -548,6 +549,7 @@ template <typename R> class Engine : public EngineBase {
     if (newcap >= (1ll << 31)) throw std::invalid_argument("residue pair list exceeds 2^31 pairs");
     pcap = (int) newcap;
     pairs.alloc((size_t) pcap);
+    cpairs.alloc((size_t) pcap);
     hbq.alloc((size_t) 3 * pcap);
     dev::NLState st;
     CK(cudaMemcpyAsync(&st, nl.p, sizeof st, cudaMemcpyDeviceToHost, s0));

@@ -63,6 +63,8 @@ struct NLState {
                       // CA-pair terms need covered by the residue pair list (0: none)
   float lst_d2max;    // max CA displacement^2 since the last emulated build (this step)
   int bad_x;          // a position was not finite (results invalid; the host reports and clears it)
+  float need;         // R_need of this step: no term reaches a pair whose contact beads are farther apart
+  int ncpairs;        // pairs of the near list (contact beads within `need`), written by the density pass
 };
 
 // Run window of one replica: integrated over steps begin..end (the
@@ -84,8 +86,11 @@ template <typename R> struct StepArgs {
   // per-residue pair-pass intermediates
   double *rho_w, *rho_h, *sig_w, *sigp_w, *sig_h, *sigp_h, *xi_w, *xi1, *xi2, *bur;
   double *e_res;  // [E_SLOTS][n_res]
-  // residue pair list: pairs (i, j), i < j, capacity pcap; per-residue counts
-  int2 *pairs;
+  // residue pair list: pairs (i, j), i < j, capacity pcap; per-residue counts.
+  // cpairs: the near list of this evaluation (the listed pairs whose contact
+  // beads are within NLState::need), written by the density pass and walked
+  // by the water-xi, pair and hydrogen-bond passes (capacity pcap)
+  int2 *pairs, *cpairs;
   int *ncount, pcap;
   double4 *cb_build;
   NLState *nl;
@@ -313,6 +318,8 @@ __device__ __forceinline__ void nl_decide(NLState *nl, int force, long long *ste
     s.steps_since++;
   }
   s.rebuild = rb;
+  s.need = need;
+  s.ncpairs = 0;
   // two residues whose CAs are farther apart than r_ev + 2 * reach have no
   // bead pair inside any excluded-volume cutoff (0.01 A covers rounding)
   float pre = s.r_ev + 2.f * s.bCAx + 0.01f;
@@ -569,6 +576,9 @@ template <typename R> __global__ void k_nl_build(StepArgs<R> a, GridArgs g, int 
 // Pairs of the list, grid-stride (the count is known only on the device)
 #define FOR_EACH_PAIR(a, p, sp) \
   for (int p = (sp).t, np_ = min((a).nl->npairs, (a).pcap); p < np_; p += (sp).nthr)
+// Pairs of the near list (written by the density pass of this evaluation)
+#define FOR_EACH_NEAR_PAIR(a, p, sp) \
+  for (int p = (sp).t, np_ = min((a).nl->ncpairs, (a).pcap); p < np_; p += (sp).nthr)
 
 // DL1: local densities of contact beads (fix_backbone.cpp:7728-7791).  The
 // well windows are tested on the FP64 r^2 in both forms, so the selection is
@@ -579,17 +589,28 @@ template <typename R, bool SEL = false> __device__ __forceinline__ void density_
 {
   const DevSys<R> &s = a.s;
   const int n = s.n_res;
-  if (!(a.groups & G_FIX)) return;
-  const bool water = p.terms & T_WATER, helix = p.terms & T_HELIX;
+  const bool fix = a.groups & G_FIX;
+  const bool water = fix && (p.terms & T_WATER), helix = fix && (p.terms & T_HELIX);
   unsigned long long *aw = (unsigned long long *) a.dacc, *ah = aw + n;
+  // the near list: the listed pairs some term can reach at this step (the
+  // bound the list's validity check uses; the margin covers its rounding)
+  const double need_sq = (double) a.nl->need * (double) a.nl->need * 1.00001;
+  const int lane = threadIdx.x & 31;
   FOR_EACH_PAIR(a, q, sp)
   {
     const int2 ij = a.pairs[q];
     const int i = ij.x, j = ij.y;
+    const double rsq = norm2(diff<double>(contact(s, i), contact(s, j)));
+    const bool near = rsq < need_sq;
+    const unsigned act = __activemask(), m = __ballot_sync(act, near);
+    const int leader = __ffs(act) - 1;
+    int at = 0;
+    if (lane == leader && m) at = atomicAdd(&a.nl->ncpairs, __popc(m));
+    at = __shfl_sync(act, at, leader) + __popc(m & ((1u << lane) - 1u));
+    if (near && at < a.pcap) a.cpairs[at] = ij;
     if (s.res_chain[j] == s.res_chain[i] && j - i <= 1) continue;
     // the window tests on the FP64 r^2 in both forms (the reference's
     // selections); the well value in the form's geometry type
-    const double rsq = norm2(diff<double>(contact(s, i), contact(s, j)));
     const R r = R(sqrt(rsq));
     if (water && rsq > p.w_rmin_sq[0] && rsq < p.w_rmax_sq[0]) {
       R th, pr;
@@ -809,9 +830,9 @@ template <typename R, bool SEL = false> __device__ __forceinline__ void water_xi
   if (!(p.terms & T_WATER) || !(a.groups & G_FIX)) return;
   unsigned long long *acc = (unsigned long long *) a.dacc + (size_t) 2 * s.n_res;
   const double *WG = s.tables + TB_WATER;
-  FOR_EACH_PAIR(a, q, sp)
+  FOR_EACH_NEAR_PAIR(a, q, sp)
   {
-    const int2 ij = a.pairs[q];
+    const int2 ij = a.cpairs[q];
     const int i = ij.x, j = ij.y;
     if (s.res_chain[j] == s.res_chain[i] && j - i < p.contact_cutoff) continue;
     const R rsq = norm2(diff<R>(contact(s, i), contact(s, j)));
@@ -877,7 +898,7 @@ template <typename R, bool SEL = false> __device__ __forceinline__ void pair_pas
   const size_t qd = 0, qp = (size_t) 2 * a.pcap;  // queue regions: DSSP (both orientations), P_AP
   unsigned long long *e_water = (unsigned long long *) a.e_fix + (size_t) 3 * n;
   unsigned long long *e_ev = (unsigned long long *) a.e_fix + (size_t) 4 * n;
-  const int lane = threadIdx.x & 31, np = min(a.nl->npairs, a.pcap);
+  const int lane = threadIdx.x & 31, np = min(a.nl->ncpairs, a.pcap);
   // Queue entries are staged per warp in shared memory and written out 32 at
   // a time with one atomic reservation: one counter update per 32 entries
   // instead of one per warp iteration (same-address atomics serialise in L2).
@@ -901,7 +922,7 @@ template <typename R, bool SEL = false> __device__ __forceinline__ void pair_pas
   };
   // excluded volume between the beads of listed pair q (1-2 bonded pairs removed)
   auto ev_of_pair = [&](int q) {
-    const int2 ij = a.pairs[q];
+    const int2 ij = a.cpairs[q];
     const int i = ij.x, j = ij.y;
     const bool other = s.res_chain[j] != s.res_chain[i];
     const int dij = j - i;
@@ -956,7 +977,7 @@ template <typename R, bool SEL = false> __device__ __forceinline__ void pair_pas
     const int q = base + lane;
     bool q_d0 = false, q_d1 = false, q_p = false, q_e = false;  // queue: DSSP O(i), DSSP O(j), P_AP; stage: EV
     if (q < np) {
-    const int2 ij = a.pairs[q];
+    const int2 ij = a.cpairs[q];
     const int i = ij.x, j = ij.y;
     // every per-residue input of the pair, loaded up front and without
     // conditions, so that the gathers are in flight together
@@ -1091,7 +1112,7 @@ template <typename R, bool SEL = false> __device__ __forceinline__ void hbond_pa
   for (int t = sp.t; t < nd + np; t += sp.nthr) {
     const bool d = t < nd;
     const int q = d ? a.hbq[t] : a.hbq[(size_t) 2 * a.pcap + (t - nd)];
-    const int2 ij = a.pairs[q < 0 ? ~q : q];
+    const int2 ij = a.cpairs[q < 0 ? ~q : q];
     const int i = q < 0 ? ij.y : ij.x, j = q < 0 ? ij.x : ij.y;
     unsigned gate = 0;
     const R e = d ? dssp_term(s, p, i, j, SEL ? &gate : nullptr) : pap_term(s, p, i, j, SEL ? &gate : nullptr);
