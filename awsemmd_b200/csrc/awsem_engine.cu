@@ -1147,8 +1147,10 @@ template <typename R> class Engine : public EngineBase {
       int best = 0, best_pb = pair_blocks;
       double tbest = 1e30;
       const int tuned_pb = pair_blocks;
-      for (int pb : {tuned_pb, 2 * sms, 4 * sms, 8 * sms}) {
-        if (pb != tuned_pb && pb == best_pb) continue;
+      std::vector<int> grids{tuned_pb};
+      for (int k : {4, 8, 16, 32})
+        if (k * sms != tuned_pb) grids.push_back(k * sms);
+      for (int pb : grids) {
         for (int f : {0, 1, 2, 3, 4}) {
           pair_blocks = pb;
           fm_grid = f * sms;

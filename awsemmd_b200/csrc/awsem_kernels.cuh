@@ -580,11 +580,11 @@ template <typename R> __global__ void k_nl_build(StepArgs<R> a, GridArgs g, int 
 #define FOR_EACH_NEAR_PAIR(a, p, sp) \
   for (int p = (sp).t, np_ = min((a).nl->ncpairs, (a).pcap); p < np_; p += (sp).nthr)
 
-// DL1: local densities of contact beads (fix_backbone.cpp:7728-7791).  The
-// well windows are tested on the FP64 r^2 in both forms, so the selection is
-// the reference's exactly; the well value is FP64 in the plain form and FP32
-// in the mixed form, and the sums are exact in 2^-40 fixed point (dacc[0],
-// dacc[1]).
+// DL1: local densities of contact beads (fix_backbone.cpp:7728-7791).  FP64
+// in both forms: the densities feed the burial and switching functions (an
+// FP32 well value here put the helix term of configuration 1 at 3e-5 of its
+// small magnitude), and the well selection is the reference's exactly.  Sums
+// in 2^-40 fixed point (dacc[0], dacc[1]).
 template <typename R, bool SEL = false> __device__ __forceinline__ void density_pass(const StepArgs<R> &a, const FFParams &p, Span sp)
 {
   const DevSys<R> &s = a.s;
@@ -609,22 +609,19 @@ template <typename R, bool SEL = false> __device__ __forceinline__ void density_
     at = __shfl_sync(act, at, leader) + __popc(m & ((1u << lane) - 1u));
     if (near && at < a.pcap) a.cpairs[at] = ij;
     if (s.res_chain[j] == s.res_chain[i] && j - i <= 1) continue;
-    // the window tests on the FP64 r^2 in both forms (the reference's
-    // selections); the well value in the form's geometry type
-    const R r = R(sqrt(rsq));
+    const double r = sqrt(rsq);
     if (water && rsq > p.w_rmin_sq[0] && rsq < p.w_rmax_sq[0]) {
-      R th, pr;
-      well_theta(r, R(p.w_rmin_th[0]), R(p.w_rmax_th[0]), R(p.water_kappa), R(p.well_rmin[0]), R(p.well_rmax[0]), th,
-                 pr);
-      const unsigned long long v = (unsigned long long) fix_dens((double) th);
+      double th, pr;
+      well_theta(r, p.w_rmin_th[0], p.w_rmax_th[0], p.water_kappa, p.well_rmin[0], p.well_rmax[0], th, pr);
+      const unsigned long long v = (unsigned long long) fix_dens(th);
       atomicAdd(aw + i, v);
       atomicAdd(aw + j, v);
       sel_rec<SEL>(a, AWSEM_SEL_DENS_WATER, 0, i, j);
     }
     if (helix && rsq > p.h_rmin_sq && rsq < p.h_rmax_sq) {
-      R th, pr;
-      well_theta(r, R(p.h_rmin_th), R(p.h_rmax_th), R(p.helix_kappa), R(p.helix_rmin), R(p.helix_rmax), th, pr);
-      const unsigned long long v = (unsigned long long) fix_dens((double) th);
+      double th, pr;
+      well_theta(r, p.h_rmin_th, p.h_rmax_th, p.helix_kappa, p.helix_rmin, p.helix_rmax, th, pr);
+      const unsigned long long v = (unsigned long long) fix_dens(th);
       atomicAdd(ah + i, v);
       atomicAdd(ah + j, v);
       sel_rec<SEL>(a, AWSEM_SEL_DENS_HELIX, 0, i, j);
