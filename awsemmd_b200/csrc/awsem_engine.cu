@@ -140,8 +140,9 @@ class EngineBase {
 void fragmem_noalloc(int device, const FMView &v, const double *d_x, double *d_f, double *d_energy,
                      cudaStream_t stream);  // awsem_noalloc.cu
 
-static const char *kKernelNames[AWSEM_NKERNELS] = {"prepare", "nl_decide", "nl_build", "density", "residue",
-                                                   "water_xi", "pair",     "hbond",     "fragmem", "finish"};
+static const char *kKernelNames[AWSEM_NKERNELS] = {"prepare",  "nl_decide", "nl_build", "density",
+                                                   "residue",  "water_xi",  "radial",   "pair",
+                                                   "hbond",    "fragmem",   "finish"};
 
 template <typename R> class Engine : public EngineBase {
 
@@ -153,6 +154,7 @@ template <typename R> class Engine : public EngineBase {
   DBuf<double4> pos, cb_build;
   DBuf<unsigned long long> facc;
   DBuf<int2> pairs, cpairs;  // residue pair list; the near list of an evaluation
+  DBuf<int> seg_n;           // near pairs per near-list segment
   DBuf<int> ncount, hbq;
   DBuf<long long> dacc;
   int pair_blocks = 1;
@@ -249,6 +251,7 @@ template <typename R> class Engine : public EngineBase {
     a.e_res = e_res.p;
     a.pairs = pairs.p;
     a.cpairs = cpairs.p;
+    a.seg_n = seg_n.p;
     a.dacc = dacc.p;
     a.hbq = hbq.p;
     a.e_fix = e_fix.p;
@@ -550,6 +553,7 @@ template <typename R> class Engine : public EngineBase {
     pcap = (int) newcap;
     pairs.alloc((size_t) pcap);
     cpairs.alloc((size_t) pcap);
+    seg_n.alloc((size_t) pcap / 32 + 2);
     hbq.alloc((size_t) 3 * pcap);
     dev::NLState st;
     CK(cudaMemcpyAsync(&st, nl.p, sizeof st, cudaMemcpyDeviceToHost, s0));
@@ -652,17 +656,21 @@ template <typename R> class Engine : public EngineBase {
       dev::k_density_sel<R><<<pair_blocks, tb, 0, s0>>>(a, p);
       dev::k_residue_sel<R><<<nb, tb, 0, s0>>>(a, p);
       dev::k_water_xi_sel<R><<<pair_blocks, tb, 0, s0>>>(a, p);
+      dev::k_radial_sel<R><<<pair_blocks, tb, 0, s0>>>(a, p);
       dev::k_pair_sel<R><<<pair_blocks, tb, 0, s0>>>(a, p);
       dev::k_hbond_sel<R><<<hb_blocks, 128, 0, s0>>>(a, p);
     } else {
       dev::k_density<R><<<pair_blocks, tb, 0, s0>>>(a, p);
       dev::k_residue<R><<<nb, tb, 0, s0>>>(a, p);
       dev::k_water_xi<R><<<pair_blocks, tb, 0, s0>>>(a, p);
+      dev::k_radial<R><<<pair_blocks, tb, 0, s0>>>(a, p);
       dev::k_pair<R><<<pair_blocks, tb, 0, s0>>>(a, p);
       dev::k_hbond<R><<<hb_blocks, 128, 0, s0>>>(a, p);
     }
     if (fm || fmt || go || px || rx) CK(cudaStreamWaitEvent(s0, ev_join, 0));
   }
+
+  int finish_blocks() const { return (n_run() + dev::kFinishRes - 1) / dev::kFinishRes; }
 
   int fm_table_blocks() const
   {
@@ -917,7 +925,7 @@ template <typename R> class Engine : public EngineBase {
         launch_step_persistent(a);
       } else {
         launch_eval(a, true);
-        dev::k_finish<R><<<nb, tb, 0, s0>>>(a, d_integ.p, g1.p, g2.p, ftot.p, x.p);
+        dev::k_finish<R><<<finish_blocks(), dev::kFinishThreads, 0, s0>>>(a, d_integ.p, g1.p, g2.p, ftot.p, x.p);
       }
       if (thermo)
         dev::k_thermo<<<n_sys(), 256, 0, s0>>>(e_res.p, e_fix.p, efix_slots, nn, dstep.p, d_integ.p, sys_begin.p, sys_end.p,
@@ -1227,16 +1235,17 @@ template <typename R> class Engine : public EngineBase {
           case 3: dev::k_density<R><<<pair_blocks, tb, 0, s0>>>(a, p); break;
           case 4: dev::k_residue<R><<<nb, tb, 0, s0>>>(a, p); break;
           case 5: dev::k_water_xi<R><<<pair_blocks, tb, 0, s0>>>(a, p); break;
-          case 6: dev::k_pair<R><<<pair_blocks, tb, 0, s0>>>(a, p); break;
-          case 7: dev::k_hbond<R><<<hb_blocks, 128, 0, s0>>>(a, p); break;
-          case 8:
+          case 6: dev::k_radial<R><<<pair_blocks, tb, 0, s0>>>(a, p); break;
+          case 7: dev::k_pair<R><<<pair_blocks, tb, 0, s0>>>(a, p); break;
+          case 8: dev::k_hbond<R><<<hb_blocks, 128, 0, s0>>>(a, p); break;
+          case 9:
             if (fm) dev::k_fragmem<R><<<fm_blocks(), tb, fm_smem(), s0>>>(a, p);
             if (p.terms & T_FM_TABLE) dev::k_fm_table<R><<<fm_table_blocks(), tb, 0, s0>>>(a, p);
             if (p.terms & T_AMHGO) dev::k_amh_go<R><<<nb, tb, 0, s0>>>(a, p);
             if (p.terms & (T_SSB | T_DH | T_CONTREST)) dev::k_pair_extra<R><<<pair_blocks, tb, 0, s0>>>(a, p);
             if (p.terms & (T_SHAKE | T_MEMB | T_VFM)) dev::k_residue_extra<R><<<nb, tb, 0, s0>>>(a, p);
             break;
-          case 9: dev::k_finish<R><<<nb, tb, 0, s0>>>(a, d_integ.p, g1.p, g2.p, ftot.p, x.p); break;
+          case 10: dev::k_finish<R><<<finish_blocks(), dev::kFinishThreads, 0, s0>>>(a, d_integ.p, g1.p, g2.p, ftot.p, x.p); break;
         }
         CK(cudaEventRecord(ev[2 * k + 1], s0));
       }

@@ -426,7 +426,7 @@ __device__ __forceinline__ bool fragmem_unit_bulk_t(int w, const FMSlices<R> &t,
       }
       // the stripes of this chunk that belong to the current row (at least one)
       const int run = max(q + 1, min(ns, blk_end - s0));
-#pragma unroll(sizeof(R) == 4 ? 2 : 1)
+#pragma unroll(sizeof(R) == 4 ? 4 : 1)
       for (; q < run; q++) {
         R rec[4];
         load_record_shared(srf, q * 32 + lane, rec);
@@ -481,21 +481,26 @@ __device__ __forceinline__ void fragmem_ring_init(unsigned char *wsm)
   __syncwarp();
 }
 
-// The kernel body: each warp takes work units w, w + warps, ... so a grid
-// smaller than the number of units (a few blocks per SM) still streams at
-// full bandwidth and leaves the rest of each SM to the concurrent pair passes.
+// The kernel body: each warp takes work units one at a time from a counter
+// (zero at launch), so a grid smaller than the number of units (a few blocks
+// per SM) still streams at full bandwidth and leaves the rest of each SM to
+// the concurrent pair passes; warps that get more of their SM take more
+// units, and the launch ends within one unit of balance.
 template <typename R, class Pos>
-__device__ __forceinline__ void fragmem_warp_bulk(const FMSlices<R> &t, const double *sig, int n, const Pos &pos,
+__device__ __forceinline__ void fragmem_warp_take(const FMSlices<R> &t, const double *sig, int n, const Pos &pos,
                                                   unsigned long long *facc, unsigned long long *e_acc,
-                                                  int e_stride, int *timed_out, unsigned char *wsm)
+                                                  int e_stride, int *timed_out, unsigned char *wsm, int *next)
 {
-  const int units = t.groups * t.dsplit;
-  const int w0 = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
-  if (w0 >= units) return;
+  const int units = t.groups * t.dsplit, lane = threadIdx.x & 31;
   fragmem_ring_init(wsm);
   unsigned kbase = 0;
-  for (int w = w0; w < units; w += nw)
-    if (!fragmem_unit_bulk(w, t, sig, n, pos, facc, e_acc, e_stride, timed_out, wsm, kbase)) return;
+  while (true) {
+    int u = 0;
+    if (lane == 0) u = atomicAdd(next, 1);
+    u = __shfl_sync(0xffffffffu, u, 0);
+    if (u >= units) return;
+    if (!fragmem_unit_bulk(u, t, sig, n, pos, facc, e_acc, e_stride, timed_out, wsm, kbase)) return;
+  }
 }
 
 }  // namespace dev

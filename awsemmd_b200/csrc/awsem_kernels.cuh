@@ -64,7 +64,14 @@ struct NLState {
   float lst_d2max;    // max CA displacement^2 since the last emulated build (this step)
   int bad_x;          // a position was not finite (results invalid; the host reports and clears it)
   float need;         // R_need of this step: no term reaches a pair whose contact beads are farther apart
-  int ncpairs;        // pairs of the near list (contact beads within `need`), written by the density pass
+  // The near list (the listed pairs whose contact beads are within `need`)
+  // is written by the density pass in segments: warp w of that pass scans
+  // the listed pairs [w seg_len, (w + 1) seg_len) and writes its near pairs,
+  // in list order, to the start of the same range of cpairs; seg_n[w] holds
+  // their count.  No shared counter: every warp owns its range.
+  int seg_len;        // pairs per segment (a multiple of 32)
+  int nseg;           // segments
+  int fm_next;        // fragment-memory work units handed out (k_fragmem), zeroed by the list decision
 };
 
 // Run window of one replica: integrated over steps begin..end (the
@@ -88,9 +95,11 @@ template <typename R> struct StepArgs {
   double *e_res;  // [E_SLOTS][n_res]
   // residue pair list: pairs (i, j), i < j, capacity pcap; per-residue counts.
   // cpairs: the near list of this evaluation (the listed pairs whose contact
-  // beads are within NLState::need), written by the density pass and walked
-  // by the water-xi, pair and hydrogen-bond passes (capacity pcap)
+  // beads are within NLState::need), written by the density pass in segments
+  // (seg_n: near pairs per segment, capacity pcap / 32 + 2) and walked by the
+  // water-xi, pair and hydrogen-bond passes (capacity pcap)
   int2 *pairs, *cpairs;
+  int *seg_n;
   int *ncount, pcap;
   double4 *cb_build;
   NLState *nl;
@@ -319,7 +328,7 @@ __device__ __forceinline__ void nl_decide(NLState *nl, int force, long long *ste
   }
   s.rebuild = rb;
   s.need = need;
-  s.ncpairs = 0;
+  s.fm_next = 0;
   // two residues whose CAs are farther apart than r_ev + 2 * reach have no
   // bead pair inside any excluded-volume cutoff (0.01 A covers rounding)
   float pre = s.r_ev + 2.f * s.bCAx + 0.01f;
@@ -576,9 +585,12 @@ template <typename R> __global__ void k_nl_build(StepArgs<R> a, GridArgs g, int 
 // Pairs of the list, grid-stride (the count is known only on the device)
 #define FOR_EACH_PAIR(a, p, sp) \
   for (int p = (sp).t, np_ = min((a).nl->npairs, (a).pcap); p < np_; p += (sp).nthr)
-// Pairs of the near list (written by the density pass of this evaluation)
-#define FOR_EACH_NEAR_PAIR(a, p, sp) \
-  for (int p = (sp).t, np_ = min((a).nl->ncpairs, (a).pcap); p < np_; p += (sp).nthr)
+// Pairs of the near list (written by the density pass of this evaluation):
+// index p is entry p % seg_len of segment p / seg_len, present when below
+// that segment's count
+#define FOR_EACH_NEAR_PAIR(a, p, sp)                                                                     \
+  for (int p = (sp).t, S_ = (a).nl->seg_len, end_ = (a).nl->nseg * S_; p < end_; p += (sp).nthr)      \
+    if (p - (p / S_) * S_ < (a).seg_n[p / S_])
 
 // DL1: local densities of contact beads (fix_backbone.cpp:7728-7791).  FP64
 // in both forms: the densities feed the burial and switching functions (an
@@ -595,20 +607,32 @@ template <typename R, bool SEL = false> __device__ __forceinline__ void density_
   // the near list: the listed pairs some term can reach at this step (the
   // bound the list's validity check uses; the margin covers its rounding)
   const double need_sq = (double) a.nl->need * (double) a.nl->need * 1.00001;
-  const int lane = threadIdx.x & 31;
-  FOR_EACH_PAIR(a, q, sp)
-  {
-    const int2 ij = a.pairs[q];
+  const int lane = threadIdx.x & 31, w = sp.t >> 5, nw = sp.nthr >> 5;
+  const int np = min(a.nl->npairs, a.pcap);
+  // one contiguous segment of the list per warp
+  const int seg = max(32, ((np + nw - 1) / nw + 31) & ~31), nseg = (np + seg - 1) / seg;
+  if (sp.t == 0) {
+    a.nl->seg_len = seg;
+    a.nl->nseg = nseg;
+  }
+  if (w >= nseg) return;
+  const int lo = w * seg, hi = min(lo + seg, np);
+  int cnt = 0;  // near pairs written so far (warp-uniform)
+  for (int base = lo; base < hi; base += 32) {
+    const int q = base + lane;
+    int2 ij = {0, 0};
+    double rsq = 0.0;
+    bool near = false;
+    if (q < hi) {
+      ij = a.pairs[q];
+      rsq = norm2(diff<double>(contact(s, ij.x), contact(s, ij.y)));
+      near = rsq < need_sq;
+    }
+    const unsigned m = __ballot_sync(0xffffffffu, near);
+    if (near) a.cpairs[lo + cnt + __popc(m & ((1u << lane) - 1u))] = ij;
+    cnt += __popc(m);
     const int i = ij.x, j = ij.y;
-    const double rsq = norm2(diff<double>(contact(s, i), contact(s, j)));
-    const bool near = rsq < need_sq;
-    const unsigned act = __activemask(), m = __ballot_sync(act, near);
-    const int leader = __ffs(act) - 1;
-    int at = 0;
-    if (lane == leader && m) at = atomicAdd(&a.nl->ncpairs, __popc(m));
-    at = __shfl_sync(act, at, leader) + __popc(m & ((1u << lane) - 1u));
-    if (near && at < a.pcap) a.cpairs[at] = ij;
-    if (s.res_chain[j] == s.res_chain[i] && j - i <= 1) continue;
+    if (q >= hi || (s.res_chain[j] == s.res_chain[i] && j - i <= 1)) continue;
     const double r = sqrt(rsq);
     if (water && rsq > p.w_rmin_sq[0] && rsq < p.w_rmax_sq[0]) {
       double th, pr;
@@ -627,6 +651,7 @@ template <typename R, bool SEL = false> __device__ __forceinline__ void density_
       sel_rec<SEL>(a, AWSEM_SEL_DENS_HELIX, 0, i, j);
     }
   }
+  if (lane == 0) a.seg_n[w] = cnt;
 }
 
 template <typename R> __global__ void k_density(StepArgs<R> a, FFParams p) { density_pass(a, p, grid_span()); }
@@ -873,107 +898,21 @@ template <typename R> __device__ __forceinline__ void scatter_fix(const DevSys<R
     if (f[c]) atomicAdd(q + c, (unsigned long long) f[c]);
 }
 
-// DL3: main pair loop (fix_backbone.cpp:7956-8134) plus excluded volume
-// between residues, one thread per listed pair i < j.  Radial contact forces
-// and excluded volume are applied to both residues.  DSSP and P_AP pairs are
-// only detected here (cheap distance and index tests) and queued: k_hbond
-// evaluates them, so their long, branchy bodies do not slow this pass.
-template <typename R, bool SEL = false> __device__ __forceinline__ void pair_pass(const StepArgs<R> &a, const FFParams &p, Span sp)
+// DL3 radial terms (fix_backbone.cpp:7956-8057, :8116-8128): the water,
+// burial and helix wells of the contact beads of every near pair, one thread
+// per pair; the radial force goes to both residues.
+template <typename R, bool SEL = false> __device__ __forceinline__ void radial_pass(const StepArgs<R> &a, const FFParams &p, Span sp)
 {
   const DevSys<R> &s = a.s;
+  const bool fix = a.groups & G_FIX;
+  if (!fix) return;
   const int n = s.n_res;
   const double *WG = s.tables + TB_WATER;
-  const bool fix = a.groups & G_FIX, evon = a.groups & G_PAIR;
-  const uint32_t T = fix ? p.terms : 0u;
-  const R ev_pre_sq = R(a.nl->ev_pre_sq), dssp_pre_sq = R(a.nl->dssp_pre_sq);
-  // the largest excluded-volume cutoff, squared, with room for its rounding
-  // to float and for the rounding of the bead distance
-  const R ev_max_sq = R(a.nl->r_ev) * R(a.nl->r_ev) * R(1.0001);
-  // smallest same-chain separation of any P_AP class (fix_backbone.cpp:3279-3383)
-  const int pap_sep = min(p.i_med_min + 2 * p.i_diff_pap, p.i_med_max + 1);
+  const uint32_t T = p.terms;
   const int dh = p.helix_i_diff;
-  const size_t qd = 0, qp = (size_t) 2 * a.pcap;  // queue regions: DSSP (both orientations), P_AP
   unsigned long long *e_water = (unsigned long long *) a.e_fix + (size_t) 3 * n;
-  unsigned long long *e_ev = (unsigned long long *) a.e_fix + (size_t) 4 * n;
-  const int lane = threadIdx.x & 31, np = min(a.nl->ncpairs, a.pcap);
-  // Queue entries are staged per warp in shared memory and written out 32 at
-  // a time with one atomic reservation: one counter update per 32 entries
-  // instead of one per warp iteration (same-address atomics serialise in L2).
-  constexpr int kStageWarps = 8;  // warps per block of any caller
-  __shared__ int stage_d[kStageWarps][96], stage_p[kStageWarps][64], stage_e[kStageWarps][64];
-  int *const sd = stage_d[threadIdx.x >> 5], *const spp = stage_p[threadIdx.x >> 5];
-  int *const se = stage_e[threadIdx.x >> 5];
-  int nsd = 0, nsp = 0, nse = 0;  // staged entries (warp-uniform)
-  // write the first `count` staged entries (count <= 32) to the queue at `region`, move the rest down
-  auto flush = [&](int *buf, int &cnt, int count, int *counter, size_t region) {
-    int at = 0;
-    if (lane == 0) at = atomicAdd(counter, count);
-    at = __shfl_sync(0xffffffffu, at, 0);
-    if (lane < count) a.hbq[region + at + lane] = buf[lane];
-    const int v1 = lane + 32 < cnt ? buf[lane + 32] : 0, v2 = lane + 64 < cnt ? buf[lane + 64] : 0;
-    __syncwarp();
-    buf[lane] = v1;
-    buf[lane + 32] = v2;  // index < 64: inside both buffers
-    __syncwarp();
-    cnt -= count;
-  };
-  // excluded volume between the beads of listed pair q (1-2 bonded pairs removed)
-  auto ev_of_pair = [&](int q) {
-    const int2 ij = a.cpairs[q];
-    const int i = ij.x, j = ij.y;
-    const bool other = s.res_chain[j] != s.res_chain[i];
-    const int dij = j - i;
-    const V3<double> ca_i = bead(s, i, B_CA), ca_j = bead(s, j, B_CA);
-    const unsigned excl = j == i + 1 ? a.excl_next[i] : 0u;
-    const bool shortr = !other && dij < 5;
-    const V3<double> bi[3] = {ca_i, bead(s, i, B_CB), bead(s, i, B_O)};
-    const int tai[3] = {a.atom_type[3 * i], a.atom_type[3 * i + 1], a.atom_type[3 * i + 2]};
-    long long Fi[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
-    double ee = 0.0;
-#pragma unroll
-    for (int b1 = 0; b1 < 3; b1++) {
-      const V3<double> bj = b1 == 0 ? ca_j : bead(s, j, b1);
-      const int tb = a.atom_type[3 * j + b1];
-      long long Fj[3] = {0, 0, 0};
-#pragma unroll
-      for (int b0 = 0; b0 < 3; b0++) {
-        if (excl & (1u << (b0 * 3 + b1))) continue;
-        const V3<R> dd = diff<R>(bi[b0], bj);
-        if (norm2(dd) > ev_max_sq) continue;  // beyond every cutoff: no table lookups
-        V3<R> f;
-        bool hit = false;
-        const R e = ev_pair(a, tai[b0], tb, shortr, dd, f, SEL ? &hit : nullptr);
-        if (hit) sel_rec<SEL>(a, AWSEM_SEL_EV, 3 * b0 + b1, i, j);
-        if (e == R(0) && f.x == R(0) && f.y == R(0) && f.z == R(0)) continue;
-        ee += (double) e;
-        const long long v[3] = {fix_force((double) f.x), fix_force((double) f.y), fix_force((double) f.z)};
-#pragma unroll
-        for (int c = 0; c < 3; c++) {
-          Fi[b0][c] += v[c];
-          Fj[c] -= v[c];
-        }
-      }
-      scatter_fix(s, j, b1, Fj);
-    }
-#pragma unroll
-    for (int b0 = 0; b0 < 3; b0++) scatter_fix(s, i, b0, Fi[b0]);
-    if (ee != 0.0) atomicAdd(e_ev + i, (unsigned long long) fix_force(ee));
-  };
-  // run the first `count` staged EV pairs (count <= 32), one per lane; move the rest down
-  auto ev_batch = [&](int count) {
-    const int q = lane < count ? se[lane] : -1;
-    const int v1 = lane + 32 < nse ? se[lane + 32] : 0;
-    __syncwarp();
-    se[lane] = v1;
-    __syncwarp();
-    nse -= count;
-    if (q >= 0) ev_of_pair(q);
-  };
-  // warp-uniform trip count: the queue appends below are warp collectives
-  for (int base = sp.t - lane; base < np; base += sp.nthr) {
-    const int q = base + lane;
-    bool q_d0 = false, q_d1 = false, q_p = false, q_e = false;  // queue: DSSP O(i), DSSP O(j), P_AP; stage: EV
-    if (q < np) {
+  FOR_EACH_NEAR_PAIR(a, q, sp)
+  {
     const int2 ij = a.cpairs[q];
     const int i = ij.x, j = ij.y;
     // every per-residue input of the pair, loaded up front and without
@@ -981,17 +920,16 @@ template <typename R, bool SEL = false> __device__ __forceinline__ void pair_pas
     const int fli = s.res_flags[i], flj = s.res_flags[j];
     const bool other = s.res_chain[j] != s.res_chain[i];
     const int ti = s.res_type[i], tj = s.res_type[j];
-    const V3<double> ca_i = bead(s, i, B_CA), ca_j = bead(s, j, B_CA);
-    const V3<double> cb_i = bead(s, i, B_CB), cb_j = bead(s, j, B_CB);
+    const V3<double> c_i = bead(s, i, (fli & R_GLY) ? B_CA : B_CB), c_j = bead(s, j, (flj & R_GLY) ? B_CA : B_CB);
     const double sw_i = a.sig_w[i], sw_j = a.sig_w[j], bur_i = a.bur[i], bur_j = a.bur[j];
     const double xi_i = water_xi(a, i), xi_j = water_xi(a, j);
     const double x1_i = a.xi1[i], x1_j = a.xi1[j];
     const double x2_i = a.xi2[max(i - dh, 0)], x2_j = a.xi2[max(j - dh, 0)];
     const int dij = j - i;
     // contact-bead radial terms
-    if (fix && (other || dij > 1)) {
+    if (other || dij > 1) {
       const bool gi = fli & R_GLY, gj = flj & R_GLY;
-      const V3<R> d = diff<R>(gi ? ca_i : cb_i, gj ? ca_j : cb_j);
+      const V3<R> d = diff<R>(c_i, c_j);
       const R rsq = norm2(d);
       const R r = m_sqrt(rsq);
       R force = 0;
@@ -1050,6 +988,121 @@ template <typename R, bool SEL = false> __device__ __forceinline__ void pair_pas
         scatter_fix(s, j, gj ? B_CA : B_CB, g);
       }
     }
+  }
+}
+
+// blocks per SM the radial and detection passes are compiled for (the
+// passes are latency bound: 8 blocks of 4 warps in FP32 fit in 64 registers
+// without spills; the FP64 form holds twice the data)
+template <typename R> constexpr int kPairMinBlocks = sizeof(R) == 4 ? 8 : 5;
+template <typename R> __global__ void __launch_bounds__(128, kPairMinBlocks<R>) k_radial(StepArgs<R> a, FFParams p)
+{
+  radial_pass(a, p, grid_span());
+}
+template <typename R> __global__ void __launch_bounds__(128) k_radial_sel(StepArgs<R> a, FFParams p)
+{
+  radial_pass<R, true>(a, p, grid_span());
+}
+
+// DL3 pair detection (fix_backbone.cpp:8064-8103) and excluded volume
+// between residues, one thread per near pair i < j.  DSSP and P_AP pairs
+// are only detected here (cheap distance and index tests) and queued:
+// k_hbond evaluates them, so their long, branchy bodies do not slow this
+// pass.  Excluded volume is applied to both residues.
+template <typename R, bool SEL = false> __device__ __forceinline__ void pair_pass(const StepArgs<R> &a, const FFParams &p, Span sp)
+{
+  const DevSys<R> &s = a.s;
+  const int n = s.n_res;
+  const bool fix = a.groups & G_FIX, evon = a.groups & G_PAIR;
+  const uint32_t T = fix ? p.terms : 0u;
+  const R ev_pre_sq = R(a.nl->ev_pre_sq), dssp_pre_sq = R(a.nl->dssp_pre_sq);
+  // the largest excluded-volume cutoff, squared, with room for its rounding
+  // to float and for the rounding of the bead distance
+  const R ev_max_sq = R(a.nl->r_ev) * R(a.nl->r_ev) * R(1.0001);
+  // smallest same-chain separation of any P_AP class (fix_backbone.cpp:3279-3383)
+  const int pap_sep = min(p.i_med_min + 2 * p.i_diff_pap, p.i_med_max + 1);
+  const size_t qd = 0, qp = (size_t) 2 * a.pcap;  // queue regions: DSSP (both orientations), P_AP
+  unsigned long long *e_ev = (unsigned long long *) a.e_fix + (size_t) 4 * n;
+  const int lane = threadIdx.x & 31, seg = a.nl->seg_len, np = a.nl->nseg * seg;
+  // Queue entries are staged per warp in shared memory and written out 32 at
+  // a time with one atomic reservation: one counter update per 32 entries
+  // instead of one per warp iteration (same-address atomics serialise in L2).
+  constexpr int kStageWarps = 8;  // warps per block of any caller
+  __shared__ int stage_d[kStageWarps][96], stage_p[kStageWarps][64], stage_e[kStageWarps][64];
+  int *const sd = stage_d[threadIdx.x >> 5], *const spp = stage_p[threadIdx.x >> 5];
+  int *const se = stage_e[threadIdx.x >> 5];
+  int nsd = 0, nsp = 0, nse = 0;  // staged entries (warp-uniform)
+  // write the first `count` staged entries (count <= 32) to the queue at `region`, move the rest down
+  auto flush = [&](int *buf, int &cnt, int count, int *counter, size_t region) {
+    int at = 0;
+    if (lane == 0) at = atomicAdd(counter, count);
+    at = __shfl_sync(0xffffffffu, at, 0);
+    if (lane < count) a.hbq[region + at + lane] = buf[lane];
+    const int v1 = lane + 32 < cnt ? buf[lane + 32] : 0, v2 = lane + 64 < cnt ? buf[lane + 64] : 0;
+    __syncwarp();
+    buf[lane] = v1;
+    buf[lane + 32] = v2;  // index < 64: inside both buffers
+    __syncwarp();
+    cnt -= count;
+  };
+  // excluded volume between the beads of listed pair q (1-2 bonded pairs removed)
+  auto ev_of_pair = [&](int q) {
+    const int2 ij = a.cpairs[q];
+    const int i = ij.x, j = ij.y;
+    const bool other = s.res_chain[j] != s.res_chain[i];
+    const int dij = j - i;
+    const unsigned excl = j == i + 1 ? a.excl_next[i] : 0u;
+    const bool shortr = !other && dij < 5;
+    double ee = 0.0;
+    // bead b of a residue: CA, CB, O for b = 0, 1, 2; each bead pair's force
+    // is scattered as it is found (few pairs come this close, and keeping
+    // nine sums live would cost the whole pass registers)
+#pragma unroll 1
+    for (int b1 = 0; b1 < 3; b1++) {
+      const V3<double> bj = bead(s, j, b1);
+      const int tb = a.atom_type[3 * j + b1];
+#pragma unroll 1
+      for (int b0 = 0; b0 < 3; b0++) {
+        if (excl & (1u << (b0 * 3 + b1))) continue;
+        const V3<R> dd = diff<R>(bead(s, i, b0), bj);
+        if (norm2(dd) > ev_max_sq) continue;  // beyond every cutoff: no table lookups
+        V3<R> f;
+        bool hit = false;
+        const R e = ev_pair(a, a.atom_type[3 * i + b0], tb, shortr, dd, f, SEL ? &hit : nullptr);
+        if (hit) sel_rec<SEL>(a, AWSEM_SEL_EV, 3 * b0 + b1, i, j);
+        if (e == R(0) && f.x == R(0) && f.y == R(0) && f.z == R(0)) continue;
+        ee += (double) e;
+        const long long v[3] = {fix_force((double) f.x), fix_force((double) f.y), fix_force((double) f.z)};
+        const long long w[3] = {-v[0], -v[1], -v[2]};
+        scatter_fix(s, i, b0, v);
+        scatter_fix(s, j, b1, w);
+      }
+    }
+    if (ee != 0.0) atomicAdd(e_ev + i, (unsigned long long) fix_force(ee));
+  };
+  // run the first `count` staged EV pairs (count <= 32), one per lane; move the rest down
+  auto ev_batch = [&](int count) {
+    const int q = lane < count ? se[lane] : -1;
+    const int v1 = lane + 32 < nse ? se[lane + 32] : 0;
+    __syncwarp();
+    se[lane] = v1;
+    __syncwarp();
+    nse -= count;
+    if (q >= 0) ev_of_pair(q);
+  };
+  // warp-uniform trip count: the queue appends below are warp collectives
+  // (a warp's 32 indices lie in one near-list segment: segments are multiples of 32 long)
+  for (int base = sp.t - lane; base < np; base += sp.nthr) {
+    const int q = base + lane, sg = base / seg, have = a.seg_n[sg] - (base - sg * seg);
+    if (have <= 0) continue;  // warp-uniform: past this segment's near pairs
+    bool q_d0 = false, q_d1 = false, q_p = false, q_e = false;  // queue: DSSP O(i), DSSP O(j), P_AP; stage: EV
+    if (lane < have) {
+    const int2 ij = a.cpairs[q];
+    const int i = ij.x, j = ij.y;
+    const int fli = s.res_flags[i], flj = s.res_flags[j];
+    const bool other = s.res_chain[j] != s.res_chain[i];
+    const V3<double> ca_i = bead(s, i, B_CA), ca_j = bead(s, j, B_CA);
+    const int dij = j - i;
     const R rca2 = norm2(diff<R>(ca_i, ca_j));
     // excluded volume between beads of i and j: staged (below), so that the
     // few pairs this close run their 3 x 3 bead loop with full warps
@@ -1085,9 +1138,6 @@ template <typename R, bool SEL = false> __device__ __forceinline__ void pair_pas
   if (nse > 0) ev_batch(nse);
 }
 
-// blocks per SM the pair pass is compiled for: its up-front gathers need the
-// registers of 5 blocks in FP32; the FP64 form holds twice the data
-template <typename R> constexpr int kPairMinBlocks = sizeof(R) == 4 ? 5 : 4;
 template <typename R> __global__ void __launch_bounds__(128, kPairMinBlocks<R>) k_pair(StepArgs<R> a, FFParams p)
 {
   pair_pass(a, p, grid_span());
@@ -1119,7 +1169,10 @@ template <typename R, bool SEL = false> __device__ __forceinline__ void hbond_pa
   }
 }
 
-template <typename R> __global__ void __launch_bounds__(128, 6) k_hbond(StepArgs<R> a, FFParams p)
+// blocks per SM the hydrogen-bond pass is compiled for (the FP64 form needs
+// the registers of 4 blocks to keep its terms out of local memory)
+template <typename R> constexpr int kHbondMinBlocks = sizeof(R) == 4 ? 6 : 4;
+template <typename R> __global__ void __launch_bounds__(128, kHbondMinBlocks<R>) k_hbond(StepArgs<R> a, FFParams p)
 {
   hbond_pass(a, p, grid_span());
 }
@@ -1141,8 +1194,9 @@ template <typename R> __global__ void __launch_bounds__(128) k_fragmem(StepArgs<
   extern __shared__ __align__(128) unsigned char fm_smem[];
   const BeadPos<R> pos{&a.s};
   unsigned char *wsm = fm_smem + (threadIdx.x >> 5) * fm_warp_smem<R>(a.fm.coef != nullptr);
-  fragmem_warp_bulk(a.fm, p.fm_sigma_sq, a.s.n_res, pos, a.s.facc,
-                    (unsigned long long *) (a.e_fix + (size_t) 2 * a.s.n_res), 1, &a.nl->fm_timeout, wsm);
+  fragmem_warp_take(a.fm, p.fm_sigma_sq, a.s.n_res, pos, a.s.facc,
+                    (unsigned long long *) (a.e_fix + (size_t) 2 * a.s.n_res), 1, &a.nl->fm_timeout, wsm,
+                    &a.nl->fm_next);
 }
 
 // Table fragment memory of residue i and separation slot jo
@@ -1578,53 +1632,67 @@ struct Integrator {
 // step+1 (half kick + drift) -- LAMMPS fix nve / fix langevin order.  Each
 // replica follows its own run window (SlotRun); outside it the replica is
 // frozen, and residues of no replica are skipped.
+//
+// One component k = 3 b + c (bead b, axis c) of residue r; returns false
+// when the residue is not integrated at this step, else its kinetic-energy
+// term m v^2 (after the final half kick) in *ke.
+template <typename R>
+__device__ __forceinline__ bool finish_comp(const StepArgs<R> &a, const Integrator &in, long long step,
+                                            const double *g1, const double *g2, double *ftot, double *x_out, int r,
+                                            int k, double *ke)
+{
+  const int rep = a.res_sys[r];
+  if (rep < 0) return false;
+  const SlotRun sr = a.slot_run[rep];
+  if (step < sr.begin || step > sr.end) return false;
+  const bool final_kick = step > sr.begin, next = step < sr.end && step < in.stop;
+  const size_t e = (size_t) 9 * r + k;  // element of the [atom][3] arrays
+  if (a.lst_x0 && a.lst_build[rep]) a.lst_x0[e] = x_out[e];  // the emulated lists were built at these positions
+  const int at = 3 * r + k / 3, c = k % 3;
+  // Every multiply and add below is rounded on its own (no contraction), as
+  // the x86-64 CPU build computes fix langevin / fix nve, and identically in
+  // every kernel that inlines this.
+  const double m = a.mass[at];
+  const double dtfm = in.dtf / m;
+  double f = (double) (long long) a.s.facc[e] * F_UNSCALE;
+  double v = a.v[e];
+  if (in.langevin) {
+    const double delta = sr.end != sr.begin ? (double) (step - sr.begin) / (double) (sr.end - sr.begin) : 0.0;
+    const double tsqrt = sqrt(__dadd_rn(sr.t_start, __dmul_rn(delta, __dsub_rn(sr.t_stop, sr.t_start))));
+    // the replica's own step count keys its noise
+    const uint64_t nkey = uniform_key(a.sys_seed[rep], step - sr.step0);
+    f = __dadd_rn(f, __dadd_rn(__dmul_rn(g1[at], v),
+                               __dmul_rn(__dmul_rn(g2[at], tsqrt), __dsub_rn(uniform01_k(nkey, a.atom_tag[at], c), 0.5))));
+  }
+  if (ftot) ftot[e] = f;
+  if (final_kick) v = __dadd_rn(v, __dmul_rn(dtfm, f));
+  *ke = __dmul_rn(__dmul_rn(m, v), v);
+  if (next) {
+    v = __dadd_rn(v, __dmul_rn(dtfm, f));
+    x_out[e] = __dadd_rn(x_out[e], __dmul_rn(in.dt, v));
+  }
+  a.v[e] = v;
+  return true;
+}
+
+// kinetic energy of a residue from its nine terms, summed in component order
+__device__ __forceinline__ double kinetic(const double t[9])
+{
+  double ke = 0.0;
+#pragma unroll
+  for (int k = 0; k < 9; k++) ke = __dadd_rn(ke, t[k]);
+  return 0.5 * 48.88821291 * 48.88821291 * ke;
+}
+
+// all nine components of residue r by one thread (the persistent step form)
 template <typename R>
 __device__ __forceinline__ void finish_one(const StepArgs<R> &a, const Integrator &in, long long step, const double *g1,
                                            const double *g2, double *ftot, double *x_out, int r)
 {
-  const int rep = a.res_sys[r];
-  if (rep < 0) return;
-  const SlotRun sr = a.slot_run[rep];
-  if (step < sr.begin || step > sr.end) return;
-  const bool final_kick = step > sr.begin, next = step < sr.end && step < in.stop;
-  if (a.lst_x0 && a.lst_build[rep])  // the emulated lists were built at these positions
-    for (int k = 0; k < 9; k++) a.lst_x0[(size_t) 9 * r + k] = x_out[(size_t) 9 * r + k];
-  const unsigned long long seed = a.sys_seed[rep];
-  const long long key = step - sr.step0;  // the replica's own step count keys its noise
-  // Every multiply and add below is rounded on its own (no contraction), as
-  // the x86-64 CPU build computes fix langevin / fix nve, and identically in
-  // every kernel that inlines this.
-  double tsqrt = 0.0;
-  const uint64_t nkey = in.langevin ? uniform_key(seed, key) : 0ull;  // once per residue, not per draw
-  if (in.langevin) {
-    double delta = sr.end != sr.begin ? (double) (step - sr.begin) / (double) (sr.end - sr.begin) : 0.0;
-    tsqrt = sqrt(__dadd_rn(sr.t_start, __dmul_rn(delta, __dsub_rn(sr.t_stop, sr.t_start))));
-  }
-  double ke = 0.0;
-  for (int b = 0; b < 3; b++) {
-    int at = 3 * r + b;
-    double m = a.mass[at];
-    double dtfm = in.dtf / m;
-    const unsigned long long *fa = a.s.facc + (size_t) 3 * at;
-    for (int c = 0; c < 3; c++) {
-      double f = (double) (long long) fa[c] * F_UNSCALE;
-      double v = a.v[3 * at + c];
-      if (in.langevin)
-        f = __dadd_rn(f, __dadd_rn(__dmul_rn(g1[at], v),
-                                   __dmul_rn(__dmul_rn(g2[at], tsqrt),
-                                             __dsub_rn(uniform01_k(nkey, a.atom_tag[at], c), 0.5))));
-      if (ftot) ftot[3 * at + c] = f;
-      if (final_kick) v = __dadd_rn(v, __dmul_rn(dtfm, f));
-      ke = __dadd_rn(ke, __dmul_rn(__dmul_rn(m, v), v));
-      if (next) {
-        v = __dadd_rn(v, __dmul_rn(dtfm, f));
-        x_out[3 * at + c] = __dadd_rn(x_out[3 * at + c], __dmul_rn(in.dt, v));
-      }
-      a.v[3 * at + c] = v;
-    }
-  }
-  // kinetic energy after the final half kick (thermo output of the step)
-  a.e_res[(size_t) E_KIN * a.s.n_res + r] = 0.5 * 48.88821291 * 48.88821291 * ke;
+  double t[9];
+  for (int k = 0; k < 9; k++)
+    if (!finish_comp(a, in, step, g1, g2, ftot, x_out, r, k, &t[k])) return;
+  a.e_res[(size_t) E_KIN * a.s.n_res + r] = kinetic(t);
 }
 
 template <typename R>
@@ -1636,11 +1704,32 @@ __device__ __forceinline__ void finish_pass(const StepArgs<R> &a, const Integrat
   for (int r = sp.t; r < a.n_run; r += sp.nthr) finish_one(a, in, step, g1, g2, ftot, x_out, r);
 }
 
+// The standalone kernel: one thread per component (nine per residue, 32
+// residues per block), so that every array is read and written with
+// consecutive threads on consecutive elements; the residue's kinetic energy
+// is summed from shared memory in the same order as finish_one sums it.
+// Compiled for 4 blocks (36 warps) per SM.
+constexpr int kFinishRes = 32, kFinishThreads = 9 * kFinishRes;
 template <typename R>
-__global__ void k_finish(StepArgs<R> a, const Integrator *inp, const double *g1, const double *g2, double *ftot,
-                         double *x_out)
+__global__ void __launch_bounds__(kFinishThreads, 4) k_finish(StepArgs<R> a, const Integrator *inp, const double *g1,
+                                                          const double *g2, double *ftot, double *x_out)
 {
-  finish_pass(a, inp, g1, g2, ftot, x_out, grid_span());
+  __shared__ double kt[kFinishThreads];
+  __shared__ int on[kFinishRes];
+  const Integrator in = *inp;
+  const long long step = *a.step;
+  const int lr = threadIdx.x / 9, k = threadIdx.x - 9 * lr;
+  for (int r0 = blockIdx.x * kFinishRes; r0 < a.n_run; r0 += gridDim.x * kFinishRes) {
+    const int r = r0 + lr;
+    double t = 0.0;
+    const bool act = r < a.n_run && finish_comp(a, in, step, g1, g2, ftot, x_out, r, k, &t);
+    kt[threadIdx.x] = t;
+    if (k == 0) on[lr] = act;
+    __syncthreads();
+    if (threadIdx.x < kFinishRes && on[threadIdx.x])
+      a.e_res[(size_t) E_KIN * a.s.n_res + r0 + threadIdx.x] = kinetic(kt + 9 * threadIdx.x);
+    __syncthreads();
+  }
 }
 
 // Continuation of a run that stopped at step `*a.step` before its window's

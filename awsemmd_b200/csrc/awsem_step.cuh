@@ -211,7 +211,10 @@ template <typename R> __global__ void __launch_bounds__(kStepThreads, 2) k_step(
     ok = grid_sync(b, 3, seen[3], 1, pass_threads, ok, q.bar_wait_limit, q.hold, NoSerial{});
     if (ok) water_xi_pass(a, p, sp);
     ok = grid_sync(b, 4, seen[4], 1, pass_threads, ok, q.bar_wait_limit, q.hold, NoSerial{});
-    if (ok) pair_pass(a, p, sp);
+    if (ok) {
+      radial_pass(a, p, sp);
+      pair_pass(a, p, sp);
+    }
     ok = grid_sync(b, 5, seen[5], 1, pass_threads, ok, q.bar_wait_limit, q.hold, NoSerial{});
     if (ok) {
       hbond_pass(a, p, sp);

@@ -290,7 +290,7 @@ def algorithmic_bytes(kernel: str, info) -> float:
     """Bytes one launch must move at least (data layout of the engine):
     fragmem -- every stored memory distance once, the block table, the two
     target beads per residue and the force accumulators it updates;
-    pair / density / water_xi -- the residue pair array (8 bytes a pair)
+    radial / pair / density / water_xi -- the residue pair array (8 bytes a pair)
     once, every residue's working coordinates and per-residue scalars once,
     the force accumulators once."""
     n_res, n_atoms, records, rbytes, nd, pcap, npairs, nonuni = [int(v) for v in info]
@@ -298,7 +298,7 @@ def algorithmic_bytes(kernel: str, info) -> float:
     if kernel == "fragmem":
         return (records * 4 * rbytes + records * rbytes * nonuni + ((n_res + 31) // 32) * nd * 8 + n_res * 2 * bead
                 + n_res * 2 * 3 * 8 * 2)
-    if kernel in ("pair", "density", "water_xi"):
+    if kernel in ("radial", "pair", "density", "water_xi"):
         return npairs * 8 + n_res * 6 * bead + n_res * 10 * 8 + n_res * 4 * 4 + n_atoms * 3 * 8
     if kernel == "prepare":
         return n_atoms * 3 * 8 + n_res * 6 * bead + n_atoms * 3 * 8 + n_res * 32
@@ -318,7 +318,7 @@ TIMER_NAMES = ["Chain", "Shake", "Chi", "Rama", "Vexcluded", "DSSP", "PAP", "Wat
 TIMER_TO_KERNELS = {"Chain": "residue", "Chi": "residue", "Rama": "residue", "DSSP": "pair (detection) + hbond",
                     "PAP": "pair (detection) + hbond", "Frag_Mem": "fragmem", "Pair_Double_Loop1": "density",
                     "Pair_Single_Loop": "residue (switching, burial, helical pairs)", "Pair_Double_Loop2": "water_xi",
-                    "Pair_Double_Loop3": "pair", "Vexcluded": "pair + residue"}
+                    "Pair_Double_Loop3": "radial + pair (detection)", "Vexcluded": "pair + residue"}
 
 
 def read_timer_log(path: str) -> dict:
@@ -597,7 +597,7 @@ def config2_extra(dev: int, tmp: str, run_kw: dict, l2buf, peak: float) -> dict:
         info = s.model_info()
     t = sum(ms) / 1e3
     per_kernel = {}
-    for k in ("fragmem", "pair", "density", "water_xi", "prepare", "finish"):
+    for k in ("fragmem", "radial", "pair", "density", "water_xi", "prepare", "finish"):
         if prof.get(k, 0) > 0:
             b = algorithmic_bytes(k, info)
             per_kernel[k] = {"ms": round(prof[k], 5), "achieved_gbs": round(b / (prof[k] * 1e-3) / 1e9, 1),
@@ -789,7 +789,7 @@ def main():
     traffic = TRAFFIC_PER_ALGORITHMIC_BYTE[top] * abytes if top in TRAFFIC_PER_ALGORITHMIC_BYTE else None
     # per kernel: algorithmic bytes / CUDA-event time against the same peak
     per_kernel = {}
-    for k in ("fragmem", "pair", "density", "water_xi", "prepare", "finish"):
+    for k in ("fragmem", "radial", "pair", "density", "water_xi", "prepare", "finish"):
         if prof.get(k, 0) > 0:
             b = algorithmic_bytes(k, info)
             per_kernel[k] = {"ms": round(prof[k], 5), "algorithmic_bytes": b,
