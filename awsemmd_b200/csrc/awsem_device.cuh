@@ -108,6 +108,7 @@ template <typename R> struct DevSys {
   const double *aps;    // [12][n_res]
   const double *tables; // TB_SIZE
   const double4 *pos;            // [n_res][6] working coordinates (FP64 in both forms)
+  const double4 *cpos;           // [n_res] contact bead (CB, CA for glycine), a copy k_prepare writes
   unsigned long long *facc;      // [n_res*3][3] fixed-point forces
   ForceWindow win;               // residues whose forces the block sums in shared memory first
 };
@@ -125,6 +126,7 @@ template <typename R> __device__ __forceinline__ DevSys<double> widen(const DevS
   d.aps = s.aps;
   d.tables = s.tables;
   d.pos = s.pos;
+  d.cpos = s.cpos;
   d.facc = s.facc;
   d.win = s.win;
   return d;
@@ -289,8 +291,10 @@ template <typename R> __device__ R chi_term(const DevSys<R> &s, const FFParams &
 
 // calcDihedralAndSlopes, fix_backbone.cpp:2341-2453.  Slopes of the five
 // real atoms CA(i-1), CA(i), CA(i+1), O(i-1), O(i), y and x parts summed.
+// The angle is atan2(Y, X); it is returned as its cosine X / |(X, Y)| and
+// sine Y / |(X, Y)| (cos 0 = 1, sin 0 = 0 when X = Y = 0, as atan2(0, 0) = 0).
 template <typename R>
-__device__ void dihedral(const DevSys<R> &s, const FFParams &p, int i, int phi, R &angle, V3<R> sl[5])
+__device__ void dihedral(const DevSys<R> &s, const FFParams &p, int i, int phi, R &cang, R &sang, V3<R> sl[5])
 {
   V3<R> a, b, c;
   V3<double> ca = bead(s, i, B_CA), n = bead(s, i, B_N), cpv = bead(s, i, B_CP);
@@ -307,8 +311,16 @@ __device__ void dihedral(const DevSys<R> &s, const FFParams &p, int i, int phi, 
   V3<R> bxa = cross(b, a), cxa = cross(c, a), cxb = cross(c, b);
   R cdbxa = dot(c, bxa);
   R Y = bm * cdbxa, X = adb * bdc - b2 * adc;
-  angle = m_atan2(Y, X);
-  R inv = R(1) / (X * X + Y * Y);
+  const R h2 = X * X + Y * Y;
+  if (h2 > R(0)) {
+    const R h = m_sqrt(h2);
+    cang = X / h;
+    sang = Y / h;
+  } else {
+    cang = R(1);
+    sang = R(0);
+  }
+  R inv = R(1) / h2;
   R dy = X * inv, dx = -Y * inv;
   b2 *= dx;
   adb *= dx;
@@ -364,12 +376,15 @@ __device__ void dihedral(const DevSys<R> &s, const FFParams &p, int i, int phi, 
 }
 
 // compute_rama_potential + compute_rama_force, fix_backbone.cpp:2455-2546
+// cos(phi + phi0) and sin(phi + phi0) by the angle-sum identities from the
+// dihedral's own cosine and sine and the well's constant cos / sin phi0,
+// instead of an atan2 and four trigonometric calls per well.
 template <typename R> __device__ R rama_term(const DevSys<R> &s, const FFParams &p, int i)
 {
-  R phi, psi;
+  R cf, sf, cs, ss;
   V3<R> sphi[5], spsi[5];
-  dihedral(s, p, i, 1, phi, sphi);
-  dihedral(s, p, i, 0, psi, spsi);
+  dihedral(s, p, i, 1, cf, sf, sphi);
+  dihedral(s, p, i, 0, cs, ss, spsi);
   int j0 = 0, j1 = p.n_rama;
   if ((s.res_flags[i] & R_PRO) && (p.terms & T_RAMA_P)) {
     j0 = 6;
@@ -379,14 +394,15 @@ template <typename R> __device__ R rama_term(const DevSys<R> &s, const FFParams 
   for (int j = j0; j < j1; j++) {
     double aps = s.aps[(size_t) j * s.n_res + i];
     if (p.ssweight[j] && aps == 0.0) continue;
-    R cphi = m_cos(phi + R(p.phi0[j])) - R(1);
-    R cpsi = m_cos(psi + R(p.psi0[j])) - R(1);
+    const R c0 = R(p.cphi0[j]), s0 = R(p.sphi0[j]), c1 = R(p.cpsi0[j]), s1 = R(p.spsi0[j]);
+    R cphi = (cf * c0 - sf * s0) - R(1);
+    R cpsi = (cs * c1 - ss * s1) - R(1);
     R pc = R(p.phiw[j]) * cphi, sc = R(p.psiw[j]) * cpsi;
     R V = R(p.w[j]) * m_exp(-cphi * pc - cpsi * sc);
     if (p.ssweight[j]) V *= R(aps);
     R f = R(2) * V;
-    g0 += f * pc * m_sin(phi + R(p.phi0[j]));
-    g1 += f * sc * m_sin(psi + R(p.psi0[j]));
+    g0 += f * pc * (sf * c0 + cf * s0);
+    g1 += f * sc * (ss * c1 + cs * s1);
     E += -V;
   }
   if (g0 != R(0) || g1 != R(0)) {

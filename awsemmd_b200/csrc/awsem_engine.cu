@@ -140,9 +140,15 @@ class EngineBase {
 void fragmem_noalloc(int device, const FMView &v, const double *d_x, double *d_f, double *d_energy,
                      cudaStream_t stream);  // awsem_noalloc.cu
 
-static const char *kKernelNames[AWSEM_NKERNELS] = {"prepare",  "nl_decide", "nl_build", "density",
-                                                   "residue",  "water_xi",  "radial",   "pair",
-                                                   "hbond",    "fragmem",   "finish"};
+static const char *kKernelNames[AWSEM_NKERNELS] = {"prepare", "nl_decide", "nl_build", "density",
+                                                   "residue", "backbone",  "water_xi", "radial",
+                                                   "pair",    "hbond",     "fragmem",  "finish"};
+// the same kernels by index
+enum KernelIndex {
+  K_PREPARE, K_NL_DECIDE, K_NL_BUILD, K_DENSITY, K_RESIDUE, K_BACKBONE, K_WATER_XI, K_RADIAL, K_PAIR, K_HBOND,
+  K_FRAGMEM, K_FINISH
+};
+static_assert(K_FINISH + 1 == AWSEM_NKERNELS, "kernel index table");
 
 template <typename R> class Engine : public EngineBase {
 
@@ -151,7 +157,8 @@ template <typename R> class Engine : public EngineBase {
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   DBuf<int> res_type, res_flags, res_chain, chain_start, chain_end, atom_tag, atom_type;
   DBuf<double> aps, tables, x, v, mass, g1, g2, ftot, work, e_res, energy;
-  DBuf<double4> pos, cb_build;
+  DBuf<double4> pos, cpos, cb_build;
+  DBuf<dev::RadRec> rrec;
   DBuf<unsigned long long> facc;
   DBuf<int2> pairs, cpairs;  // residue pair list; the near list of an evaluation
   DBuf<int> seg_n;           // near pairs per near-list segment
@@ -230,6 +237,7 @@ template <typename R> class Engine : public EngineBase {
     a.s.aps = aps.p;
     a.s.tables = tables.p;
     a.s.pos = pos.p;
+    a.s.cpos = cpos.p;
     a.s.facc = facc.p;
     a.n_atoms = natoms();
     a.x = x.p;
@@ -248,6 +256,7 @@ template <typename R> class Engine : public EngineBase {
     a.xi1 = w + 7 * nn;
     a.xi2 = w + 8 * nn;
     a.bur = w + 9 * nn;
+    a.rrec = rrec.p;
     a.e_res = e_res.p;
     a.pairs = pairs.p;
     a.cpairs = cpairs.p;
@@ -392,6 +401,8 @@ template <typename R> class Engine : public EngineBase {
     e_res.alloc((size_t) E_SLOTS * nn);
     e_res.zero(s0);
     pos.alloc((size_t) dev::N_BEADS * nn);
+    cpos.alloc((size_t) nn);
+    rrec.alloc((size_t) nn);
     pos.zero(s0);  // residues of no replica keep finite (zero) working positions
     cb_build.alloc(nn);
     cb_build.zero(s0);
@@ -496,6 +507,30 @@ template <typename R> class Engine : public EngineBase {
       for (int b = 1; b <= t.ntypes; b++)
         if (t.ev_pref[a * N + b] != 0.0) evmax = std::max(evmax, std::max(t.ev_cl[a * N + b], t.ev_cs[a * N + b]));
     st.r_ev = (float) evmax;
+    // excluded-volume cutoffs by bead kind (CA, CB, O): over the atom types
+    // found at each position, or (serving handles, whose requests bring
+    // their own types) over every type
+    {
+      std::vector<std::vector<char>> at_pos(3, std::vector<char>(N, server ? 1 : 0));
+      if (!server)
+        for (size_t k = 0; k < t.atom_type.size(); k++) {
+          const int ty = t.atom_type[k];
+          if (ty >= 0 && ty < N) at_pos[k % 3][ty] = 1;
+        }
+      for (int b0 = 0; b0 < 3; b0++)
+        for (int b1 = 0; b1 < 3; b1++) {
+          double cs = 0.0, cl = 0.0;
+          for (int a = 1; a < N; a++)
+            for (int b = 1; b < N; b++)
+              if (at_pos[b0][a] && at_pos[b1][b] && t.ev_pref[a * N + b] != 0.0) {
+                cs = std::max(cs, t.ev_cs[a * N + b]);
+                cl = std::max(cl, t.ev_cl[a * N + b]);
+              }
+          // rounded up so that the float bound never falls below the cutoff
+          st.ev_cutk[0][b0][b1] = cs > 0.0 ? std::nextafter((float) cs, 1e30f) : 0.f;
+          st.ev_cutk[1][b0][b1] = cl > 0.0 ? std::nextafter((float) cl, 1e30f) : 0.f;
+        }
+    }
     st.skin = (float) skin;
     // LAMMPS defaults: neigh_modify delay 0 every 1 check yes
     st.lst_skin = skin;
@@ -641,10 +676,16 @@ template <typename R> class Engine : public EngineBase {
     // the emulated lists' decision for this step, before anything reads it
     if (lists_emulated())
       dev::k_list_decide<<<(n_sys() + 127) / 128, 128, 0, s0>>>(nl.p, n_sys(), lst_ago.p, lst_over.p, lst_build.p);
-    if (fm || fmt || go || px || rx) {
-      // fragment memory is independent of the pair passes: second stream
+    // the backbone terms (chain, chi, rama; one kernel of the residue pass)
+    // need only the positions; the recording pass of awsem_debug_selections
+    // runs the whole residue pass instead
+    const bool bb = !a.sel;
+    if (fm || fmt || go || px || rx || bb) {
+      // fragment memory and the backbone terms are independent of the pair
+      // passes: second stream
       CK(cudaEventRecord(ev_fork, s0));
       CK(cudaStreamWaitEvent(s1, ev_fork, 0));
+      if (bb) dev::k_backbone<R><<<nb, tb, 0, s1>>>(a, p);
       if (fm) dev::k_fragmem<R><<<fm_blocks(), tb, fm_smem(), s1>>>(a, p);
       if (fmt) dev::k_fm_table<R><<<fm_table_blocks(), tb, 0, s1>>>(a, p);
       if (go) dev::k_amh_go<R><<<nb, tb, 0, s1>>>(a, p);
@@ -667,7 +708,7 @@ template <typename R> class Engine : public EngineBase {
       dev::k_pair<R><<<pair_blocks, tb, 0, s0>>>(a, p);
       dev::k_hbond<R><<<hb_blocks, 128, 0, s0>>>(a, p);
     }
-    if (fm || fmt || go || px || rx) CK(cudaStreamWaitEvent(s0, ev_join, 0));
+    if (fm || fmt || go || px || rx || bb) CK(cudaStreamWaitEvent(s0, ev_join, 0));
   }
 
   int finish_blocks() const { return (n_run() + dev::kFinishRes - 1) / dev::kFinishRes; }
@@ -1130,7 +1171,7 @@ template <typename R> class Engine : public EngineBase {
       for (int d : {1, 2, 3, 6, nd}) {
         if (d > nd) continue;
         fm_dsplit = d;
-        const double t = time_of({8});
+        const double t = time_of({K_FRAGMEM});
         if (t < tbest) tbest = t, best = d;
       }
       fm_dsplit = best;
@@ -1146,8 +1187,8 @@ template <typename R> class Engine : public EngineBase {
       }
       blocks = best;
     };
-    tune_blocks(pair_blocks, {3, 5, 6});
-    tune_blocks(hb_blocks, {7});
+    tune_blocks(pair_blocks, {K_DENSITY, K_WATER_XI, K_RADIAL, K_PAIR});
+    tune_blocks(hb_blocks, {K_HBOND});
     // fragment-memory grid with the pair-pass grid, judged together on whole
     // steps: fragment memory (HBM-bound, second stream) can only overlap the
     // latency-bound pair passes when their grids leave it room on the SMs
@@ -1229,23 +1270,24 @@ template <typename R> class Engine : public EngineBase {
       for (int k = 0; k < AWSEM_NKERNELS; k++) {
         CK(cudaEventRecord(ev[2 * k], s0));
         switch (k) {
-          case 0: dev::k_prepare<R><<<nb, tb, 0, s0>>>(a, p); break;
-          case 1: dev::k_nl_decide<<<1, 1, 0, s0>>>(nl.p, 0, dstep.p); break;
-          case 2: launch_list_build(a, s0); break;
-          case 3: dev::k_density<R><<<pair_blocks, tb, 0, s0>>>(a, p); break;
-          case 4: dev::k_residue<R><<<nb, tb, 0, s0>>>(a, p); break;
-          case 5: dev::k_water_xi<R><<<pair_blocks, tb, 0, s0>>>(a, p); break;
-          case 6: dev::k_radial<R><<<pair_blocks, tb, 0, s0>>>(a, p); break;
-          case 7: dev::k_pair<R><<<pair_blocks, tb, 0, s0>>>(a, p); break;
-          case 8: dev::k_hbond<R><<<hb_blocks, 128, 0, s0>>>(a, p); break;
-          case 9:
+          case K_PREPARE: dev::k_prepare<R><<<nb, tb, 0, s0>>>(a, p); break;
+          case K_NL_DECIDE: dev::k_nl_decide<<<1, 1, 0, s0>>>(nl.p, 0, dstep.p); break;
+          case K_NL_BUILD: launch_list_build(a, s0); break;
+          case K_DENSITY: dev::k_density<R><<<pair_blocks, tb, 0, s0>>>(a, p); break;
+          case K_RESIDUE: dev::k_residue<R><<<nb, tb, 0, s0>>>(a, p); break;
+          case K_BACKBONE: dev::k_backbone<R><<<nb, tb, 0, s0>>>(a, p); break;
+          case K_WATER_XI: dev::k_water_xi<R><<<pair_blocks, tb, 0, s0>>>(a, p); break;
+          case K_RADIAL: dev::k_radial<R><<<pair_blocks, tb, 0, s0>>>(a, p); break;
+          case K_PAIR: dev::k_pair<R><<<pair_blocks, tb, 0, s0>>>(a, p); break;
+          case K_HBOND: dev::k_hbond<R><<<hb_blocks, 128, 0, s0>>>(a, p); break;
+          case K_FRAGMEM:
             if (fm) dev::k_fragmem<R><<<fm_blocks(), tb, fm_smem(), s0>>>(a, p);
             if (p.terms & T_FM_TABLE) dev::k_fm_table<R><<<fm_table_blocks(), tb, 0, s0>>>(a, p);
             if (p.terms & T_AMHGO) dev::k_amh_go<R><<<nb, tb, 0, s0>>>(a, p);
             if (p.terms & (T_SSB | T_DH | T_CONTREST)) dev::k_pair_extra<R><<<pair_blocks, tb, 0, s0>>>(a, p);
             if (p.terms & (T_SHAKE | T_MEMB | T_VFM)) dev::k_residue_extra<R><<<nb, tb, 0, s0>>>(a, p);
             break;
-          case 10: dev::k_finish<R><<<finish_blocks(), dev::kFinishThreads, 0, s0>>>(a, d_integ.p, g1.p, g2.p, ftot.p, x.p); break;
+          case K_FINISH: dev::k_finish<R><<<finish_blocks(), dev::kFinishThreads, 0, s0>>>(a, d_integ.p, g1.p, g2.p, ftot.p, x.p); break;
         }
         CK(cudaEventRecord(ev[2 * k + 1], s0));
       }
@@ -2039,7 +2081,7 @@ template <typename R> class Engine : public EngineBase {
     auto add = [&](const auto &buf) { b += (long long) (buf.n * sizeof(*buf.p)); };
     add(res_type), add(res_flags), add(res_chain), add(chain_start), add(chain_end), add(atom_tag), add(atom_type);
     add(aps), add(tables), add(x), add(v), add(mass), add(g1), add(g2), add(ftot), add(work), add(e_res), add(energy);
-    add(pos), add(cb_build), add(facc), add(pairs), add(ncount), add(hbq), add(dacc), add(e_fix), add(nl), add(dstep);
+    add(pos), add(cpos), add(rrec), add(cb_build), add(facc), add(pairs), add(ncount), add(hbq), add(dacc), add(e_fix), add(nl), add(dstep);
     add(ev_pref), add(ev_cs), add(ev_cl), add(excl_self), add(excl_next), add(bond_i), add(bond_j), add(bond_k);
     add(bond_r0), add(fm_soff), add(fm_slen), add(fm_rf), add(fm_coef), add(tb_data), add(tb_present);
     add(go_start), add(go_partner), add(go_rnat), add(go_gamma), add(go_sig_sq), add(go_norm);

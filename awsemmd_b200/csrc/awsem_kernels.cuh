@@ -43,10 +43,16 @@ struct NLState {
   float skin;
   float r_contact, r_dssp, r_pap, r_ev;  // term cutoffs on the bead pairs they test
   float bCAx;         // max distance of a residue's CB or O from its own CA (this step)
+  float bCBx, bOx;    // the same for CB and for O alone (this step, reduced by k_prepare)
   float ev_pre_sq;    // CA-CA distance^2 beyond which no bead pair of two residues is in excluded-volume range
+  // Excluded volume by bead kind (0 CA, 1 CB, 2 O): the largest cutoff of
+  // any type pair found at those positions (short range [0], long range
+  // [1]; 0 when no such pair interacts; set by the host), and this step's
+  // reach of each kind from its residue's CA (0 for CA itself).
+  float ev_cutk[2][3][3];
+  float ev_reach[3];
   float bNCA;         // max distance of a residue's virtual N from its own CA (this step)
   float dssp_pre_sq;  // CA-CA distance^2 beyond which neither O-N pair of two residues is within the DSSP cutoff
-  int n_dssp, n_pap;  // hydrogen-bond queue lengths of the current evaluation
   int npairs;         // pairs in the residue pair list (may exceed its capacity: overflow)
   int fm_timeout;     // a fragment-memory stream wait gave up (results invalid)
   int tb_error;       // table fragment memory: 1 a distance outside the table's range, 2 a grid index outside it
@@ -71,7 +77,13 @@ struct NLState {
   // their count.  No shared counter: every warp owns its range.
   int seg_len;        // pairs per segment (a multiple of 32)
   int nseg;           // segments
-  int fm_next;        // fragment-memory work units handed out (k_fragmem), zeroed by the list decision
+  // Counters updated with atomics during a pass, each on its own cache line:
+  // reads of a line that other threads are updating atomically wait for
+  // those atomics
+  alignas(128) int n_dssp;  // hydrogen-bond queue lengths of the current evaluation
+  alignas(128) int n_pap;
+  alignas(128) int fm_next;  // fragment-memory work units handed out (k_fragmem), zeroed by the list decision
+  alignas(128) int end_pad;
 };
 
 // Run window of one replica: integrated over steps begin..end (the
@@ -80,6 +92,14 @@ struct NLState {
 struct SlotRun {
   long long begin, end, step0;
   double t_start, t_stop;
+};
+
+// What the radial pass reads of a residue, packed into one 64-byte record
+// (written by the residue pass): three cache lines per residue of a pair
+// (this record, the contact bead, the water-xi sum) instead of ten arrays.
+struct __align__(64) RadRec {
+  double sw, bur, x1, x2, sigp;  // sigma_water, burial coefficient, helix xi1, xi2 of residue r - helix_i_diff, sigma_water'
+  int type, flags, chain, pad;
 };
 
 template <typename R> struct StepArgs {
@@ -92,6 +112,7 @@ template <typename R> struct StepArgs {
   const int *atom_tag;
   // per-residue pair-pass intermediates
   double *rho_w, *rho_h, *sig_w, *sigp_w, *sig_h, *sigp_h, *xi_w, *xi1, *xi2, *bur;
+  RadRec *rrec;  // [n_res]
   double *e_res;  // [E_SLOTS][n_res]
   // residue pair list: pairs (i, j), i < j, capacity pcap; per-residue counts.
   // cpairs: the near list of this evaluation (the listed pairs whose contact
@@ -188,7 +209,11 @@ __device__ __forceinline__ void atomic_max_f(float *addr, float v)
 
 template <typename R> __device__ __forceinline__ void prepare_pass(const StepArgs<R> &a, const FFParams &p, Span sp)
 {
-  float d2 = 0.f, oO = 0.f, oN = 0.f, oCA = 0.f, oAll = 0.f, oX = 0.f, oNCA = 0.f, dl = 0.f;
+  float d2 = 0.f, dl = 0.f;
+  // squared bead offsets, maximised over this thread's residues; the square
+  // root of the maximum is the maximum of the square roots (both roundings
+  // are monotonic), so one root per thread gives the same maxima
+  double qO = 0.0, qN = 0.0, qCA = 0.0, qAll = 0.0, qB = 0.0, qX = 0.0, qNCA = 0.0;
   const int lane = threadIdx.x & 31;
   // warp-uniform trip count: the maxima are reduced across the warp below
   for (int r0 = sp.t - lane; r0 < a.n_run; r0 += sp.nthr) {
@@ -247,30 +272,38 @@ template <typename R> __device__ __forceinline__ void prepare_pass(const StepArg
     w[B_H] = make_double4(h[0], h[1], h[2], 0.0);
     w[B_CP] = make_double4(cp[0], cp[1], cp[2], 0.0);
     {
+      const double *cc = (fl & R_GLY) ? ca : cb;
+      const_cast<double4 *>(a.s.cpos)[r] = make_double4(cc[0], cc[1], cc[2], 0.0);
+    }
+    {
       // reach of the residue's beads around its CA (excluded-volume prefilter)
       double ux = cb[0] - ca[0], uy = cb[1] - ca[1], uz = cb[2] - ca[2];
       double wx = o[0] - ca[0], wy = o[1] - ca[1], wz = o[2] - ca[2];
-      oX = fmaxf(oX, (float) sqrt(fmax(ux * ux + uy * uy + uz * uz, wx * wx + wy * wy + wz * wz)));
+      qB = fmax(qB, ux * ux + uy * uy + uz * uz);
+      qX = fmax(qX, wx * wx + wy * wy + wz * wz);
     }
     // list-validity data: contact-bead displacement and bead offsets
     const double *c = (fl & R_GLY) ? ca : cb;
     double4 b0 = a.cb_build[r];
     double dx = c[0] - b0.x, dy = c[1] - b0.y, dz = c[2] - b0.z;
     d2 = fmaxf(d2, (float) (dx * dx + dy * dy + dz * dz));
-    auto off = [&](const double *q) {
+    auto off2 = [&](const double *q) {
       double ex = q[0] - c[0], ey = q[1] - c[1], ez = q[2] - c[2];
-      return (float) sqrt(ex * ex + ey * ey + ez * ez);
+      return ex * ex + ey * ey + ez * ez;
     };
-    oO = fmaxf(oO, off(o));
-    oCA = fmaxf(oCA, off(ca));
-    oAll = fmaxf(oAll, fmaxf(fmaxf(off(ca), off(cb)), off(o)));
+    const double o_o = off2(o), o_ca = off2(ca);
+    qO = fmax(qO, o_o);
+    qCA = fmax(qCA, o_ca);
+    qAll = fmax(qAll, fmax(fmax(o_ca, off2(cb)), o_o));
     if (!(fl & R_FIRST)) {
-      oN = fmaxf(oN, off(n));
+      qN = fmax(qN, off2(n));
       const double ex = n[0] - ca[0], ey = n[1] - ca[1], ez = n[2] - ca[2];
-      oNCA = fmaxf(oNCA, (float) sqrt(ex * ex + ey * ey + ez * ez));
+      qNCA = fmax(qNCA, ex * ex + ey * ey + ez * ez);
     }
   }
   }
+  float oO = (float) sqrt(qO), oN = (float) sqrt(qN), oCA = (float) sqrt(qCA), oAll = (float) sqrt(qAll);
+  float oB = (float) sqrt(qB), oX = (float) sqrt(qX), oNCA = (float) sqrt(qNCA);
   // warp max, block max, then one atomic per block and quantity (every
   // thread of the block calls this pass)
   for (int s = 16; s > 0; s >>= 1) {
@@ -279,23 +312,25 @@ template <typename R> __device__ __forceinline__ void prepare_pass(const StepArg
     oN = fmaxf(oN, __shfl_xor_sync(0xffffffffu, oN, s));
     oCA = fmaxf(oCA, __shfl_xor_sync(0xffffffffu, oCA, s));
     oAll = fmaxf(oAll, __shfl_xor_sync(0xffffffffu, oAll, s));
+    oB = fmaxf(oB, __shfl_xor_sync(0xffffffffu, oB, s));
     oX = fmaxf(oX, __shfl_xor_sync(0xffffffffu, oX, s));
     oNCA = fmaxf(oNCA, __shfl_xor_sync(0xffffffffu, oNCA, s));
     dl = fmaxf(dl, __shfl_xor_sync(0xffffffffu, dl, s));
   }
-  __shared__ float red[8][32];
+  __shared__ float red[9][32];
   if (lane == 0) {
     const int w = threadIdx.x >> 5;
     red[0][w] = d2, red[1][w] = oO, red[2][w] = oN, red[3][w] = oCA, red[4][w] = oAll, red[5][w] = oX;
-    red[6][w] = oNCA, red[7][w] = dl;
+    red[6][w] = oNCA, red[7][w] = dl, red[8][w] = oB;
   }
   __syncthreads();
-  if (threadIdx.x < 8) {
+  if (threadIdx.x < 9) {
     const int k = threadIdx.x;
     float m = 0.f;
     for (int w = 0; w < (int) (blockDim.x >> 5); w++) m = fmaxf(m, red[k][w]);
     float *dst = k == 0 ? &a.nl->d2max : k == 1 ? &a.nl->bO : k == 2 ? &a.nl->bN : k == 3 ? &a.nl->bCA
-               : k == 4 ? &a.nl->bAll : k == 5 ? &a.nl->bCAx : k == 6 ? &a.nl->bNCA : &a.nl->lst_d2max;
+               : k == 4 ? &a.nl->bAll : k == 5 ? &a.nl->bOx : k == 6 ? &a.nl->bNCA : k == 7 ? &a.nl->lst_d2max
+               : &a.nl->bCBx;
     if (m > 0.f) atomic_max_f(dst, m);  // the maxima start each step at 0
   }
 }
@@ -329,14 +364,25 @@ __device__ __forceinline__ void nl_decide(NLState *nl, int force, long long *ste
   s.rebuild = rb;
   s.need = need;
   s.fm_next = 0;
-  // two residues whose CAs are farther apart than r_ev + 2 * reach have no
-  // bead pair inside any excluded-volume cutoff (0.01 A covers rounding)
-  float pre = s.r_ev + 2.f * s.bCAx + 0.01f;
+  s.bCAx = fmaxf(s.bCBx, s.bOx);
+  // |b(i) - b'(j)| >= |CA(i) - CA(j)| - reach(b) - reach(b'): two residues
+  // whose CAs are farther apart than the largest cutoff + reaches of any
+  // interacting bead kinds have no bead pair in excluded-volume range
+  // (0.01 A covers rounding)
+  s.ev_reach[0] = 0.f;
+  s.ev_reach[1] = s.bCBx;
+  s.ev_reach[2] = s.bOx;
+  float pre = 0.f;
+  for (int r = 0; r < 2; r++)
+    for (int b0 = 0; b0 < 3; b0++)
+      for (int b1 = 0; b1 < 3; b1++)
+        if (s.ev_cutk[r][b0][b1] > 0.f) pre = fmaxf(pre, s.ev_cutk[r][b0][b1] + s.ev_reach[b0] + s.ev_reach[b1]);
+  pre += 0.01f;
   s.ev_pre_sq = pre * pre;
   // |O(i) - N(j)| >= |CA(i) - CA(j)| - |O(i) - CA(i)| - |N(j) - CA(j)|, and bCAx bounds |O - CA|
   const float dpre = s.r_dssp + s.bCAx + s.bNCA + 0.01f;
   s.dssp_pre_sq = dpre * dpre;
-  s.d2max = s.bO = s.bN = s.bCA = s.bAll = s.bCAx = s.bNCA = 0.f;
+  s.d2max = s.bO = s.bN = s.bCA = s.bAll = s.bCBx = s.bOx = s.bNCA = 0.f;
   s.n_dssp = s.n_pap = 0;
   s.lst_setup = s.lst_force;
   s.lst_force = 0;
@@ -345,9 +391,11 @@ __device__ __forceinline__ void nl_decide(NLState *nl, int force, long long *ste
 
 __global__ void k_nl_decide(NLState *nl, int force, long long *step) { nl_decide(nl, force, step); }
 
+// contact bead of residue r (one load, no dependence on the residue's flags)
 template <typename R> __device__ __forceinline__ V3<double> contact(const DevSys<R> &s, int r)
 {
-  return bead(s, r, (s.res_flags[r] & R_GLY) ? B_CA : B_CB);
+  const double4 q = s.cpos[r];
+  return {q.x, q.y, q.z};
 }
 
 // Cell grids for large replicas (more than kGridMin residues): each such
@@ -698,17 +746,20 @@ __device__ __forceinline__ R ev_pair(const StepArgs<R> &a, int ta, int tb, bool 
 }
 
 // bond_style harmonic, the bonds whose first atom is in residue r (run by
-// k_residue's thread of that residue)
-template <typename R> __device__ __forceinline__ void bonds_of(const StepArgs<R> &a, const DevSys<R> &s, int r)
+// k_residue's thread of that residue).  FP64 in both forms: a bond's energy
+// k (r - r0)^2 is a small difference near equilibrium, and FP32 geometry put
+// the bond energy of configuration 3 at 5e-6 relative.
+template <typename R, typename Q>
+__device__ __forceinline__ void bonds_of(const StepArgs<R> &a, const DevSys<Q> &s, int r)
 {
   double e = 0.0;
   for (int b = r * a.bond_cap; b < (r + 1) * a.bond_cap && a.bond_i[b] >= 0; b++) {
     int ai = a.bond_i[b], aj = a.bond_j[b];
-    V3<R> d = diff<R>(bead(s, ai / 3, ai % 3), bead(s, aj / 3, aj % 3));
-    R rr = m_sqrt(norm2(d));
-    R dr = rr - R(a.bond_r0[b]);
-    R rk = R(a.bond_k[b]) * dr;
-    R fb = rr > R(0) ? R(-2) * rk / rr : R(0);
+    V3<Q> d = diff<Q>(bead(s, ai / 3, ai % 3), bead(s, aj / 3, aj % 3));
+    Q rr = m_sqrt(norm2(d));
+    Q dr = rr - Q(a.bond_r0[b]);
+    Q rk = Q(a.bond_k[b]) * dr;
+    Q fb = rr > Q(0) ? Q(-2) * rk / rr : Q(0);
     e = __dadd_rn(e, (double) mul_rn(rk, dr));
     scatter(s, ai / 3, ai % 3, d.x * fb, d.y * fb, d.z * fb);
     scatter(s, aj / 3, aj % 3, -d.x * fb, -d.y * fb, -d.z * fb);
@@ -716,8 +767,15 @@ template <typename R> __device__ __forceinline__ void bonds_of(const StepArgs<R>
   a.e_res[(size_t) E_BOND * s.n_res + r] = e;
 }
 
+// Parts of the per-residue pass: the density-dependent terms (switching,
+// burial, helical pair), the excluded volume inside the residue and the
+// bonds (RES_SL), and the backbone terms chain, chi and rama (RES_BB), which
+// need only the positions and run as their own kernel beside the pair
+// passes.
+constexpr int RES_SL = 1, RES_BB = 2, RES_ALL = 3;
+
 // SL and the per-residue backbone terms
-template <typename R, bool SEL = false>
+template <typename R, bool SEL = false, int PART = RES_ALL>
 __device__ __forceinline__ void residue_one(const StepArgs<R> &a, const FFParams &p, int i, ForceWindow win = {})
 {
   DevSys<R> s = a.s;
@@ -729,6 +787,7 @@ __device__ __forceinline__ void residue_one(const StepArgs<R> &a, const FFParams
   int n = s.n_res, fl = s.res_flags[i];
   double *E = a.e_res;
   const bool fix = a.groups & G_FIX;
+  if constexpr (PART & RES_SL) {
   bool water = fix && (p.terms & T_WATER), helix = fix && (p.terms & T_HELIX);
   double sw = 0, swp = 0, sh = 0, shp = 0;
   const double rw = density(a, 0, i), rh = density(a, 1, i);
@@ -773,7 +832,24 @@ __device__ __forceinline__ void residue_one(const StepArgs<R> &a, const FFParams
   }
   a.xi1[i] = x1;
   a.xi2[i] = x2;
+  {
+    RadRec &rr = a.rrec[i];
+    rr.sw = sw;
+    rr.bur = bc;
+    rr.x1 = x1;
+    rr.sigp = swp;
+    rr.type = s.res_type[i];
+    rr.flags = fl;
+    rr.chain = s.res_chain[i];
+    // xi2 is read at residue r + helix_i_diff: stored with that residue's
+    // record; a record whose residue r - helix_i_diff is not integrated (no
+    // residue, or a free residue of a serving handle) holds 0
+    if (i + p.helix_i_diff < n) a.rrec[i + p.helix_i_diff].x2 = x2;
+    if (i < p.helix_i_diff || a.res_sys[i - p.helix_i_diff] < 0) rr.x2 = 0.0;
+  }
   E[(size_t) E_HELIX * n + i] = eh;
+  }
+  if constexpr (PART & RES_BB) {
   double ec = 0.0, ex = 0.0, er = 0.0;
   if (fix && (p.terms & T_CHAIN)) ec = (double) chain_term(sd, p, i);
   bool inner = fix && !(fl & (R_FIRST | R_LAST | R_GLY));
@@ -782,6 +858,8 @@ __device__ __forceinline__ void residue_one(const StepArgs<R> &a, const FFParams
   E[(size_t) E_CHAIN * n + i] = ec;
   E[(size_t) E_CHI * n + i] = ex;
   E[(size_t) E_RAMA * n + i] = er;
+  }
+  if constexpr (PART & RES_SL) {
   // excluded volume inside the residue (1-3 pairs; 1-2 pairs are excluded)
   double ev = 0.0;
   unsigned ex_self = (a.groups & G_PAIR) ? a.excl_self[i] : 0x1ffu;
@@ -800,7 +878,8 @@ __device__ __forceinline__ void residue_one(const StepArgs<R> &a, const FFParams
       }
     }
   E[(size_t) E_PAIR * n + i] = ev;
-  if (a.groups & G_BOND) bonds_of(a, s, i);
+  if (a.groups & G_BOND) bonds_of(a, sd, i);
+  }
 }
 
 template <typename R, bool SEL = false> __device__ __forceinline__ void residue_pass(const StepArgs<R> &a, const FFParams &p, Span sp)
@@ -816,7 +895,7 @@ template <typename R, bool SEL = false> __device__ __forceinline__ void residue_
 // to fixed point before it is summed, so the result is the direct scatter's
 // bit for bit.
 constexpr int kResBlock = 128, kResHalo = 5, kResWin = kResBlock + kResHalo;
-template <typename R, bool SEL> __device__ __forceinline__ void residue_pass_window(const StepArgs<R> &a, const FFParams &p)
+template <typename R, bool SEL, int PART> __device__ __forceinline__ void residue_pass_window(const StepArgs<R> &a, const FFParams &p)
 {
   __shared__ unsigned long long acc[kResWin * 9];
   const uint32_t addr = (uint32_t) __cvta_generic_to_shared(acc);
@@ -824,7 +903,7 @@ template <typename R, bool SEL> __device__ __forceinline__ void residue_pass_win
     for (int k = threadIdx.x; k < kResWin * 9; k += kResBlock) acc[k] = 0ull;
     __syncthreads();
     const int i = r0 + threadIdx.x;
-    if (i < a.n_run && a.res_sys[i] >= 0) residue_one<R, SEL>(a, p, i, ForceWindow{addr, r0 - 1, kResWin});
+    if (i < a.n_run && a.res_sys[i] >= 0) residue_one<R, SEL, PART>(a, p, i, ForceWindow{addr, r0 - 1, kResWin});
     __syncthreads();
     for (int k = threadIdx.x; k < kResWin * 9; k += kResBlock) {
       const unsigned long long v = acc[k];
@@ -836,11 +915,15 @@ template <typename R, bool SEL> __device__ __forceinline__ void residue_pass_win
 }
 template <typename R> __global__ void __launch_bounds__(kResBlock, 4) k_residue(StepArgs<R> a, FFParams p)
 {
-  residue_pass_window<R, false>(a, p);
+  residue_pass_window<R, false, RES_SL>(a, p);
+}
+template <typename R> __global__ void __launch_bounds__(kResBlock, 4) k_backbone(StepArgs<R> a, FFParams p)
+{
+  residue_pass_window<R, false, RES_BB>(a, p);
 }
 template <typename R> __global__ void __launch_bounds__(kResBlock) k_residue_sel(StepArgs<R> a, FFParams p)
 {
-  residue_pass_window<R, true>(a, p);
+  residue_pass_window<R, true, RES_ALL>(a, p);
 }
 
 // DL2: water-mediated density derivative coefficients (fix_backbone.cpp:
@@ -917,14 +1000,14 @@ template <typename R, bool SEL = false> __device__ __forceinline__ void radial_p
     const int i = ij.x, j = ij.y;
     // every per-residue input of the pair, loaded up front and without
     // conditions, so that the gathers are in flight together
-    const int fli = s.res_flags[i], flj = s.res_flags[j];
-    const bool other = s.res_chain[j] != s.res_chain[i];
-    const int ti = s.res_type[i], tj = s.res_type[j];
-    const V3<double> c_i = bead(s, i, (fli & R_GLY) ? B_CA : B_CB), c_j = bead(s, j, (flj & R_GLY) ? B_CA : B_CB);
-    const double sw_i = a.sig_w[i], sw_j = a.sig_w[j], bur_i = a.bur[i], bur_j = a.bur[j];
-    const double xi_i = water_xi(a, i), xi_j = water_xi(a, j);
-    const double x1_i = a.xi1[i], x1_j = a.xi1[j];
-    const double x2_i = a.xi2[max(i - dh, 0)], x2_j = a.xi2[max(j - dh, 0)];
+    const RadRec ri = a.rrec[i], rj = a.rrec[j];
+    const V3<double> c_i = contact(s, i), c_j = contact(s, j);
+    const double ui = (double) a.dacc[(size_t) 2 * n + i], uj = (double) a.dacc[(size_t) 2 * n + j];
+    const int fli = ri.flags, flj = rj.flags, ti = ri.type, tj = rj.type;
+    const bool other = rj.chain != ri.chain;
+    const double sw_i = ri.sw, sw_j = rj.sw, bur_i = ri.bur, bur_j = rj.bur;
+    const double xi_i = ui * D_UNSCALE * ri.sigp, xi_j = uj * D_UNSCALE * rj.sigp;  // water_xi
+    const double x1_i = ri.x1, x1_j = rj.x1, x2_i = ri.x2, x2_j = rj.x2;
     const int dij = j - i;
     // contact-bead radial terms
     if (other || dij > 1) {
@@ -1045,42 +1128,23 @@ template <typename R, bool SEL = false> __device__ __forceinline__ void pair_pas
     __syncwarp();
     cnt -= count;
   };
-  // excluded volume between the beads of listed pair q (1-2 bonded pairs removed)
-  auto ev_of_pair = [&](int q) {
-    const int2 ij = a.cpairs[q];
-    const int i = ij.x, j = ij.y;
-    const bool other = s.res_chain[j] != s.res_chain[i];
-    const int dij = j - i;
-    const unsigned excl = j == i + 1 ? a.excl_next[i] : 0u;
-    const bool shortr = !other && dij < 5;
-    double ee = 0.0;
-    // bead b of a residue: CA, CB, O for b = 0, 1, 2; each bead pair's force
-    // is scattered as it is found (few pairs come this close, and keeping
-    // nine sums live would cost the whole pass registers)
-#pragma unroll 1
-    for (int b1 = 0; b1 < 3; b1++) {
-      const V3<double> bj = bead(s, j, b1);
-      const int tb = a.atom_type[3 * j + b1];
-#pragma unroll 1
-      for (int b0 = 0; b0 < 3; b0++) {
-        if (excl & (1u << (b0 * 3 + b1))) continue;
-        const V3<R> dd = diff<R>(bead(s, i, b0), bj);
-        if (norm2(dd) > ev_max_sq) continue;  // beyond every cutoff: no table lookups
-        V3<R> f;
-        bool hit = false;
-        const R e = ev_pair(a, a.atom_type[3 * i + b0], tb, shortr, dd, f, SEL ? &hit : nullptr);
-        if (hit) sel_rec<SEL>(a, AWSEM_SEL_EV, 3 * b0 + b1, i, j);
-        if (e == R(0) && f.x == R(0) && f.y == R(0) && f.z == R(0)) continue;
-        ee += (double) e;
-        const long long v[3] = {fix_force((double) f.x), fix_force((double) f.y), fix_force((double) f.z)};
-        const long long w[3] = {-v[0], -v[1], -v[2]};
-        scatter_fix(s, i, b0, v);
-        scatter_fix(s, j, b1, w);
-      }
-    }
-    if (ee != 0.0) atomicAdd(e_ev + i, (unsigned long long) fix_force(ee));
-  };
-  // run the first `count` staged EV pairs (count <= 32), one per lane; move the rest down
+  // Excluded volume between the beads of the staged pairs, in two steps.
+  // First a lane per pair: which of its nine bead pairs (bead kinds CA, CB,
+  // O = 0, 1, 2) can be in range -- not excluded (1-2 bonded pairs), a
+  // type pair that interacts at those kinds, and |CA(i) - CA(j)| at most
+  // the kinds' cutoff plus their reach from the CA.  Then a lane per
+  // surviving bead pair, 32 at a time, so that the bead loads of a batch
+  // are independent of one another.  Each bead pair's force and energy go
+  // to fixed point and are added as they are found.
+  // this step's bead-kind cutoffs (lanes 0-17: [short / long][b0][b1]) and
+  // reaches (lanes 18-20), read once: the list state shares cache lines with
+  // the queue counters this pass updates atomically, and reads of those
+  // lines during the pass wait for the atomics
+  const float tab = lane < 18 ? (&a.nl->ev_cutk[0][0][0])[lane] : lane < 21 ? a.nl->ev_reach[lane - 18] : 0.f;
+  __shared__ int ev_item[kStageWarps][9 * 32];
+  __shared__ int ev_pi[kStageWarps][32], ev_pj[kStageWarps][32];
+  int *const items = ev_item[threadIdx.x >> 5], *const pi = ev_pi[threadIdx.x >> 5], *const pj = ev_pj[threadIdx.x >> 5];
+  // run the first `count` staged EV pairs (count <= 32); move the rest down
   auto ev_batch = [&](int count) {
     const int q = lane < count ? se[lane] : -1;
     const int v1 = lane + 32 < nse ? se[lane + 32] : 0;
@@ -1088,7 +1152,61 @@ template <typename R, bool SEL = false> __device__ __forceinline__ void pair_pas
     se[lane] = v1;
     __syncwarp();
     nse -= count;
-    if (q >= 0) ev_of_pair(q);
+    unsigned mask = 0u;  // bead pairs c = 3 b0 + b1 that may be in range
+    int i = 0, j = 0, sh = 9;
+    float dca = 0.f;
+    if (q >= 0) {
+      const int2 ij = a.cpairs[q];
+      i = ij.x, j = ij.y;
+      const bool shortr = s.res_chain[j] == s.res_chain[i] && j - i < 5;
+      sh = shortr ? 0 : 9;
+      const unsigned excl = j == i + 1 ? a.excl_next[i] : 0u;
+      dca = sqrtf((float) norm2(diff<R>(bead(s, i, B_CA), bead(s, j, B_CA))));
+      mask = ~excl & 0x1ffu;
+    }
+#pragma unroll
+    for (int c = 0; c < 9; c++) {
+      const float ck = __shfl_sync(0xffffffffu, tab, sh + c);
+      const float r0 = __shfl_sync(0xffffffffu, tab, 18 + c / 3), r1 = __shfl_sync(0xffffffffu, tab, 18 + c % 3);
+      if (!(ck > 0.f) || dca > ck + r0 + r1 + 0.01f) mask &= ~(1u << c);
+    }
+    pi[lane] = i;
+    pj[lane] = j | (sh ? 0 : 1 << 30);  // bit 30: short range
+    // exclusive prefix of the survivors over the lanes
+    const int cnt = __popc(mask);
+    int off = cnt;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const int t = __shfl_up_sync(0xffffffffu, off, d);
+      if (lane >= d) off += t;
+    }
+    const int total = __shfl_sync(0xffffffffu, off, 31);
+    off -= cnt;
+    for (unsigned m = mask; m; m &= m - 1u) items[off++] = lane << 4 | (__ffs(m) - 1);
+    __syncwarp();
+    for (int b = 0; b < total; b += 32) {
+      if (b + lane < total) {
+        const int it = items[b + lane], src = it >> 4, c = it & 15, b0 = c / 3, b1 = c - 3 * b0;
+        const int ii = pi[src], jw = pj[src], jj = jw & ((1 << 30) - 1);
+        const bool shortr = jw >> 30;
+        const V3<R> dd = diff<R>(bead(s, ii, b0), bead(s, jj, b1));
+        if (norm2(dd) <= ev_max_sq) {  // beyond every cutoff: no table lookups
+          V3<R> f;
+          bool hit = false;
+          const R e = ev_pair(a, a.atom_type[3 * ii + b0], a.atom_type[3 * jj + b1], shortr, dd, f, SEL ? &hit : nullptr);
+          if (hit) sel_rec<SEL>(a, AWSEM_SEL_EV, c, ii, jj);
+          if (e != R(0) || f.x != R(0) || f.y != R(0) || f.z != R(0)) {
+            const long long v[3] = {fix_force((double) f.x), fix_force((double) f.y), fix_force((double) f.z)};
+            const long long w[3] = {-v[0], -v[1], -v[2]};
+            scatter_fix(s, ii, b0, v);
+            scatter_fix(s, jj, b1, w);
+            const long long ef = fix_force((double) e);
+            if (ef) atomicAdd(e_ev + ii, (unsigned long long) ef);
+          }
+        }
+      }
+    }
+    __syncwarp();
   };
   // warp-uniform trip count: the queue appends below are warp collectives
   // (a warp's 32 indices lie in one near-list segment: segments are multiples of 32 long)

@@ -239,6 +239,10 @@ void read_coeff_file(const std::string &path, ForceField &ff)
   p.k_global_pap *= p.epsilon;
   for (int j = 0; j < p.n_rama; j++) p.w[j] *= k_rama;
   for (int j = 0; j < p.n_rama_p; j++) p.w[j + i_rp] *= k_rama;
+  for (int j = 0; j < 12; j++) {
+    p.cphi0[j] = cos(p.phi0[j]), p.sphi0[j] = sin(p.phi0[j]);
+    p.cpsi0[j] = cos(p.psi0[j]), p.spsi0[j] = sin(p.psi0[j]);
+  }
   p.k_fm = ff.k_fm_raw;
   p.k_amh_go *= p.epsilon;
   p.k_cont_rest *= p.epsilon;

@@ -46,6 +46,7 @@ struct FFParams {
   double an, bn, cn, ap, bp, cp, ah, bh, ch;
   double k_chain[3], r_ncb0, r_cpcb0, r_ncp0, k_chi, chi0;
   double w[12], phiw[12], phi0[12], psiw[12], psi0[12];
+  double cphi0[12], sphi0[12], cpsi0[12], spsi0[12];  // cos / sin of phi0, psi0 (angle-sum form of rama)
   double hbscl[4][9];
   double sigma_NO_sqinv, sigma_HO_sqinv, NO_zero, HO_zero, k_dssp, dssp_cut, dssp_cut_sq;
   double pref[2], d_nu0, nu_cut_sq[2];

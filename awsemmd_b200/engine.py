@@ -28,7 +28,7 @@ FP64 = 0
 MIXED = 1
 TERMS_FIX, TERMS_PAIR, TERMS_BOND = 1, 2, 4
 TERMS_ALL = 7
-NKERNELS = 11  # AWSEM_NKERNELS: kernels of one MD step, in launch order
+NKERNELS = 12  # AWSEM_NKERNELS: kernels of one MD step, in launch order
 
 ENERGY_NAMES = ["total", "chain", "shake", "chi", "rama", "excluded", "dssp", "p_ap", "water", "burial",
                 "helix", "amh_go", "frag_mem", "vec_fm", "contact_restraints", "membrane", "ssb", "dh",

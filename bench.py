@@ -315,7 +315,7 @@ TIMER_NAMES = ["Chain", "Shake", "Chi", "Rama", "Vexcluded", "DSSP", "PAP", "Wat
                "Frag_Mem", "Vec_FM", "Membrane", "SSB", "DH", "Frust_Analysis", "Pair", "Pair_Double_Loop1",
                "Pair_Single_Loop", "Pair_Double_Loop2", "Pair_Double_Loop3", "Total"]
 # the GPU kernels that do the work of each timed reference section
-TIMER_TO_KERNELS = {"Chain": "residue", "Chi": "residue", "Rama": "residue", "DSSP": "pair (detection) + hbond",
+TIMER_TO_KERNELS = {"Chain": "backbone", "Chi": "backbone", "Rama": "backbone", "DSSP": "pair (detection) + hbond",
                     "PAP": "pair (detection) + hbond", "Frag_Mem": "fragmem", "Pair_Double_Loop1": "density",
                     "Pair_Single_Loop": "residue (switching, burial, helical pairs)", "Pair_Double_Loop2": "water_xi",
                     "Pair_Double_Loop3": "radial + pair (detection)", "Vexcluded": "pair + residue"}

@@ -285,7 +285,7 @@ int awsem_neighbor_stats(awsem_system *sys, int *nbuilds, double *radius, int *m
 long long awsem_step(const awsem_system *sys);
 
 /* Kernels of one MD step, in launch order (names for awsem_profile_step). */
-#define AWSEM_NKERNELS 11
+#define AWSEM_NKERNELS 12
 const char *awsem_kernel_name(int k);
 
 /* Average device time (ms) of each kernel of one MD step, measured with CUDA
