@@ -1340,6 +1340,7 @@ template <typename R> class Engine : public EngineBase {
           size_t row = (size_t) (32 * g + l) * fm.nd + d;
           len = std::max(len, fm.row_start[row + 1] - fm.row_start[row]);
         }
+        len += len & 1;  // even: the kernels take a row's records in pairs
         soff[(size_t) g * nd + d] = (int) stripes;
         slen[(size_t) g * nd + d] = len;
         stripes += len;
@@ -1854,6 +1855,7 @@ template <typename R> class Engine : public EngineBase {
           size_t row = (size_t) (32 * g + l) * fm.nd + d;
           len = std::max(len, fm.row_start[row + 1] - fm.row_start[row]);
         }
+        len += len & 1;  // even: the kernels take a row's records in pairs
         slen[(size_t) g * nd + d] = len;
         stripes += len;
       }

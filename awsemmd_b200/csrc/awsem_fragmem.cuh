@@ -9,13 +9,17 @@
 // m carries record m of each of the 32 rows side by side, lane l's record
 // at [stripe][l].  Rows shorter than `len` are padded with records whose
 // distances are 1e30 and whose coefficient is 0: their Gaussian is exactly
-// zero, so padding never changes a sum.  Blocks are stored g-major
-// (block = g * nd + d), so the data of one group is contiguous.
+// zero, so padding never changes a sum.  Block lengths are even, so every
+// block starts on an even stripe.  Blocks are stored g-major (block =
+// g * nd + d), so the data of one group is contiguous.
 //
 // Kernel mapping.  One warp per (group, chunk of separations); lane l owns
 // residue i = 32g + l and streams its rows stripe by stripe: every load of
 // the warp is 32 consecutive records (512 B FP32, 1 KiB FP64) and each lane
-// keeps its own sums, so no cross-lane reduction is needed.  Forces are
+// keeps its own sums, so no cross-lane reduction is needed.  A row's even
+// and odd records go to two sets of sums, added at the row's end: two
+// independent dependency chains per lane, and the same sums in every path
+// that reads the table (the records pair up the same way in each).  Forces are
 // converted to 64-bit fixed point (2^-32) per (row, atom pair) and added to
 // the accumulator of j with integer atomics; i's forces are summed in
 // registers over the chunk first.  Everything is order independent, so a
@@ -176,14 +180,19 @@ __device__ __forceinline__ void fragmem_unit_reg_t(int w, const FMSlices<R> &t, 
     for (int k = 0; k < 4; k++) r[k] = m_sqrt(norm2(dv[k]));
     const R s2 = R(sig[t.min_sep + d]);
     const R k2 = fm_k2(s2);
-    R es = 0, fs[4] = {0, 0, 0, 0};
-#pragma unroll 4
-    for (int m = 0; m < len; m++) {
+    R es = 0, fs[4] = {0, 0, 0, 0}, es1 = 0, fs1[4] = {0, 0, 0, 0};
+#pragma unroll 2
+    for (int m = 0; m < len; m += 2) {  // len is even
       const size_t at = base + (size_t) m * 32;
-      R rec[4];
+      R rec[4], rec1[4];
       load_record(t.rf, at, rec);
+      load_record(t.rf, at + 32, rec1);
       fm_record<COEF>(rec, COEF ? t.coef[at] : R(1), r, k2, es, fs);
+      fm_record<COEF>(rec1, COEF ? t.coef[at + 32] : R(1), r, k2, es1, fs1);
     }
+    es = es + es1;
+#pragma unroll
+    for (int k = 0; k < 4; k++) fs[k] = fs[k] + fs1[k];
     e += (double) (scale * es);
     // atom pair k acts on CA(i) (k < 2) or CB(i), and on CA(j) (k even) or CB(j)
     long long fja[3] = {0, 0, 0}, fjb[3] = {0, 0, 0};
@@ -361,7 +370,7 @@ __device__ __forceinline__ bool fragmem_unit_bulk_t(int w, const FMSlices<R> &t,
   // current row (block d): geometry and sums
   int d = d0, blk_end = 0, j = 0;
   V3<R> dv[4];
-  R r[4], s2 = 1, k2 = -1, es = 0, fs[4] = {0, 0, 0, 0};
+  R r[4], s2 = 1, k2 = -1, es = 0, fs[4] = {0, 0, 0, 0}, es1 = 0, fs1[4] = {0, 0, 0, 0};
   auto begin_row = [&]() {  // d: the next non-empty block at or after d
     while (d < d1 && t.slen[g * t.nd + d] == 0) d++;
     if (d >= d1) return;
@@ -376,11 +385,14 @@ __device__ __forceinline__ bool fragmem_unit_bulk_t(int w, const FMSlices<R> &t,
     for (int k = 0; k < 4; k++) r[k] = m_sqrt(norm2(dv[k]));
     s2 = R(sig[t.min_sep + d]);
     k2 = fm_k2(s2);
-    es = 0;
+    es = es1 = 0;
 #pragma unroll
-    for (int k = 0; k < 4; k++) fs[k] = 0;
+    for (int k = 0; k < 4; k++) fs[k] = fs1[k] = 0;
   };
   auto end_row = [&]() {
+    es = es + es1;
+#pragma unroll
+    for (int k = 0; k < 4; k++) fs[k] = fs[k] + fs1[k];
     e += (double) (scale * es);
     long long fja[3] = {0, 0, 0}, fjb[3] = {0, 0, 0};
 #pragma unroll
@@ -424,13 +436,17 @@ __device__ __forceinline__ bool fragmem_unit_bulk_t(int w, const FMSlices<R> &t,
         end_row();
         begin_row();
       }
-      // the stripes of this chunk that belong to the current row (at least one)
-      const int run = max(q + 1, min(ns, blk_end - s0));
-#pragma unroll(sizeof(R) == 4 ? 4 : 1)
-      for (; q < run; q++) {
-        R rec[4];
+      // the stripes of this chunk that belong to the current row (rows,
+      // chunks and their ends fall on even stripes: records pair up as in
+      // the register path)
+      const int run = max(q + 2, min(ns, blk_end - s0));
+#pragma unroll(sizeof(R) == 4 ? 2 : 1)
+      for (; q < run; q += 2) {
+        R rec[4], rec1[4];
         load_record_shared(srf, q * 32 + lane, rec);
+        load_record_shared(srf, (q + 1) * 32 + lane, rec1);
         fm_record<COEF>(rec, COEF ? scf[q * 32 + lane] : R(1), r, k2, es, fs);
+        fm_record<COEF>(rec1, COEF ? scf[(q + 1) * 32 + lane] : R(1), r, k2, es1, fs1);
       }
     }
     __syncwarp();  // every lane has read the stage
