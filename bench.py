@@ -274,8 +274,8 @@ def c3_seed(k: int, rank: int = 0) -> int:
 # DRAM bytes (read + write) per algorithmic byte of a launch, from one ncu
 # capture of the kernel on the first 256 replicas of configuration 3, whose
 # fragment-memory table (458 MB) is larger than L2
-# (profiles/sections_c3_256replicas.txt: 482.7 MB for 458.1 MB)
-TRAFFIC_PER_ALGORITHMIC_BYTE = {"fragmem": 482.695 / 458.053744}
+# (profiles/sections_c3_256replicas.txt: 483.8 MB for 458.1 MB)
+TRAFFIC_PER_ALGORITHMIC_BYTE = {"fragmem": 483.8 / 458.053744}
 TRAFFIC_SOURCE = "ncu dram read+write of a 256-replica launch per algorithmic byte, times this launch's algorithmic " \
                  "bytes (profiles/sections_c3_256replicas.txt)"
 
