@@ -640,6 +640,26 @@ template <typename R> __global__ void k_nl_build(StepArgs<R> a, GridArgs g, int 
   for (int p = (sp).t, S_ = (a).nl->seg_len, end_ = (a).nl->nseg * S_; p < end_; p += (sp).nthr)      \
     if (p - (p / S_) * S_ < (a).seg_n[p / S_])
 
+// Density well value (FP64 in both forms).  The plain FP64 form evaluates
+// the reference's 0.25 (1 + tanh(kappa (r - rmin))) (1 + tanh(kappa (rmax -
+// r))); the mixed form the same from two exponentials,
+// 1 / ((1 + e^(-2 kappa (r - rmin))) (1 + e^(-2 kappa (rmax - r)))), one
+// division instead of the two inside two tanh (equal to about 1e-16).
+template <typename R>
+__device__ __forceinline__ double density_well(double r, double rmin_th, double rmax_th, double kappa, double rmin,
+                                               double rmax)
+{
+  if constexpr (sizeof(R) == 4) {
+    if (r < rmin_th || r > rmax_th) return 0.0;
+    const double ea = exp(-2.0 * kappa * (r - rmin)), eb = exp(-2.0 * kappa * (rmax - r));
+    return 1.0 / ((1.0 + ea) * (1.0 + eb));
+  } else {
+    double th, pr;
+    well_theta(r, rmin_th, rmax_th, kappa, rmin, rmax, th, pr);
+    return th;
+  }
+}
+
 // DL1: local densities of contact beads (fix_backbone.cpp:7728-7791).  FP64
 // in both forms: the densities feed the burial and switching functions (an
 // FP32 well value here put the helix term of configuration 1 at 3e-5 of its
@@ -683,16 +703,14 @@ template <typename R, bool SEL = false> __device__ __forceinline__ void density_
     if (q >= hi || (s.res_chain[j] == s.res_chain[i] && j - i <= 1)) continue;
     const double r = sqrt(rsq);
     if (water && rsq > p.w_rmin_sq[0] && rsq < p.w_rmax_sq[0]) {
-      double th, pr;
-      well_theta(r, p.w_rmin_th[0], p.w_rmax_th[0], p.water_kappa, p.well_rmin[0], p.well_rmax[0], th, pr);
+      const double th = density_well<R>(r, p.w_rmin_th[0], p.w_rmax_th[0], p.water_kappa, p.well_rmin[0], p.well_rmax[0]);
       const unsigned long long v = (unsigned long long) fix_dens(th);
       atomicAdd(aw + i, v);
       atomicAdd(aw + j, v);
       sel_rec<SEL>(a, AWSEM_SEL_DENS_WATER, 0, i, j);
     }
     if (helix && rsq > p.h_rmin_sq && rsq < p.h_rmax_sq) {
-      double th, pr;
-      well_theta(r, p.h_rmin_th, p.h_rmax_th, p.helix_kappa, p.helix_rmin, p.helix_rmax, th, pr);
+      const double th = density_well<R>(r, p.h_rmin_th, p.h_rmax_th, p.helix_kappa, p.helix_rmin, p.helix_rmax);
       const unsigned long long v = (unsigned long long) fix_dens(th);
       atomicAdd(ah + i, v);
       atomicAdd(ah + j, v);
