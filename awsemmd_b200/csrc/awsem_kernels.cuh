@@ -99,8 +99,10 @@ struct SlotRun {
 // (this record, the contact bead, the water-xi sum) instead of ten arrays.
 struct __align__(64) RadRec {
   double sw, bur, x1, x2, sigp;  // sigma_water, burial coefficient, helix xi1, xi2 of residue r - helix_i_diff, sigma_water'
-  int type, flags, chain, pad;
+  double pad0;
+  int type, flags, chain, pad;   // the last 16 bytes, read alone as an int4 by the detection pass
 };
+static_assert(sizeof(RadRec) == 64 && offsetof(RadRec, type) == 48, "RadRec layout");
 
 template <typename R> struct StepArgs {
   DevSys<R> s;
@@ -957,12 +959,13 @@ template <typename R, bool SEL = false> __device__ __forceinline__ void water_xi
   {
     const int2 ij = a.cpairs[q];
     const int i = ij.x, j = ij.y;
-    if (s.res_chain[j] == s.res_chain[i] && j - i < p.contact_cutoff) continue;
+    // the residues' packed records (written by the residue pass) and contact beads
+    const RadRec ri = a.rrec[i], rj = a.rrec[j];
+    if (rj.chain == ri.chain && j - i < p.contact_cutoff) continue;
     const R rsq = norm2(diff<R>(contact(s, i), contact(s, j)));
-    const int ti = s.res_type[i], tj = s.res_type[j];
+    const int ti = ri.type, tj = rj.type;
     // pairs with a phosphorylated residue use the phosphorylation gammas (fix_backbone.cpp:2872-2885)
-    const double *W = ((p.terms & T_PHOSPH) && ((s.res_flags[i] | s.res_flags[j]) & R_PHOSPH))
-                          ? s.tables + TB_WATER_PHOSPH : WG;
+    const double *W = ((p.terms & T_PHOSPH) && ((ri.flags | rj.flags) & R_PHOSPH)) ? s.tables + TB_WATER_PHOSPH : WG;
     for (int w = 0; w < p.n_wells; w++) {
       if (!p.well_flag[w]) continue;
       const double g0 = W[w * 800 + (ti * 20 + tj) * 2], g1 = W[w * 800 + (ti * 20 + tj) * 2 + 1];
@@ -973,8 +976,8 @@ template <typename R, bool SEL = false> __device__ __forceinline__ void water_xi
         well_theta(m_sqrt(rsq), R(p.w_rmin_th[w]), R(p.w_rmax_th[w]), R(p.water_kappa), R(p.well_rmin[w]),
                    R(p.well_rmax[w]), th, pr);
         const double tg = (g1 - g0) * (double) th;
-        atomicAdd(acc + i, (unsigned long long) fix_dens(tg * a.sig_w[j]));
-        atomicAdd(acc + j, (unsigned long long) fix_dens(tg * a.sig_w[i]));
+        atomicAdd(acc + i, (unsigned long long) fix_dens(tg * rj.sw));
+        atomicAdd(acc + j, (unsigned long long) fix_dens(tg * ri.sw));
       }
     }
   }
@@ -1235,8 +1238,9 @@ template <typename R, bool SEL = false> __device__ __forceinline__ void pair_pas
     if (lane < have) {
     const int2 ij = a.cpairs[q];
     const int i = ij.x, j = ij.y;
-    const int fli = s.res_flags[i], flj = s.res_flags[j];
-    const bool other = s.res_chain[j] != s.res_chain[i];
+    const int4 ri = reinterpret_cast<const int4 *>(a.rrec + i)[3], rj = reinterpret_cast<const int4 *>(a.rrec + j)[3];
+    const int fli = ri.y, flj = rj.y;  // RadRec's last 16 bytes: type, flags, chain, pad
+    const bool other = rj.z != ri.z;
     const V3<double> ca_i = bead(s, i, B_CA), ca_j = bead(s, j, B_CA);
     const int dij = j - i;
     const R rca2 = norm2(diff<R>(ca_i, ca_j));
