@@ -131,6 +131,14 @@ class EngineBase {
                             double dt, double damp) = 0;
   virtual int admit(const ReplicaArrays &ra, unsigned long long seed, long long nsteps, double t_start,
                     double t_stop) = 0;  // slot, or -1 when the request does not fit now
+  // admit in two parts: the host-side preparation (topology, memory table
+  // slices; touches no device state and may run on another thread while
+  // advance runs), then the placement and uploads
+  virtual void *prepare_request(const ReplicaArrays &ra) = 0;
+  virtual int admit_prepared(void *prep, unsigned long long seed, long long nsteps, double t_start,
+                             double t_stop) = 0;
+  using PreparedDeleter = void (*)(void *);
+  virtual PreparedDeleter prepared_deleter() const = 0;
   virtual void progress(int slot, long long *done, long long *total) = 0;
   virtual void advance(long long nsteps) = 0;
   virtual void release(int slot) = 0;
@@ -1819,17 +1827,89 @@ template <typename R> class Engine : public EngineBase {
     CK(cudaStreamSynchronize(s0));
   }
 
-  int admit(const ReplicaArrays &ra, unsigned long long seed, long long nsteps, double t_start, double t_stop) override
-  {
-    if (nsteps < 0) throw std::invalid_argument("nsteps must be >= 0");
-    if (t_start < 0 || t_stop < 0) throw std::invalid_argument("temperatures must be >= 0");
+  // A request prepared on the host: its system, the slices of its memory
+  // table in the engine's arithmetic type, at local stripe offsets
+  struct Prepared {
     SystemInput S;
+    std::vector<int> slen, loff;  // [groups][nd] block lengths and first local stripes
+    long long stripes = 0;
+    int groups = 0;
+    std::vector<R> rf, cf;  // [stripes][32][4] distances, [stripes][32] coefficients
+  };
+
+  void *prepare_request(const ReplicaArrays &ra) override
+  {
+    if (!server) throw std::invalid_argument("not a serving handle");
+    auto P = std::make_unique<Prepared>();
+    SystemInput &S = P->S;
     load_system_arrays(*sf, ra, S);
     const Topology &t = S.top;
     const FMTable &fm = S.fm;
     const int nd = in.ff.p.fm_nd, n = t.n_res, groups = (n + 31) / 32;
     if ((in.ff.p.terms & T_FM) && fm.nd > nd)
       throw std::invalid_argument("memory separations exceed the fragment-memory table of this handle");
+    // slices of the request's rows (local groups)
+    P->groups = groups;
+    P->slen.assign((size_t) groups * std::max(nd, 1), 0);
+    P->loff.assign(P->slen.size(), 0);
+    long long stripes = 0;
+    for (int g = 0; g < groups; g++)
+      for (int d = 0; d < fm.nd; d++) {
+        int len = 0;
+        for (int l = 0; l < 32 && 32 * g + l < n; l++) {
+          size_t row = (size_t) (32 * g + l) * fm.nd + d;
+          len = std::max(len, fm.row_start[row + 1] - fm.row_start[row]);
+        }
+        len += len & 1;  // even: the kernels take a row's records in pairs
+        P->slen[(size_t) g * nd + d] = len;
+        stripes += len;
+      }
+    P->stripes = stripes;
+    if (nd > 0) {
+      P->rf.assign((size_t) stripes * 32 * 4, R(FMTable::FM_SKIP));
+      P->cf.assign((size_t) stripes * 32, R(0));
+      long long at_stripe = 0;
+      for (int g = 0; g < groups; g++)
+        for (int d = 0; d < nd; d++) {
+          const size_t blk = (size_t) g * nd + d;
+          P->loff[blk] = (int) at_stripe;
+          for (int l = 0; l < 32 && 32 * g + l < n && d < fm.nd; l++) {
+            size_t row = (size_t) (32 * g + l) * fm.nd + d;
+            for (int m = 0, rec = fm.row_start[row]; rec < fm.row_start[row + 1]; m++, rec++) {
+              size_t e = (size_t) (at_stripe + m) * 32 + l;
+              for (int k = 0; k < 4; k++) P->rf[e * 4 + k] = (R) fm.rf[(size_t) rec * 4 + k];
+              P->cf[e] = (R) (fm.uniform ? fm.uniform_coef : fm.coef[rec]);
+            }
+          }
+          at_stripe += P->slen[blk];
+        }
+    }
+    return P.release();
+  }
+
+  static void delete_prepared(void *prep) { delete static_cast<Prepared *>(prep); }
+  PreparedDeleter prepared_deleter() const override { return &Engine::delete_prepared; }
+
+  int admit(const ReplicaArrays &ra, unsigned long long seed, long long nsteps, double t_start, double t_stop) override
+  {
+    if (nsteps < 0) throw std::invalid_argument("nsteps must be >= 0");
+    if (t_start < 0 || t_stop < 0) throw std::invalid_argument("temperatures must be >= 0");
+    std::unique_ptr<Prepared> P(static_cast<Prepared *>(prepare_request(ra)));
+    return admit_prepared(P.get(), seed, nsteps, t_start, t_stop);
+  }
+
+  int admit_prepared(void *prep, unsigned long long seed, long long nsteps, double t_start, double t_stop) override
+  {
+    if (!server) throw std::invalid_argument("not a serving handle");
+    if (nsteps < 0) throw std::invalid_argument("nsteps must be >= 0");
+    if (t_start < 0 || t_stop < 0) throw std::invalid_argument("temperatures must be >= 0");
+    Prepared &P = *static_cast<Prepared *>(prep);
+    SystemInput &S = P.S;
+    const Topology &t = S.top;
+    const FMTable &fm = S.fm;
+    const int nd = in.ff.p.fm_nd, n = t.n_res, groups = P.groups;
+    const long long stripes = P.stripes;
+    const std::vector<int> &slen = P.slen;
     // coefficient mode: a uniform coefficient shared by every request so far,
     // else a per-record coefficient pool
     if ((in.ff.p.terms & T_FM) && fm.records() > 0 && !fm_coef_mode) {
@@ -1845,20 +1925,6 @@ template <typename R> class Engine : public EngineBase {
         release_graphs();
       }
     }
-    // slices of the request's rows (local groups)
-    std::vector<int> slen((size_t) groups * std::max(nd, 1), 0);
-    long long stripes = 0;
-    for (int g = 0; g < groups; g++)
-      for (int d = 0; d < fm.nd; d++) {
-        int len = 0;
-        for (int l = 0; l < 32 && 32 * g + l < n; l++) {
-          size_t row = (size_t) (32 * g + l) * fm.nd + d;
-          len = std::max(len, fm.row_start[row + 1] - fm.row_start[row]);
-        }
-        len += len & 1;  // even: the kernels take a row's records in pairs
-        slen[(size_t) g * nd + d] = len;
-        stripes += len;
-      }
     int slot_id = -1;
     for (int k = 0; k < (int) slots.size(); k++)
       if (!slots[k].used) {
@@ -1912,26 +1978,11 @@ template <typename R> class Engine : public EngineBase {
     // fragment memory: the request's blocks at stripe st0
     if (nd > 0) {
       std::vector<int> soff((size_t) groups * nd, 0);
-      std::vector<R> rf((size_t) stripes * 32 * 4, R(FMTable::FM_SKIP)), cf(fm_coef_mode ? (size_t) stripes * 32 : 0, R(0));
-      long long at_stripe = 0;
-      for (int g = 0; g < groups; g++)
-        for (int d = 0; d < nd; d++) {
-          const size_t blk = (size_t) g * nd + d;
-          soff[blk] = (int) (st0 + at_stripe);
-          for (int l = 0; l < 32 && 32 * g + l < n && d < fm.nd; l++) {
-            size_t row = (size_t) (32 * g + l) * fm.nd + d;
-            for (int m = 0, rec = fm.row_start[row]; rec < fm.row_start[row + 1]; m++, rec++) {
-              size_t e = (size_t) (at_stripe + m) * 32 + l;
-              for (int k = 0; k < 4; k++) rf[e * 4 + k] = (R) fm.rf[(size_t) rec * 4 + k];
-              if (fm_coef_mode) cf[e] = (R) (fm.uniform ? fm.uniform_coef : fm.coef[rec]);
-            }
-          }
-          at_stripe += slen[blk];
-        }
+      for (size_t blk = 0; blk < soff.size(); blk++) soff[blk] = (int) (st0 + P.loff[blk]);
       put(fm_soff, (size_t) g0 * nd, soff.data(), soff.size());
       put(fm_slen, (size_t) g0 * nd, slen.data(), slen.size());
-      put(fm_rf, (size_t) st0 * 32 * 4, rf.data(), rf.size());
-      if (fm_coef_mode) put(fm_coef, (size_t) st0 * 32, cf.data(), cf.size());
+      put(fm_rf, (size_t) st0 * 32 * 4, P.rf.data(), P.rf.size());
+      if (fm_coef_mode) put(fm_coef, (size_t) st0 * 32, P.cf.data(), P.cf.size());
       CK(cudaStreamSynchronize(s0));
     }
     // run window: the next evaluation is this request's setup evaluation
@@ -2477,6 +2528,59 @@ int awsem_server_admit(awsem_system *sys, const awsem_replica_desc *d, long long
   }
   if (slot) *slot = got;
   return AWSEM_OK;
+}
+
+// A request prepared on the host for one serving handle
+struct awsem_request {
+  const EngineBase *eng;  // the handle it was prepared for
+  void *prep;
+  EngineBase::PreparedDeleter del;
+  unsigned long long seed;
+};
+
+int awsem_server_prepare(awsem_system *sys, const awsem_replica_desc *d, awsem_request **out)
+{
+  if (!serving(sys, "awsem_server_prepare")) return AWSEM_EINVAL;
+  if (!d || !out) {
+    g_last_error = "awsem_server_prepare: null request or output";
+    return AWSEM_EINVAL;
+  }
+  *out = nullptr;
+  return guarded([&] {
+    ReplicaArrays ra{d->n_res, d->n_chains, d->chain_len, d->seq, d->ssweight, d->x, d->v, d->n_mem,
+                     d->mem_pos, d->mem_len, d->mem_weight, d->mem_seq, d->mem_ca, d->mem_cb};
+    void *prep = sys->eng->prepare_request(ra);
+    *out = new awsem_request{sys->eng.get(), prep, sys->eng->prepared_deleter(), d->seed};
+  });
+}
+
+int awsem_server_admit_prepared(awsem_system *sys, awsem_request *req, long long nsteps, double t_start,
+                                double t_stop, int *slot)
+{
+  if (!serving(sys, "awsem_server_admit_prepared")) return AWSEM_EINVAL;
+  if (!req || req->eng != sys->eng.get()) {
+    g_last_error = "awsem_server_admit_prepared: the request was not prepared for this handle";
+    return AWSEM_EINVAL;
+  }
+  int got = -1;
+  int rc = guarded([&] {
+    CK(cudaSetDevice(sys->eng->device));
+    got = sys->eng->admit_prepared(req->prep, req->seed, nsteps, t_start, t_stop);
+  });
+  if (rc != AWSEM_OK) return rc;
+  if (got < 0) {
+    g_last_error = "awsem_server_admit_prepared: no free slot, residue range or memory-record room now";
+    return AWSEM_EBUSY;
+  }
+  if (slot) *slot = got;
+  return AWSEM_OK;
+}
+
+void awsem_request_free(awsem_request *req)
+{
+  if (!req) return;
+  req->del(req->prep);
+  delete req;
 }
 
 int awsem_server_advance(awsem_system *sys, long long nsteps)

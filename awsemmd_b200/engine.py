@@ -140,6 +140,10 @@ def load_library(path: str = LIB_PATH):
     ll = C.c_longlong
     lib.awsem_server_create.argtypes = [cp, cp, cp, cp, ip, ip, ll, ip, ll, C.c_double, C.c_double, C.POINTER(vp)]
     lib.awsem_server_admit.argtypes = [vp, C.POINTER(ReplicaDesc), ll, C.c_double, C.c_double, C.POINTER(ip)]
+    lib.awsem_server_prepare.argtypes = [vp, C.POINTER(ReplicaDesc), C.POINTER(vp)]
+    lib.awsem_server_admit_prepared.argtypes = [vp, vp, ll, C.c_double, C.c_double, C.POINTER(ip)]
+    lib.awsem_request_free.argtypes = [vp]
+    lib.awsem_request_free.restype = None
     lib.awsem_server_advance.argtypes = [vp, ll]
     lib.awsem_server_progress.argtypes = [vp, ip, C.POINTER(ll), C.POINTER(ll)]
     lib.awsem_server_collect.argtypes = [vp, ip, vp, vp, vp]
@@ -487,6 +491,21 @@ class AwsemBatch(AwsemSystem):
 EBUSY = -6
 
 
+class PreparedRequest:
+    """A request prepared on the host for one serving handle (awsem_request)."""
+
+    def __init__(self, lib, h, n_res: int):
+        self.lib, self.h, self.n_res = lib, h, n_res
+
+    def free(self):
+        if getattr(self, "h", None):
+            self.lib.awsem_request_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.free()
+
+
 class AwsemServer:
     """Continuous batching of MD requests on one GPU (awsem_server_* C ABI).
 
@@ -524,15 +543,31 @@ class AwsemServer:
     def __exit__(self, *exc):
         self.close()
 
-    def admit(self, chain: dict, nsteps: int, t_start: float = 300.0, t_stop: float = 300.0, seed: int = 1):
+    def prepare(self, chain: dict, seed: int = 1) -> "PreparedRequest":
+        """Host-side preparation of a request (awsem_server_prepare): safe to
+        call from another thread while `advance` runs."""
         d = replica_desc(chain, seed)
+        out = C.c_void_p()
+        _check(self.lib, self.lib.awsem_server_prepare(self.h, C.byref(d), C.byref(out)), "awsem_server_prepare")
+        return PreparedRequest(self.lib, out, int(chain["n_res"]))
+
+    def admit(self, chain, nsteps: int, t_start: float = 300.0, t_stop: float = 300.0, seed: int = 1):
+        """Place a request (chain arrays, or a PreparedRequest whose seed was
+        given to `prepare`); None when it does not fit now."""
         slot = C.c_int()
-        rc = self.lib.awsem_server_admit(self.h, C.byref(d), int(nsteps), float(t_start), float(t_stop),
-                                         C.byref(slot))
+        if isinstance(chain, PreparedRequest):
+            rc = self.lib.awsem_server_admit_prepared(self.h, chain.h, int(nsteps), float(t_start), float(t_stop),
+                                                      C.byref(slot))
+            what, n_res = "awsem_server_admit_prepared", chain.n_res
+        else:
+            d = replica_desc(chain, seed)
+            rc = self.lib.awsem_server_admit(self.h, C.byref(d), int(nsteps), float(t_start), float(t_stop),
+                                             C.byref(slot))
+            what, n_res = "awsem_server_admit", int(chain["n_res"])
         if rc == EBUSY:
             return None
-        _check(self.lib, rc, "awsem_server_admit")
-        self.natoms[slot.value] = 3 * int(chain["n_res"])
+        _check(self.lib, rc, what)
+        self.natoms[slot.value] = 3 * n_res
         return slot.value
 
     def advance(self, nsteps: int):

@@ -13,6 +13,7 @@ both on the loop's wall clock.
 from __future__ import annotations
 
 import time
+from concurrent.futures import ThreadPoolExecutor
 from collections import deque
 from dataclasses import dataclass, field
 
@@ -61,33 +62,62 @@ def run_stream(server, requests: list, chunk: int = 50, clock=time.perf_counter,
     """Serve `requests` in real time on `server` (an AwsemServer or anything
     with its admit / advance / progress / collect methods).  Between GPU
     chunks of at most `chunk` steps (shorter when a request is about to
-    finish) the loop admits every arrived request that fits and collects
-    every finished one."""
+    finish) the loop admits every arrived request that fits, first come first
+    served, and collects every finished one.  When the server can prepare
+    requests on the host (AwsemServer.prepare), a worker thread prepares each
+    request as it arrives while the GPU advances the others, and admission
+    only places the prepared request."""
     pending = deque(sorted(requests, key=lambda r: r.arrival))
     active = {}  # slot -> (request, admitted time)
     done = []
+    prep = {}  # rid -> future of the prepared request
+    pool = ThreadPoolExecutor(max_workers=1) if hasattr(server, "prepare") else None
     t0 = clock()
-    while pending or active:
-        now = clock() - t0
-        while pending and pending[0].arrival <= now:
-            r = pending[0]
-            slot = server.admit(r.chain, r.nsteps, r.t_start, r.t_stop, r.seed)
-            if slot is None:
-                break  # first come first served: later arrivals wait behind it
-            pending.popleft()
-            active[slot] = (r, now)
-        if not active:
-            if pending:
-                sleep(max(0.0, pending[0].arrival - (clock() - t0)))
-            continue
-        left = min(total - got for got, total in (server.progress(s) for s in active))
-        server.advance(max(1, min(chunk, left)))
-        now = clock() - t0
-        for slot in [s for s in active if (lambda p: p[0] >= p[1])(server.progress(s))]:
-            r, adm = active.pop(slot)
-            x, _, e = server.collect(slot)
-            done.append(Completed(r.rid, r.arrival, adm, now, int(r.chain["n_res"]), r.nsteps,
-                                  x if keep_state else None, e if keep_state else None))
+    try:
+        while pending or active:
+            now = clock() - t0
+            if pool is not None:  # prepare every request that has arrived
+                for r in pending:
+                    if r.arrival > now:
+                        break
+                    if r.rid not in prep:
+                        prep[r.rid] = pool.submit(server.prepare, r.chain, r.seed)
+            while pending and pending[0].arrival <= now:
+                r = pending[0]
+                if pool is not None:
+                    fut = prep[r.rid]
+                    if not fut.done() and active:
+                        break  # keep the GPU busy; admit it after the next chunk
+                    what = fut.result()
+                else:
+                    what = r.chain
+                slot = server.admit(what, r.nsteps, r.t_start, r.t_stop, r.seed)
+                if slot is None:
+                    if not active:
+                        raise ValueError(f"request {r.rid} ({int(r.chain['n_res'])} residues) does not fit the "
+                                         "empty serving handle")
+                    break  # first come first served: later arrivals wait behind it
+                pending.popleft()
+                if pool is not None:
+                    prep.pop(r.rid).result().free()
+                active[slot] = (r, now)
+            if not active:
+                if pending and pending[0].arrival > clock() - t0:
+                    sleep(max(0.0, pending[0].arrival - (clock() - t0)))
+                continue
+            left = min(total - got for got, total in (server.progress(s) for s in active))
+            server.advance(max(1, min(chunk, left)))
+            now = clock() - t0
+            for slot in [s for s in active if (lambda p: p[0] >= p[1])(server.progress(s))]:
+                r, adm = active.pop(slot)
+                x, _, e = server.collect(slot)
+                done.append(Completed(r.rid, r.arrival, adm, now, int(r.chain["n_res"]), r.nsteps,
+                                      x if keep_state else None, e if keep_state else None))
+    finally:
+        if pool is not None:
+            pool.shutdown(wait=True)
+            for fut in prep.values():
+                fut.result().free()
     return done
 
 

@@ -410,6 +410,21 @@ int awsem_server_create(const char *workdir, const char *coeff_file, const char 
                         long long max_memory_records, double dt, double damp, awsem_system **out);
 int awsem_server_admit(awsem_system *srv, const awsem_replica_desc *request, long long nsteps, double t_start,
                        double t_stop, int *slot);
+/* Admission in two parts, so that a serving loop can prepare the next
+ * arrivals while the GPU advances: awsem_server_prepare builds a request's
+ * host-side data (topology, fragment-memory table slices in the handle's
+ * arithmetic type; no device work, and it may run on another host thread
+ * while awsem_server_advance runs on this handle); awsem_server_admit_prepared
+ * places it (AWSEM_EBUSY when it does not fit now: the prepared request stays
+ * valid and may be admitted later; AWSEM_EINVAL for a request prepared for
+ * another handle).  awsem_request_free releases a prepared request, admitted
+ * or not, and may be called after the handle is destroyed.
+ * awsem_server_admit is prepare + admit_prepared + free. */
+typedef struct awsem_request awsem_request;
+int awsem_server_prepare(awsem_system *srv, const awsem_replica_desc *request, awsem_request **out);
+int awsem_server_admit_prepared(awsem_system *srv, awsem_request *request, long long nsteps, double t_start,
+                                double t_stop, int *slot);
+void awsem_request_free(awsem_request *request);
 int awsem_server_advance(awsem_system *srv, long long nsteps);
 int awsem_server_progress(awsem_system *srv, int slot, long long *done, long long *total);
 int awsem_server_collect(awsem_system *srv, int slot, double *x, double *v, double *energies);

@@ -100,3 +100,35 @@ def test_stream_serves_every_request(ff, gpu_lib):
         assert np.all(np.isfinite(d.x)) and np.isfinite(d.energies).all()
     st = serve.stream_stats(done)
     assert st["p99_s"] >= st["p50_s"] > 0
+
+
+def test_prepared_admission_equals_direct_admission(ff, gpu_lib):
+    """awsem_server_prepare + awsem_server_admit_prepared place the same
+    request as awsem_server_admit, bit for bit; a request prepared for one
+    handle is refused by another; a request that does not fit now stays
+    valid and is admitted later."""
+    from awsemmd_b200.engine import AwsemError, AwsemServer
+
+    c = chains()
+    kw = dict(max_residues=512, max_requests=8, max_memory_records=200000)
+    with AwsemServer(ff, **kw) as srv:
+        a = srv.admit(c["C"], 70, 500.0, 300.0, seed=21)
+        direct = serve_until_done(srv, {"C": a})["C"]
+    with AwsemServer(ff, **kw) as srv, AwsemServer(ff, **kw) as other:
+        p = srv.prepare(c["C"], seed=21)
+        with pytest.raises(AwsemError, match="not prepared for this handle"):
+            other.admit(p, 70, 500.0, 300.0)
+        a = srv.admit(p, 70, 500.0, 300.0)
+        p.free()
+        prepared = serve_until_done(srv, {"C": a})["C"]
+    for u, w in zip(direct, prepared):
+        assert np.array_equal(u, w)
+    with AwsemServer(ff, max_residues=96, max_requests=4, max_memory_records=200000) as srv:
+        a = srv.admit(c["A"], 10)  # 61 residues: two of three 32-residue groups
+        p = srv.prepare(c["B"], seed=3)  # 45 residues: two more groups
+        assert srv.admit(p, 10) is None
+        serve_until_done(srv, {"A": a})
+        b = srv.admit(p, 10)
+        assert b is not None
+        p.free()
+        serve_until_done(srv, {"B": b})
