@@ -61,9 +61,10 @@ def run_stream(server, requests: list, chunk: int = 50, clock=time.perf_counter,
                keep_state: bool = True) -> list:
     """Serve `requests` in real time on `server` (an AwsemServer or anything
     with its admit / advance / progress / collect methods).  Between GPU
-    chunks of at most `chunk` steps (shorter when a request is about to
-    finish) the loop admits every arrived request that fits, first come first
-    served, and collects every finished one.  When the server can prepare
+    chunks of `chunk` steps the loop admits every arrived request that fits,
+    first come first served, and collects every finished one (a request that
+    finishes inside a chunk stays frozen; its completion time is the chunk's
+    end).  When the server can prepare
     requests on the host (AwsemServer.prepare), a worker thread prepares each
     request as it arrives while the GPU advances the others, and admission
     only places the prepared request."""
@@ -105,8 +106,10 @@ def run_stream(server, requests: list, chunk: int = 50, clock=time.perf_counter,
                 if pending and pending[0].arrival > clock() - t0:
                     sleep(max(0.0, pending[0].arrival - (clock() - t0)))
                 continue
-            left = min(total - got for got, total in (server.progress(s) for s in active))
-            server.advance(max(1, min(chunk, left)))
+            # fixed chunks: a request that finishes inside one stays frozen
+            # until its end, and stopping at every completion would leave the
+            # GPU idle at each of them
+            server.advance(chunk)
             now = clock() - t0
             for slot in [s for s in active if (lambda p: p[0] >= p[1])(server.progress(s))]:
                 r, adm = active.pop(slot)

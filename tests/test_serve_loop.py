@@ -1,5 +1,5 @@
 """Host logic of the serving loop, on a fake serving handle (no GPU): FIFO
-admission by capacity, chunked advance up to the next completion, latency
+admission by capacity, advance in fixed chunks, latency
 bookkeeping, and the one-at-a-time queue model."""
 import numpy as np
 
@@ -59,8 +59,9 @@ def test_fifo_admission_and_completion():
     assert fake.admitted == [0, 1, 2]
     # 1 and 2 then run side by side; the shorter one finishes first
     assert [d.rid for d in done] == [0, 2, 1]
-    # advance never overshoots the next completion (setup evaluation + nsteps)
-    assert fake.advances == [4, 4, 3, 3, 1, 2]
+    # fixed chunks: request 0 (setup evaluation + 10 steps) finishes inside
+    # the third chunk and is collected at its end; 2 and 1 likewise
+    assert fake.advances == [4, 4, 4, 4, 4]
     assert all(d.finished >= d.admitted >= d.arrival for d in done)
 
 
