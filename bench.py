@@ -70,7 +70,7 @@ WORKLOADS = {
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=40)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="c3", choices=list(WORKLOADS))
@@ -153,7 +153,7 @@ class ClockSampler:
     def start(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except OSError:
             return
@@ -836,9 +836,9 @@ def main():
     if dist.rank == 0 and dist.world == 1 and not args.no_baseline:
         try:
             if args.workload == "c3":
-                v, rs, busy, wall, tm, nrep = reference_c3(1, md, args.replicas, sample=16)
+                v, rs, busy, wall, tm, nsamp = reference_c3(1, md, args.replicas, sample=16)
                 base = {"value": v, "unit": "residue-steps/s", "cores": 1, "kind": "reference",
-                        "sample": f"{nrep} random replicas x {md} MD steps ({rs} residue-steps, {busy:.1f} s) on 1 "
+                        "sample": f"{nsamp} random replicas x {md} MD steps ({rs} residue-steps, {busy:.1f} s) on 1 "
                                   f"host core; reference FixBackbone + PairExcludedVolume compiled -O2 against the "
                                   f"LAMMPS-API shim, 1 MPI rank",
                         "reference_timer_log": timer_breakdown(tm)}
