@@ -163,6 +163,8 @@ template <typename R> class Engine : public EngineBase {
  public:
   cudaStream_t s0 = nullptr, s1 = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  cudaStream_t s2 = nullptr;  // the detection pass and the hydrogen-bond terms
+  cudaEvent_t ev_dens = nullptr, ev_join2 = nullptr;
   DBuf<int> res_type, res_flags, res_chain, chain_start, chain_end, atom_tag, atom_type;
   DBuf<double> aps, tables, x, v, mass, g1, g2, ftot, work, e_res, energy;
   DBuf<double4> pos, cpos, cb_build;
@@ -225,8 +227,11 @@ template <typename R> class Engine : public EngineBase {
     if (ev_run1) cudaEventDestroy(ev_run1);
     if (ev_fork) cudaEventDestroy(ev_fork);
     if (ev_join) cudaEventDestroy(ev_join);
+    if (ev_dens) cudaEventDestroy(ev_dens);
+    if (ev_join2) cudaEventDestroy(ev_join2);
     if (s0) cudaStreamDestroy(s0);
     if (s1) cudaStreamDestroy(s1);
+    if (s2) cudaStreamDestroy(s2);
   }
 
   int n() const { return in.top.n_res; }
@@ -377,8 +382,11 @@ template <typename R> class Engine : public EngineBase {
     CK(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
     CK(cudaStreamCreateWithPriority(&s0, cudaStreamNonBlocking, prio_hi));
     CK(cudaStreamCreateWithPriority(&s1, cudaStreamNonBlocking, prio_lo));
+    CK(cudaStreamCreateWithPriority(&s2, cudaStreamNonBlocking, prio_hi));
     CK(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
     CK(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&ev_dens, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&ev_join2, cudaEventDisableTiming));
     const Topology &t = in.top;
     int nn = n(), na = natoms();
     res_sys.upload(in.res_sys, s0);
@@ -710,11 +718,18 @@ template <typename R> class Engine : public EngineBase {
       dev::k_hbond_sel<R><<<hb_blocks, 128, 0, s0>>>(a, p);
     } else {
       dev::k_density<R><<<pair_blocks, tb, 0, s0>>>(a, p);
+      // detection, excluded volume and the hydrogen-bond terms need only the
+      // positions and the near list: a third stream, beside the
+      // density-dependent passes
+      CK(cudaEventRecord(ev_dens, s0));
+      CK(cudaStreamWaitEvent(s2, ev_dens, 0));
+      dev::k_pair<R><<<pair_blocks, tb, 0, s2>>>(a, p);
+      dev::k_hbond<R><<<hb_blocks, 128, 0, s2>>>(a, p);
+      CK(cudaEventRecord(ev_join2, s2));
       dev::k_residue<R><<<nb, tb, 0, s0>>>(a, p);
       dev::k_water_xi<R><<<pair_blocks, tb, 0, s0>>>(a, p);
       dev::k_radial<R><<<pair_blocks, tb, 0, s0>>>(a, p);
-      dev::k_pair<R><<<pair_blocks, tb, 0, s0>>>(a, p);
-      dev::k_hbond<R><<<hb_blocks, 128, 0, s0>>>(a, p);
+      CK(cudaStreamWaitEvent(s0, ev_join2, 0));
     }
     if (fm || fmt || go || px || rx || bb) CK(cudaStreamWaitEvent(s0, ev_join, 0));
   }

@@ -100,7 +100,7 @@ struct SlotRun {
 struct __align__(64) RadRec {
   double sw, bur, x1, x2, sigp;  // sigma_water, burial coefficient, helix xi1, xi2 of residue r - helix_i_diff, sigma_water'
   double pad0;
-  int type, flags, chain, pad;   // the last 16 bytes, read alone as an int4 by the detection pass
+  int type, flags, chain, pad;
 };
 static_assert(sizeof(RadRec) == 64 && offsetof(RadRec, type) == 48, "RadRec layout");
 
@@ -1238,9 +1238,10 @@ template <typename R, bool SEL = false> __device__ __forceinline__ void pair_pas
     if (lane < have) {
     const int2 ij = a.cpairs[q];
     const int i = ij.x, j = ij.y;
-    const int4 ri = reinterpret_cast<const int4 *>(a.rrec + i)[3], rj = reinterpret_cast<const int4 *>(a.rrec + j)[3];
-    const int fli = ri.y, flj = rj.y;  // RadRec's last 16 bytes: type, flags, chain, pad
-    const bool other = rj.z != ri.z;
+    // (the topology arrays, not the residue pass's records: this pass runs
+    // beside the residue pass)
+    const int fli = s.res_flags[i], flj = s.res_flags[j];
+    const bool other = s.res_chain[j] != s.res_chain[i];
     const V3<double> ca_i = bead(s, i, B_CA), ca_j = bead(s, j, B_CA);
     const int dij = j - i;
     const R rca2 = norm2(diff<R>(ca_i, ca_j));
