@@ -696,12 +696,11 @@ template <typename R> class Engine : public EngineBase {
     // need only the positions; the recording pass of awsem_debug_selections
     // runs the whole residue pass instead
     const bool bb = !a.sel;
-    if (fm || fmt || go || px || rx || bb) {
-      // fragment memory and the backbone terms are independent of the pair
+    if (fm || fmt || go || px || rx) {
+      // fragment memory and the optional terms are independent of the pair
       // passes: second stream
       CK(cudaEventRecord(ev_fork, s0));
       CK(cudaStreamWaitEvent(s1, ev_fork, 0));
-      if (bb) dev::k_backbone<R><<<nb, tb, 0, s1>>>(a, p);
       if (fm) dev::k_fragmem<R><<<fm_blocks(), tb, fm_smem(), s1>>>(a, p);
       if (fmt) dev::k_fm_table<R><<<fm_table_blocks(), tb, 0, s1>>>(a, p);
       if (go) dev::k_amh_go<R><<<nb, tb, 0, s1>>>(a, p);
@@ -717,10 +716,14 @@ template <typename R> class Engine : public EngineBase {
       dev::k_pair_sel<R><<<pair_blocks, tb, 0, s0>>>(a, p);
       dev::k_hbond_sel<R><<<hb_blocks, 128, 0, s0>>>(a, p);
     } else {
+      // the backbone terms need only the positions, detection, excluded
+      // volume and the hydrogen-bond terms the positions and the near list:
+      // a third stream, beside fragment memory (second) and the
+      // density-dependent passes (first)
+      CK(cudaEventRecord(ev_fork, s0));
+      CK(cudaStreamWaitEvent(s2, ev_fork, 0));
+      if (bb) dev::k_backbone<R><<<nb, tb, 0, s2>>>(a, p);
       dev::k_density<R><<<pair_blocks, tb, 0, s0>>>(a, p);
-      // detection, excluded volume and the hydrogen-bond terms need only the
-      // positions and the near list: a third stream, beside the
-      // density-dependent passes
       CK(cudaEventRecord(ev_dens, s0));
       CK(cudaStreamWaitEvent(s2, ev_dens, 0));
       dev::k_pair<R><<<pair_blocks, tb, 0, s2>>>(a, p);
@@ -731,7 +734,7 @@ template <typename R> class Engine : public EngineBase {
       dev::k_radial<R><<<pair_blocks, tb, 0, s0>>>(a, p);
       CK(cudaStreamWaitEvent(s0, ev_join2, 0));
     }
-    if (fm || fmt || go || px || rx || bb) CK(cudaStreamWaitEvent(s0, ev_join, 0));
+    if (fm || fmt || go || px || rx) CK(cudaStreamWaitEvent(s0, ev_join, 0));
   }
 
   int finish_blocks() const { return (n_run() + dev::kFinishRes - 1) / dev::kFinishRes; }
