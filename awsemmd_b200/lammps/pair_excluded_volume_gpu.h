@@ -1,8 +1,9 @@
 /* pair_style vexcluded/gpu: PairExcludedVolume (src/pair_excluded_volume.h:12,
    src/pair_excluded_volume.cpp:50-370) evaluated by libawsem_gpu.so.
 
-   A LAMMPS style class a maintainer adds beside pair_excluded_volume.h.  The
-   input script keeps the reference commands and only renames the style:
+   A LAMMPS style class a maintainer adds beside pair_excluded_volume.h
+   (registered as vexcluded/gpu and as excluded_volume/gpu).  The input
+   script keeps the reference commands and only renames the style:
 
      pair_style vexcluded/gpu p cut_short cut_long [fp64|mixed] [device N] [groups CA-group CB-group O-group]
      pair_coeff i j lambda [cut_short cut_long]
@@ -22,6 +23,7 @@
 #ifdef PAIR_CLASS
 // clang-format off
 PairStyle(vexcluded/gpu,PairExcludedVolumeGPU);
+PairStyle(excluded_volume/gpu,PairExcludedVolumeGPU);
 // clang-format on
 #else
 
