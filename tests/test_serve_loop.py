@@ -83,3 +83,48 @@ def test_stream_generators():
     L = serve.log_uniform_lengths(5000, 30, 1000, rng)
     assert L.min() >= 30 and L.max() <= 1000
     assert abs(np.median(L) - np.sqrt(30 * 1000)) < 25  # log-uniform: median is the geometric mean
+
+
+class PreparingServer(FakeServer):
+    """A fake handle that also prepares requests on the host (as AwsemServer):
+    the loop must prepare each request once, admit the prepared object in
+    arrival order and free every prepared object."""
+
+    class Prepared:
+        def __init__(self, chain, seed, log):
+            self.chain, self.seed, self.freed = chain, seed, False
+            log.append(self)
+
+        def free(self):
+            self.freed = True
+
+    def __init__(self, capacity):
+        super().__init__(capacity)
+        self.prepared = []
+
+    def prepare(self, chain, seed=1):
+        return PreparingServer.Prepared(chain, seed, self.prepared)
+
+    def admit(self, what, nsteps, t_start, t_stop, seed):
+        assert isinstance(what, PreparingServer.Prepared) and what.seed == seed and not what.freed
+        return super().admit(what.chain, nsteps, t_start, t_stop, seed)
+
+
+def test_prepared_admission_keeps_fifo_and_frees():
+    fake = PreparingServer(capacity=100)
+    reqs = [make(0, 0.0, 60, 10), make(1, 0.0, 60, 5), make(2, 0.0, 30, 3)]
+    for k, r in enumerate(reqs):
+        r.seed = 40 + k
+    t = [0.0]
+    done = serve.run_stream(fake, reqs, chunk=4, clock=lambda: t[0], sleep=lambda s: None)
+    assert fake.admitted == [0, 1, 2]
+    assert sorted(d.rid for d in done) == [0, 1, 2]
+    assert len(fake.prepared) == 3 and all(p.freed for p in fake.prepared)
+
+
+def test_request_that_never_fits_is_refused():
+    import pytest
+
+    fake = FakeServer(capacity=50)
+    with pytest.raises(ValueError, match="does not fit"):
+        serve.run_stream(fake, [make(0, 0.0, 60, 10)], chunk=4, clock=lambda: 0.0, sleep=lambda s: None)
