@@ -156,3 +156,26 @@ def test_oracle_q_matches_reference(name, tmp_path, oracle_built):
                 assert abs(got - want) <= 1e-12 * max(abs(want), 1e-3), (str(words), got, want)
     finally:
         os.chdir(cwd)
+
+
+@pytest.mark.skipif(not os.path.isdir(REFERENCE_SRC), reason="reference tree not present")
+@pytest.mark.parametrize("L", [2, 3, 5, 8, 9, 10])
+def test_oracle_matches_reference_on_short_chains(L, tmp_path, oracle_built):
+    """Chains of 2 to 10 residues (no fragment-memory window below 9
+    residues): the edge cases of the ragged GPU batch
+    (tests/test_gpu_ragged.py), pinned to the reference here."""
+    import ref
+    from awsemmd_b200 import synth
+
+    c = synth.chain_arrays(L, seed=500 + L, n_mem_per_window=2)
+    files = synth.write_chain_arrays(c, str(tmp_path / f"s{L}"))
+    r = ref.RefSystem(files)
+    fr = r.compute(0)
+    er = r.energies()
+    o = ref.OracleSystem(files)
+    x = r.get("x")
+    fo, eo = o.compute(x)
+    for k in range(20):
+        assert abs(eo[k] - er[k]) <= 1e-11 * max(abs(er[k]), 1e-3), (k, eo[k], er[k])
+    assert rel_err(fo, fr) < 1e-12
+    assert np.array_equal(np.sort(r.touches()), np.sort(o.selections(x, "touch")))
