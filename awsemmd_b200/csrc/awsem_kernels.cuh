@@ -1774,18 +1774,40 @@ struct Integrator {
 // replica follows its own run window (SlotRun); outside it the replica is
 // frozen, and residues of no replica are skipped.
 //
-// One component k = 3 b + c (bead b, axis c) of residue r; returns false
-// when the residue is not integrated at this step, else its kinetic-energy
-// term m v^2 (after the final half kick) in *ke.
+// Whether residue r is integrated at `step`, and its run-window values:
+// the thermostat temperature's square root and the Langevin stream's key
+// (the replica's own step count keys its noise).
 template <typename R>
-__device__ __forceinline__ bool finish_comp(const StepArgs<R> &a, const Integrator &in, long long step,
-                                            const double *g1, const double *g2, double *ftot, double *x_out, int r,
-                                            int k, double *ke)
+__device__ __forceinline__ bool finish_residue(const StepArgs<R> &a, const Integrator &in, long long step, int r,
+                                               double *tsqrt, uint64_t *nkey)
 {
   const int rep = a.res_sys[r];
   if (rep < 0) return false;
   const SlotRun sr = a.slot_run[rep];
   if (step < sr.begin || step > sr.end) return false;
+  if (in.langevin) {
+    // every multiply and add rounded on its own, as the x86-64 CPU build
+    // computes fix langevin
+    const double delta = sr.end != sr.begin ? (double) (step - sr.begin) / (double) (sr.end - sr.begin) : 0.0;
+    *tsqrt = sqrt(__dadd_rn(sr.t_start, __dmul_rn(delta, __dsub_rn(sr.t_stop, sr.t_start))));
+    *nkey = uniform_key(a.sys_seed[rep], step - sr.step0);
+  } else {
+    *tsqrt = 0.0;
+    *nkey = 0ull;
+  }
+  return true;
+}
+
+// One component k = 3 b + c (bead b, axis c) of an integrated residue r,
+// given its atom's dtfm = dtf / m and the residue's window values; writes
+// its kinetic-energy term m v^2 (after the final half kick) to *ke.
+template <typename R>
+__device__ __forceinline__ void finish_comp(const StepArgs<R> &a, const Integrator &in, long long step,
+                                            const double *g1, const double *g2, double *ftot, double *x_out, int r,
+                                            int k, double dtfm, double tsqrt, uint64_t nkey, double *ke)
+{
+  const int rep = a.res_sys[r];
+  const SlotRun sr = a.slot_run[rep];
   const bool final_kick = step > sr.begin, next = step < sr.end && step < in.stop;
   const size_t e = (size_t) 9 * r + k;  // element of the [atom][3] arrays
   if (a.lst_x0 && a.lst_build[rep]) a.lst_x0[e] = x_out[e];  // the emulated lists were built at these positions
@@ -1794,17 +1816,11 @@ __device__ __forceinline__ bool finish_comp(const StepArgs<R> &a, const Integrat
   // the x86-64 CPU build computes fix langevin / fix nve, and identically in
   // every kernel that inlines this.
   const double m = a.mass[at];
-  const double dtfm = in.dtf / m;
   double f = (double) (long long) a.s.facc[e] * F_UNSCALE;
   double v = a.v[e];
-  if (in.langevin) {
-    const double delta = sr.end != sr.begin ? (double) (step - sr.begin) / (double) (sr.end - sr.begin) : 0.0;
-    const double tsqrt = sqrt(__dadd_rn(sr.t_start, __dmul_rn(delta, __dsub_rn(sr.t_stop, sr.t_start))));
-    // the replica's own step count keys its noise
-    const uint64_t nkey = uniform_key(a.sys_seed[rep], step - sr.step0);
+  if (in.langevin)
     f = __dadd_rn(f, __dadd_rn(__dmul_rn(g1[at], v),
                                __dmul_rn(__dmul_rn(g2[at], tsqrt), __dsub_rn(uniform01_k(nkey, a.atom_tag[at], c), 0.5))));
-  }
   if (ftot) ftot[e] = f;
   if (final_kick) v = __dadd_rn(v, __dmul_rn(dtfm, f));
   *ke = __dmul_rn(__dmul_rn(m, v), v);
@@ -1813,7 +1829,6 @@ __device__ __forceinline__ bool finish_comp(const StepArgs<R> &a, const Integrat
     x_out[e] = __dadd_rn(x_out[e], __dmul_rn(in.dt, v));
   }
   a.v[e] = v;
-  return true;
 }
 
 // kinetic energy of a residue from its nine terms, summed in component order
@@ -1830,9 +1845,11 @@ template <typename R>
 __device__ __forceinline__ void finish_one(const StepArgs<R> &a, const Integrator &in, long long step, const double *g1,
                                            const double *g2, double *ftot, double *x_out, int r)
 {
-  double t[9];
+  double tsqrt, t[9];
+  uint64_t nkey;
+  if (!finish_residue(a, in, step, r, &tsqrt, &nkey)) return;
   for (int k = 0; k < 9; k++)
-    if (!finish_comp(a, in, step, g1, g2, ftot, x_out, r, k, &t[k])) return;
+    finish_comp(a, in, step, g1, g2, ftot, x_out, r, k, in.dtf / a.mass[3 * r + k / 3], tsqrt, nkey, &t[k]);
   a.e_res[(size_t) E_KIN * a.s.n_res + r] = kinetic(t);
 }
 
@@ -1847,25 +1864,39 @@ __device__ __forceinline__ void finish_pass(const StepArgs<R> &a, const Integrat
 
 // The standalone kernel: one thread per component (nine per residue, 32
 // residues per block), so that every array is read and written with
-// consecutive threads on consecutive elements; the residue's kinetic energy
-// is summed from shared memory in the same order as finish_one sums it.
-// Compiled for 4 blocks (36 warps) per SM.
+// consecutive threads on consecutive elements.  The values shared by a
+// residue (its window, the noise key) and by an atom (dtf / m) are formed
+// once into shared memory, by the same operations as finish_one forms them;
+// the residue's kinetic energy is summed from shared memory in the order
+// finish_one sums it.  Compiled for 4 blocks (36 warps) per SM.
 constexpr int kFinishRes = 32, kFinishThreads = 9 * kFinishRes;
 template <typename R>
 __global__ void __launch_bounds__(kFinishThreads, 4) k_finish(StepArgs<R> a, const Integrator *inp, const double *g1,
-                                                          const double *g2, double *ftot, double *x_out)
+                                                             const double *g2, double *ftot, double *x_out)
 {
-  __shared__ double kt[kFinishThreads];
+  __shared__ double kt[kFinishThreads], s_dtfm[3 * kFinishRes], s_tsqrt[kFinishRes];
+  __shared__ unsigned long long s_key[kFinishRes];
   __shared__ int on[kFinishRes];
   const Integrator in = *inp;
   const long long step = *a.step;
   const int lr = threadIdx.x / 9, k = threadIdx.x - 9 * lr;
   for (int r0 = blockIdx.x * kFinishRes; r0 < a.n_run; r0 += gridDim.x * kFinishRes) {
+    if (threadIdx.x < kFinishRes) {
+      const int r = r0 + threadIdx.x;
+      double tsqrt = 0.0;
+      uint64_t nkey = 0ull;
+      on[threadIdx.x] = r < a.n_run && finish_residue(a, in, step, r, &tsqrt, &nkey);
+      s_tsqrt[threadIdx.x] = tsqrt;
+      s_key[threadIdx.x] = nkey;
+    } else if (threadIdx.x < 4 * kFinishRes) {
+      const int at = 3 * r0 + (int) threadIdx.x - kFinishRes;
+      s_dtfm[threadIdx.x - kFinishRes] = at < 3 * a.n_run ? in.dtf / a.mass[at] : 0.0;
+    }
+    __syncthreads();
     const int r = r0 + lr;
     double t = 0.0;
-    const bool act = r < a.n_run && finish_comp(a, in, step, g1, g2, ftot, x_out, r, k, &t);
+    if (on[lr]) finish_comp(a, in, step, g1, g2, ftot, x_out, r, k, s_dtfm[3 * lr + k / 3], s_tsqrt[lr], s_key[lr], &t);
     kt[threadIdx.x] = t;
-    if (k == 0) on[lr] = act;
     __syncthreads();
     if (threadIdx.x < kFinishRes && on[threadIdx.x])
       a.e_res[(size_t) E_KIN * a.s.n_res + r0 + threadIdx.x] = kinetic(kt + 9 * threadIdx.x);
