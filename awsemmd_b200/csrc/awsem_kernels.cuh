@@ -1,22 +1,32 @@
 // Per-step kernels of the AWSEM engine (sm_100a).
 //
-// One MD step is this chain of launches (captured into a CUDA graph):
+// One MD step is this set of launches (captured into a CUDA graph), on three
+// streams joined before `finish`:
 //   prepare      thread/residue: CA, CB, O -> working copy + virtual N, H, C'
-//                (fix_backbone.cpp:7067-7138); zero forces; list-check data
+//                (fix_backbone.cpp:7067-7138) and the contact-bead copy;
+//                zero forces; list-check data
 //   nl_decide    1 thread: rebuild decision for the residue pair list
 //   nl_build     warp/residue: pairs i < j of contact beads within the list
 //                radius, appended to a flat pair array
-//   density      thread/pair: rho_water, rho_helix (DL1, :7728-7791)
-//   residue      thread/residue: switching functions, burial (SL, :7795-7841),
-//                helical (i,i+4) pairs (:7843-7868), chain/chi/rama,
-//                harmonic bonds
-//   water_xi     thread/pair: xi_water (DL2, :7877-7954)
-//   pair         thread/pair: water/burial/helix radial forces, excluded
-//                volume (DL3, :7956-8134); queues DSSP and P_AP pairs
+// first stream:
+//   density      warp/list segment: rho_water, rho_helix (DL1, :7728-7791);
+//                writes the near list
+//   residue      thread/residue: switching functions, burial (SL,
+//                :7795-7841), helical (i,i+4) pairs (:7843-7868), harmonic
+//                bonds, excluded volume inside the residue
+//   water_xi     thread/near pair: xi_water (DL2, :7877-7954)
+//   radial       thread/near pair: water/burial/helix radial forces (DL3,
+//                :7956-8057)
+// third stream:
+//   backbone     thread/residue: chain, chi, rama (:2062-2546)
+//   pair         thread/near pair: DSSP and P_AP detection into queues,
+//                excluded volume between residues (DL3, :8064-8103)
 //   hbond        thread/queued pair: DSSP hydrogen bonds, P_AP
+// second stream:
 //   fragmem      warp/32 residues, lane/residue row: fragment-memory
-//                Gaussians (:4079-4177), on a second stream
-//   finish       thread/residue: fixed-point -> FP64 forces, Langevin,
+//                Gaussians (:4079-4177)
+// then
+//   finish       thread/component: fixed-point -> FP64 forces, Langevin,
 //                velocity-Verlet half kicks and drift
 // Residue-owned quantities are written by their owner without atomics;
 // sums over pairs (forces, densities, pair energies) use 64-bit integer
@@ -552,9 +562,9 @@ template <typename R> __global__ void k_grid_fill(StepArgs<R> a, GridArgs g)
 // the candidates twice (count, then write after one atomic reservation), so
 // a residue's pairs are contiguous.  Candidates: the higher residues of its
 // replica, or for a gridded replica the residues of the 27 cells around its
-// own.  Every pair pass below runs one thread per listed pair and scatters to
-// both residues with fixed-point atomics: each pair is evaluated once, as in
-// the reference's half neighbour list.
+// own.  Every pair pass below runs one thread per listed (or near) pair and
+// scatters to both residues with fixed-point atomics: each pair is evaluated
+// once, as in the reference's half neighbour list.
 template <typename R> __device__ __forceinline__ void nl_build_one(const StepArgs<R> &a, const GridArgs &g, int i,
                                                                int lane)
 {
