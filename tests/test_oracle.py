@@ -179,3 +179,30 @@ def test_oracle_matches_reference_on_short_chains(L, tmp_path, oracle_built):
         assert abs(eo[k] - er[k]) <= 1e-11 * max(abs(er[k]), 1e-3), (k, eo[k], er[k])
     assert rel_err(fo, fr) < 1e-12
     assert np.array_equal(np.sort(r.touches()), np.sort(o.selections(x, "touch")))
+
+
+@pytest.mark.skipif(not os.path.isdir(REFERENCE_SRC), reason="reference tree not present")
+def test_oracle_matches_reference_on_longest_config3_replica(tmp_path, oracle_built):
+    """The benchmark workload's longest replica (500 residues, 20 memories
+    per 9-residue window, the seed the benchmark gives it): the oracle that
+    the GPU's configuration-3 sample is compared with
+    (tests/test_gpu_c3_sample.py) equals the compiled reference on it --
+    energies, forces and the reference's cache entries (selections)."""
+    import ref
+    from awsemmd_b200 import synth
+
+    lens = synth.replica_lengths(n=1024)
+    k = int(np.argmax(lens))
+    assert lens[k] == 500
+    c = synth.chain_arrays(lens[k], 3000 + k)
+    files = synth.write_chain_arrays(c, str(tmp_path / "r"))
+    r = ref.RefSystem(files)
+    fr = r.compute(0)
+    er = r.energies()
+    o = ref.OracleSystem(files)
+    x = r.get("x")
+    fo, eo = o.compute(x)
+    for i in range(20):
+        assert abs(eo[i] - er[i]) <= 1e-11 * max(abs(er[i]), 1e-3), (i, eo[i], er[i])
+    assert rel_err(fo, fr) < 1e-12
+    assert np.array_equal(np.sort(r.touches()), np.sort(o.selections(x, "touch")))
